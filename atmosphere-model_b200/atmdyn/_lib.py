@@ -1,0 +1,85 @@
+"""ctypes binding of libatmdyn.so (the C ABI declared in include/atmdyn.h).
+
+The library is built in-tree by ``make -C atmosphere-model_b200/csrc`` (or
+``__graft_entry__.build()``).  There is no fallback: if the shared library is
+missing or a CUDA call fails, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libatmdyn.so')
+CSRC = os.path.join(os.path.dirname(HERE), 'csrc')
+
+ATM_DP, ATM_PT, ATM_UD, ATM_VD, ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX = range(8)
+ATM_DPC, ATM_PTC, ATM_UC, ATM_VC = range(8, 12)
+ATM_FP64, ATM_MIXED = 0, 1
+STATUS = {0: 'ATM_OK', 1: 'ATM_ERR_ARG', 2: 'ATM_ERR_CUDA', 3: 'ATM_ERR_STATE',
+          4: 'ATM_ERR_NOMEM', 5: 'ATM_ERR_UNSUPPORTED'}
+
+# every entry point of include/atmdyn.h
+EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_step', 'atm_cgrid_halo',
+           'atm_dgrid_step', 'atm_remap', 'atm_dgrid_halo', 'atm_check_stability', 'atm_mass',
+           'atm_set_net_flux', 'atm_step', 'atm_sync', 'atm_destroy', 'atm_last_error',
+           'atm_upload_device', 'atm_download_device', 'atm_set_stream', 'atm_remap_trace',
+           'atm_device_pow_log', 'atm_version')
+
+_lib = None
+
+
+class AtmError(RuntimeError):
+    pass
+
+
+def build():
+    subprocess.run(['make', '-s', '-C', CSRC], check=True)
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise AtmError('libatmdyn.so is not built (run make -C %s)' % CSRC)
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER(ctypes.c_double)
+    vp = ctypes.c_void_p
+    i = ctypes.c_int
+    d = ctypes.c_double
+    lib.atm_create.argtypes = [ctypes.POINTER(vp), i, i, i, d, d, P, P, d, d, d, d, i, i]
+    lib.atm_upload.argtypes = [vp, i, P]
+    lib.atm_download.argtypes = [vp, i, P]
+    for f in ('atm_init', 'atm_cgrid_halo', 'atm_remap', 'atm_dgrid_halo', 'atm_sync', 'atm_destroy'):
+        getattr(lib, f).argtypes = [vp]
+    lib.atm_cgrid_step.argtypes = [vp, d]
+    lib.atm_dgrid_step.argtypes = [vp, d]
+    lib.atm_check_stability.argtypes = [vp, ctypes.POINTER(i)]
+    lib.atm_mass.argtypes = [vp, P]
+    lib.atm_set_net_flux.argtypes = [vp, P]
+    lib.atm_step.argtypes = [vp, d, i, ctypes.POINTER(i)]
+    lib.atm_last_error.argtypes = [vp]
+    lib.atm_last_error.restype = ctypes.c_char_p
+    lib.atm_upload_device.argtypes = [vp, i, vp, i]
+    lib.atm_download_device.argtypes = [vp, i, vp, i]
+    lib.atm_set_stream.argtypes = [vp, vp]
+    lib.atm_remap_trace.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(i)]
+    lib.atm_device_pow_log.argtypes = [P, d, P, P, i]
+    lib.atm_version.restype = ctypes.c_char_p
+    for f in EXPORTS:
+        getattr(lib, f)  # raises AttributeError if the symbol is missing
+    _lib = lib
+    return lib
+
+
+def check(rc: int, ctx=None, what: str = ''):
+    if rc != 0:
+        msg = ''
+        if ctx is not None and _lib is not None:
+            try:
+                msg = _lib.atm_last_error(ctx).decode()
+            except Exception:
+                msg = ''
+        raise AtmError('%s failed with %s %s' % (what, STATUS.get(rc, rc), msg))

@@ -1,0 +1,148 @@
+"""Host-side mirror of the reference's dycore interface over libatmdyn.
+
+:class:`Dycore` exposes the routines of src/mod_sw_dyn.f90:17-19 and
+src/mod_remap.f90:13 (``cgrid_step``/``cgrid_halo``/``dgrid_step``/
+``remap``/``dgrid_halo``) plus ``check_stability`` of src/mod_fields.f90:69,
+so :func:`atmdyn.model.run_model` drives it exactly like the reference's
+time loop drives the Fortran modules.  Fields are numpy arrays of shape
+(K, ny, nx) (interior) or (K, ny+14, nx+14) (with the 7-wide halo), the
+memory layout of the reference's Fortran arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import numpy as np
+
+from . import _lib
+from ._lib import check, ATM_DP, ATM_PT, ATM_UD, ATM_VD, ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX
+
+HALO = 7
+FIELDS = {'dp': ATM_DP, 'pt': ATM_PT, 'ud': ATM_UD, 'vd': ATM_VD, 'gz': ATM_GZ,
+          'plev': ATM_PLEV, 'pkap': ATM_PKAP, 'net_flux': ATM_NET_FLUX,
+          'dpc': 8, 'ptc': 9, 'uc': 10, 'vc': 11}
+_P = ctypes.POINTER(ctypes.c_double)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_P)
+
+
+def with_halo(interior: np.ndarray) -> np.ndarray:
+    """(K, ny, nx) interior -> (K, ny+14, nx+14) array with a zero halo."""
+    K, ny, nx = interior.shape
+    out = np.zeros((K, ny + 2 * HALO, nx + 2 * HALO))
+    out[:, HALO:HALO + ny, HALO:HALO + nx] = interior
+    return out
+
+
+class Dycore:
+    """One single-image dycore domain on the current CUDA device."""
+
+    def __init__(self, st, precision: str = 'fp64'):
+        self.lib = _lib.load()
+        self.st = st
+        self.nx, self.ny, self.nlay = st.nx, st.ny, st.nlay
+        self.precision = precision
+        ak = np.ascontiguousarray(st.ak, dtype=np.float64)
+        bk = np.ascontiguousarray(st.bk, dtype=np.float64)
+        ctx = ctypes.c_void_p()
+        prec = {'fp64': _lib.ATM_FP64, 'mixed': _lib.ATM_MIXED}[precision]
+        rc = self.lib.atm_create(ctypes.byref(ctx), st.nx, st.ny, st.nlay, st.dx, st.dy, _ptr(ak), _ptr(bk),
+                                 st.gravity, st.coriolis, st.divdamp, st.vortdamp, prec, 0)
+        check(rc, None, 'atm_create')
+        self.ctx = ctx
+        for f, a in ((ATM_DP, st.dp), (ATM_PT, st.pt), (ATM_UD, st.u), (ATM_VD, st.v)):
+            self.upload(f, with_halo(np.asarray(a, dtype=np.float64)))
+        gz = np.zeros((st.nlay + 1, st.ny, st.nx))
+        gz[0] = st.gzs
+        self.upload(ATM_GZ, with_halo(gz))
+        check(self.lib.atm_init(self.ctx), self.ctx, 'atm_init')
+
+    def close(self):
+        if getattr(self, 'ctx', None):
+            self.lib.atm_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def levels(self, field):
+        return self.nlay + 1 if field in (ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX) else self.nlay
+
+    def upload(self, field, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        check(self.lib.atm_upload(self.ctx, field, _ptr(a)), self.ctx, 'atm_upload')
+
+    def get(self, field, halo=False):
+        if isinstance(field, str):
+            field = FIELDS[field]
+        K = self.levels(field)
+        out = np.empty((K, self.ny + 2 * HALO, self.nx + 2 * HALO))
+        check(self.lib.atm_download(self.ctx, field, _ptr(out)), self.ctx, 'atm_download')
+        return out if halo else out[:, HALO:HALO + self.ny, HALO:HALO + self.nx].copy()
+
+    def set_net_flux(self, nf_halo):
+        if nf_halo is None:
+            check(self.lib.atm_set_net_flux(self.ctx, None), self.ctx, 'atm_set_net_flux')
+            return
+        a = np.ascontiguousarray(nf_halo, dtype=np.float64)
+        check(self.lib.atm_set_net_flux(self.ctx, _ptr(a)), self.ctx, 'atm_set_net_flux')
+
+    # the reference's dycore entry points
+    def cgrid_step(self, dt_half):
+        check(self.lib.atm_cgrid_step(self.ctx, dt_half), self.ctx, 'atm_cgrid_step')
+
+    def cgrid_halo(self):
+        check(self.lib.atm_cgrid_halo(self.ctx), self.ctx, 'atm_cgrid_halo')
+
+    def dgrid_step(self, dt):
+        check(self.lib.atm_dgrid_step(self.ctx, dt), self.ctx, 'atm_dgrid_step')
+
+    def remap(self):
+        check(self.lib.atm_remap(self.ctx), self.ctx, 'atm_remap')
+
+    def dgrid_halo(self):
+        check(self.lib.atm_dgrid_halo(self.ctx), self.ctx, 'atm_dgrid_halo')
+
+    def check_stability(self):
+        s = ctypes.c_int(0)
+        check(self.lib.atm_check_stability(self.ctx, ctypes.byref(s)), self.ctx, 'atm_check_stability')
+        return bool(s.value)
+
+    def step(self, dt, remap=False, check_stable=True):
+        s = ctypes.c_int(1)
+        check(self.lib.atm_step(self.ctx, dt, int(remap), ctypes.byref(s) if check_stable else None),
+              self.ctx, 'atm_step')
+        return bool(s.value)
+
+    def mass(self):
+        m = ctypes.c_double(0.)
+        check(self.lib.atm_mass(self.ctx, ctypes.byref(m)), self.ctx, 'atm_mass')
+        return m.value
+
+    def sync(self):
+        check(self.lib.atm_sync(self.ctx), self.ctx, 'atm_sync')
+
+    def remap_trace(self):
+        """Arm the pair trace for the next remap; returns (buffer, fallback)."""
+        buf = np.full((3, self.ny + 2, self.nx + 2, self.nlay, 5), -1, dtype=np.int32)
+        fb = ctypes.c_int(0)
+        self._trace_keep = (buf, fb)
+        check(self.lib.atm_remap_trace(self.ctx, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                       ctypes.byref(fb)), self.ctx, 'atm_remap_trace')
+        return buf, fb
+
+    def state(self):
+        return {name: self.get(f) for name, f in (('dp', ATM_DP), ('pt', ATM_PT), ('ud', ATM_UD), ('vd', ATM_VD))}
+
+
+def device_pow_log(x, y):
+    lib = _lib.load()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    p = np.empty_like(x)
+    lg = np.empty_like(x)
+    check(lib.atm_device_pow_log(_ptr(x), float(y), _ptr(p), _ptr(lg), x.size), None, 'atm_device_pow_log')
+    return p, lg

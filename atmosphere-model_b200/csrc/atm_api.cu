@@ -1,0 +1,581 @@
+// C-ABI of the B200 dynamical core (declarations and reference citations in
+// include/atmdyn.h).  One context = one single-image domain on one device:
+// all fields live in HBM with the reference's 7-wide halo, ping-pong
+// buffers hold two time levels of the prognostic state, and every entry
+// point enqueues kernels on the context's stream.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "atmdyn.h"
+#include "atm_ops.h"
+
+using atm::Geom;
+using atm::H;
+using atm::XOFF;
+
+namespace {
+
+enum { F_DP = 0, F_PT = 1, F_UD = 2, F_VD = 3 };
+enum { C_DPC = 0, C_PTC = 1, C_UC = 2, C_VC = 3 };
+
+// interior <-> contiguous (K, ny, nx) device buffer, with type conversion
+template <typename A, typename B>
+__global__ void k_interior(Geom g, const A* __restrict__ src, B* __restrict__ dst, int K, int to_field) {
+  long long n = (long long)g.nx * g.ny * K;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % g.nx);
+    long long r = q / g.nx;
+    int j = (int)(r % g.ny);
+    int k = (int)(r / g.ny);
+    long long o = g.at(i, j, k);
+    if (to_field)
+      dst[o] = B(src[q]);
+    else
+      dst[q] = B(src[o]);
+  }
+}
+
+__global__ void k_fill(double* p, long long n, double v) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    p[q] = v;
+}
+
+}  // namespace
+
+struct atm_ctx {
+  int nx = 0, ny = 0, L = 0, precision = 0, flags = 0;
+  double dx = 0, dy = 0;
+  std::vector<double> ak, bk;
+  Geom geo{};
+  atm::Consts cst{};
+  const atm::Ops* ops = nullptr;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  void* st[2][4] = {{nullptr}};
+  int cur = 0;
+  void* cg[4] = {nullptr};
+  double *pkap = nullptr, *gz = nullptr, *pkapb = nullptr, *gzb = nullptr, *stage = nullptr;
+  void *urem = nullptr, *vrem = nullptr;
+  double *nf = nullptr, *heat = nullptr;
+  bool heating = false;
+  double *d_ak = nullptr, *d_bk = nullptr, *partial = nullptr, *d_mass = nullptr;
+  atm::Status* status = nullptr;
+  atm::Status* h_status = nullptr;  // pinned
+  double* h_mass = nullptr;         // pinned
+  int uploaded = 0;
+  bool initialized = false;
+  bool flag_valid = false;
+  bool remapped = false;
+  int32_t* trace_host = nullptr;
+  int* trace_fallback = nullptr;
+  int* d_trace = nullptr;
+  size_t trace_elems = 0;
+  std::string err;
+};
+
+namespace {
+
+const int MASS_BLOCKS = 296;
+
+int fail(atm_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(atm_ctx* c, const char* what, cudaError_t e) {
+  return fail(c, ATM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                               \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, #call, e_);   \
+  } while (0)
+
+int field_levels(const atm_ctx* c, int f) {
+  switch (f) {
+    case ATM_DP: case ATM_PT: case ATM_UD: case ATM_VD: return c->L;
+    case ATM_DPC: case ATM_PTC: case ATM_UC: case ATM_VC: return c->L;
+    case ATM_GZ: case ATM_PLEV: case ATM_PKAP: case ATM_NET_FLUX: return c->L + 1;
+    default: return -1;
+  }
+}
+
+size_t level_elems(const atm_ctx* c) { return (size_t)c->geo.S; }
+
+atm::Consts step_consts(const atm_ctx* c, double dt) {
+  atm::Consts k = c->cst;
+  k.dt = dt;
+  k.dtdx = dt * k.rdx;  // mod_sw_dyn.f90:85-86,429-430
+  k.dtdy = dt * k.rdy;
+  return k;
+}
+
+atm::RemapArgs remap_args(const atm_ctx* c) {
+  return atm::RemapArgs{c->d_ak, c->d_bk, c->cst.ptop, c->cst.pk_top};
+}
+
+void free_all(atm_ctx* c) {
+  for (int t = 0; t < 2; ++t)
+    for (int f = 0; f < 4; ++f) cudaFree(c->st[t][f]);
+  for (int f = 0; f < 4; ++f) cudaFree(c->cg[f]);
+  void* ps[] = {c->pkap, c->gz, c->pkapb, c->gzb, c->stage, c->urem, c->vrem, c->nf, c->heat,
+                c->d_ak, c->d_bk, c->partial, c->d_mass, c->status, c->d_trace};
+  for (void* p : ps) cudaFree(p);
+  if (c->h_status) cudaFreeHost(c->h_status);
+  if (c->h_mass) cudaFreeHost(c->h_mass);
+  if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
+}
+
+// host (is:ie, js:je, 1:K) FP64 array <-> pitched FP64 device array
+cudaError_t h2d_pitched(atm_ctx* c, double* dev, const double* host, int K) {
+  const int wrow = c->nx + 2 * H;
+  return cudaMemcpy2DAsync(dev + XOFF, (size_t)c->geo.P * 8, host, (size_t)wrow * 8, (size_t)wrow * 8,
+                           (size_t)c->geo.NYP * K, cudaMemcpyHostToDevice, c->stream);
+}
+cudaError_t d2h_pitched(atm_ctx* c, double* host, const double* dev, int K) {
+  const int wrow = c->nx + 2 * H;
+  return cudaMemcpy2DAsync(host, (size_t)wrow * 8, dev + XOFF, (size_t)c->geo.P * 8, (size_t)wrow * 8,
+                           (size_t)c->geo.NYP * K, cudaMemcpyDeviceToHost, c->stream);
+}
+
+int require_init(atm_ctx* c) {
+  if (!c) return ATM_ERR_ARG;
+  if (!c->initialized) return fail(c, ATM_ERR_STATE, "atm_init has not been called");
+  return ATM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* atm_version(void) { return "libatmdyn 0.1 (sm_100a)"; }
+
+const char* atm_last_error(atm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int atm_create(atm_ctx** out, int nx, int ny, int nlay, double dx, double dy, const double* ak, const double* bk,
+               double g, double f, double divdamp, double vortdamp, int precision, int flags) {
+  if (!out) return ATM_ERR_ARG;
+  *out = nullptr;
+  if (nx < H || ny < H || nlay < 3 || nlay > atm::MAX_LAYERS || !(dx > 0) || !(dy > 0) || !ak || !bk ||
+      (precision != ATM_FP64 && precision != ATM_MIXED))
+    return ATM_ERR_ARG;
+  atm_ctx* ctx = new atm_ctx();
+  ctx->nx = nx; ctx->ny = ny; ctx->L = nlay; ctx->dx = dx; ctx->dy = dy;
+  ctx->precision = precision; ctx->flags = flags;
+  ctx->ak.assign(ak, ak + nlay + 1);
+  ctx->bk.assign(bk, bk + nlay + 1);
+  ctx->ops = precision == ATM_FP64 ? &atm::ops_fp64 : &atm::ops_mixed;
+  Geom& geo = ctx->geo;
+  geo.nx = nx; geo.ny = ny; geo.L = nlay;
+  geo.P = ((XOFF + nx + 2 * H) + 31) / 32 * 32;
+  geo.NYP = ny + 2 * H;
+  geo.S = (long long)geo.P * geo.NYP;
+  // init_sw_dyn, src/mod_sw_dyn.f90:961-1021
+  atm::Consts& k = ctx->cst;
+  k.rdx = 1. / dx;
+  k.rdx2 = 1. / (dx * dx);
+  k.rdy = 1. / dy;
+  k.rdy2 = 1. / (dy * dy);
+  k.rdx2rdy2 = k.rdx2 + k.rdy2;
+  k.rA = 1. / (dx * dy);
+  double dd = divdamp * dx * dy;
+  k.divdamp = dd * dd;
+  double vortdamp_coeff = vortdamp * dx * dy;
+  k.vdx = dy * k.rdx * vortdamp_coeff;
+  k.vdy = dx * k.rdy * vortdamp_coeff;
+  k.coriolis = f;
+  k.gravity = g;
+  k.ptop = ak[0];
+  k.pk_top = atm_pow(ak[0], atm::KAPPA);
+
+  cudaError_t e;
+  if ((e = cudaGetDevice(&ctx->device)) != cudaSuccess) { int r = cuda_fail(ctx, "cudaGetDevice", e); delete ctx; return r; }
+  if ((e = ctx->ops->setup()) != cudaSuccess) { int r = cuda_fail(ctx, "kernel set-up", e); delete ctx; return r; }
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    int r = cuda_fail(ctx, "cudaStreamCreate", e); delete ctx; return r;
+  }
+  const size_t es = (size_t)ctx->ops->elem;
+  const size_t lay = level_elems(ctx) * nlay * es;
+  const size_t lev = level_elems(ctx) * (nlay + 1) * 8;
+  bool ok = true;
+  auto alloc = [&](void** p, size_t bytes) {
+    if (!ok) return;
+    if (cudaMalloc(p, bytes) != cudaSuccess) { ok = false; return; }
+    if (cudaMemset(*p, 0, bytes) != cudaSuccess) ok = false;
+  };
+  for (int t = 0; t < 2; ++t)
+    for (int fi = 0; fi < 4; ++fi) alloc(&ctx->st[t][fi], lay);
+  for (int fi = 0; fi < 4; ++fi) alloc(&ctx->cg[fi], lay);
+  alloc(&ctx->urem, lay);
+  alloc(&ctx->vrem, lay);
+  alloc((void**)&ctx->pkap, lev);
+  alloc((void**)&ctx->gz, lev);
+  alloc((void**)&ctx->pkapb, lev);
+  alloc((void**)&ctx->gzb, lev);
+  alloc((void**)&ctx->stage, lev);
+  alloc((void**)&ctx->d_ak, (nlay + 1) * 8);
+  alloc((void**)&ctx->d_bk, (nlay + 1) * 8);
+  alloc((void**)&ctx->partial, MASS_BLOCKS * 8);
+  alloc((void**)&ctx->d_mass, 8);
+  alloc((void**)&ctx->status, sizeof(atm::Status));
+  if (ok && cudaMallocHost((void**)&ctx->h_status, sizeof(atm::Status)) != cudaSuccess) ok = false;
+  if (ok && cudaMallocHost((void**)&ctx->h_mass, 8) != cudaSuccess) ok = false;
+  if (!ok) {
+    cudaGetLastError();
+    free_all(ctx);
+    delete ctx;
+    return ATM_ERR_NOMEM;
+  }
+  if (cudaMemcpy(ctx->d_ak, ak, (nlay + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(ctx->d_bk, bk, (nlay + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+    free_all(ctx);
+    delete ctx;
+    return ATM_ERR_CUDA;
+  }
+  *out = ctx;
+  return ATM_OK;
+}
+
+int atm_destroy(atm_ctx* ctx) {
+  if (!ctx) return ATM_ERR_ARG;
+  cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  delete ctx;
+  return ATM_OK;
+}
+
+int atm_set_stream(atm_ctx* ctx, void* stream) {
+  if (!ctx) return ATM_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->own_stream) CK(cudaStreamDestroy(ctx->stream));
+  if (stream) {
+    ctx->stream = (cudaStream_t)stream;
+    ctx->own_stream = false;
+  } else {
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->own_stream = true;
+  }
+  return ATM_OK;
+}
+
+int atm_upload(atm_ctx* ctx, int field, const double* host) {
+  if (!ctx || !host) return ATM_ERR_ARG;
+  const atm::Ops& ops = *ctx->ops;
+  if (field >= ATM_DP && field <= ATM_VD) {
+    void* dst = ctx->st[ctx->cur][field];
+    if (ctx->precision == ATM_FP64) {
+      CK(h2d_pitched(ctx, (double*)dst, host, ctx->L));
+    } else {
+      CK(h2d_pitched(ctx, ctx->stage, host, ctx->L));
+      CK(ops.from_double(ctx->stage, dst, ctx->geo.S * ctx->L, ctx->stream));
+    }
+  } else if (field == ATM_GZ) {
+    CK(h2d_pitched(ctx, ctx->gz, host, 1));  // level 1: surface geopotential
+  } else if (field == ATM_NET_FLUX) {
+    return atm_set_net_flux(ctx, host);
+  } else {
+    return fail(ctx, ATM_ERR_ARG, "field cannot be uploaded");
+  }
+  ctx->uploaded |= 1 << field;
+  ctx->flag_valid = false;
+  return ATM_OK;
+}
+
+int atm_upload_device(atm_ctx* ctx, int field, const void* dev, int dtype_bytes) {
+  if (!ctx || !dev || (dtype_bytes != 4 && dtype_bytes != 8)) return ATM_ERR_ARG;
+  if (field < ATM_DP || field > ATM_GZ) return fail(ctx, ATM_ERR_ARG, "field cannot be uploaded");
+  const int K = field == ATM_GZ ? 1 : ctx->L;
+  const bool dbl_field = field == ATM_GZ || ctx->precision == ATM_FP64;
+  void* dst = field == ATM_GZ ? (void*)ctx->gz : ctx->st[ctx->cur][field];
+  dim3 grid(1184), block(256);
+  if (dbl_field && dtype_bytes == 8) k_interior<double, double><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const double*)dev, (double*)dst, K, 1);
+  else if (dbl_field) k_interior<float, double><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const float*)dev, (double*)dst, K, 1);
+  else if (dtype_bytes == 8) k_interior<double, float><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const double*)dev, (float*)dst, K, 1);
+  else k_interior<float, float><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const float*)dev, (float*)dst, K, 1);
+  CK(cudaGetLastError());
+  // the halo of a device upload is the periodic image of the interior
+  if (field == ATM_GZ) {
+    void* f1[1] = {ctx->gz};
+    CK(atm::ops_fp64.ring(ctx->geo, f1, nullptr, 1, 1, false, ctx->stream));
+  } else {
+    void* f1[1] = {dst};
+    CK(ctx->ops->ring(ctx->geo, f1, nullptr, 1, ctx->L, false, ctx->stream));
+  }
+  ctx->uploaded |= 1 << field;
+  ctx->flag_valid = false;
+  return ATM_OK;
+}
+
+int atm_download_device(atm_ctx* ctx, int field, void* dev, int dtype_bytes) {
+  if (!ctx || !dev || (dtype_bytes != 4 && dtype_bytes != 8)) return ATM_ERR_ARG;
+  if (field < ATM_DP || field > ATM_VD) return fail(ctx, ATM_ERR_ARG, "only prognostic fields");
+  const bool dbl_field = ctx->precision == ATM_FP64;
+  const void* src = ctx->st[ctx->cur][field];
+  dim3 grid(1184), block(256);
+  if (dbl_field && dtype_bytes == 8) k_interior<double, double><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const double*)src, (double*)dev, ctx->L, 0);
+  else if (dbl_field) k_interior<double, float><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const double*)src, (float*)dev, ctx->L, 0);
+  else if (dtype_bytes == 8) k_interior<float, double><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const float*)src, (double*)dev, ctx->L, 0);
+  else k_interior<float, float><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const float*)src, (float*)dev, ctx->L, 0);
+  CK(cudaGetLastError());
+  return ATM_OK;
+}
+
+int atm_download(atm_ctx* ctx, int field, double* host) {
+  if (!ctx || !host) return ATM_ERR_ARG;
+  const atm::Ops& ops = *ctx->ops;
+  const int K = field_levels(ctx, field);
+  if (K < 0) return fail(ctx, ATM_ERR_ARG, "unknown field");
+  if ((field >= ATM_DP && field <= ATM_VD) || (field >= ATM_DPC && field <= ATM_VC)) {
+    const void* src = field <= ATM_VD ? ctx->st[ctx->cur][field] : ctx->cg[field - ATM_DPC];
+    if (ctx->precision == ATM_FP64) {
+      CK(d2h_pitched(ctx, host, (const double*)src, K));
+    } else {
+      CK(ops.to_double(src, ctx->stage, ctx->geo.S * K, ctx->stream));
+      CK(d2h_pitched(ctx, host, ctx->stage, K));
+    }
+  } else if (field == ATM_NET_FLUX) {
+    if (ctx->nf) {
+      CK(d2h_pitched(ctx, host, ctx->nf, K));
+    } else {
+      std::memset(host, 0, sizeof(double) * (size_t)(ctx->nx + 2 * H) * (ctx->ny + 2 * H) * K);
+      return ATM_OK;
+    }
+  } else {
+    // column diagnostics from the current dp and pt over the whole array
+    int r = require_init(ctx);
+    if (r) return r;
+    atm::Consts k = step_consts(ctx, 0.);
+    CK(ops.column(ctx->geo, k, ctx->st[ctx->cur][F_DP], ctx->st[ctx->cur][F_PT], ctx->pkap, ctx->gz, -H, H,
+                  ctx->stage, ctx->stream));
+    const double* src = field == ATM_PLEV ? ctx->stage : field == ATM_PKAP ? ctx->pkap : ctx->gz;
+    CK(d2h_pitched(ctx, host, src, K));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATM_OK;
+}
+
+int atm_set_net_flux(atm_ctx* ctx, const double* host) {
+  if (!ctx) return ATM_ERR_ARG;
+  if (!host) {
+    ctx->heating = false;
+    return ATM_OK;
+  }
+  const size_t lev = level_elems(ctx) * (ctx->L + 1) * 8;
+  if (!ctx->nf) {
+    CK(cudaMalloc((void**)&ctx->nf, lev));
+    CK(cudaMemset(ctx->nf, 0, lev));
+  }
+  if (!ctx->heat) {
+    CK(cudaMalloc((void**)&ctx->heat, lev));
+    CK(cudaMemset(ctx->heat, 0, lev));
+  }
+  CK(h2d_pitched(ctx, ctx->nf, host, ctx->L + 1));
+  ctx->heating = true;
+  return ATM_OK;
+}
+
+int atm_init(atm_ctx* ctx) {
+  if (!ctx) return ATM_ERR_ARG;
+  const int need = (1 << ATM_DP) | (1 << ATM_PT) | (1 << ATM_UD) | (1 << ATM_VD) | (1 << ATM_GZ);
+  if ((ctx->uploaded & need) != need) return fail(ctx, ATM_ERR_STATE, "upload dp, pt, ud, vd and gz before atm_init");
+  const Geom& g = ctx->geo;
+  // initial_halo_exchange (src/mod_input.f90:247): dp, pt, ud, vd and the
+  // surface geopotential
+  CK(ctx->ops->ring(g, ctx->st[ctx->cur], nullptr, 4, ctx->L, false, ctx->stream));
+  void* gz1[1] = {ctx->gz};
+  CK(atm::ops_fp64.ring(g, gz1, nullptr, 1, 1, false, ctx->stream));
+  // model-top constants: pkap(nlay+1) and pkapb(nlay+1) = Ak(1)**kappa
+  // (src/mod_input.f90:229-231, src/mod_sw_dyn.f90:991)
+  k_fill<<<148, 256, 0, ctx->stream>>>(ctx->pkap + g.S * ctx->L, g.S, ctx->cst.pk_top);
+  k_fill<<<148, 256, 0, ctx->stream>>>(ctx->pkapb + g.S * ctx->L, g.S, ctx->cst.pk_top);
+  CK(cudaGetLastError());
+  // gzb(:,:,1) from the surface geopotential, src/mod_sw_dyn.f90:995-996
+  CK(atm::corners(g, ctx->pkap, ctx->gz, ctx->pkapb, ctx->gzb, 0, 0, 1, ctx->stream));
+  ctx->initialized = true;
+  ctx->flag_valid = false;
+  return ATM_OK;
+}
+
+int atm_cgrid_step(atm_ctx* ctx, double dt_half) {
+  int r = require_init(ctx);
+  if (r) return r;
+  const atm::Ops& ops = *ctx->ops;
+  const Geom& g = ctx->geo;
+  atm::Consts k = step_consts(ctx, dt_half);
+  void* const* s = ctx->st[ctx->cur];
+  const double* heat = nullptr;
+  if (ctx->heating) {
+    CK(ops.heating(g, k, s[F_DP], ctx->nf, ctx->heat, ctx->stream));
+    heat = ctx->heat;
+  }
+  // dpc, ptc on is+5:ie-5 (src/mod_sw_dyn.f90:94-270)
+  CK(ops.mass(g, k, s[F_DP], s[F_PT], s[F_UD], s[F_VD], heat, ctx->cg[C_DPC], ctx->cg[C_PTC], -2, 2, nullptr, true,
+              ctx->stream));
+  // plev, pkap, gz (src/mod_sw_dyn.f90:276-292)
+  CK(ops.column(g, k, ctx->cg[C_DPC], ctx->cg[C_PTC], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+  // uc, vc (src/mod_sw_dyn.f90:294-414)
+  CK(ops.c_mom(g, k, s[F_UD], s[F_VD], ctx->pkap, ctx->gz, ctx->cg[C_UC], ctx->cg[C_VC], ctx->stream));
+  return ATM_OK;
+}
+
+int atm_cgrid_halo(atm_ctx* ctx) {
+  int r = require_init(ctx);
+  if (r) return r;
+  CK(ctx->ops->ring(ctx->geo, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
+  return ATM_OK;
+}
+
+int atm_dgrid_step(atm_ctx* ctx, double dt) {
+  int r = require_init(ctx);
+  if (r) return r;
+  const atm::Ops& ops = *ctx->ops;
+  const Geom& g = ctx->geo;
+  atm::Consts k = step_consts(ctx, dt);
+  const int old = ctx->cur, nxt = 1 - ctx->cur;
+  void* const* so = ctx->st[old];
+  void* const* sn = ctx->st[nxt];
+  const double* heat = nullptr;
+  if (ctx->heating) {
+    CK(ops.heating(g, k, ctx->cg[C_DPC], ctx->nf, ctx->heat, ctx->stream));  // from dpc, :433-464
+    heat = ctx->heat;
+  }
+  // the new time level keeps the old halo until the D-grid halo exchange
+  CK(ops.ring(g, ctx->st[nxt], (const void* const*)ctx->st[old], 4, ctx->L, true, ctx->stream));
+  CK(cudaMemsetAsync(&ctx->status->nonfinite_step, 0, sizeof(int), ctx->stream));
+  // dp, pt on is+4:ie-4 (src/mod_sw_dyn.f90:439-600)
+  CK(ops.mass(g, k, so[F_DP], so[F_PT], ctx->cg[C_UC], ctx->cg[C_VC], heat, sn[F_DP], sn[F_PT], -3, 3,
+              &ctx->status->nonfinite_step, false, ctx->stream));
+  // plev, pkap, gz, pkapb, gzb (src/mod_sw_dyn.f90:606-632)
+  CK(ops.column(g, k, sn[F_DP], sn[F_PT], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+  CK(atm::corners(g, ctx->pkap, ctx->gz, ctx->pkapb, ctx->gzb, 1, 0, ctx->L, ctx->stream));
+  // ud, vd on the interior (src/mod_sw_dyn.f90:634-771)
+  CK(ops.d_mom(g, k, so[F_UD], so[F_VD], ctx->cg[C_UC], ctx->cg[C_VC], ctx->pkapb, ctx->gzb, sn[F_UD], sn[F_VD],
+               &ctx->status->nonfinite_step, ctx->stream));
+  ctx->cur = nxt;
+  ctx->flag_valid = true;
+  ctx->remapped = false;
+  return ATM_OK;
+}
+
+int atm_remap(atm_ctx* ctx) {
+  int r = require_init(ctx);
+  if (r) return r;
+  const atm::Ops& ops = *ctx->ops;
+  const Geom& g = ctx->geo;
+  const int src = ctx->cur, dst = 1 - ctx->cur;
+  void* const* s = ctx->st[src];
+  void* const* d = ctx->st[dst];
+  // outside the interior the remapped fields keep the arrays' current values
+  CK(ops.ring(g, ctx->st[dst], (const void* const*)ctx->st[src], 4, ctx->L, true, ctx->stream));
+  CK(cudaMemsetAsync(&ctx->status->nonfinite_remap, 0, sizeof(int), ctx->stream));
+  CK(cudaMemsetAsync(&ctx->status->fallback_pairs, 0, sizeof(int), ctx->stream));
+  int* trace = nullptr;
+  if (ctx->trace_host) {
+    size_t n = (size_t)3 * (ctx->ny + 2) * (ctx->nx + 2) * ctx->L * 5;
+    if (n != ctx->trace_elems) {
+      cudaFree(ctx->d_trace);
+      ctx->d_trace = nullptr;
+      CK(cudaMalloc((void**)&ctx->d_trace, n * 4));
+      ctx->trace_elems = n;
+    }
+    CK(cudaMemsetAsync(ctx->d_trace, 0xff, n * 4, ctx->stream));
+    trace = ctx->d_trace;
+  }
+  atm::RemapArgs ra = remap_args(ctx);
+  CK(ops.remap_winds(g, ra, s[F_DP], s[F_UD], s[F_VD], ctx->urem, ctx->vrem, trace, ctx->status, ctx->stream));
+  CK(ops.remap_energy(g, ra, s[F_DP], s[F_PT], s[F_UD], s[F_VD], ctx->urem, ctx->vrem, ctx->gz, d[F_DP], d[F_PT],
+                      d[F_UD], d[F_VD], trace, ctx->status, ctx->stream));
+  ctx->cur = dst;
+  ctx->remapped = true;
+  if (ctx->trace_host) {
+    CK(cudaMemcpyAsync(ctx->trace_host, ctx->d_trace, ctx->trace_elems * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_status, ctx->status, sizeof(atm::Status), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->trace_fallback) *ctx->trace_fallback = ctx->h_status->fallback_pairs;
+    ctx->trace_host = nullptr;
+    ctx->trace_fallback = nullptr;
+  }
+  return ATM_OK;
+}
+
+int atm_dgrid_halo(atm_ctx* ctx) {
+  int r = require_init(ctx);
+  if (r) return r;
+  CK(ctx->ops->ring(ctx->geo, ctx->st[ctx->cur], nullptr, 4, ctx->L, false, ctx->stream));
+  return ATM_OK;
+}
+
+int atm_check_stability(atm_ctx* ctx, int* stable) {
+  if (!ctx || !stable) return ATM_ERR_ARG;
+  if (!ctx->flag_valid) {
+    CK(cudaMemsetAsync(&ctx->status->nonfinite_check, 0, sizeof(int), ctx->stream));
+    CK(ctx->ops->check_finite(ctx->geo, (const void* const*)ctx->st[ctx->cur], &ctx->status->nonfinite_check,
+                              ctx->stream));
+  }
+  CK(cudaMemcpyAsync(ctx->h_status, ctx->status, sizeof(atm::Status), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  int bad = !ctx->flag_valid ? ctx->h_status->nonfinite_check
+                             : (ctx->remapped ? ctx->h_status->nonfinite_remap : ctx->h_status->nonfinite_step);
+  *stable = bad ? 0 : 1;
+  return ATM_OK;
+}
+
+int atm_mass(atm_ctx* ctx, double* total) {
+  if (!ctx || !total) return ATM_ERR_ARG;
+  CK(ctx->ops->mass_sum(ctx->geo, ctx->st[ctx->cur][F_DP], ctx->partial, MASS_BLOCKS, ctx->d_mass, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->h_mass, ctx->d_mass, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *total = *ctx->h_mass;
+  return ATM_OK;
+}
+
+int atm_step(atm_ctx* ctx, double dt, int do_remap, int* stable) {
+  int r;
+  if ((r = atm_cgrid_step(ctx, dt / 2.))) return r;  // src/mod_model.f90:147
+  if ((r = atm_cgrid_halo(ctx))) return r;
+  if ((r = atm_dgrid_step(ctx, dt))) return r;
+  if (do_remap && (r = atm_remap(ctx))) return r;
+  if ((r = atm_dgrid_halo(ctx))) return r;
+  if (stable) return atm_check_stability(ctx, stable);
+  return ATM_OK;
+}
+
+int atm_sync(atm_ctx* ctx) {
+  if (!ctx) return ATM_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATM_OK;
+}
+
+int atm_remap_trace(atm_ctx* ctx, int32_t* buf, int* fallback_columns) {
+  if (!ctx) return ATM_ERR_ARG;
+  ctx->trace_host = buf;
+  ctx->trace_fallback = fallback_columns;
+  return ATM_OK;
+}
+
+int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_out, int n) {
+  if (n <= 0 || !x || !pow_out || !log_out) return ATM_ERR_ARG;
+  double *dx = nullptr, *dp = nullptr, *dl = nullptr;
+  size_t b = (size_t)n * 8;
+  if (cudaMalloc((void**)&dx, b) != cudaSuccess || cudaMalloc((void**)&dp, b) != cudaSuccess ||
+      cudaMalloc((void**)&dl, b) != cudaSuccess) {
+    cudaFree(dx); cudaFree(dp); cudaFree(dl);
+    return ATM_ERR_NOMEM;
+  }
+  int rc = ATM_OK;
+  if (cudaMemcpy(dx, x, b, cudaMemcpyHostToDevice) != cudaSuccess ||
+      atm::device_pow_log(dx, y, dp, dl, n, 0) != cudaSuccess ||
+      cudaMemcpy(pow_out, dp, b, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(log_out, dl, b, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = ATM_ERR_CUDA;
+  cudaFree(dx); cudaFree(dp); cudaFree(dl);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,55 @@
+// Precision-independent table of the device operations of one form of the
+// dynamical core.  atm_fp64.cu fills it for the FP64 form (compiled without
+// fused multiply-add so that it matches the FP64 restatement bit for bit),
+// atm_mixed.cu for the FP32-sweep form.  Buffers are passed as void* and
+// hold the form's sweep type; pressure, pkap and geopotential are double.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "atm_common.cuh"
+
+namespace atm {
+
+struct Ops {
+  int elem;  // bytes of the sweep type
+  cudaError_t (*setup)();
+  // C- or D-grid mass/potential-temperature sweep of every layer
+  cudaError_t (*mass)(const Geom&, const Consts&, const void* dp, const void* pt, const void* u, const void* v,
+                      const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, bool cgrid,
+                      cudaStream_t);
+  // plev/pkap/gz columns over [lo, n-1+hi]^2
+  cudaError_t (*column)(const Geom&, const Consts&, const void* dpl, const void* ptl, double* pkap, double* gz,
+                        int lo, int hi, double* plev, cudaStream_t);
+  cudaError_t (*heating)(const Geom&, const Consts&, const void* dpl, const double* net_flux, double* heat,
+                         cudaStream_t);
+  cudaError_t (*c_mom)(const Geom&, const Consts&, const void* ud, const void* vd, const double* pkap,
+                       const double* gz, void* uc, void* vc, cudaStream_t);
+  cudaError_t (*d_mom)(const Geom&, const Consts&, const void* ud, const void* vd, const void* uc, const void* vc,
+                       const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, cudaStream_t);
+  // periodic halo fill (copy = false) or ring copy src -> f (copy = true) of nf fields
+  cudaError_t (*ring)(const Geom&, void* const* f, const void* const* src, int nf, int K, bool copy, cudaStream_t);
+  cudaError_t (*remap_winds)(const Geom&, const RemapArgs&, const void* dp, const void* ud, const void* vd,
+                             void* urem, void* vrem, int* trace, Status*, cudaStream_t);
+  cudaError_t (*remap_energy)(const Geom&, const RemapArgs&, const void* dp, const void* pt, const void* ud,
+                              const void* vd, const void* urem, const void* vrem, const double* gzs, void* dpo,
+                              void* pto, void* udo, void* vdo, int* trace, Status*, cudaStream_t);
+  cudaError_t (*check_finite)(const Geom&, const void* const* f, int* flag, cudaStream_t);
+  cudaError_t (*mass_sum)(const Geom&, const void* dp, double* partial, int nblocks, double* out, cudaStream_t);
+  cudaError_t (*to_double)(const void* src, double* dst, long long n, cudaStream_t);
+  cudaError_t (*from_double)(const double* src, void* dst, long long n, cudaStream_t);
+};
+
+extern const Ops ops_fp64;
+extern const Ops ops_mixed;
+
+// interpolate_to_corners of pkap/gz (double in both forms)
+cudaError_t corners(const Geom&, const double* pkap, const double* gz, double* pkapb, double* gzb, int with_pkap,
+                    int lev0, int nlev, cudaStream_t);
+
+// x**y and log(x) of the portable math on the device (tests)
+cudaError_t device_pow_log(const double* x, double y, double* p, double* l, int n, cudaStream_t);
+
+// largest number of layers the vertical remap supports
+constexpr int MAX_LAYERS = 128;
+
+}  // namespace atm

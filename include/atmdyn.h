@@ -1,0 +1,164 @@
+/*
+ * libatmdyn -- B200 (sm_100a) dynamical-core step of
+ * felix-goddard/atmosphere-model behind a plain C ABI.
+ *
+ * The reference has no plugin API: its dycore is the Fortran module
+ * interface of mod_sw_dyn / mod_remap / mod_sync, whose routines take only
+ * dt and work on module-global arrays (src/mod_fields.f90:16-37).  Each
+ * entry point below replaces one of those routines; the Fortran host binds
+ * them through ISO_C_BINDING with the same call order
+ * as run_model (src/mod_model.f90:146-177).
+ *
+ * Conventions
+ *  - Every function returns an int status: ATM_OK (0) or an ATM_ERR_* code;
+ *    atm_last_error(ctx) returns a message for the last failure.  The
+ *    reference logs a fatal message and stops (src/mod_util.f90:13-19); the
+ *    Fortran wrapper does the same on a non-zero status.
+ *  - Host field arrays are the reference's allocatable arrays passed with
+ *    c_loc: FP64, Fortran order (i fastest), bounds (is:ie, js:je, 1:K) with
+ *    is = 1 - 7, ie = nx + 7, js = 1 - 7, je = ny + 7 (the single-image
+ *    tiling of src/mod_tiles.f90:222-241), K = nlay or nlay + 1 (see the
+ *    field table).  The library copies and keeps no host pointer.
+ *  - Device memory and one CUDA stream belong to the context; calls are
+ *    asynchronous on that stream until a download, atm_sync,
+ *    atm_check_stability or atm_mass.  A context is not thread-safe.
+ */
+#ifndef ATMDYN_H
+#define ATMDYN_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct atm_ctx atm_ctx;
+
+/* fields (host arrays are (is:ie, js:je, 1:K)) */
+enum {
+  ATM_DP = 0,        /* pressure thickness dp, K = nlay          (mod_fields.f90:17) */
+  ATM_PT = 1,        /* potential temperature pt, K = nlay       (:18) */
+  ATM_UD = 2,        /* D-grid u, K = nlay                        (:19) */
+  ATM_VD = 3,        /* D-grid v, K = nlay                        (:20) */
+  ATM_GZ = 4,        /* geopotential on interfaces, K = nlay + 1; level 1 is the
+                        surface geopotential gzs, the only level read on upload (:29) */
+  ATM_PLEV = 5,      /* interface pressure, K = nlay + 1 (download only; see below) */
+  ATM_PKAP = 6,      /* plev**kappa, K = nlay + 1 (download only) */
+  ATM_NET_FLUX = 7,  /* radiative net flux, K = nlay + 1 (upload via atm_set_net_flux) */
+  /* download only: the C-grid half step's arrays dpc, ptc, uc, vc, private
+     module variables of the reference (src/mod_sw_dyn.f90:23-27), K = nlay;
+     valid on the ranges cgrid_dynamics_step writes and, after
+     atm_cgrid_halo, everywhere */
+  ATM_DPC = 8, ATM_PTC = 9, ATM_UC = 10, ATM_VC = 11
+};
+
+/* forms */
+enum {
+  ATM_FP64 = 0,      /* the reference's FP64 arithmetic, bit-identical to the FP64 restatement */
+  ATM_MIXED = 1      /* FP32 horizontal sweeps, FP64 column sums / pkap / gz / remap / mass */
+};
+
+/* status codes */
+enum {
+  ATM_OK = 0,
+  ATM_ERR_ARG = 1,       /* invalid argument (sizes, field id, null pointer) */
+  ATM_ERR_CUDA = 2,      /* a CUDA call failed; the message names it */
+  ATM_ERR_STATE = 3,     /* call out of order (e.g. a step before atm_init) */
+  ATM_ERR_NOMEM = 4,     /* device allocation failed */
+  ATM_ERR_UNSUPPORTED = 5
+};
+
+/* flags for atm_create */
+#define ATM_FLAG_NONE 0
+
+/* init_sw_dyn + allocate_remapping_arrays + allocate_sync_buffers
+   (src/mod_sw_dyn.f90:958-1023, src/mod_remap.f90:358-388,
+   src/mod_sync.f90:219-230): allocates the device state for an
+   nx x ny x nlay single-image domain.  ak, bk: the hybrid coordinate,
+   nlay+1 entries (Ak(1) is the model-top pressure, src/mod_remap.f90:362).
+   g, f, divdamp, vortdamp: the physics_parameters namelist
+   (src/mod_config.f90:47-51, src/mod_constants.f90:20-27).
+   Requires nx, ny >= 7 and 3 <= nlay <= 128. */
+int atm_create(atm_ctx** out, int nx, int ny, int nlay, double dx, double dy, const double* ak,
+               const double* bk, double g, double f, double divdamp, double vortdamp,
+               int precision, int flags);
+
+/* copy a field from / to a host (is:ie, js:je, 1:K) FP64 array.  Upload
+   accepts ATM_DP, ATM_PT, ATM_UD, ATM_VD and ATM_GZ (level 1 only).
+   Download of ATM_PLEV / ATM_PKAP / ATM_GZ returns the column diagnostics
+   recomputed from the current dp and pt (plev = Ak(1) + suffix sum of dp,
+   pkap = plev**kappa, hydrostatic gz), on the whole array. */
+int atm_upload(atm_ctx* ctx, int field, const double* host);
+int atm_download(atm_ctx* ctx, int field, double* host);
+
+/* initial_halo_exchange (src/mod_input.f90:247-252) of dp, pt, gz, ud, vd
+   and the set-up that needs gz (src/mod_sw_dyn.f90:990-996).  Call after
+   the uploads and before the first step. */
+int atm_init(atm_ctx* ctx);
+
+/* cgrid_dynamics_step(dt) (src/mod_sw_dyn.f90:80-416); dt_half is the
+   argument the reference receives (run_model passes dt/2.). */
+int atm_cgrid_step(atm_ctx* ctx, double dt_half);
+/* cgrid_halo_exchange (src/mod_sw_dyn.f90:418-422): periodic halo fill */
+int atm_cgrid_halo(atm_ctx* ctx);
+/* dgrid_dynamics_step(dt) (src/mod_sw_dyn.f90:424-773) */
+int atm_dgrid_step(atm_ctx* ctx, double dt);
+/* perform_vertical_remapping (src/mod_remap.f90:27-163); call it where
+   run_model does, after the D-grid step and before the D-grid halo */
+int atm_remap(atm_ctx* ctx);
+/* dgrid_halo_exchange (src/mod_sw_dyn.f90:775-779): periodic halo fill */
+int atm_dgrid_halo(atm_ctx* ctx);
+
+/* check_stability (src/mod_fields.f90:69-106) with the co_reduce of
+   src/mod_model.f90:176: *stable = 1 when dp, pt, ud, vd are finite on the
+   interior.  Synchronises the stream. */
+int atm_check_stability(atm_ctx* ctx, int* stable);
+/* total mass: FP64 sum of the interior dp, in a fixed order (no reference
+   counterpart; conservation diagnostic).  Synchronises the stream. */
+int atm_mass(atm_ctx* ctx, double* total);
+/* net_flux, the radiative input of the heating term
+   (src/mod_sw_dyn.f90:103-106,461-464); a host (is:ie, js:je, 1:nlay+1)
+   array.  NULL restores the default of zero flux (no heating). */
+int atm_set_net_flux(atm_ctx* ctx, const double* host);
+
+/* one full model step as run_model orders it (src/mod_model.f90:146-177):
+   C-grid half step, halo, D-grid step, remap when do_remap != 0, halo; then
+   *stable as atm_check_stability when stable != NULL (no reference
+   counterpart as a single call; it is the sequence above). */
+int atm_step(atm_ctx* ctx, double dt, int do_remap, int* stable);
+
+int atm_sync(atm_ctx* ctx);
+int atm_destroy(atm_ctx* ctx);
+const char* atm_last_error(atm_ctx* ctx);
+
+/* ---- device-resident access (the PyTorch binding; no reference counterpart) ----
+   Copy a field between the context and a caller-owned device buffer holding
+   the interior only: FP64 (for ATM_FP64) or the form's sweep type, shape
+   (K, ny, nx) contiguous, i fastest.  Stream-ordered on the context's stream. */
+int atm_upload_device(atm_ctx* ctx, int field, const void* dev, int dtype_bytes);
+int atm_download_device(atm_ctx* ctx, int field, void* dev, int dtype_bytes);
+/* use an external CUDA stream (cudaStream_t passed as void*; NULL = own) */
+int atm_set_stream(atm_ctx* ctx, void* stream);
+
+/* ---- validation (no reference counterpart) ----
+   When buf != NULL, the next atm_remap also writes the set of contributing
+   source layers of every remap_column call into buf, a host int32 array
+   [3][ny+2][nx+2][nlay][5]: for variable 0 = u, 1 = v, 2 = energy, each
+   column of [isd-1, ied+1]^2 and each destination layer m, {first k, last k,
+   case of the first pair, case of the last pair, number of pairs}
+   (src/mod_remap.f90:176-283); columns a variable does not remap hold -1.
+   *fallback_columns (may be NULL) receives how many columns used the
+   reference's all-pairs search because a coordinate was not monotone. */
+int atm_remap_trace(atm_ctx* ctx, int32_t* buf, int* fallback_columns);
+
+/* the portable x**y and log(x) the FP64 form evaluates on the device, on n
+   host values (accuracy and bit-identity tests) */
+int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_out, int n);
+
+/* library version string */
+const char* atm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ATMDYN_H */

@@ -1,0 +1,148 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` use this module.  PARITY UNPINNED: see atm_oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+HALO = 7
+DP, PT, UD, VD, GZ, PLEV, PKAP, NET_FLUX, DPC, PTC, UC, VC = range(12)
+
+_libs: dict = {}
+_P = ctypes.POINTER(ctypes.c_double)
+
+
+def build():
+    subprocess.run(['make', '-s', '-C', HERE], check=True)
+
+
+def load(variant: str = 'portable'):
+    """variant: 'portable' (the pow/log the CUDA library reproduces bit for
+    bit), 'libm' (the C library's pow/log) or 'checked' (bounds checks)."""
+    if variant in _libs:
+        return _libs[variant]
+    name = {'portable': 'liboracle.so', 'libm': 'liboracle_libm.so',
+            'checked': 'liboracle_chk.so'}[variant]
+    path = os.path.join(HERE, name)
+    if not os.path.exists(path):
+        build()
+    lib = ctypes.CDLL(path)
+    lib.orc_create.restype = ctypes.c_void_p
+    lib.orc_create.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 2 + [_P, _P] + [ctypes.c_double] * 4
+    vp = [ctypes.c_void_p]
+    lib.orc_destroy.argtypes = vp
+    lib.orc_set_field.argtypes = vp + [ctypes.c_int, _P, ctypes.c_int]
+    lib.orc_get_field.argtypes = vp + [ctypes.c_int, _P, ctypes.c_int]
+    lib.orc_field_levels.argtypes = vp + [ctypes.c_int]
+    for f in ('orc_init', 'orc_cgrid_halo', 'orc_remap', 'orc_dgrid_halo'):
+        getattr(lib, f).argtypes = vp
+    lib.orc_cgrid_step.argtypes = vp + [ctypes.c_double]
+    lib.orc_dgrid_step.argtypes = vp + [ctypes.c_double]
+    lib.orc_check_stability.argtypes = vp
+    lib.orc_mass.argtypes = vp
+    lib.orc_mass.restype = ctypes.c_double
+    lib.orc_set_threads.argtypes = vp + [ctypes.c_int]
+    lib.orc_set_poison.argtypes = vp + [ctypes.c_int]
+    lib.orc_set_remap_trace.argtypes = vp + [ctypes.POINTER(ctypes.c_int32)]
+    lib.orc_pow_array.argtypes = [_P, ctypes.c_double, _P, ctypes.c_int]
+    lib.orc_log_array.argtypes = [_P, _P, ctypes.c_int]
+    _libs[variant] = lib
+    return lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_P)
+
+
+class OracleModel:
+    """The oracle with the stepper interface of atmdyn.model.run_model."""
+
+    def __init__(self, st, threads: int = 1, variant: str = 'portable', poison: bool = False):
+        self.lib = load(variant)
+        self.st = st
+        self.nx, self.ny, self.nlay = st.nx, st.ny, st.nlay
+        ak = np.ascontiguousarray(st.ak, dtype=np.float64)
+        bk = np.ascontiguousarray(st.bk, dtype=np.float64)
+        self.s = self.lib.orc_create(st.nx, st.ny, st.nlay, st.dx, st.dy, _ptr(ak), _ptr(bk),
+                                     st.gravity, st.coriolis, st.divdamp, st.vortdamp)
+        if not self.s:
+            raise ValueError('orc_create rejected the configuration')
+        self.lib.orc_set_threads(self.s, threads)
+        self.lib.orc_set_poison(self.s, int(poison))
+        for f, a in ((DP, st.dp), (PT, st.pt), (UD, st.u), (VD, st.v)):
+            self.set(f, a)
+        gz = np.zeros((st.nlay + 1, st.ny, st.nx))
+        gz[0] = st.gzs
+        self.set(GZ, gz)
+        self.lib.orc_init(self.s)
+        self._trace = None
+
+    def __del__(self):
+        if getattr(self, 's', None):
+            self.lib.orc_destroy(self.s)
+            self.s = None
+
+    def levels(self, field):
+        return self.lib.orc_field_levels(self.s, field)
+
+    def set(self, field, a, halo=False):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if self.lib.orc_set_field(self.s, field, _ptr(a), int(halo)) != 0:
+            raise ValueError('bad field')
+
+    def get(self, field, halo=False):
+        K = self.levels(field)
+        shape = (K, self.ny + 2 * HALO, self.nx + 2 * HALO) if halo else (K, self.ny, self.nx)
+        out = np.empty(shape)
+        self.lib.orc_get_field(self.s, field, _ptr(out), int(halo))
+        return out
+
+    # stepper interface
+    def cgrid_step(self, dt_half):
+        self.lib.orc_cgrid_step(self.s, dt_half)
+
+    def cgrid_halo(self):
+        self.lib.orc_cgrid_halo(self.s)
+
+    def dgrid_step(self, dt):
+        self.lib.orc_dgrid_step(self.s, dt)
+
+    def remap(self):
+        self.lib.orc_remap(self.s)
+
+    def dgrid_halo(self):
+        self.lib.orc_dgrid_halo(self.s)
+
+    def check_stability(self):
+        return bool(self.lib.orc_check_stability(self.s))
+
+    def mass(self):
+        return self.lib.orc_mass(self.s)
+
+    def enable_trace(self):
+        self._trace = np.full((3, self.ny + 2, self.nx + 2, self.nlay, 5), -1, dtype=np.int32)
+        self.lib.orc_set_remap_trace(self.s, self._trace.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        return self._trace
+
+    def state(self):
+        return {name: self.get(f) for name, f in (('dp', DP), ('pt', PT), ('ud', UD), ('vd', VD))}
+
+
+def pow_array(x, y, variant='portable'):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    load(variant).orc_pow_array(_ptr(x), float(y), _ptr(out), x.size)
+    return out
+
+
+def log_array(x, variant='portable'):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    load(variant).orc_log_array(_ptr(x), _ptr(out), x.size)
+    return out
