@@ -25,7 +25,8 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_dgrid_step', 'atm_remap', 'atm_dgrid_halo', 'atm_check_stability', 'atm_mass',
            'atm_set_net_flux', 'atm_step', 'atm_sync', 'atm_destroy', 'atm_last_error',
            'atm_upload_device', 'atm_download_device', 'atm_set_stream', 'atm_remap_trace',
-           'atm_device_pow_log', 'atm_version')
+           'atm_device_pow_log', 'atm_version', 'atm_profile', 'atm_profile_read', 'atm_profile_stage',
+           'atm_launch_count')
 
 _lib = None
 
@@ -68,6 +69,11 @@ def load():
     lib.atm_remap_trace.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(i)]
     lib.atm_device_pow_log.argtypes = [P, d, P, P, i]
     lib.atm_version.restype = ctypes.c_char_p
+    lib.atm_profile.argtypes = [vp, i]
+    lib.atm_profile_read.argtypes = [vp, P, ctypes.POINTER(i), i]
+    lib.atm_profile_stage.argtypes = [i]
+    lib.atm_profile_stage.restype = ctypes.c_char_p
+    lib.atm_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     for f in EXPORTS:
         getattr(lib, f)  # raises AttributeError if the symbol is missing
     _lib = lib

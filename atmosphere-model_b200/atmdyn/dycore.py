@@ -84,6 +84,16 @@ class Dycore:
         check(self.lib.atm_download(self.ctx, field, _ptr(out)), self.ctx, 'atm_download')
         return out if halo else out[:, HALO:HALO + self.ny, HALO:HALO + self.nx].copy()
 
+    def get_into(self, field, out):
+        """Download a field with its halo straight into ``out`` (a contiguous
+        float64 array of shape (K, ny+14, nx+14), e.g. pinned host memory)."""
+        if isinstance(field, str):
+            field = FIELDS[field]
+        assert out.dtype == np.float64 and out.flags.c_contiguous
+        assert out.shape == (self.levels(field), self.ny + 2 * HALO, self.nx + 2 * HALO)
+        check(self.lib.atm_download(self.ctx, field, _ptr(out)), self.ctx, 'atm_download')
+        return out
+
     def set_net_flux(self, nf_halo):
         if nf_halo is None:
             check(self.lib.atm_set_net_flux(self.ctx, None), self.ctx, 'atm_set_net_flux')
@@ -134,6 +144,34 @@ class Dycore:
         check(self.lib.atm_remap_trace(self.ctx, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                                        ctypes.byref(fb)), self.ctx, 'atm_remap_trace')
         return buf, fb
+
+    def set_stream(self, stream_ptr):
+        """Run on an external CUDA stream (an int cudaStream_t, or 0 for own)."""
+        check(self.lib.atm_set_stream(self.ctx, ctypes.c_void_p(stream_ptr or None)), self.ctx, 'atm_set_stream')
+
+    def profile(self, enable=True):
+        check(self.lib.atm_profile(self.ctx, int(enable)), self.ctx, 'atm_profile')
+
+    def profile_read(self):
+        """{stage: (total ms, launches)} since profile(True)."""
+        n = 0
+        names = []
+        while True:
+            nm = self.lib.atm_profile_stage(n)
+            if nm is None:
+                break
+            names.append(nm.decode())
+            n += 1
+        ms = np.zeros(n)
+        cnt = np.zeros(n, dtype=np.int32)
+        check(self.lib.atm_profile_read(self.ctx, _ptr(ms), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n),
+              self.ctx, 'atm_profile_read')
+        return {names[i]: (float(ms[i]), int(cnt[i])) for i in range(n)}
+
+    def launch_count(self):
+        v = ctypes.c_longlong(0)
+        check(self.lib.atm_launch_count(self.ctx, ctypes.byref(v)), self.ctx, 'atm_launch_count')
+        return v.value
 
     def state(self):
         return {name: self.get(f) for name, f in (('dp', ATM_DP), ('pt', ATM_PT), ('ud', ATM_UD), ('vd', ATM_VD))}

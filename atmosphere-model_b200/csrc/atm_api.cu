@@ -75,6 +75,12 @@ struct atm_ctx {
   int* trace_fallback = nullptr;
   int* d_trace = nullptr;
   size_t trace_elems = 0;
+  // per-stage CUDA-event timing (atm_profile) and the kernel launch counter
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_stage;  // stage of each recorded (start, stop) pair
+  size_t ev_used = 0;
+  long long launches = 0;
   std::string err;
 };
 
@@ -130,6 +136,7 @@ void free_all(atm_ctx* c) {
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_mass) cudaFreeHost(c->h_mass);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
 }
 
 // host (is:ie, js:je, 1:K) FP64 array <-> pitched FP64 device array
@@ -143,6 +150,38 @@ cudaError_t d2h_pitched(atm_ctx* c, double* host, const double* dev, int K) {
   return cudaMemcpy2DAsync(host, (size_t)wrow * 8, dev + XOFF, (size_t)c->geo.P * 8, (size_t)wrow * 8,
                            (size_t)c->geo.NYP * K, cudaMemcpyDeviceToHost, c->stream);
 }
+
+const char* const STAGE_NAMES[] = {"c_mass",  "c_column", "c_mom",        "c_halo",      "d_ring",
+                                   "d_mass",  "d_column", "d_corners",    "d_mom",       "remap_ring",
+                                   "remap_winds", "remap_energy", "d_halo", "heating", "check"};
+constexpr int NSTAGE = 15;
+enum { S_CMASS, S_CCOL, S_CMOM, S_CHALO, S_DRING, S_DMASS, S_DCOL, S_DCORN, S_DMOM, S_RRING, S_RWIND, S_RENER,
+       S_DHALO, S_HEAT, S_CHECK };
+
+// Brackets one stage (one kernel launch unless noted) with CUDA events on
+// the context's stream when profiling is on, and counts the launch.
+struct Stage {
+  atm_ctx* c;
+  int id;
+  int nlaunch;
+  size_t slot;
+  Stage(atm_ctx* ctx, int stage, int n = 1) : c(ctx), id(stage), nlaunch(n), slot(0) {
+    if (!c->prof) return;
+    slot = c->ev_used;
+    while (c->ev_pool.size() < slot + 2) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      c->ev_pool.push_back(e);
+    }
+    c->ev_used += 2;
+    c->ev_stage.push_back(id);
+    cudaEventRecord(c->ev_pool[slot], c->stream);
+  }
+  ~Stage() {
+    c->launches += nlaunch;
+    if (c->prof) cudaEventRecord(c->ev_pool[slot + 1], c->stream);
+  }
+};
 
 int require_init(atm_ctx* c) {
   if (!c) return ATM_ERR_ARG;
@@ -411,22 +450,33 @@ int atm_cgrid_step(atm_ctx* ctx, double dt_half) {
   void* const* s = ctx->st[ctx->cur];
   const double* heat = nullptr;
   if (ctx->heating) {
+    Stage t(ctx, S_HEAT);
     CK(ops.heating(g, k, s[F_DP], ctx->nf, ctx->heat, ctx->stream));
     heat = ctx->heat;
   }
   // dpc, ptc on is+5:ie-5 (src/mod_sw_dyn.f90:94-270)
-  CK(ops.mass(g, k, s[F_DP], s[F_PT], s[F_UD], s[F_VD], heat, ctx->cg[C_DPC], ctx->cg[C_PTC], -2, 2, nullptr, true,
-              ctx->stream));
+  {
+    Stage t(ctx, S_CMASS);
+    CK(ops.mass(g, k, s[F_DP], s[F_PT], s[F_UD], s[F_VD], heat, ctx->cg[C_DPC], ctx->cg[C_PTC], -2, 2, nullptr, true,
+                ctx->stream));
+  }
   // plev, pkap, gz (src/mod_sw_dyn.f90:276-292)
-  CK(ops.column(g, k, ctx->cg[C_DPC], ctx->cg[C_PTC], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+  {
+    Stage t(ctx, S_CCOL);
+    CK(ops.column(g, k, ctx->cg[C_DPC], ctx->cg[C_PTC], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+  }
   // uc, vc (src/mod_sw_dyn.f90:294-414)
-  CK(ops.c_mom(g, k, s[F_UD], s[F_VD], ctx->pkap, ctx->gz, ctx->cg[C_UC], ctx->cg[C_VC], ctx->stream));
+  {
+    Stage t(ctx, S_CMOM);
+    CK(ops.c_mom(g, k, s[F_UD], s[F_VD], ctx->pkap, ctx->gz, ctx->cg[C_UC], ctx->cg[C_VC], ctx->stream));
+  }
   return ATM_OK;
 }
 
 int atm_cgrid_halo(atm_ctx* ctx) {
   int r = require_init(ctx);
   if (r) return r;
+  Stage t(ctx, S_CHALO);
   CK(ctx->ops->ring(ctx->geo, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
   return ATM_OK;
 }
@@ -442,21 +492,37 @@ int atm_dgrid_step(atm_ctx* ctx, double dt) {
   void* const* sn = ctx->st[nxt];
   const double* heat = nullptr;
   if (ctx->heating) {
+    Stage t(ctx, S_HEAT);
     CK(ops.heating(g, k, ctx->cg[C_DPC], ctx->nf, ctx->heat, ctx->stream));  // from dpc, :433-464
     heat = ctx->heat;
   }
   // the new time level keeps the old halo until the D-grid halo exchange
-  CK(ops.ring(g, ctx->st[nxt], (const void* const*)ctx->st[old], 4, ctx->L, true, ctx->stream));
+  {
+    Stage t(ctx, S_DRING);
+    CK(ops.ring(g, ctx->st[nxt], (const void* const*)ctx->st[old], 4, ctx->L, true, ctx->stream));
+  }
   CK(cudaMemsetAsync(&ctx->status->nonfinite_step, 0, sizeof(int), ctx->stream));
   // dp, pt on is+4:ie-4 (src/mod_sw_dyn.f90:439-600)
-  CK(ops.mass(g, k, so[F_DP], so[F_PT], ctx->cg[C_UC], ctx->cg[C_VC], heat, sn[F_DP], sn[F_PT], -3, 3,
-              &ctx->status->nonfinite_step, false, ctx->stream));
+  {
+    Stage t(ctx, S_DMASS);
+    CK(ops.mass(g, k, so[F_DP], so[F_PT], ctx->cg[C_UC], ctx->cg[C_VC], heat, sn[F_DP], sn[F_PT], -3, 3,
+                &ctx->status->nonfinite_step, false, ctx->stream));
+  }
   // plev, pkap, gz, pkapb, gzb (src/mod_sw_dyn.f90:606-632)
-  CK(ops.column(g, k, sn[F_DP], sn[F_PT], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
-  CK(atm::corners(g, ctx->pkap, ctx->gz, ctx->pkapb, ctx->gzb, 1, 0, ctx->L, ctx->stream));
+  {
+    Stage t(ctx, S_DCOL);
+    CK(ops.column(g, k, sn[F_DP], sn[F_PT], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+  }
+  {
+    Stage t(ctx, S_DCORN);
+    CK(atm::corners(g, ctx->pkap, ctx->gz, ctx->pkapb, ctx->gzb, 1, 0, ctx->L, ctx->stream));
+  }
   // ud, vd on the interior (src/mod_sw_dyn.f90:634-771)
-  CK(ops.d_mom(g, k, so[F_UD], so[F_VD], ctx->cg[C_UC], ctx->cg[C_VC], ctx->pkapb, ctx->gzb, sn[F_UD], sn[F_VD],
-               &ctx->status->nonfinite_step, ctx->stream));
+  {
+    Stage t(ctx, S_DMOM);
+    CK(ops.d_mom(g, k, so[F_UD], so[F_VD], ctx->cg[C_UC], ctx->cg[C_VC], ctx->pkapb, ctx->gzb, sn[F_UD], sn[F_VD],
+                 &ctx->status->nonfinite_step, ctx->stream));
+  }
   ctx->cur = nxt;
   ctx->flag_valid = true;
   ctx->remapped = false;
@@ -472,7 +538,10 @@ int atm_remap(atm_ctx* ctx) {
   void* const* s = ctx->st[src];
   void* const* d = ctx->st[dst];
   // outside the interior the remapped fields keep the arrays' current values
-  CK(ops.ring(g, ctx->st[dst], (const void* const*)ctx->st[src], 4, ctx->L, true, ctx->stream));
+  {
+    Stage t(ctx, S_RRING);
+    CK(ops.ring(g, ctx->st[dst], (const void* const*)ctx->st[src], 4, ctx->L, true, ctx->stream));
+  }
   CK(cudaMemsetAsync(&ctx->status->nonfinite_remap, 0, sizeof(int), ctx->stream));
   CK(cudaMemsetAsync(&ctx->status->fallback_pairs, 0, sizeof(int), ctx->stream));
   int* trace = nullptr;
@@ -488,9 +557,15 @@ int atm_remap(atm_ctx* ctx) {
     trace = ctx->d_trace;
   }
   atm::RemapArgs ra = remap_args(ctx);
-  CK(ops.remap_winds(g, ra, s[F_DP], s[F_UD], s[F_VD], ctx->urem, ctx->vrem, trace, ctx->status, ctx->stream));
-  CK(ops.remap_energy(g, ra, s[F_DP], s[F_PT], s[F_UD], s[F_VD], ctx->urem, ctx->vrem, ctx->gz, d[F_DP], d[F_PT],
-                      d[F_UD], d[F_VD], trace, ctx->status, ctx->stream));
+  {
+    Stage t(ctx, S_RWIND);
+    CK(ops.remap_winds(g, ra, s[F_DP], s[F_UD], s[F_VD], ctx->urem, ctx->vrem, trace, ctx->status, ctx->stream));
+  }
+  {
+    Stage t(ctx, S_RENER);
+    CK(ops.remap_energy(g, ra, s[F_DP], s[F_PT], s[F_UD], s[F_VD], ctx->urem, ctx->vrem, ctx->gz, d[F_DP], d[F_PT],
+                        d[F_UD], d[F_VD], trace, ctx->status, ctx->stream));
+  }
   ctx->cur = dst;
   ctx->remapped = true;
   if (ctx->trace_host) {
@@ -507,6 +582,7 @@ int atm_remap(atm_ctx* ctx) {
 int atm_dgrid_halo(atm_ctx* ctx) {
   int r = require_init(ctx);
   if (r) return r;
+  Stage t(ctx, S_DHALO);
   CK(ctx->ops->ring(ctx->geo, ctx->st[ctx->cur], nullptr, 4, ctx->L, false, ctx->stream));
   return ATM_OK;
 }
@@ -515,6 +591,7 @@ int atm_check_stability(atm_ctx* ctx, int* stable) {
   if (!ctx || !stable) return ATM_ERR_ARG;
   if (!ctx->flag_valid) {
     CK(cudaMemsetAsync(&ctx->status->nonfinite_check, 0, sizeof(int), ctx->stream));
+    Stage t(ctx, S_CHECK);
     CK(ctx->ops->check_finite(ctx->geo, (const void* const*)ctx->st[ctx->cur], &ctx->status->nonfinite_check,
                               ctx->stream));
   }
@@ -549,6 +626,39 @@ int atm_step(atm_ctx* ctx, double dt, int do_remap, int* stable) {
 int atm_sync(atm_ctx* ctx) {
   if (!ctx) return ATM_ERR_ARG;
   CK(cudaStreamSynchronize(ctx->stream));
+  return ATM_OK;
+}
+
+int atm_profile(atm_ctx* ctx, int enable) {
+  if (!ctx) return ATM_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->prof = enable != 0;
+  ctx->ev_used = 0;
+  ctx->ev_stage.clear();
+  return ATM_OK;
+}
+
+int atm_profile_read(atm_ctx* ctx, double* ms, int* count, int nstage) {
+  if (!ctx || !ms || !count) return ATM_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < nstage; ++i) { ms[i] = 0.; count[i] = 0; }
+  for (size_t p = 0; p < ctx->ev_stage.size(); ++p) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, ctx->ev_pool[2 * p], ctx->ev_pool[2 * p + 1]));
+    int id = ctx->ev_stage[p];
+    if (id < nstage) {
+      ms[id] += t;
+      count[id] += 1;
+    }
+  }
+  return ATM_OK;
+}
+
+const char* atm_profile_stage(int i) { return (i >= 0 && i < NSTAGE) ? STAGE_NAMES[i] : nullptr; }
+
+int atm_launch_count(atm_ctx* ctx, long long* n) {
+  if (!ctx || !n) return ATM_ERR_ARG;
+  *n = ctx->launches;
   return ATM_OK;
 }
 

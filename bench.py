@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Throughput of the dynamical-core step on B200: cell-steps/s.
+
+One step is one model step of run_model (src/mod_model.f90:146-177): the
+C-grid half step, its halo fill, the D-grid step, the vertical remap when
+due (every 8 steps) and the D-grid halo fill, then the stability check.
+One cell-step is one interior (i, j, k) cell advanced by one such step.
+
+Workload: the seeded zonal-jet case at 1024 x 1024 x 64 (dx = 25 km,
+dt = 30 s, remap every 8 steps), synthetic data from atmdyn.ic.jet_case.
+The headline ``value`` is the FP64 form (the reference's arithmetic,
+bit-identical to the FP64 restatement); the mixed-precision form is
+measured on the same workload and reported under ``forms``.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank advances its own replica of the domain
+(the path shards, but one domain fits one GPU; replicas only) and the time
+is the maximum over ranks.  ``--impl reference`` times the reference's CPU
+algorithm (the FP64 restatement) on the host cores, on a 256 x 256 x 64
+sample of the same case.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, 'atmosphere-model_b200'))
+
+import numpy as np  # noqa: E402
+
+METRIC = 'cell-steps/s fwd+adjoint on 1 B200 vs FP64 form, % HBM roofline, err vs FP64'
+NX = NY = 1024
+NLAY = 64
+DT = 30.0
+REMAP_EVERY = 8
+SAMPLE_N = 256
+
+# Algorithmic HBM words per interior cell and launch of each kernel: every
+# field the kernel must read or write once (layer-nlay slabs and halo rings
+# are excluded).  FP64 form: 8 bytes per word; the mixed form stores the
+# sweep fields in 4 bytes and pkap/gz in 8.
+#                 (sweep-type words, fp64 words)
+WORDS = {
+    'c_mass': (6, 0),        # read dp, pt, ud, vd; write dpc, ptc
+    'c_column': (2, 2),      # read dpc, ptc; write pkap, gz
+    'c_mom': (4, 2),         # read ud, vd, pkap, gz; write uc, vc
+    'd_mass': (6, 0),        # read dp, pt, uc, vc; write dp, pt
+    'd_column': (2, 2),      # read dp, pt; write pkap, gz
+    'd_corners': (0, 4),     # read pkap, gz; write pkapb, gzb
+    'd_mom': (6, 2),         # read ud, vd, uc, vc, pkapb, gzb; write ud, vd
+    'remap_winds': (5, 0),   # read dp, ud, vd; write u, v remapped
+    'remap_energy': (10, 0),  # read dp, pt, ud, vd, u, v remapped; write dp, pt, ud, vd
+}
+
+
+def kernel_bytes(stage, form, cells):
+    w_t, w_d = WORDS.get(stage, (0, 0))
+    es = 8 if form == 'fp64' else 4
+    return (w_t * es + w_d * 8) * cells
+
+
+def load_peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self):
+        self.f = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
+        try:
+            self.p = subprocess.Popen(['nvidia-smi', '--query-gpu=' + self.Q, '--format=csv,noheader,nounits',
+                                       '-lms', '200'], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith('active'):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': max(smax), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    return world, rank, local
+
+
+def cpu_sample_throughput(steps, warmup, threads):
+    """The FP64 restatement of the reference on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import pyoracle
+    from atmdyn import ic
+    st = ic.jet_case(SAMPLE_N, SAMPLE_N, NLAY, 25e3, 25e3, seed=0)
+    o = pyoracle.OracleModel(st, threads=threads)
+    n = 0
+
+    def one():
+        nonlocal n
+        n += 1
+        o.cgrid_step(DT / 2.)
+        o.cgrid_halo()
+        o.dgrid_step(DT)
+        if n % REMAP_EVERY == 0:
+            o.remap()
+        o.dgrid_halo()
+        return o.check_stability()
+
+    for _ in range(warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    t = time.perf_counter() - t0
+    return st.cells * steps / t, t
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    threads = len(os.sched_getaffinity(0))
+    steps, warmup = args.steps, args.warmup
+    v, t = cpu_sample_throughput(steps, warmup, threads)
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'cell-steps/s', 'n_gpus': args.gpus,
+        'steps': steps, 'warmup': warmup, 'ms_per_step': 1000 * t / steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+        'data': 'synthetic (seeded jet case)',
+        'config': {'workload': 'jet case, the reference algorithm on the host cores, sample %dx%dx%d per step' % (
+            SAMPLE_N, SAMPLE_N, NLAY), 'nx': SAMPLE_N, 'ny': SAMPLE_N, 'nlay': NLAY, 'remap_every': REMAP_EVERY},
+        'cpu_baseline': {'value': v, 'unit': 'cell-steps/s', 'cores': threads, 'kind': 'port',
+                         'sample': 'jet %dx%dx%d, %d steps after %d warm-up (1/16 of the 1024^2 domain)' % (
+                             SAMPLE_N, SAMPLE_N, NLAY, steps, warmup)},
+        'e2e': {'value': v, 'unit': 'cell-steps/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=timedelta(seconds=300), device_id=torch.device('cuda', local))
+    else:
+        torch.cuda.set_device(0)
+    from atmdyn import ic, Dycore
+    st = ic.jet_case(args.nx, args.nx, args.nlay, 25e3, 25e3, seed=0)
+    cells = st.cells
+    K, W = args.steps, args.warmup
+    peak, peak_kind = load_peaks()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device='cuda')
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    states = {}
+    clocks = None
+    forms = args.forms.split(',')
+    for form in forms:
+        dy = Dycore(st, form)
+        stream = torch.cuda.Stream()
+        dy.set_stream(stream.cuda_stream)
+        n = 0
+
+        def one():
+            nonlocal n
+            n += 1
+            return dy.step(DT, remap=(n % REMAP_EVERY == 0), check_stable=True)
+
+        for _ in range(W):
+            one()
+        barrier()
+        if form == 'fp64':
+            clk = Clocks()
+        l0 = dy.launch_count()
+        dy.profile(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        stable = True
+        for _ in range(K):
+            stable = one() and stable
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if form == 'fp64':
+            clocks = clk.stop()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        prof = dy.profile_read()
+        dy.profile(False)
+        launches = dy.launch_count() - l0
+        barrier()
+        kern = {}
+        for stage, (tms, cnt) in prof.items():
+            if cnt == 0:
+                continue
+            b = kernel_bytes(stage, form, cells)
+            avg = tms / cnt
+            kern[stage] = {'ms_avg': round(avg, 4), 'launches': cnt, 'share': round(tms / max(ms, 1e-9), 4)}
+            if b:
+                kern[stage]['algorithmic_bytes'] = b
+                kern[stage]['gbs'] = round(b / (avg * 1e-3) / 1e9, 1)
+        value = world * cells * K / (ms * 1e-3)
+        results[form] = {'value': value, 'ms_per_step': ms / K, 'stable': stable, 'kernels': kern,
+                         'gpu_launches': launches, 'steps_done': n}
+        states[form] = dy.state()
+        if form == 'fp64' and not args.no_e2e:
+            results[form]['e2e'], results[form]['e2e_resident'] = e2e_runs(dy, st, K, stream, torch, max_over_ranks,
+                                                                            world)
+        dy.close()
+        del dy
+        torch.cuda.empty_cache()
+
+    # error of the mixed form against the FP64 form after the same steps
+    err = {}
+    for name in (('dp', 'pt', 'ud', 'vd') if len(states) == 2 else ()):
+        a, b = states['fp64'][name], states['mixed'][name]
+        err[name] = {'rel_l2': float(np.linalg.norm(b - a) / max(np.linalg.norm(a), 1e-300)),
+                     'rel_max': float(np.abs(b - a).max() / max(np.abs(a).max(), 1e-300))}
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    f64 = results['fp64']
+    mixed = results.get('mixed')
+    dom = max(f64['kernels'].items(), key=lambda kv: kv[1]['ms_avg'] * kv[1]['launches'])
+    dom_name, dom_k = dom
+    achieved = dom_k.get('gbs', 0.0)
+    line = {
+        'metric': METRIC, 'value': f64['value'], 'unit': 'cell-steps/s', 'n_gpus': world, 'steps': K, 'warmup': W,
+        'ms_per_step': f64['ms_per_step'], 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f64', 'data': 'synthetic (seeded jet case, atmdyn.ic.jet_case)',
+        'config': {'workload': 'jet %dx%dx%d, dx=25 km, dt=30 s, remap every %d steps, FP64 form' % (
+            args.nx, args.nx, args.nlay, REMAP_EVERY), 'nx': args.nx, 'ny': args.nx, 'nlay': args.nlay,
+            'remap_every': REMAP_EVERY,
+            'l2': 'inputs larger than L2 (each prognostic field is 552 MB)',
+            'parallelism': 'replicas' if world > 1 else 'single GPU'},
+        'roofline': {'bound': 'hbm', 'kernel': dom_name, 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                     'frac': achieved / peak, 'peak_kind': peak_kind, 'traffic': None},
+        'e2e': f64.get('e2e'),
+        'e2e_resident': f64.get('e2e_resident'),
+        'gpu_launches': f64['gpu_launches'],
+        'clocks': clocks,
+        'kernels': f64['kernels'],
+        'forms': {
+            'fp64': {'value': f64['value'], 'ms_per_step': f64['ms_per_step'], 'stable': f64['stable']},
+        },
+    }
+    if mixed:
+        line['forms']['mixed'] = {'value': mixed['value'], 'ms_per_step': mixed['ms_per_step'],
+                                  'stable': mixed['stable'], 'speedup_vs_fp64': mixed['value'] / f64['value'],
+                                  'err_vs_fp64_after_%d_steps' % (K + W): err, 'kernels': mixed['kernels']}
+    if world == 1 and not args.no_cpu:
+        threads = len(os.sched_getaffinity(0))
+        v, t = cpu_sample_throughput(max(2, REMAP_EVERY // 2), 1, threads)
+        line['cpu_baseline'] = {'value': v, 'unit': 'cell-steps/s', 'cores': threads, 'kind': 'port',
+                                'sample': 'jet %dx%dx%d, %d steps after 1 warm-up (1/16 of the domain)' % (
+                                    SAMPLE_N, SAMPLE_N, NLAY, max(2, REMAP_EVERY // 2))}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def e2e_runs(dy, st, K, stream, torch, max_over_ranks, world):
+    """End to end through the C ABI with host buffers.
+
+    e2e: every step uploads the four prognostic fields from pinned host
+    memory (the reference's host arrays), runs the step and downloads them
+    with the stability flag -- the drop-in used from a host time loop that
+    keeps its state in host arrays.
+    e2e_resident: the state is uploaded from pinned host memory before the
+    first step and downloaded after the last, inside the timed region, with
+    the stability flag read back every step."""
+    from atmdyn.dycore import with_halo, HALO
+    from atmdyn._lib import ATM_DP, ATM_PT, ATM_UD, ATM_VD
+    fields = (ATM_DP, ATM_PT, ATM_UD, ATM_VD)
+    shape = (st.nlay, st.ny + 2 * HALO, st.nx + 2 * HALO)
+    host = [torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for _ in fields]
+    for h, f in zip(host, fields):
+        dy.get_into(f, h)
+    nbytes = sum(h.nbytes for h in host)
+    cells = st.cells
+    out = []
+    for mode in ('roundtrip', 'resident'):
+        Ke = max(2, min(K, 6)) if mode == 'roundtrip' else K
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        if mode == 'resident':
+            for h, f in zip(host, fields):
+                dy.upload(f, h)
+        for s in range(Ke):
+            if mode == 'roundtrip':
+                for h, f in zip(host, fields):
+                    dy.upload(f, h)
+            dy.step(DT, remap=((s + 1) % REMAP_EVERY == 0), check_stable=True)
+            if mode == 'roundtrip':
+                for h, f in zip(host, fields):
+                    dy.get_into(f, h)
+        if mode == 'resident':
+            for h, f in zip(host, fields):
+                dy.get_into(f, h)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        v = world * cells * Ke / (ms * 1e-3)
+        if mode == 'roundtrip':
+            out.append({'value': v, 'unit': 'cell-steps/s', 'h2d_bytes_per_step': nbytes,
+                        'd2h_bytes_per_step': nbytes + 4, 'steps': Ke,
+                        'how': 'per step: upload dp/pt/ud/vd from pinned host, atm_step, download + stability flag'})
+        else:
+            out.append({'value': v, 'unit': 'cell-steps/s', 'h2d_bytes_per_step': nbytes / Ke,
+                        'd2h_bytes_per_step': nbytes / Ke + 4, 'steps': Ke,
+                        'how': 'state uploaded before step 1 and downloaded after step K inside the timed region'})
+    return out[0], out[1]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=16)
+    ap.add_argument('--warmup', type=int, default=8)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
+    ap.add_argument('--nx', type=int, default=NX, help='grid size (profiling runs use smaller cases)')
+    ap.add_argument('--nlay', type=int, default=NLAY)
+    ap.add_argument('--forms', default='fp64,mixed')
+    ap.add_argument('--no-e2e', action='store_true')
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == '__main__':
+    main()

@@ -151,6 +151,18 @@ int atm_set_stream(atm_ctx* ctx, void* stream);
    reference's all-pairs search because a coordinate was not monotone. */
 int atm_remap_trace(atm_ctx* ctx, int32_t* buf, int* fallback_columns);
 
+/* ---- measurement (no reference counterpart) ----
+   atm_profile(ctx, 1) starts bracketing every kernel the step entry points
+   launch with CUDA events on the context's stream (and clears earlier
+   records); atm_profile_read synchronises and returns, per stage, the total
+   milliseconds and the number of launches since then.  Stage i is named by
+   atm_profile_stage(i) (NULL past the last).  atm_launch_count returns how
+   many kernels the context's step entry points have launched. */
+int atm_profile(atm_ctx* ctx, int enable);
+int atm_profile_read(atm_ctx* ctx, double* ms, int* count, int nstage);
+const char* atm_profile_stage(int i);
+int atm_launch_count(atm_ctx* ctx, long long* n);
+
 /* the portable x**y and log(x) the FP64 form evaluates on the device, on n
    host values (accuracy and bit-identity tests) */
 int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_out, int n);
