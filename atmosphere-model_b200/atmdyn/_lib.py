@@ -18,7 +18,7 @@ ATM_DP, ATM_PT, ATM_UD, ATM_VD, ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX = range
 ATM_DPC, ATM_PTC, ATM_UC, ATM_VC = range(8, 12)
 ATM_FP64, ATM_MIXED = 0, 1
 STATUS = {0: 'ATM_OK', 1: 'ATM_ERR_ARG', 2: 'ATM_ERR_CUDA', 3: 'ATM_ERR_STATE',
-          4: 'ATM_ERR_NOMEM', 5: 'ATM_ERR_UNSUPPORTED'}
+          4: 'ATM_ERR_NOMEM', 5: 'ATM_ERR_UNSUPPORTED', 6: 'ATM_ERR_TOO_LARGE'}
 
 # every entry point of include/atmdyn.h
 EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_step', 'atm_cgrid_halo',
@@ -26,7 +26,7 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_set_net_flux', 'atm_step', 'atm_sync', 'atm_destroy', 'atm_last_error',
            'atm_upload_device', 'atm_download_device', 'atm_set_stream', 'atm_remap_trace',
            'atm_device_pow_log', 'atm_version', 'atm_profile', 'atm_profile_read', 'atm_profile_stage',
-           'atm_launch_count')
+           'atm_launch_count', 'atm_remap_noalloc')
 
 _lib = None
 

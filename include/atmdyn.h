@@ -65,7 +65,8 @@ enum {
   ATM_ERR_CUDA = 2,      /* a CUDA call failed; the message names it */
   ATM_ERR_STATE = 3,     /* call out of order (e.g. a step before atm_init) */
   ATM_ERR_NOMEM = 4,     /* device allocation failed */
-  ATM_ERR_UNSUPPORTED = 5
+  ATM_ERR_UNSUPPORTED = 5,
+  ATM_ERR_TOO_LARGE = 6  /* atm_remap_noalloc: the domain needs more than its fixed scratch */
 };
 
 /* flags for atm_create */
@@ -166,6 +167,35 @@ int atm_launch_count(atm_ctx* ctx, long long* n);
 /* the portable x**y and log(x) the FP64 form evaluates on the device, on n
    host values (accuracy and bit-identity tests) */
 int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_out, int n);
+
+/* ---- vertical remap without allocation (no counterpart in the reference) ----
+   perform_vertical_remapping (src/mod_remap.f90:27-163) for callers that
+   cannot let the library allocate device memory: a host loop that fixes
+   its device-memory budget at start-up, or one that must not meet the
+   device-wide synchronisation cudaMalloc/cudaFree can cause mid-step.  It
+   needs no context and calls no cudaMalloc, cudaFree or other allocating
+   routine: its scratch (the remapped face winds of every column) is one
+   file-scope device array of 2^20 doubles (8 MiB) that every GPU loading
+   the library holds until the process exits.  Sizes with
+   2 (nx+14)(ny+14) nlay + 2 (nlay+1) + 64 > 2^20 (e.g. above 64x64x64 or
+   128x128x24) return ATM_ERR_TOO_LARGE.
+   Inputs dp, pt, ud, vd and outputs dp_out .. vd_out are caller-owned FP64
+   device arrays in the reference's layout (is:ie, js:je, 1:nlay) without
+   row padding; gzs is the (is:ie, js:je) surface geopotential on the
+   device; ak, bk are host arrays of nlay+1 hybrid coefficients.  Like the
+   reference, ud and vd are read one point outside the interior, where they
+   still hold the halo of the previous step.  Only the interior of the
+   outputs is written; outputs must not alias inputs.  The call is
+   asynchronous on stream (a cudaStream_t, NULL = the default stream); its
+   result is bit-identical to atm_remap of the FP64 form.  Every call shares
+   the one scratch array, so calls that overlap on the GPU (other streams,
+   other threads) race and must be serialised by the caller.  The first
+   call on a device looks up the array's device address
+   (cudaGetSymbolAddress) with that device current; make that first call
+   before any stream capture. */
+int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, const double* bk, const double* dp,
+                      const double* pt, const double* ud, const double* vd, const double* gzs,
+                      double* dp_out, double* pt_out, double* ud_out, double* vd_out, void* stream);
 
 /* library version string */
 const char* atm_version(void);
