@@ -11,7 +11,8 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, 'libatmdyn.so')
+# ATMDYN_LIBRARY selects another build of the library (e.g. an installed copy)
+LIB_PATH = os.environ.get('ATMDYN_LIBRARY') or os.path.join(HERE, 'libatmdyn.so')
 CSRC = os.path.join(os.path.dirname(HERE), 'csrc')
 
 ATM_DP, ATM_PT, ATM_UD, ATM_VD, ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX = range(8)
@@ -26,7 +27,12 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_set_net_flux', 'atm_step', 'atm_sync', 'atm_destroy', 'atm_last_error',
            'atm_upload_device', 'atm_download_device', 'atm_set_stream', 'atm_remap_trace',
            'atm_device_pow_log', 'atm_version', 'atm_profile', 'atm_profile_read', 'atm_profile_stage',
-           'atm_launch_count', 'atm_remap_noalloc')
+           'atm_launch_count', 'atm_remap_noalloc', 'atm_device_div_check')
+
+# the entry points every build must export
+CORE = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_step', 'atm_cgrid_halo',
+        'atm_dgrid_step', 'atm_remap', 'atm_dgrid_halo', 'atm_check_stability', 'atm_mass', 'atm_step',
+        'atm_sync', 'atm_destroy', 'atm_last_error', 'atm_set_stream')
 
 _lib = None
 
@@ -46,6 +52,9 @@ def load():
     if not os.path.exists(LIB_PATH):
         raise AtmError('libatmdyn.so is not built (run make -C %s)' % CSRC)
     lib = ctypes.CDLL(LIB_PATH)
+    missing = [f for f in CORE if not hasattr(lib, f)]
+    if missing:
+        raise AtmError('libatmdyn.so lacks %s' % ', '.join(missing))
     P = ctypes.POINTER(ctypes.c_double)
     vp = ctypes.c_void_p
     i = ctypes.c_int
@@ -69,13 +78,19 @@ def load():
     lib.atm_remap_trace.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(i)]
     lib.atm_device_pow_log.argtypes = [P, d, P, P, i]
     lib.atm_version.restype = ctypes.c_char_p
-    lib.atm_profile.argtypes = [vp, i]
-    lib.atm_profile_read.argtypes = [vp, P, ctypes.POINTER(i), i]
-    lib.atm_profile_stage.argtypes = [i]
-    lib.atm_profile_stage.restype = ctypes.c_char_p
-    lib.atm_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
-    for f in EXPORTS:
-        getattr(lib, f)  # raises AttributeError if the symbol is missing
+    # measurement and test entry points (an older build may lack some)
+    optional = {
+        'atm_profile': ([vp, i], None),
+        'atm_profile_read': ([vp, P, ctypes.POINTER(i), i], None),
+        'atm_profile_stage': ([i], ctypes.c_char_p),
+        'atm_launch_count': ([vp, ctypes.POINTER(ctypes.c_longlong)], None),
+        'atm_device_div_check': ([ctypes.c_longlong, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)], None),
+    }
+    for f, (args, res) in optional.items():
+        if hasattr(lib, f):
+            getattr(lib, f).argtypes = args
+            if res is not None:
+                getattr(lib, f).restype = res
     _lib = lib
     return lib
 

@@ -457,8 +457,8 @@ int atm_cgrid_step(atm_ctx* ctx, double dt_half) {
   // dpc, ptc on is+5:ie-5 (src/mod_sw_dyn.f90:94-270)
   {
     Stage t(ctx, S_CMASS);
-    CK(ops.mass(g, k, s[F_DP], s[F_PT], s[F_UD], s[F_VD], heat, ctx->cg[C_DPC], ctx->cg[C_PTC], -2, 2, nullptr, true,
-                ctx->stream));
+    CK(ops.mass(g, k, s[F_DP], s[F_PT], s[F_UD], s[F_VD], heat, ctx->cg[C_DPC], ctx->cg[C_PTC], -2, 2, nullptr,
+                &ctx->status->tma_timeout, true, ctx->stream));
   }
   // plev, pkap, gz (src/mod_sw_dyn.f90:276-292)
   {
@@ -468,7 +468,8 @@ int atm_cgrid_step(atm_ctx* ctx, double dt_half) {
   // uc, vc (src/mod_sw_dyn.f90:294-414)
   {
     Stage t(ctx, S_CMOM);
-    CK(ops.c_mom(g, k, s[F_UD], s[F_VD], ctx->pkap, ctx->gz, ctx->cg[C_UC], ctx->cg[C_VC], ctx->stream));
+    CK(ops.c_mom(g, k, s[F_UD], s[F_VD], ctx->pkap, ctx->gz, ctx->cg[C_UC], ctx->cg[C_VC], &ctx->status->tma_timeout,
+                 ctx->stream));
   }
   return ATM_OK;
 }
@@ -506,7 +507,7 @@ int atm_dgrid_step(atm_ctx* ctx, double dt) {
   {
     Stage t(ctx, S_DMASS);
     CK(ops.mass(g, k, so[F_DP], so[F_PT], ctx->cg[C_UC], ctx->cg[C_VC], heat, sn[F_DP], sn[F_PT], -3, 3,
-                &ctx->status->nonfinite_step, false, ctx->stream));
+                &ctx->status->nonfinite_step, &ctx->status->tma_timeout, false, ctx->stream));
   }
   // plev, pkap, gz, pkapb, gzb (src/mod_sw_dyn.f90:606-632)
   {
@@ -521,7 +522,7 @@ int atm_dgrid_step(atm_ctx* ctx, double dt) {
   {
     Stage t(ctx, S_DMOM);
     CK(ops.d_mom(g, k, so[F_UD], so[F_VD], ctx->cg[C_UC], ctx->cg[C_VC], ctx->pkapb, ctx->gzb, sn[F_UD], sn[F_VD],
-                 &ctx->status->nonfinite_step, ctx->stream));
+                 &ctx->status->nonfinite_step, &ctx->status->tma_timeout, ctx->stream));
   }
   ctx->cur = nxt;
   ctx->flag_valid = true;
@@ -597,6 +598,7 @@ int atm_check_stability(atm_ctx* ctx, int* stable) {
   }
   CK(cudaMemcpyAsync(ctx->h_status, ctx->status, sizeof(atm::Status), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->h_status->tma_timeout) return fail(ctx, ATM_ERR_CUDA, "a TMA tile load did not complete (wait limit)");
   int bad = !ctx->flag_valid ? ctx->h_status->nonfinite_check
                              : (ctx->remapped ? ctx->h_status->nonfinite_remap : ctx->h_status->nonfinite_step);
   *stable = bad ? 0 : 1;
@@ -667,6 +669,20 @@ int atm_remap_trace(atm_ctx* ctx, int32_t* buf, int* fallback_columns) {
   ctx->trace_host = buf;
   ctx->trace_fallback = fallback_columns;
   return ATM_OK;
+}
+
+int atm_device_div_check(long long n, long long seed, long long* mismatches) {
+  if (n <= 0 || !mismatches) return ATM_ERR_ARG;
+  unsigned long long* d = nullptr;
+  if (cudaMalloc((void**)&d, 8) != cudaSuccess) return ATM_ERR_NOMEM;
+  int rc = ATM_OK;
+  unsigned long long h = 0;
+  if (cudaMemset(d, 0, 8) != cudaSuccess || atm::device_div_check(n, seed, d, 0) != cudaSuccess ||
+      cudaMemcpy(&h, d, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = ATM_ERR_CUDA;
+  cudaFree(d);
+  *mismatches = (long long)h;
+  return rc;
 }
 
 int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_out, int n) {

@@ -60,6 +60,7 @@ struct Status {
   int nonfinite_remap;  // ... or the vertical remap
   int nonfinite_check;  // standalone stability check
   int fallback_pairs;   // columns whose remap used the all-pairs search
+  int tma_timeout;      // a TMA tile load did not complete within its wait limit
 };
 
 // Hybrid coordinate of the vertical remap (src/mod_remap.f90:57-71).
@@ -80,11 +81,37 @@ __device__ __forceinline__ float cpsign(float a, float b) { return copysignf(a, 
 __device__ __forceinline__ double fab(double a) { return fabs(a); }
 __device__ __forceinline__ float fab(float a) { return fabsf(a); }
 
+// Division by the constants 3 and 12 of the PPM formulas
+// (src/mod_sw_dyn.f90:878-879,899), correctly rounded like an IEEE
+// division: q = x*RN(1/b) is within one ulp of x/b, the remainder
+// r = x - q*b is exact in one FMA, and RN(q + r*RN(1/b)) is the correctly
+// rounded quotient (P. Markstein, IBM J. Res. Dev. 34(1), 1990).  Zeros,
+// infinities, NaN and magnitudes near the ends of the exponent range take
+// the IEEE division.
+static __device__ __noinline__ double div_ieee(double x, double b) { return x / b; }
+static __device__ __noinline__ float div_ieee(float x, float b) { return x / b; }
+template <int B> __device__ __forceinline__ double div_const(double x) {
+  constexpr double r = 1.0 / B;  // RN(1/B)
+  double a = fabs(x);
+  if (!(a > 0x1p-960 && a < 0x1p1000)) return div_ieee(x, (double)B);
+  double q = x * r;
+  double e = __fma_rn(-q, (double)B, x);
+  return __fma_rn(e, r, q);
+}
+template <int B> __device__ __forceinline__ float div_const(float x) {
+  constexpr float r = 1.0f / B;
+  float a = fabsf(x);
+  if (!(a > 0x1p-100f && a < 0x1p100f)) return div_ieee(x, (float)B);
+  float q = x * r;
+  float e = __fmaf_rn(-q, (float)B, x);
+  return __fmaf_rn(e, r, q);
+}
+
 // Monotone slope dqi_mono(i) and raw slope dqi(i) of src/mod_sw_dyn.f90:870-875
 // from q(i-1), q(i), q(i+1).
 template <typename T>
 __device__ __forceinline__ void slopes(T qm, T q0, T qp, T& dqi, T& mono) {
-  dqi = (qp - qm) / T(4);
+  dqi = (qp - qm) * T(0.25);
   T dmax = mx3(qp, q0, qm) - q0;
   T dmin = q0 - mn3(qp, q0, qm);
   mono = cpsign(mn3(fab(dqi), dmin, dmax), dqi);
@@ -99,8 +126,8 @@ __device__ __forceinline__ void edges(const T* q, int s, T& eL, T& eR) {
   slopes(qm2, qm1, q0, d_m, mono_m);
   slopes(qm1, q0, qp1, d_0, mono_0);
   slopes(q0, qp1, qp2, d_p, mono_p);
-  eL = (qm1 - q0) / T(2) + (mono_m - mono_0) / T(3);
-  eR = (qp1 - q0) / T(2) + (mono_0 - mono_p) / T(3);
+  eL = (qm1 - q0) * T(0.5) + div_const<3>(mono_m - mono_0);
+  eR = (qp1 - q0) * T(0.5) + div_const<3>(mono_0 - mono_p);
   if (V == PPM_CON || V == PPM_NN) {
     T lim = T(2) * fab(d_0);
     eL = -cpsign(mn(lim, fab(eL)), d_0);
@@ -110,7 +137,7 @@ __device__ __forceinline__ void edges(const T* q, int s, T& eL, T& eR) {
       eR = mx(eR, -q0);
       T a = eR - eL;
       T b = T(-3) * (eR + eL);
-      if ((fab(a) < -b) && (q0 + a * a / (T(4) * b) + b / T(12) < T(0))) {
+      if ((fab(a) < -b) && (q0 + a * a / (T(4) * b) + div_const<12>(b) < T(0))) {
         if (eL * eR > T(0)) {
           eL = T(0);
           eR = T(0);

@@ -22,6 +22,39 @@ static __global__ void k_pow_log(const double* x, double y, double* p, double* l
   }
 }
 
+// random bit patterns of every exponent, and small integers
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ULL;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+static __global__ void k_div_check(unsigned long long n, unsigned long long seed, unsigned long long* bad) {
+  unsigned long long local = 0;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned long long b = mix64(seed * 0x100000001b3ULL + i);
+    double x = __longlong_as_double((long long)b);
+    if (i % 7 == 0) x = (double)(long long)(b % 2000001) - 1000000.0;
+    float xf = __int_as_float((int)(unsigned)b);
+    bool ok = true;
+    double q3 = div_const<3>(x), t3 = x / 3.0;
+    double q12 = div_const<12>(x), t12 = x / 12.0;
+    ok = ok && (__double_as_longlong(q3) == __double_as_longlong(t3) || (q3 != q3 && t3 != t3));
+    ok = ok && (__double_as_longlong(q12) == __double_as_longlong(t12) || (q12 != q12 && t12 != t12));
+    float f3 = div_const<3>(xf), g3 = xf / 3.0f, f12 = div_const<12>(xf), g12 = xf / 12.0f;
+    ok = ok && (__float_as_int(f3) == __float_as_int(g3) || (f3 != f3 && g3 != g3));
+    ok = ok && (__float_as_int(f12) == __float_as_int(g12) || (f12 != f12 && g12 != g12));
+    if (!ok) ++local;
+  }
+  if (local) atomicAdd(bad, local);
+}
+
+cudaError_t device_div_check(unsigned long long n, unsigned long long seed, unsigned long long* bad, cudaStream_t s) {
+  k_div_check<<<1184, 256, 0, s>>>(n, seed, bad);
+  return cudaGetLastError();
+}
+
 cudaError_t device_pow_log(const double* x, double y, double* p, double* l, int n, cudaStream_t s) {
   k_pow_log<<<(n + 255) / 256, 256, 0, s>>>(x, y, p, l, n);
   return cudaGetLastError();

@@ -50,155 +50,6 @@ __device__ __forceinline__ void flag_nonfinite(int* flag, bool bad) {
 __device__ __forceinline__ bool finite_(double v) { return isfinite(v); }
 __device__ __forceinline__ bool finite_(float v) { return isfinite(v); }
 
-// ============================================================ mass sweeps ==
-// One kernel serves both the C-grid half step (CGRID: C-grid winds built
-// from the D-grid winds, PPM_UNCONSTRAINED, src/mod_sw_dyn.f90:109-268) and
-// the D-grid step (C-grid winds read directly, PPM_NONNEGATIVE,
-// src/mod_sw_dyn.f90:441-598).  Outputs: the new pressure thickness and
-// potential temperature on [lo, n-1+hi]^2 (C: is+5:ie-5, D: is+4:ie-4).
-template <typename T, int TX, int TY>
-struct MassSmem {
-  static constexpr size_t bytes =
-      2 * box_bytes<T>(TX + 6, TY + 6) +              // dp, pt
-      box_bytes<T>(TX + 2, TY + 7) + box_bytes<T>(TX + 7, TY + 2) +  // ud, vd boxes (C grid only)
-      box_bytes<T>(TX + 1, TY + 6) + box_bytes<T>(TX + 6, TY + 1) +  // uc, vc
-      2 * box_bytes<T>(TX + 6, TY) + 2 * box_bytes<T>(TX, TY + 6) +  // tmp (y-inner), tmp (x-inner)
-      2 * box_bytes<T>(TX + 2, TY + 2) +                            // laplacians
-      2 * box_bytes<T>(TX + 1, TY) + 2 * box_bytes<T>(TX, TY + 1);  // x and y fluxes
-};
-
-template <typename T, int TX, int TY, bool CGRID>
-__global__ void __launch_bounds__(NT) k_mass(Geom g, Consts c, const T* __restrict__ dp, const T* __restrict__ pt,
-                                             const T* __restrict__ uin, const T* __restrict__ vin,
-                                             const double* __restrict__ heat, T* __restrict__ dpo,
-                                             T* __restrict__ pto, int lo, int hi, int* nonfinite) {
-  constexpr int V = CGRID ? PPM_UNC : PPM_NN;
-  extern __shared__ __align__(16) unsigned char smem[];
-  unsigned char* p = smem;
-  const int k = blockIdx.z;
-  const int ox = lo + blockIdx.x * TX, oy = lo + blockIdx.y * TY;
-  const T dt = T(c.dt), dtdx = T(c.dtdx), dtdy = T(c.dtdy), rA = T(c.rA);
-
-  Sm<T> sdp = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
-  Sm<T> spt = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
-  Sm<T> sud = carve<T>(p, ox - 1, oy - 3, TX + 2, TY + 7);
-  Sm<T> svd = carve<T>(p, ox - 3, oy - 1, TX + 7, TY + 2);
-  Sm<T> suc = carve<T>(p, ox, oy - 3, TX + 1, TY + 6);
-  Sm<T> svc = carve<T>(p, ox - 3, oy, TX + 6, TY + 1);
-  Sm<T> tyd = carve<T>(p, ox - 3, oy, TX + 6, TY);
-  Sm<T> typ = carve<T>(p, ox - 3, oy, TX + 6, TY);
-  Sm<T> txd = carve<T>(p, ox, oy - 3, TX, TY + 6);
-  Sm<T> txp = carve<T>(p, ox, oy - 3, TX, TY + 6);
-  Sm<T> lpd = carve<T>(p, ox - 1, oy - 1, TX + 2, TY + 2);
-  Sm<T> lpp = carve<T>(p, ox - 1, oy - 1, TX + 2, TY + 2);
-  Sm<T> fxd = carve<T>(p, ox, oy, TX + 1, TY);
-  Sm<T> fxp = carve<T>(p, ox, oy, TX + 1, TY);
-  Sm<T> fyd = carve<T>(p, ox, oy, TX, TY + 1);
-  Sm<T> fyp = carve<T>(p, ox, oy, TX, TY + 1);
-
-  load_box(sdp.p, dp, g, k, ox - 3, oy - 3, TX + 6, TY + 6);
-  load_box(spt.p, pt, g, k, ox - 3, oy - 3, TX + 6, TY + 6);
-  if (CGRID) {
-    load_box(sud.p, uin, g, k, ox - 1, oy - 3, TX + 2, TY + 7);
-    load_box(svd.p, vin, g, k, ox - 3, oy - 1, TX + 7, TY + 2);
-  } else {
-    load_box(suc.p, uin, g, k, ox, oy - 3, TX + 1, TY + 6);
-    load_box(svc.p, vin, g, k, ox - 3, oy, TX + 6, TY + 1);
-  }
-  __syncthreads();
-
-  if (CGRID) {  // C-grid winds from the D-grid winds, mod_sw_dyn.f90:109-117
-    for (int idx = threadIdx.x; idx < (TX + 1) * (TY + 6); idx += NT) {
-      int x = ox + idx % (TX + 1), y = oy - 3 + idx / (TX + 1);
-      T ub = T(.5) * (sud(x, y) + sud(x - 1, y));
-      suc(x, y) = T(.5) * (ub + T(.5) * (sud(x, y + 1) + sud(x - 1, y + 1)));
-    }
-    for (int idx = threadIdx.x; idx < (TX + 6) * (TY + 1); idx += NT) {
-      int x = ox - 3 + idx % (TX + 6), y = oy + idx / (TX + 6);
-      T vb = T(.5) * (svd(x, y) + svd(x, y - 1));
-      svc(x, y) = T(.5) * (vb + T(.5) * (svd(x + 1, y) + svd(x + 1, y - 1)));
-    }
-    __syncthreads();
-  }
-
-  // inner sweeps (piecewise constant) and Laplacians
-  // y-inner for the x-outer sweep: mod_sw_dyn.f90:142-155 (C), 470-482 (D)
-  for (int idx = threadIdx.x; idx < (TX + 6) * TY; idx += NT) {
-    int x = ox - 3 + idx % (TX + 6), y = oy + idx / (TX + 6);
-    T cy0 = dtdx * svc(x, y), cy1 = dtdx * svc(x, y + 1);
-    T den = T(1) / (T(1) - dtdy * (svc(x, y + 1) - svc(x, y)));
-    T f0 = (cy0 > T(0)) ? sdp(x, y - 1) : sdp(x, y);
-    T f1 = (cy1 > T(0)) ? sdp(x, y) : sdp(x, y + 1);
-    tyd(x, y) = T(.5) * (sdp(x, y) + den * (sdp(x, y) - rA * (f1 - f0)));
-    f0 = (cy0 > T(0)) ? spt(x, y - 1) : spt(x, y);
-    f1 = (cy1 > T(0)) ? spt(x, y) : spt(x, y + 1);
-    typ(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
-  }
-  // x-inner for the y-outer sweep: mod_sw_dyn.f90:176-185 (C), 503-511 (D)
-  for (int idx = threadIdx.x; idx < TX * (TY + 6); idx += NT) {
-    int x = ox + idx % TX, y = oy - 3 + idx / TX;
-    T cx0 = dtdx * suc(x, y), cx1 = dtdx * suc(x + 1, y);
-    T den = T(1) / (T(1) - dtdx * (suc(x + 1, y) - suc(x, y)));
-    T f0 = (cx0 > T(0)) ? sdp(x - 1, y) : sdp(x, y);
-    T f1 = (cx1 > T(0)) ? sdp(x, y) : sdp(x + 1, y);
-    txd(x, y) = T(.5) * (sdp(x, y) + den * (sdp(x, y) - rA * (f1 - f0)));
-    f0 = (cx0 > T(0)) ? spt(x - 1, y) : spt(x, y);
-    f1 = (cx1 > T(0)) ? spt(x, y) : spt(x + 1, y);
-    txp(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
-  }
-  {
-    const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
-    for (int idx = threadIdx.x; idx < (TX + 2) * (TY + 2); idx += NT) {
-      int x = ox - 1 + idx % (TX + 2), y = oy - 1 + idx / (TX + 2);
-      lpd(x, y) = T(-2.) * sdp(x, y) * rdxy + (sdp(x + 1, y) + sdp(x - 1, y)) * rdx2 +
-                  (sdp(x, y + 1) + sdp(x, y - 1)) * rdy2;
-      lpp(x, y) = T(-2.) * spt(x, y) * rdxy + (spt(x + 1, y) + spt(x - 1, y)) * rdx2 +
-                  (spt(x, y + 1) + spt(x, y - 1)) * rdy2;
-    }
-  }
-  __syncthreads();
-
-  // outer sweeps (PPM): x fluxes on the tile's rows, y fluxes on its columns
-  for (int idx = threadIdx.x; idx < (TX + 1) * TY; idx += NT) {
-    int x = ox + idx % (TX + 1), y = oy + idx / (TX + 1);
-    T cx = dtdx * suc(x, y);
-    fxd(x, y) = flux<T, V>(tyd.ptr(x, y), 1, cx) * cx;
-    fxp(x, y) = flux<T, V>(typ.ptr(x, y), 1, cx);
-  }
-  for (int idx = threadIdx.x; idx < TX * (TY + 1); idx += NT) {
-    int x = ox + idx % TX, y = oy + idx / TX;
-    T cy = dtdx * svc(x, y);
-    fyd(x, y) = flux<T, V>(txd.ptr(x, y), TX, cy) * cy;
-    fyp(x, y) = flux<T, V>(txp.ptr(x, y), TX, cy);
-  }
-  __syncthreads();
-
-  // updates, mod_sw_dyn.f90:163-172,193-202,230-237,258-267 (C);
-  // 490-499,519-528,555-562,582-591 (D)
-  const int xhi = g.nx - 1 + hi, yhi = g.ny - 1 + hi;
-  const T dxv = dtdx * T(c.vdx), dyv = dtdy * T(c.vdy), vdx = T(c.vdx), vdy = T(c.vdy);
-  for (int idx = threadIdx.x; idx < TX * TY; idx += NT) {
-    int x = ox + idx % TX, y = oy + idx / TX;
-    if (x > xhi || y > yhi) continue;
-    T d = sdp(x, y);
-    T v = d - (fxd(x + 1, y) - fxd(x, y) + dxv * (lpd(x + 1, y) - T(2.) * lpd(x, y) + lpd(x - 1, y)));
-    v = v - (fyd(x, y + 1) - fyd(x, y) + dyv * (lpd(x, y + 1) - T(2.) * lpd(x, y) + lpd(x, y - 1)));
-    T q = d * spt(x, y) - (fxp(x + 1, y) * fxd(x + 1, y) - fxp(x, y) * fxd(x, y) +
-                           vdx * ((lpp(x + 1, y) - lpp(x, y)) * fxd(x + 1, y) - (lpp(x, y) - lpp(x - 1, y)) * fxd(x, y)));
-    q = q - (fyp(x, y + 1) * fyd(x, y + 1) - fyp(x, y) * fyd(x, y) +
-             vdy * ((lpp(x, y + 1) - lpp(x, y)) * fyd(x, y + 1) - (lpp(x, y) - lpp(x, y - 1)) * fyd(x, y)));
-    if (heat) q = q + dt * d * T(heat[g.at(x, y, k)]);
-    q = q / v;
-    long long o = g.at(x, y, k);
-    dpo[o] = v;
-    pto[o] = q;
-    if (nonfinite) {
-      bool inside = x >= 0 && x < g.nx && y >= 0 && y < g.ny;
-      flag_nonfinite(nonfinite, inside && !(finite_(v) && finite_(q)));
-    }
-  }
-}
-
 // ====================================================== column pressure ====
 // plev = ptop + suffix sum of dp from the model top, pkap = plev**kappa,
 // hydrostatic gz from the bottom (src/mod_sw_dyn.f90:276-292 and 606-626).
@@ -208,7 +59,7 @@ template <typename T>
 __global__ void __launch_bounds__(64) k_column(Geom g, Consts c, const T* __restrict__ dpl, const T* __restrict__ ptl,
                                                double* __restrict__ pkap, double* __restrict__ gz, int lo, int hi,
                                                double* __restrict__ plev_out) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   double* spk = reinterpret_cast<double*>(smem);  // [L+1][64]
   const int w = g.nx - lo + hi;
   const int hgt = g.ny - lo + hi;
@@ -286,287 +137,6 @@ static __global__ void k_corners(Geom g, const double* __restrict__ pkap, const 
     if (with_pkap) pkapb[o] = corner(pkap, o, g.P);
     long long o1 = g.at(x, y, l + (with_pkap ? 1 : 0));
     gzb[o1] = corner(gz, o1, g.P);
-  }
-}
-
-// ======================================================== C-grid momentum ==
-// Second layer loop of the C-grid half step, src/mod_sw_dyn.f90:294-412:
-// kinetic energy (PPM, with the A-grid winds of layer nlay that the first
-// loop leaves in ua/va), vorticity, pressure-gradient force, and the
-// vorticity-flux update of uc and vc on the interior.
-template <typename T, int TX, int TY>
-struct CMomSmem {
-  static constexpr size_t bytes =
-      2 * box_bytes<T>(TX + 7, TY + 7) + 2 * box_bytes<T>(TX + 3, TY + 3) + 4 * box_bytes<double>(TX + 1, TY + 1) +
-      2 * box_bytes<T>(TX + 6, TY + 6) + 2 * box_bytes<T>(TX + 1, TY + 1) + box_bytes<T>(TX + 5, TY + 5) +
-      box_bytes<T>(TX + 1, TY + 1) + box_bytes<T>(TX, TY + 5) + box_bytes<T>(TX + 5, TY) + box_bytes<T>(TX + 1, TY + 1);
-};
-
-template <typename T, int TX, int TY>
-__global__ void __launch_bounds__(NT) k_c_mom(Geom g, Consts c, const T* __restrict__ ud, const T* __restrict__ vd,
-                                              const double* __restrict__ pkap, const double* __restrict__ gz,
-                                              T* __restrict__ uc, T* __restrict__ vc) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  unsigned char* p = smem;
-  const int k = blockIdx.z, L = g.L;
-  const int ox = blockIdx.x * TX, oy = blockIdx.y * TY;
-  const T dt = T(c.dt), dtdx = T(c.dtdx), dtdy = T(c.dtdy), rA = T(c.rA);
-  const T rdx = T(c.rdx), rdy = T(c.rdy);
-
-  Sm<T> sud = carve<T>(p, ox - 4, oy - 3, TX + 7, TY + 7);
-  Sm<T> svd = carve<T>(p, ox - 3, oy - 4, TX + 7, TY + 7);
-  Sm<T> udL = carve<T>(p, ox - 2, oy - 2, TX + 3, TY + 3);
-  Sm<T> vdL = carve<T>(p, ox - 2, oy - 2, TX + 3, TY + 3);
-  Sm<double> pk0 = carve<double>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<double> pk1 = carve<double>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<double> gz0 = carve<double>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<double> gz1 = carve<double>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<T> uc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
-  Sm<T> vc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
-  Sm<T> uaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<T> vaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<T> vor = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
-  Sm<T> ke = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<T> tU = carve<T>(p, ox, oy - 2, TX, TY + 5);
-  Sm<T> tV = carve<T>(p, ox - 2, oy, TX + 5, TY);
-  Sm<T> lap = carve<T>(p, ox, oy, TX + 1, TY + 1);
-
-  load_box(sud.p, ud, g, k, ox - 4, oy - 3, TX + 7, TY + 7);
-  load_box(svd.p, vd, g, k, ox - 3, oy - 4, TX + 7, TY + 7);
-  load_box(udL.p, ud, g, L - 1, ox - 2, oy - 2, TX + 3, TY + 3);
-  load_box(vdL.p, vd, g, L - 1, ox - 2, oy - 2, TX + 3, TY + 3);
-  load_box(pk0.p, pkap, g, k, ox - 1, oy - 1, TX + 1, TY + 1);
-  load_box(pk1.p, pkap, g, k + 1, ox - 1, oy - 1, TX + 1, TY + 1);
-  load_box(gz0.p, gz, g, k, ox - 1, oy - 1, TX + 1, TY + 1);
-  load_box(gz1.p, gz, g, k + 1, ox - 1, oy - 1, TX + 1, TY + 1);
-  __syncthreads();
-
-  // C-grid winds of this layer (first-loop values, mod_sw_dyn.f90:110-117)
-  for (int idx = threadIdx.x; idx < (TX + 6) * (TY + 6); idx += NT) {
-    int x = ox - 3 + idx % (TX + 6), y = oy - 3 + idx / (TX + 6);
-    T ub = T(.5) * (sud(x, y) + sud(x - 1, y));
-    uc1(x, y) = T(.5) * (ub + T(.5) * (sud(x, y + 1) + sud(x - 1, y + 1)));
-    T vb = T(.5) * (svd(x, y) + svd(x, y - 1));
-    vc1(x, y) = T(.5) * (vb + T(.5) * (svd(x + 1, y) + svd(x + 1, y - 1)));
-  }
-  // A-grid winds of layer nlay (mod_sw_dyn.f90:110-125 at k = nlay)
-  for (int idx = threadIdx.x; idx < (TX + 1) * (TY + 1); idx += NT) {
-    int x = ox - 1 + idx % (TX + 1), y = oy - 1 + idx / (TX + 1);
-    T ub = T(.5) * (udL(x, y) + udL(x - 1, y));
-    T ucl = T(.5) * (ub + T(.5) * (udL(x, y + 1) + udL(x - 1, y + 1)));
-    uaL(x, y) = T(.5) * (ucl + T(.25) * (udL(x + 1, y) + udL(x, y) + udL(x + 1, y + 1) + udL(x, y + 1)));
-    T vb = T(.5) * (vdL(x, y) + vdL(x, y - 1));
-    T vcl = T(.5) * (vb + T(.5) * (vdL(x + 1, y) + vdL(x + 1, y - 1)));
-    vaL(x, y) = T(.5) * (vcl + T(.25) * (vdL(x, y + 1) + vdL(x, y) + vdL(x + 1, y + 1) + vdL(x + 1, y)));
-  }
-  __syncthreads();
-
-  // vorticity (mod_sw_dyn.f90:319-323) and kinetic energy (:299-317)
-  const T f = T(c.coriolis);
-  for (int idx = threadIdx.x; idx < (TX + 5) * (TY + 5); idx += NT) {
-    int x = ox - 2 + idx % (TX + 5), y = oy - 2 + idx / (TX + 5);
-    vor(x, y) = f - (uc1(x, y) - uc1(x, y - 1)) * rdy + (vc1(x, y) - vc1(x - 1, y)) * rdx;
-  }
-  for (int idx = threadIdx.x; idx < (TX + 1) * (TY + 1); idx += NT) {
-    int x = ox - 1 + idx % (TX + 1), y = oy - 1 + idx / (TX + 1);
-    // q(j) = vc(i, j+1) and q(i) = uc(i+1, j): the shifted sections of :300,310
-    T fy = flux<T, PPM_UNC>(vc1.ptr(x, y + 1), TX + 6, dtdy * vaL(x, y));
-    T kv = vaL(x, y) * fy;
-    T fx = flux<T, PPM_UNC>(uc1.ptr(x + 1, y), 1, dtdx * uaL(x, y));
-    ke(x, y) = T(.5) * (kv + uaL(x, y) * fx);
-  }
-  __syncthreads();
-
-  // vorticity advection: inner sweeps and Laplacian (mod_sw_dyn.f90:344-367, 388-397)
-  for (int idx = threadIdx.x; idx < TX * (TY + 5); idx += NT) {
-    int x = ox + idx % TX, y = oy - 2 + idx / TX;
-    // c(i) = cx(i-1, j): the shifted section cx(is+1:ie-3, j) of :355
-    T c0 = dtdx * sud(x - 1, y), c1 = dtdx * sud(x, y);
-    T den = T(1) / (T(1) - dtdx * (sud(x, y) - sud(x - 1, y)));
-    T f0 = (c0 > T(0)) ? vor(x - 1, y) : vor(x, y);
-    T f1 = (c1 > T(0)) ? vor(x, y) : vor(x + 1, y);
-    tU(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
-  }
-  for (int idx = threadIdx.x; idx < (TX + 5) * TY; idx += NT) {
-    int x = ox - 2 + idx % (TX + 5), y = oy + idx / (TX + 5);
-    // c(j) = cy(i, j-1): the shifted section cy(i, js+1:je-3) of :390
-    T c0 = dtdx * svd(x, y - 1), c1 = dtdx * svd(x, y);
-    T den = T(1) / (T(1) - dtdy * (svd(x, y) - svd(x, y - 1)));
-    T f0 = (c0 > T(0)) ? vor(x, y - 1) : vor(x, y);
-    T f1 = (c1 > T(0)) ? vor(x, y) : vor(x, y + 1);
-    tV(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
-  }
-  {
-    const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
-    for (int idx = threadIdx.x; idx < (TX + 1) * (TY + 1); idx += NT) {
-      int x = ox + idx % (TX + 1), y = oy + idx / (TX + 1);
-      lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 +
-                  (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
-    }
-  }
-  __syncthreads();
-
-  // uc, vc updates (mod_sw_dyn.f90:369-381, 399-411) with the PGF (:325-339)
-  const T vdx = T(c.vdx), vdy = T(c.vdy);
-  for (int idx = threadIdx.x; idx < TX * TY; idx += NT) {
-    int x = ox + idx % TX, y = oy + idx / TX;
-    if (x >= g.nx || y >= g.ny) continue;
-    double pgx = ((pk0(x, y) - pk1(x - 1, y)) * (gz0(x - 1, y) - gz1(x, y)) +
-                  (pk0(x - 1, y) - pk1(x, y)) * (gz1(x - 1, y) - gz0(x, y))) /
-                 (pk0(x, y) - pk1(x - 1, y) + pk0(x - 1, y) - pk1(x, y));
-    double pgy = ((pk0(x, y) - pk1(x, y - 1)) * (gz0(x, y - 1) - gz1(x, y)) +
-                  (pk0(x, y - 1) - pk1(x, y)) * (gz1(x, y - 1) - gz0(x, y))) /
-                 (pk0(x, y) - pk1(x, y - 1) + pk0(x, y - 1) - pk1(x, y));
-    // q(j) = tmp(i, j+1) (the section tmp(i, js+5:je-3) of :370)
-    T fy = flux<T, PPM_UNC>(tU.ptr(x, y + 1), TX, dtdx * svd(x, y));
-    T u = uc1(x, y) + dt * (svd(x, y) * fy + vdy * (lap(x, y + 1) - lap(x, y))) -
-          dtdx * (ke(x, y) - ke(x - 1, y) - T(pgx));
-    // q(i) = tmp(i+1, j) (the section tmp(is+5:ie-3, j) of :400)
-    T fx = flux<T, PPM_UNC>(tV.ptr(x + 1, y), 1, dtdx * sud(x, y));
-    T v = vc1(x, y) - dt * (sud(x, y) * fx + vdx * (lap(x + 1, y) - lap(x, y))) -
-          dtdy * (ke(x, y) - ke(x, y - 1) - T(pgy));
-    long long o = g.at(x, y, k);
-    uc[o] = u;
-    vc[o] = v;
-  }
-}
-
-// ======================================================== D-grid momentum ==
-// Third layer loop of the D-grid step, src/mod_sw_dyn.f90:634-771.  The
-// B-grid winds ub/vb, the Courant numbers cx/cy and denom_x/denom_y are the
-// ones the first loop leaves behind for layer nlay (:441-454), so they are
-// built from uc/vc of layer nlay.
-template <typename T, int TX, int TY>
-struct DMomSmem {
-  static constexpr size_t bytes =
-      2 * box_bytes<T>(TX + 6, TY + 6) + box_bytes<T>(TX + 1, TY + 5) + box_bytes<T>(TX + 5, TY + 1) +
-      4 * box_bytes<double>(TX + 1, TY + 1) + box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 5, TY + 5) +
-      box_bytes<T>(TX + 3, TY + 3) + box_bytes<T>(TX + 1, TY + 1) * 4 + box_bytes<T>(TX, TY + 5) +
-      box_bytes<T>(TX + 5, TY) + box_bytes<T>(TX + 1, TY + 1);
-};
-
-template <typename T, int TX, int TY>
-__global__ void __launch_bounds__(NT) k_d_mom(Geom g, Consts c, const T* __restrict__ ud, const T* __restrict__ vd,
-                                              const T* __restrict__ uc, const T* __restrict__ vc,
-                                              const double* __restrict__ pkapb, const double* __restrict__ gzb,
-                                              T* __restrict__ udo, T* __restrict__ vdo, int* nonfinite) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  unsigned char* p = smem;
-  const int k = blockIdx.z, L = g.L;
-  const int ox = blockIdx.x * TX, oy = blockIdx.y * TY;
-  const T dt = T(c.dt), dtdx = T(c.dtdx), dtdy = T(c.dtdy), rA = T(c.rA);
-  const T rdx = T(c.rdx), rdy = T(c.rdy);
-
-  Sm<T> sud = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
-  Sm<T> svd = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
-  Sm<T> ucL = carve<T>(p, ox, oy - 3, TX + 1, TY + 5);
-  Sm<T> vcL = carve<T>(p, ox - 3, oy, TX + 5, TY + 1);
-  Sm<double> pb0 = carve<double>(p, ox, oy, TX + 1, TY + 1);
-  Sm<double> pb1 = carve<double>(p, ox, oy, TX + 1, TY + 1);
-  Sm<double> gb0 = carve<double>(p, ox, oy, TX + 1, TY + 1);
-  Sm<double> gb1 = carve<double>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> vor = carve<T>(p, ox - 3, oy - 3, TX + 5, TY + 5);
-  Sm<T> dv0 = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
-  Sm<T> dv2 = carve<T>(p, ox - 1, oy - 1, TX + 3, TY + 3);
-  Sm<T> dv4 = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> ubL = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> vbL = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> ke = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> tU = carve<T>(p, ox, oy - 3, TX, TY + 5);
-  Sm<T> tV = carve<T>(p, ox - 3, oy, TX + 5, TY);
-  Sm<T> lap = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-
-  load_box(sud.p, ud, g, k, ox - 3, oy - 3, TX + 6, TY + 6);
-  load_box(svd.p, vd, g, k, ox - 3, oy - 3, TX + 6, TY + 6);
-  load_box(ucL.p, uc, g, L - 1, ox, oy - 3, TX + 1, TY + 5);
-  load_box(vcL.p, vc, g, L - 1, ox - 3, oy, TX + 5, TY + 1);
-  load_box(pb0.p, pkapb, g, k, ox, oy, TX + 1, TY + 1);
-  load_box(pb1.p, pkapb, g, k + 1, ox, oy, TX + 1, TY + 1);
-  load_box(gb0.p, gzb, g, k, ox, oy, TX + 1, TY + 1);
-  load_box(gb1.p, gzb, g, k + 1, ox, oy, TX + 1, TY + 1);
-  __syncthreads();
-
-  const T f = T(c.coriolis);
-  // vorticity (mod_sw_dyn.f90:659-663), divergence (:682-685), B-grid winds of layer nlay (:441-444)
-  for (int idx = threadIdx.x; idx < (TX + 5) * (TY + 5); idx += NT) {
-    int x = ox - 3 + idx % (TX + 5), y = oy - 3 + idx / (TX + 5);
-    vor(x, y) = f - (sud(x, y + 1) - sud(x, y)) * rdy + (svd(x + 1, y) - svd(x, y)) * rdx;
-    int xd = x + 1, yd = y + 1;
-    dv0(xd, yd) = rdx * (sud(xd, yd) - sud(xd - 1, yd)) + rdy * (svd(xd, yd) - svd(xd, yd - 1));
-  }
-  for (int idx = threadIdx.x; idx < (TX + 1) * (TY + 1); idx += NT) {
-    int x = ox + idx % (TX + 1), y = oy + idx / (TX + 1);
-    ubL(x, y) = T(.5) * (ucL(x, y) + ucL(x, y - 1));
-    vbL(x, y) = T(.5) * (vcL(x, y) + vcL(x - 1, y));
-  }
-  __syncthreads();
-
-  const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
-  // kinetic energy with PPM_CONSTRAINED (:639-657)
-  for (int idx = threadIdx.x; idx < (TX + 1) * (TY + 1); idx += NT) {
-    int x = ox + idx % (TX + 1), y = oy + idx / (TX + 1);
-    T fy = flux<T, PPM_CON>(svd.ptr(x, y), TX + 6, dtdy * vbL(x, y));
-    T kv = vbL(x, y) * fy;
-    T fx = flux<T, PPM_CON>(sud.ptr(x, y), 1, dtdx * ubL(x, y));
-    ke(x, y) = T(.5) * (kv + ubL(x, y) * fx);
-  }
-  // del^2 of the divergence (:688-692)
-  for (int idx = threadIdx.x; idx < (TX + 3) * (TY + 3); idx += NT) {
-    int x = ox - 1 + idx % (TX + 3), y = oy - 1 + idx / (TX + 3);
-    dv2(x, y) = T(-2.) * dv0(x, y) * rdxy + (dv0(x + 1, y) + dv0(x - 1, y)) * rdx2 + (dv0(x, y + 1) + dv0(x, y - 1)) * rdy2;
-  }
-  // inner sweeps of the vorticity with the layer-nlay Courant numbers (:708-722, 744-753)
-  for (int idx = threadIdx.x; idx < TX * (TY + 5); idx += NT) {
-    int x = ox + idx % TX, y = oy - 3 + idx / TX;
-    T c0 = dtdx * ucL(x, y), c1 = dtdx * ucL(x + 1, y);
-    T den = T(1) / (T(1) - dtdx * (ucL(x + 1, y) - ucL(x, y)));
-    T f0 = (c0 > T(0)) ? vor(x - 1, y) : vor(x, y);
-    T f1 = (c1 > T(0)) ? vor(x, y) : vor(x + 1, y);
-    tU(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
-  }
-  for (int idx = threadIdx.x; idx < (TX + 5) * TY; idx += NT) {
-    int x = ox - 3 + idx % (TX + 5), y = oy + idx / (TX + 5);
-    T c0 = dtdx * vcL(x, y), c1 = dtdx * vcL(x, y + 1);
-    T den = T(1) / (T(1) - dtdy * (vcL(x, y + 1) - vcL(x, y)));
-    T f0 = (c0 > T(0)) ? vor(x, y - 1) : vor(x, y);
-    T f1 = (c1 > T(0)) ? vor(x, y) : vor(x, y + 1);
-    tV(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
-  }
-  for (int idx = threadIdx.x; idx < (TX + 1) * (TY + 1); idx += NT) {
-    int x = ox - 1 + idx % (TX + 1), y = oy - 1 + idx / (TX + 1);
-    lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 + (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
-  }
-  __syncthreads();
-  // del^4 damping (:695-702)
-  const T divdamp = T(c.divdamp);
-  for (int idx = threadIdx.x; idx < (TX + 1) * (TY + 1); idx += NT) {
-    int x = ox + idx % (TX + 1), y = oy + idx / (TX + 1);
-    T d4 = T(-2.) * dv2(x, y) * rdxy + (dv2(x + 1, y) + dv2(x - 1, y)) * rdx2 + (dv2(x, y + 1) + dv2(x, y - 1)) * rdy2;
-    dv4(x, y) = divdamp * d4;
-  }
-  __syncthreads();
-
-  // ud, vd updates (:724-738, 755-769) with the B-grid PGF (:665-679)
-  const T vdx = T(c.vdx), vdy = T(c.vdy);
-  for (int idx = threadIdx.x; idx < TX * TY; idx += NT) {
-    int x = ox + idx % TX, y = oy + idx / TX;
-    if (x >= g.nx || y >= g.ny) continue;
-    double pgx = ((pb0(x + 1, y) - pb1(x, y)) * (gb0(x, y) - gb1(x + 1, y)) +
-                  (pb0(x, y) - pb1(x + 1, y)) * (gb1(x, y) - gb0(x + 1, y))) /
-                 (pb0(x + 1, y) - pb1(x, y) + pb0(x, y) - pb1(x + 1, y));
-    double pgy = ((pb0(x, y + 1) - pb1(x, y)) * (gb0(x, y) - gb1(x, y + 1)) +
-                  (pb0(x, y) - pb1(x, y + 1)) * (gb1(x, y) - gb0(x, y + 1))) /
-                 (pb0(x, y + 1) - pb1(x, y) + pb0(x, y) - pb1(x, y + 1));
-    long long o = g.at(x, y, k);
-    T fy = flux<T, PPM_CON>(tU.ptr(x, y), TX, dtdx * vcL(x, y));
-    T u = sud(x, y) + dt * (vc[o] * fy + vdy * (lap(x, y) - lap(x, y - 1))) -
-          dtdx * (ke(x + 1, y) - ke(x, y) - dv4(x + 1, y) + dv4(x, y) - T(pgx));
-    T fx = flux<T, PPM_CON>(tV.ptr(x, y), 1, dtdx * ucL(x, y));
-    T v = svd(x, y) - dt * (uc[o] * fx + vdx * (lap(x, y) - lap(x - 1, y))) -
-          dtdy * (ke(x, y + 1) - ke(x, y) - dv4(x, y + 1) + dv4(x, y) - T(pgy));
-    udo[o] = u;
-    vdo[o] = v;
-    flag_nonfinite(nonfinite, !(finite_(u) && finite_(v)));
   }
 }
 

@@ -3,8 +3,15 @@
 // (T = float), which each define ATM_FORM_T and ATM_OPS_NAME.
 #pragma once
 
+#include <cudaTypedefs.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "atm_kernels.cuh"
 #include "atm_ops.h"
+#include "atm_sweeps.cuh"
 
 namespace atm {
 namespace {
@@ -12,33 +19,91 @@ namespace {
 using T = ATM_FORM_T;
 constexpr int TX = 32, TY = 8;
 
+// ---- TMA tensor maps: one per (buffer, box shape), built once and cached
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+using MapKey = std::tuple<const void*, int, int, int, int, int, int>;
+std::mutex g_map_mu;
+std::map<MapKey, CUtensorMap> g_maps;
+
+// map of a field (K levels of ny+14 rows of pitch P, element size es) for
+// boxes of bw x bh elements
+cudaError_t tmap(const void* base, int es, const Geom& g, int K, int bw, int bh, CUtensorMap* out) {
+  MapKey key{base, es, g.P, g.NYP, K, bw, bh};
+  std::lock_guard<std::mutex> lock(g_map_mu);
+  auto it = g_maps.find(key);
+  if (it != g_maps.end()) {
+    *out = it->second;
+    return cudaSuccess;
+  }
+  auto fn = encode_fn();
+  if (!fn) return cudaErrorNotSupported;
+  CUtensorMap m;
+  cuuint64_t dims[3] = {(cuuint64_t)g.P, (cuuint64_t)g.NYP, (cuuint64_t)K};
+  cuuint64_t strides[2] = {(cuuint64_t)g.P * es, (cuuint64_t)g.S * es};
+  cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(&m, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                  const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  g_maps.emplace(key, m);
+  *out = m;
+  return cudaSuccess;
+}
+
 inline dim3 tiles(int lo, int hi, const Geom& g, int layers) {
   int w = g.nx - lo + hi, h = g.ny - lo + hi;
   return dim3((w + TX - 1) / TX, (h + TY - 1) / TY, layers);
 }
 
+template <typename K>
+cudaError_t smem_attr(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 cudaError_t setup() {
   cudaError_t e;
-  e = cudaFuncSetAttribute(k_mass<T, TX, TY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MassSmem<T, TX, TY>::bytes);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_mass<T, TX, TY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MassSmem<T, TX, TY>::bytes);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_c_mom<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CMomSmem<T, TX, TY>::bytes);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_d_mom<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DMomSmem<T, TX, TY>::bytes);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_column<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (MAX_LAYERS + 1) * 64 * 8);
+  if ((e = smem_attr(k_mass2<T, TX, TY, true>, MassL<T, TX, TY, true>::bytes)) != cudaSuccess) return e;
+  if ((e = smem_attr(k_mass2<T, TX, TY, false>, MassL<T, TX, TY, false>::bytes)) != cudaSuccess) return e;
+  if ((e = smem_attr(k_c_mom2<T, TX, TY>, CMomL<T, TX, TY>::bytes)) != cudaSuccess) return e;
+  if ((e = smem_attr(k_d_mom2<T, TX, TY>, DMomL<T, TX, TY>::bytes)) != cudaSuccess) return e;
+  return smem_attr(k_column<T>, (MAX_LAYERS + 1) * 64 * 8);
 }
 
 cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt, const void* u, const void* v,
-                 const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, bool cgrid, cudaStream_t s) {
+                 const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, int* timeout, bool cgrid,
+                 cudaStream_t s) {
   dim3 grid = tiles(lo, hi, g, g.L);
-  if (cgrid)
-    k_mass<T, TX, TY, true><<<grid, NT, MassSmem<T, TX, TY>::bytes, s>>>(
-        g, c, (const T*)dp, (const T*)pt, (const T*)u, (const T*)v, heat, (T*)dpo, (T*)pto, lo, hi, nonfinite);
-  else
-    k_mass<T, TX, TY, false><<<grid, NT, MassSmem<T, TX, TY>::bytes, s>>>(
-        g, c, (const T*)dp, (const T*)pt, (const T*)u, (const T*)v, heat, (T*)dpo, (T*)pto, lo, hi, nonfinite);
+  constexpr int es = sizeof(T);
+  CUtensorMap md, mp, mu, mv;
+  cudaError_t e;
+  if (cgrid) {
+    using Lay = MassL<T, TX, TY, true>;
+    if ((e = tmap(dp, es, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, es, g, g.L, Lay::WD, Lay::HD, &mp)) ||
+        (e = tmap(u, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, es, g, g.L, Lay::WV, Lay::HV, &mv)))
+      return e;
+    k_mass2<T, TX, TY, true><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (T*)dpo, (T*)pto, lo, hi,
+                                                          nonfinite, timeout);
+  } else {
+    using Lay = MassL<T, TX, TY, false>;
+    if ((e = tmap(dp, es, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, es, g, g.L, Lay::WD, Lay::HD, &mp)) ||
+        (e = tmap(u, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, es, g, g.L, Lay::WV, Lay::HV, &mv)))
+      return e;
+    k_mass2<T, TX, TY, false><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (T*)dpo, (T*)pto, lo, hi,
+                                                           nonfinite, timeout);
+  }
   return cudaGetLastError();
 }
 
@@ -57,16 +122,34 @@ cudaError_t heating(const Geom& g, const Consts& c, const void* dpl, const doubl
 }
 
 cudaError_t c_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const double* pkap, const double* gz,
-                  void* uc, void* vc, cudaStream_t s) {
-  k_c_mom<T, TX, TY><<<tiles(0, 0, g, g.L), NT, CMomSmem<T, TX, TY>::bytes, s>>>(g, c, (const T*)ud, (const T*)vd, pkap,
-                                                                                gz, (T*)uc, (T*)vc);
+                  void* uc, void* vc, int* timeout, cudaStream_t s) {
+  using Lay = CMomL<T, TX, TY>;
+  constexpr int es = sizeof(T);
+  CUtensorMap mu, mv, muL, mvL, mpk, mgz;
+  cudaError_t e;
+  if ((e = tmap(ud, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, es, g, g.L, Lay::WV, Lay::HV, &mv)) ||
+      (e = tmap(ud, es, g, g.L, Lay::WL, Lay::HL, &muL)) || (e = tmap(vd, es, g, g.L, Lay::WL, Lay::HL, &mvL)) ||
+      (e = tmap(pkap, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpk)) || (e = tmap(gz, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgz)))
+    return e;
+  k_c_mom2<T, TX, TY><<<tiles(0, 0, g, g.L), NT, Lay::bytes, s>>>(mu, mv, muL, mvL, mpk, mgz, g, c, (T*)uc, (T*)vc,
+                                                                  timeout);
   return cudaGetLastError();
 }
 
 cudaError_t d_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const void* uc, const void* vc,
-                  const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, cudaStream_t s) {
-  k_d_mom<T, TX, TY><<<tiles(0, 0, g, g.L), NT, DMomSmem<T, TX, TY>::bytes, s>>>(
-      g, c, (const T*)ud, (const T*)vd, (const T*)uc, (const T*)vc, pkapb, gzb, (T*)udo, (T*)vdo, nonfinite);
+                  const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, int* timeout,
+                  cudaStream_t s) {
+  using Lay = DMomL<T, TX, TY>;
+  constexpr int es = sizeof(T);
+  CUtensorMap mu, mv, muL, mvL, muc, mvc, mpb, mgb;
+  cudaError_t e;
+  if ((e = tmap(ud, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, es, g, g.L, Lay::WU, Lay::HU, &mv)) ||
+      (e = tmap(uc, es, g, g.L, Lay::WUL, Lay::HUL, &muL)) || (e = tmap(vc, es, g, g.L, Lay::WVL, Lay::HVL, &mvL)) ||
+      (e = tmap(uc, es, g, g.L, Lay::WC, Lay::HC, &muc)) || (e = tmap(vc, es, g, g.L, Lay::WC, Lay::HC, &mvc)) ||
+      (e = tmap(pkapb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpb)) || (e = tmap(gzb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgb)))
+    return e;
+  k_d_mom2<T, TX, TY><<<tiles(0, 0, g, g.L), NT, Lay::bytes, s>>>(mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c,
+                                                                  (T*)udo, (T*)vdo, nonfinite, timeout);
   return cudaGetLastError();
 }
 

@@ -15,17 +15,18 @@ struct Ops {
   cudaError_t (*setup)();
   // C- or D-grid mass/potential-temperature sweep of every layer
   cudaError_t (*mass)(const Geom&, const Consts&, const void* dp, const void* pt, const void* u, const void* v,
-                      const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, bool cgrid,
-                      cudaStream_t);
+                      const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, int* timeout,
+                      bool cgrid, cudaStream_t);
   // plev/pkap/gz columns over [lo, n-1+hi]^2
   cudaError_t (*column)(const Geom&, const Consts&, const void* dpl, const void* ptl, double* pkap, double* gz,
                         int lo, int hi, double* plev, cudaStream_t);
   cudaError_t (*heating)(const Geom&, const Consts&, const void* dpl, const double* net_flux, double* heat,
                          cudaStream_t);
   cudaError_t (*c_mom)(const Geom&, const Consts&, const void* ud, const void* vd, const double* pkap,
-                       const double* gz, void* uc, void* vc, cudaStream_t);
+                       const double* gz, void* uc, void* vc, int* timeout, cudaStream_t);
   cudaError_t (*d_mom)(const Geom&, const Consts&, const void* ud, const void* vd, const void* uc, const void* vc,
-                       const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, cudaStream_t);
+                       const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, int* timeout,
+                       cudaStream_t);
   // periodic halo fill (copy = false) or ring copy src -> f (copy = true) of nf fields
   cudaError_t (*ring)(const Geom&, void* const* f, const void* const* src, int nf, int K, bool copy, cudaStream_t);
   cudaError_t (*remap_winds)(const Geom&, const RemapArgs&, const void* dp, const void* ud, const void* vd,
@@ -48,6 +49,9 @@ cudaError_t corners(const Geom&, const double* pkap, const double* gz, double* p
 
 // x**y and log(x) of the portable math on the device (tests)
 cudaError_t device_pow_log(const double* x, double y, double* p, double* l, int n, cudaStream_t);
+
+// count of arguments where div_const<3>/<12> differs from IEEE division (tests)
+cudaError_t device_div_check(unsigned long long n, unsigned long long seed, unsigned long long* bad, cudaStream_t);
 
 // largest number of layers the vertical remap supports
 constexpr int MAX_LAYERS = 128;

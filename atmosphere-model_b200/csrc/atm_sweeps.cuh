@@ -1,0 +1,647 @@
+// Per-layer sweep kernels of the B200 dynamical core (one CTA = one
+// TX x TY tile of one layer), second generation:
+//  * the input tiles plus their stencil halo arrive by TMA (atm_tma.cuh);
+//  * every PPM sweep is split into per-cell stages: the monotone slopes
+//    dqi_mono (src/mod_sw_dyn.f90:870-875) once per cell, for
+//    PPM_CONSTRAINED also the edge values once per cell (:877-911), and
+//    then the per-interface flux (:802-838) from those, as the reference's
+//    ppm/flux pair does for a whole row.
+// Formulas, index shifts and evaluation order are those of the first
+// generation (and of the reference), so the FP64 results are unchanged.
+#pragma once
+
+#include "atm_kernels.cuh"
+#include "atm_tma.cuh"
+
+namespace atm {
+
+// Edge anomalies of a cell from precomputed monotone slopes.  q points at
+// the cell (cell spacing sq), mono at its monotone slope (spacing sm).  The
+// raw slope dqi of the cell is recomputed from q exactly as slopes() forms it.
+template <typename T, int V>
+__device__ __forceinline__ void edges_pre(const T* q, int sq, const T* mono, int sm, T& eL, T& eR) {
+  const T q0 = q[0];
+  eL = (q[-sq] - q0) * T(0.5) + div_const<3>(mono[-sm] - mono[0]);
+  eR = (q[sq] - q0) * T(0.5) + div_const<3>(mono[0] - mono[sm]);
+  if (V == PPM_CON || V == PPM_NN) {
+    const T d0 = (q[sq] - q[-sq]) * T(0.25);
+    const T lim = T(2) * fab(d0);
+    eL = -cpsign(mn(lim, fab(eL)), d0);
+    eR = +cpsign(mn(lim, fab(eR)), d0);
+    if (V == PPM_NN) {
+      eL = mx(eL, -q0);
+      eR = mx(eR, -q0);
+      T a = eR - eL;
+      T b = T(-3) * (eR + eL);
+      if ((fab(a) < -b) && (q0 + a * a / (T(4) * b) + div_const<12>(b) < T(0))) {
+        if (eL * eR > T(0)) {
+          eL = T(0);
+          eR = T(0);
+        } else if (eL > eR) {
+          eL = T(2) * fab(eR);
+        } else {
+          eR = T(2) * fab(eL);
+        }
+      }
+    }
+  }
+}
+
+// Flux at the interface between cells i-1 and i with slopes precomputed
+// (PPM_UNCONSTRAINED / PPM_NONNEGATIVE): only the upwind cell's edges.
+// q and mono point at cell i.
+template <typename T, int V>
+__device__ __forceinline__ T flux_pre(const T* q, int sq, const T* mono, int sm, T c) {
+  T sa = fab(c);
+  T k1 = (T(1) - T(2) * sa) * (T(1) - sa);
+  T k2 = sa * (sa - T(1));
+  T eL, eR;
+  if (c > T(0)) {
+    edges_pre<T, V>(q - sq, sq, mono - sm, sm, eL, eR);
+    return q[-sq] + k1 * eR + k2 * eL;
+  }
+  edges_pre<T, V>(q, sq, mono, sm, eL, eR);
+  return q[0] + k1 * eL + k2 * eR;
+}
+
+// Flux with precomputed edges (PPM_CONSTRAINED): q points at cell i
+// (spacing sq), eL and eR at its edges (spacing se).
+template <typename T>
+__device__ __forceinline__ T flux_con_pre(const T* q, int sq, const T* eL, const T* eR, int se, T c) {
+  const T eLm = eL[-se], eRm = eR[-se], eL0 = eL[0], eR0 = eR[0];
+  if ((T(3) * fab(eL0 + eR0) > fab(eL0 - eR0)) && (T(3) * fab(eLm + eRm) > fab(eLm - eRm)))
+    return (c > T(0)) ? q[-sq] : q[0];
+  T sa = fab(c);
+  T k1 = (T(1) - T(2) * sa) * (T(1) - sa);
+  T k2 = sa * (sa - T(1));
+  if (c > T(0)) return q[-sq] + k1 * eRm + k2 * eLm;
+  return q[0] + k1 * eL0 + k2 * eR0;
+}
+
+// Monotone slope of one cell from its neighbours along s.
+template <typename T>
+__device__ __forceinline__ T slope_at(const T* q, int s) {
+  T mono, dqi;
+  slopes(q[-s], q[0], q[s], dqi, mono);
+  return mono;
+}
+
+// 128-byte aligned start of the dynamic shared memory (TMA destinations)
+__device__ __forceinline__ unsigned char* smem_base(unsigned char* raw) {
+  return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
+}
+
+// Region loop: body(x, y) for every point of [x0, x0+W) x [y0, y0+Hh).
+template <int W, int Hh, typename F>
+__device__ __forceinline__ void region(int x0, int y0, F&& body) {
+  for (int idx = threadIdx.x; idx < W * Hh; idx += NT) {
+    const int y = idx / W;
+    const int x = idx - y * W;
+    body(x0 + x, y0 + y);
+  }
+}
+
+// Start of a TMA box whose first wanted column is i0, rounded down to a
+// 16-byte boundary of the tensor row.
+template <typename T>
+__device__ __forceinline__ int tma_x0(int i0) {
+  constexpr int q = tma_q<T>();
+  return ((i0 + H + XOFF) / q) * q - H - XOFF;
+}
+
+// ---------------------------------------------------------------- mass ----
+template <typename T, int TX, int TY, bool CGRID>
+struct MassL {
+  // TMA boxes: dp and pt, and the u, v boxes (D winds on the C grid step,
+  // C winds on the D grid step)
+  static constexpr int WD = tma_width<T>(TX + 6), HD = TY + 6;
+  static constexpr int WU = tma_width<T>(CGRID ? TX + 2 : TX + 1), HU = CGRID ? TY + 7 : TY + 6;
+  static constexpr int WV = tma_width<T>(CGRID ? TX + 7 : TX + 6), HV = CGRID ? TY + 2 : TY + 1;
+  static constexpr uint32_t tx_bytes = (uint32_t)((2 * WD * HD + WU * HU + WV * HV) * sizeof(T));
+  static constexpr size_t boxes = 2 * tma_box_bytes(WD, HD, sizeof(T)) + tma_box_bytes(WU, HU, sizeof(T)) +
+                                  tma_box_bytes(WV, HV, sizeof(T));
+  static constexpr bool NN = !CGRID;
+  static constexpr size_t work =
+      (CGRID ? box_bytes<T>(TX + 1, TY + 6) + box_bytes<T>(TX + 6, TY + 1) : 0) +  // uc, vc (C grid)
+      2 * box_bytes<T>(TX + 6, TY) + 2 * box_bytes<T>(TX, TY + 6) +               // inner sweeps
+      2 * box_bytes<T>(TX + 2, TY + 2) +                                         // Laplacians
+      2 * box_bytes<T>(TX + 4, TY) + 2 * box_bytes<T>(TX, TY + 4) +               // slopes
+      2 * box_bytes<T>(TX + 1, TY) + 2 * box_bytes<T>(TX, TY + 1);                // fluxes
+  static constexpr size_t bytes = boxes + work + 128;
+};
+
+template <typename T, int TX, int TY, bool CGRID>
+__global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMap m_dp,
+                                              const __grid_constant__ CUtensorMap m_pt,
+                                              const __grid_constant__ CUtensorMap m_u,
+                                              const __grid_constant__ CUtensorMap m_v, Geom g, Consts c,
+                                              const double* __restrict__ heat, T* __restrict__ dpo,
+                                              T* __restrict__ pto, int lo, int hi, int* nonfinite, int* timeout) {
+  using Lay = MassL<T, TX, TY, CGRID>;
+  constexpr int V = CGRID ? PPM_UNC : PPM_NN;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ok;
+  unsigned char* p = smem_base(smem);
+  const int k = blockIdx.z;
+  const int ox = lo + blockIdx.x * TX, oy = lo + blockIdx.y * TY;
+  const T dt = T(c.dt), dtdx = T(c.dtdx), dtdy = T(c.dtdy), rA = T(c.rA);
+
+  auto tbox = [&](int i0, int j0, int w, int h) {
+    Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
+    p += tma_box_bytes(w, h, sizeof(T));
+    return s;
+  };
+  Sm<T> sdp = tbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
+  Sm<T> spt = tbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
+  Sm<T> su = CGRID ? tbox(ox - 1, oy - 3, Lay::WU, Lay::HU) : tbox(ox, oy - 3, Lay::WU, Lay::HU);
+  Sm<T> sv = CGRID ? tbox(ox - 3, oy - 1, Lay::WV, Lay::HV) : tbox(ox - 3, oy, Lay::WV, Lay::HV);
+  {
+    const TmaBox boxes[4] = {{&m_dp, sdp.p, sdp.x0, sdp.y0, k},
+                             {&m_pt, spt.p, spt.x0, spt.y0, k},
+                             {&m_u, su.p, su.x0, su.y0, k},
+                             {&m_v, sv.p, sv.x0, sv.y0, k}};
+    if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
+  }
+  // C-grid winds: built from the D-grid winds (C step) or the loaded boxes (D step)
+  Sm<T> suc = su, svc = sv;
+  if (CGRID) {
+    suc = carve<T>(p, ox, oy - 3, TX + 1, TY + 6);
+    svc = carve<T>(p, ox - 3, oy, TX + 6, TY + 1);
+  }
+  Sm<T> tyd = carve<T>(p, ox - 3, oy, TX + 6, TY);
+  Sm<T> typ = carve<T>(p, ox - 3, oy, TX + 6, TY);
+  Sm<T> txd = carve<T>(p, ox, oy - 3, TX, TY + 6);
+  Sm<T> txp = carve<T>(p, ox, oy - 3, TX, TY + 6);
+  Sm<T> lpd = carve<T>(p, ox - 1, oy - 1, TX + 2, TY + 2);
+  Sm<T> lpp = carve<T>(p, ox - 1, oy - 1, TX + 2, TY + 2);
+  Sm<T> mxd = carve<T>(p, ox - 2, oy, TX + 4, TY);
+  Sm<T> mxp = carve<T>(p, ox - 2, oy, TX + 4, TY);
+  Sm<T> myd = carve<T>(p, ox, oy - 2, TX, TY + 4);
+  Sm<T> myp = carve<T>(p, ox, oy - 2, TX, TY + 4);
+  Sm<T> fxd = carve<T>(p, ox, oy, TX + 1, TY);
+  Sm<T> fxp = carve<T>(p, ox, oy, TX + 1, TY);
+  Sm<T> fyd = carve<T>(p, ox, oy, TX, TY + 1);
+  Sm<T> fyp = carve<T>(p, ox, oy, TX, TY + 1);
+
+  if (CGRID) {  // mod_sw_dyn.f90:109-117
+    region<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
+      T ub = T(.5) * (su(x, y) + su(x - 1, y));
+      suc(x, y) = T(.5) * (ub + T(.5) * (su(x, y + 1) + su(x - 1, y + 1)));
+    });
+    region<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
+      T vb = T(.5) * (sv(x, y) + sv(x, y - 1));
+      svc(x, y) = T(.5) * (vb + T(.5) * (sv(x + 1, y) + sv(x + 1, y - 1)));
+    });
+    __syncthreads();
+  }
+  // inner sweeps and Laplacians: mod_sw_dyn.f90:142-155,176-185 (C); 470-482,503-511 (D)
+  region<TX + 6, TY>(ox - 3, oy, [&](int x, int y) {
+    T cy0 = dtdx * svc(x, y), cy1 = dtdx * svc(x, y + 1);
+    T den = T(1) / (T(1) - dtdy * (svc(x, y + 1) - svc(x, y)));
+    T f0 = (cy0 > T(0)) ? sdp(x, y - 1) : sdp(x, y);
+    T f1 = (cy1 > T(0)) ? sdp(x, y) : sdp(x, y + 1);
+    tyd(x, y) = T(.5) * (sdp(x, y) + den * (sdp(x, y) - rA * (f1 - f0)));
+    f0 = (cy0 > T(0)) ? spt(x, y - 1) : spt(x, y);
+    f1 = (cy1 > T(0)) ? spt(x, y) : spt(x, y + 1);
+    typ(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
+  });
+  region<TX, TY + 6>(ox, oy - 3, [&](int x, int y) {
+    T cx0 = dtdx * suc(x, y), cx1 = dtdx * suc(x + 1, y);
+    T den = T(1) / (T(1) - dtdx * (suc(x + 1, y) - suc(x, y)));
+    T f0 = (cx0 > T(0)) ? sdp(x - 1, y) : sdp(x, y);
+    T f1 = (cx1 > T(0)) ? sdp(x, y) : sdp(x + 1, y);
+    txd(x, y) = T(.5) * (sdp(x, y) + den * (sdp(x, y) - rA * (f1 - f0)));
+    f0 = (cx0 > T(0)) ? spt(x - 1, y) : spt(x, y);
+    f1 = (cx1 > T(0)) ? spt(x, y) : spt(x + 1, y);
+    txp(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
+  });
+  {
+    const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
+    region<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
+      lpd(x, y) = T(-2.) * sdp(x, y) * rdxy + (sdp(x + 1, y) + sdp(x - 1, y)) * rdx2 +
+                  (sdp(x, y + 1) + sdp(x, y - 1)) * rdy2;
+      lpp(x, y) = T(-2.) * spt(x, y) * rdxy + (spt(x + 1, y) + spt(x - 1, y)) * rdx2 +
+                  (spt(x, y + 1) + spt(x, y - 1)) * rdy2;
+    });
+  }
+  __syncthreads();
+  // monotone slopes of the outer sweeps (ppm, :870-875)
+  region<TX + 4, TY>(ox - 2, oy, [&](int x, int y) {
+    mxd(x, y) = slope_at(tyd.ptr(x, y), 1);
+    mxp(x, y) = slope_at(typ.ptr(x, y), 1);
+  });
+  region<TX, TY + 4>(ox, oy - 2, [&](int x, int y) {
+    myd(x, y) = slope_at(txd.ptr(x, y), TX);
+    myp(x, y) = slope_at(txp.ptr(x, y), TX);
+  });
+  __syncthreads();
+  // outer sweeps (PPM)
+  region<TX + 1, TY>(ox, oy, [&](int x, int y) {
+    T cx = dtdx * suc(x, y);
+    fxd(x, y) = flux_pre<T, V>(tyd.ptr(x, y), 1, mxd.ptr(x, y), 1, cx) * cx;
+    fxp(x, y) = flux_pre<T, V>(typ.ptr(x, y), 1, mxp.ptr(x, y), 1, cx);
+  });
+  region<TX, TY + 1>(ox, oy, [&](int x, int y) {
+    T cy = dtdx * svc(x, y);
+    fyd(x, y) = flux_pre<T, V>(txd.ptr(x, y), TX, myd.ptr(x, y), TX, cy) * cy;
+    fyp(x, y) = flux_pre<T, V>(txp.ptr(x, y), TX, myp.ptr(x, y), TX, cy);
+  });
+  __syncthreads();
+
+  // updates, mod_sw_dyn.f90:163-172,193-202,230-237,258-267 (C); 490-499,519-528,555-562,582-591 (D)
+  const int xhi = g.nx - 1 + hi, yhi = g.ny - 1 + hi;
+  const T dxv = dtdx * T(c.vdx), dyv = dtdy * T(c.vdy), vdx = T(c.vdx), vdy = T(c.vdy);
+  bool bad = false;
+  region<TX, TY>(ox, oy, [&](int x, int y) {
+    if (x > xhi || y > yhi) return;
+    T d = sdp(x, y);
+    T v = d - (fxd(x + 1, y) - fxd(x, y) + dxv * (lpd(x + 1, y) - T(2.) * lpd(x, y) + lpd(x - 1, y)));
+    v = v - (fyd(x, y + 1) - fyd(x, y) + dyv * (lpd(x, y + 1) - T(2.) * lpd(x, y) + lpd(x, y - 1)));
+    T q = d * spt(x, y) - (fxp(x + 1, y) * fxd(x + 1, y) - fxp(x, y) * fxd(x, y) +
+                           vdx * ((lpp(x + 1, y) - lpp(x, y)) * fxd(x + 1, y) - (lpp(x, y) - lpp(x - 1, y)) * fxd(x, y)));
+    q = q - (fyp(x, y + 1) * fyd(x, y + 1) - fyp(x, y) * fyd(x, y) +
+             vdy * ((lpp(x, y + 1) - lpp(x, y)) * fyd(x, y + 1) - (lpp(x, y) - lpp(x, y - 1)) * fyd(x, y)));
+    if (heat) q = q + dt * d * T(heat[g.at(x, y, k)]);
+    q = q / v;
+    long long o = g.at(x, y, k);
+    dpo[o] = v;
+    pto[o] = q;
+    bool inside = x >= 0 && x < g.nx && y >= 0 && y < g.ny;
+    bad = bad || (inside && !(finite_(v) && finite_(q)));
+  });
+  if (nonfinite) flag_nonfinite(nonfinite, bad);
+}
+
+// ======================================================== C-grid momentum ==
+template <typename T, int TX, int TY>
+struct CMomL {
+  static constexpr int WU = tma_width<T>(TX + 7), HU = TY + 7;   // ud box x in [ox-4, ox+TX+2]
+  static constexpr int WV = tma_width<T>(TX + 7), HV = TY + 7;   // vd box x in [ox-3, ox+TX+3]
+  static constexpr int WL = tma_width<T>(TX + 3), HL = TY + 3;   // layer-nlay ud, vd
+  static constexpr int WP = tma_width<double>(TX + 1), HP = TY + 1;  // pkap, gz at k and k+1
+  static constexpr uint32_t tx_bytes =
+      (uint32_t)((WU * HU + WV * HV + 2 * WL * HL) * sizeof(T) + 4 * WP * HP * sizeof(double));
+  static constexpr size_t boxes = tma_box_bytes(WU, HU, sizeof(T)) + tma_box_bytes(WV, HV, sizeof(T)) +
+                                  2 * tma_box_bytes(WL, HL, sizeof(T)) + 4 * tma_box_bytes(WP, HP, 8);
+  static constexpr size_t work = 2 * box_bytes<T>(TX + 6, TY + 6) + 2 * box_bytes<T>(TX + 1, TY + 1) +
+                                 box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 1, TY + 1) +
+                                 box_bytes<T>(TX, TY + 5) + box_bytes<T>(TX + 5, TY) + box_bytes<T>(TX + 1, TY + 1) +
+                                 box_bytes<T>(TX + 1, TY + 4) + box_bytes<T>(TX + 4, TY + 1) +
+                                 box_bytes<T>(TX, TY + 3) + box_bytes<T>(TX + 3, TY);
+  static constexpr size_t bytes = boxes + work + 128;
+};
+
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorMap m_ud,
+                                               const __grid_constant__ CUtensorMap m_vd,
+                                               const __grid_constant__ CUtensorMap m_udL,
+                                               const __grid_constant__ CUtensorMap m_vdL,
+                                               const __grid_constant__ CUtensorMap m_pk,
+                                               const __grid_constant__ CUtensorMap m_gz, Geom g, Consts c,
+                                               T* __restrict__ uc, T* __restrict__ vc, int* timeout) {
+  using Lay = CMomL<T, TX, TY>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ok;
+  unsigned char* p = smem_base(smem);
+  const int k = blockIdx.z, L = g.L;
+  const int ox = blockIdx.x * TX, oy = blockIdx.y * TY;
+  const T dt = T(c.dt), dtdx = T(c.dtdx), dtdy = T(c.dtdy), rA = T(c.rA);
+  const T rdx = T(c.rdx), rdy = T(c.rdy);
+
+  auto tbox = [&](int i0, int j0, int w, int h) {
+    Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
+    p += tma_box_bytes(w, h, sizeof(T));
+    return s;
+  };
+  auto dbox = [&](int i0, int j0, int w, int h) {
+    Sm<double> s{reinterpret_cast<double*>(p), tma_x0<double>(i0), j0, w};
+    p += tma_box_bytes(w, h, 8);
+    return s;
+  };
+  Sm<T> sud = tbox(ox - 4, oy - 3, Lay::WU, Lay::HU);
+  Sm<T> svd = tbox(ox - 3, oy - 4, Lay::WV, Lay::HV);
+  Sm<T> udL = tbox(ox - 2, oy - 2, Lay::WL, Lay::HL);
+  Sm<T> vdL = tbox(ox - 2, oy - 2, Lay::WL, Lay::HL);
+  Sm<double> pk0 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
+  Sm<double> pk1 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
+  Sm<double> gz0 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
+  Sm<double> gz1 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
+  {
+    const TmaBox boxes[8] = {{&m_ud, sud.p, sud.x0, sud.y0, k},     {&m_vd, svd.p, svd.x0, svd.y0, k},
+                             {&m_udL, udL.p, udL.x0, udL.y0, L - 1}, {&m_vdL, vdL.p, vdL.x0, vdL.y0, L - 1},
+                             {&m_pk, pk0.p, pk0.x0, pk0.y0, k},      {&m_pk, pk1.p, pk1.x0, pk1.y0, k + 1},
+                             {&m_gz, gz0.p, gz0.x0, gz0.y0, k},      {&m_gz, gz1.p, gz1.x0, gz1.y0, k + 1}};
+    if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
+  }
+  Sm<T> uc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
+  Sm<T> vc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
+  Sm<T> uaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
+  Sm<T> vaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
+  Sm<T> vor = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
+  Sm<T> ke = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
+  Sm<T> tU = carve<T>(p, ox, oy - 2, TX, TY + 5);
+  Sm<T> tV = carve<T>(p, ox - 2, oy, TX + 5, TY);
+  Sm<T> lap = carve<T>(p, ox, oy, TX + 1, TY + 1);
+  Sm<T> mvy = carve<T>(p, ox - 1, oy - 2, TX + 1, TY + 4);  // slopes of vc1 along y
+  Sm<T> mux = carve<T>(p, ox - 2, oy - 1, TX + 4, TY + 1);  // slopes of uc1 along x
+  Sm<T> mtU = carve<T>(p, ox, oy - 1, TX, TY + 3);          // slopes of tU along y
+  Sm<T> mtV = carve<T>(p, ox - 1, oy, TX + 3, TY);          // slopes of tV along x
+
+  // C-grid winds of this layer (first-loop values, mod_sw_dyn.f90:110-117)
+  region<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
+    T ub = T(.5) * (sud(x, y) + sud(x - 1, y));
+    uc1(x, y) = T(.5) * (ub + T(.5) * (sud(x, y + 1) + sud(x - 1, y + 1)));
+    T vb = T(.5) * (svd(x, y) + svd(x, y - 1));
+    vc1(x, y) = T(.5) * (vb + T(.5) * (svd(x + 1, y) + svd(x + 1, y - 1)));
+  });
+  // A-grid winds of layer nlay (mod_sw_dyn.f90:110-125 at k = nlay)
+  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
+    T ub = T(.5) * (udL(x, y) + udL(x - 1, y));
+    T ucl = T(.5) * (ub + T(.5) * (udL(x, y + 1) + udL(x - 1, y + 1)));
+    uaL(x, y) = T(.5) * (ucl + T(.25) * (udL(x + 1, y) + udL(x, y) + udL(x + 1, y + 1) + udL(x, y + 1)));
+    T vb = T(.5) * (vdL(x, y) + vdL(x, y - 1));
+    T vcl = T(.5) * (vb + T(.5) * (vdL(x + 1, y) + vdL(x + 1, y - 1)));
+    vaL(x, y) = T(.5) * (vcl + T(.25) * (vdL(x, y + 1) + vdL(x, y) + vdL(x + 1, y + 1) + vdL(x + 1, y)));
+  });
+  __syncthreads();
+
+  const T f = T(c.coriolis);
+  // vorticity (mod_sw_dyn.f90:319-323), slopes of the KE sweeps
+  region<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
+    vor(x, y) = f - (uc1(x, y) - uc1(x, y - 1)) * rdy + (vc1(x, y) - vc1(x - 1, y)) * rdx;
+  });
+  region<TX + 1, TY + 4>(ox - 1, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(vc1.ptr(x, y), TX + 6); });
+  region<TX + 4, TY + 1>(ox - 2, oy - 1, [&](int x, int y) { mux(x, y) = slope_at(uc1.ptr(x, y), 1); });
+  __syncthreads();
+
+  // kinetic energy (:299-317): q(j) = vc(i, j+1), q(i) = uc(i+1, j)
+  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
+    T fy = flux_pre<T, PPM_UNC>(vc1.ptr(x, y + 1), TX + 6, mvy.ptr(x, y + 1), TX + 1, dtdy * vaL(x, y));
+    T kv = vaL(x, y) * fy;
+    T fx = flux_pre<T, PPM_UNC>(uc1.ptr(x + 1, y), 1, mux.ptr(x + 1, y), 1, dtdx * uaL(x, y));
+    ke(x, y) = T(.5) * (kv + uaL(x, y) * fx);
+  });
+  // vorticity advection: inner sweeps and Laplacian (:344-367, 388-397)
+  region<TX, TY + 5>(ox, oy - 2, [&](int x, int y) {
+    T c0 = dtdx * sud(x - 1, y), c1 = dtdx * sud(x, y);
+    T den = T(1) / (T(1) - dtdx * (sud(x, y) - sud(x - 1, y)));
+    T f0 = (c0 > T(0)) ? vor(x - 1, y) : vor(x, y);
+    T f1 = (c1 > T(0)) ? vor(x, y) : vor(x + 1, y);
+    tU(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
+  });
+  region<TX + 5, TY>(ox - 2, oy, [&](int x, int y) {
+    T c0 = dtdx * svd(x, y - 1), c1 = dtdx * svd(x, y);
+    T den = T(1) / (T(1) - dtdy * (svd(x, y) - svd(x, y - 1)));
+    T f0 = (c0 > T(0)) ? vor(x, y - 1) : vor(x, y);
+    T f1 = (c1 > T(0)) ? vor(x, y) : vor(x, y + 1);
+    tV(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
+  });
+  {
+    const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
+    region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
+      lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 +
+                  (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
+    });
+  }
+  __syncthreads();
+  region<TX, TY + 3>(ox, oy - 1, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); });
+  region<TX + 3, TY>(ox - 1, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); });
+  __syncthreads();
+
+  // uc, vc updates (:369-381, 399-411) with the PGF (:325-339)
+  const T vdx = T(c.vdx), vdy = T(c.vdy);
+  region<TX, TY>(ox, oy, [&](int x, int y) {
+    if (x >= g.nx || y >= g.ny) return;
+    double pgx = ((pk0(x, y) - pk1(x - 1, y)) * (gz0(x - 1, y) - gz1(x, y)) +
+                  (pk0(x - 1, y) - pk1(x, y)) * (gz1(x - 1, y) - gz0(x, y))) /
+                 (pk0(x, y) - pk1(x - 1, y) + pk0(x - 1, y) - pk1(x, y));
+    double pgy = ((pk0(x, y) - pk1(x, y - 1)) * (gz0(x, y - 1) - gz1(x, y)) +
+                  (pk0(x, y - 1) - pk1(x, y)) * (gz1(x, y - 1) - gz0(x, y))) /
+                 (pk0(x, y) - pk1(x, y - 1) + pk0(x, y - 1) - pk1(x, y));
+    T fy = flux_pre<T, PPM_UNC>(tU.ptr(x, y + 1), TX, mtU.ptr(x, y + 1), TX, dtdx * svd(x, y));
+    T u = uc1(x, y) + dt * (svd(x, y) * fy + vdy * (lap(x, y + 1) - lap(x, y))) -
+          dtdx * (ke(x, y) - ke(x - 1, y) - T(pgx));
+    T fx = flux_pre<T, PPM_UNC>(tV.ptr(x + 1, y), 1, mtV.ptr(x + 1, y), 1, dtdx * sud(x, y));
+    T v = vc1(x, y) - dt * (sud(x, y) * fx + vdx * (lap(x + 1, y) - lap(x, y))) -
+          dtdy * (ke(x, y) - ke(x, y - 1) - T(pgy));
+    long long o = g.at(x, y, k);
+    uc[o] = u;
+    vc[o] = v;
+  });
+}
+
+// ======================================================== D-grid momentum ==
+template <typename T, int TX, int TY>
+struct DMomL {
+  static constexpr int WU = tma_width<T>(TX + 6), HU = TY + 6;       // ud, vd: [ox-3, ox+TX+2]^2
+  static constexpr int WUL = tma_width<T>(TX + 1), HUL = TY + 5;     // uc layer nlay: x [ox, ox+TX], y [oy-3, oy+TY+1]
+  static constexpr int WVL = tma_width<T>(TX + 5), HVL = TY + 1;     // vc layer nlay: x [ox-3, ox+TX+1], y [oy, oy+TY]
+  static constexpr int WC = tma_width<T>(TX), HC = TY;               // uc, vc of the layer at the outputs
+  static constexpr int WP = tma_width<double>(TX + 1), HP = TY + 1;  // pkapb, gzb
+  static constexpr uint32_t tx_bytes =
+      (uint32_t)((2 * WU * HU + WUL * HUL + WVL * HVL + 2 * WC * HC) * sizeof(T) + 4 * WP * HP * sizeof(double));
+  static constexpr size_t boxes = 2 * tma_box_bytes(WU, HU, sizeof(T)) + tma_box_bytes(WUL, HUL, sizeof(T)) +
+                                  tma_box_bytes(WVL, HVL, sizeof(T)) + 2 * tma_box_bytes(WC, HC, sizeof(T)) +
+                                  4 * tma_box_bytes(WP, HP, 8);
+  static constexpr size_t work =
+      box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 3, TY + 3) +
+      4 * box_bytes<T>(TX + 1, TY + 1) + box_bytes<T>(TX, TY + 5) + box_bytes<T>(TX + 5, TY) +
+      box_bytes<T>(TX + 1, TY + 1);
+  // slopes of the KE sweeps, later of the vorticity-flux sweeps (one buffer)
+  static constexpr size_t slopes_ke = box_bytes<T>(TX + 1, TY + 4) + box_bytes<T>(TX + 4, TY + 1);
+  static constexpr size_t slopes_vf = box_bytes<T>(TX, TY + 3) + box_bytes<T>(TX + 3, TY);
+  static constexpr size_t slopes = slopes_ke > slopes_vf ? slopes_ke : slopes_vf;
+  // edges of the KE sweeps, later of the vorticity-flux sweeps (one buffer)
+  static constexpr size_t edges_ke = 2 * box_bytes<T>(TX + 1, TY + 2) + 2 * box_bytes<T>(TX + 2, TY + 1);
+  static constexpr size_t edges_vf = 2 * box_bytes<T>(TX, TY + 1) + 2 * box_bytes<T>(TX + 1, TY);
+  static constexpr size_t edges = edges_ke > edges_vf ? edges_ke : edges_vf;
+  static constexpr size_t bytes = boxes + work + slopes + edges + 128;
+};
+
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorMap m_ud,
+                                               const __grid_constant__ CUtensorMap m_vd,
+                                               const __grid_constant__ CUtensorMap m_ucL,
+                                               const __grid_constant__ CUtensorMap m_vcL,
+                                               const __grid_constant__ CUtensorMap m_uc,
+                                               const __grid_constant__ CUtensorMap m_vc,
+                                               const __grid_constant__ CUtensorMap m_pkb,
+                                               const __grid_constant__ CUtensorMap m_gzb, Geom g, Consts c,
+                                               T* __restrict__ udo, T* __restrict__ vdo, int* nonfinite,
+                                               int* timeout) {
+  using Lay = DMomL<T, TX, TY>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ok;
+  unsigned char* p = smem_base(smem);
+  const int k = blockIdx.z, L = g.L;
+  const int ox = blockIdx.x * TX, oy = blockIdx.y * TY;
+  const T dt = T(c.dt), dtdx = T(c.dtdx), dtdy = T(c.dtdy), rA = T(c.rA);
+  const T rdx = T(c.rdx), rdy = T(c.rdy);
+
+  auto tbox = [&](int i0, int j0, int w, int h) {
+    Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
+    p += tma_box_bytes(w, h, sizeof(T));
+    return s;
+  };
+  auto dbox = [&](int i0, int j0, int w, int h) {
+    Sm<double> s{reinterpret_cast<double*>(p), tma_x0<double>(i0), j0, w};
+    p += tma_box_bytes(w, h, 8);
+    return s;
+  };
+  Sm<T> sud = tbox(ox - 3, oy - 3, Lay::WU, Lay::HU);
+  Sm<T> svd = tbox(ox - 3, oy - 3, Lay::WU, Lay::HU);
+  Sm<T> ucL = tbox(ox, oy - 3, Lay::WUL, Lay::HUL);
+  Sm<T> vcL = tbox(ox - 3, oy, Lay::WVL, Lay::HVL);
+  Sm<T> suc = tbox(ox, oy, Lay::WC, Lay::HC);
+  Sm<T> svc = tbox(ox, oy, Lay::WC, Lay::HC);
+  Sm<double> pb0 = dbox(ox, oy, Lay::WP, Lay::HP);
+  Sm<double> pb1 = dbox(ox, oy, Lay::WP, Lay::HP);
+  Sm<double> gb0 = dbox(ox, oy, Lay::WP, Lay::HP);
+  Sm<double> gb1 = dbox(ox, oy, Lay::WP, Lay::HP);
+  {
+    const TmaBox boxes[10] = {
+        {&m_ud, sud.p, sud.x0, sud.y0, k},       {&m_vd, svd.p, svd.x0, svd.y0, k},
+        {&m_ucL, ucL.p, ucL.x0, ucL.y0, L - 1},  {&m_vcL, vcL.p, vcL.x0, vcL.y0, L - 1},
+        {&m_uc, suc.p, suc.x0, suc.y0, k},       {&m_vc, svc.p, svc.x0, svc.y0, k},
+        {&m_pkb, pb0.p, pb0.x0, pb0.y0, k},      {&m_pkb, pb1.p, pb1.x0, pb1.y0, k + 1},
+        {&m_gzb, gb0.p, gb0.x0, gb0.y0, k},      {&m_gzb, gb1.p, gb1.x0, gb1.y0, k + 1}};
+    if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
+  }
+  Sm<T> vor = carve<T>(p, ox - 3, oy - 3, TX + 5, TY + 5);
+  Sm<T> dv0 = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
+  Sm<T> dv2 = carve<T>(p, ox - 1, oy - 1, TX + 3, TY + 3);
+  Sm<T> dv4 = carve<T>(p, ox, oy, TX + 1, TY + 1);
+  Sm<T> ubL = carve<T>(p, ox, oy, TX + 1, TY + 1);
+  Sm<T> vbL = carve<T>(p, ox, oy, TX + 1, TY + 1);
+  Sm<T> ke = carve<T>(p, ox, oy, TX + 1, TY + 1);
+  Sm<T> tU = carve<T>(p, ox, oy - 3, TX, TY + 5);
+  Sm<T> tV = carve<T>(p, ox - 3, oy, TX + 5, TY);
+  Sm<T> lap = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
+  // the KE sweeps' slopes and edges are dead before the vorticity-flux
+  // sweeps' ones are written (two __syncthreads apart): they share memory
+  unsigned char* ps = p;
+  Sm<T> mvy = carve<T>(ps, ox, oy - 2, TX + 1, TY + 4);
+  Sm<T> mux = carve<T>(ps, ox - 2, oy, TX + 4, TY + 1);
+  ps = p;
+  Sm<T> mtU = carve<T>(ps, ox, oy - 2, TX, TY + 3);
+  Sm<T> mtV = carve<T>(ps, ox - 2, oy, TX + 3, TY);
+  p += Lay::slopes;
+  unsigned char* pe = p;
+  Sm<T> lvy = carve<T>(pe, ox, oy - 1, TX + 1, TY + 2), rvy = carve<T>(pe, ox, oy - 1, TX + 1, TY + 2);
+  Sm<T> lux = carve<T>(pe, ox - 1, oy, TX + 2, TY + 1), rux = carve<T>(pe, ox - 1, oy, TX + 2, TY + 1);
+  pe = p;
+  Sm<T> ltU = carve<T>(pe, ox, oy - 1, TX, TY + 1), rtU = carve<T>(pe, ox, oy - 1, TX, TY + 1);
+  Sm<T> ltV = carve<T>(pe, ox - 1, oy, TX + 1, TY), rtV = carve<T>(pe, ox - 1, oy, TX + 1, TY);
+  p += Lay::edges;
+
+  const T f = T(c.coriolis);
+  // vorticity (:659-663), divergence (:682-685), layer-nlay B-grid winds (:441-444),
+  // slopes of the KE sweeps
+  region<TX + 5, TY + 5>(ox - 3, oy - 3, [&](int x, int y) {
+    vor(x, y) = f - (sud(x, y + 1) - sud(x, y)) * rdy + (svd(x + 1, y) - svd(x, y)) * rdx;
+    int xd = x + 1, yd = y + 1;
+    dv0(xd, yd) = rdx * (sud(xd, yd) - sud(xd - 1, yd)) + rdy * (svd(xd, yd) - svd(xd, yd - 1));
+  });
+  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
+    ubL(x, y) = T(.5) * (ucL(x, y) + ucL(x, y - 1));
+    vbL(x, y) = T(.5) * (vcL(x, y) + vcL(x - 1, y));
+  });
+  region<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(svd.ptr(x, y), Lay::WU); });
+  region<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { mux(x, y) = slope_at(sud.ptr(x, y), 1); });
+  __syncthreads();
+
+  const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
+  // edges of the KE sweeps; del^2 of the divergence (:688-692); inner
+  // sweeps of the vorticity with the layer-nlay Courant numbers (:708-722, 744-753)
+  region<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
+    T eL, eR;
+    edges_pre<T, PPM_CON>(svd.ptr(x, y), Lay::WU, mvy.ptr(x, y), TX + 1, eL, eR);
+    lvy(x, y) = eL;
+    rvy(x, y) = eR;
+  });
+  region<TX + 2, TY + 1>(ox - 1, oy, [&](int x, int y) {
+    T eL, eR;
+    edges_pre<T, PPM_CON>(sud.ptr(x, y), 1, mux.ptr(x, y), 1, eL, eR);
+    lux(x, y) = eL;
+    rux(x, y) = eR;
+  });
+  region<TX + 3, TY + 3>(ox - 1, oy - 1, [&](int x, int y) {
+    dv2(x, y) = T(-2.) * dv0(x, y) * rdxy + (dv0(x + 1, y) + dv0(x - 1, y)) * rdx2 + (dv0(x, y + 1) + dv0(x, y - 1)) * rdy2;
+  });
+  region<TX, TY + 5>(ox, oy - 3, [&](int x, int y) {
+    T c0 = dtdx * ucL(x, y), c1 = dtdx * ucL(x + 1, y);
+    T den = T(1) / (T(1) - dtdx * (ucL(x + 1, y) - ucL(x, y)));
+    T f0 = (c0 > T(0)) ? vor(x - 1, y) : vor(x, y);
+    T f1 = (c1 > T(0)) ? vor(x, y) : vor(x + 1, y);
+    tU(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
+  });
+  region<TX + 5, TY>(ox - 3, oy, [&](int x, int y) {
+    T c0 = dtdx * vcL(x, y), c1 = dtdx * vcL(x, y + 1);
+    T den = T(1) / (T(1) - dtdy * (vcL(x, y + 1) - vcL(x, y)));
+    T f0 = (c0 > T(0)) ? vor(x, y - 1) : vor(x, y);
+    T f1 = (c1 > T(0)) ? vor(x, y) : vor(x, y + 1);
+    tV(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
+  });
+  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
+    lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 + (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
+  });
+  __syncthreads();
+  // kinetic energy with PPM_CONSTRAINED (:639-657), del^4 (:695-702),
+  // slopes of the vorticity-flux sweeps
+  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
+    T fy = flux_con_pre<T>(svd.ptr(x, y), Lay::WU, lvy.ptr(x, y), rvy.ptr(x, y), TX + 1, dtdy * vbL(x, y));
+    T kv = vbL(x, y) * fy;
+    T fx = flux_con_pre<T>(sud.ptr(x, y), 1, lux.ptr(x, y), rux.ptr(x, y), 1, dtdx * ubL(x, y));
+    ke(x, y) = T(.5) * (kv + ubL(x, y) * fx);
+  });
+  const T divdamp = T(c.divdamp);
+  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
+    T d4 = T(-2.) * dv2(x, y) * rdxy + (dv2(x + 1, y) + dv2(x - 1, y)) * rdx2 + (dv2(x, y + 1) + dv2(x, y - 1)) * rdy2;
+    dv4(x, y) = divdamp * d4;
+  });
+  region<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); });
+  region<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); });
+  __syncthreads();
+  region<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
+    T eL, eR;
+    edges_pre<T, PPM_CON>(tU.ptr(x, y), TX, mtU.ptr(x, y), TX, eL, eR);
+    ltU(x, y) = eL;
+    rtU(x, y) = eR;
+  });
+  region<TX + 1, TY>(ox - 1, oy, [&](int x, int y) {
+    T eL, eR;
+    edges_pre<T, PPM_CON>(tV.ptr(x, y), 1, mtV.ptr(x, y), 1, eL, eR);
+    ltV(x, y) = eL;
+    rtV(x, y) = eR;
+  });
+  __syncthreads();
+
+  // ud, vd updates (:724-738, 755-769) with the B-grid PGF (:665-679)
+  const T vdx = T(c.vdx), vdy = T(c.vdy);
+  bool bad = false;
+  region<TX, TY>(ox, oy, [&](int x, int y) {
+    if (x >= g.nx || y >= g.ny) return;
+    double pgx = ((pb0(x + 1, y) - pb1(x, y)) * (gb0(x, y) - gb1(x + 1, y)) +
+                  (pb0(x, y) - pb1(x + 1, y)) * (gb1(x, y) - gb0(x + 1, y))) /
+                 (pb0(x + 1, y) - pb1(x, y) + pb0(x, y) - pb1(x + 1, y));
+    double pgy = ((pb0(x, y + 1) - pb1(x, y)) * (gb0(x, y) - gb1(x, y + 1)) +
+                  (pb0(x, y) - pb1(x, y + 1)) * (gb1(x, y) - gb0(x, y + 1))) /
+                 (pb0(x, y + 1) - pb1(x, y) + pb0(x, y) - pb1(x, y + 1));
+    T fy = flux_con_pre<T>(tU.ptr(x, y), TX, ltU.ptr(x, y), rtU.ptr(x, y), TX, dtdx * vcL(x, y));
+    T u = sud(x, y) + dt * (svc(x, y) * fy + vdy * (lap(x, y) - lap(x, y - 1))) -
+          dtdx * (ke(x + 1, y) - ke(x, y) - dv4(x + 1, y) + dv4(x, y) - T(pgx));
+    T fx = flux_con_pre<T>(tV.ptr(x, y), 1, ltV.ptr(x, y), rtV.ptr(x, y), 1, dtdx * ucL(x, y));
+    T v = svd(x, y) - dt * (suc(x, y) * fx + vdx * (lap(x, y) - lap(x - 1, y))) -
+          dtdy * (ke(x, y + 1) - ke(x, y) - dv4(x, y + 1) + dv4(x, y) - T(pgy));
+    long long o = g.at(x, y, k);
+    udo[o] = u;
+    vdo[o] = v;
+    bad = bad || !(finite_(u) && finite_(v));
+  });
+  flag_nonfinite(nonfinite, bad);
+}
+
+}  // namespace atm

@@ -105,3 +105,12 @@ def test_bubble_100_steps_bit_exact_and_mass():
     for name, f in (('dp', pyoracle.DP), ('pt', pyoracle.PT), ('ud', pyoracle.UD), ('vd', pyoracle.VD)):
         _assert_same(g.get(name, halo=True), o.get(f, halo=True), name)
     assert abs(g.mass() - m0) / m0 <= 1e-13
+
+
+def test_division_by_constants_is_ieee_division():
+    import ctypes
+    from atmdyn import load
+    lib = load()
+    bad = ctypes.c_longlong(-1)
+    assert lib.atm_device_div_check(400_000_000, 12345, ctypes.byref(bad)) == 0
+    assert bad.value == 0
