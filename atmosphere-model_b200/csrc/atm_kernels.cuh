@@ -53,35 +53,42 @@ __device__ __forceinline__ bool finite_(float v) { return isfinite(v); }
 // ====================================================== column pressure ====
 // plev = ptop + suffix sum of dp from the model top, pkap = plev**kappa,
 // hydrostatic gz from the bottom (src/mod_sw_dyn.f90:276-292 and 606-626).
-// One thread per column over [lo, n-1+hi]^2; pkap of the column is kept in
-// shared memory between the downward and the upward pass.
+// One thread per column over [lo, n-1+hi]^2.  The downward pass writes
+// pkap; the upward pass reads it back (from L2: a block's columns were just
+// written), so no shared memory limits the occupancy.  The next layer's dp
+// is loaded one iteration ahead so that its latency overlaps atm_pow.
 template <typename T>
-__global__ void __launch_bounds__(64) k_column(Geom g, Consts c, const T* __restrict__ dpl, const T* __restrict__ ptl,
-                                               double* __restrict__ pkap, double* __restrict__ gz, int lo, int hi,
-                                               double* __restrict__ plev_out) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  double* spk = reinterpret_cast<double*>(smem);  // [L+1][64]
+__global__ void __launch_bounds__(128) k_column(Geom g, Consts c, const T* __restrict__ dpl, const T* __restrict__ ptl,
+                                                double* __restrict__ pkap, double* __restrict__ gz, int lo, int hi,
+                                                double* __restrict__ plev_out) {
   const int w = g.nx - lo + hi;
   const int hgt = g.ny - lo + hi;
-  const int col = blockIdx.x * 64 + threadIdx.x;
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= w * hgt) return;
   const int x = lo + col % w, y = lo + col / w;
   const long long o = g.at(x, y);
+  const long long S = g.S;
   const int L = g.L;
   double plev = c.ptop;
-  spk[L * 64 + threadIdx.x] = c.pk_top;
-  if (plev_out) plev_out[o + (long long)L * g.S] = plev;
+  if (plev_out) plev_out[o + (long long)L * S] = plev;
+  double dnext = (double)dpl[o + (long long)(L - 1) * S];
   for (int k = L - 1; k >= 0; --k) {
-    plev = plev + (double)dpl[o + (long long)k * g.S];
-    if (plev_out) plev_out[o + (long long)k * g.S] = plev;
-    double pk = atm_pow(plev, KAPPA);
-    spk[k * 64 + threadIdx.x] = pk;
-    pkap[o + (long long)k * g.S] = pk;
+    const double d = dnext;
+    if (k > 0) dnext = (double)dpl[o + (long long)(k - 1) * S];
+    plev = plev + d;
+    if (plev_out) plev_out[o + (long long)k * S] = plev;
+    pkap[o + (long long)k * S] = atm_pow(plev, KAPPA);
   }
   double z = gz[o];
+  double pk0 = pkap[o];
+  double ptn = (double)ptl[o];
   for (int k = 0; k < L; ++k) {
-    z = z + CP_DRY * (double)ptl[o + (long long)k * g.S] * (spk[k * 64 + threadIdx.x] - spk[(k + 1) * 64 + threadIdx.x]);
-    gz[o + (long long)(k + 1) * g.S] = z;
+    const double pk1 = k + 1 < L ? pkap[o + (long long)(k + 1) * S] : c.pk_top;
+    const double pt = ptn;
+    if (k + 1 < L) ptn = (double)ptl[o + (long long)(k + 1) * S];
+    z = z + CP_DRY * pt * (pk0 - pk1);
+    gz[o + (long long)(k + 1) * S] = z;
+    pk0 = pk1;
   }
 }
 

@@ -79,7 +79,7 @@ cudaError_t setup() {
   if ((e = smem_attr(k_mass2<T, TX, TY, false>, MassL<T, TX, TY, false>::bytes)) != cudaSuccess) return e;
   if ((e = smem_attr(k_c_mom2<T, TX, TY>, CMomL<T, TX, TY>::bytes)) != cudaSuccess) return e;
   if ((e = smem_attr(k_d_mom2<T, TX, TY>, DMomL<T, TX, TY>::bytes)) != cudaSuccess) return e;
-  return smem_attr(k_column<T>, (MAX_LAYERS + 1) * 64 * 8);
+  return cudaSuccess;
 }
 
 cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt, const void* u, const void* v,
@@ -110,8 +110,7 @@ cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt,
 cudaError_t column(const Geom& g, const Consts& c, const void* dpl, const void* ptl, double* pkap, double* gz, int lo,
                    int hi, double* plev, cudaStream_t s) {
   int n = (g.nx - lo + hi) * (g.ny - lo + hi);
-  k_column<T><<<(n + 63) / 64, 64, (size_t)(g.L + 1) * 64 * 8, s>>>(g, c, (const T*)dpl, (const T*)ptl, pkap, gz, lo, hi,
-                                                                     plev);
+  k_column<T><<<(n + 127) / 128, 128, 0, s>>>(g, c, (const T*)dpl, (const T*)ptl, pkap, gz, lo, hi, plev);
   return cudaGetLastError();
 }
 
