@@ -13,6 +13,7 @@
 // precision literals (7./12., 1./12., 2./3., R_dry) follow the Fortran.
 // Build with -ffp-contract=off so that no multiply-add is fused.
 #include "atm_oracle.h"
+#include "dual.h"
 
 #include <cmath>
 #include <cstdio>
@@ -35,6 +36,12 @@ static inline double orc_log_impl(double x) { return std::log(x); }
 static inline double orc_pow_impl(double x, double y) { return atm_pow(x, y); }
 static inline double orc_log_impl(double x) { return atm_log(x); }
 #endif
+// x**y and log(x) of a dual number: d(x**y) = y x**y / x dx, d log x = dx / x
+static inline Dual orc_pow_impl(const Dual& x, double y) {
+  double p = orc_pow_impl(x.v, y);
+  return Dual(p, y * p / x.v * x.d);
+}
+static inline Dual orc_log_impl(const Dual& x) { return Dual(orc_log_impl(x.v), x.d / x.v); }
 
 namespace {
 
@@ -66,39 +73,42 @@ enum { PIECEWISE_CONSTANT = 0, PPM_UNCONSTRAINED = 1, PPM_CONSTRAINED = 2,
 #define CHK(cond, what, a, b, c) do { } while (0)
 #endif
 
+template <class R>
 struct A1 {
-  std::vector<double> v;
+  std::vector<R> v;
   int lb = 0, ub = -1;
-  void alloc(int l, int u) { lb = l; ub = u; v.assign((size_t)(u - l + 1), NAN); }
-  double& operator()(int i) {
+  void alloc(int l, int u) { lb = l; ub = u; v.assign((size_t)(u - l + 1), R(NAN)); }
+  R& operator()(int i) {
     CHK(i >= lb && i <= ub, "A1", i, lb, ub);
     return v[(size_t)(i - lb)];
   }
 };
 
+template <class R>
 struct A2 {
-  std::vector<double> v;
+  std::vector<R> v;
   int i0 = 0, i1 = -1, j0 = 0, j1 = -1, ni = 0;
   void alloc(int a, int b, int c, int d) {
     i0 = a; i1 = b; j0 = c; j1 = d; ni = b - a + 1;
-    v.assign((size_t)ni * (size_t)(d - c + 1), NAN);
+    v.assign((size_t)ni * (size_t)(d - c + 1), R(NAN));
   }
-  void poison() { std::fill(v.begin(), v.end(), NAN); }
-  double& operator()(int i, int j) {
+  void poison() { std::fill(v.begin(), v.end(), R(NAN)); }
+  R& operator()(int i, int j) {
     CHK(i >= i0 && i <= i1 && j >= j0 && j <= j1, "A2", i, j, 0);
     return v[(size_t)(i - i0) + (size_t)(j - j0) * (size_t)ni];
   }
 };
 
+template <class R>
 struct A3 {
-  std::vector<double> v;
+  std::vector<R> v;
   int i0 = 0, i1 = -1, j0 = 0, j1 = -1, k0 = 1, k1 = 0, ni = 0, nj = 0;
-  void alloc(int a, int b, int c, int d, int e, int f, double init = NAN) {
+  void alloc(int a, int b, int c, int d, int e, int f, R init = R(NAN)) {
     i0 = a; i1 = b; j0 = c; j1 = d; k0 = e; k1 = f;
     ni = b - a + 1; nj = d - c + 1;
     v.assign((size_t)ni * nj * (size_t)(f - e + 1), init);
   }
-  double& operator()(int i, int j, int k) {
+  R& operator()(int i, int j, int k) {
     CHK(i >= i0 && i <= i1 && j >= j0 && j <= j1 && k >= k0 && k <= k1, "A3", i, j, k);
     return v[(size_t)(i - i0) + (size_t)ni * ((size_t)(j - j0) + (size_t)nj * (size_t)(k - k0))];
   }
@@ -107,83 +117,86 @@ struct A3 {
 
 // A 1-D window onto an array section, indexed with the callee's bounds
 // (Fortran passes e.g. vc(i, js+3:je-1, k) to a dummy q(js+2:je-2)).
+template <class R>
 struct V {
-  double* p;
+  R* p;
   ptrdiff_t s;
   int lb;
-  double& operator()(int i) const { return p[(ptrdiff_t)(i - lb) * s]; }
+  R& operator()(int i) const { return p[(ptrdiff_t)(i - lb) * s]; }
 };
 
-inline V row(A2& a, int ifirst, int j, int lb) { return V{&a(ifirst, j), 1, lb}; }
-inline V col(A2& a, int i, int jfirst, int lb) { return V{&a(i, jfirst), (ptrdiff_t)a.ni, lb}; }
-inline V row3(A3& a, int ifirst, int j, int k, int lb) { return V{&a(ifirst, j, k), 1, lb}; }
-inline V col3(A3& a, int i, int jfirst, int k, int lb) { return V{&a(i, jfirst, k), a.sj(), lb}; }
+template <class R> inline V<R> row(A2<R>& a, int ifirst, int j, int lb) { return V<R>{&a(ifirst, j), 1, lb}; }
+template <class R> inline V<R> col(A2<R>& a, int i, int jfirst, int lb) { return V<R>{&a(i, jfirst), (ptrdiff_t)a.ni, lb}; }
+template <class R> inline V<R> row3(A3<R>& a, int ifirst, int j, int k, int lb) { return V<R>{&a(ifirst, j, k), 1, lb}; }
+template <class R> inline V<R> col3(A3<R>& a, int i, int jfirst, int k, int lb) { return V<R>{&a(i, jfirst, k), a.sj(), lb}; }
 
-inline double fmax3(double a, double b, double c) { return std::max(std::max(a, b), c); }
-inline double fmin3(double a, double b, double c) { return std::min(std::min(a, b), c); }
+template <class R> inline R fmax3(const R& a, const R& b, const R& c) { return std::max(std::max(a, b), c); }
+template <class R> inline R fmin3(const R& a, const R& b, const R& c) { return std::min(std::min(a, b), c); }
 
 // The module-level scratch of mod_sw_dyn (mod_sw_dyn.f90:29-71).  In the
 // serial mode there is one instance shared by every layer, exactly like the
 // Fortran module variables; the layer-parallel mode gives each thread one.
+template <class R>
 struct Scratch {
-  A2 vorticity, kinetic_energy, divergence, laplacian, pgfx, pgfy;
-  A2 ua, va, ub, vb, tmp, cx, cy, dpfx, dpfy, denom_x, denom_y;
-  A1 fx, fy, edge_L, edge_R, dqi, dqi_mono, ctmp;
+  A2<R> vorticity, kinetic_energy, divergence, laplacian, pgfx, pgfy;
+  A2<R> ua, va, ub, vb, tmp, cx, cy, dpfx, dpfy, denom_x, denom_y;
+  A1<R> fx, fy, edge_L, edge_R, dqi, dqi_mono, ctmp;
   void alloc(int is, int ie, int js, int je) {
-    A2* a2[] = {&vorticity, &kinetic_energy, &divergence, &laplacian, &pgfx, &pgfy,
+    A2<R>* a2[] = {&vorticity, &kinetic_energy, &divergence, &laplacian, &pgfx, &pgfy,
                 &ua, &va, &ub, &vb, &tmp, &cx, &cy, &dpfx, &dpfy, &denom_x, &denom_y};
-    for (A2* a : a2) a->alloc(is, ie, js, je);
+    for (A2<R>* a : a2) a->alloc(is, ie, js, je);
     int lo = std::min(is, js), hi = std::max(ie, je);
-    A1* a1[] = {&fx, &fy, &edge_L, &edge_R, &dqi, &dqi_mono, &ctmp};
-    for (A1* a : a1) a->alloc(lo, hi);
+    A1<R>* a1[] = {&fx, &fy, &edge_L, &edge_R, &dqi, &dqi_mono, &ctmp};
+    for (A1<R>* a : a1) a->alloc(lo, hi);
   }
   void poison() {
-    A2* a2[] = {&vorticity, &kinetic_energy, &divergence, &laplacian, &pgfx, &pgfy,
+    A2<R>* a2[] = {&vorticity, &kinetic_energy, &divergence, &laplacian, &pgfx, &pgfy,
                 &tmp, &dpfx, &dpfy};
-    for (A2* a : a2) a->poison();
+    for (A2<R>* a : a2) a->poison();
   }
   void poison_courant() {
-    A2* a2[] = {&cx, &cy, &denom_x, &denom_y};
-    for (A2* a : a2) a->poison();
+    A2<R>* a2[] = {&cx, &cy, &denom_x, &denom_y};
+    for (A2<R>* a : a2) a->poison();
   }
   void poison_winds() {
-    A2* a2[] = {&ua, &va, &ub, &vb};
-    for (A2* a : a2) a->poison();
+    A2<R>* a2[] = {&ua, &va, &ub, &vb};
+    for (A2<R>* a : a2) a->poison();
     poison_courant();
   }
 };
 
 // mod_sw_dyn.f90:848-919
-void ppm(Scratch& sc, const V& q, int isl, int iel, int variant) {
-  A1& dqi = sc.dqi;
-  A1& dqi_mono = sc.dqi_mono;
-  A1& edge_L = sc.edge_L;
-  A1& edge_R = sc.edge_R;
+template <class R>
+void ppm(Scratch<R>& sc, const V<R>& q, int isl, int iel, int variant) {
+  A1<R>& dqi = sc.dqi;
+  A1<R>& dqi_mono = sc.dqi_mono;
+  A1<R>& edge_L = sc.edge_L;
+  A1<R>& edge_R = sc.edge_R;
   for (int i = isl + 1; i <= iel - 1; ++i) {
     dqi(i) = (q(i + 1) - q(i - 1)) / 4.;
-    double dqi_max = fmax3(q(i + 1), q(i), q(i - 1)) - q(i);
-    double dqi_min = q(i) - fmin3(q(i + 1), q(i), q(i - 1));
-    dqi_mono(i) = std::copysign(fmin3(std::fabs(dqi(i)), dqi_min, dqi_max), dqi(i));
+    R dqi_max = fmax3(q(i + 1), q(i), q(i - 1)) - q(i);
+    R dqi_min = q(i) - fmin3(q(i + 1), q(i), q(i - 1));
+    dqi_mono(i) = copysign_(fmin3(fabs_(dqi(i)), dqi_min, dqi_max), dqi(i));
   }
   for (int i = isl + 2; i <= iel - 2; ++i) {
     edge_L(i) = (q(i - 1) - q(i)) / 2. + (dqi_mono(i - 1) - dqi_mono(i)) / 3.;
     edge_R(i) = (q(i + 1) - q(i)) / 2. + (dqi_mono(i) - dqi_mono(i + 1)) / 3.;
     if (variant == PPM_CONSTRAINED || variant == PPM_NONNEGATIVE) {
-      edge_L(i) = -std::copysign(std::min(2. * std::fabs(dqi(i)), std::fabs(edge_L(i))), dqi(i));
-      edge_R(i) = +std::copysign(std::min(2. * std::fabs(dqi(i)), std::fabs(edge_R(i))), dqi(i));
+      edge_L(i) = -copysign_(std::min(R(2. * fabs_(dqi(i))), fabs_(edge_L(i))), dqi(i));
+      edge_R(i) = +copysign_(std::min(R(2. * fabs_(dqi(i))), fabs_(edge_R(i))), dqi(i));
       if (variant == PPM_NONNEGATIVE) {
-        edge_L(i) = std::max(edge_L(i), -q(i));
-        edge_R(i) = std::max(edge_R(i), -q(i));
-        double a = edge_R(i) - edge_L(i);
-        double b = -3. * (edge_R(i) + edge_L(i));
-        if ((std::fabs(a) < -b) && (q(i) + a * a / (4. * b) + b / 12. < 0.)) {
+        edge_L(i) = std::max(edge_L(i), R(-q(i)));
+        edge_R(i) = std::max(edge_R(i), R(-q(i)));
+        R a = edge_R(i) - edge_L(i);
+        R b = -3. * (edge_R(i) + edge_L(i));
+        if ((fabs_(a) < -b) && (q(i) + a * a / (4. * b) + b / 12. < 0.)) {
           if (edge_L(i) * edge_R(i) > 0.) {
             edge_L(i) = 0.;
             edge_R(i) = 0.;
           } else if (edge_L(i) > edge_R(i)) {
-            edge_L(i) = 2. * std::fabs(edge_R(i));
+            edge_L(i) = 2. * fabs_(edge_R(i));
           } else {
-            edge_R(i) = 2. * std::fabs(edge_L(i));
+            edge_R(i) = 2. * fabs_(edge_L(i));
           }
         }
       }
@@ -192,18 +205,19 @@ void ppm(Scratch& sc, const V& q, int isl, int iel, int variant) {
 }
 
 // mod_sw_dyn.f90:781-846
-void flux(Scratch& sc, const V& f, const V& q, const V& c, int isl, int iel, int variant) {
+template <class R>
+void flux(Scratch<R>& sc, const V<R>& f, const V<R>& q, const V<R>& c, int isl, int iel, int variant) {
   if (variant == PPM_UNCONSTRAINED || variant == PPM_CONSTRAINED || variant == PPM_NONNEGATIVE) {
     ppm(sc, q, isl, iel, variant);
-    A1& edge_L = sc.edge_L;
-    A1& edge_R = sc.edge_R;
+    A1<R>& edge_L = sc.edge_L;
+    A1<R>& edge_R = sc.edge_R;
     for (int i = isl + 3; i <= iel - 2; ++i) {
-      double s = std::fabs(c(i));
-      double k1 = (1. - 2. * s) * (1. - s);
-      double k2 = s * (s - 1.);
+      R s = fabs_(c(i));
+      R k1 = (1. - 2. * s) * (1. - s);
+      R k2 = s * (s - 1.);
       if (variant == PPM_CONSTRAINED &&
-          (3. * std::fabs(edge_L(i) + edge_R(i)) > std::fabs(edge_L(i) - edge_R(i))) &&
-          (3. * std::fabs(edge_L(i - 1) + edge_R(i - 1)) > std::fabs(edge_L(i - 1) - edge_R(i - 1)))) {
+          (3. * fabs_(edge_L(i) + edge_R(i)) > fabs_(edge_L(i) - edge_R(i))) &&
+          (3. * fabs_(edge_L(i - 1) + edge_R(i - 1)) > fabs_(edge_L(i - 1) - edge_R(i - 1)))) {
         if (c(i) > 0.) f(i) = q(i - 1);
         else f(i) = q(i);
       } else {
@@ -220,22 +234,25 @@ void flux(Scratch& sc, const V& f, const V& q, const V& c, int isl, int iel, int
 }
 
 // Fortran passes the expression dtdy*va(i, js+2:je-2) as a temporary array.
-V scaled_temp(Scratch& sc, double a, const V& src, int lo, int hi) {
+template <class R>
+V<R> scaled_temp(Scratch<R>& sc, double a, const V<R>& src, int lo, int hi) {
   for (int i = lo; i <= hi; ++i) sc.ctmp(i) = a * src(i);
-  return V{&sc.ctmp(lo), 1, lo};
+  return V<R>{&sc.ctmp(lo), 1, lo};
 }
 
 // mod_sw_dyn.f90:921-956; out/q are windows with bounds (isl:iel, jsl:jel)
+template <class R>
 struct W2 {
-  double* p;
+  R* p;
   ptrdiff_t sj;
   int i0, j0;
-  double& operator()(int i, int j) const { return p[(ptrdiff_t)(i - i0) + (ptrdiff_t)(j - j0) * sj]; }
+  R& operator()(int i, int j) const { return p[(ptrdiff_t)(i - i0) + (ptrdiff_t)(j - j0) * sj]; }
 };
-void interpolate_to_corners(const W2& out, const W2& q, int isl, int iel, int jsl, int jel) {
+template <class R>
+void interpolate_to_corners(const W2<R>& out, const W2<R>& q, int isl, int iel, int jsl, int jel) {
   int ni = iel - isl + 1;
-  std::vector<double> t((size_t)ni * (size_t)(jel - jsl + 1), NAN);
-  W2 tmpl{t.data(), ni, isl, jsl};
+  std::vector<R> t((size_t)ni * (size_t)(jel - jsl + 1), R(NAN));
+  W2<R> tmpl{t.data(), ni, isl, jsl};
   for (int j = jsl; j <= jel; ++j)
     for (int i = isl + 2; i <= iel - 1; ++i)
       tmpl(i, j) = C7_12 * (q(i, j) + q(i - 1, j)) - C1_12 * (q(i + 1, j) + q(i - 2, j));
@@ -250,49 +267,55 @@ void interpolate_to_corners(const W2& out, const W2& q, int isl, int iel, int js
       out(i, j) = out(i, j) + C9_32 * (tmpl(i, j) + tmpl(i - 1, j)) - C1_32 * (tmpl(i + 1, j) + tmpl(i - 2, j));
 }
 
-W2 w3(A3& a, int i0, int j0, int k) { return W2{&a(i0, j0, k), a.sj(), i0, j0}; }
+template <class R>
+W2<R> w3(A3<R>& a, int i0, int j0, int k) { return W2<R>{&a(i0, j0, k), a.sj(), i0, j0}; }
 
 }  // namespace
 
-struct orc_state {
+template <class R>
+struct StateT {
   int nx, ny, nlay;
   double dx, dy;
   int is, ie, js, je, isd, ied, jsd, jed;
   double gravity, coriolis, divergence_damping, vorticity_damping;
   double rdx, rdx2, rdy, rdy2, rdx2rdy2, rA;
   double divdamp_coeff, vortdamp_xcoeff, vortdamp_ycoeff;
-  A1 coord_Ak, coord_Bk;
+  A1<double> coord_Ak, coord_Bk;
   // mod_fields
-  A3 dp, pt, ud, vd, plev, pkap, playkap, gz, net_flux;
+  A3<R> dp, pt, ud, vd, plev, pkap, playkap, gz, net_flux;
   // mod_sw_dyn module arrays
-  A3 dpc, ptc, uc, vc, heating_rate, pkapb, gzb;
-  Scratch sc;
+  A3<R> dpc, ptc, uc, vc, heating_rate, pkapb, gzb;
+  Scratch<R> sc;
   // mod_remap module arrays
   double top_pressure;
-  A3 u_remap, v_remap, pt_remap, target_plev, target_pkap, target_playkap;
+  A3<R> u_remap, v_remap, pt_remap, target_plev, target_pkap, target_playkap;
   // mod_sync buffers (single image: every neighbour is this image)
-  std::vector<double> edge_buffer, corner_buffer;
+  std::vector<R> edge_buffer, corner_buffer;
   int nthreads = 1;
   bool poison = false;
   int32_t* trace = nullptr;
 };
 
+struct orc_state : StateT<double> {};
+struct orc_tlm : StateT<Dual> {};
+
 namespace {
 
 // ---------------------------------------------------------------- halo ----
 // mod_sync.f90:109-135 and 164-190 with neighbours(:) == this_image()
+template <class R>
 struct Halo {
-  orc_state* s;
+  StateT<R>* s;
   size_t nb;  // max(nx, ny)
-  double& eb(int a, int w, int k, int n, int idx) {
+  R& eb(int a, int w, int k, int n, int idx) {
     size_t L1 = (size_t)s->nlay + 1;
     return s->edge_buffer[(size_t)(a - 1) + nb * ((size_t)(w - 1) + HALO * ((size_t)(k - 1) + L1 * ((size_t)(n - 1) + 4 * (size_t)(idx - 1))))];
   }
-  double& cb(int a, int w, int k, int n, int idx) {
+  R& cb(int a, int w, int k, int n, int idx) {
     size_t L1 = (size_t)s->nlay + 1;
     return s->corner_buffer[(size_t)(a - 1) + HALO * ((size_t)(w - 1) + HALO * ((size_t)(k - 1) + L1 * ((size_t)(n - 1) + 4 * (size_t)(idx - 1))))];
   }
-  void to_buffer(A3& q, int idx, int kmax) {
+  void to_buffer(A3<R>& q, int idx, int kmax) {
     int isd = s->isd, ied = s->ied, jsd = s->jsd, jed = s->jed;
     for (int i = 0; i <= HALO - 1; ++i)
       for (int k = 1; k <= kmax; ++k) {
@@ -312,7 +335,7 @@ struct Halo {
         }
       }
   }
-  void from_buffer(A3& q, int idx, int kmax) {
+  void from_buffer(A3<R>& q, int idx, int kmax) {
     int isd = s->isd, ied = s->ied, jsd = s->jsd, jed = s->jed, js = s->js;
     for (int i = 1; i <= HALO; ++i)
       for (int k = 1; k <= kmax; ++k) {
@@ -334,15 +357,17 @@ struct Halo {
   }
 };
 
-void halo_exchange(orc_state* s, A3* const* f, int n, int kmax) {
-  Halo h{s, (size_t)std::max(s->nx, s->ny)};
+template <class R>
+void halo_exchange(StateT<R>* s, A3<R>* const* f, int n, int kmax) {
+  Halo<R> h{s, (size_t)std::max(s->nx, s->ny)};
   for (int a = 0; a < n; ++a) h.to_buffer(*f[a], a + 1, kmax);
   for (int a = 0; a < n; ++a) h.from_buffer(*f[a], a + 1, kmax);
 }
 
 // ------------------------------------------------------------ C grid ----
 // first layer loop body, mod_sw_dyn.f90:99-268
-void c_winds(orc_state* s, Scratch& sc, int k) {
+template <class R>
+void c_winds(StateT<R>* s, Scratch<R>& sc, int k) {
   int is = s->is, ie = s->ie, js = s->js, je = s->je;
   for (int j = js + 1; j <= je - 1; ++j)
     for (int i = is + 1; i <= ie - 1; ++i) {
@@ -357,11 +382,12 @@ void c_winds(orc_state* s, Scratch& sc, int k) {
     }
 }
 
-void c_layer1(orc_state* s, Scratch& sc, int k, double dt) {
+template <class R>
+void c_layer1(StateT<R>* s, Scratch<R>& sc, int k, double dt) {
   int is = s->is, ie = s->ie, js = s->js, je = s->je;
   double dtdx = dt * s->rdx, dtdy = dt * s->rdy, rA = s->rA;
-  A3 &dp = s->dp, &pt = s->pt, &uc = s->uc, &vc = s->vc, &dpc = s->dpc, &ptc = s->ptc;
-  A3 &pkap = s->pkap;
+  A3<R> &dp = s->dp, &pt = s->pt, &uc = s->uc, &vc = s->vc, &dpc = s->dpc, &ptc = s->ptc;
+  A3<R> &pkap = s->pkap;
   if (s->poison) { sc.poison(); sc.poison_winds(); }
 
   for (int j = js; j <= je; ++j)
@@ -384,9 +410,9 @@ void c_layer1(orc_state* s, Scratch& sc, int k, double dt) {
       sc.denom_y(i, j) = 1. / (1. - dtdy * (vc(i, j + 1, k) - vc(i, j, k)));
     }
 
-  A1 &fx = sc.fx, &fy = sc.fy;
-  A2 &tmp = sc.tmp, &lap = sc.laplacian, &dpfx = sc.dpfx, &dpfy = sc.dpfy;
-  V fxv{&fx.v[0], 1, fx.lb}, fyv{&fy.v[0], 1, fy.lb};
+  A1<R> &fx = sc.fx, &fy = sc.fy;
+  A2<R> &tmp = sc.tmp, &lap = sc.laplacian, &dpfx = sc.dpfx, &dpfy = sc.dpfy;
+  V<R> fxv{&fx.v[0], 1, fx.lb}, fyv{&fy.v[0], 1, fy.lb};
 
   // ---- dpc
   for (int i = is + 2; i <= ie - 2; ++i) {
@@ -457,22 +483,23 @@ void c_layer1(orc_state* s, Scratch& sc, int k, double dt) {
 
 // second layer loop body, mod_sw_dyn.f90:296-412.  ua/va are the module
 // arrays left by the LAST iteration of the first loop (layer nlay).
-void c_layer2(orc_state* s, Scratch& sc, int k, double dt, A2& ua, A2& va) {
+template <class R>
+void c_layer2(StateT<R>* s, Scratch<R>& sc, int k, double dt, A2<R>& ua, A2<R>& va) {
   int is = s->is, ie = s->ie, js = s->js, je = s->je;
   double dtdx = dt * s->rdx, dtdy = dt * s->rdy, rA = s->rA;
-  A3 &ud = s->ud, &vd = s->vd, &uc = s->uc, &vc = s->vc, &pkap = s->pkap, &gz = s->gz;
-  A1 &fx = sc.fx, &fy = sc.fy;
-  A2 &tmp = sc.tmp, &lap = sc.laplacian, &ke = sc.kinetic_energy, &vort = sc.vorticity;
-  V fxv{&fx.v[0], 1, fx.lb}, fyv{&fy.v[0], 1, fy.lb};
+  A3<R> &ud = s->ud, &vd = s->vd, &uc = s->uc, &vc = s->vc, &pkap = s->pkap, &gz = s->gz;
+  A1<R> &fx = sc.fx, &fy = sc.fy;
+  A2<R> &tmp = sc.tmp, &lap = sc.laplacian, &ke = sc.kinetic_energy, &vort = sc.vorticity;
+  V<R> fxv{&fx.v[0], 1, fx.lb}, fyv{&fy.v[0], 1, fy.lb};
   if (s->poison) { sc.poison(); sc.poison_courant(); }
 
   for (int i = is + 5; i <= ie - 5; ++i) {
-    V cv = scaled_temp(sc, dtdy, col(va, i, js + 2, js + 2), js + 2, je - 2);
+    V<R> cv = scaled_temp(sc, dtdy, col(va, i, js + 2, js + 2), js + 2, je - 2);
     flux(sc, fyv, col3(vc, i, js + 3, k, js + 2), cv, js + 2, je - 2, PPM_UNCONSTRAINED);
     for (int j = js + 5; j <= je - 5; ++j) ke(i, j) = va(i, j) * fy(j);
   }
   for (int j = js + 5; j <= je - 5; ++j) {
-    V cv = scaled_temp(sc, dtdx, row(ua, is + 2, j, is + 2), is + 2, ie - 2);
+    V<R> cv = scaled_temp(sc, dtdx, row(ua, is + 2, j, is + 2), is + 2, ie - 2);
     flux(sc, fxv, row3(uc, is + 3, j, k, is + 2), cv, is + 2, ie - 2, PPM_UNCONSTRAINED);
     for (int i = is + 5; i <= ie - 5; ++i) ke(i, j) = .5 * (ke(i, j) + ua(i, j) * fx(i));
   }
@@ -542,14 +569,16 @@ void par_for(int nthreads, int lo, int hi, F&& body) {
   for (std::thread& th : pool) th.join();
 }
 
-std::vector<Scratch> make_scratch(orc_state* s) {
-  std::vector<Scratch> t((size_t)std::max(1, s->nthreads));
-  for (Scratch& x : t) x.alloc(s->is, s->ie, s->js, s->je);
+template <class R>
+std::vector<Scratch<R>> make_scratch(StateT<R>* s) {
+  std::vector<Scratch<R>> t((size_t)std::max(1, s->nthreads));
+  for (Scratch<R>& x : t) x.alloc(s->is, s->ie, s->js, s->je);
   return t;
 }
 
 // mod_sw_dyn.f90:80-416
-void cgrid_dynamics_step(orc_state* s, double dt) {
+template <class R>
+void cgrid_dynamics_step(StateT<R>* s, double dt) {
   int is = s->is, ie = s->ie, js = s->js, je = s->je, L = s->nlay;
   par_for(s->nthreads, js, je, [&](int j, int t) { (void)t;
     for (int k = L; k >= 1; --k)
@@ -561,7 +590,7 @@ void cgrid_dynamics_step(orc_state* s, double dt) {
   if (s->nthreads <= 1) {
     for (int k = 1; k <= L; ++k) c_layer1(s, s->sc, k, dt);
   } else {
-    std::vector<Scratch> ts = make_scratch(s);
+    std::vector<Scratch<R>> ts = make_scratch(s);
     par_for(s->nthreads, 1, L, [&](int k, int t) { (void)t; c_layer1(s, ts[(size_t)t], k, dt); });
     c_winds(s, s->sc, L);  // the module ua/va keep layer nlay
   }
@@ -578,16 +607,17 @@ void cgrid_dynamics_step(orc_state* s, double dt) {
   if (s->nthreads <= 1) {
     for (int k = 1; k <= L; ++k) c_layer2(s, s->sc, k, dt, s->sc.ua, s->sc.va);
   } else {
-    std::vector<Scratch> ts = make_scratch(s);
+    std::vector<Scratch<R>> ts = make_scratch(s);
     par_for(s->nthreads, 1, L, [&](int k, int t) { (void)t; c_layer2(s, ts[(size_t)t], k, dt, s->sc.ua, s->sc.va); });
   }
 }
 
 // ------------------------------------------------------------ D grid ----
-void d_winds(orc_state* s, Scratch& sc, int k, double dt) {
+template <class R>
+void d_winds(StateT<R>* s, Scratch<R>& sc, int k, double dt) {
   int is = s->is, ie = s->ie, js = s->js, je = s->je;
   double dtdx = dt * s->rdx, dtdy = dt * s->rdy;
-  A3 &uc = s->uc, &vc = s->vc;
+  A3<R> &uc = s->uc, &vc = s->vc;
   for (int j = js + 1; j <= je; ++j)
     for (int i = is + 1; i <= ie; ++i) {
       sc.ub(i, j) = .5 * (uc(i, j, k) + uc(i, j - 1, k));
@@ -606,10 +636,11 @@ void d_winds(orc_state* s, Scratch& sc, int k, double dt) {
 }
 
 // first layer loop body, mod_sw_dyn.f90:441-598
-void d_layer1(orc_state* s, Scratch& sc, int k, double dt) {
+template <class R>
+void d_layer1(StateT<R>* s, Scratch<R>& sc, int k, double dt) {
   int is = s->is, ie = s->ie, js = s->js, je = s->je;
   double dtdx = dt * s->rdx, dtdy = dt * s->rdy, rA = s->rA;
-  A3 &dp = s->dp, &pt = s->pt, &dpc = s->dpc, &ptc = s->ptc, &pkap = s->pkap;
+  A3<R> &dp = s->dp, &pt = s->pt, &dpc = s->dpc, &ptc = s->ptc, &pkap = s->pkap;
   if (s->poison) { sc.poison(); sc.poison_winds(); }
   d_winds(s, sc, k, dt);
   for (int j = js; j <= je; ++j)
@@ -618,9 +649,9 @@ void d_layer1(orc_state* s, Scratch& sc, int k, double dt) {
       s->heating_rate(i, j, k) = (s->net_flux(i, j, k + 1) - s->net_flux(i, j, k)) /
                                  (CP_DRY * dpc(i, j, k) / s->gravity) / s->playkap(i, j, k);
     }
-  A1 &fx = sc.fx, &fy = sc.fy;
-  A2 &tmp = sc.tmp, &lap = sc.laplacian, &dpfx = sc.dpfx, &dpfy = sc.dpfy;
-  V fxv{&fx.v[0], 1, fx.lb}, fyv{&fy.v[0], 1, fy.lb};
+  A1<R> &fx = sc.fx, &fy = sc.fy;
+  A2<R> &tmp = sc.tmp, &lap = sc.laplacian, &dpfx = sc.dpfx, &dpfy = sc.dpfy;
+  V<R> fxv{&fx.v[0], 1, fx.lb}, fyv{&fy.v[0], 1, fy.lb};
 
   // ---- dp
   for (int i = is + 1; i <= ie - 1; ++i) {
@@ -696,22 +727,23 @@ void d_layer1(orc_state* s, Scratch& sc, int k, double dt) {
 // third layer loop body, mod_sw_dyn.f90:636-769.  ub, vb, cx, cy, denom_x
 // and denom_y are the module arrays left by the LAST iteration of the first
 // loop (layer nlay): w holds them.
-void d_layer3(orc_state* s, Scratch& sc, Scratch& w, int k, double dt) {
+template <class R>
+void d_layer3(StateT<R>* s, Scratch<R>& sc, Scratch<R>& w, int k, double dt) {
   int is = s->is, ie = s->ie, js = s->js, je = s->je;
   double dtdx = dt * s->rdx, dtdy = dt * s->rdy, rA = s->rA;
-  A3 &ud = s->ud, &vd = s->vd, &uc = s->uc, &vc = s->vc, &pkapb = s->pkapb, &gzb = s->gzb;
-  A1 &fx = sc.fx, &fy = sc.fy;
-  A2 &tmp = sc.tmp, &lap = sc.laplacian, &ke = sc.kinetic_energy, &vort = sc.vorticity, &div = sc.divergence;
-  V fxv{&fx.v[0], 1, fx.lb}, fyv{&fy.v[0], 1, fy.lb};
+  A3<R> &ud = s->ud, &vd = s->vd, &uc = s->uc, &vc = s->vc, &pkapb = s->pkapb, &gzb = s->gzb;
+  A1<R> &fx = sc.fx, &fy = sc.fy;
+  A2<R> &tmp = sc.tmp, &lap = sc.laplacian, &ke = sc.kinetic_energy, &vort = sc.vorticity, &div = sc.divergence;
+  V<R> fxv{&fx.v[0], 1, fx.lb}, fyv{&fy.v[0], 1, fy.lb};
   if (s->poison) sc.poison();
 
   for (int i = is + 4; i <= ie - 4; ++i) {
-    V cv = scaled_temp(sc, dtdy, col(w.vb, i, js + 1, js + 1), js + 1, je - 1);
+    V<R> cv = scaled_temp(sc, dtdy, col(w.vb, i, js + 1, js + 1), js + 1, je - 1);
     flux(sc, fyv, col3(vd, i, js + 1, k, js + 1), cv, js + 1, je - 1, PPM_CONSTRAINED);
     for (int j = js + 4; j <= je - 4; ++j) ke(i, j) = w.vb(i, j) * fy(j);
   }
   for (int j = js + 4; j <= je - 4; ++j) {
-    V cv = scaled_temp(sc, dtdx, row(w.ub, is + 1, j, is + 1), is + 1, ie - 1);
+    V<R> cv = scaled_temp(sc, dtdx, row(w.ub, is + 1, j, is + 1), is + 1, ie - 1);
     flux(sc, fxv, row3(ud, is + 1, j, k, is + 1), cv, is + 1, ie - 1, PPM_CONSTRAINED);
     for (int i = is + 4; i <= ie - 4; ++i) ke(i, j) = .5 * (ke(i, j) + w.ub(i, j) * fx(i));
   }
@@ -771,7 +803,8 @@ void d_layer3(orc_state* s, Scratch& sc, Scratch& w, int k, double dt) {
 }
 
 // mod_sw_dyn.f90:424-773
-void dgrid_dynamics_step(orc_state* s, double dt) {
+template <class R>
+void dgrid_dynamics_step(StateT<R>* s, double dt) {
   int is = s->is, ie = s->ie, js = s->js, je = s->je, L = s->nlay;
   par_for(s->nthreads, js, je, [&](int j, int t) { (void)t;
     for (int k = L; k >= 1; --k)
@@ -783,7 +816,7 @@ void dgrid_dynamics_step(orc_state* s, double dt) {
   if (s->nthreads <= 1) {
     for (int k = 1; k <= L; ++k) d_layer1(s, s->sc, k, dt);
   } else {
-    std::vector<Scratch> ts = make_scratch(s);
+    std::vector<Scratch<R>> ts = make_scratch(s);
     par_for(s->nthreads, 1, L, [&](int k, int t) { (void)t; d_layer1(s, ts[(size_t)t], k, dt); });
     d_winds(s, s->sc, L, dt);  // module ub, vb, cx, cy, denom keep layer nlay
   }
@@ -809,20 +842,21 @@ void dgrid_dynamics_step(orc_state* s, double dt) {
   if (s->nthreads <= 1) {
     for (int k = 1; k <= L; ++k) d_layer3(s, s->sc, s->sc, k, dt);
   } else {
-    std::vector<Scratch> ts = make_scratch(s);
+    std::vector<Scratch<R>> ts = make_scratch(s);
     par_for(s->nthreads, 1, L, [&](int k, int t) { (void)t; d_layer3(s, ts[(size_t)t], s->sc, k, dt); });
   }
 }
 
 // ------------------------------------------------------------- remap ----
+template <class R>
 struct PPMCol {
-  std::vector<double> btm_edge, top_edge, curvature, gam, level_var;
+  std::vector<R> btm_edge, top_edge, curvature, gam, level_var;
   void alloc(int L) {
-    btm_edge.assign((size_t)L + 1, NAN);
-    top_edge.assign((size_t)L + 1, NAN);
-    curvature.assign((size_t)L + 1, NAN);
-    gam.assign((size_t)L + 2, NAN);
-    level_var.assign((size_t)L + 2, NAN);
+    btm_edge.assign((size_t)L + 1, R(NAN));
+    top_edge.assign((size_t)L + 1, R(NAN));
+    curvature.assign((size_t)L + 1, R(NAN));
+    gam.assign((size_t)L + 2, R(NAN));
+    level_var.assign((size_t)L + 2, R(NAN));
   }
 };
 
@@ -830,10 +864,11 @@ struct PPMCol {
 // last interface reads gam(nlay+1), one past the end of gam; it cannot
 // change the result because level_var(nlay) is already clamped to the
 // same bounds at :319-320, so it is evaluated with both clamps here.
-void vertical_ppm(PPMCol& w, int L, const double* var, const double* coord) {
-  double* gam = w.gam.data();
-  double* level_var = w.level_var.data();
-  double alpha, beta;
+template <class R>
+void vertical_ppm(PPMCol<R>& w, int L, const R* var, const R* coord) {
+  R* gam = w.gam.data();
+  R* level_var = w.level_var.data();
+  R alpha, beta;
   alpha = (coord[L] - coord[L - 1]) / (coord[L + 1] - coord[L]);
   beta = alpha * (.5 + alpha);
   level_var[L + 1] = (2. * alpha * (1. + alpha) * var[L] + var[L - 1]) / beta;
@@ -853,7 +888,7 @@ void vertical_ppm(PPMCol& w, int L, const double* var, const double* coord) {
   level_var[2] = std::min(level_var[2], std::max(var[2], var[1]));
   level_var[2] = std::max(level_var[2], std::min(var[2], var[1]));
   for (int k = 2; k <= L - 1; ++k) {
-    double lo = std::min(var[k], var[k + 1]), hi = std::max(var[k], var[k + 1]);
+    R lo = std::min(var[k], var[k + 1]), hi = std::max(var[k], var[k + 1]);
     if (k + 2 > L || gam[k + 2] * gam[k] > 0) {
       level_var[k + 1] = std::min(level_var[k + 1], hi);
       level_var[k + 1] = std::max(level_var[k + 1], lo);
@@ -863,15 +898,15 @@ void vertical_ppm(PPMCol& w, int L, const double* var, const double* coord) {
       level_var[k + 1] = std::min(level_var[k + 1], hi);
     }
   }
-  double* top_edge = w.top_edge.data();
-  double* btm_edge = w.btm_edge.data();
+  R* top_edge = w.top_edge.data();
+  R* btm_edge = w.btm_edge.data();
   for (int k = 1; k <= L; ++k) {
     top_edge[k] = level_var[k + 1];
     btm_edge[k] = level_var[k];
   }
   for (int k = 2; k <= L - 1; ++k) {
-    double pmp1 = var[k + 1] - 2. * gam[k];
-    double lac1 = pmp1 + 1.5 * gam[k - 1];
+    R pmp1 = var[k + 1] - 2. * gam[k];
+    R lac1 = pmp1 + 1.5 * gam[k - 1];
     top_edge[k + 1] = std::min(std::max(top_edge[k + 1], fmin3(var[k + 1], pmp1, lac1)), fmax3(var[k + 1], pmp1, lac1));
     pmp1 = var[k + 1] + 2. * gam[k + 1];
     lac1 = pmp1 - 1.5 * gam[k];
@@ -881,13 +916,14 @@ void vertical_ppm(PPMCol& w, int L, const double* var, const double* coord) {
 }
 
 // mod_remap.f90:165-285; the O(nlay^2) pair loop of the reference.
-void remap_column(PPMCol& w, int L, const double* src_var, double* dst_var, const double* src_coord,
-                  const double* dst_coord, int32_t* trace) {
+template <class R>
+void remap_column(PPMCol<R>& w, int L, const R* src_var, R* dst_var, const R* src_coord,
+                  const R* dst_coord, int32_t* trace) {
   for (int m = 1; m <= L; ++m) dst_var[m] = 0.;
   vertical_ppm(w, L, src_var, src_coord);
-  const double* btm_edge = w.btm_edge.data();
-  const double* top_edge = w.top_edge.data();
-  const double* curvature = w.curvature.data();
+  const R* btm_edge = w.btm_edge.data();
+  const R* top_edge = w.top_edge.data();
+  const R* curvature = w.curvature.data();
   if (trace)
     for (int m = 1; m <= L; ++m) {
       int32_t* t = trace + 5 * (m - 1);
@@ -896,15 +932,15 @@ void remap_column(PPMCol& w, int L, const double* src_var, double* dst_var, cons
     }
   for (int k = 1; k <= L; ++k)
     for (int m = 1; m <= L; ++m) {
-      double dsrc_coord = src_coord[k + 1] - src_coord[k];
-      double s1 = (dst_coord[m] - src_coord[k]) / dsrc_coord;
-      double s2 = (dst_coord[m + 1] - src_coord[k]) / dsrc_coord;
-      double integral_factor = dsrc_coord / (dst_coord[m + 1] - dst_coord[m]);
+      R dsrc_coord = src_coord[k + 1] - src_coord[k];
+      R s1 = (dst_coord[m] - src_coord[k]) / dsrc_coord;
+      R s2 = (dst_coord[m + 1] - src_coord[k]) / dsrc_coord;
+      R integral_factor = dsrc_coord / (dst_coord[m + 1] - dst_coord[m]);
       if (src_coord[k + 1] >= dst_coord[m] || src_coord[k] <= dst_coord[m + 1]) continue;
       int which = 0;
-      double tmp3 = 2. * s1 * s1;
+      R tmp3 = 2. * s1 * s1;
       if (dst_coord[m + 1] <= src_coord[k + 1] && src_coord[k + 1] < dst_coord[m] && dst_coord[m] < src_coord[k]) {
-        double tmp1 = s1 - 1., tmp2 = s1 + 1.;
+        R tmp1 = s1 - 1., tmp2 = s1 + 1.;
         dst_var[m] = dst_var[m] + tmp1 / 6. *
                                       (3. * (btm_edge[k] * tmp1 - top_edge[k] * tmp2) + curvature[k] * (tmp3 - tmp2)) *
                                       integral_factor;
@@ -921,7 +957,7 @@ void remap_column(PPMCol& w, int L, const double* src_var, double* dst_var, cons
         which = which * 10 + 5;
       }
       if (src_coord[k + 1] < dst_coord[m + 1] && dst_coord[m] < src_coord[k]) {
-        double tmp1 = s1 + s2;
+        R tmp1 = s1 + s2;
         dst_var[m] = dst_var[m] + (s1 - s2) / 6. *
                                       (3. * (btm_edge[k] * (tmp1 - 2.) - top_edge[k] * tmp1) +
                                        curvature[k] * (tmp3 + tmp1 * (2. * s2 - 3.))) *
@@ -940,26 +976,27 @@ void remap_column(PPMCol& w, int L, const double* src_var, double* dst_var, cons
 }
 
 // mod_remap.f90:27-163
-void perform_vertical_remapping(orc_state* s) {
+template <class R>
+void perform_vertical_remapping(StateT<R>* s) {
   int L = s->nlay, isd = s->isd, ied = s->ied, jsd = s->jsd, jed = s->jed;
   int isl = isd - 3, iel = ied + 3, jsl = jsd - 3, jel = jed + 3;
-  A3 &plev = s->plev, &pkap = s->pkap, &playkap = s->playkap, &gz = s->gz;
-  A3 &tpl = s->target_plev, &tpk = s->target_pkap, &tplk = s->target_playkap;
-  A3 &dp = s->dp, &pt = s->pt, &ud = s->ud, &vd = s->vd;
+  A3<R> &plev = s->plev, &pkap = s->pkap, &playkap = s->playkap, &gz = s->gz;
+  A3<R> &tpl = s->target_plev, &tpk = s->target_pkap, &tplk = s->target_playkap;
+  A3<R> &dp = s->dp, &pt = s->pt, &ud = s->ud, &vd = s->vd;
 
   par_for(s->nthreads, jsl, jel, [&](int j, int t) { (void)t;
     for (int k = L; k >= 1; --k)
       for (int i = isl; i <= iel; ++i) {
         plev(i, j, k) = plev(i, j, k + 1) + dp(i, j, k);
         pkap(i, j, k) = orc_pow_impl(plev(i, j, k), KAPPA);
-        double plog = orc_log_impl(pkap(i, j, k + 1) / pkap(i, j, k));
+        R plog = orc_log_impl(pkap(i, j, k + 1) / pkap(i, j, k));
         playkap(i, j, k) = (pkap(i, j, k + 1) - pkap(i, j, k)) / plog;
       }
     for (int k = L; k >= 1; --k)
       for (int i = isl; i <= iel; ++i) {
         tpl(i, j, k) = s->coord_Ak(k) + s->coord_Bk(k) * (plev(i, j, 1) - s->top_pressure);
         tpk(i, j, k) = orc_pow_impl(tpl(i, j, k), KAPPA);
-        double plog = orc_log_impl(tpk(i, j, k + 1) / tpk(i, j, k));
+        R plog = orc_log_impl(tpk(i, j, k + 1) / tpk(i, j, k));
         tplk(i, j, k) = (tpk(i, j, k + 1) - tpk(i, j, k)) / plog;
       }
     for (int k = 1; k <= L; ++k)
@@ -976,9 +1013,9 @@ void perform_vertical_remapping(orc_state* s) {
     for (size_t q = 0; q < (size_t)3 * nyr * nxr * L * 5; ++q) s->trace[q] = -1;
 
   par_for(s->nthreads, isd - 1, ied + 1, [&](int i, int t) { (void)t;
-    PPMCol w;
+    PPMCol<R> w;
     w.alloc(L);
-    std::vector<double> src_plev(L + 2), dst_plev(L + 2), col(L + 2), out(L + 2);
+    std::vector<R> src_plev(L + 2), dst_plev(L + 2), col(L + 2), out(L + 2);
     for (int j = jsd - 1; j <= jed + 1; ++j) {
       for (int k = 1; k <= L + 1; ++k) {
         src_plev[k] = C7_12 * (plev(i, j, k) + plev(i, j - 1, k)) - C1_12 * (plev(i, j + 1, k) + plev(i, j - 2, k));
@@ -997,12 +1034,12 @@ void perform_vertical_remapping(orc_state* s) {
     }
   });
 
-  A3 &ur = s->u_remap, &vr = s->v_remap;
+  A3<R> &ur = s->u_remap, &vr = s->v_remap;
   par_for(s->nthreads, isd, ied, [&](int i, int t) { (void)t;
-    PPMCol w;
+    PPMCol<R> w;
     w.alloc(L);
-    std::vector<double> energy(L + 2), energy_remap(L + 2), gz_remap(L + 2), ua(L + 2), va(L + 2);
-    std::vector<double> src(L + 2), dst(L + 2);
+    std::vector<R> energy(L + 2), energy_remap(L + 2), gz_remap(L + 2), ua(L + 2), va(L + 2);
+    std::vector<R> src(L + 2), dst(L + 2);
     for (int j = jsd; j <= jed; ++j) {
       for (int k = 1; k <= L; ++k) {
         ua[k] = (.25 * (ud(i, j, k) + ud(i, j + 1, k)) +
@@ -1043,7 +1080,8 @@ void perform_vertical_remapping(orc_state* s) {
   });
 }
 
-A3* field_ptr(orc_state* s, int f) {
+template <class R>
+A3<R>* field_ptr(StateT<R>* s, int f) {
   switch (f) {
     case ORC_DP: return &s->dp;
     case ORC_PT: return &s->pt;
@@ -1063,12 +1101,12 @@ A3* field_ptr(orc_state* s, int f) {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-orc_state* orc_create(int nx, int ny, int nlay, double dx, double dy, const double* ak, const double* bk,
-                      double gravity, double coriolis, double divdamp, double vortdamp) {
-  if (nx < HALO || ny < HALO || nlay < 3 || !ak || !bk) return nullptr;
-  orc_state* s = new orc_state();
+template <class R>
+bool setup_state(StateT<R>* s, int nx, int ny, int nlay, double dx, double dy, const double* ak, const double* bk,
+                 double gravity, double coriolis, double divdamp, double vortdamp) {
+  if (nx < HALO || ny < HALO || nlay < 3 || !ak || !bk) return false;
   s->nx = nx; s->ny = ny; s->nlay = nlay; s->dx = dx; s->dy = dy;
   s->isd = 1; s->ied = nx; s->jsd = 1; s->jed = ny;  // mod_tiles.f90:222-241, one image
   s->is = s->isd - HALO; s->ie = s->ied + HALO; s->js = s->jsd - HALO; s->je = s->jed + HALO;
@@ -1078,11 +1116,11 @@ orc_state* orc_create(int nx, int ny, int nlay, double dx, double dy, const doub
   s->coord_Bk.alloc(1, nlay + 1);
   for (int k = 1; k <= nlay + 1; ++k) { s->coord_Ak(k) = ak[k - 1]; s->coord_Bk(k) = bk[k - 1]; }
   int is = s->is, ie = s->ie, js = s->js, je = s->je, L = nlay;
-  for (A3* a : {&s->dp, &s->pt, &s->ud, &s->vd, &s->playkap}) a->alloc(is, ie, js, je, 1, L);
-  for (A3* a : {&s->plev, &s->pkap, &s->gz}) a->alloc(is, ie, js, je, 1, L + 1);
-  s->net_flux.alloc(is, ie, js, je, 1, L + 1, 0.0);  // radiation is off: zero flux
-  for (A3* a : {&s->dpc, &s->ptc, &s->uc, &s->vc, &s->heating_rate}) a->alloc(is, ie, js, je, 1, L);
-  for (A3* a : {&s->pkapb, &s->gzb}) a->alloc(is, ie, js, je, 1, L + 1);
+  for (A3<R>* a : {&s->dp, &s->pt, &s->ud, &s->vd, &s->playkap}) a->alloc(is, ie, js, je, 1, L);
+  for (A3<R>* a : {&s->plev, &s->pkap, &s->gz}) a->alloc(is, ie, js, je, 1, L + 1);
+  s->net_flux.alloc(is, ie, js, je, 1, L + 1, R(0.0));  // radiation is off: zero flux
+  for (A3<R>* a : {&s->dpc, &s->ptc, &s->uc, &s->vc, &s->heating_rate}) a->alloc(is, ie, js, je, 1, L);
+  for (A3<R>* a : {&s->pkapb, &s->gzb}) a->alloc(is, ie, js, je, 1, L + 1);
   s->sc.alloc(is, ie, js, je);
   s->u_remap.alloc(s->isd - 1, s->ied + 1, s->jsd - 1, s->jed + 1, 1, L);
   s->v_remap.alloc(s->isd - 1, s->ied + 1, s->jsd - 1, s->jed + 1, 1, L);
@@ -1091,47 +1129,54 @@ orc_state* orc_create(int nx, int ny, int nlay, double dx, double dy, const doub
   s->target_pkap.alloc(s->isd - 3, s->ied + 3, s->jsd - 3, s->jed + 3, 1, L + 1);
   s->target_playkap.alloc(s->isd - 3, s->ied + 3, s->jsd - 3, s->jed + 3, 1, L);
   size_t nb = (size_t)std::max(nx, ny);
-  s->edge_buffer.assign(nb * HALO * (L + 1) * 4 * 5, NAN);
-  s->corner_buffer.assign((size_t)HALO * HALO * (L + 1) * 4 * 5, NAN);
-  return s;
+  s->edge_buffer.assign(nb * HALO * (L + 1) * 4 * 5, R(NAN));
+  s->corner_buffer.assign((size_t)HALO * HALO * (L + 1) * 4 * 5, R(NAN));
+  return true;
 }
 
-void orc_destroy(orc_state* s) { delete s; }
-
-int orc_field_levels(orc_state* s, int field) {
-  A3* a = field_ptr(s, field);
-  return a ? a->k1 : -1;
+// copy a field between the state and flat (val, tan) arrays; tan may be NULL
+template <class R> inline void put_(R& x, double v, const double* tan, size_t n);
+template <> inline void put_<double>(double& x, double v, const double*, size_t) { x = v; }
+template <> inline void put_<Dual>(Dual& x, double v, const double* tan, size_t n) { x = Dual(v, tan ? tan[n] : 0.); }
+template <class R> inline void get_(const R& x, double* v, double* tan, size_t n);
+template <> inline void get_<double>(const double& x, double* v, double*, size_t n) { v[n] = x; }
+template <> inline void get_<Dual>(const Dual& x, double* v, double* tan, size_t n) {
+  if (v) v[n] = x.v;
+  if (tan) tan[n] = x.d;
 }
 
-int orc_set_field(orc_state* s, int field, const double* a, int with_halo) {
-  A3* f = field_ptr(s, field);
+template <class R>
+int set_field(StateT<R>* s, int field, const double* a, const double* tan, int with_halo) {
+  A3<R>* f = field_ptr(s, field);
   if (!f || !a) return -1;
   if (with_halo) {
-    std::memcpy(f->v.data(), a, f->v.size() * sizeof(double));
+    for (size_t n = 0; n < f->v.size(); ++n) put_<R>(f->v[n], a[n], tan, n);
     return 0;
   }
   size_t n = 0;
   for (int k = 1; k <= f->k1; ++k)
     for (int j = s->jsd; j <= s->jed; ++j)
-      for (int i = s->isd; i <= s->ied; ++i) (*f)(i, j, k) = a[n++];
+      for (int i = s->isd; i <= s->ied; ++i, ++n) put_<R>((*f)(i, j, k), a[n], tan, n);
   return 0;
 }
 
-int orc_get_field(orc_state* s, int field, double* a, int with_halo) {
-  A3* f = field_ptr(s, field);
-  if (!f || !a) return -1;
+template <class R>
+int get_field(StateT<R>* s, int field, double* a, double* tan, int with_halo) {
+  A3<R>* f = field_ptr(s, field);
+  if (!f) return -1;
   if (with_halo) {
-    std::memcpy(a, f->v.data(), f->v.size() * sizeof(double));
+    for (size_t n = 0; n < f->v.size(); ++n) get_<R>(f->v[n], a, tan, n);
     return 0;
   }
   size_t n = 0;
   for (int k = 1; k <= f->k1; ++k)
     for (int j = s->jsd; j <= s->jed; ++j)
-      for (int i = s->isd; i <= s->ied; ++i) a[n++] = (*f)(i, j, k);
+      for (int i = s->isd; i <= s->ied; ++i, ++n) get_<R>((*f)(i, j, k), a, tan, n);
   return 0;
 }
 
-void orc_init(orc_state* s) {
+template <class R>
+void init_state(StateT<R>* s) {
   int is = s->is, ie = s->ie, js = s->js, je = s->je, L = s->nlay;
   double top = s->coord_Ak(1);
   // mod_input.f90:229-231
@@ -1142,7 +1187,7 @@ void orc_init(orc_state* s) {
     }
   // mod_input.f90:247: halo_exchange(dp, pt, gz, ud, vd) through the
   // 5 x nlay-layer interface, so gz levels 1..nlay are exchanged
-  A3* f5[] = {&s->dp, &s->pt, &s->gz, &s->ud, &s->vd};
+  A3<R>* f5[] = {&s->dp, &s->pt, &s->gz, &s->ud, &s->vd};
   halo_exchange(s, f5, 5, L);
   // init_sw_dyn, mod_sw_dyn.f90:958-1023
   s->rdx = 1. / s->dx;
@@ -1168,21 +1213,51 @@ void orc_init(orc_state* s) {
     }
 }
 
-void orc_cgrid_step(orc_state* s, double dt) { cgrid_dynamics_step(s, dt); }
-void orc_cgrid_halo(orc_state* s) {
-  A3* f4[] = {&s->dpc, &s->ptc, &s->uc, &s->vc};
+template <class R>
+void cgrid_halo(StateT<R>* s) {
+  A3<R>* f4[] = {&s->dpc, &s->ptc, &s->uc, &s->vc};
   halo_exchange(s, f4, 4, s->nlay);
 }
-void orc_dgrid_step(orc_state* s, double dt) { dgrid_dynamics_step(s, dt); }
-void orc_remap(orc_state* s) { perform_vertical_remapping(s); }
-void orc_dgrid_halo(orc_state* s) {
-  A3* f4[] = {&s->dp, &s->pt, &s->ud, &s->vd};
+template <class R>
+void dgrid_halo(StateT<R>* s) {
+  A3<R>* f4[] = {&s->dp, &s->pt, &s->ud, &s->vd};
   halo_exchange(s, f4, 4, s->nlay);
 }
 
+}  // namespace
+
+extern "C" {
+
+orc_state* orc_create(int nx, int ny, int nlay, double dx, double dy, const double* ak, const double* bk,
+                      double gravity, double coriolis, double divdamp, double vortdamp) {
+  orc_state* s = new orc_state();
+  if (!setup_state<double>(s, nx, ny, nlay, dx, dy, ak, bk, gravity, coriolis, divdamp, vortdamp)) {
+    delete s;
+    return nullptr;
+  }
+  return s;
+}
+void orc_destroy(orc_state* s) { delete s; }
+int orc_field_levels(orc_state* s, int field) {
+  A3<double>* a = field_ptr<double>(s, field);
+  return a ? a->k1 : -1;
+}
+int orc_set_field(orc_state* s, int field, const double* a, int with_halo) {
+  return set_field<double>(s, field, a, nullptr, with_halo);
+}
+int orc_get_field(orc_state* s, int field, double* a, int with_halo) {
+  return a ? get_field<double>(s, field, a, nullptr, with_halo) : -1;
+}
+void orc_init(orc_state* s) { init_state<double>(s); }
+void orc_cgrid_step(orc_state* s, double dt) { cgrid_dynamics_step<double>(s, dt); }
+void orc_cgrid_halo(orc_state* s) { cgrid_halo<double>(s); }
+void orc_dgrid_step(orc_state* s, double dt) { dgrid_dynamics_step<double>(s, dt); }
+void orc_remap(orc_state* s) { perform_vertical_remapping<double>(s); }
+void orc_dgrid_halo(orc_state* s) { dgrid_halo<double>(s); }
+
 // mod_fields.f90:69-106
 int orc_check_stability(orc_state* s) {
-  for (A3* a : {&s->dp, &s->pt, &s->ud, &s->vd})
+  for (A3<double>* a : {&s->dp, &s->pt, &s->ud, &s->vd})
     for (int k = 1; k <= s->nlay; ++k)
       for (int j = s->jsd; j <= s->jed; ++j)
         for (int i = s->isd; i <= s->ied; ++i)
@@ -1208,5 +1283,30 @@ void orc_pow_array(const double* x, double y, double* out, int n) {
 void orc_log_array(const double* x, double* out, int n) {
   for (int i = 0; i < n; ++i) out[i] = orc_log_impl(x[i]);
 }
+
+// ---- tangent-linear model: the same restatement on dual numbers
+orc_tlm* tlm_create(int nx, int ny, int nlay, double dx, double dy, const double* ak, const double* bk,
+                    double gravity, double coriolis, double divdamp, double vortdamp) {
+  orc_tlm* s = new orc_tlm();
+  if (!setup_state<Dual>(s, nx, ny, nlay, dx, dy, ak, bk, gravity, coriolis, divdamp, vortdamp)) {
+    delete s;
+    return nullptr;
+  }
+  return s;
+}
+void tlm_destroy(orc_tlm* s) { delete s; }
+int tlm_set_field(orc_tlm* s, int field, const double* val, const double* tan, int with_halo) {
+  return set_field<Dual>(s, field, val, tan, with_halo);
+}
+int tlm_get_field(orc_tlm* s, int field, double* val, double* tan, int with_halo) {
+  return get_field<Dual>(s, field, val, tan, with_halo);
+}
+void tlm_init(orc_tlm* s) { init_state<Dual>(s); }
+void tlm_cgrid_step(orc_tlm* s, double dt) { cgrid_dynamics_step<Dual>(s, dt); }
+void tlm_cgrid_halo(orc_tlm* s) { cgrid_halo<Dual>(s); }
+void tlm_dgrid_step(orc_tlm* s, double dt) { dgrid_dynamics_step<Dual>(s, dt); }
+void tlm_remap(orc_tlm* s) { perform_vertical_remapping<Dual>(s); }
+void tlm_dgrid_halo(orc_tlm* s) { dgrid_halo<Dual>(s); }
+void tlm_set_threads(orc_tlm* s, int n) { s->nthreads = n < 1 ? 1 : n; }
 
 }  // extern "C"

@@ -74,6 +74,24 @@ void orc_set_poison(orc_state* s, int on);
    Columns that a variable does not remap hold -1. NULL disables. */
 void orc_set_remap_trace(orc_state* s, int32_t* buf);
 
+/* Tangent-linear model: the same restatement on dual numbers (dual.h).  A
+   field carries values and tangents; the value part is bit-identical to the
+   FP64 run, so the tangents are the derivative of the branch-frozen step. */
+typedef struct orc_tlm orc_tlm;
+orc_tlm* tlm_create(int nx, int ny, int nlay, double dx, double dy, const double* ak, const double* bk,
+                    double gravity, double coriolis, double divdamp, double vortdamp);
+void tlm_destroy(orc_tlm* s);
+/* tan may be NULL (zero tangents on set; not returned on get) */
+int tlm_set_field(orc_tlm* s, int field, const double* val, const double* tan, int with_halo);
+int tlm_get_field(orc_tlm* s, int field, double* val, double* tan, int with_halo);
+void tlm_init(orc_tlm* s);
+void tlm_cgrid_step(orc_tlm* s, double dt);
+void tlm_cgrid_halo(orc_tlm* s);
+void tlm_dgrid_step(orc_tlm* s, double dt);
+void tlm_remap(orc_tlm* s);
+void tlm_dgrid_halo(orc_tlm* s);
+void tlm_set_threads(orc_tlm* s, int nthreads);
+
 /* the x**y and log(x) the oracle uses, element-wise (accuracy tests) */
 void orc_pow_array(const double* x, double y, double* out, int n);
 void orc_log_array(const double* x, double* out, int n);

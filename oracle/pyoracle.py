@@ -146,3 +146,78 @@ def log_array(x, variant='portable'):
     out = np.empty_like(x)
     load(variant).orc_log_array(_ptr(x), _ptr(out), x.size)
     return out
+
+
+class TLMModel:
+    """Tangent-linear model of the oracle (dual numbers, branches frozen at
+    the FP64 trajectory); the stepper interface of atmdyn.model.run_model."""
+
+    def __init__(self, st, tangents=None, threads: int = 1):
+        self.lib = load('portable')
+        lib = self.lib
+        if not hasattr(lib, '_tlm_ready'):
+            vp = [ctypes.c_void_p]
+            lib.tlm_create.restype = ctypes.c_void_p
+            lib.tlm_create.argtypes = lib.orc_create.argtypes
+            lib.tlm_destroy.argtypes = vp
+            lib.tlm_set_field.argtypes = vp + [ctypes.c_int, _P, _P, ctypes.c_int]
+            lib.tlm_get_field.argtypes = vp + [ctypes.c_int, _P, _P, ctypes.c_int]
+            for f in ('tlm_init', 'tlm_cgrid_halo', 'tlm_remap', 'tlm_dgrid_halo'):
+                getattr(lib, f).argtypes = vp
+            lib.tlm_cgrid_step.argtypes = vp + [ctypes.c_double]
+            lib.tlm_dgrid_step.argtypes = vp + [ctypes.c_double]
+            lib.tlm_set_threads.argtypes = vp + [ctypes.c_int]
+            lib._tlm_ready = True
+        self.st = st
+        self.nx, self.ny, self.nlay = st.nx, st.ny, st.nlay
+        ak = np.ascontiguousarray(st.ak, dtype=np.float64)
+        bk = np.ascontiguousarray(st.bk, dtype=np.float64)
+        self.s = lib.tlm_create(st.nx, st.ny, st.nlay, st.dx, st.dy, _ptr(ak), _ptr(bk),
+                                st.gravity, st.coriolis, st.divdamp, st.vortdamp)
+        lib.tlm_set_threads(self.s, threads)
+        tangents = tangents or {}
+        for name, f, a in (('dp', DP, st.dp), ('pt', PT, st.pt), ('ud', UD, st.u), ('vd', VD, st.v)):
+            self.set(f, a, tangents.get(name))
+        gz = np.zeros((st.nlay + 1, st.ny, st.nx))
+        gz[0] = st.gzs
+        self.set(GZ, gz, None)
+        lib.tlm_init(self.s)
+
+    def __del__(self):
+        if getattr(self, 's', None):
+            self.lib.tlm_destroy(self.s)
+            self.s = None
+
+    def levels(self, field):
+        return self.nlay + 1 if field in (GZ, PLEV, PKAP, NET_FLUX) else self.nlay
+
+    def set(self, field, val, tan=None, halo=False):
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        t = None if tan is None else np.ascontiguousarray(tan, dtype=np.float64)
+        assert self.lib.tlm_set_field(self.s, field, _ptr(val), None if t is None else _ptr(t), int(halo)) == 0
+
+    def get(self, field, halo=False):
+        K = self.levels(field)
+        shape = (K, self.ny + 2 * HALO, self.nx + 2 * HALO) if halo else (K, self.ny, self.nx)
+        v = np.empty(shape)
+        t = np.empty(shape)
+        assert self.lib.tlm_get_field(self.s, field, _ptr(v), _ptr(t), int(halo)) == 0
+        return v, t
+
+    def cgrid_step(self, dt_half):
+        self.lib.tlm_cgrid_step(self.s, dt_half)
+
+    def cgrid_halo(self):
+        self.lib.tlm_cgrid_halo(self.s)
+
+    def dgrid_step(self, dt):
+        self.lib.tlm_dgrid_step(self.s, dt)
+
+    def remap(self):
+        self.lib.tlm_remap(self.s)
+
+    def dgrid_halo(self):
+        self.lib.tlm_dgrid_halo(self.s)
+
+    def check_stability(self):
+        return True
