@@ -27,7 +27,11 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_set_net_flux', 'atm_step', 'atm_sync', 'atm_destroy', 'atm_last_error',
            'atm_upload_device', 'atm_download_device', 'atm_set_stream', 'atm_remap_trace',
            'atm_device_pow_log', 'atm_version', 'atm_profile', 'atm_profile_read', 'atm_profile_stage',
-           'atm_launch_count', 'atm_remap_noalloc', 'atm_device_div_check')
+           'atm_launch_count', 'atm_remap_noalloc', 'atm_device_div_check',
+           'atm_adj_enable', 'atm_adj_zero', 'atm_adj_set', 'atm_adj_get', 'atm_adj_set_device',
+           'atm_adj_get_device', 'atm_adj_step', 'atm_adj_halo', 'atm_adj_cgrid_halo', 'atm_adj_cgrid_step',
+           'atm_adj_dgrid_step', 'atm_adj_remap', 'atm_state_bytes', 'atm_state_save', 'atm_state_load')
+ATM_ADJ_IN, ATM_ADJ_OUT = 0, 1
 
 # the entry points every build must export
 CORE = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_step', 'atm_cgrid_halo',
@@ -85,6 +89,21 @@ def load():
         'atm_profile_stage': ([i], ctypes.c_char_p),
         'atm_launch_count': ([vp, ctypes.POINTER(ctypes.c_longlong)], None),
         'atm_device_div_check': ([ctypes.c_longlong, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)], None),
+        'atm_adj_enable': ([vp], None),
+        'atm_adj_zero': ([vp], None),
+        'atm_adj_set': ([vp, i, i, P], None),
+        'atm_adj_get': ([vp, i, i, P], None),
+        'atm_adj_set_device': ([vp, i, i, vp], None),
+        'atm_adj_get_device': ([vp, i, i, vp], None),
+        'atm_adj_step': ([vp, d, i], None),
+        'atm_adj_halo': ([vp, i], None),
+        'atm_adj_cgrid_halo': ([vp], None),
+        'atm_adj_cgrid_step': ([vp, d], None),
+        'atm_adj_dgrid_step': ([vp, d], None),
+        'atm_adj_remap': ([vp], None),
+        'atm_state_bytes': ([vp, ctypes.POINTER(ctypes.c_longlong)], None),
+        'atm_state_save': ([vp, vp], None),
+        'atm_state_load': ([vp, vp], None),
     }
     for f, (args, res) in optional.items():
         if hasattr(lib, f):

@@ -176,6 +176,70 @@ class Dycore:
     def state(self):
         return {name: self.get(f) for name, f in (('dp', ATM_DP), ('pt', ATM_PT), ('ud', ATM_UD), ('vd', ATM_VD))}
 
+    # ---- adjoint (FP64 form): hand-written reverse mode of the step
+    def adj_enable(self):
+        check(self.lib.atm_adj_enable(self.ctx), self.ctx, 'atm_adj_enable')
+
+    def adj_zero(self):
+        check(self.lib.atm_adj_zero(self.ctx), self.ctx, 'atm_adj_zero')
+
+    def adj_set(self, slot, field, a_halo):
+        """Adjoint field of slot 'in'/'out' (dp, pt, ud, vd) or a C-grid
+        adjoint (dpc, ptc, uc, vc) from a (K, ny+14, nx+14) array."""
+        if isinstance(field, str):
+            field = FIELDS[field]
+        a = np.ascontiguousarray(a_halo, dtype=np.float64)
+        check(self.lib.atm_adj_set(self.ctx, _SLOTS[slot], field, _ptr(a)), self.ctx, 'atm_adj_set')
+
+    def adj_get(self, slot, field, halo=True):
+        if isinstance(field, str):
+            field = FIELDS[field]
+        out = np.empty((self.nlay, self.ny + 2 * HALO, self.nx + 2 * HALO))
+        check(self.lib.atm_adj_get(self.ctx, _SLOTS[slot], field, _ptr(out)), self.ctx, 'atm_adj_get')
+        return out if halo else out[:, HALO:HALO + self.ny, HALO:HALO + self.nx].copy()
+
+    def adj_set_device(self, slot, field, ptr):
+        """Interior adjoint from a contiguous float64 (nlay, ny, nx) device buffer."""
+        if isinstance(field, str):
+            field = FIELDS[field]
+        check(self.lib.atm_adj_set_device(self.ctx, _SLOTS[slot], field, ctypes.c_void_p(ptr)), self.ctx,
+              'atm_adj_set_device')
+
+    def adj_get_device(self, slot, field, ptr):
+        if isinstance(field, str):
+            field = FIELDS[field]
+        check(self.lib.atm_adj_get_device(self.ctx, _SLOTS[slot], field, ctypes.c_void_p(ptr)), self.ctx,
+              'atm_adj_get_device')
+
+    def adj_step(self, dt, remap=False):
+        check(self.lib.atm_adj_step(self.ctx, dt, int(remap)), self.ctx, 'atm_adj_step')
+
+    def adj_halo(self, slot='out'):
+        check(self.lib.atm_adj_halo(self.ctx, _SLOTS[slot]), self.ctx, 'atm_adj_halo')
+
+    def adj_cgrid_halo(self):
+        check(self.lib.atm_adj_cgrid_halo(self.ctx), self.ctx, 'atm_adj_cgrid_halo')
+
+    def adj_cgrid_step(self, dt_half):
+        check(self.lib.atm_adj_cgrid_step(self.ctx, dt_half), self.ctx, 'atm_adj_cgrid_step')
+
+    def adj_dgrid_step(self, dt):
+        check(self.lib.atm_adj_dgrid_step(self.ctx, dt), self.ctx, 'atm_adj_dgrid_step')
+
+    def adj_remap(self):
+        check(self.lib.atm_adj_remap(self.ctx), self.ctx, 'atm_adj_remap')
+
+    def state_bytes(self):
+        n = ctypes.c_longlong(0)
+        check(self.lib.atm_state_bytes(self.ctx, ctypes.byref(n)), self.ctx, 'atm_state_bytes')
+        return n.value
+
+    def state_save(self, ptr):
+        check(self.lib.atm_state_save(self.ctx, ctypes.c_void_p(ptr)), self.ctx, 'atm_state_save')
+
+    def state_load(self, ptr):
+        check(self.lib.atm_state_load(self.ctx, ctypes.c_void_p(ptr)), self.ctx, 'atm_state_load')
+
 
 def device_pow_log(x, y):
     lib = _lib.load()
@@ -184,3 +248,7 @@ def device_pow_log(x, y):
     lg = np.empty_like(x)
     check(lib.atm_device_pow_log(_ptr(x), float(y), _ptr(p), _ptr(lg), x.size), None, 'atm_device_pow_log')
     return p, lg
+
+
+_SLOTS = {'in': _lib.ATM_ADJ_IN, 'out': _lib.ATM_ADJ_OUT, _lib.ATM_ADJ_IN: _lib.ATM_ADJ_IN,
+          _lib.ATM_ADJ_OUT: _lib.ATM_ADJ_OUT}

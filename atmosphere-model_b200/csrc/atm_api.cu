@@ -81,6 +81,15 @@ struct atm_ctx {
   std::vector<int> ev_stage;  // stage of each recorded (start, stop) pair
   size_t ev_used = 0;
   long long launches = 0;
+  // adjoint (FP64): two slots of state adjoints (physical index of slot IN
+  // is slot_in; the slots swap as steps are reversed), the C-grid adjoints,
+  // and the adjoints of pkap, gz, pkapb, gzb and the remapped face winds
+  bool adj = false;
+  double* lam[2][4] = {{nullptr}};
+  double* lam_cg[4] = {nullptr};
+  double *lam_pk = nullptr, *lam_gz = nullptr, *lam_pkb = nullptr, *lam_gzb = nullptr;
+  double *lam_ur = nullptr, *lam_vr = nullptr;
+  int slot_in = 0;
   std::string err;
 };
 
@@ -133,6 +142,11 @@ void free_all(atm_ctx* c) {
   void* ps[] = {c->pkap, c->gz, c->pkapb, c->gzb, c->stage, c->urem, c->vrem, c->nf, c->heat,
                 c->d_ak, c->d_bk, c->partial, c->d_mass, c->status, c->d_trace};
   for (void* p : ps) cudaFree(p);
+  for (int t = 0; t < 2; ++t)
+    for (int f = 0; f < 4; ++f) cudaFree(c->lam[t][f]);
+  for (int f = 0; f < 4; ++f) cudaFree(c->lam_cg[f]);
+  double* pl[] = {c->lam_pk, c->lam_gz, c->lam_pkb, c->lam_gzb, c->lam_ur, c->lam_vr};
+  for (double* p : pl) cudaFree(p);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_mass) cudaFreeHost(c->h_mass);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
@@ -153,10 +167,12 @@ cudaError_t d2h_pitched(atm_ctx* c, double* host, const double* dev, int K) {
 
 const char* const STAGE_NAMES[] = {"c_mass",  "c_column", "c_mom",        "c_halo",      "d_ring",
                                    "d_mass",  "d_column", "d_corners",    "d_mom",       "remap_ring",
-                                   "remap_winds", "remap_energy", "d_halo", "heating", "check"};
-constexpr int NSTAGE = 15;
+                                   "remap_winds", "remap_energy", "d_halo", "heating", "check",
+                                   "adj_forward", "adj_remap", "adj_d_mom", "adj_d_column", "adj_d_mass",
+                                   "adj_c_column", "adj_c_mom", "adj_c_mass", "adj_halo"};
+constexpr int NSTAGE = 24;
 enum { S_CMASS, S_CCOL, S_CMOM, S_CHALO, S_DRING, S_DMASS, S_DCOL, S_DCORN, S_DMOM, S_RRING, S_RWIND, S_RENER,
-       S_DHALO, S_HEAT, S_CHECK };
+       S_DHALO, S_HEAT, S_CHECK, S_AFWD, S_ARMP, S_ADMOM, S_ADCOL, S_ADMASS, S_ACCOL, S_ACMOM, S_ACMASS, S_AHALO };
 
 // Brackets one stage (one kernel launch unless noted) with CUDA events on
 // the context's stream when profiling is on, and counts the launch.
@@ -702,6 +718,340 @@ int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_o
     rc = ATM_ERR_CUDA;
   cudaFree(dx); cudaFree(dp); cudaFree(dl);
   return rc;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- adjoint ----
+namespace {
+
+int require_adj(atm_ctx* c) {
+  int r = require_init(c);
+  if (r) return r;
+  if (!c->adj) return fail(c, ATM_ERR_STATE, "atm_adj_enable has not been called");
+  if (c->heating) return fail(c, ATM_ERR_UNSUPPORTED, "the adjoint holds the heating term at zero: clear net_flux");
+  return ATM_OK;
+}
+
+double** slot_fields(atm_ctx* c, int slot) { return c->lam[slot == ATM_ADJ_IN ? c->slot_in : 1 - c->slot_in]; }
+
+cudaError_t zero_fields(atm_ctx* c, double* const* f, int n, int K) {
+  for (int i = 0; i < n; ++i) {
+    cudaError_t e = cudaMemsetAsync(f[i], 0, (size_t)c->geo.S * K * 8, c->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// forward C step from the state s into cg, pkap, gz (no halo)
+int fwd_c(atm_ctx* ctx, double dt_half, void* const* s) {
+  const atm::Ops& ops = *ctx->ops;
+  const Geom& g = ctx->geo;
+  atm::Consts k = step_consts(ctx, dt_half);
+  CK(ops.mass(g, k, s[F_DP], s[F_PT], s[F_UD], s[F_VD], nullptr, ctx->cg[C_DPC], ctx->cg[C_PTC], -2, 2, nullptr,
+              &ctx->status->tma_timeout, true, ctx->stream));
+  CK(ops.column(g, k, ctx->cg[C_DPC], ctx->cg[C_PTC], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+  CK(ops.c_mom(g, k, s[F_UD], s[F_VD], ctx->pkap, ctx->gz, ctx->cg[C_UC], ctx->cg[C_VC], &ctx->status->tma_timeout,
+               ctx->stream));
+  ctx->launches += 3;
+  return ATM_OK;
+}
+
+// forward D step from so (and cg) into sn, without advancing the state
+int fwd_d(atm_ctx* ctx, double dt, void* const* so, void* const* sn) {
+  const atm::Ops& ops = *ctx->ops;
+  const Geom& g = ctx->geo;
+  atm::Consts k = step_consts(ctx, dt);
+  CK(ops.ring(g, sn, (const void* const*)so, 4, ctx->L, true, ctx->stream));
+  CK(ops.mass(g, k, so[F_DP], so[F_PT], ctx->cg[C_UC], ctx->cg[C_VC], nullptr, sn[F_DP], sn[F_PT], -3, 3,
+              &ctx->status->nonfinite_step, &ctx->status->tma_timeout, false, ctx->stream));
+  CK(ops.column(g, k, sn[F_DP], sn[F_PT], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+  CK(atm::corners(g, ctx->pkap, ctx->gz, ctx->pkapb, ctx->gzb, 1, 0, ctx->L, ctx->stream));
+  CK(ops.d_mom(g, k, so[F_UD], so[F_VD], ctx->cg[C_UC], ctx->cg[C_VC], ctx->pkapb, ctx->gzb, sn[F_UD], sn[F_VD],
+               &ctx->status->nonfinite_step, &ctx->status->tma_timeout, ctx->stream));
+  ctx->launches += 5;
+  return ATM_OK;
+}
+
+// lin += (C step)^T lam_cg at the state s; cg must hold the step's dpc, ptc
+int adj_c(atm_ctx* ctx, double dt_half, void* const* s, double* const* lin) {
+  const Geom& g = ctx->geo;
+  atm::Consts k = step_consts(ctx, dt_half);
+  const double* const* sd = (const double* const*)s;
+  double* const* cg = (double* const*)ctx->cg;
+  {
+    Stage t(ctx, S_ACCOL, 2);
+    CK(ctx->ops->column(g, k, cg[C_DPC], cg[C_PTC], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+    CK(cudaMemsetAsync(ctx->lam_pk, 0, (size_t)g.S * (ctx->L + 1) * 8, ctx->stream));
+    CK(cudaMemsetAsync(ctx->lam_gz, 0, (size_t)g.S * (ctx->L + 1) * 8, ctx->stream));
+  }
+  {
+    Stage t(ctx, S_ACMOM);
+    CK(atm::adj_c_mom(g, k, sd[F_UD], sd[F_VD], ctx->pkap, ctx->gz, ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], lin[F_UD],
+                      lin[F_VD], ctx->lam_pk, ctx->lam_gz, &ctx->status->tma_timeout, ctx->stream));
+  }
+  {
+    Stage t(ctx, S_ACCOL);
+    CK(atm::adj_column(g, k, cg[C_DPC], cg[C_PTC], ctx->lam_pk, ctx->lam_gz, ctx->lam_cg[C_DPC], ctx->lam_cg[C_PTC], -2,
+                       2, ctx->stream));
+  }
+  {
+    Stage t(ctx, S_ACMASS);
+    CK(atm::adj_mass(g, k, sd[F_DP], sd[F_PT], sd[F_UD], sd[F_VD], ctx->lam_cg[C_DPC], ctx->lam_cg[C_PTC], lin[F_DP],
+                     lin[F_PT], lin[F_UD], lin[F_VD], -2, 2, &ctx->status->tma_timeout, true, ctx->stream));
+  }
+  return ATM_OK;
+}
+
+// lin, lam_cg += (D step)^T lout at so (with cg) -> sn; lout is consumed
+int adj_d(atm_ctx* ctx, double dt, void* const* so, void* const* sn, double* const* lout, double* const* lin) {
+  const Geom& g = ctx->geo;
+  atm::Consts k = step_consts(ctx, dt);
+  const double* const* o = (const double* const*)so;
+  const double* const* n = (const double* const*)sn;
+  const double* const* cg = (const double* const*)ctx->cg;
+  const size_t lev = (size_t)g.S * (ctx->L + 1) * 8;
+  CK(cudaMemsetAsync(ctx->lam_pk, 0, lev, ctx->stream));
+  CK(cudaMemsetAsync(ctx->lam_gz, 0, lev, ctx->stream));
+  CK(cudaMemsetAsync(ctx->lam_pkb, 0, lev, ctx->stream));
+  CK(cudaMemsetAsync(ctx->lam_gzb, 0, lev, ctx->stream));
+  {
+    Stage t(ctx, S_ADMOM);
+    CK(atm::adj_d_mom(g, k, o[F_UD], o[F_VD], cg[C_UC], cg[C_VC], ctx->pkapb, ctx->gzb, lout[F_UD], lout[F_VD],
+                      lin[F_UD], lin[F_VD], ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], ctx->lam_pkb, ctx->lam_gzb,
+                      &ctx->status->tma_timeout, ctx->stream));
+  }
+  {
+    Stage t(ctx, S_ADCOL, 2);
+    CK(atm::adj_corners(g, ctx->lam_pkb, ctx->lam_gzb, ctx->lam_pk, ctx->lam_gz, ctx->stream));
+    CK(atm::adj_column(g, k, n[F_DP], n[F_PT], ctx->lam_pk, ctx->lam_gz, lout[F_DP], lout[F_PT], -2, 2, ctx->stream));
+  }
+  {
+    Stage t(ctx, S_ADMASS);
+    CK(atm::adj_mass(g, k, o[F_DP], o[F_PT], cg[C_UC], cg[C_VC], lout[F_DP], lout[F_PT], lin[F_DP], lin[F_PT],
+                     ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], -3, 3, &ctx->status->tma_timeout, false, ctx->stream));
+  }
+  {
+    Stage t(ctx, S_AHALO);
+    CK(atm::adj_ring_copy(g, lout, lin, ctx->L, 3, 0, ctx->stream));
+  }
+  return ATM_OK;
+}
+
+// lin += (remap)^T lout at the pre-remap state s1
+int adj_r(atm_ctx* ctx, void* const* s1, double* const* lout, double* const* lin) {
+  const Geom& g = ctx->geo;
+  const double* const* s = (const double* const*)s1;
+  atm::RemapArgs ra = remap_args(ctx);
+  Stage t(ctx, S_ARMP, 4);
+  CK(ctx->ops->remap_winds(g, ra, s1[F_DP], s1[F_UD], s1[F_VD], ctx->urem, ctx->vrem, nullptr, ctx->status,
+                           ctx->stream));
+  CK(cudaMemsetAsync(ctx->lam_ur, 0, (size_t)g.S * ctx->L * 8, ctx->stream));
+  CK(cudaMemsetAsync(ctx->lam_vr, 0, (size_t)g.S * ctx->L * 8, ctx->stream));
+  CK(atm::adj_remap_energy(g, ra, s[F_DP], s[F_PT], s[F_UD], s[F_VD], (const double*)ctx->urem,
+                           (const double*)ctx->vrem, ctx->gz, lout[F_DP], lout[F_PT], lout[F_UD], lout[F_VD], lin[F_DP],
+                           lin[F_PT], lin[F_UD], lin[F_VD], ctx->lam_ur, ctx->lam_vr, ctx->stream));
+  CK(atm::adj_remap_winds(g, ra, s[F_DP], s[F_UD], s[F_VD], ctx->lam_ur, ctx->lam_vr, lin[F_DP], lin[F_UD], lin[F_VD],
+                          ctx->stream));
+  // the remapped fields keep the pre-remap ring
+  CK(atm::adj_ring_copy(g, lout, lin, ctx->L, 0, 0, ctx->stream));
+  return ATM_OK;
+}
+
+double* adj_field(atm_ctx* c, int slot, int field) {
+  if (field >= ATM_DP && field <= ATM_VD) {
+    if (slot != ATM_ADJ_IN && slot != ATM_ADJ_OUT) return nullptr;
+    return slot_fields(c, slot)[field];
+  }
+  if (field >= ATM_DPC && field <= ATM_VC) return c->lam_cg[field - ATM_DPC];
+  return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int atm_adj_enable(atm_ctx* ctx) {
+  if (!ctx) return ATM_ERR_ARG;
+  if (ctx->precision != ATM_FP64) return fail(ctx, ATM_ERR_UNSUPPORTED, "the adjoint is defined for the FP64 form");
+  if (ctx->adj) return atm_adj_zero(ctx);
+  cudaError_t e = atm::adj_setup();
+  if (e != cudaSuccess) return cuda_fail(ctx, "adjoint kernel set-up", e);
+  const size_t lay = (size_t)ctx->geo.S * ctx->L * 8, lev = (size_t)ctx->geo.S * (ctx->L + 1) * 8;
+  bool ok = true;
+  auto alloc = [&](double** p, size_t bytes) {
+    if (ok && cudaMalloc((void**)p, bytes) != cudaSuccess) ok = false;
+  };
+  for (int t = 0; t < 2; ++t)
+    for (int f = 0; f < 4; ++f) alloc(&ctx->lam[t][f], lay);
+  for (int f = 0; f < 4; ++f) alloc(&ctx->lam_cg[f], lay);
+  alloc(&ctx->lam_pk, lev);
+  alloc(&ctx->lam_gz, lev);
+  alloc(&ctx->lam_pkb, lev);
+  alloc(&ctx->lam_gzb, lev);
+  alloc(&ctx->lam_ur, lay);
+  alloc(&ctx->lam_vr, lay);
+  if (!ok) {
+    cudaGetLastError();
+    return fail(ctx, ATM_ERR_NOMEM, "adjoint fields do not fit on the device");
+  }
+  ctx->adj = true;
+  return atm_adj_zero(ctx);
+}
+
+int atm_adj_zero(atm_ctx* ctx) {
+  if (!ctx) return ATM_ERR_ARG;
+  if (!ctx->adj) return fail(ctx, ATM_ERR_STATE, "atm_adj_enable has not been called");
+  CK(zero_fields(ctx, ctx->lam[0], 4, ctx->L));
+  CK(zero_fields(ctx, ctx->lam[1], 4, ctx->L));
+  CK(zero_fields(ctx, ctx->lam_cg, 4, ctx->L));
+  ctx->slot_in = 0;
+  return ATM_OK;
+}
+
+int atm_adj_set(atm_ctx* ctx, int slot, int field, const double* host) {
+  if (!ctx || !host) return ATM_ERR_ARG;
+  if (!ctx->adj) return fail(ctx, ATM_ERR_STATE, "atm_adj_enable has not been called");
+  double* f = adj_field(ctx, slot, field);
+  if (!f) return fail(ctx, ATM_ERR_ARG, "no such adjoint field");
+  CK(h2d_pitched(ctx, f, host, ctx->L));
+  return ATM_OK;
+}
+
+int atm_adj_get(atm_ctx* ctx, int slot, int field, double* host) {
+  if (!ctx || !host) return ATM_ERR_ARG;
+  if (!ctx->adj) return fail(ctx, ATM_ERR_STATE, "atm_adj_enable has not been called");
+  double* f = adj_field(ctx, slot, field);
+  if (!f) return fail(ctx, ATM_ERR_ARG, "no such adjoint field");
+  CK(d2h_pitched(ctx, host, f, ctx->L));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATM_OK;
+}
+
+int atm_adj_set_device(atm_ctx* ctx, int slot, int field, const double* dev) {
+  if (!ctx || !dev) return ATM_ERR_ARG;
+  if (!ctx->adj) return fail(ctx, ATM_ERR_STATE, "atm_adj_enable has not been called");
+  double* f = adj_field(ctx, slot, field);
+  if (!f) return fail(ctx, ATM_ERR_ARG, "no such adjoint field");
+  CK(cudaMemsetAsync(f, 0, (size_t)ctx->geo.S * ctx->L * 8, ctx->stream));
+  k_interior<double, double><<<1184, 256, 0, ctx->stream>>>(ctx->geo, dev, f, ctx->L, 1);
+  CK(cudaGetLastError());
+  return ATM_OK;
+}
+
+int atm_adj_get_device(atm_ctx* ctx, int slot, int field, double* dev) {
+  if (!ctx || !dev) return ATM_ERR_ARG;
+  if (!ctx->adj) return fail(ctx, ATM_ERR_STATE, "atm_adj_enable has not been called");
+  double* f = adj_field(ctx, slot, field);
+  if (!f) return fail(ctx, ATM_ERR_ARG, "no such adjoint field");
+  k_interior<double, double><<<1184, 256, 0, ctx->stream>>>(ctx->geo, f, dev, ctx->L, 0);
+  CK(cudaGetLastError());
+  return ATM_OK;
+}
+
+int atm_adj_halo(atm_ctx* ctx, int slot) {
+  int r = require_adj(ctx);
+  if (r) return r;
+  if (slot != ATM_ADJ_IN && slot != ATM_ADJ_OUT) return fail(ctx, ATM_ERR_ARG, "no such adjoint slot");
+  Stage t(ctx, S_AHALO);
+  CK(atm::adj_ring_fold(ctx->geo, slot_fields(ctx, slot), 4, ctx->L, ctx->stream));
+  return ATM_OK;
+}
+
+int atm_adj_cgrid_halo(atm_ctx* ctx) {
+  int r = require_adj(ctx);
+  if (r) return r;
+  Stage t(ctx, S_AHALO);
+  CK(atm::adj_ring_fold(ctx->geo, ctx->lam_cg, 4, ctx->L, ctx->stream));
+  return ATM_OK;
+}
+
+int atm_adj_cgrid_step(atm_ctx* ctx, double dt_half) {
+  int r = require_adj(ctx);
+  if (r) return r;
+  void* const* s = ctx->st[ctx->cur];
+  {
+    Stage t(ctx, S_AFWD, 0);
+    if ((r = fwd_c(ctx, dt_half, s))) return r;
+  }
+  return adj_c(ctx, dt_half, s, slot_fields(ctx, ATM_ADJ_IN));
+}
+
+int atm_adj_dgrid_step(atm_ctx* ctx, double dt) {
+  int r = require_adj(ctx);
+  if (r) return r;
+  const int cur = ctx->cur;
+  {
+    Stage t(ctx, S_AFWD, 1);
+    if ((r = fwd_c(ctx, dt / 2., ctx->st[cur]))) return r;
+    CK(ctx->ops->ring(ctx->geo, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
+    if ((r = fwd_d(ctx, dt, ctx->st[cur], ctx->st[1 - cur]))) return r;
+  }
+  return adj_d(ctx, dt, ctx->st[cur], ctx->st[1 - cur], slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN));
+}
+
+int atm_adj_remap(atm_ctx* ctx) {
+  int r = require_adj(ctx);
+  if (r) return r;
+  return adj_r(ctx, ctx->st[ctx->cur], slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN));
+}
+
+int atm_adj_step(atm_ctx* ctx, double dt, int do_remap) {
+  int r = require_adj(ctx);
+  if (r) return r;
+  const Geom& g = ctx->geo;
+  const int cur = ctx->cur, nxt = 1 - ctx->cur;
+  // dgrid_halo_exchange
+  {
+    Stage t(ctx, S_AHALO);
+    CK(atm::adj_ring_fold(g, slot_fields(ctx, ATM_ADJ_OUT), 4, ctx->L, ctx->stream));
+  }
+  // the forward step from the current state, kept in the other time level
+  {
+    Stage t(ctx, S_AFWD, 1);
+    if ((r = fwd_c(ctx, dt / 2., ctx->st[cur]))) return r;
+    CK(ctx->ops->ring(g, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
+    if ((r = fwd_d(ctx, dt, ctx->st[cur], ctx->st[nxt]))) return r;
+  }
+  if (do_remap) {
+    CK(zero_fields(ctx, slot_fields(ctx, ATM_ADJ_IN), 4, ctx->L));
+    if ((r = adj_r(ctx, ctx->st[nxt], slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN)))) return r;
+    ctx->slot_in = 1 - ctx->slot_in;
+  }
+  CK(zero_fields(ctx, slot_fields(ctx, ATM_ADJ_IN), 4, ctx->L));
+  CK(zero_fields(ctx, ctx->lam_cg, 4, ctx->L));
+  if ((r = adj_d(ctx, dt, ctx->st[cur], ctx->st[nxt], slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN))))
+    return r;
+  {
+    Stage t(ctx, S_AHALO);
+    CK(atm::adj_ring_fold(g, ctx->lam_cg, 4, ctx->L, ctx->stream));
+  }
+  if ((r = adj_c(ctx, dt / 2., ctx->st[cur], slot_fields(ctx, ATM_ADJ_IN)))) return r;
+  ctx->slot_in = 1 - ctx->slot_in;
+  return ATM_OK;
+}
+
+int atm_state_bytes(atm_ctx* ctx, long long* bytes) {
+  if (!ctx || !bytes) return ATM_ERR_ARG;
+  *bytes = 4LL * ctx->L * ctx->geo.S * ctx->ops->elem;
+  return ATM_OK;
+}
+
+int atm_state_save(atm_ctx* ctx, void* dev) {
+  if (!ctx || !dev) return ATM_ERR_ARG;
+  const size_t f = (size_t)ctx->L * ctx->geo.S * ctx->ops->elem;
+  for (int i = 0; i < 4; ++i)
+    CK(cudaMemcpyAsync((char*)dev + i * f, ctx->st[ctx->cur][i], f, cudaMemcpyDeviceToDevice, ctx->stream));
+  return ATM_OK;
+}
+
+int atm_state_load(atm_ctx* ctx, const void* dev) {
+  if (!ctx || !dev) return ATM_ERR_ARG;
+  const size_t f = (size_t)ctx->L * ctx->geo.S * ctx->ops->elem;
+  for (int i = 0; i < 4; ++i)
+    CK(cudaMemcpyAsync(ctx->st[ctx->cur][i], (const char*)dev + i * f, f, cudaMemcpyDeviceToDevice, ctx->stream));
+  ctx->flag_valid = false;
+  return ATM_OK;
 }
 
 }  // extern "C"

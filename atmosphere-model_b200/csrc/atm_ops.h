@@ -53,6 +53,35 @@ cudaError_t device_pow_log(const double* x, double y, double* p, double* l, int 
 // count of arguments where div_const<3>/<12> differs from IEEE division (tests)
 cudaError_t device_div_check(unsigned long long n, unsigned long long seed, unsigned long long* bad, cudaStream_t);
 
+// ---- FP64 adjoint (atm_adjoint.cu); lam_* are adjoint fields laid out like
+// the fields they belong to, accumulated with +=
+cudaError_t adj_setup();
+cudaError_t adj_mass(const Geom&, const Consts&, const double* dp, const double* pt, const double* u, const double* v,
+                     const double* lam_dpo, const double* lam_pto, double* lam_dp, double* lam_pt, double* lam_u,
+                     double* lam_v, int lo, int hi, int* timeout, bool cgrid, cudaStream_t);
+cudaError_t adj_c_mom(const Geom&, const Consts&, const double* ud, const double* vd, const double* pkap,
+                      const double* gz, const double* lam_uc, const double* lam_vc, double* lam_ud, double* lam_vd,
+                      double* lam_pk, double* lam_gz, int* timeout, cudaStream_t);
+cudaError_t adj_d_mom(const Geom&, const Consts&, const double* ud, const double* vd, const double* uc,
+                      const double* vc, const double* pkapb, const double* gzb, const double* lam_udo,
+                      const double* lam_vdo, double* lam_ud, double* lam_vd, double* lam_uc, double* lam_vc,
+                      double* lam_pkb, double* lam_gzb, int* timeout, cudaStream_t);
+cudaError_t adj_column(const Geom&, const Consts&, const double* dp, const double* pt, const double* lam_pk,
+                       const double* lam_gz, double* lam_dp, double* lam_pt, int lo, int hi, cudaStream_t);
+cudaError_t adj_corners(const Geom&, const double* lam_pkb, const double* lam_gzb, double* lam_pk, double* lam_gz,
+                        cudaStream_t);
+cudaError_t adj_ring_fold(const Geom&, double* const* f, int nf, int K, cudaStream_t);
+cudaError_t adj_ring_copy(const Geom&, double* const* dst, double* const* src, int K, int band01, int band23,
+                          cudaStream_t);
+cudaError_t adj_remap_energy(const Geom&, const RemapArgs&, const double* dp, const double* pt, const double* ud,
+                             const double* vd, const double* urem, const double* vrem, const double* gzs,
+                             const double* lam_dpo, const double* lam_pto, const double* lam_udo,
+                             const double* lam_vdo, double* lam_dp, double* lam_pt, double* lam_ud, double* lam_vd,
+                             double* lam_ur, double* lam_vr, cudaStream_t);
+cudaError_t adj_remap_winds(const Geom&, const RemapArgs&, const double* dp, const double* ud, const double* vd,
+                            const double* lam_ur, const double* lam_vr, double* lam_dp, double* lam_ud, double* lam_vd,
+                            cudaStream_t);
+
 // largest number of layers the vertical remap supports
 constexpr int MAX_LAYERS = 128;
 

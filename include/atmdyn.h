@@ -202,6 +202,50 @@ int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, const double* 
    constants 3 and 12 differs from IEEE division (expected: 0) */
 int atm_device_div_check(long long n, long long seed, long long* mismatches);
 
+/* ---- adjoint of the FP64 step (the gradient work; no reference counterpart) ----
+   Hand-written reverse mode of cgrid_dynamics_step, dgrid_dynamics_step
+   (src/mod_sw_dyn.f90:80-773), perform_vertical_remapping
+   (src/mod_remap.f90:27-356) and the halo exchanges (src/mod_sync.f90:67-217)
+   with every limiter, upwind and remap-overlap branch frozen at the forward
+   trajectory (the forward is recomputed bit for bit inside the adjoint).
+   Adjoints are FP64 fields shaped like the state, in two slots:
+   ATM_ADJ_OUT holds the adjoint of the state after a step and
+   ATM_ADJ_IN receives the adjoint of the state before it.  FP64 contexts
+   only, with the heating term off (net_flux unset). */
+enum { ATM_ADJ_IN = 0, ATM_ADJ_OUT = 1 };
+/* allocate (or clear) the adjoint fields */
+int atm_adj_enable(atm_ctx* ctx);
+int atm_adj_zero(atm_ctx* ctx);
+/* adjoint field of a slot (ATM_DP..ATM_VD) or a C-grid adjoint
+   (ATM_DPC..ATM_VC, slot ignored) from / to a host (is:ie, js:je, 1:nlay)
+   array, halo included */
+int atm_adj_set(atm_ctx* ctx, int slot, int field, const double* host);
+int atm_adj_get(atm_ctx* ctx, int slot, int field, double* host);
+/* the same for device (nlay, ny, nx) interiors; set clears the halo */
+int atm_adj_set_device(atm_ctx* ctx, int slot, int field, const double* dev);
+int atm_adj_get_device(atm_ctx* ctx, int slot, int field, double* dev);
+/* one step reversed: on entry slot OUT is the adjoint of the state after
+   atm_step(ctx, dt, do_remap) taken from the context's current state; on
+   return slot OUT is the adjoint of the current state (its halo still
+   holds the ring's share: atm_adj_halo folds it).  The state is not
+   advanced; the other time level and the C-grid fields are overwritten. */
+int atm_adj_step(atm_ctx* ctx, double dt, int do_remap);
+/* adjoint of a periodic halo fill: each ring adjoint added to its interior
+   image and cleared (slot ATM_ADJ_IN or ATM_ADJ_OUT; C-grid adjoints) */
+int atm_adj_halo(atm_ctx* ctx, int slot);
+int atm_adj_cgrid_halo(atm_ctx* ctx);
+/* single stages at the current state: slot IN += C^T (C-grid adjoints);
+   slot IN, C-grid += D^T slot OUT (after the call's own C step and halo;
+   slot OUT is consumed); slot IN += R^T slot OUT */
+int atm_adj_cgrid_step(atm_ctx* ctx, double dt_half);
+int atm_adj_dgrid_step(atm_ctx* ctx, double dt);
+int atm_adj_remap(atm_ctx* ctx);
+/* checkpoints: the whole prognostic state (both halos) to / from a device
+   buffer of atm_state_bytes bytes */
+int atm_state_bytes(atm_ctx* ctx, long long* bytes);
+int atm_state_save(atm_ctx* ctx, void* dev);
+int atm_state_load(atm_ctx* ctx, const void* dev);
+
 /* library version string */
 const char* atm_version(void);
 
