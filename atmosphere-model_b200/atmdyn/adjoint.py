@@ -1,0 +1,125 @@
+"""PyTorch binding of the FP64 step and its hand-written adjoint.
+
+:class:`DycoreSegment` is a ``torch.autograd.Function`` that advances the
+prognostic interior (dp, pt, ud, vd as float64 CUDA tensors of shape
+(nlay, ny, nx)) through a segment of steps with libatmdyn.  Its forward
+keeps only the segment's initial state (a checkpoint).  Its backward
+restores that state, recomputes the segment once keeping each step's
+initial state, and then runs the adjoint steps in reverse order
+(``atm_adj_step``: the CUDA adjoint kernels of the sweeps, the remap and the
+halo fills, with the limiter branches of the recomputed forward).
+:func:`integrate` chains segments of ``checkpoint_every`` steps, so memory
+grows with the number of checkpoints plus one segment of states.
+
+The step is the reference's time loop (src/mod_model.f90:146-177): C-grid
+half step, C-grid halo, D-grid step, vertical remap every ``remap_every``
+steps, D-grid halo.  The heating term is held at zero.
+"""
+from __future__ import annotations
+
+import torch
+
+from .dycore import Dycore
+
+FIELD_NAMES = ('dp', 'pt', 'ud', 'vd')
+
+
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the handle of the legacy default stream
+
+
+def _bind_stream(dyn: Dycore):
+    """Enqueue the library's work on torch's current stream.  torch reports
+    the legacy default stream as handle 0, which atm_set_stream reads as
+    'use your own stream', so that case passes cudaStreamLegacy."""
+    h = torch.cuda.current_stream().cuda_stream
+    dyn.set_stream(h if h else CUDA_STREAM_LEGACY)
+
+
+def _upload(dyn: Dycore, fields):
+    from ._lib import ATM_DP, ATM_PT, ATM_UD, ATM_VD
+    for f, t in zip((ATM_DP, ATM_PT, ATM_UD, ATM_VD), fields):
+        t = t.detach().contiguous()
+        assert t.dtype == torch.float64 and t.is_cuda
+        dyn.upload_device(f, t)
+
+
+def _download(dyn: Dycore, like):
+    from ._lib import ATM_DP, ATM_PT, ATM_UD, ATM_VD
+    outs = []
+    for f in (ATM_DP, ATM_PT, ATM_UD, ATM_VD):
+        o = torch.empty_like(like)
+        dyn.download_device(f, o)
+        outs.append(o)
+    return outs
+
+
+class DycoreSegment(torch.autograd.Function):
+    """(dp, pt, ud, vd) -> the state after ``len(remaps)`` steps of size dt;
+    remaps[i] says whether step i ends with the vertical remap."""
+
+    @staticmethod
+    def forward(ctx, dyn: Dycore, dt: float, remaps, dp, pt, ud, vd):
+        _bind_stream(dyn)
+        _upload(dyn, (dp, pt, ud, vd))
+        ckpt = torch.empty(dyn.state_bytes() // 8, dtype=torch.float64, device=dp.device)
+        dyn.state_save(ckpt.data_ptr())
+        for r in remaps:
+            dyn.step(dt, remap=bool(r), check_stable=False)
+        outs = _download(dyn, dp)
+        ctx.dyn, ctx.dt, ctx.remaps = dyn, dt, tuple(bool(r) for r in remaps)
+        ctx.save_for_backward(ckpt)
+        ctx.mark_non_differentiable()
+        return tuple(outs)
+
+    @staticmethod
+    def backward(ctx, gdp, gpt, gud, gvd):
+        dyn, dt, remaps = ctx.dyn, ctx.dt, ctx.remaps
+        (ckpt,) = ctx.saved_tensors
+        _bind_stream(dyn)
+        dyn.state_load(ckpt.data_ptr())
+        # recompute the segment, keeping the initial state of every step
+        states = []
+        for r in remaps:
+            s = torch.empty_like(ckpt)
+            dyn.state_save(s.data_ptr())
+            states.append(s)
+            dyn.step(dt, remap=r, check_stable=False)
+        dyn.adj_zero()
+        grads = [g if g is not None else torch.zeros_like(ckpt[:0]) for g in (gdp, gpt, gud, gvd)]
+        for name, g in zip(FIELD_NAMES, grads):
+            if g.numel():
+                dyn.adj_set_device('out', name, g.detach().contiguous().data_ptr())
+        for s, r in zip(reversed(states), reversed(remaps)):
+            dyn.state_load(s.data_ptr())
+            dyn.adj_step(dt, remap=r)
+        dyn.adj_halo('out')  # the initial state's halo is the periodic image of its interior
+        like = gdp if gdp is not None else (gpt if gpt is not None else (gud if gud is not None else gvd))
+        outs = []
+        for name in FIELD_NAMES:
+            o = torch.empty_like(like)
+            dyn.adj_get_device('out', name, o.data_ptr())
+            outs.append(o)
+        return (None, None, None, *outs)
+
+
+def integrate(dyn: Dycore, fields, nsteps: int, dt: float, remap_every: int, checkpoint_every: int,
+              first_step: int = 0):
+    """Advance (dp, pt, ud, vd) by nsteps with checkpoints every
+    ``checkpoint_every`` steps; differentiable with respect to the inputs."""
+    out = tuple(fields)
+    s = first_step
+    end = first_step + nsteps
+    while s < end:
+        n = min(checkpoint_every, end - s)
+        remaps = [(q + 1) % remap_every == 0 for q in range(s, s + n)]
+        out = DycoreSegment.apply(dyn, dt, remaps, *out)
+        s += n
+    return out
+
+
+def gaussian_mask(st, radius: float, device=None):
+    """exp(-(r / radius)^2) around the domain centre on the cell centres."""
+    x = (torch.arange(st.nx, dtype=torch.float64, device=device) + 0.5) * st.dx
+    y = (torch.arange(st.ny, dtype=torch.float64, device=device) + 0.5) * st.dy
+    r2 = (x[None, :] - st.nx * st.dx / 2) ** 2 + (y[:, None] - st.ny * st.dy / 2) ** 2
+    return torch.exp(-r2 / radius ** 2)

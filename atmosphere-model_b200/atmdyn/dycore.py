@@ -176,6 +176,23 @@ class Dycore:
     def state(self):
         return {name: self.get(f) for name, f in (('dp', ATM_DP), ('pt', ATM_PT), ('ud', ATM_UD), ('vd', ATM_VD))}
 
+    # device-resident access (torch tensors or raw device pointers)
+    def upload_device(self, field, t, dtype_bytes=None):
+        """Interior (nlay, ny, nx) from a contiguous device buffer; the halo
+        becomes the periodic image of the interior."""
+        if isinstance(field, str):
+            field = FIELDS[field]
+        ptr = t if isinstance(t, int) else t.data_ptr()
+        nb = dtype_bytes or (8 if isinstance(t, int) else t.element_size())
+        check(self.lib.atm_upload_device(self.ctx, field, ctypes.c_void_p(ptr), nb), self.ctx, 'atm_upload_device')
+
+    def download_device(self, field, t, dtype_bytes=None):
+        if isinstance(field, str):
+            field = FIELDS[field]
+        ptr = t if isinstance(t, int) else t.data_ptr()
+        nb = dtype_bytes or (8 if isinstance(t, int) else t.element_size())
+        check(self.lib.atm_download_device(self.ctx, field, ctypes.c_void_p(ptr), nb), self.ctx, 'atm_download_device')
+
     # ---- adjoint (FP64 form): hand-written reverse mode of the step
     def adj_enable(self):
         check(self.lib.atm_adj_enable(self.ctx), self.ctx, 'atm_adj_enable')

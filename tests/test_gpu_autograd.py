@@ -1,0 +1,95 @@
+"""The checkpointed torch.autograd.Function over the FP64 step.
+
+* dot-product test of 20 steps (remap every 5, checkpoints every 5)
+  against the oracle's tangent-linear model, to 1e-12;
+* gradient of J = sum(mask * theta^2) at the final step against central
+  finite differences of the GPU forward (eps = 1e-6 along random unit
+  directions) on a state without limiter ties.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip('torch')
+
+from atmdyn import ic, Dycore
+from atmdyn.adjoint import integrate, gaussian_mask
+import pyoracle
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ('dp', 'pt', 'ud', 'vd')
+STATE = {'dp': pyoracle.DP, 'pt': pyoracle.PT, 'ud': pyoracle.UD, 'vd': pyoracle.VD}
+SCALE = {'dp': 10.0, 'pt': 0.01, 'ud': 0.5, 'vd': 0.5}
+P0K = 1.0e5 ** ic.KAPPA  # theta = pt * p0**kappa
+
+
+def small_jet(seed=2, noisy=False):
+    st = ic.jet_case(48, 40, 12, 25e3, 25e3, width=200e3, seed=seed)
+    st.dt = 30.0
+    if noisy:  # no exact ties anywhere (uniform dp, x-independent winds)
+        rng = np.random.default_rng(seed + 100)
+        st.dp = st.dp + rng.normal(0, 5.0, st.dp.shape)
+        st.u = st.u + rng.normal(0, 0.5, st.u.shape)
+        st.v = st.v + rng.normal(0, 0.5, st.v.shape)
+    return st
+
+
+def tensors(st):
+    return [torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device='cuda', requires_grad=True)
+            for a in (st.dp, st.pt, st.u, st.v)]
+
+
+def test_twenty_steps_dot_product():
+    st = small_jet()
+    nsteps, remap_every, ckpt = 20, 5, 5
+    rng = np.random.default_rng(11)
+    v = {n: rng.normal(0, SCALE[n], (st.nlay, st.ny, st.nx)) for n in NAMES}
+    w = {n: rng.normal(0, SCALE[n], (st.nlay, st.ny, st.nx)) for n in NAMES}
+    t = pyoracle.TLMModel(st, v, threads=8)
+    for s in range(nsteps):
+        t.cgrid_step(st.dt / 2)
+        t.cgrid_halo()
+        t.dgrid_step(st.dt)
+        if (s + 1) % remap_every == 0:
+            t.remap()
+        t.dgrid_halo()
+    lhs = sum(np.sum(w[n] * t.get(STATE[n])[1]) for n in NAMES)
+    dyn = Dycore(st)
+    dyn.adj_enable()
+    x = tensors(st)
+    y = integrate(dyn, x, nsteps, st.dt, remap_every, ckpt)
+    J = sum((torch.tensor(w[n], device='cuda') * yy).sum() for n, yy in zip(NAMES, y))
+    J.backward()
+    rhs = sum(np.sum(v[n] * xx.grad.cpu().numpy()) for n, xx in zip(NAMES, x))
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs)), (lhs, rhs)
+
+
+def test_gradient_matches_central_differences():
+    st = small_jet(noisy=True)
+    nsteps, remap_every, ckpt = 10, 5, 5
+    dyn = Dycore(st)
+    dyn.adj_enable()
+    mask = gaussian_mask(st, 300e3, device='cuda')
+
+    def loss(fields):
+        out = integrate(dyn, fields, nsteps, st.dt, remap_every, ckpt)
+        return (mask * (out[1] * P0K) ** 2).sum()
+
+    x = tensors(st)
+    J = loss(x)
+    J.backward()
+    grad = torch.cat([xx.grad.flatten() for xx in x])
+    gen = torch.Generator(device='cpu').manual_seed(5)
+    worst = 0.
+    for _ in range(4):
+        d = torch.randn(grad.numel(), generator=gen, dtype=torch.float64).cuda()
+        d /= d.norm()
+        eps = 1e-6
+        parts = torch.split(d, [xx.numel() for xx in x])
+        with torch.no_grad():
+            xp = [(xx + eps * p.view_as(xx)).detach() for xx, p in zip(x, parts)]
+            xm = [(xx - eps * p.view_as(xx)).detach() for xx, p in zip(x, parts)]
+            fd = (loss(xp) - loss(xm)).item() / (2 * eps)
+        ad = torch.dot(grad, d).item()
+        worst = max(worst, abs(fd - ad) / abs(ad))
+    assert worst <= 1e-4, worst
