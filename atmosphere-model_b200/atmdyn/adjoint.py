@@ -5,9 +5,10 @@ prognostic interior (dp, pt, ud, vd as float64 CUDA tensors of shape
 (nlay, ny, nx)) through a segment of steps with libatmdyn.  Its forward
 keeps only the segment's initial state (a checkpoint).  Its backward
 restores that state, recomputes the segment once keeping each step's
-initial state, and then runs the adjoint steps in reverse order
-(``atm_adj_step``: the CUDA adjoint kernels of the sweeps, the remap and the
-halo fills, with the limiter branches of the recomputed forward).
+initial state and forward products (``atm_step_tape``), and then runs the
+adjoint steps in reverse order (``atm_adj_step_tape``: the CUDA adjoint
+kernels of the sweeps, the remap and the halo fills, with the limiter
+branches of the recomputed forward).
 :func:`integrate` chains segments of ``checkpoint_every`` steps, so memory
 grows with the number of checkpoints plus one segment of states.
 
@@ -77,21 +78,24 @@ class DycoreSegment(torch.autograd.Function):
         (ckpt,) = ctx.saved_tensors
         _bind_stream(dyn)
         dyn.state_load(ckpt.data_ptr())
-        # recompute the segment, keeping the initial state of every step
-        states = []
+        # recompute the segment, keeping every step's initial state and its
+        # forward products (C-grid fields, pre-remap state) on a tape
+        states, tapes = [], []
         for r in remaps:
             s = torch.empty_like(ckpt)
             dyn.state_save(s.data_ptr())
             states.append(s)
-            dyn.step(dt, remap=r, check_stable=False)
+            tp = torch.empty(dyn.tape_bytes() // 8, dtype=torch.float64, device=ckpt.device)
+            dyn.step_tape(dt, r, tp.data_ptr())
+            tapes.append(tp)
         dyn.adj_zero()
         grads = [g if g is not None else torch.zeros_like(ckpt[:0]) for g in (gdp, gpt, gud, gvd)]
         for name, g in zip(FIELD_NAMES, grads):
             if g.numel():
                 dyn.adj_set_device('out', name, g.detach().contiguous().data_ptr())
-        for s, r in zip(reversed(states), reversed(remaps)):
+        for s, tp, r in zip(reversed(states), reversed(tapes), reversed(remaps)):
             dyn.state_load(s.data_ptr())
-            dyn.adj_step(dt, remap=r)
+            dyn.adj_step_tape(dt, r, tp.data_ptr())
         dyn.adj_halo('out')  # the initial state's halo is the periodic image of its interior
         like = gdp if gdp is not None else (gpt if gpt is not None else (gud if gud is not None else gvd))
         outs = []

@@ -246,6 +246,19 @@ class Dycore:
     def adj_remap(self):
         check(self.lib.atm_adj_remap(self.ctx), self.ctx, 'atm_adj_remap')
 
+    def tape_bytes(self):
+        n = ctypes.c_longlong(0)
+        check(self.lib.atm_tape_bytes(self.ctx, ctypes.byref(n)), self.ctx, 'atm_tape_bytes')
+        return n.value
+
+    def step_tape(self, dt, remap, ptr):
+        """A step that records its forward products at the device address ptr."""
+        check(self.lib.atm_step_tape(self.ctx, dt, int(remap), ctypes.c_void_p(ptr)), self.ctx, 'atm_step_tape')
+
+    def adj_step_tape(self, dt, remap, ptr):
+        check(self.lib.atm_adj_step_tape(self.ctx, dt, int(remap), ctypes.c_void_p(ptr)), self.ctx,
+              'atm_adj_step_tape')
+
     def state_bytes(self):
         n = ctypes.c_longlong(0)
         check(self.lib.atm_state_bytes(self.ctx, ctypes.byref(n)), self.ctx, 'atm_state_bytes')

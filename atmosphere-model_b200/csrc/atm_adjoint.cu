@@ -42,14 +42,14 @@ cudaError_t adj_mass(const Geom& g, const Consts& c, const double* dp, const dou
     if ((e = tmap(dp, 8, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, 8, g, g.L, Lay::WD, Lay::HD, &mp)) ||
         (e = tmap(u, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, 8, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
-    k_mass_adj<TXA, TYA, true><<<tiles_a(lo, hi, g), NT, MassAdjL<TXA, TYA, true>::bytes, s>>>(
+    k_mass_adj<TXA, TYA, true><<<tiles_a(lo, hi, g), NTA, MassAdjL<TXA, TYA, true>::bytes, s>>>(
         md, mp, mu, mv, g, c, lam_dpo, lam_pto, lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
   } else {
     using Lay = MassL<double, TXA, TYA, false>;
     if ((e = tmap(dp, 8, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, 8, g, g.L, Lay::WD, Lay::HD, &mp)) ||
         (e = tmap(u, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, 8, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
-    k_mass_adj<TXA, TYA, false><<<tiles_a(lo, hi, g), NT, MassAdjL<TXA, TYA, false>::bytes, s>>>(
+    k_mass_adj<TXA, TYA, false><<<tiles_a(lo, hi, g), NTA, MassAdjL<TXA, TYA, false>::bytes, s>>>(
         md, mp, mu, mv, g, c, lam_dpo, lam_pto, lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
   }
   return cudaGetLastError();
@@ -65,7 +65,7 @@ cudaError_t adj_c_mom(const Geom& g, const Consts& c, const double* ud, const do
       (e = tmap(ud, 8, g, g.L, Lay::WL, Lay::HL, &muL)) || (e = tmap(vd, 8, g, g.L, Lay::WL, Lay::HL, &mvL)) ||
       (e = tmap(pkap, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpk)) || (e = tmap(gz, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgz)))
     return e;
-  k_c_mom_adj<TXA, TYA><<<tiles_a(0, 0, g), NT, CMomAdjL<TXA, TYA>::bytes, s>>>(
+  k_c_mom_adj<TXA, TYA><<<tiles_a(0, 0, g), NTA, CMomAdjL<TXA, TYA>::bytes, s>>>(
       mu, mv, muL, mvL, mpk, mgz, g, c, lam_uc, lam_vc, lam_ud, lam_vd, lam_pk, lam_gz, timeout);
   return cudaGetLastError();
 }
@@ -82,7 +82,7 @@ cudaError_t adj_d_mom(const Geom& g, const Consts& c, const double* ud, const do
       (e = tmap(uc, 8, g, g.L, Lay::WC, Lay::HC, &muc)) || (e = tmap(vc, 8, g, g.L, Lay::WC, Lay::HC, &mvc)) ||
       (e = tmap(pkapb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpb)) || (e = tmap(gzb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgb)))
     return e;
-  k_d_mom_adj<TXA, TYA><<<tiles_a(0, 0, g), NT, DMomAdjL<TXA, TYA>::bytes, s>>>(
+  k_d_mom_adj<TXA, TYA><<<tiles_a(0, 0, g), NTA, DMomAdjL<TXA, TYA>::bytes, s>>>(
       mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c, lam_udo, lam_vdo, lam_ud, lam_vd, lam_uc, lam_vc, lam_pkb, lam_gzb,
       timeout);
   return cudaGetLastError();

@@ -21,26 +21,78 @@
 
 namespace atm {
 
-__device__ __forceinline__ void sadd(double* p, double v) { atomicAdd(p, v); }
+// threads per block of the adjoint tile kernels
+constexpr int NTA = 256;
+
+// add to a shared-memory adjoint (p points into shared memory): a reduction
+// in the shared state space, not a generic-address atomic
+__device__ __forceinline__ void sadd(double* p, double v) {
+  asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(smem_u32(p)), "d"(v) : "memory");
+}
 
 // zero the doubles of [a, b)
 __device__ __forceinline__ void zero_smem(unsigned char* a, unsigned char* b) {
   double* p = reinterpret_cast<double*>(a);
   const int n = (int)((b - a) / 8);
-  for (int i = threadIdx.x; i < n; i += NT) p[i] = 0.;
+  for (int i = threadIdx.x; i < n; i += NTA) p[i] = 0.;
+}
+
+// region loop of the adjoint kernels: body(x, y) over [x0, x0+W) x [y0, y0+Hh)
+template <int W, int Hh, typename F>
+__device__ __forceinline__ void aregion(int x0, int y0, F&& body) {
+  for (int idx = threadIdx.x; idx < W * Hh; idx += NTA) {
+    const int y = idx / W;
+    const int x = idx - y * W;
+    body(x0 + x, y0 + y);
+  }
 }
 
 // ---- adjoint building blocks -------------------------------------------
 
-// mono = monotone slope of q(-s), q(0), q(+s) (src/mod_sw_dyn.f90:870-875)
+// index (0, 1, 2) of the argument that mn3 / mx3 return
+__device__ __forceinline__ int sel_mn3(double a, double b, double c) {
+  int i = (b < a) ? 1 : 0;
+  double t = (b < a) ? b : a;
+  return (c < t) ? 2 : i;
+}
+__device__ __forceinline__ int sel_mx3(double a, double b, double c) {
+  int i = (a < b) ? 1 : 0;
+  double t = (a < b) ? b : a;
+  return (t < c) ? 2 : i;
+}
+
+// mono = monotone slope of q(-s), q(0), q(+s) (src/mod_sw_dyn.f90:870-875):
+// mono = copysign(mn3(|dqi|, dmin, dmax), dqi) with dqi = (q(+s) - q(-s))/4,
+// dmin = q0 - mn3(q(+s), q0, q(-s)), dmax = mx3(q(+s), q0, q(-s)) - q0;
+// the derivative follows the argument each mn3/mx3 returns
 __device__ __forceinline__ void slope_adj(const double* q, int s, double lam, double* lq, int ls) {
   if (lam == 0.) return;
-  DV<3> a = DV<3>::seeded(q[-s], 0), b = DV<3>::seeded(q[0], 1), c = DV<3>::seeded(q[s], 2);
-  DV<3> dqi, mono;
-  slopes(a, b, c, dqi, mono);
-  if (mono.d[0] != 0.) sadd(lq - ls, mono.d[0] * lam);
-  if (mono.d[1] != 0.) sadd(lq, mono.d[1] * lam);
-  if (mono.d[2] != 0.) sadd(lq + ls, mono.d[2] * lam);
+  const double qm = q[-s], q0 = q[0], qp = q[s];
+  const double dqi = (qp - qm) * 0.25;
+  const double A = fabs(dqi);
+  const double B = q0 - mn3(qp, q0, qm);
+  const double C = mx3(qp, q0, qm) - q0;
+  const int sel = sel_mn3(A, B, C);
+  const double m3 = sel == 0 ? A : (sel == 1 ? B : C);
+  if (!(m3 > 0.)) return;
+  const double l = (signbit(dqi) ? -lam : lam);
+  double am = 0., a0 = 0., ap = 0.;
+  if (sel == 0) {
+    const double gq = (dqi > 0. ? .25 : -.25) * l;
+    ap += gq;
+    am -= gq;
+  } else if (sel == 1) {
+    a0 += l;
+    const int j = sel_mn3(qp, q0, qm);
+    if (j == 0) ap -= l; else if (j == 1) a0 -= l; else am -= l;
+  } else {
+    a0 -= l;
+    const int j = sel_mx3(qp, q0, qm);
+    if (j == 0) ap += l; else if (j == 1) a0 += l; else am += l;
+  }
+  if (am != 0.) sadd(lq - ls, am);
+  if (a0 != 0.) sadd(lq, a0);
+  if (ap != 0.) sadd(lq + ls, ap);
 }
 
 // edge anomalies (eL, eR) of one cell from q(-1..1) and mono(-1..1)
@@ -95,6 +147,88 @@ __device__ __forceinline__ double flux_pre_adj(const double* q, int sq, const do
     lamc += F.d[6] * lamF;
   }
   return F.v;
+}
+
+// F = flux_pre<PPM_UNC>(q, mono, c), by hand: with u the upwind cell,
+// eL = (q(u-1) - q(u))/2 + (m(u-1) - m(u))/3, eR = (q(u+1) - q(u))/2 + (m(u) - m(u+1))/3,
+// F = q(u) + k1 eR + k2 eL (c > 0) or q(u) + k1 eL + k2 eR, k1 = (1-2s)(1-s),
+// k2 = s(s-1), s = |c|.  Same contract as flux_pre_adj.
+__device__ __forceinline__ double flux_unc_adj(const double* q, int sq, const double* mono, int sm, double c,
+                                               double lamF, double* lq, int slq, double* lm, int slm, double& lamc) {
+  const int o = (c > 0.) ? -1 : 0;
+  const double* qu = q + o * sq;
+  const double* mu = mono + o * sm;
+  const double qm = qu[-sq], q0 = qu[0], qp = qu[sq], mm = mu[-sm], m0 = mu[0], mp = mu[sm];
+  const double eL = (qm - q0) * 0.5 + div_const<3>(mm - m0);
+  const double eR = (qp - q0) * 0.5 + div_const<3>(m0 - mp);
+  const double sa = fabs(c);
+  const double k1 = (1. - 2. * sa) * (1. - sa);
+  const double k2 = sa * (sa - 1.);
+  const double F = (c > 0.) ? q0 + k1 * eR + k2 * eL : q0 + k1 * eL + k2 * eR;
+  if (lamF != 0.) {
+    const double aR = (c > 0.) ? k1 : k2, aL = (c > 0.) ? k2 : k1;
+    const double lR = aR * lamF, lL = aL * lamF;
+    double* lqu = lq + o * slq;
+    double* lmu = lm + o * slm;
+    sadd(lqu - slq, .5 * lL);
+    sadd(lqu, lamF - .5 * (lL + lR));
+    sadd(lqu + slq, .5 * lR);
+    sadd(lmu - slm, lL / 3.);
+    sadd(lmu, (lR - lL) / 3.);
+    sadd(lmu + slm, -lR / 3.);
+    const double sg = c > 0. ? 1. : (c < 0. ? -1. : 0.);
+    const double dk1 = 4. * sa - 3., dk2 = 2. * sa - 1.;
+    lamc += sg * ((c > 0.) ? dk1 * eR + dk2 * eL : dk1 * eL + dk2 * eR) * lamF;
+  }
+  return F;
+}
+
+// (eL, eR) = edges_pre<PPM_CONSTRAINED>(q, mono) of one cell, by hand
+// (src/mod_sw_dyn.f90:877-893): the raw edges, limited by 2|dqi| with the
+// sign of dqi.  Same contract as edges_adj.
+__device__ __forceinline__ void edges_con_adj(const double* q, int sq, const double* mono, int sm, double lamL,
+                                              double lamR, double* lq, int slq, double* lm, int slm) {
+  if (lamL == 0. && lamR == 0.) return;
+  const double qm = q[-sq], q0 = q[0], qp = q[sq], mm = mono[-sm], m0 = mono[0], mp = mono[sm];
+  const double eLr = (qm - q0) * 0.5 + div_const<3>(mm - m0);
+  const double eRr = (qp - q0) * 0.5 + div_const<3>(m0 - mp);
+  const double d0 = (qp - qm) * 0.25;
+  const double lim = 2. * fabs(d0);
+  const double sb = signbit(d0) ? -1. : 1.;
+  const double sd = d0 > 0. ? 1. : (d0 < 0. ? -1. : 0.);
+  double lLr = 0., lRr = 0., ld0 = 0.;
+  {  // eL = -copysign(mn(lim, |eLr|), d0)
+    const double a = fabs(eLr);
+    const bool raw = a < lim;
+    const double av = raw ? a : lim;
+    const double la = -(av > 0. ? sb : 0.) * lamL;
+    if (raw) lLr = (eLr > 0. ? 1. : (eLr < 0. ? -1. : 0.)) * la;
+    else ld0 += 2. * sd * la;
+  }
+  {  // eR = +copysign(mn(lim, |eRr|), d0)
+    const double a = fabs(eRr);
+    const bool raw = a < lim;
+    const double av = raw ? a : lim;
+    const double la = (av > 0. ? sb : 0.) * lamR;
+    if (raw) lRr = (eRr > 0. ? 1. : (eRr < 0. ? -1. : 0.)) * la;
+    else ld0 += 2. * sd * la;
+  }
+  const double a_m = .5 * lLr - .25 * ld0, a_0 = -.5 * (lLr + lRr), a_p = .5 * lRr + .25 * ld0;
+  if (a_m != 0.) sadd(lq - slq, a_m);
+  if (a_0 != 0.) sadd(lq, a_0);
+  if (a_p != 0.) sadd(lq + slq, a_p);
+  const double b_m = lLr / 3., b_0 = (lRr - lLr) / 3., b_p = -lRr / 3.;
+  if (b_m != 0.) sadd(lm - slm, b_m);
+  if (b_0 != 0.) sadd(lm, b_0);
+  if (b_p != 0.) sadd(lm + slm, b_p);
+}
+
+// flux adjoint of variant V: by hand for PPM_UNCONSTRAINED, else on DV numbers
+template <int V>
+__device__ __forceinline__ double flux_adj(const double* q, int sq, const double* mono, int sm, double c, double lamF,
+                                           double* lq, int slq, double* lm, int slm, double& lamc) {
+  if constexpr (V == PPM_UNC) return flux_unc_adj(q, sq, mono, sm, c, lamF, lq, slq, lm, slm, lamc);
+  else return flux_pre_adj<V>(q, sq, mono, sm, c, lamF, lq, slq, lm, slm, lamc);
 }
 
 // F = flux_con_pre(q, eL, eR, c) with precomputed PPM_CONSTRAINED edges
@@ -171,7 +305,7 @@ __device__ __forceinline__ PgfAdj pgf_adj(double p0, double p1, double g0, doubl
 // add a tile-local adjoint box to a global adjoint field (level k)
 __device__ __forceinline__ void flush_box(const Sm<double>& a, int w, int h, double* dst, const Geom& g, int k) {
   if (!dst) return;
-  for (int idx = threadIdx.x; idx < w * h; idx += NT) {
+  for (int idx = threadIdx.x; idx < w * h; idx += NTA) {
     const int yy = idx / w, xx = idx - yy * w;
     const double v = a.p[idx];
     const int x = a.x0 + xx, y = a.y0 + yy;
@@ -196,7 +330,7 @@ struct MassAdjL {
 };
 
 template <int TX, int TY, bool CGRID>
-__global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtensorMap m_dp,
+__global__ void __launch_bounds__(NTA, 2) k_mass_adj(const __grid_constant__ CUtensorMap m_dp,
                                                  const __grid_constant__ CUtensorMap m_pt,
                                                  const __grid_constant__ CUtensorMap m_u,
                                                  const __grid_constant__ CUtensorMap m_v, Geom g, Consts c,
@@ -281,17 +415,17 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
 
   // ---- forward recomputation (as k_mass2)
   if (CGRID) {
-    region<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
+    aregion<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
       T ub = T(.5) * (su(x, y) + su(x - 1, y));
       suc(x, y) = T(.5) * (ub + T(.5) * (su(x, y + 1) + su(x - 1, y + 1)));
     });
-    region<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
+    aregion<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
       T vb = T(.5) * (sv(x, y) + sv(x, y - 1));
       svc(x, y) = T(.5) * (vb + T(.5) * (sv(x + 1, y) + sv(x + 1, y - 1)));
     });
     __syncthreads();
   }
-  region<TX + 6, TY>(ox - 3, oy, [&](int x, int y) {
+  aregion<TX + 6, TY>(ox - 3, oy, [&](int x, int y) {
     T cy0 = dtdx * svc(x, y), cy1 = dtdx * svc(x, y + 1);
     T den = T(1) / (T(1) - dtdy * (svc(x, y + 1) - svc(x, y)));
     T f0 = (cy0 > T(0)) ? sdp(x, y - 1) : sdp(x, y);
@@ -301,7 +435,7 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
     f1 = (cy1 > T(0)) ? spt(x, y) : spt(x, y + 1);
     typ(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
   });
-  region<TX, TY + 6>(ox, oy - 3, [&](int x, int y) {
+  aregion<TX, TY + 6>(ox, oy - 3, [&](int x, int y) {
     T cx0 = dtdx * suc(x, y), cx1 = dtdx * suc(x + 1, y);
     T den = T(1) / (T(1) - dtdx * (suc(x + 1, y) - suc(x, y)));
     T f0 = (cx0 > T(0)) ? sdp(x - 1, y) : sdp(x, y);
@@ -312,28 +446,28 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
     txp(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
   });
   const T rdx2 = c.rdx2, rdy2 = c.rdy2, rdxy = c.rdx2rdy2;
-  region<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
+  aregion<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
     lpd(x, y) = T(-2.) * sdp(x, y) * rdxy + (sdp(x + 1, y) + sdp(x - 1, y)) * rdx2 +
                 (sdp(x, y + 1) + sdp(x, y - 1)) * rdy2;
     lpp(x, y) = T(-2.) * spt(x, y) * rdxy + (spt(x + 1, y) + spt(x - 1, y)) * rdx2 +
                 (spt(x, y + 1) + spt(x, y - 1)) * rdy2;
   });
   __syncthreads();
-  region<TX + 4, TY>(ox - 2, oy, [&](int x, int y) {
+  aregion<TX + 4, TY>(ox - 2, oy, [&](int x, int y) {
     mxd(x, y) = slope_at(tyd.ptr(x, y), 1);
     mxp(x, y) = slope_at(typ.ptr(x, y), 1);
   });
-  region<TX, TY + 4>(ox, oy - 2, [&](int x, int y) {
+  aregion<TX, TY + 4>(ox, oy - 2, [&](int x, int y) {
     myd(x, y) = slope_at(txd.ptr(x, y), TX);
     myp(x, y) = slope_at(txp.ptr(x, y), TX);
   });
   __syncthreads();
-  region<TX + 1, TY>(ox, oy, [&](int x, int y) {
+  aregion<TX + 1, TY>(ox, oy, [&](int x, int y) {
     T cx = dtdx * suc(x, y);
     fxd(x, y) = flux_pre<T, V>(tyd.ptr(x, y), 1, mxd.ptr(x, y), 1, cx) * cx;
     fxp(x, y) = flux_pre<T, V>(typ.ptr(x, y), 1, mxp.ptr(x, y), 1, cx);
   });
-  region<TX, TY + 1>(ox, oy, [&](int x, int y) {
+  aregion<TX, TY + 1>(ox, oy, [&](int x, int y) {
     T cy = dtdx * svc(x, y);
     fyd(x, y) = flux_pre<T, V>(txd.ptr(x, y), TX, myd.ptr(x, y), TX, cy) * cy;
     fyp(x, y) = flux_pre<T, V>(txp.ptr(x, y), TX, myp.ptr(x, y), TX, cy);
@@ -345,7 +479,7 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
   const T dxv = dtdx * c.vdx, dyv = dtdy * c.vdy, vdx = c.vdx, vdy = c.vdy;
   // updates (:163-172,193-202,230-237,258-267 / :490-499,519-528,555-562,582-591):
   // Lv = adjoint of the new dp, Lq = adjoint of the numerator of the new pt
-  region<TX, TY>(ox, oy, [&](int x, int y) {
+  aregion<TX, TY>(ox, oy, [&](int x, int y) {
     double lv = 0., lq = 0.;
     if (x <= xhi && y <= yhi) {
       T d = sdp(x, y);
@@ -370,7 +504,7 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
   auto LV = [&](int x, int y) { return inT(x, y) ? Lv(x, y) : 0.; };
   auto LQ = [&](int x, int y) { return inT(x, y) ? Lq(x, y) : 0.; };
   // Laplacians' adjoints (gather)
-  region<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
+  aregion<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
     alpd(x, y) = dxv * (2. * LV(x, y) - LV(x - 1, y) - LV(x + 1, y)) + dyv * (2. * LV(x, y) - LV(x, y - 1) - LV(x, y + 1));
     double a = 0., b = 0.;
     if (inT(x - 1, y)) a -= fxd(x, y) * Lq(x - 1, y);
@@ -382,42 +516,42 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
     alpp(x, y) = vdx * a + vdy * b;
   });
   // outer PPM sweeps (:156-161,186-191 / :484-489,513-518)
-  region<TX + 1, TY>(ox, oy, [&](int x, int y) {
+  aregion<TX + 1, TY>(ox, oy, [&](int x, int y) {
     const double ql = LQ(x - 1, y), qr = LQ(x, y);
     const double lfd = (LV(x, y) - LV(x - 1, y)) + (fxp(x, y) + vdx * (lpp(x, y) - lpp(x - 1, y))) * (qr - ql);
     const double lfp = fxd(x, y) * (qr - ql);
     if (lfd == 0. && lfp == 0.) return;
     const T cx = dtdx * suc(x, y);
     double lc = 0.;
-    double F = flux_pre_adj<V>(tyd.ptr(x, y), 1, mxd.ptr(x, y), 1, cx, lfd * cx, atyd.ptr(x, y), 1, amxd.ptr(x, y), 1, lc);
+    double F = flux_adj<V>(tyd.ptr(x, y), 1, mxd.ptr(x, y), 1, cx, lfd * cx, atyd.ptr(x, y), 1, amxd.ptr(x, y), 1, lc);
     lc += lfd * F;
-    flux_pre_adj<V>(typ.ptr(x, y), 1, mxp.ptr(x, y), 1, cx, lfp, atyp.ptr(x, y), 1, amxp.ptr(x, y), 1, lc);
+    flux_adj<V>(typ.ptr(x, y), 1, mxp.ptr(x, y), 1, cx, lfp, atyp.ptr(x, y), 1, amxp.ptr(x, y), 1, lc);
     asuc(x, y) += dtdx * lc;
   });
-  region<TX, TY + 1>(ox, oy, [&](int x, int y) {
+  aregion<TX, TY + 1>(ox, oy, [&](int x, int y) {
     const double ql = LQ(x, y - 1), qr = LQ(x, y);
     const double lfd = (LV(x, y) - LV(x, y - 1)) + (fyp(x, y) + vdy * (lpp(x, y) - lpp(x, y - 1))) * (qr - ql);
     const double lfp = fyd(x, y) * (qr - ql);
     if (lfd == 0. && lfp == 0.) return;
     const T cy = dtdx * svc(x, y);
     double lc = 0.;
-    double F = flux_pre_adj<V>(txd.ptr(x, y), TX, myd.ptr(x, y), TX, cy, lfd * cy, atxd.ptr(x, y), TX, amyd.ptr(x, y), TX, lc);
+    double F = flux_adj<V>(txd.ptr(x, y), TX, myd.ptr(x, y), TX, cy, lfd * cy, atxd.ptr(x, y), TX, amyd.ptr(x, y), TX, lc);
     lc += lfd * F;
-    flux_pre_adj<V>(txp.ptr(x, y), TX, myp.ptr(x, y), TX, cy, lfp, atxp.ptr(x, y), TX, amyp.ptr(x, y), TX, lc);
+    flux_adj<V>(txp.ptr(x, y), TX, myp.ptr(x, y), TX, cy, lfp, atxp.ptr(x, y), TX, amyp.ptr(x, y), TX, lc);
     asvc(x, y) += dtdx * lc;
   });
   __syncthreads();
   // slopes (:870-875) and the Laplacians (:148-153,178-183 / :476-481,505-510)
-  region<TX + 4, TY>(ox - 2, oy, [&](int x, int y) {
+  aregion<TX + 4, TY>(ox - 2, oy, [&](int x, int y) {
     slope_adj(tyd.ptr(x, y), 1, amxd(x, y), atyd.ptr(x, y), 1);
     slope_adj(typ.ptr(x, y), 1, amxp(x, y), atyp.ptr(x, y), 1);
   });
-  region<TX, TY + 4>(ox, oy - 2, [&](int x, int y) {
+  aregion<TX, TY + 4>(ox, oy - 2, [&](int x, int y) {
     slope_adj(txd.ptr(x, y), TX, amyd(x, y), atxd.ptr(x, y), TX);
     slope_adj(txp.ptr(x, y), TX, amyp(x, y), atxp.ptr(x, y), TX);
   });
   auto inL = [&](int x, int y) { return x >= ox - 1 && x < ox + TX + 1 && y >= oy - 1 && y < oy + TY + 1; };
-  region<TX + 4, TY + 4>(ox - 2, oy - 2, [&](int x, int y) {
+  aregion<TX + 4, TY + 4>(ox - 2, oy - 2, [&](int x, int y) {
     double ad = 0., ap = 0.;
     if (inL(x, y)) { ad += -2. * rdxy * alpd(x, y); ap += -2. * rdxy * alpp(x, y); }
     if (inL(x - 1, y)) { ad += rdx2 * alpd(x - 1, y); ap += rdx2 * alpp(x - 1, y); }
@@ -429,7 +563,7 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
   });
   __syncthreads();
   // inner sweeps (:142-147,176-177,210-216,238-243 / :470-475,503-504,531-536,563-568)
-  region<TX + 6, TY>(ox - 3, oy, [&](int x, int y) {
+  aregion<TX + 6, TY>(ox - 3, oy, [&](int x, int y) {
     const double ld = atyd(x, y), lp = atyp(x, y);
     if (ld == 0. && lp == 0.) return;
     const T w0 = svc(x, y), w1 = svc(x, y + 1);
@@ -444,7 +578,7 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
       sadd(asvc.ptr(x, y), -lw);
     }
   });
-  region<TX, TY + 6>(ox, oy - 3, [&](int x, int y) {
+  aregion<TX, TY + 6>(ox, oy - 3, [&](int x, int y) {
     const double ld = atxd(x, y), lp = atxp(x, y);
     if (ld == 0. && lp == 0.) return;
     const T w0 = suc(x, y), w1 = suc(x + 1, y);
@@ -461,7 +595,7 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
   });
   __syncthreads();
   if (CGRID) {  // C-grid winds from the D-grid winds (:109-117)
-    region<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
+    aregion<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
       const double l = .25 * asuc(x, y);
       if (l == 0.) return;
       sadd(asu.ptr(x, y), l);
@@ -469,7 +603,7 @@ __global__ void __launch_bounds__(NT) k_mass_adj(const __grid_constant__ CUtenso
       sadd(asu.ptr(x, y + 1), l);
       sadd(asu.ptr(x - 1, y + 1), l);
     });
-    region<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
+    aregion<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
       const double l = .25 * asvc(x, y);
       if (l == 0.) return;
       sadd(asv.ptr(x, y), l);
@@ -500,11 +634,12 @@ struct CMomAdjL {
       box_bytes<double>(TX, TY + 3) + box_bytes<double>(TX + 3, TY) +                  // mtU, mtV
       2 * box_bytes<double>(TX + 7, TY + 7) + 2 * box_bytes<double>(TX + 3, TY + 3) +  // ud, vd (k, nlay)
       4 * box_bytes<double>(TX + 1, TY + 1);                                           // pkap, gz (k, k+1)
-  static constexpr size_t bytes = F::bytes + lam;
+  // the forward's ke and lap values are not needed by the reverse
+  static constexpr size_t bytes = F::bytes - 2 * box_bytes<double>(TX + 1, TY + 1) + lam;
 };
 
 template <int TX, int TY>
-__global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtensorMap m_ud,
+__global__ void __launch_bounds__(NTA, 1) k_c_mom_adj(const __grid_constant__ CUtensorMap m_ud,
                                                   const __grid_constant__ CUtensorMap m_vd,
                                                   const __grid_constant__ CUtensorMap m_udL,
                                                   const __grid_constant__ CUtensorMap m_vdL,
@@ -549,10 +684,8 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
   Sm<T> uaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
   Sm<T> vaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
   Sm<T> vor = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
-  Sm<T> ke = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
   Sm<T> tU = carve<T>(p, ox, oy - 2, TX, TY + 5);
   Sm<T> tV = carve<T>(p, ox - 2, oy, TX + 5, TY);
-  Sm<T> lap = carve<T>(p, ox, oy, TX + 1, TY + 1);
   Sm<T> mvy = carve<T>(p, ox - 1, oy - 2, TX + 1, TY + 4);
   Sm<T> mux = carve<T>(p, ox - 2, oy - 1, TX + 4, TY + 1);
   Sm<T> mtU = carve<T>(p, ox, oy - 1, TX, TY + 3);
@@ -582,13 +715,13 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
   zero_smem(lam0, p);
 
   // ---- forward recomputation (as k_c_mom2)
-  region<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
+  aregion<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
     T ub = T(.5) * (sud(x, y) + sud(x - 1, y));
     uc1(x, y) = T(.5) * (ub + T(.5) * (sud(x, y + 1) + sud(x - 1, y + 1)));
     T vb = T(.5) * (svd(x, y) + svd(x, y - 1));
     vc1(x, y) = T(.5) * (vb + T(.5) * (svd(x + 1, y) + svd(x + 1, y - 1)));
   });
-  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
+  aregion<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
     T ub = T(.5) * (udL(x, y) + udL(x - 1, y));
     T ucl = T(.5) * (ub + T(.5) * (udL(x, y + 1) + udL(x - 1, y + 1)));
     uaL(x, y) = T(.5) * (ucl + T(.25) * (udL(x + 1, y) + udL(x, y) + udL(x + 1, y + 1) + udL(x, y + 1)));
@@ -598,26 +731,20 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
   });
   __syncthreads();
   const T f = c.coriolis;
-  region<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
+  aregion<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
     vor(x, y) = f - (uc1(x, y) - uc1(x, y - 1)) * rdy + (vc1(x, y) - vc1(x - 1, y)) * rdx;
   });
-  region<TX + 1, TY + 4>(ox - 1, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(vc1.ptr(x, y), TX + 6); });
-  region<TX + 4, TY + 1>(ox - 2, oy - 1, [&](int x, int y) { mux(x, y) = slope_at(uc1.ptr(x, y), 1); });
+  aregion<TX + 1, TY + 4>(ox - 1, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(vc1.ptr(x, y), TX + 6); });
+  aregion<TX + 4, TY + 1>(ox - 2, oy - 1, [&](int x, int y) { mux(x, y) = slope_at(uc1.ptr(x, y), 1); });
   __syncthreads();
-  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
-    T fy = flux_pre<T, PPM_UNC>(vc1.ptr(x, y + 1), TX + 6, mvy.ptr(x, y + 1), TX + 1, dtdy * vaL(x, y));
-    T kv = vaL(x, y) * fy;
-    T fx = flux_pre<T, PPM_UNC>(uc1.ptr(x + 1, y), 1, mux.ptr(x + 1, y), 1, dtdx * uaL(x, y));
-    ke(x, y) = T(.5) * (kv + uaL(x, y) * fx);
-  });
-  region<TX, TY + 5>(ox, oy - 2, [&](int x, int y) {
+  aregion<TX, TY + 5>(ox, oy - 2, [&](int x, int y) {
     T c0 = dtdx * sud(x - 1, y), c1 = dtdx * sud(x, y);
     T den = T(1) / (T(1) - dtdx * (sud(x, y) - sud(x - 1, y)));
     T f0 = (c0 > T(0)) ? vor(x - 1, y) : vor(x, y);
     T f1 = (c1 > T(0)) ? vor(x, y) : vor(x + 1, y);
     tU(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
   });
-  region<TX + 5, TY>(ox - 2, oy, [&](int x, int y) {
+  aregion<TX + 5, TY>(ox - 2, oy, [&](int x, int y) {
     T c0 = dtdx * svd(x, y - 1), c1 = dtdx * svd(x, y);
     T den = T(1) / (T(1) - dtdy * (svd(x, y) - svd(x, y - 1)));
     T f0 = (c0 > T(0)) ? vor(x, y - 1) : vor(x, y);
@@ -625,24 +752,21 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
     tV(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
   });
   const T rdx2 = c.rdx2, rdy2 = c.rdy2, rdxy = c.rdx2rdy2;
-  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-    lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 + (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
-  });
   __syncthreads();
-  region<TX, TY + 3>(ox, oy - 1, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); });
-  region<TX + 3, TY>(ox - 1, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); });
+  aregion<TX, TY + 3>(ox, oy - 1, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); });
+  aregion<TX + 3, TY>(ox - 1, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); });
   __syncthreads();
 
   // ---- reverse: uc, vc updates with the PGF (:325-339, 369-381, 399-411)
   const T vdx = c.vdx, vdy = c.vdy;
-  region<TX, TY>(ox, oy, [&](int x, int y) {
+  aregion<TX, TY>(ox, oy, [&](int x, int y) {
     if (x >= g.nx || y >= g.ny) return;
     const long long o = g.at(x, y, k);
     const double lu = lam_uc[o], lv = lam_vc[o];
     if (lu != 0.) {
       sadd(auc1.ptr(x, y), lu);
       double lc = 0.;
-      double F = flux_pre_adj<PPM_UNC>(tU.ptr(x, y + 1), TX, mtU.ptr(x, y + 1), TX, dtdx * svd(x, y), dt * svd(x, y) * lu,
+      double F = flux_unc_adj(tU.ptr(x, y + 1), TX, mtU.ptr(x, y + 1), TX, dtdx * svd(x, y), dt * svd(x, y) * lu,
                                        atU.ptr(x, y + 1), TX, amtU.ptr(x, y + 1), TX, lc);
       sadd(asvd.ptr(x, y), dt * F * lu + dtdx * lc);
       sadd(alap.ptr(x, y + 1), dt * vdy * lu);
@@ -663,7 +787,7 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
     if (lv != 0.) {
       sadd(avc1.ptr(x, y), lv);
       double lc = 0.;
-      double F = flux_pre_adj<PPM_UNC>(tV.ptr(x + 1, y), 1, mtV.ptr(x + 1, y), 1, dtdx * sud(x, y), -dt * sud(x, y) * lv,
+      double F = flux_unc_adj(tV.ptr(x + 1, y), 1, mtV.ptr(x + 1, y), 1, dtdx * sud(x, y), -dt * sud(x, y) * lv,
                                        atV.ptr(x + 1, y), 1, amtV.ptr(x + 1, y), 1, lc);
       sadd(asud.ptr(x, y), -dt * F * lv + dtdx * lc);
       sadd(alap.ptr(x + 1, y), -dt * vdx * lv);
@@ -685,10 +809,10 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
   __syncthreads();
   // slopes of the vorticity-flux sweeps; Laplacian (:388-397, gather);
   // kinetic energy (:299-317)
-  region<TX, TY + 3>(ox, oy - 1, [&](int x, int y) { slope_adj(tU.ptr(x, y), TX, amtU(x, y), atU.ptr(x, y), TX); });
-  region<TX + 3, TY>(ox - 1, oy, [&](int x, int y) { slope_adj(tV.ptr(x, y), 1, amtV(x, y), atV.ptr(x, y), 1); });
+  aregion<TX, TY + 3>(ox, oy - 1, [&](int x, int y) { slope_adj(tU.ptr(x, y), TX, amtU(x, y), atU.ptr(x, y), TX); });
+  aregion<TX + 3, TY>(ox - 1, oy, [&](int x, int y) { slope_adj(tV.ptr(x, y), 1, amtV(x, y), atV.ptr(x, y), 1); });
   auto inL = [&](int x, int y) { return x >= ox && x <= ox + TX && y >= oy && y <= oy + TY; };
-  region<TX + 3, TY + 3>(ox - 1, oy - 1, [&](int x, int y) {
+  aregion<TX + 3, TY + 3>(ox - 1, oy - 1, [&](int x, int y) {
     double a = 0.;
     if (inL(x, y)) a += -2. * rdxy * alap(x, y);
     if (inL(x - 1, y)) a += rdx2 * alap(x - 1, y);
@@ -697,23 +821,23 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
     if (inL(x, y + 1)) a += rdy2 * alap(x, y + 1);
     avor(x, y) += a;
   });
-  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
+  aregion<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
     const double l = ake(x, y);
     if (l == 0.) return;
     const T va = vaL(x, y), ua = uaL(x, y);
     double lcy = 0., lcx = 0.;
-    double fy = flux_pre_adj<PPM_UNC>(vc1.ptr(x, y + 1), TX + 6, mvy.ptr(x, y + 1), TX + 1, dtdy * va, .5 * va * l,
+    double fy = flux_unc_adj(vc1.ptr(x, y + 1), TX + 6, mvy.ptr(x, y + 1), TX + 1, dtdy * va, .5 * va * l,
                                       avc1.ptr(x, y + 1), TX + 6, amvy.ptr(x, y + 1), TX + 1, lcy);
-    double fx = flux_pre_adj<PPM_UNC>(uc1.ptr(x + 1, y), 1, mux.ptr(x + 1, y), 1, dtdx * ua, .5 * ua * l,
+    double fx = flux_unc_adj(uc1.ptr(x + 1, y), 1, mux.ptr(x + 1, y), 1, dtdx * ua, .5 * ua * l,
                                       auc1.ptr(x + 1, y), 1, amux.ptr(x + 1, y), 1, lcx);
     avaL(x, y) += .5 * fy * l + dtdy * lcy;
     auaL(x, y) += .5 * fx * l + dtdx * lcx;
   });
   __syncthreads();
   // slopes of the KE sweeps; inner vorticity sweeps (:344-367, 383-397); layer-nlay A-grid winds
-  region<TX + 1, TY + 4>(ox - 1, oy - 2, [&](int x, int y) { slope_adj(vc1.ptr(x, y), TX + 6, amvy(x, y), avc1.ptr(x, y), TX + 6); });
-  region<TX + 4, TY + 1>(ox - 2, oy - 1, [&](int x, int y) { slope_adj(uc1.ptr(x, y), 1, amux(x, y), auc1.ptr(x, y), 1); });
-  region<TX, TY + 5>(ox, oy - 2, [&](int x, int y) {
+  aregion<TX + 1, TY + 4>(ox - 1, oy - 2, [&](int x, int y) { slope_adj(vc1.ptr(x, y), TX + 6, amvy(x, y), avc1.ptr(x, y), TX + 6); });
+  aregion<TX + 4, TY + 1>(ox - 2, oy - 1, [&](int x, int y) { slope_adj(uc1.ptr(x, y), 1, amux(x, y), auc1.ptr(x, y), 1); });
+  aregion<TX, TY + 5>(ox, oy - 2, [&](int x, int y) {
     const double l = atU(x, y);
     if (l == 0.) return;
     const T w0 = sud(x - 1, y), w1 = sud(x, y);
@@ -726,7 +850,7 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
       sadd(asud.ptr(x - 1, y), -lw);
     }
   });
-  region<TX + 5, TY>(ox - 2, oy, [&](int x, int y) {
+  aregion<TX + 5, TY>(ox - 2, oy, [&](int x, int y) {
     const double l = atV(x, y);
     if (l == 0.) return;
     const T w0 = svd(x, y - 1), w1 = svd(x, y);
@@ -739,7 +863,7 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
       sadd(asvd.ptr(x, y - 1), -lw);
     }
   });
-  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
+  aregion<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
     const double lu = auaL(x, y), lv = avaL(x, y);
     if (lu != 0.) {
       sadd(audL.ptr(x, y), .25 * lu);
@@ -760,7 +884,7 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
   });
   __syncthreads();
   // vorticity (:319-323)
-  region<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
+  aregion<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
     const double l = avor(x, y);
     if (l == 0.) return;
     sadd(auc1.ptr(x, y), -rdy * l);
@@ -770,7 +894,7 @@ __global__ void __launch_bounds__(NT) k_c_mom_adj(const __grid_constant__ CUtens
   });
   __syncthreads();
   // C-grid winds of the layer (:110-117)
-  region<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
+  aregion<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
     const double lu = .25 * auc1(x, y), lv = .25 * avc1(x, y);
     if (lu != 0.) {
       sadd(asud.ptr(x, y), lu);
@@ -803,18 +927,21 @@ template <int TX, int TY>
 struct DMomAdjL {
   using F = DMomL<double, TX, TY>;
   // forward work arrays without aliasing (the reverse needs every one)
-  static constexpr size_t fwd = box_bytes<double>(TX + 5, TY + 5) * 2 + box_bytes<double>(TX + 3, TY + 3) +
+  // (the divergence, its Laplacians, ke and lap values are not needed by the reverse)
+  static constexpr size_t fwd = box_bytes<double>(TX + 5, TY + 5) + 2 * box_bytes<double>(TX + 1, TY + 1) +
+                                box_bytes<double>(TX, TY + 5) + box_bytes<double>(TX + 5, TY) + F::slopes_ke +
+                                F::slopes_vf + F::edges_ke + F::edges_vf;
+  static constexpr size_t lam = box_bytes<double>(TX + 5, TY + 5) * 2 + box_bytes<double>(TX + 3, TY + 3) +
                                 4 * box_bytes<double>(TX + 1, TY + 1) + box_bytes<double>(TX, TY + 5) +
                                 box_bytes<double>(TX + 5, TY) + box_bytes<double>(TX + 1, TY + 1) + F::slopes_ke +
-                                F::slopes_vf + F::edges_ke + F::edges_vf;
-  static constexpr size_t lam = fwd + 2 * box_bytes<double>(TX + 6, TY + 6) + box_bytes<double>(TX + 1, TY + 5) +
-                                box_bytes<double>(TX + 5, TY + 1) + 2 * box_bytes<double>(TX, TY) +
-                                4 * box_bytes<double>(TX + 1, TY + 1);
+                                F::slopes_vf + F::edges_ke + F::edges_vf + 2 * box_bytes<double>(TX + 6, TY + 6) +
+                                box_bytes<double>(TX + 1, TY + 5) + box_bytes<double>(TX + 5, TY + 1) +
+                                2 * box_bytes<double>(TX, TY) + 4 * box_bytes<double>(TX + 1, TY + 1);
   static constexpr size_t bytes = F::boxes + fwd + lam + 128;
 };
 
 template <int TX, int TY>
-__global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtensorMap m_ud,
+__global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CUtensorMap m_ud,
                                                   const __grid_constant__ CUtensorMap m_vd,
                                                   const __grid_constant__ CUtensorMap m_ucL,
                                                   const __grid_constant__ CUtensorMap m_vcL,
@@ -861,15 +988,10 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
     if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
   }
   Sm<T> vor = carve<T>(p, ox - 3, oy - 3, TX + 5, TY + 5);
-  Sm<T> dv0 = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
-  Sm<T> dv2 = carve<T>(p, ox - 1, oy - 1, TX + 3, TY + 3);
-  Sm<T> dv4 = carve<T>(p, ox, oy, TX + 1, TY + 1);
   Sm<T> ubL = carve<T>(p, ox, oy, TX + 1, TY + 1);
   Sm<T> vbL = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> ke = carve<T>(p, ox, oy, TX + 1, TY + 1);
   Sm<T> tU = carve<T>(p, ox, oy - 3, TX, TY + 5);
   Sm<T> tV = carve<T>(p, ox - 3, oy, TX + 5, TY);
-  Sm<T> lap = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
   Sm<T> mvy = carve<T>(p, ox, oy - 2, TX + 1, TY + 4);
   Sm<T> mux = carve<T>(p, ox - 2, oy, TX + 4, TY + 1);
   Sm<T> mtU = carve<T>(p, ox, oy - 2, TX, TY + 3);
@@ -911,73 +1033,55 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
 
   // ---- forward recomputation (as k_d_mom2)
   const T f = c.coriolis;
-  region<TX + 5, TY + 5>(ox - 3, oy - 3, [&](int x, int y) {
+  aregion<TX + 5, TY + 5>(ox - 3, oy - 3, [&](int x, int y) {
     vor(x, y) = f - (sud(x, y + 1) - sud(x, y)) * rdy + (svd(x + 1, y) - svd(x, y)) * rdx;
-    int xd = x + 1, yd = y + 1;
-    dv0(xd, yd) = rdx * (sud(xd, yd) - sud(xd - 1, yd)) + rdy * (svd(xd, yd) - svd(xd, yd - 1));
   });
-  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
+  aregion<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
     ubL(x, y) = T(.5) * (ucL(x, y) + ucL(x, y - 1));
     vbL(x, y) = T(.5) * (vcL(x, y) + vcL(x - 1, y));
   });
-  region<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(svd.ptr(x, y), Lay::WU); });
-  region<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { mux(x, y) = slope_at(sud.ptr(x, y), 1); });
+  aregion<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(svd.ptr(x, y), Lay::WU); });
+  aregion<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { mux(x, y) = slope_at(sud.ptr(x, y), 1); });
   __syncthreads();
   const T rdx2 = c.rdx2, rdy2 = c.rdy2, rdxy = c.rdx2rdy2;
-  region<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
+  aregion<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
     T eL, eR;
     edges_pre<T, PPM_CON>(svd.ptr(x, y), Lay::WU, mvy.ptr(x, y), TX + 1, eL, eR);
     lvy(x, y) = eL;
     rvy(x, y) = eR;
   });
-  region<TX + 2, TY + 1>(ox - 1, oy, [&](int x, int y) {
+  aregion<TX + 2, TY + 1>(ox - 1, oy, [&](int x, int y) {
     T eL, eR;
     edges_pre<T, PPM_CON>(sud.ptr(x, y), 1, mux.ptr(x, y), 1, eL, eR);
     lux(x, y) = eL;
     rux(x, y) = eR;
   });
-  region<TX + 3, TY + 3>(ox - 1, oy - 1, [&](int x, int y) {
-    dv2(x, y) = T(-2.) * dv0(x, y) * rdxy + (dv0(x + 1, y) + dv0(x - 1, y)) * rdx2 + (dv0(x, y + 1) + dv0(x, y - 1)) * rdy2;
-  });
-  region<TX, TY + 5>(ox, oy - 3, [&](int x, int y) {
+  aregion<TX, TY + 5>(ox, oy - 3, [&](int x, int y) {
     T c0 = dtdx * ucL(x, y), c1 = dtdx * ucL(x + 1, y);
     T den = T(1) / (T(1) - dtdx * (ucL(x + 1, y) - ucL(x, y)));
     T f0 = (c0 > T(0)) ? vor(x - 1, y) : vor(x, y);
     T f1 = (c1 > T(0)) ? vor(x, y) : vor(x + 1, y);
     tU(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
   });
-  region<TX + 5, TY>(ox - 3, oy, [&](int x, int y) {
+  aregion<TX + 5, TY>(ox - 3, oy, [&](int x, int y) {
     T c0 = dtdx * vcL(x, y), c1 = dtdx * vcL(x, y + 1);
     T den = T(1) / (T(1) - dtdy * (vcL(x, y + 1) - vcL(x, y)));
     T f0 = (c0 > T(0)) ? vor(x, y - 1) : vor(x, y);
     T f1 = (c1 > T(0)) ? vor(x, y) : vor(x, y + 1);
     tV(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
   });
-  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
-    lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 + (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
-  });
   __syncthreads();
-  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-    T fy = flux_con_pre<T>(svd.ptr(x, y), Lay::WU, lvy.ptr(x, y), rvy.ptr(x, y), TX + 1, dtdy * vbL(x, y));
-    T kv = vbL(x, y) * fy;
-    T fx = flux_con_pre<T>(sud.ptr(x, y), 1, lux.ptr(x, y), rux.ptr(x, y), 1, dtdx * ubL(x, y));
-    ke(x, y) = T(.5) * (kv + ubL(x, y) * fx);
-  });
   const T divdamp = c.divdamp;
-  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-    T d4 = T(-2.) * dv2(x, y) * rdxy + (dv2(x + 1, y) + dv2(x - 1, y)) * rdx2 + (dv2(x, y + 1) + dv2(x, y - 1)) * rdy2;
-    dv4(x, y) = divdamp * d4;
-  });
-  region<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); });
-  region<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); });
+  aregion<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); });
+  aregion<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); });
   __syncthreads();
-  region<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
+  aregion<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
     T eL, eR;
     edges_pre<T, PPM_CON>(tU.ptr(x, y), TX, mtU.ptr(x, y), TX, eL, eR);
     ltU(x, y) = eL;
     rtU(x, y) = eR;
   });
-  region<TX + 1, TY>(ox - 1, oy, [&](int x, int y) {
+  aregion<TX + 1, TY>(ox - 1, oy, [&](int x, int y) {
     T eL, eR;
     edges_pre<T, PPM_CON>(tV.ptr(x, y), 1, mtV.ptr(x, y), 1, eL, eR);
     ltV(x, y) = eL;
@@ -987,7 +1091,7 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
 
   // ---- reverse: ud, vd updates with the B-grid PGF (:665-679, 724-738, 755-769)
   const T vdx = c.vdx, vdy = c.vdy;
-  region<TX, TY>(ox, oy, [&](int x, int y) {
+  aregion<TX, TY>(ox, oy, [&](int x, int y) {
     if (x >= g.nx || y >= g.ny) return;
     const long long o = g.at(x, y, k);
     const double lu = lam_udo[o], lv = lam_vdo[o];
@@ -1043,13 +1147,13 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
   __syncthreads();
   // edges of the vorticity-flux sweeps; kinetic energy (:639-657);
   // del^4 (:695-702, gather); Laplacian of the vorticity (:712-721, gather)
-  region<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
-    edges_adj<PPM_CON>(tU.ptr(x, y), TX, mtU.ptr(x, y), TX, altU(x, y), artU(x, y), atU.ptr(x, y), TX, amtU.ptr(x, y), TX);
+  aregion<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
+    edges_con_adj(tU.ptr(x, y), TX, mtU.ptr(x, y), TX, altU(x, y), artU(x, y), atU.ptr(x, y), TX, amtU.ptr(x, y), TX);
   });
-  region<TX + 1, TY>(ox - 1, oy, [&](int x, int y) {
-    edges_adj<PPM_CON>(tV.ptr(x, y), 1, mtV.ptr(x, y), 1, altV(x, y), artV(x, y), atV.ptr(x, y), 1, amtV.ptr(x, y), 1);
+  aregion<TX + 1, TY>(ox - 1, oy, [&](int x, int y) {
+    edges_con_adj(tV.ptr(x, y), 1, mtV.ptr(x, y), 1, altV(x, y), artV(x, y), atV.ptr(x, y), 1, amtV.ptr(x, y), 1);
   });
-  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
+  aregion<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
     const double l = ake(x, y);
     if (l == 0.) return;
     const T vb = vbL(x, y), ub = ubL(x, y);
@@ -1062,7 +1166,7 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
     aubL(x, y) += .5 * fx * l + dtdx * lcx;
   });
   auto in4 = [&](int x, int y) { return x >= ox && x <= ox + TX && y >= oy && y <= oy + TY; };
-  region<TX + 3, TY + 3>(ox - 1, oy - 1, [&](int x, int y) {
+  aregion<TX + 3, TY + 3>(ox - 1, oy - 1, [&](int x, int y) {
     double a = 0.;
     if (in4(x, y)) a += -2. * rdxy * adv4(x, y);
     if (in4(x - 1, y)) a += rdx2 * adv4(x - 1, y);
@@ -1072,7 +1176,7 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
     adv2(x, y) = divdamp * a;
   });
   auto inP = [&](int x, int y) { return x >= ox - 1 && x <= ox + TX - 1 && y >= oy - 1 && y <= oy + TY - 1; };
-  region<TX + 3, TY + 3>(ox - 2, oy - 2, [&](int x, int y) {
+  aregion<TX + 3, TY + 3>(ox - 2, oy - 2, [&](int x, int y) {
     double a = 0.;
     if (inP(x, y)) a += -2. * rdxy * alap(x, y);
     if (inP(x - 1, y)) a += rdx2 * alap(x - 1, y);
@@ -1084,17 +1188,17 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
   __syncthreads();
   // slopes of the vorticity-flux sweeps; edges of the KE sweeps; del^2 of
   // the divergence (gather); layer-nlay B-grid winds (:441-444)
-  region<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { slope_adj(tU.ptr(x, y), TX, amtU(x, y), atU.ptr(x, y), TX); });
-  region<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { slope_adj(tV.ptr(x, y), 1, amtV(x, y), atV.ptr(x, y), 1); });
-  region<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
-    edges_adj<PPM_CON>(svd.ptr(x, y), Lay::WU, mvy.ptr(x, y), TX + 1, alvy(x, y), arvy(x, y), asvd.ptr(x, y), TX + 6,
+  aregion<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { slope_adj(tU.ptr(x, y), TX, amtU(x, y), atU.ptr(x, y), TX); });
+  aregion<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { slope_adj(tV.ptr(x, y), 1, amtV(x, y), atV.ptr(x, y), 1); });
+  aregion<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
+    edges_con_adj(svd.ptr(x, y), Lay::WU, mvy.ptr(x, y), TX + 1, alvy(x, y), arvy(x, y), asvd.ptr(x, y), TX + 6,
                        amvy.ptr(x, y), TX + 1);
   });
-  region<TX + 2, TY + 1>(ox - 1, oy, [&](int x, int y) {
-    edges_adj<PPM_CON>(sud.ptr(x, y), 1, mux.ptr(x, y), 1, alux(x, y), arux(x, y), asud.ptr(x, y), 1, amux.ptr(x, y), 1);
+  aregion<TX + 2, TY + 1>(ox - 1, oy, [&](int x, int y) {
+    edges_con_adj(sud.ptr(x, y), 1, mux.ptr(x, y), 1, alux(x, y), arux(x, y), asud.ptr(x, y), 1, amux.ptr(x, y), 1);
   });
   auto in2 = [&](int x, int y) { return x >= ox - 1 && x <= ox + TX + 1 && y >= oy - 1 && y <= oy + TY + 1; };
-  region<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
+  aregion<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
     double a = 0.;
     if (in2(x, y)) a += -2. * rdxy * adv2(x, y);
     if (in2(x - 1, y)) a += rdx2 * adv2(x - 1, y);
@@ -1103,7 +1207,7 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
     if (in2(x, y + 1)) a += rdy2 * adv2(x, y + 1);
     adv0(x, y) = a;
   });
-  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
+  aregion<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
     const double lu = .5 * aubL(x, y), lv = .5 * avbL(x, y);
     if (lu != 0.) {
       sadd(aucL.ptr(x, y), lu);
@@ -1116,11 +1220,11 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
   });
   __syncthreads();
   // slopes of the KE sweeps; inner vorticity sweeps (:704-722, 740-753); divergence (:682-685)
-  region<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) {
+  aregion<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) {
     slope_adj(svd.ptr(x, y), Lay::WU, amvy(x, y), asvd.ptr(x, y), TX + 6);
   });
-  region<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { slope_adj(sud.ptr(x, y), 1, amux(x, y), asud.ptr(x, y), 1); });
-  region<TX, TY + 5>(ox, oy - 3, [&](int x, int y) {
+  aregion<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { slope_adj(sud.ptr(x, y), 1, amux(x, y), asud.ptr(x, y), 1); });
+  aregion<TX, TY + 5>(ox, oy - 3, [&](int x, int y) {
     const double l = atU(x, y);
     if (l == 0.) return;
     const T w0 = ucL(x, y), w1 = ucL(x + 1, y);
@@ -1133,7 +1237,7 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
       sadd(aucL.ptr(x, y), -lw);
     }
   });
-  region<TX + 5, TY>(ox - 3, oy, [&](int x, int y) {
+  aregion<TX + 5, TY>(ox - 3, oy, [&](int x, int y) {
     const double l = atV(x, y);
     if (l == 0.) return;
     const T w0 = vcL(x, y), w1 = vcL(x, y + 1);
@@ -1146,7 +1250,7 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
       sadd(avcL.ptr(x, y), -lw);
     }
   });
-  region<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
+  aregion<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
     const double l = adv0(x, y);
     if (l == 0.) return;
     sadd(asud.ptr(x, y), rdx * l);
@@ -1156,7 +1260,7 @@ __global__ void __launch_bounds__(NT) k_d_mom_adj(const __grid_constant__ CUtens
   });
   __syncthreads();
   // vorticity (:659-663)
-  region<TX + 5, TY + 5>(ox - 3, oy - 3, [&](int x, int y) {
+  aregion<TX + 5, TY + 5>(ox - 3, oy - 3, [&](int x, int y) {
     const double l = avor(x, y);
     if (l == 0.) return;
     sadd(asud.ptr(x, y + 1), -rdy * l);
@@ -1385,18 +1489,6 @@ __device__ void vppm_record(RemapAdjWork<LM>& w, int L, const double* var, const
     w.btm[k + 1] = mn(mx(w.btm[k + 1], mn3(var[k + 1], pmp1, lac1)), mx3(var[k + 1], pmp1, lac1));
   }
   for (int k = 1; k <= L; ++k) w.curv[k] = 6. * var[k] - 3. * (w.top[k] + w.btm[k]);
-}
-
-// index (0, 1, 2) of the argument that mn3 / mx3 return
-__device__ __forceinline__ int sel_mn3(double a, double b, double c) {
-  int i = (b < a) ? 1 : 0;
-  double t = (b < a) ? b : a;
-  return (c < t) ? 2 : i;
-}
-__device__ __forceinline__ int sel_mx3(double a, double b, double c) {
-  int i = (a < b) ? 1 : 0;
-  double t = (a < b) ? b : a;
-  return (t < c) ? 2 : i;
 }
 
 // adjoint of r = mn(mx(x0, mn3(a, b, c)), mx3(a, b, c)) for the edge limiter

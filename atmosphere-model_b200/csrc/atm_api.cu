@@ -773,12 +773,12 @@ int fwd_d(atm_ctx* ctx, double dt, void* const* so, void* const* sn) {
   return ATM_OK;
 }
 
-// lin += (C step)^T lam_cg at the state s; cg must hold the step's dpc, ptc
-int adj_c(atm_ctx* ctx, double dt_half, void* const* s, double* const* lin) {
+// lin += (C step)^T lam_cg at the state s; cgf holds the step's dpc, ptc
+int adj_c(atm_ctx* ctx, double dt_half, void* const* s, double* const* lin, const void* const* cgf) {
   const Geom& g = ctx->geo;
   atm::Consts k = step_consts(ctx, dt_half);
   const double* const* sd = (const double* const*)s;
-  double* const* cg = (double* const*)ctx->cg;
+  const double* const* cg = (const double* const*)cgf;
   {
     Stage t(ctx, S_ACCOL, 2);
     CK(ctx->ops->column(g, k, cg[C_DPC], cg[C_PTC], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
@@ -803,13 +803,15 @@ int adj_c(atm_ctx* ctx, double dt_half, void* const* s, double* const* lin) {
   return ATM_OK;
 }
 
-// lin, lam_cg += (D step)^T lout at so (with cg) -> sn; lout is consumed
-int adj_d(atm_ctx* ctx, double dt, void* const* so, void* const* sn, double* const* lout, double* const* lin) {
+// lin, lam_cg += (D step)^T lout at so (with the C-grid fields cgf) -> sn;
+// pkapb, gzb must hold the step's values; lout is consumed
+int adj_d(atm_ctx* ctx, double dt, const void* const* so, const void* const* sn, double* const* lout,
+          double* const* lin, const void* const* cgf) {
   const Geom& g = ctx->geo;
   atm::Consts k = step_consts(ctx, dt);
   const double* const* o = (const double* const*)so;
   const double* const* n = (const double* const*)sn;
-  const double* const* cg = (const double* const*)ctx->cg;
+  const double* const* cg = (const double* const*)cgf;
   const size_t lev = (size_t)g.S * (ctx->L + 1) * 8;
   CK(cudaMemsetAsync(ctx->lam_pk, 0, lev, ctx->stream));
   CK(cudaMemsetAsync(ctx->lam_gz, 0, lev, ctx->stream));
@@ -839,12 +841,12 @@ int adj_d(atm_ctx* ctx, double dt, void* const* so, void* const* sn, double* con
 }
 
 // lin += (remap)^T lout at the pre-remap state s1
-int adj_r(atm_ctx* ctx, void* const* s1, double* const* lout, double* const* lin) {
+int adj_r(atm_ctx* ctx, const void* const* s1, double* const* lout, double* const* lin) {
   const Geom& g = ctx->geo;
   const double* const* s = (const double* const*)s1;
   atm::RemapArgs ra = remap_args(ctx);
   Stage t(ctx, S_ARMP, 4);
-  CK(ctx->ops->remap_winds(g, ra, s1[F_DP], s1[F_UD], s1[F_VD], ctx->urem, ctx->vrem, nullptr, ctx->status,
+  CK(ctx->ops->remap_winds(g, ra, s[F_DP], s[F_UD], s[F_VD], ctx->urem, ctx->vrem, nullptr, ctx->status,
                            ctx->stream));
   CK(cudaMemsetAsync(ctx->lam_ur, 0, (size_t)g.S * ctx->L * 8, ctx->stream));
   CK(cudaMemsetAsync(ctx->lam_vr, 0, (size_t)g.S * ctx->L * 8, ctx->stream));
@@ -974,7 +976,7 @@ int atm_adj_cgrid_step(atm_ctx* ctx, double dt_half) {
     Stage t(ctx, S_AFWD, 0);
     if ((r = fwd_c(ctx, dt_half, s))) return r;
   }
-  return adj_c(ctx, dt_half, s, slot_fields(ctx, ATM_ADJ_IN));
+  return adj_c(ctx, dt_half, s, slot_fields(ctx, ATM_ADJ_IN), (const void* const*)ctx->cg);
 }
 
 int atm_adj_dgrid_step(atm_ctx* ctx, double dt) {
@@ -987,14 +989,47 @@ int atm_adj_dgrid_step(atm_ctx* ctx, double dt) {
     CK(ctx->ops->ring(ctx->geo, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
     if ((r = fwd_d(ctx, dt, ctx->st[cur], ctx->st[1 - cur]))) return r;
   }
-  return adj_d(ctx, dt, ctx->st[cur], ctx->st[1 - cur], slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN));
+  return adj_d(ctx, dt, (const void* const*)ctx->st[cur], (const void* const*)ctx->st[1 - cur],
+               slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN), (const void* const*)ctx->cg);
 }
 
 int atm_adj_remap(atm_ctx* ctx) {
   int r = require_adj(ctx);
   if (r) return r;
-  return adj_r(ctx, ctx->st[ctx->cur], slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN));
+  return adj_r(ctx, (const void* const*)ctx->st[ctx->cur], slot_fields(ctx, ATM_ADJ_OUT),
+               slot_fields(ctx, ATM_ADJ_IN));
 }
+
+namespace {
+
+// the reverse of one step given its forward products: cgf = C-grid fields
+// after the C-grid halo, s1 = the state after the D-grid step (before the
+// remap); pkapb, gzb must hold the D step's values
+int adj_step_given(atm_ctx* ctx, double dt, int do_remap, const void* const* cgf, const void* const* s1) {
+  const Geom& g = ctx->geo;
+  const void* const* s0 = (const void* const*)ctx->st[ctx->cur];
+  if (do_remap) {
+    CK(zero_fields(ctx, slot_fields(ctx, ATM_ADJ_IN), 4, ctx->L));
+    int r = adj_r(ctx, s1, slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN));
+    if (r) return r;
+    ctx->slot_in = 1 - ctx->slot_in;
+  }
+  CK(zero_fields(ctx, slot_fields(ctx, ATM_ADJ_IN), 4, ctx->L));
+  CK(zero_fields(ctx, ctx->lam_cg, 4, ctx->L));
+  int r = adj_d(ctx, dt, s0, s1, slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN), cgf);
+  if (r) return r;
+  {
+    Stage t(ctx, S_AHALO);
+    CK(atm::adj_ring_fold(g, ctx->lam_cg, 4, ctx->L, ctx->stream));
+  }
+  if ((r = adj_c(ctx, dt / 2., ctx->st[ctx->cur], slot_fields(ctx, ATM_ADJ_IN), cgf))) return r;
+  ctx->slot_in = 1 - ctx->slot_in;
+  return ATM_OK;
+}
+
+size_t field_bytes(const atm_ctx* c) { return (size_t)c->L * c->geo.S * 8; }
+
+}  // namespace
 
 int atm_adj_step(atm_ctx* ctx, double dt, int do_remap) {
   int r = require_adj(ctx);
@@ -1013,22 +1048,52 @@ int atm_adj_step(atm_ctx* ctx, double dt, int do_remap) {
     CK(ctx->ops->ring(g, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
     if ((r = fwd_d(ctx, dt, ctx->st[cur], ctx->st[nxt]))) return r;
   }
-  if (do_remap) {
-    CK(zero_fields(ctx, slot_fields(ctx, ATM_ADJ_IN), 4, ctx->L));
-    if ((r = adj_r(ctx, ctx->st[nxt], slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN)))) return r;
-    ctx->slot_in = 1 - ctx->slot_in;
-  }
-  CK(zero_fields(ctx, slot_fields(ctx, ATM_ADJ_IN), 4, ctx->L));
-  CK(zero_fields(ctx, ctx->lam_cg, 4, ctx->L));
-  if ((r = adj_d(ctx, dt, ctx->st[cur], ctx->st[nxt], slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN))))
-    return r;
-  {
-    Stage t(ctx, S_AHALO);
-    CK(atm::adj_ring_fold(g, ctx->lam_cg, 4, ctx->L, ctx->stream));
-  }
-  if ((r = adj_c(ctx, dt / 2., ctx->st[cur], slot_fields(ctx, ATM_ADJ_IN)))) return r;
-  ctx->slot_in = 1 - ctx->slot_in;
+  return adj_step_given(ctx, dt, do_remap, (const void* const*)ctx->cg, (const void* const*)ctx->st[nxt]);
+}
+
+int atm_tape_bytes(atm_ctx* ctx, long long* bytes) {
+  if (!ctx || !bytes) return ATM_ERR_ARG;
+  *bytes = 8LL * (long long)field_bytes(ctx);
   return ATM_OK;
+}
+
+int atm_step_tape(atm_ctx* ctx, double dt, int do_remap, void* tape) {
+  int r = require_init(ctx);
+  if (r) return r;
+  if (ctx->precision != ATM_FP64) return fail(ctx, ATM_ERR_UNSUPPORTED, "tapes are defined for the FP64 form");
+  if (!tape) return ATM_ERR_ARG;
+  const size_t fb = field_bytes(ctx);
+  char* t = (char*)tape;
+  if ((r = atm_cgrid_step(ctx, dt / 2.))) return r;
+  if ((r = atm_cgrid_halo(ctx))) return r;
+  for (int i = 0; i < 4; ++i) CK(cudaMemcpyAsync(t + i * fb, ctx->cg[i], fb, cudaMemcpyDeviceToDevice, ctx->stream));
+  if ((r = atm_dgrid_step(ctx, dt))) return r;
+  for (int i = 0; i < 4; ++i)
+    CK(cudaMemcpyAsync(t + (4 + i) * fb, ctx->st[ctx->cur][i], fb, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (do_remap && (r = atm_remap(ctx))) return r;
+  return atm_dgrid_halo(ctx);
+}
+
+int atm_adj_step_tape(atm_ctx* ctx, double dt, int do_remap, const void* tape) {
+  int r = require_adj(ctx);
+  if (r) return r;
+  if (!tape) return ATM_ERR_ARG;
+  const Geom& g = ctx->geo;
+  const size_t fb = field_bytes(ctx);
+  const char* t = (const char*)tape;
+  const void* cgf[4] = {t, t + fb, t + 2 * fb, t + 3 * fb};
+  const void* s1[4] = {t + 4 * fb, t + 5 * fb, t + 6 * fb, t + 7 * fb};
+  {
+    Stage st(ctx, S_AHALO);
+    CK(atm::adj_ring_fold(g, slot_fields(ctx, ATM_ADJ_OUT), 4, ctx->L, ctx->stream));
+  }
+  {  // pkapb, gzb of the D step from its new dp, pt
+    Stage st(ctx, S_AFWD, 2);
+    atm::Consts k = step_consts(ctx, dt);
+    CK(ctx->ops->column(g, k, s1[F_DP], s1[F_PT], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+    CK(atm::corners(g, ctx->pkap, ctx->gz, ctx->pkapb, ctx->gzb, 1, 0, ctx->L, ctx->stream));
+  }
+  return adj_step_given(ctx, dt, do_remap, cgf, s1);
 }
 
 int atm_state_bytes(atm_ctx* ctx, long long* bytes) {

@@ -230,6 +230,14 @@ int atm_adj_get_device(atm_ctx* ctx, int slot, int field, double* dev);
    holds the ring's share: atm_adj_halo folds it).  The state is not
    advanced; the other time level and the C-grid fields are overwritten. */
 int atm_adj_step(atm_ctx* ctx, double dt, int do_remap);
+/* the same with the step's forward products recorded by atm_step_tape
+   instead of recomputed: atm_step_tape advances the state like atm_step
+   and writes the C-grid fields (after their halo) and the pre-remap state
+   into a device buffer of atm_tape_bytes bytes; atm_adj_step_tape reverses
+   that step from the restored state before it (atm_state_load) */
+int atm_tape_bytes(atm_ctx* ctx, long long* bytes);
+int atm_step_tape(atm_ctx* ctx, double dt, int do_remap, void* tape);
+int atm_adj_step_tape(atm_ctx* ctx, double dt, int do_remap, const void* tape);
 /* adjoint of a periodic halo fill: each ring adjoint added to its interior
    image and cleared (slot ATM_ADJ_IN or ATM_ADJ_OUT; C-grid adjoints) */
 int atm_adj_halo(atm_ctx* ctx, int slot);
