@@ -302,6 +302,27 @@ __device__ __forceinline__ PgfAdj pgf_adj(double p0, double p1, double g0, doubl
   return PgfAdj{la, -la, lc, -lc, lb, -lb, ld, -ld};
 }
 
+// true in every thread when some output adjoint of the tile [ox, ox+TX) x
+// [oy, oy+TY) (points with x <= xhi, y <= yhi) is nonzero: adjoint
+// sensitivities are local (a loss over a sub-domain reaches only its
+// domain of dependence), and a tile whose outputs carry no adjoint adds
+// nothing to any input adjoint
+template <int TX, int TY>
+__device__ __forceinline__ bool tile_active(const double* a, const double* b, const Geom& g, int k, int ox, int oy,
+                                            int xhi, int yhi, int* s_flag) {
+  if (threadIdx.x == 0) *s_flag = 0;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < TX * TY; idx += NTA) {
+    const int x = ox + idx % TX, y = oy + idx / TX;
+    if (x <= xhi && y <= yhi) {
+      const long long o = g.at(x, y, k);
+      if (a[o] != 0. || b[o] != 0.) *s_flag = 1;
+    }
+  }
+  __syncthreads();
+  return *s_flag != 0;
+}
+
 // add a tile-local adjoint box to a global adjoint field (level k)
 __device__ __forceinline__ void flush_box(const Sm<double>& a, int w, int h, double* dst, const Geom& g, int k) {
   if (!dst) return;
@@ -348,6 +369,7 @@ __global__ void __launch_bounds__(NTA, 2) k_mass_adj(const __grid_constant__ CUt
   const int k = blockIdx.z;
   const int ox = lo + blockIdx.x * TX, oy = lo + blockIdx.y * TY;
   const T dtdx = c.dtdx, dtdy = c.dtdy, rA = c.rA;
+  if (!tile_active<TX, TY>(lam_dpo, lam_pto, g, k, ox, oy, g.nx - 1 + hi, g.ny - 1 + hi, &s_ok)) return;
 
   auto tbox = [&](int i0, int j0, int w, int h) {
     Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
@@ -658,6 +680,7 @@ __global__ void __launch_bounds__(NTA, 1) k_c_mom_adj(const __grid_constant__ CU
   const int ox = blockIdx.x * TX, oy = blockIdx.y * TY;
   const T dt = c.dt, dtdx = c.dtdx, dtdy = c.dtdy, rA = c.rA;
   const T rdx = c.rdx, rdy = c.rdy;
+  if (!tile_active<TX, TY>(lam_uc, lam_vc, g, k, ox, oy, g.nx - 1, g.ny - 1, &s_ok)) return;
 
   auto tbox = [&](int i0, int j0, int w, int h) {
     Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
@@ -962,6 +985,7 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
   const int ox = blockIdx.x * TX, oy = blockIdx.y * TY;
   const T dt = c.dt, dtdx = c.dtdx, dtdy = c.dtdy, rA = c.rA;
   const T rdx = c.rdx, rdy = c.rdy;
+  if (!tile_active<TX, TY>(lam_udo, lam_vdo, g, k, ox, oy, g.nx - 1, g.ny - 1, &s_ok)) return;
 
   auto tbox = [&](int i0, int j0, int w, int h) {
     Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
@@ -1769,6 +1793,16 @@ __global__ void __launch_bounds__(64) k_remap_energy_adj(Geom g, RemapArgs ra, c
   double Lplev[LM + 2], Ltpl[LM + 2], Lpk[LM + 2], Ltpk[LM + 2], Len[LM + 2], Ler[LM + 2];
   RemapAdjWork<LM> wk;
   PPMWork<LM> wf;
+  // ud = urem and vd = vrem (:156-161); the column's energy and pressure
+  // adjoints are zero unless its new dp or pt carry an adjoint
+  bool any = false;
+  for (int k = 1; k <= L; ++k) {
+    long long ok = o + (long long)(k - 1) * S;
+    if (lam_udo[ok] != 0.) atomicAdd(lam_ur + ok, lam_udo[ok]);
+    if (lam_vdo[ok] != 0.) atomicAdd(lam_vr + ok, lam_vdo[ok]);
+    any = any || lam_dpo[ok] != 0. || lam_pto[ok] != 0.;
+  }
+  if (!any) return;
   // forward recomputation, as k_remap_energy
   plev[L + 1] = ra.ptop;
   pk[L + 1] = ra.pk_top;
@@ -1809,14 +1843,12 @@ __global__ void __launch_bounds__(64) k_remap_energy_adj(Geom g, RemapArgs ra, c
   for (int k = 0; k <= L + 1; ++k) {
     Lplev[k] = 0.; Ltpl[k] = 0.; Lpk[k] = 0.; Ltpk[k] = 0.; Len[k] = 0.; Ler[k] = 0.;
   }
-  // outputs: dp = tpl(k) - tpl(k+1), ud = urem, vd = vrem (:156-161)
+  // outputs: dp = tpl(k) - tpl(k+1) (:156-161)
   for (int k = 1; k <= L; ++k) {
     long long ok = o + (long long)(k - 1) * S;
     const double ld = lam_dpo[ok];
     Ltpl[k] += ld;
     Ltpl[k + 1] -= ld;
-    if (lam_udo[ok] != 0.) atomicAdd(lam_ur + ok, lam_udo[ok]);
-    if (lam_vdo[ok] != 0.) atomicAdd(lam_vr + ok, lam_vdo[ok]);
   }
   // pt recovery and the remapped geopotential (:130-150), reverse
   {

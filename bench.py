@@ -10,7 +10,11 @@ Workload: the seeded zonal-jet case at 1024 x 1024 x 64 (dx = 25 km,
 dt = 30 s, remap every 8 steps), synthetic data from atmdyn.ic.jet_case.
 The headline ``value`` is the FP64 form (the reference's arithmetic,
 bit-identical to the FP64 restatement); the mixed-precision form is
-measured on the same workload and reported under ``forms``.
+measured on the same workload and reported under ``forms``, and the
+gradient (forward with checkpoints + hand-written adjoint, through the
+torch.autograd binding) under ``adjoint``: fwd+adjoint cell-steps/s on the
+same workload, the backward/forward time ratio, and the finite-difference
+check of the 512 x 512 x 32 differentiation case.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -41,6 +45,7 @@ NX = NY = 1024
 NLAY = 64
 DT = 30.0
 REMAP_EVERY = 8
+ADJ_CKPT = 8
 SAMPLE_N = 256
 
 # Algorithmic HBM words per interior cell and launch of each kernel: every
@@ -267,6 +272,9 @@ def run_ours(args):
         del dy
         torch.cuda.empty_cache()
 
+    adjoint = None if args.no_adjoint else adjoint_leg(args, torch, max_over_ranks, world)
+    ensemble = None if (args.no_ensemble or world > 1) else ensemble_leg(args, torch)
+
     # error of the mixed form against the FP64 form after the same steps
     err = {}
     for name in (('dp', 'pt', 'ud', 'vd') if len(states) == 2 else ()):
@@ -278,8 +286,8 @@ def run_ours(args):
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-    f64 = results['fp64']
-    mixed = results.get('mixed')
+    f64 = results['fp64'] if 'fp64' in results else next(iter(results.values()))
+    mixed = results.get('mixed') if 'fp64' in results else None
     dom = max(f64['kernels'].items(), key=lambda kv: kv[1]['ms_avg'] * kv[1]['launches'])
     dom_name, dom_k = dom
     achieved = dom_k.get('gbs', 0.0)
@@ -307,6 +315,10 @@ def run_ours(args):
         line['forms']['mixed'] = {'value': mixed['value'], 'ms_per_step': mixed['ms_per_step'],
                                   'stable': mixed['stable'], 'speedup_vs_fp64': mixed['value'] / f64['value'],
                                   'err_vs_fp64_after_%d_steps' % (K + W): err, 'kernels': mixed['kernels']}
+    if adjoint is not None:
+        line['adjoint'] = adjoint
+    if ensemble is not None:
+        line['ensemble'] = ensemble
     if world == 1 and not args.no_cpu:
         threads = len(os.sched_getaffinity(0))
         v, t = cpu_sample_throughput(max(2, REMAP_EVERY // 2), 1, threads)
@@ -316,6 +328,202 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+P0K = 1.0e5 ** (287.052874 / 1005.0)  # theta = pt * p0**kappa
+
+
+def adjoint_leg(args, torch, max_over_ranks, world):
+    """fwd+adjoint through atmdyn.adjoint.integrate (checkpoints every
+    ADJ_CKPT steps, tapes within a segment) on the headline workload, and
+    the finite-difference check of the differentiation case: 512 x 512 x 32
+    jet (seed 2), 20 steps, checkpoints every 5, J = sum(mask theta^2) at
+    the final step with a 300 km Gaussian mask at mid-domain, central
+    differences with eps = 1e-6 along 8 seeded random unit directions."""
+    from atmdyn import ic, Dycore
+    from atmdyn.adjoint import integrate, gaussian_mask
+    out = {}
+
+    def timed(st, nsteps, remap_every, ckpt, reps):
+        dyn = Dycore(st)
+        dyn.adj_enable()
+        mask = gaussian_mask(st, 300e3, device='cuda')
+        x = [torch.tensor(np.ascontiguousarray(a), device='cuda', requires_grad=True)
+             for a in (st.dp, st.pt, st.u, st.v)]
+
+        def final_theta(fields):
+            return integrate(dyn, fields, nsteps, st.dt, remap_every, ckpt)[1] * P0K
+
+        def loss(fields):
+            return (mask * final_theta(fields) ** 2).sum()
+
+        J = loss(x)  # warm-up (tensor maps, allocator)
+        J.backward()
+        best = None
+        for _ in range(reps):
+            for xx in x:
+                xx.grad = None
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            torch.cuda.synchronize()
+            dyn.profile(True)
+            l0 = dyn.launch_count()
+            clk = Clocks()
+            ev[0].record()
+            J = loss(x)
+            ev[1].record()
+            J.backward()
+            ev[2].record()
+            torch.cuda.synchronize()
+            clocks = clk.stop()
+            tf = max_over_ranks(ev[0].elapsed_time(ev[1]))
+            tb = max_over_ranks(ev[1].elapsed_time(ev[2]))
+            if best is None or tf + tb < best[0] + best[1]:
+                prof = {k: (round(v[0], 3), v[1]) for k, v in dyn.profile_read().items() if v[1]}
+                best = (tf, tb, prof, dyn.launch_count() - l0, clocks)
+            dyn.profile(False)
+        return dyn, x, final_theta, mask, J, best
+
+    # headline workload
+    st = ic.jet_case(args.nx, args.nx, args.nlay, 25e3, 25e3, seed=0)
+    st.dt = DT
+    nsteps = args.adj_steps
+    try:
+        dyn, x, _, _, J, (tf, tb, prof, launches, clocks) = timed(st, nsteps, REMAP_EVERY, ADJ_CKPT, 2)
+        cells = st.cells
+        out['value'] = world * cells * nsteps / ((tf + tb) * 1e-3)
+        out['unit'] = 'cell-steps/s (forward + adjoint)'
+        out['workload'] = 'jet %dx%dx%d, %d steps, remap every %d, checkpoints every %d, J = sum(mask theta^2)' % (
+            args.nx, args.nx, args.nlay, nsteps, REMAP_EVERY, ADJ_CKPT)
+        out['forward_ms'] = tf
+        out['backward_ms'] = tb
+        out['backward_over_forward'] = tb / tf
+        out['stages_ms'] = prof
+        out['gpu_launches'] = launches
+        out['clocks'] = clocks
+        dyn.close()
+        del dyn, x, J
+    except Exception as e:  # e.g. the tapes do not fit
+        out['error'] = repr(e)[:300]
+    torch.cuda.empty_cache()
+    # differentiation case: finite-difference check and timing
+    def fd_check(dyn, x, final_theta, mask, gen, eps_list):
+        grad = torch.cat([xx.grad.flatten() for xx in x])
+        fd = []
+        for eps in eps_list:
+            for _ in range(8):
+                d = torch.randn(grad.numel(), generator=gen, dtype=torch.float64).cuda()
+                d /= d.norm()
+                parts = torch.split(d, [xx.numel() for xx in x])
+                with torch.no_grad():
+                    tp = final_theta([(xx + eps * q.view_as(xx)).detach() for xx, q in zip(x, parts)])
+                    tm = final_theta([(xx - eps * q.view_as(xx)).detach() for xx, q in zip(x, parts)])
+                    # J(x + eps d) - J(x - eps d) summed as mask (tp - tm)(tp + tm): no cancellation of two 1e9 sums
+                    fdv = (mask * (tp - tm) * (tp + tm)).sum().item() / (2 * eps)
+                ad = torch.dot(grad, d).item()
+                fd.append({'eps': eps, 'adjoint': ad, 'central_difference': fdv,
+                           'rel_diff': abs(fdv - ad) / max(abs(ad), 1e-300)})
+        return {'directions_per_eps': 8,
+                'max_rel_diff': {str(e): max(f['rel_diff'] for f in fd if f['eps'] == e) for e in eps_list},
+                'per_direction': fd}
+
+    st4 = ic.config(4)
+    dyn, x, final_theta, mask, J, (tf, tb, prof, launches, clocks) = timed(st4, st4.nsteps, st4.remap_every, 5, 1)
+    gen = torch.Generator(device='cpu').manual_seed(4)
+    fd_spec = fd_check(dyn, x, final_theta, mask, gen, (1e-6, 1e-3))
+    dyn.close()
+    torch.cuda.empty_cache()
+    # the same case with the exact ties of its initial state broken (uniform
+    # dp, x-independent winds, v = 0 make the limiters non-differentiable
+    # there): 0.01 Pa, 1e-4 K and 1e-3 m/s of seeded noise
+    st4n = ic.config(4)
+    rng = np.random.default_rng(40)
+    st4n.dp = st4n.dp + rng.normal(0, 0.01, st4n.dp.shape)
+    st4n.pt = st4n.pt + rng.normal(0, 1e-4 / P0K, st4n.pt.shape)
+    st4n.u = st4n.u + rng.normal(0, 1e-3, st4n.u.shape)
+    st4n.v = st4n.v + rng.normal(0, 1e-3, st4n.v.shape)
+    dyn, x, final_theta, mask, _, _ = timed(st4n, st4n.nsteps, st4n.remap_every, 5, 0)
+    fd_generic = fd_check(dyn, x, final_theta, mask, gen, (1e-6,))
+    out['differentiation_case'] = {
+        'workload': 'jet 512x512x32 (seed 2), 20 steps, dt 30 s, remap every 5, checkpoints every 5',
+        'J': J.item(), 'forward_ms': tf, 'backward_ms': tb, 'backward_over_forward': tb / tf,
+        'cell_steps_per_s': st4.cells * st4.nsteps / ((tf + tb) * 1e-3),
+        'fd_check': fd_spec,
+        'fd_check_ties_broken': fd_generic,
+        'clocks': clocks,
+    }
+    dyn.close()
+    torch.cuda.empty_cache()
+    return out
+
+
+def ensemble_leg(args, torch):
+    """The batched ensemble: 64 members of uneven sizes (grids from
+    {64, 128, 256, 512}^2, layers from {20, 32, 48, 64}, bubble or jet,
+    seed 3), mixed form, remap every 5 steps, 100 steps: CUDA-graph replay
+    of whole remap cycles over 8 streams against launching the members one
+    by one on one stream; then the gradient of J = sum(mask theta^2) of 8
+    members (FP64 form, 20 steps, checkpoints every 5)."""
+    from atmdyn import ic
+    from atmdyn.ensemble import Ensemble
+    from atmdyn.adjoint import integrate, gaussian_mask
+    from atmdyn import Dycore
+    members = ic.ensemble_members(64, seed=3)
+    out = {'members': len(members), 'cells': sum(st.cells for st in members),
+           'workload': '64 members, grids {64..512}^2 x {20..64} layers, bubble or jet (seed 3), mixed form, '
+                       'remap every 5 steps, 100 steps'}
+    nsteps = 100
+    # one stream, member after member
+    ens = Ensemble(members, 'mixed', nstreams=1)
+    ens.step_eager(5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ens.step_eager(10)
+    torch.cuda.synchronize()
+    t_seq = (time.perf_counter() - t0) / 10
+    ens.close()
+    del ens
+    torch.cuda.empty_cache()
+    # graph replay over 8 streams
+    ens = Ensemble(members, 'mixed', nstreams=8)
+    ens.step_eager(5)
+    ens.capture(5)
+    ens.replay(1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.replay(nsteps // ens.cycle)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    steps = (nsteps // ens.cycle) * ens.cycle
+    out['graph'] = {'cell_steps_per_s': out['cells'] * steps / (ms * 1e-3), 'ms_per_step': ms / steps,
+                    'steps': steps, 'streams': 8, 'graph_launches': nsteps // ens.cycle,
+                    'stable': ens.stable()}
+    out['one_stream_eager'] = {'cell_steps_per_s': out['cells'] / t_seq, 'ms_per_step': 1e3 * t_seq}
+    out['graph_speedup'] = out['graph']['cell_steps_per_s'] / out['one_stream_eager']['cell_steps_per_s']
+    ens.close()
+    del ens
+    torch.cuda.empty_cache()
+    # adjoint on 8 members
+    adj = []
+    t0 = time.perf_counter()
+    for st in members[:8]:
+        dyn = Dycore(st)
+        dyn.adj_enable()
+        mask = gaussian_mask(st, min(300e3, 0.2 * st.nx * st.dx), device='cuda')
+        x = [torch.tensor(np.ascontiguousarray(a), device='cuda', requires_grad=True)
+             for a in (st.dp, st.pt, st.u, st.v)]
+        y = integrate(dyn, x, 20, st.dt, st.remap_every, 5)
+        J = (mask * (y[1] * P0K) ** 2).sum()
+        J.backward()
+        gn = float(sum(xx.grad.norm() ** 2 for xx in x) ** 0.5)
+        adj.append({'member': st.name, 'nx': st.nx, 'nlay': st.nlay, 'J': J.item(), 'grad_norm': gn,
+                    'finite': bool(np.isfinite(gn))})
+        dyn.close()
+    torch.cuda.synchronize()
+    out['adjoint_members'] = {'count': 8, 'steps': 20, 'checkpoint_every': 5, 'wall_s': time.perf_counter() - t0,
+                              'members': adj}
+    return out
 
 
 def e2e_runs(dy, st, K, stream, torch, max_over_ranks, world):
@@ -384,6 +592,9 @@ def main():
     ap.add_argument('--nlay', type=int, default=NLAY)
     ap.add_argument('--forms', default='fp64,mixed')
     ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-adjoint', action='store_true', help='skip the forward + adjoint leg')
+    ap.add_argument('--adj-steps', type=int, default=16, help='steps of the timed forward + adjoint run')
+    ap.add_argument('--no-ensemble', action='store_true', help='skip the batched-ensemble leg')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -108,3 +108,14 @@ def test_initial_conditions_are_hydrostatic_and_seeded():
     st = ic.config(1)
     assert (st.nx, st.ny, st.nlay, st.dt, st.remap_every, st.nsteps) == (128, 128, 20, 60.0, 5, 100)
     assert st.ak[0] == 1e4 and st.bk[0] == 1.0 and st.bk[-1] == 0.0
+
+
+def test_ensemble_balance():
+    """Longest-processing-time assignment of the ensemble members to streams."""
+    from atmdyn.ensemble import balance
+    sizes = [64 ** 2 * 20, 512 ** 2 * 64, 128 ** 2 * 32, 256 ** 2 * 48, 64 ** 2 * 64, 512 ** 2 * 20, 256 ** 2 * 20]
+    b = balance(sizes, 3)
+    assert len(b) == len(sizes) and set(b) <= {0, 1, 2}
+    loads = [sum(s for s, k in zip(sizes, b) if k == j) for j in range(3)]
+    assert max(loads) <= sum(sizes) / 3 + max(sizes)
+    assert b[1] != b[5]  # the two largest members run on different streams
