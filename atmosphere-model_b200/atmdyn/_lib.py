@@ -31,7 +31,8 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_adj_enable', 'atm_adj_zero', 'atm_adj_set', 'atm_adj_get', 'atm_adj_set_device',
            'atm_adj_get_device', 'atm_adj_step', 'atm_adj_halo', 'atm_adj_cgrid_halo', 'atm_adj_cgrid_step',
            'atm_adj_dgrid_step', 'atm_adj_remap', 'atm_state_bytes', 'atm_state_save', 'atm_state_load',
-           'atm_tape_bytes', 'atm_step_tape', 'atm_adj_step_tape')
+           'atm_tape_bytes', 'atm_step_tape', 'atm_adj_step_tape', 'atm_output_enable', 'atm_output_reset',
+           'atm_accumulate_output', 'atm_output_read', 'atm_output_time')
 ATM_ADJ_IN, ATM_ADJ_OUT = 0, 1
 
 # the entry points every build must export
@@ -108,6 +109,11 @@ def load():
         'atm_tape_bytes': ([vp, ctypes.POINTER(ctypes.c_longlong)], None),
         'atm_step_tape': ([vp, d, i, vp], None),
         'atm_adj_step_tape': ([vp, d, i, vp], None),
+        'atm_output_enable': ([vp], None),
+        'atm_output_reset': ([vp], None),
+        'atm_accumulate_output': ([vp, d], None),
+        'atm_output_read': ([vp, i, P], None),
+        'atm_output_time': ([vp, P], None),
     }
     for f, (args, res) in optional.items():
         if hasattr(lib, f):

@@ -193,6 +193,24 @@ class Dycore:
         nb = dtype_bytes or (8 if isinstance(t, int) else t.element_size())
         check(self.lib.atm_download_device(self.ctx, field, ctypes.c_void_p(ptr), nb), self.ctx, 'atm_download_device')
 
+    # output accumulation on the device (accumulate_output / write_output)
+    def output_enable(self):
+        check(self.lib.atm_output_enable(self.ctx), self.ctx, 'atm_output_enable')
+
+    def output_reset(self):
+        check(self.lib.atm_output_reset(self.ctx), self.ctx, 'atm_output_reset')
+
+    def accumulate_output(self, dt):
+        check(self.lib.atm_accumulate_output(self.ctx, dt), self.ctx, 'atm_accumulate_output')
+
+    def output_read(self, name):
+        """Mean over the interval of 'dp', 'pt', 'u', 'v' or 'nflx', (K, ny, nx)."""
+        which = {'dp': 0, 'pt': 1, 'u': 2, 'v': 3, 'nflx': 4}[name]
+        K = self.nlay + 1 if name == 'nflx' else self.nlay
+        out = np.empty((K, self.ny, self.nx))
+        check(self.lib.atm_output_read(self.ctx, which, _ptr(out)), self.ctx, 'atm_output_read')
+        return out
+
     # ---- adjoint (FP64 form): hand-written reverse mode of the step
     def adj_enable(self):
         check(self.lib.atm_adj_enable(self.ctx), self.ctx, 'atm_adj_enable')

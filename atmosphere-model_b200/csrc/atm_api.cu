@@ -39,6 +39,31 @@ __global__ void k_interior(Geom g, const A* __restrict__ src, B* __restrict__ ds
   }
 }
 
+// accumulate_output (src/mod_output.f90:94-128): each sum gains dt * value
+// with the reference's operations; its compensated_sum never stores the
+// compensation, so every update is the plain FP64 add out + val.  The
+// winds are the cell-centre averages .5 (ud(j) + ud(j+1)), .5 (vd(i) + vd(i+1)).
+template <typename T>
+__global__ void k_accumulate(Geom g, const T* __restrict__ dp, const T* __restrict__ pt, const T* __restrict__ ud,
+                             const T* __restrict__ vd, const double* __restrict__ nf, double dt, double* acc_dp,
+                             double* acc_pt, double* acc_u, double* acc_v, double* acc_nf) {
+  const long long n = (long long)g.nx * g.ny;
+  const long long total = n * (g.L + 1);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(q / n);
+    const long long r = q - (long long)k * n;
+    const int j = (int)(r / g.nx), i = (int)(r - (long long)j * g.nx);
+    const long long o = g.at(i, j, k);
+    if (k < g.L) {
+      acc_dp[q] = acc_dp[q] + dt * (double)dp[o];
+      acc_pt[q] = acc_pt[q] + dt * (double)pt[o];
+      acc_u[q] = acc_u[q] + dt * .5 * ((double)ud[o] + (double)ud[o + g.P]);
+      acc_v[q] = acc_v[q] + dt * .5 * ((double)vd[o] + (double)vd[o + 1]);
+    }
+    acc_nf[q] = acc_nf[q] + dt * (nf ? nf[o] : 0.);
+  }
+}
+
 __global__ void k_fill(double* p, long long n, double v) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
     p[q] = v;
@@ -90,6 +115,10 @@ struct atm_ctx {
   double *lam_pk = nullptr, *lam_gz = nullptr, *lam_pkb = nullptr, *lam_gzb = nullptr;
   double *lam_ur = nullptr, *lam_vr = nullptr;
   int slot_in = 0;
+  // output accumulation (src/mod_output.f90:94-142): interior (nx, ny, K)
+  // sums of dt * dp, pt, u, v (nlay levels) and net_flux (nlay+1 levels)
+  double* acc[5] = {nullptr};
+  double acc_time = 0.;
   std::string err;
 };
 
@@ -147,6 +176,7 @@ void free_all(atm_ctx* c) {
   for (int f = 0; f < 4; ++f) cudaFree(c->lam_cg[f]);
   double* pl[] = {c->lam_pk, c->lam_gz, c->lam_pkb, c->lam_gzb, c->lam_ur, c->lam_vr};
   for (double* p : pl) cudaFree(p);
+  for (double* p : c->acc) cudaFree(p);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_mass) cudaFreeHost(c->h_mass);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
@@ -1116,6 +1146,69 @@ int atm_state_load(atm_ctx* ctx, const void* dev) {
   for (int i = 0; i < 4; ++i)
     CK(cudaMemcpyAsync(ctx->st[ctx->cur][i], (const char*)dev + i * f, f, cudaMemcpyDeviceToDevice, ctx->stream));
   ctx->flag_valid = false;
+  return ATM_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ output ----
+extern "C" {
+
+int atm_output_enable(atm_ctx* ctx) {
+  int r = require_init(ctx);
+  if (r) return r;
+  const size_t lay = (size_t)ctx->nx * ctx->ny * ctx->L * 8, lev = (size_t)ctx->nx * ctx->ny * (ctx->L + 1) * 8;
+  for (int f = 0; f < 5; ++f) {
+    if (!ctx->acc[f]) CK(cudaMalloc((void**)&ctx->acc[f], f < 4 ? lay : lev));
+  }
+  return atm_output_reset(ctx);
+}
+
+int atm_output_reset(atm_ctx* ctx) {
+  if (!ctx) return ATM_ERR_ARG;
+  if (!ctx->acc[0]) return fail(ctx, ATM_ERR_STATE, "atm_output_enable has not been called");
+  const size_t lay = (size_t)ctx->nx * ctx->ny * ctx->L * 8, lev = (size_t)ctx->nx * ctx->ny * (ctx->L + 1) * 8;
+  for (int f = 0; f < 5; ++f) CK(cudaMemsetAsync(ctx->acc[f], 0, f < 4 ? lay : lev, ctx->stream));
+  ctx->acc_time = 0.;
+  return ATM_OK;
+}
+
+int atm_accumulate_output(atm_ctx* ctx, double dt) {
+  int r = require_init(ctx);
+  if (r) return r;
+  if (!ctx->acc[0]) return fail(ctx, ATM_ERR_STATE, "atm_output_enable has not been called");
+  void* const* s = ctx->st[ctx->cur];
+  const double* nf = ctx->heating ? ctx->nf : nullptr;
+  if (ctx->precision == ATM_FP64)
+    k_accumulate<double><<<1184, 256, 0, ctx->stream>>>(ctx->geo, (const double*)s[F_DP], (const double*)s[F_PT],
+                                                         (const double*)s[F_UD], (const double*)s[F_VD], nf, dt,
+                                                         ctx->acc[0], ctx->acc[1], ctx->acc[2], ctx->acc[3],
+                                                         ctx->acc[4]);
+  else
+    k_accumulate<float><<<1184, 256, 0, ctx->stream>>>(ctx->geo, (const float*)s[F_DP], (const float*)s[F_PT],
+                                                        (const float*)s[F_UD], (const float*)s[F_VD], nf, dt,
+                                                        ctx->acc[0], ctx->acc[1], ctx->acc[2], ctx->acc[3], ctx->acc[4]);
+  CK(cudaGetLastError());
+  ctx->launches += 1;
+  ctx->acc_time = ctx->acc_time + dt;
+  return ATM_OK;
+}
+
+int atm_output_read(atm_ctx* ctx, int which, double* host) {
+  if (!ctx || !host || which < 0 || which > 4) return ATM_ERR_ARG;
+  if (!ctx->acc[0]) return fail(ctx, ATM_ERR_STATE, "atm_output_enable has not been called");
+  const size_t n = (size_t)ctx->nx * ctx->ny * (which < 4 ? ctx->L : ctx->L + 1);
+  CK(cudaMemcpyAsync(host, ctx->acc[which], n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  // write_output (src/mod_output.f90:152): output_field / accumulation_time
+  const double t = ctx->acc_time;
+  for (size_t q = 0; q < n; ++q) host[q] = host[q] / t;
+  return ATM_OK;
+}
+
+int atm_output_time(atm_ctx* ctx, double* t) {
+  if (!ctx || !t) return ATM_ERR_ARG;
+  *t = ctx->acc_time;
   return ATM_OK;
 }
 

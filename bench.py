@@ -405,6 +405,8 @@ def adjoint_leg(args, torch, max_over_ranks, world):
     except Exception as e:  # e.g. the tapes do not fit
         out['error'] = repr(e)[:300]
     torch.cuda.empty_cache()
+    if args.no_fdcheck:
+        return out
     # differentiation case: finite-difference check and timing
     def fd_check(dyn, x, final_theta, mask, gen, eps_list):
         grad = torch.cat([xx.grad.flatten() for xx in x])
@@ -595,6 +597,7 @@ def main():
     ap.add_argument('--no-adjoint', action='store_true', help='skip the forward + adjoint leg')
     ap.add_argument('--adj-steps', type=int, default=16, help='steps of the timed forward + adjoint run')
     ap.add_argument('--no-ensemble', action='store_true', help='skip the batched-ensemble leg')
+    ap.add_argument('--no-fdcheck', action='store_true', help='skip the differentiation case of the adjoint leg')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -254,6 +254,22 @@ int atm_state_bytes(atm_ctx* ctx, long long* bytes);
 int atm_state_save(atm_ctx* ctx, void* dev);
 int atm_state_load(atm_ctx* ctx, const void* dev);
 
+/* ---- output accumulation on the device (accumulate_output / write_output,
+   src/mod_output.f90:94-176) ----
+   atm_accumulate_output(ctx, dt) adds dt * (dp, pt, u, v, net_flux) of the
+   current state to device sums, with u, v the cell-centre averages of the
+   D-grid winds, exactly as the reference (whose compensated sum keeps no
+   compensation: plain FP64 adds); atm_output_read returns one mean (sum /
+   accumulated time) as a host (nlay or nlay+1, ny, nx) array, field
+   ATM_OUT_DP..ATM_OUT_NFLX; atm_output_reset starts a new interval.  The
+   surface temperature ts is a physics field and stays with the caller. */
+enum { ATM_OUT_DP = 0, ATM_OUT_PT = 1, ATM_OUT_U = 2, ATM_OUT_V = 3, ATM_OUT_NFLX = 4 };
+int atm_output_enable(atm_ctx* ctx);
+int atm_output_reset(atm_ctx* ctx);
+int atm_accumulate_output(atm_ctx* ctx, double dt);
+int atm_output_read(atm_ctx* ctx, int which, double* host);
+int atm_output_time(atm_ctx* ctx, double* t);
+
 /* library version string */
 const char* atm_version(void);
 
