@@ -9,11 +9,19 @@
 namespace atm {
 namespace {
 
-constexpr int TXA = 32, TYA = 8;
+// tile of the mass adjoints (TXA x TYA) and of the momentum adjoints
+// (TXA x TYM)
+#ifndef ATM_ADJ_TYA
+#define ATM_ADJ_TYA 8
+#endif
+#ifndef ATM_ADJ_TYM
+#define ATM_ADJ_TYM 4
+#endif
+constexpr int TXA = 32, TYA = ATM_ADJ_TYA, TYM = ATM_ADJ_TYM;
 
-inline dim3 tiles_a(int lo, int hi, const Geom& g) {
+inline dim3 tiles_a(int lo, int hi, const Geom& g, int ty) {
   int w = g.nx - lo + hi, h = g.ny - lo + hi;
-  return dim3((w + TXA - 1) / TXA, (h + TYA - 1) / TYA, g.L);
+  return dim3((w + TXA - 1) / TXA, (h + ty - 1) / ty, g.L);
 }
 
 template <typename K>
@@ -27,8 +35,8 @@ cudaError_t adj_setup() {
   cudaError_t e;
   if ((e = smem_attr(k_mass_adj<TXA, TYA, true>, MassAdjL<TXA, TYA, true>::bytes))) return e;
   if ((e = smem_attr(k_mass_adj<TXA, TYA, false>, MassAdjL<TXA, TYA, false>::bytes))) return e;
-  if ((e = smem_attr(k_c_mom_adj<TXA, TYA>, CMomAdjL<TXA, TYA>::bytes))) return e;
-  if ((e = smem_attr(k_d_mom_adj<TXA, TYA>, DMomAdjL<TXA, TYA>::bytes))) return e;
+  if ((e = smem_attr(k_c_mom_adj<TXA, TYM>, CMomAdjL<TXA, TYM>::bytes))) return e;
+  if ((e = smem_attr(k_d_mom_adj<TXA, TYM>, DMomAdjL<TXA, TYM>::bytes))) return e;
   return cudaSuccess;
 }
 
@@ -42,14 +50,14 @@ cudaError_t adj_mass(const Geom& g, const Consts& c, const double* dp, const dou
     if ((e = tmap(dp, 8, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, 8, g, g.L, Lay::WD, Lay::HD, &mp)) ||
         (e = tmap(u, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, 8, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
-    k_mass_adj<TXA, TYA, true><<<tiles_a(lo, hi, g), NTA, MassAdjL<TXA, TYA, true>::bytes, s>>>(
+    k_mass_adj<TXA, TYA, true><<<tiles_a(lo, hi, g, TYA), NTA, MassAdjL<TXA, TYA, true>::bytes, s>>>(
         md, mp, mu, mv, g, c, lam_dpo, lam_pto, lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
   } else {
     using Lay = MassL<double, TXA, TYA, false>;
     if ((e = tmap(dp, 8, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, 8, g, g.L, Lay::WD, Lay::HD, &mp)) ||
         (e = tmap(u, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, 8, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
-    k_mass_adj<TXA, TYA, false><<<tiles_a(lo, hi, g), NTA, MassAdjL<TXA, TYA, false>::bytes, s>>>(
+    k_mass_adj<TXA, TYA, false><<<tiles_a(lo, hi, g, TYA), NTA, MassAdjL<TXA, TYA, false>::bytes, s>>>(
         md, mp, mu, mv, g, c, lam_dpo, lam_pto, lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
   }
   return cudaGetLastError();
@@ -58,14 +66,14 @@ cudaError_t adj_mass(const Geom& g, const Consts& c, const double* dp, const dou
 cudaError_t adj_c_mom(const Geom& g, const Consts& c, const double* ud, const double* vd, const double* pkap,
                       const double* gz, const double* lam_uc, const double* lam_vc, double* lam_ud, double* lam_vd,
                       double* lam_pk, double* lam_gz, int* timeout, cudaStream_t s) {
-  using Lay = CMomL<double, TXA, TYA>;
+  using Lay = CMomL<double, TXA, TYM>;
   CUtensorMap mu, mv, muL, mvL, mpk, mgz;
   cudaError_t e;
   if ((e = tmap(ud, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, 8, g, g.L, Lay::WV, Lay::HV, &mv)) ||
       (e = tmap(ud, 8, g, g.L, Lay::WL, Lay::HL, &muL)) || (e = tmap(vd, 8, g, g.L, Lay::WL, Lay::HL, &mvL)) ||
       (e = tmap(pkap, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpk)) || (e = tmap(gz, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgz)))
     return e;
-  k_c_mom_adj<TXA, TYA><<<tiles_a(0, 0, g), NTA, CMomAdjL<TXA, TYA>::bytes, s>>>(
+  k_c_mom_adj<TXA, TYM><<<tiles_a(0, 0, g, TYM), NTA, CMomAdjL<TXA, TYM>::bytes, s>>>(
       mu, mv, muL, mvL, mpk, mgz, g, c, lam_uc, lam_vc, lam_ud, lam_vd, lam_pk, lam_gz, timeout);
   return cudaGetLastError();
 }
@@ -74,7 +82,7 @@ cudaError_t adj_d_mom(const Geom& g, const Consts& c, const double* ud, const do
                       const double* vc, const double* pkapb, const double* gzb, const double* lam_udo,
                       const double* lam_vdo, double* lam_ud, double* lam_vd, double* lam_uc, double* lam_vc,
                       double* lam_pkb, double* lam_gzb, int* timeout, cudaStream_t s) {
-  using Lay = DMomL<double, TXA, TYA>;
+  using Lay = DMomL<double, TXA, TYM>;
   CUtensorMap mu, mv, muL, mvL, muc, mvc, mpb, mgb;
   cudaError_t e;
   if ((e = tmap(ud, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, 8, g, g.L, Lay::WU, Lay::HU, &mv)) ||
@@ -82,7 +90,7 @@ cudaError_t adj_d_mom(const Geom& g, const Consts& c, const double* ud, const do
       (e = tmap(uc, 8, g, g.L, Lay::WC, Lay::HC, &muc)) || (e = tmap(vc, 8, g, g.L, Lay::WC, Lay::HC, &mvc)) ||
       (e = tmap(pkapb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpb)) || (e = tmap(gzb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgb)))
     return e;
-  k_d_mom_adj<TXA, TYA><<<tiles_a(0, 0, g), NTA, DMomAdjL<TXA, TYA>::bytes, s>>>(
+  k_d_mom_adj<TXA, TYM><<<tiles_a(0, 0, g, TYM), NTA, DMomAdjL<TXA, TYM>::bytes, s>>>(
       mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c, lam_udo, lam_vdo, lam_ud, lam_vd, lam_uc, lam_vc, lam_pkb, lam_gzb,
       timeout);
   return cudaGetLastError();
