@@ -18,7 +18,8 @@
   record dimension ``t``, FP32 data by default (``dtype='f8'`` keeps FP64).
 
 netCDF-3 classic through ``scipy.io.netcdf_file`` (no netCDF library is
-needed).
+needed); netCDF-4/HDF5 files (xarray's default format) need the netCDF
+library, which this image does not have.
 """
 from __future__ import annotations
 
@@ -33,9 +34,6 @@ from .model import TimeControl, NEVER
 
 
 # ------------------------------------------------------------- namelist ----
-_GROUP = re.compile(r'&(\w+)(.*?)(?:^\s*/\s*$|/\s*$)', re.S | re.M)
-
-
 def _strip_comment(line):
     out, q = [], None
     for ch in line:
@@ -236,10 +234,12 @@ def read_initial(path: str, config: Config | None = None) -> InitialState:
 
 
 def write_initial(path: str, st: InitialState, ts=None, t0: float = 0.0):
-    """An initial-conditions file in the layout of the reference's generator
-    (variables over (yc, xc, lay, t))."""
+    """An initial-conditions file with the variables and dimension order of
+    the reference's generator (variables over (yc, xc, lay, t)).  netCDF-3
+    allows a record dimension only in first place, so ``t`` is a fixed
+    dimension of length 1 here; the reference reads it by name either way."""
     with netcdf_file(path, 'w') as nc:
-        nc.createDimension('t', None)
+        nc.createDimension('t', 1)
         for n, size in (('xc', st.nx), ('yc', st.ny), ('xf', st.nx), ('yf', st.ny), ('lay', st.nlay),
                         ('lev', st.nlay + 1)):
             nc.createDimension(n, size)

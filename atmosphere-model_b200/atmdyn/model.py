@@ -86,10 +86,13 @@ class RunResult:
 
 
 def run_model(stepper, tc: TimeControl, max_steps: int | None = None,
-              on_step=None) -> RunResult:
+              on_step=None, accumulate=None, write=None) -> RunResult:
     """The dycore part of ``run_model`` (mod_model.f90:112-193): each step is
     C-grid half step, halo, D-grid step, remap if due, halo, stability
-    check.  Radiation (net_flux) and physics tendencies are not computed."""
+    check, then ``accumulate(dt)`` (accumulate_output) and, when the
+    schedule says so, ``write(time_stamp)`` (write_output, stamped
+    .5 (previous_write_time + time) as the reference does).  Radiation
+    (net_flux) and physics tendencies are not computed."""
     sch = Schedule(tc)
     time = tc.t_initial
     n = 0
@@ -112,7 +115,12 @@ def run_model(stepper, tc: TimeControl, max_steps: int | None = None,
         if not stable:
             break
         time = time + dt
-        sch.write_this_step = False
+        if accumulate is not None:
+            accumulate(dt)
+        if sch.write_this_step:
+            if write is not None:
+                write(.5 * (sch.previous_write_time + time))
+            sch.write_this_step = False
         if on_step is not None:
             on_step(n, time)
         if max_steps is not None and n >= max_steps:
