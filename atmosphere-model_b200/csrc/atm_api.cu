@@ -296,7 +296,8 @@ int atm_create(atm_ctx** out, int nx, int ny, int nlay, double dx, double dy, co
   };
   for (int t = 0; t < 2; ++t)
     for (int fi = 0; fi < 4; ++fi) alloc(&ctx->st[t][fi], lay);
-  for (int fi = 0; fi < 4; ++fi) alloc(&ctx->cg[fi], lay);
+  const size_t lay_cg = level_elems(ctx) * nlay * (size_t)ctx->ops->cg_elem;
+  for (int fi = 0; fi < 4; ++fi) alloc(&ctx->cg[fi], lay_cg);
   alloc(&ctx->urem, lay);
   alloc(&ctx->vrem, lay);
   alloc((void**)&ctx->pkap, lev);
@@ -354,7 +355,7 @@ int atm_upload(atm_ctx* ctx, int field, const double* host) {
   const atm::Ops& ops = *ctx->ops;
   if (field >= ATM_DP && field <= ATM_VD) {
     void* dst = ctx->st[ctx->cur][field];
-    if (ctx->precision == ATM_FP64) {
+    if (ops.elem == 8) {
       CK(h2d_pitched(ctx, (double*)dst, host, ctx->L));
     } else {
       CK(h2d_pitched(ctx, ctx->stage, host, ctx->L));
@@ -376,7 +377,7 @@ int atm_upload_device(atm_ctx* ctx, int field, const void* dev, int dtype_bytes)
   if (!ctx || !dev || (dtype_bytes != 4 && dtype_bytes != 8)) return ATM_ERR_ARG;
   if (field < ATM_DP || field > ATM_GZ) return fail(ctx, ATM_ERR_ARG, "field cannot be uploaded");
   const int K = field == ATM_GZ ? 1 : ctx->L;
-  const bool dbl_field = field == ATM_GZ || ctx->precision == ATM_FP64;
+  const bool dbl_field = field == ATM_GZ || ctx->ops->elem == 8;
   void* dst = field == ATM_GZ ? (void*)ctx->gz : ctx->st[ctx->cur][field];
   dim3 grid(1184), block(256);
   if (dbl_field && dtype_bytes == 8) k_interior<double, double><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const double*)dev, (double*)dst, K, 1);
@@ -400,7 +401,7 @@ int atm_upload_device(atm_ctx* ctx, int field, const void* dev, int dtype_bytes)
 int atm_download_device(atm_ctx* ctx, int field, void* dev, int dtype_bytes) {
   if (!ctx || !dev || (dtype_bytes != 4 && dtype_bytes != 8)) return ATM_ERR_ARG;
   if (field < ATM_DP || field > ATM_VD) return fail(ctx, ATM_ERR_ARG, "only prognostic fields");
-  const bool dbl_field = ctx->precision == ATM_FP64;
+  const bool dbl_field = ctx->ops->elem == 8;
   const void* src = ctx->st[ctx->cur][field];
   dim3 grid(1184), block(256);
   if (dbl_field && dtype_bytes == 8) k_interior<double, double><<<grid, block, 0, ctx->stream>>>(ctx->geo, (const double*)src, (double*)dev, ctx->L, 0);
@@ -418,7 +419,7 @@ int atm_download(atm_ctx* ctx, int field, double* host) {
   if (K < 0) return fail(ctx, ATM_ERR_ARG, "unknown field");
   if ((field >= ATM_DP && field <= ATM_VD) || (field >= ATM_DPC && field <= ATM_VC)) {
     const void* src = field <= ATM_VD ? ctx->st[ctx->cur][field] : ctx->cg[field - ATM_DPC];
-    if (ctx->precision == ATM_FP64) {
+    if ((field <= ATM_VD ? ops.elem : ops.cg_elem) == 8) {
       CK(d2h_pitched(ctx, host, (const double*)src, K));
     } else {
       CK(ops.to_double(src, ctx->stage, ctx->geo.S * K, ctx->stream));
@@ -436,7 +437,7 @@ int atm_download(atm_ctx* ctx, int field, double* host) {
     int r = require_init(ctx);
     if (r) return r;
     atm::Consts k = step_consts(ctx, 0.);
-    CK(ops.column(ctx->geo, k, ctx->st[ctx->cur][F_DP], ctx->st[ctx->cur][F_PT], ctx->pkap, ctx->gz, -H, H,
+    CK(ops.column(ctx->geo, k, ctx->st[ctx->cur][F_DP], ctx->st[ctx->cur][F_PT], ops.elem, ctx->pkap, ctx->gz, -H, H,
                   ctx->stage, ctx->stream));
     const double* src = field == ATM_PLEV ? ctx->stage : field == ATM_PKAP ? ctx->pkap : ctx->gz;
     CK(d2h_pitched(ctx, host, src, K));
@@ -497,7 +498,7 @@ int atm_cgrid_step(atm_ctx* ctx, double dt_half) {
   const double* heat = nullptr;
   if (ctx->heating) {
     Stage t(ctx, S_HEAT);
-    CK(ops.heating(g, k, s[F_DP], ctx->nf, ctx->heat, ctx->stream));
+    CK(ops.heating(g, k, s[F_DP], ops.elem, ctx->nf, ctx->heat, ctx->stream));
     heat = ctx->heat;
   }
   // dpc, ptc on is+5:ie-5 (src/mod_sw_dyn.f90:94-270)
@@ -509,7 +510,7 @@ int atm_cgrid_step(atm_ctx* ctx, double dt_half) {
   // plev, pkap, gz (src/mod_sw_dyn.f90:276-292)
   {
     Stage t(ctx, S_CCOL);
-    CK(ops.column(g, k, ctx->cg[C_DPC], ctx->cg[C_PTC], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+    CK(ops.column(g, k, ctx->cg[C_DPC], ctx->cg[C_PTC], ops.cg_elem, ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
   }
   // uc, vc (src/mod_sw_dyn.f90:294-414)
   {
@@ -524,7 +525,7 @@ int atm_cgrid_halo(atm_ctx* ctx) {
   int r = require_init(ctx);
   if (r) return r;
   Stage t(ctx, S_CHALO);
-  CK(ctx->ops->ring(ctx->geo, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
+  CK(ctx->ops->ring_cg(ctx->geo, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
   return ATM_OK;
 }
 
@@ -540,7 +541,7 @@ int atm_dgrid_step(atm_ctx* ctx, double dt) {
   const double* heat = nullptr;
   if (ctx->heating) {
     Stage t(ctx, S_HEAT);
-    CK(ops.heating(g, k, ctx->cg[C_DPC], ctx->nf, ctx->heat, ctx->stream));  // from dpc, :433-464
+    CK(ops.heating(g, k, ctx->cg[C_DPC], ops.cg_elem, ctx->nf, ctx->heat, ctx->stream));  // from dpc, :433-464
     heat = ctx->heat;
   }
   // the new time level keeps the old halo until the D-grid halo exchange
@@ -558,7 +559,7 @@ int atm_dgrid_step(atm_ctx* ctx, double dt) {
   // plev, pkap, gz, pkapb, gzb (src/mod_sw_dyn.f90:606-632)
   {
     Stage t(ctx, S_DCOL);
-    CK(ops.column(g, k, sn[F_DP], sn[F_PT], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+    CK(ops.column(g, k, sn[F_DP], sn[F_PT], ops.elem, ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
   }
   {
     Stage t(ctx, S_DCORN);
@@ -780,7 +781,7 @@ int fwd_c(atm_ctx* ctx, double dt_half, void* const* s) {
   atm::Consts k = step_consts(ctx, dt_half);
   CK(ops.mass(g, k, s[F_DP], s[F_PT], s[F_UD], s[F_VD], nullptr, ctx->cg[C_DPC], ctx->cg[C_PTC], -2, 2, nullptr,
               &ctx->status->tma_timeout, true, ctx->stream));
-  CK(ops.column(g, k, ctx->cg[C_DPC], ctx->cg[C_PTC], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+  CK(ops.column(g, k, ctx->cg[C_DPC], ctx->cg[C_PTC], ops.cg_elem, ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
   CK(ops.c_mom(g, k, s[F_UD], s[F_VD], ctx->pkap, ctx->gz, ctx->cg[C_UC], ctx->cg[C_VC], &ctx->status->tma_timeout,
                ctx->stream));
   ctx->launches += 3;
@@ -795,7 +796,7 @@ int fwd_d(atm_ctx* ctx, double dt, void* const* so, void* const* sn) {
   CK(ops.ring(g, sn, (const void* const*)so, 4, ctx->L, true, ctx->stream));
   CK(ops.mass(g, k, so[F_DP], so[F_PT], ctx->cg[C_UC], ctx->cg[C_VC], nullptr, sn[F_DP], sn[F_PT], -3, 3,
               &ctx->status->nonfinite_step, &ctx->status->tma_timeout, false, ctx->stream));
-  CK(ops.column(g, k, sn[F_DP], sn[F_PT], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+  CK(ops.column(g, k, sn[F_DP], sn[F_PT], ops.elem, ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
   CK(atm::corners(g, ctx->pkap, ctx->gz, ctx->pkapb, ctx->gzb, 1, 0, ctx->L, ctx->stream));
   CK(ops.d_mom(g, k, so[F_UD], so[F_VD], ctx->cg[C_UC], ctx->cg[C_VC], ctx->pkapb, ctx->gzb, sn[F_UD], sn[F_VD],
                &ctx->status->nonfinite_step, &ctx->status->tma_timeout, ctx->stream));
@@ -811,7 +812,8 @@ int adj_c(atm_ctx* ctx, double dt_half, void* const* s, double* const* lin, cons
   const double* const* cg = (const double* const*)cgf;
   {
     Stage t(ctx, S_ACCOL, 2);
-    CK(ctx->ops->column(g, k, cg[C_DPC], cg[C_PTC], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+    CK(ctx->ops->column(g, k, cg[C_DPC], cg[C_PTC], ctx->ops->cg_elem, ctx->pkap, ctx->gz, -2, 2, nullptr,
+                        ctx->stream));
     CK(cudaMemsetAsync(ctx->lam_pk, 0, (size_t)g.S * (ctx->L + 1) * 8, ctx->stream));
     CK(cudaMemsetAsync(ctx->lam_gz, 0, (size_t)g.S * (ctx->L + 1) * 8, ctx->stream));
   }
@@ -1016,7 +1018,7 @@ int atm_adj_dgrid_step(atm_ctx* ctx, double dt) {
   {
     Stage t(ctx, S_AFWD, 1);
     if ((r = fwd_c(ctx, dt / 2., ctx->st[cur]))) return r;
-    CK(ctx->ops->ring(ctx->geo, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
+    CK(ctx->ops->ring_cg(ctx->geo, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
     if ((r = fwd_d(ctx, dt, ctx->st[cur], ctx->st[1 - cur]))) return r;
   }
   return adj_d(ctx, dt, (const void* const*)ctx->st[cur], (const void* const*)ctx->st[1 - cur],
@@ -1075,7 +1077,7 @@ int atm_adj_step(atm_ctx* ctx, double dt, int do_remap) {
   {
     Stage t(ctx, S_AFWD, 1);
     if ((r = fwd_c(ctx, dt / 2., ctx->st[cur]))) return r;
-    CK(ctx->ops->ring(g, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
+    CK(ctx->ops->ring_cg(g, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
     if ((r = fwd_d(ctx, dt, ctx->st[cur], ctx->st[nxt]))) return r;
   }
   return adj_step_given(ctx, dt, do_remap, (const void* const*)ctx->cg, (const void* const*)ctx->st[nxt]);
@@ -1120,7 +1122,7 @@ int atm_adj_step_tape(atm_ctx* ctx, double dt, int do_remap, const void* tape) {
   {  // pkapb, gzb of the D step from its new dp, pt
     Stage st(ctx, S_AFWD, 2);
     atm::Consts k = step_consts(ctx, dt);
-    CK(ctx->ops->column(g, k, s1[F_DP], s1[F_PT], ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
+    CK(ctx->ops->column(g, k, s1[F_DP], s1[F_PT], ctx->ops->elem, ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
     CK(atm::corners(g, ctx->pkap, ctx->gz, ctx->pkapb, ctx->gzb, 1, 0, ctx->L, ctx->stream));
   }
   return adj_step_given(ctx, dt, do_remap, cgf, s1);
@@ -1179,7 +1181,7 @@ int atm_accumulate_output(atm_ctx* ctx, double dt) {
   if (!ctx->acc[0]) return fail(ctx, ATM_ERR_STATE, "atm_output_enable has not been called");
   void* const* s = ctx->st[ctx->cur];
   const double* nf = ctx->heating ? ctx->nf : nullptr;
-  if (ctx->precision == ATM_FP64)
+  if (ctx->ops->elem == 8)
     k_accumulate<double><<<1184, 256, 0, ctx->stream>>>(ctx->geo, (const double*)s[F_DP], (const double*)s[F_PT],
                                                          (const double*)s[F_UD], (const double*)s[F_VD], nf, dt,
                                                          ctx->acc[0], ctx->acc[1], ctx->acc[2], ctx->acc[3],

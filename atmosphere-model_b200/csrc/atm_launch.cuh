@@ -11,7 +11,9 @@
 namespace atm {
 namespace {
 
-using T = ATM_FORM_T;
+using T = ATM_FORM_T;  // sweep arithmetic
+using S = double;      // prognostic state (dp, pt, ud, vd), both forms
+using C = T;           // C-grid fields (dpc, ptc, uc, vc)
 constexpr int TX = 32, TY = 8;
 
 inline dim3 tiles(int lo, int hi, const Geom& g, int layers) {
@@ -26,10 +28,11 @@ cudaError_t smem_attr(K kernel, size_t bytes) {
 
 cudaError_t setup() {
   cudaError_t e;
-  if ((e = smem_attr(k_mass2<T, TX, TY, true>, MassL<T, TX, TY, true>::bytes)) != cudaSuccess) return e;
-  if ((e = smem_attr(k_mass2<T, TX, TY, false>, MassL<T, TX, TY, false>::bytes)) != cudaSuccess) return e;
-  if ((e = smem_attr(k_c_mom2<T, TX, TY>, CMomL<T, TX, TY>::bytes)) != cudaSuccess) return e;
-  if ((e = smem_attr(k_d_mom2<T, TX, TY>, DMomL<T, TX, TY>::bytes)) != cudaSuccess) return e;
+  if ((e = smem_attr(k_mass2<T, TX, TY, true, S, C>, MassL<T, TX, TY, true, S, C>::bytes)) != cudaSuccess) return e;
+  if ((e = smem_attr(k_mass2<T, TX, TY, false, S, C>, MassL<T, TX, TY, false, S, C>::bytes)) != cudaSuccess)
+    return e;
+  if ((e = smem_attr(k_c_mom2<T, TX, TY, S, C>, CMomL<T, TX, TY, S>::bytes)) != cudaSuccess) return e;
+  if ((e = smem_attr(k_d_mom2<T, TX, TY, S, C>, DMomL<T, TX, TY, S, C>::bytes)) != cudaSuccess) return e;
   return cudaSuccess;
 }
 
@@ -37,94 +40,113 @@ cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt,
                  const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, int* timeout, bool cgrid,
                  cudaStream_t s) {
   dim3 grid = tiles(lo, hi, g, g.L);
-  constexpr int es = sizeof(T);
   CUtensorMap md, mp, mu, mv;
   cudaError_t e;
-  if (cgrid) {
-    using Lay = MassL<T, TX, TY, true>;
-    if ((e = tmap(dp, es, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, es, g, g.L, Lay::WD, Lay::HD, &mp)) ||
-        (e = tmap(u, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, es, g, g.L, Lay::WV, Lay::HV, &mv)))
+  if (cgrid) {  // state in, C-grid fields out
+    using Lay = MassL<T, TX, TY, true, S, C>;
+    constexpr int eu = sizeof(typename Lay::UB);
+    if ((e = tmap(dp, sizeof(S), g, g.L, Lay::WD, Lay::HD, &md)) ||
+        (e = tmap(pt, sizeof(S), g, g.L, Lay::WD, Lay::HD, &mp)) || (e = tmap(u, eu, g, g.L, Lay::WU, Lay::HU, &mu)) ||
+        (e = tmap(v, eu, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
-    k_mass2<T, TX, TY, true><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (T*)dpo, (T*)pto, lo, hi,
-                                                          nonfinite, timeout);
-  } else {
-    using Lay = MassL<T, TX, TY, false>;
-    if ((e = tmap(dp, es, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, es, g, g.L, Lay::WD, Lay::HD, &mp)) ||
-        (e = tmap(u, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, es, g, g.L, Lay::WV, Lay::HV, &mv)))
+    k_mass2<T, TX, TY, true, S, C><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (C*)dpo, (C*)pto, lo,
+                                                                 hi, nonfinite, timeout);
+  } else {  // state and C-grid winds in, state out
+    using Lay = MassL<T, TX, TY, false, S, C>;
+    constexpr int eu = sizeof(typename Lay::UB);
+    if ((e = tmap(dp, sizeof(S), g, g.L, Lay::WD, Lay::HD, &md)) ||
+        (e = tmap(pt, sizeof(S), g, g.L, Lay::WD, Lay::HD, &mp)) || (e = tmap(u, eu, g, g.L, Lay::WU, Lay::HU, &mu)) ||
+        (e = tmap(v, eu, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
-    k_mass2<T, TX, TY, false><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (T*)dpo, (T*)pto, lo, hi,
-                                                           nonfinite, timeout);
+    k_mass2<T, TX, TY, false, S, C><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (S*)dpo, (S*)pto, lo,
+                                                                  hi, nonfinite, timeout);
   }
   return cudaGetLastError();
 }
 
-cudaError_t column(const Geom& g, const Consts& c, const void* dpl, const void* ptl, double* pkap, double* gz, int lo,
-                   int hi, double* plev, cudaStream_t s) {
+cudaError_t column(const Geom& g, const Consts& c, const void* dpl, const void* ptl, int es, double* pkap, double* gz,
+                   int lo, int hi, double* plev, cudaStream_t s) {
   int n = (g.nx - lo + hi) * (g.ny - lo + hi);
-  k_column<T><<<(n + 127) / 128, 128, 0, s>>>(g, c, (const T*)dpl, (const T*)ptl, pkap, gz, lo, hi, plev);
+  if (es == 8)
+    k_column<double><<<(n + 127) / 128, 128, 0, s>>>(g, c, (const double*)dpl, (const double*)ptl, pkap, gz, lo, hi,
+                                                     plev);
+  else
+    k_column<float><<<(n + 127) / 128, 128, 0, s>>>(g, c, (const float*)dpl, (const float*)ptl, pkap, gz, lo, hi,
+                                                    plev);
   return cudaGetLastError();
 }
 
-cudaError_t heating(const Geom& g, const Consts& c, const void* dpl, const double* nf, double* heat, cudaStream_t s) {
+cudaError_t heating(const Geom& g, const Consts& c, const void* dpl, int es, const double* nf, double* heat,
+                    cudaStream_t s) {
   int n = (g.nx + 2 * H) * g.NYP;
-  k_heating<T><<<(n + 63) / 64, 64, 0, s>>>(g, c, (const T*)dpl, nf, heat);
+  if (es == 8) k_heating<double><<<(n + 63) / 64, 64, 0, s>>>(g, c, (const double*)dpl, nf, heat);
+  else k_heating<float><<<(n + 63) / 64, 64, 0, s>>>(g, c, (const float*)dpl, nf, heat);
   return cudaGetLastError();
 }
 
 cudaError_t c_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const double* pkap, const double* gz,
                   void* uc, void* vc, int* timeout, cudaStream_t s) {
-  using Lay = CMomL<T, TX, TY>;
-  constexpr int es = sizeof(T);
+  using Lay = CMomL<T, TX, TY, S>;
+  constexpr int es = sizeof(S);
   CUtensorMap mu, mv, muL, mvL, mpk, mgz;
   cudaError_t e;
   if ((e = tmap(ud, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, es, g, g.L, Lay::WV, Lay::HV, &mv)) ||
       (e = tmap(ud, es, g, g.L, Lay::WL, Lay::HL, &muL)) || (e = tmap(vd, es, g, g.L, Lay::WL, Lay::HL, &mvL)) ||
       (e = tmap(pkap, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpk)) || (e = tmap(gz, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgz)))
     return e;
-  k_c_mom2<T, TX, TY><<<tiles(0, 0, g, g.L), NT, Lay::bytes, s>>>(mu, mv, muL, mvL, mpk, mgz, g, c, (T*)uc, (T*)vc,
-                                                                  timeout);
+  k_c_mom2<T, TX, TY, S, C><<<tiles(0, 0, g, g.L), NT, Lay::bytes, s>>>(mu, mv, muL, mvL, mpk, mgz, g, c, (C*)uc,
+                                                                        (C*)vc, timeout);
   return cudaGetLastError();
 }
 
 cudaError_t d_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const void* uc, const void* vc,
                   const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, int* timeout,
                   cudaStream_t s) {
-  using Lay = DMomL<T, TX, TY>;
-  constexpr int es = sizeof(T);
+  using Lay = DMomL<T, TX, TY, S, C>;
+  constexpr int es = sizeof(S), ec = sizeof(C);
   CUtensorMap mu, mv, muL, mvL, muc, mvc, mpb, mgb;
   cudaError_t e;
   if ((e = tmap(ud, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, es, g, g.L, Lay::WU, Lay::HU, &mv)) ||
-      (e = tmap(uc, es, g, g.L, Lay::WUL, Lay::HUL, &muL)) || (e = tmap(vc, es, g, g.L, Lay::WVL, Lay::HVL, &mvL)) ||
-      (e = tmap(uc, es, g, g.L, Lay::WC, Lay::HC, &muc)) || (e = tmap(vc, es, g, g.L, Lay::WC, Lay::HC, &mvc)) ||
+      (e = tmap(uc, ec, g, g.L, Lay::WUL, Lay::HUL, &muL)) || (e = tmap(vc, ec, g, g.L, Lay::WVL, Lay::HVL, &mvL)) ||
+      (e = tmap(uc, ec, g, g.L, Lay::WC, Lay::HC, &muc)) || (e = tmap(vc, ec, g, g.L, Lay::WC, Lay::HC, &mvc)) ||
       (e = tmap(pkapb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpb)) || (e = tmap(gzb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgb)))
     return e;
-  k_d_mom2<T, TX, TY><<<tiles(0, 0, g, g.L), NT, Lay::bytes, s>>>(mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c,
-                                                                  (T*)udo, (T*)vdo, nonfinite, timeout);
+  k_d_mom2<T, TX, TY, S, C><<<tiles(0, 0, g, g.L), NT, Lay::bytes, s>>>(mu, mv, muL, mvL, muc, mvc, mpb, mgb, g,
+                                                                        c, (S*)udo, (S*)vdo, nonfinite, timeout);
   return cudaGetLastError();
 }
 
-cudaError_t ring(const Geom& g, void* const* f, const void* const* src, int nf, int K, bool copy, cudaStream_t s) {
+template <typename E>
+cudaError_t ring_t(const Geom& g, void* const* f, const void* const* src, int nf, int K, bool copy, cudaStream_t s) {
   int nring = 2 * H * (g.nx + 2 * H) + 2 * H * g.ny;
   dim3 grid((nring + 255) / 256, K, nf);
-  T* d[4] = {nullptr, nullptr, nullptr, nullptr};
-  const T* q[4] = {nullptr, nullptr, nullptr, nullptr};
+  E* d[4] = {nullptr, nullptr, nullptr, nullptr};
+  const E* q[4] = {nullptr, nullptr, nullptr, nullptr};
   for (int i = 0; i < nf; ++i) {
-    d[i] = (T*)f[i];
-    if (src) q[i] = (const T*)src[i];
+    d[i] = (E*)f[i];
+    if (src) q[i] = (const E*)src[i];
   }
   if (copy)
-    k_ring<T, true><<<grid, 256, 0, s>>>(g, d[0], d[1], d[2], d[3], q[0], q[1], q[2], q[3], K);
+    k_ring<E, true><<<grid, 256, 0, s>>>(g, d[0], d[1], d[2], d[3], q[0], q[1], q[2], q[3], K);
   else
-    k_ring<T, false><<<grid, 256, 0, s>>>(g, d[0], d[1], d[2], d[3], q[0], q[1], q[2], q[3], K);
+    k_ring<E, false><<<grid, 256, 0, s>>>(g, d[0], d[1], d[2], d[3], q[0], q[1], q[2], q[3], K);
   return cudaGetLastError();
+}
+
+// halo passes of the state fields and of the C-grid fields
+cudaError_t ring(const Geom& g, void* const* f, const void* const* src, int nf, int K, bool copy, cudaStream_t s) {
+  return ring_t<S>(g, f, src, nf, K, copy, s);
+}
+cudaError_t ring_cg(const Geom& g, void* const* f, const void* const* src, int nf, int K, bool copy, cudaStream_t s) {
+  return ring_t<C>(g, f, src, nf, K, copy, s);
 }
 
 template <int LM>
 cudaError_t remap_winds_lm(const Geom& g, const RemapArgs& ra, const void* dp, const void* ud, const void* vd,
                            void* urem, void* vrem, int* trace, Status* st, cudaStream_t s) {
   int n = (g.nx + 2) * (g.ny + 2);
-  k_remap_winds<T, LM><<<(n + 63) / 64, 64, 0, s>>>(g, ra, (const T*)dp, (const T*)ud, (const T*)vd, (T*)urem,
-                                                    (T*)vrem, trace, st);
+  k_remap_winds<S, LM><<<(n + 63) / 64, 64, 0, s>>>(g, ra, (const S*)dp, (const S*)ud, (const S*)vd, (S*)urem,
+                                                    (S*)vrem, trace, st);
   return cudaGetLastError();
 }
 template <int LM>
@@ -132,9 +154,9 @@ cudaError_t remap_energy_lm(const Geom& g, const RemapArgs& ra, const void* dp, 
                             const void* vd, const void* urem, const void* vrem, const double* gzs, void* dpo,
                             void* pto, void* udo, void* vdo, int* trace, Status* st, cudaStream_t s) {
   int n = g.nx * g.ny;
-  k_remap_energy<T, LM><<<(n + 63) / 64, 64, 0, s>>>(g, ra, (const T*)dp, (const T*)pt, (const T*)ud, (const T*)vd,
-                                                     (const T*)urem, (const T*)vrem, gzs, (T*)dpo, (T*)pto, (T*)udo,
-                                                     (T*)vdo, trace, st);
+  k_remap_energy<S, LM><<<(n + 63) / 64, 64, 0, s>>>(g, ra, (const S*)dp, (const S*)pt, (const S*)ud, (const S*)vd,
+                                                     (const S*)urem, (const S*)vrem, gzs, (S*)dpo, (S*)pto, (S*)udo,
+                                                     (S*)vdo, trace, st);
   return cudaGetLastError();
 }
 
@@ -154,12 +176,12 @@ cudaError_t remap_energy(const Geom& g, const RemapArgs& ra, const void* dp, con
 }
 
 cudaError_t check_finite(const Geom& g, const void* const* f, int* flag, cudaStream_t s) {
-  k_check_finite<T><<<296, 256, 0, s>>>(g, (const T*)f[0], (const T*)f[1], (const T*)f[2], (const T*)f[3], flag);
+  k_check_finite<S><<<296, 256, 0, s>>>(g, (const S*)f[0], (const S*)f[1], (const S*)f[2], (const S*)f[3], flag);
   return cudaGetLastError();
 }
 
 cudaError_t mass_sum(const Geom& g, const void* dp, double* partial, int nblocks, double* out, cudaStream_t s) {
-  k_mass_partial<T><<<nblocks, 256, 0, s>>>(g, (const T*)dp, partial);
+  k_mass_partial<S><<<nblocks, 256, 0, s>>>(g, (const S*)dp, partial);
   k_mass_final<<<1, 32, 0, s>>>(partial, nblocks, out);
   return cudaGetLastError();
 }
@@ -175,8 +197,9 @@ cudaError_t from_double(const double* src, void* dst, long long n, cudaStream_t 
 
 }  // namespace
 
-const Ops ATM_OPS_NAME = {(int)sizeof(T), setup,        mass,         column,       heating,
-                          c_mom,          d_mom,        ring,         remap_winds,  remap_energy,
-                          check_finite,   mass_sum,     to_double,    from_double};
+const Ops ATM_OPS_NAME = {(int)sizeof(S), (int)sizeof(C), setup,        mass,       column,
+                          heating,        c_mom,          d_mom,        ring,       ring_cg,
+                          remap_winds,    remap_energy,   check_finite, mass_sum,   to_double,
+                          from_double};
 
 }  // namespace atm

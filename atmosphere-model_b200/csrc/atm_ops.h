@@ -11,24 +11,28 @@
 namespace atm {
 
 struct Ops {
-  int elem;  // bytes of the sweep type
+  int elem;     // bytes of an element of the prognostic state (dp, pt, ud, vd)
+  int cg_elem;  // bytes of an element of the C-grid fields (dpc, ptc, uc, vc)
   cudaError_t (*setup)();
   // C- or D-grid mass/potential-temperature sweep of every layer
   cudaError_t (*mass)(const Geom&, const Consts&, const void* dp, const void* pt, const void* u, const void* v,
                       const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, int* timeout,
                       bool cgrid, cudaStream_t);
-  // plev/pkap/gz columns over [lo, n-1+hi]^2
-  cudaError_t (*column)(const Geom&, const Consts&, const void* dpl, const void* ptl, double* pkap, double* gz,
-                        int lo, int hi, double* plev, cudaStream_t);
-  cudaError_t (*heating)(const Geom&, const Consts&, const void* dpl, const double* net_flux, double* heat,
+  // plev/pkap/gz columns over [lo, n-1+hi]^2 from dp, pt of element size es
+  cudaError_t (*column)(const Geom&, const Consts&, const void* dpl, const void* ptl, int es, double* pkap,
+                        double* gz, int lo, int hi, double* plev, cudaStream_t);
+  cudaError_t (*heating)(const Geom&, const Consts&, const void* dpl, int es, const double* net_flux, double* heat,
                          cudaStream_t);
   cudaError_t (*c_mom)(const Geom&, const Consts&, const void* ud, const void* vd, const double* pkap,
                        const double* gz, void* uc, void* vc, int* timeout, cudaStream_t);
   cudaError_t (*d_mom)(const Geom&, const Consts&, const void* ud, const void* vd, const void* uc, const void* vc,
                        const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, int* timeout,
                        cudaStream_t);
-  // periodic halo fill (copy = false) or ring copy src -> f (copy = true) of nf fields
+  // periodic halo fill (copy = false) or ring copy src -> f (copy = true) of
+  // nf state fields (ring) or C-grid fields (ring_cg)
   cudaError_t (*ring)(const Geom&, void* const* f, const void* const* src, int nf, int K, bool copy, cudaStream_t);
+  cudaError_t (*ring_cg)(const Geom&, void* const* f, const void* const* src, int nf, int K, bool copy,
+                         cudaStream_t);
   cudaError_t (*remap_winds)(const Geom&, const RemapArgs&, const void* dp, const void* ud, const void* vd,
                              void* urem, void* vrem, int* trace, Status*, cudaStream_t);
   cudaError_t (*remap_energy)(const Geom&, const RemapArgs&, const void* dp, const void* pt, const void* ud,
@@ -36,6 +40,7 @@ struct Ops {
                               void* pto, void* udo, void* vdo, int* trace, Status*, cudaStream_t);
   cudaError_t (*check_finite)(const Geom&, const void* const* f, int* flag, cudaStream_t);
   cudaError_t (*mass_sum)(const Geom&, const void* dp, double* partial, int nblocks, double* out, cudaStream_t);
+  // C-grid-type <-> double conversion of whole padded fields
   cudaError_t (*to_double)(const void* src, double* dst, long long n, cudaStream_t);
   cudaError_t (*from_double)(const double* src, void* dst, long long n, cudaStream_t);
 };

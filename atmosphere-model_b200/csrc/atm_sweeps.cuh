@@ -10,6 +10,8 @@
 // generation (and of the reference), so the FP64 results are unchanged.
 #pragma once
 
+#include <type_traits>
+
 #include "atm_kernels.cuh"
 #include "atm_tma.cuh"
 
@@ -91,6 +93,13 @@ __device__ __forceinline__ unsigned char* smem_base(unsigned char* raw) {
   return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
 }
 
+// A shared-memory window of type S read as the sweep type T.
+template <typename S, typename T>
+struct SmAs {
+  Sm<S> s;
+  __device__ __forceinline__ T operator()(int x, int y) const { return T(s(x, y)); }
+};
+
 // Region loop: body(x, y) for every point of [x0, x0+W) x [y0, y0+Hh).
 template <int W, int Hh, typename F>
 __device__ __forceinline__ void region(int x0, int y0, F&& body) {
@@ -110,16 +119,23 @@ __device__ __forceinline__ int tma_x0(int i0) {
 }
 
 // ---------------------------------------------------------------- mass ----
-template <typename T, int TX, int TY, bool CGRID>
+// S: element type of the prognostic state (dp, pt, ud, vd), C: of the
+// C-grid fields (dpc, ptc, uc, vc), T: the sweep arithmetic.  The FP64 form
+// has S = C = T = double; the mixed form keeps the state in double, the
+// C-grid fields in float and sweeps in float.
+template <typename T, int TX, int TY, bool CGRID, typename S = T, typename C = T>
 struct MassL {
-  // TMA boxes: dp and pt, and the u, v boxes (D winds on the C grid step,
-  // C winds on the D grid step)
-  static constexpr int WD = tma_width<T>(TX + 6), HD = TY + 6;
-  static constexpr int WU = tma_width<T>(CGRID ? TX + 2 : TX + 1), HU = CGRID ? TY + 7 : TY + 6;
-  static constexpr int WV = tma_width<T>(CGRID ? TX + 7 : TX + 6), HV = CGRID ? TY + 2 : TY + 1;
-  static constexpr uint32_t tx_bytes = (uint32_t)((2 * WD * HD + WU * HU + WV * HV) * sizeof(T));
-  static constexpr size_t boxes = 2 * tma_box_bytes(WD, HD, sizeof(T)) + tma_box_bytes(WU, HU, sizeof(T)) +
-                                  tma_box_bytes(WV, HV, sizeof(T));
+  // TMA boxes: dp and pt (state), and the u, v boxes (D winds on the C grid
+  // step, C winds on the D grid step)
+  using UB = std::conditional_t<CGRID, S, C>;
+  static_assert(CGRID || std::is_same_v<C, T>, "the D-grid step sweeps with the C-grid winds' type");
+  static constexpr int WD = tma_width<S>(TX + 6), HD = TY + 6;
+  static constexpr int WU = tma_width<UB>(CGRID ? TX + 2 : TX + 1), HU = CGRID ? TY + 7 : TY + 6;
+  static constexpr int WV = tma_width<UB>(CGRID ? TX + 7 : TX + 6), HV = CGRID ? TY + 2 : TY + 1;
+  static constexpr uint32_t tx_bytes =
+      (uint32_t)(2 * WD * HD * sizeof(S) + (WU * HU + WV * HV) * sizeof(UB));
+  static constexpr size_t boxes = 2 * tma_box_bytes(WD, HD, sizeof(S)) + tma_box_bytes(WU, HU, sizeof(UB)) +
+                                  tma_box_bytes(WV, HV, sizeof(UB));
   static constexpr bool NN = !CGRID;
   static constexpr size_t work =
       (CGRID ? box_bytes<T>(TX + 1, TY + 6) + box_bytes<T>(TX + 6, TY + 1) : 0) +  // uc, vc (C grid)
@@ -130,14 +146,18 @@ struct MassL {
   static constexpr size_t bytes = boxes + work + 128;
 };
 
-template <typename T, int TX, int TY, bool CGRID>
+template <typename T, int TX, int TY, bool CGRID, typename S = T, typename C = T>
 __global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMap m_dp,
                                               const __grid_constant__ CUtensorMap m_pt,
                                               const __grid_constant__ CUtensorMap m_u,
                                               const __grid_constant__ CUtensorMap m_v, Geom g, Consts c,
-                                              const double* __restrict__ heat, T* __restrict__ dpo,
-                                              T* __restrict__ pto, int lo, int hi, int* nonfinite, int* timeout) {
-  using Lay = MassL<T, TX, TY, CGRID>;
+                                              const double* __restrict__ heat,
+                                              std::conditional_t<CGRID, C, S>* __restrict__ dpo,
+                                              std::conditional_t<CGRID, C, S>* __restrict__ pto, int lo, int hi,
+                                              int* nonfinite, int* timeout) {
+  using Lay = MassL<T, TX, TY, CGRID, S, C>;
+  using UB = typename Lay::UB;
+  using O = std::conditional_t<CGRID, C, S>;
   constexpr int V = CGRID ? PPM_UNC : PPM_NN;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -147,15 +167,20 @@ __global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMa
   const int ox = lo + blockIdx.x * TX, oy = lo + blockIdx.y * TY;
   const T dt = T(c.dt), dtdx = T(c.dtdx), dtdy = T(c.dtdy), rA = T(c.rA);
 
-  auto tbox = [&](int i0, int j0, int w, int h) {
-    Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
-    p += tma_box_bytes(w, h, sizeof(T));
+  auto sbox = [&](int i0, int j0, int w, int h) {
+    Sm<S> s{reinterpret_cast<S*>(p), tma_x0<S>(i0), j0, w};
+    p += tma_box_bytes(w, h, sizeof(S));
     return s;
   };
-  Sm<T> sdp = tbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
-  Sm<T> spt = tbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
-  Sm<T> su = CGRID ? tbox(ox - 1, oy - 3, Lay::WU, Lay::HU) : tbox(ox, oy - 3, Lay::WU, Lay::HU);
-  Sm<T> sv = CGRID ? tbox(ox - 3, oy - 1, Lay::WV, Lay::HV) : tbox(ox - 3, oy, Lay::WV, Lay::HV);
+  auto ubox = [&](int i0, int j0, int w, int h) {
+    Sm<UB> s{reinterpret_cast<UB*>(p), tma_x0<UB>(i0), j0, w};
+    p += tma_box_bytes(w, h, sizeof(UB));
+    return s;
+  };
+  Sm<S> sdp = sbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
+  Sm<S> spt = sbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
+  Sm<UB> su = CGRID ? ubox(ox - 1, oy - 3, Lay::WU, Lay::HU) : ubox(ox, oy - 3, Lay::WU, Lay::HU);
+  Sm<UB> sv = CGRID ? ubox(ox - 3, oy - 1, Lay::WV, Lay::HV) : ubox(ox - 3, oy, Lay::WV, Lay::HV);
   {
     const TmaBox boxes[4] = {{&m_dp, sdp.p, sdp.x0, sdp.y0, k},
                              {&m_pt, spt.p, spt.x0, spt.y0, k},
@@ -164,10 +189,13 @@ __global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMa
     if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
   }
   // C-grid winds: built from the D-grid winds (C step) or the loaded boxes (D step)
-  Sm<T> suc = su, svc = sv;
-  if (CGRID) {
+  Sm<T> suc, svc;
+  if constexpr (CGRID) {
     suc = carve<T>(p, ox, oy - 3, TX + 1, TY + 6);
     svc = carve<T>(p, ox - 3, oy, TX + 6, TY + 1);
+  } else {
+    suc = su;
+    svc = sv;
   }
   Sm<T> tyd = carve<T>(p, ox - 3, oy, TX + 6, TY);
   Sm<T> typ = carve<T>(p, ox - 3, oy, TX + 6, TY);
@@ -184,14 +212,14 @@ __global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMa
   Sm<T> fyd = carve<T>(p, ox, oy, TX, TY + 1);
   Sm<T> fyp = carve<T>(p, ox, oy, TX, TY + 1);
 
-  if (CGRID) {  // mod_sw_dyn.f90:109-117
+  if constexpr (CGRID) {  // mod_sw_dyn.f90:109-117
     region<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
-      T ub = T(.5) * (su(x, y) + su(x - 1, y));
-      suc(x, y) = T(.5) * (ub + T(.5) * (su(x, y + 1) + su(x - 1, y + 1)));
+      T ub = T(.5) * (T(su(x, y)) + T(su(x - 1, y)));
+      suc(x, y) = T(.5) * (ub + T(.5) * (T(su(x, y + 1)) + T(su(x - 1, y + 1))));
     });
     region<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
-      T vb = T(.5) * (sv(x, y) + sv(x, y - 1));
-      svc(x, y) = T(.5) * (vb + T(.5) * (sv(x + 1, y) + sv(x + 1, y - 1)));
+      T vb = T(.5) * (T(sv(x, y)) + T(sv(x, y - 1)));
+      svc(x, y) = T(.5) * (vb + T(.5) * (T(sv(x + 1, y)) + T(sv(x + 1, y - 1))));
     });
     __syncthreads();
   }
@@ -199,30 +227,34 @@ __global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMa
   region<TX + 6, TY>(ox - 3, oy, [&](int x, int y) {
     T cy0 = dtdx * svc(x, y), cy1 = dtdx * svc(x, y + 1);
     T den = T(1) / (T(1) - dtdy * (svc(x, y + 1) - svc(x, y)));
-    T f0 = (cy0 > T(0)) ? sdp(x, y - 1) : sdp(x, y);
-    T f1 = (cy1 > T(0)) ? sdp(x, y) : sdp(x, y + 1);
-    tyd(x, y) = T(.5) * (sdp(x, y) + den * (sdp(x, y) - rA * (f1 - f0)));
-    f0 = (cy0 > T(0)) ? spt(x, y - 1) : spt(x, y);
-    f1 = (cy1 > T(0)) ? spt(x, y) : spt(x, y + 1);
-    typ(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
+    const T d0 = T(sdp(x, y)), dm = T(sdp(x, y - 1)), dq = T(sdp(x, y + 1));
+    T f0 = (cy0 > T(0)) ? dm : d0;
+    T f1 = (cy1 > T(0)) ? d0 : dq;
+    tyd(x, y) = T(.5) * (d0 + den * (d0 - rA * (f1 - f0)));
+    const T p0 = T(spt(x, y)), pm = T(spt(x, y - 1)), pq = T(spt(x, y + 1));
+    f0 = (cy0 > T(0)) ? pm : p0;
+    f1 = (cy1 > T(0)) ? p0 : pq;
+    typ(x, y) = T(.5) * (p0 + den * (p0 - rA * (f1 - f0)));
   });
   region<TX, TY + 6>(ox, oy - 3, [&](int x, int y) {
     T cx0 = dtdx * suc(x, y), cx1 = dtdx * suc(x + 1, y);
     T den = T(1) / (T(1) - dtdx * (suc(x + 1, y) - suc(x, y)));
-    T f0 = (cx0 > T(0)) ? sdp(x - 1, y) : sdp(x, y);
-    T f1 = (cx1 > T(0)) ? sdp(x, y) : sdp(x + 1, y);
-    txd(x, y) = T(.5) * (sdp(x, y) + den * (sdp(x, y) - rA * (f1 - f0)));
-    f0 = (cx0 > T(0)) ? spt(x - 1, y) : spt(x, y);
-    f1 = (cx1 > T(0)) ? spt(x, y) : spt(x + 1, y);
-    txp(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
+    const T d0 = T(sdp(x, y)), dm = T(sdp(x - 1, y)), dq = T(sdp(x + 1, y));
+    T f0 = (cx0 > T(0)) ? dm : d0;
+    T f1 = (cx1 > T(0)) ? d0 : dq;
+    txd(x, y) = T(.5) * (d0 + den * (d0 - rA * (f1 - f0)));
+    const T p0 = T(spt(x, y)), pm = T(spt(x - 1, y)), pq = T(spt(x + 1, y));
+    f0 = (cx0 > T(0)) ? pm : p0;
+    f1 = (cx1 > T(0)) ? p0 : pq;
+    txp(x, y) = T(.5) * (p0 + den * (p0 - rA * (f1 - f0)));
   });
   {
     const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
     region<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
-      lpd(x, y) = T(-2.) * sdp(x, y) * rdxy + (sdp(x + 1, y) + sdp(x - 1, y)) * rdx2 +
-                  (sdp(x, y + 1) + sdp(x, y - 1)) * rdy2;
-      lpp(x, y) = T(-2.) * spt(x, y) * rdxy + (spt(x + 1, y) + spt(x - 1, y)) * rdx2 +
-                  (spt(x, y + 1) + spt(x, y - 1)) * rdy2;
+      lpd(x, y) = T(-2.) * T(sdp(x, y)) * rdxy + (T(sdp(x + 1, y)) + T(sdp(x - 1, y))) * rdx2 +
+                  (T(sdp(x, y + 1)) + T(sdp(x, y - 1))) * rdy2;
+      lpp(x, y) = T(-2.) * T(spt(x, y)) * rdxy + (T(spt(x + 1, y)) + T(spt(x - 1, y))) * rdx2 +
+                  (T(spt(x, y + 1)) + T(spt(x, y - 1))) * rdy2;
     });
   }
   __syncthreads();
@@ -255,35 +287,55 @@ __global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMa
   bool bad = false;
   region<TX, TY>(ox, oy, [&](int x, int y) {
     if (x > xhi || y > yhi) return;
-    T d = sdp(x, y);
-    T v = d - (fxd(x + 1, y) - fxd(x, y) + dxv * (lpd(x + 1, y) - T(2.) * lpd(x, y) + lpd(x - 1, y)));
-    v = v - (fyd(x, y + 1) - fyd(x, y) + dyv * (lpd(x, y + 1) - T(2.) * lpd(x, y) + lpd(x, y - 1)));
-    T q = d * spt(x, y) - (fxp(x + 1, y) * fxd(x + 1, y) - fxp(x, y) * fxd(x, y) +
-                           vdx * ((lpp(x + 1, y) - lpp(x, y)) * fxd(x + 1, y) - (lpp(x, y) - lpp(x - 1, y)) * fxd(x, y)));
-    q = q - (fyp(x, y + 1) * fyd(x, y + 1) - fyp(x, y) * fyd(x, y) +
-             vdy * ((lpp(x, y + 1) - lpp(x, y)) * fyd(x, y + 1) - (lpp(x, y) - lpp(x, y - 1)) * fyd(x, y)));
-    if (heat) q = q + dt * d * T(heat[g.at(x, y, k)]);
-    q = q / v;
+    O vo, qo;
+    if constexpr (std::is_same_v<S, T>) {  // the reference's operations, in order
+      T d = sdp(x, y);
+      T v = d - (fxd(x + 1, y) - fxd(x, y) + dxv * (lpd(x + 1, y) - T(2.) * lpd(x, y) + lpd(x - 1, y)));
+      v = v - (fyd(x, y + 1) - fyd(x, y) + dyv * (lpd(x, y + 1) - T(2.) * lpd(x, y) + lpd(x, y - 1)));
+      T q = d * spt(x, y) - (fxp(x + 1, y) * fxd(x + 1, y) - fxp(x, y) * fxd(x, y) +
+                             vdx * ((lpp(x + 1, y) - lpp(x, y)) * fxd(x + 1, y) - (lpp(x, y) - lpp(x - 1, y)) * fxd(x, y)));
+      q = q - (fyp(x, y + 1) * fyd(x, y + 1) - fyp(x, y) * fyd(x, y) +
+               vdy * ((lpp(x, y + 1) - lpp(x, y)) * fyd(x, y + 1) - (lpp(x, y) - lpp(x, y - 1)) * fyd(x, y)));
+      if (heat) q = q + dt * d * T(heat[g.at(x, y, k)]);
+      q = q / v;
+      vo = O(v);
+      qo = O(q);
+    } else {
+      // the same update in flux form: interface fluxes (advective plus
+      // vorticity-damping) in the sweep type, their differences applied to
+      // the state's type, so that mass and dp*pt telescope in S
+      auto Fx = [&](int xx) { return fxd(xx, y) + dxv * (lpd(xx, y) - lpd(xx - 1, y)); };
+      auto Fy = [&](int yy) { return fyd(x, yy) + dyv * (lpd(x, yy) - lpd(x, yy - 1)); };
+      auto Hx = [&](int xx) { return (fxp(xx, y) + vdx * (lpp(xx, y) - lpp(xx - 1, y))) * fxd(xx, y); };
+      auto Hy = [&](int yy) { return (fyp(x, yy) + vdy * (lpp(x, yy) - lpp(x, yy - 1))) * fyd(x, yy); };
+      const S d = sdp(x, y);
+      const S v = d - ((S(Fx(x + 1)) - S(Fx(x))) + (S(Fy(y + 1)) - S(Fy(y))));
+      S q = d * spt(x, y) - ((S(Hx(x + 1)) - S(Hx(x))) + (S(Hy(y + 1)) - S(Hy(y))));
+      if (heat) q = q + S(c.dt) * d * S(heat[g.at(x, y, k)]);
+      q = q / v;
+      vo = O(v);
+      qo = O(q);
+    }
     long long o = g.at(x, y, k);
-    dpo[o] = v;
-    pto[o] = q;
+    dpo[o] = vo;
+    pto[o] = qo;
     bool inside = x >= 0 && x < g.nx && y >= 0 && y < g.ny;
-    bad = bad || (inside && !(finite_(v) && finite_(q)));
+    bad = bad || (inside && !(finite_(vo) && finite_(qo)));
   });
   if (nonfinite) flag_nonfinite(nonfinite, bad);
 }
 
 // ======================================================== C-grid momentum ==
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, typename S = T>
 struct CMomL {
-  static constexpr int WU = tma_width<T>(TX + 7), HU = TY + 7;   // ud box x in [ox-4, ox+TX+2]
-  static constexpr int WV = tma_width<T>(TX + 7), HV = TY + 7;   // vd box x in [ox-3, ox+TX+3]
-  static constexpr int WL = tma_width<T>(TX + 3), HL = TY + 3;   // layer-nlay ud, vd
+  static constexpr int WU = tma_width<S>(TX + 7), HU = TY + 7;   // ud box x in [ox-4, ox+TX+2]
+  static constexpr int WV = tma_width<S>(TX + 7), HV = TY + 7;   // vd box x in [ox-3, ox+TX+3]
+  static constexpr int WL = tma_width<S>(TX + 3), HL = TY + 3;   // layer-nlay ud, vd
   static constexpr int WP = tma_width<double>(TX + 1), HP = TY + 1;  // pkap, gz at k and k+1
   static constexpr uint32_t tx_bytes =
-      (uint32_t)((WU * HU + WV * HV + 2 * WL * HL) * sizeof(T) + 4 * WP * HP * sizeof(double));
-  static constexpr size_t boxes = tma_box_bytes(WU, HU, sizeof(T)) + tma_box_bytes(WV, HV, sizeof(T)) +
-                                  2 * tma_box_bytes(WL, HL, sizeof(T)) + 4 * tma_box_bytes(WP, HP, 8);
+      (uint32_t)((WU * HU + WV * HV + 2 * WL * HL) * sizeof(S) + 4 * WP * HP * sizeof(double));
+  static constexpr size_t boxes = tma_box_bytes(WU, HU, sizeof(S)) + tma_box_bytes(WV, HV, sizeof(S)) +
+                                  2 * tma_box_bytes(WL, HL, sizeof(S)) + 4 * tma_box_bytes(WP, HP, 8);
   static constexpr size_t work = 2 * box_bytes<T>(TX + 6, TY + 6) + 2 * box_bytes<T>(TX + 1, TY + 1) +
                                  box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 1, TY + 1) +
                                  box_bytes<T>(TX, TY + 5) + box_bytes<T>(TX + 5, TY) + box_bytes<T>(TX + 1, TY + 1) +
@@ -292,15 +344,15 @@ struct CMomL {
   static constexpr size_t bytes = boxes + work + 128;
 };
 
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, typename S = T, typename C = T>
 __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorMap m_ud,
                                                const __grid_constant__ CUtensorMap m_vd,
                                                const __grid_constant__ CUtensorMap m_udL,
                                                const __grid_constant__ CUtensorMap m_vdL,
                                                const __grid_constant__ CUtensorMap m_pk,
                                                const __grid_constant__ CUtensorMap m_gz, Geom g, Consts c,
-                                               T* __restrict__ uc, T* __restrict__ vc, int* timeout) {
-  using Lay = CMomL<T, TX, TY>;
+                                               C* __restrict__ uc, C* __restrict__ vc, int* timeout) {
+  using Lay = CMomL<T, TX, TY, S>;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
@@ -311,8 +363,8 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
   const T rdx = T(c.rdx), rdy = T(c.rdy);
 
   auto tbox = [&](int i0, int j0, int w, int h) {
-    Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
-    p += tma_box_bytes(w, h, sizeof(T));
+    Sm<S> s{reinterpret_cast<S*>(p), tma_x0<S>(i0), j0, w};
+    p += tma_box_bytes(w, h, sizeof(S));
     return s;
   };
   auto dbox = [&](int i0, int j0, int w, int h) {
@@ -320,17 +372,18 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
     p += tma_box_bytes(w, h, 8);
     return s;
   };
-  Sm<T> sud = tbox(ox - 4, oy - 3, Lay::WU, Lay::HU);
-  Sm<T> svd = tbox(ox - 3, oy - 4, Lay::WV, Lay::HV);
-  Sm<T> udL = tbox(ox - 2, oy - 2, Lay::WL, Lay::HL);
-  Sm<T> vdL = tbox(ox - 2, oy - 2, Lay::WL, Lay::HL);
+  Sm<S> bud = tbox(ox - 4, oy - 3, Lay::WU, Lay::HU);
+  Sm<S> bvd = tbox(ox - 3, oy - 4, Lay::WV, Lay::HV);
+  Sm<S> budL = tbox(ox - 2, oy - 2, Lay::WL, Lay::HL);
+  Sm<S> bvdL = tbox(ox - 2, oy - 2, Lay::WL, Lay::HL);
+  const SmAs<S, T> sud{bud}, svd{bvd}, udL{budL}, vdL{bvdL};
   Sm<double> pk0 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
   Sm<double> pk1 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
   Sm<double> gz0 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
   Sm<double> gz1 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
   {
-    const TmaBox boxes[8] = {{&m_ud, sud.p, sud.x0, sud.y0, k},     {&m_vd, svd.p, svd.x0, svd.y0, k},
-                             {&m_udL, udL.p, udL.x0, udL.y0, L - 1}, {&m_vdL, vdL.p, vdL.x0, vdL.y0, L - 1},
+    const TmaBox boxes[8] = {{&m_ud, bud.p, bud.x0, bud.y0, k},     {&m_vd, bvd.p, bvd.x0, bvd.y0, k},
+                             {&m_udL, budL.p, budL.x0, budL.y0, L - 1}, {&m_vdL, bvdL.p, bvdL.x0, bvdL.y0, L - 1},
                              {&m_pk, pk0.p, pk0.x0, pk0.y0, k},      {&m_pk, pk1.p, pk1.x0, pk1.y0, k + 1},
                              {&m_gz, gz0.p, gz0.x0, gz0.y0, k},      {&m_gz, gz1.p, gz1.x0, gz1.y0, k + 1}};
     if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
@@ -427,22 +480,26 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
     T v = vc1(x, y) - dt * (sud(x, y) * fx + vdx * (lap(x + 1, y) - lap(x, y))) -
           dtdy * (ke(x, y) - ke(x, y - 1) - T(pgy));
     long long o = g.at(x, y, k);
-    uc[o] = u;
-    vc[o] = v;
+    uc[o] = C(u);
+    vc[o] = C(v);
   });
 }
 
 // ======================================================== D-grid momentum ==
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, typename S = T, typename C = T>
 struct DMomL {
-  static constexpr int WU = tma_width<T>(TX + 6), HU = TY + 6;       // ud, vd: [ox-3, ox+TX+2]^2
+  static_assert(std::is_same_v<C, T>, "the D-grid step sweeps with the C-grid winds' type");
+  static constexpr int WU = tma_width<S>(TX + 6), HU = TY + 6;       // ud, vd: [ox-3, ox+TX+2]^2
   static constexpr int WUL = tma_width<T>(TX + 1), HUL = TY + 5;     // uc layer nlay: x [ox, ox+TX], y [oy-3, oy+TY+1]
   static constexpr int WVL = tma_width<T>(TX + 5), HVL = TY + 1;     // vc layer nlay: x [ox-3, ox+TX+1], y [oy, oy+TY]
   static constexpr int WC = tma_width<T>(TX), HC = TY;               // uc, vc of the layer at the outputs
   static constexpr int WP = tma_width<double>(TX + 1), HP = TY + 1;  // pkapb, gzb
-  static constexpr uint32_t tx_bytes =
-      (uint32_t)((2 * WU * HU + WUL * HUL + WVL * HVL + 2 * WC * HC) * sizeof(T) + 4 * WP * HP * sizeof(double));
-  static constexpr size_t boxes = 2 * tma_box_bytes(WU, HU, sizeof(T)) + tma_box_bytes(WUL, HUL, sizeof(T)) +
+  static constexpr uint32_t tx_bytes = (uint32_t)(2 * WU * HU * sizeof(S) +
+                                                   (WUL * HUL + WVL * HVL + 2 * WC * HC) * sizeof(T) +
+                                                   4 * WP * HP * sizeof(double));
+  // the state's ud, vd as sweep-type copies when the types differ
+  static constexpr size_t conv = std::is_same_v<S, T> ? 0 : 2 * box_bytes<T>(TX + 6, TY + 6);
+  static constexpr size_t boxes = 2 * tma_box_bytes(WU, HU, sizeof(S)) + tma_box_bytes(WUL, HUL, sizeof(T)) +
                                   tma_box_bytes(WVL, HVL, sizeof(T)) + 2 * tma_box_bytes(WC, HC, sizeof(T)) +
                                   4 * tma_box_bytes(WP, HP, 8);
   static constexpr size_t work =
@@ -457,10 +514,10 @@ struct DMomL {
   static constexpr size_t edges_ke = 2 * box_bytes<T>(TX + 1, TY + 2) + 2 * box_bytes<T>(TX + 2, TY + 1);
   static constexpr size_t edges_vf = 2 * box_bytes<T>(TX, TY + 1) + 2 * box_bytes<T>(TX + 1, TY);
   static constexpr size_t edges = edges_ke > edges_vf ? edges_ke : edges_vf;
-  static constexpr size_t bytes = boxes + work + slopes + edges + 128;
+  static constexpr size_t bytes = boxes + conv + work + slopes + edges + 128;
 };
 
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, typename S = T, typename C = T>
 __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorMap m_ud,
                                                const __grid_constant__ CUtensorMap m_vd,
                                                const __grid_constant__ CUtensorMap m_ucL,
@@ -469,9 +526,9 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
                                                const __grid_constant__ CUtensorMap m_vc,
                                                const __grid_constant__ CUtensorMap m_pkb,
                                                const __grid_constant__ CUtensorMap m_gzb, Geom g, Consts c,
-                                               T* __restrict__ udo, T* __restrict__ vdo, int* nonfinite,
+                                               S* __restrict__ udo, S* __restrict__ vdo, int* nonfinite,
                                                int* timeout) {
-  using Lay = DMomL<T, TX, TY>;
+  using Lay = DMomL<T, TX, TY, S, C>;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
@@ -491,8 +548,13 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
     p += tma_box_bytes(w, h, 8);
     return s;
   };
-  Sm<T> sud = tbox(ox - 3, oy - 3, Lay::WU, Lay::HU);
-  Sm<T> svd = tbox(ox - 3, oy - 3, Lay::WU, Lay::HU);
+  auto sbox = [&](int i0, int j0, int w, int h) {
+    Sm<S> s{reinterpret_cast<S*>(p), tma_x0<S>(i0), j0, w};
+    p += tma_box_bytes(w, h, sizeof(S));
+    return s;
+  };
+  Sm<S> bud = sbox(ox - 3, oy - 3, Lay::WU, Lay::HU);
+  Sm<S> bvd = sbox(ox - 3, oy - 3, Lay::WU, Lay::HU);
   Sm<T> ucL = tbox(ox, oy - 3, Lay::WUL, Lay::HUL);
   Sm<T> vcL = tbox(ox - 3, oy, Lay::WVL, Lay::HVL);
   Sm<T> suc = tbox(ox, oy, Lay::WC, Lay::HC);
@@ -503,12 +565,27 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
   Sm<double> gb1 = dbox(ox, oy, Lay::WP, Lay::HP);
   {
     const TmaBox boxes[10] = {
-        {&m_ud, sud.p, sud.x0, sud.y0, k},       {&m_vd, svd.p, svd.x0, svd.y0, k},
+        {&m_ud, bud.p, bud.x0, bud.y0, k},       {&m_vd, bvd.p, bvd.x0, bvd.y0, k},
         {&m_ucL, ucL.p, ucL.x0, ucL.y0, L - 1},  {&m_vcL, vcL.p, vcL.x0, vcL.y0, L - 1},
         {&m_uc, suc.p, suc.x0, suc.y0, k},       {&m_vc, svc.p, svc.x0, svc.y0, k},
         {&m_pkb, pb0.p, pb0.x0, pb0.y0, k},      {&m_pkb, pb1.p, pb1.x0, pb1.y0, k + 1},
         {&m_gzb, gb0.p, gb0.x0, gb0.y0, k},      {&m_gzb, gb1.p, gb1.x0, gb1.y0, k + 1}};
     if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
+  }
+  // ud, vd in the sweep type (the boxes themselves when the types agree)
+  constexpr int WQ = std::is_same_v<S, T> ? Lay::WU : TX + 6;
+  Sm<T> sud, svd;
+  if constexpr (std::is_same_v<S, T>) {
+    sud = bud;
+    svd = bvd;
+  } else {
+    sud = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
+    svd = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
+    region<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
+      sud(x, y) = T(bud(x, y));
+      svd(x, y) = T(bvd(x, y));
+    });
+    __syncthreads();
   }
   Sm<T> vor = carve<T>(p, ox - 3, oy - 3, TX + 5, TY + 5);
   Sm<T> dv0 = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
@@ -549,7 +626,7 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
     ubL(x, y) = T(.5) * (ucL(x, y) + ucL(x, y - 1));
     vbL(x, y) = T(.5) * (vcL(x, y) + vcL(x - 1, y));
   });
-  region<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(svd.ptr(x, y), Lay::WU); });
+  region<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(svd.ptr(x, y), WQ); });
   region<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { mux(x, y) = slope_at(sud.ptr(x, y), 1); });
   __syncthreads();
 
@@ -558,7 +635,7 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
   // sweeps of the vorticity with the layer-nlay Courant numbers (:708-722, 744-753)
   region<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
     T eL, eR;
-    edges_pre<T, PPM_CON>(svd.ptr(x, y), Lay::WU, mvy.ptr(x, y), TX + 1, eL, eR);
+    edges_pre<T, PPM_CON>(svd.ptr(x, y), WQ, mvy.ptr(x, y), TX + 1, eL, eR);
     lvy(x, y) = eL;
     rvy(x, y) = eR;
   });
@@ -592,7 +669,7 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
   // kinetic energy with PPM_CONSTRAINED (:639-657), del^4 (:695-702),
   // slopes of the vorticity-flux sweeps
   region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-    T fy = flux_con_pre<T>(svd.ptr(x, y), Lay::WU, lvy.ptr(x, y), rvy.ptr(x, y), TX + 1, dtdy * vbL(x, y));
+    T fy = flux_con_pre<T>(svd.ptr(x, y), WQ, lvy.ptr(x, y), rvy.ptr(x, y), TX + 1, dtdy * vbL(x, y));
     T kv = vbL(x, y) * fy;
     T fx = flux_con_pre<T>(sud.ptr(x, y), 1, lux.ptr(x, y), rux.ptr(x, y), 1, dtdx * ubL(x, y));
     ke(x, y) = T(.5) * (kv + ubL(x, y) * fx);
@@ -631,11 +708,21 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
                   (pb0(x, y) - pb1(x, y + 1)) * (gb1(x, y) - gb0(x, y + 1))) /
                  (pb0(x, y + 1) - pb1(x, y) + pb0(x, y) - pb1(x, y + 1));
     T fy = flux_con_pre<T>(tU.ptr(x, y), TX, ltU.ptr(x, y), rtU.ptr(x, y), TX, dtdx * vcL(x, y));
-    T u = sud(x, y) + dt * (svc(x, y) * fy + vdy * (lap(x, y) - lap(x, y - 1))) -
-          dtdx * (ke(x + 1, y) - ke(x, y) - dv4(x + 1, y) + dv4(x, y) - T(pgx));
     T fx = flux_con_pre<T>(tV.ptr(x, y), 1, ltV.ptr(x, y), rtV.ptr(x, y), 1, dtdx * ucL(x, y));
-    T v = svd(x, y) - dt * (suc(x, y) * fx + vdx * (lap(x, y) - lap(x - 1, y))) -
+    S u, v;
+    if constexpr (std::is_same_v<S, T>) {  // the reference's operations, in order
+      u = sud(x, y) + dt * (svc(x, y) * fy + vdy * (lap(x, y) - lap(x, y - 1))) -
+          dtdx * (ke(x + 1, y) - ke(x, y) - dv4(x + 1, y) + dv4(x, y) - T(pgx));
+      v = svd(x, y) - dt * (suc(x, y) * fx + vdx * (lap(x, y) - lap(x - 1, y))) -
           dtdy * (ke(x, y + 1) - ke(x, y) - dv4(x, y + 1) + dv4(x, y) - T(pgy));
+    } else {  // the tendency in the sweep type added to the state's type
+      const T du = dt * (svc(x, y) * fy + vdy * (lap(x, y) - lap(x, y - 1))) -
+                   dtdx * (ke(x + 1, y) - ke(x, y) - dv4(x + 1, y) + dv4(x, y) - T(pgx));
+      const T dv = -dt * (suc(x, y) * fx + vdx * (lap(x, y) - lap(x - 1, y))) -
+                   dtdy * (ke(x, y + 1) - ke(x, y) - dv4(x, y + 1) + dv4(x, y) - T(pgy));
+      u = bud(x, y) + S(du);
+      v = bvd(x, y) + S(dv);
+    }
     long long o = g.at(x, y, k);
     udo[o] = u;
     vdo[o] = v;

@@ -50,20 +50,27 @@ SAMPLE_N = 256
 
 # Algorithmic HBM words per interior cell and launch of each kernel: every
 # field the kernel must read or write once (layer-nlay slabs and halo rings
-# are excluded).  FP64 form: 8 bytes per word; the mixed form stores the
-# sweep fields in 4 bytes and pkap/gz in 8.
-#                 (sweep-type words, fp64 words)
+# are excluded), split by storage type: (state words, C-grid words, fp64
+# words).  The state (dp, pt, ud, vd) is FP64 in both forms; the C-grid
+# fields (dpc, ptc, uc, vc) are FP64 in the FP64 form and FP32 in the mixed
+# form; pkap, gz, pkapb, gzb are FP64.
 WORDS = {
-    'c_mass': (6, 0),        # read dp, pt, ud, vd; write dpc, ptc
-    'c_column': (2, 2),      # read dpc, ptc; write pkap, gz
-    'c_mom': (4, 2),         # read ud, vd, pkap, gz; write uc, vc
-    'd_mass': (6, 0),        # read dp, pt, uc, vc; write dp, pt
-    'd_column': (2, 2),      # read dp, pt; write pkap, gz
-    'd_corners': (0, 4),     # read pkap, gz; write pkapb, gzb
-    'd_mom': (6, 2),         # read ud, vd, uc, vc, pkapb, gzb; write ud, vd
-    'remap_winds': (5, 0),   # read dp, ud, vd; write u, v remapped
-    'remap_energy': (10, 0),  # read dp, pt, ud, vd, u, v remapped; write dp, pt, ud, vd
+    'c_mass': (4, 2, 0),        # read dp, pt, ud, vd; write dpc, ptc
+    'c_column': (0, 2, 2),      # read dpc, ptc; write pkap, gz
+    'c_mom': (2, 2, 2),         # read ud, vd, pkap, gz; write uc, vc
+    'd_mass': (4, 2, 0),        # read dp, pt, uc, vc; write dp, pt
+    'd_column': (2, 0, 2),      # read dp, pt; write pkap, gz
+    'd_corners': (0, 0, 4),     # read pkap, gz; write pkapb, gzb
+    'd_mom': (4, 2, 2),         # read ud, vd, uc, vc, pkapb, gzb; write ud, vd
+    'remap_winds': (5, 0, 0),   # read dp, ud, vd; write u, v remapped
+    'remap_energy': (10, 0, 0),  # read dp, pt, ud, vd, u, v remapped; write dp, pt, ud, vd
 }
+
+
+def kernel_bytes(stage, form, cells):
+    w_s, w_c, w_d = WORDS.get(stage, (0, 0, 0))
+    ec = 8 if form == 'fp64' else 4
+    return (w_s * 8 + w_c * ec + w_d * 8) * cells
 
 
 # DRAM bytes per interior cell and launch measured by ncu on the FP64 form
@@ -71,12 +78,6 @@ WORDS = {
 # cells; the profile summary in profiles/ gives the command)
 TRAFFIC_PER_CELL_FP64 = {'c_mass': 48.3, 'c_mom': 48.3, 'd_mass': 48.4, 'd_mom': 66.2, 'c_column': 31.4,
                          'd_column': 31.4}
-
-
-def kernel_bytes(stage, form, cells):
-    w_t, w_d = WORDS.get(stage, (0, 0))
-    es = 8 if form == 'fp64' else 4
-    return (w_t * es + w_d * 8) * cells
 
 
 def load_peaks():
