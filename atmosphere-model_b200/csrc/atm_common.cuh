@@ -89,7 +89,6 @@ __device__ __forceinline__ float fab(float a) { return fabsf(a); }
 // infinities, NaN and magnitudes near the ends of the exponent range take
 // the IEEE division.
 static __device__ __noinline__ double div_ieee(double x, double b) { return x / b; }
-static __device__ __noinline__ float div_ieee(float x, float b) { return x / b; }
 template <int B> __device__ __forceinline__ double div_const(double x) {
   constexpr double r = 1.0 / B;  // RN(1/B)
   double a = fabs(x);
@@ -98,14 +97,9 @@ template <int B> __device__ __forceinline__ double div_const(double x) {
   double e = __fma_rn(-q, (double)B, x);
   return __fma_rn(e, r, q);
 }
-template <int B> __device__ __forceinline__ float div_const(float x) {
-  constexpr float r = 1.0f / B;
-  float a = fabsf(x);
-  if (!(a > 0x1p-100f && a < 0x1p100f)) return div_ieee(x, (float)B);
-  float q = x * r;
-  float e = __fmaf_rn(-q, (float)B, x);
-  return __fmaf_rn(e, r, q);
-}
+// The mixed form's FP32 sweeps need no correctly rounded quotient: a
+// multiplication by the rounded reciprocal.
+template <int B> __device__ __forceinline__ float div_const(float x) { return x * (1.0f / B); }
 
 // Monotone slope dqi_mono(i) and raw slope dqi(i) of src/mod_sw_dyn.f90:870-875
 // from q(i-1), q(i), q(i+1).

@@ -36,15 +36,11 @@ static __global__ void k_div_check(unsigned long long n, unsigned long long seed
     unsigned long long b = mix64(seed * 0x100000001b3ULL + i);
     double x = __longlong_as_double((long long)b);
     if (i % 7 == 0) x = (double)(long long)(b % 2000001) - 1000000.0;
-    float xf = __int_as_float((int)(unsigned)b);
     bool ok = true;
     double q3 = div_const<3>(x), t3 = x / 3.0;
     double q12 = div_const<12>(x), t12 = x / 12.0;
     ok = ok && (__double_as_longlong(q3) == __double_as_longlong(t3) || (q3 != q3 && t3 != t3));
     ok = ok && (__double_as_longlong(q12) == __double_as_longlong(t12) || (q12 != q12 && t12 != t12));
-    float f3 = div_const<3>(xf), g3 = xf / 3.0f, f12 = div_const<12>(xf), g12 = xf / 12.0f;
-    ok = ok && (__float_as_int(f3) == __float_as_int(g3) || (f3 != f3 && g3 != g3));
-    ok = ok && (__float_as_int(f12) == __float_as_int(g12) || (f12 != f12 && g12 != g12));
     if (!ok) ++local;
   }
   if (local) atomicAdd(bad, local);

@@ -197,8 +197,8 @@ int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, const double* 
                       const double* pt, const double* ud, const double* vd, const double* gzs,
                       double* dp_out, double* pt_out, double* ud_out, double* vd_out, void* stream);
 
-/* the number of the n pseudo-random FP64 and FP32 arguments (all exponents,
-   plus integers) for which the device's FMA-corrected division by the
+/* the number of the n pseudo-random FP64 arguments (all exponents, plus
+   integers) for which the FP64 form's FMA-corrected division by the
    constants 3 and 12 differs from IEEE division (expected: 0) */
 int atm_device_div_check(long long n, long long seed, long long* mismatches);
 
