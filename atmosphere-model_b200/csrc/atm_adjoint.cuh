@@ -8,15 +8,17 @@
 // contributions that several points of one stage make to the same input
 // are summed with shared-memory atomics.  The adjoints of the tile's input
 // boxes are finally added to the global adjoint fields with atomics (tiles
-// overlap in their halos).  Local derivatives of the PPM and limiter
-// functions come from evaluating the forward's own templated functions on
-// DV numbers (atm_dual.cuh): the derivative of the branch-frozen forward.
+// overlap in their halos).  The local derivatives of the PPM fluxes, edge
+// limiters and monotone slopes are written out by hand, each following the
+// branch the forward took: the derivative of the branch-frozen forward.
+// Conventions at kinks (shared with the oracle's tangent-linear model):
+// d|x|/dx = 0 at x = 0; d copysign(a, b)/da = sgn(a) * (sign of b);
+// min/max pass the derivative of the argument they return.
 //
 // The reverse of each stage is cited by the forward lines it inverts; the
 // forward is src/mod_sw_dyn.f90 (C grid :80-416, D grid :424-773).
 #pragma once
 
-#include "atm_dual.cuh"
 #include "atm_sweeps.cuh"
 
 namespace atm {
@@ -95,64 +97,11 @@ __device__ __forceinline__ void slope_adj(const double* q, int s, double lam, do
   if (ap != 0.) sadd(lq + ls, ap);
 }
 
-// edge anomalies (eL, eR) of one cell from q(-1..1) and mono(-1..1)
-// (src/mod_sw_dyn.f90:877-911, flux_con_pre's precomputed edges)
-template <int V>
-__device__ __forceinline__ void edges_adj(const double* q, int sq, const double* mono, int sm, double lamL, double lamR,
-                                          double* lq, int slq, double* lm, int slm) {
-  if (lamL == 0. && lamR == 0.) return;
-  DV<6> qq[3], mm[3];
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    qq[j] = DV<6>::seeded(q[(j - 1) * sq], j);
-    mm[j] = DV<6>::seeded(mono[(j - 1) * sm], 3 + j);
-  }
-  DV<6> eL, eR;
-  edges_pre<DV<6>, V>(&qq[1], 1, &mm[1], 1, eL, eR);
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    double a = eL.d[j] * lamL + eR.d[j] * lamR;
-    double b = eL.d[3 + j] * lamL + eR.d[3 + j] * lamR;
-    if (a != 0.) sadd(lq + (j - 1) * slq, a);
-    if (b != 0.) sadd(lm + (j - 1) * slm, b);
-  }
-}
-
-// F = flux_pre<V>(q, mono, c) (src/mod_sw_dyn.f90:802-838 with the slopes
-// precomputed): adds lamF * dF/d(q, mono) to lq, lm and lamF * dF/dc to
-// lamc; returns F.
-template <int V>
-__device__ __forceinline__ double flux_pre_adj(const double* q, int sq, const double* mono, int sm, double c,
-                                               double lamF, double* lq, int slq, double* lm, int slm, double& lamc) {
-  const int o = (c > 0.) ? -1 : 0;  // upwind cell
-  DV<7> qq[3], mm[3];
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    qq[j] = DV<7>::seeded(q[(o + j - 1) * sq], j);
-    mm[j] = DV<7>::seeded(mono[(o + j - 1) * sm], 3 + j);
-  }
-  DV<7> cc = DV<7>::seeded(c, 6);
-  DV<7> sa = fab(cc);
-  DV<7> k1 = (DV<7>(1.) - DV<7>(2.) * sa) * (DV<7>(1.) - sa);
-  DV<7> k2 = sa * (sa - DV<7>(1.));
-  DV<7> eL, eR;
-  edges_pre<DV<7>, V>(&qq[1], 1, &mm[1], 1, eL, eR);
-  DV<7> F = (c > 0.) ? qq[1] + k1 * eR + k2 * eL : qq[1] + k1 * eL + k2 * eR;
-  if (lamF != 0.) {
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      if (F.d[j] != 0.) sadd(lq + (o + j - 1) * slq, F.d[j] * lamF);
-      if (F.d[3 + j] != 0.) sadd(lm + (o + j - 1) * slm, F.d[3 + j] * lamF);
-    }
-    lamc += F.d[6] * lamF;
-  }
-  return F.v;
-}
-
 // F = flux_pre<PPM_UNC>(q, mono, c), by hand: with u the upwind cell,
 // eL = (q(u-1) - q(u))/2 + (m(u-1) - m(u))/3, eR = (q(u+1) - q(u))/2 + (m(u) - m(u+1))/3,
 // F = q(u) + k1 eR + k2 eL (c > 0) or q(u) + k1 eL + k2 eR, k1 = (1-2s)(1-s),
-// k2 = s(s-1), s = |c|.  Same contract as flux_pre_adj.
+// k2 = s(s-1), s = |c|.  Adds lamF * dF/d(q, mono) to lq, lm (spacings
+// slq, slm around cell i) and lamF * dF/dc to lamc; returns F.
 __device__ __forceinline__ double flux_unc_adj(const double* q, int sq, const double* mono, int sm, double c,
                                                double lamF, double* lq, int slq, double* lm, int slm, double& lamc) {
   const int o = (c > 0.) ? -1 : 0;
@@ -185,7 +134,8 @@ __device__ __forceinline__ double flux_unc_adj(const double* q, int sq, const do
 
 // (eL, eR) = edges_pre<PPM_CONSTRAINED>(q, mono) of one cell, by hand
 // (src/mod_sw_dyn.f90:877-893): the raw edges, limited by 2|dqi| with the
-// sign of dqi.  Same contract as edges_adj.
+// sign of dqi: adds lamL * deL + lamR * deR with respect to q(-1..1) and
+// mono(-1..1) to lq, lm.
 __device__ __forceinline__ void edges_con_adj(const double* q, int sq, const double* mono, int sm, double lamL,
                                               double lamR, double* lq, int slq, double* lm, int slm) {
   if (lamL == 0. && lamR == 0.) return;
@@ -223,12 +173,94 @@ __device__ __forceinline__ void edges_con_adj(const double* q, int sq, const dou
   if (b_p != 0.) sadd(lm + slm, b_p);
 }
 
-// flux adjoint of variant V: by hand for PPM_UNCONSTRAINED, else on DV numbers
+// F = flux_pre<PPM_NONNEGATIVE>(q, mono, c), by hand: the upwind cell's
+// edges go through the chain of src/mod_sw_dyn.f90:877-911 -- raw edges,
+// the 2|dqi| clamp with the sign of dqi, the floor at -q0, and the
+// curvature fix-up (both zero, or one edge twice the other's magnitude) --
+// each step's derivative following the branch the forward took.  Same
+// contract as flux_unc_adj.
+__device__ __forceinline__ double flux_nn_adj(const double* q, int sq, const double* mono, int sm, double c,
+                                              double lamF, double* lq, int slq, double* lm, int slm, double& lamc) {
+  const int o = (c > 0.) ? -1 : 0;
+  const double* qu = q + o * sq;
+  const double* mu = mono + o * sm;
+  const double qm = qu[-sq], q0 = qu[0], qp = qu[sq], mm = mu[-sm], m0 = mu[0], mp = mu[sm];
+  // forward, with edges_pre's operations
+  const double eLr = (qm - q0) * 0.5 + div_const<3>(mm - m0);
+  const double eRr = (qp - q0) * 0.5 + div_const<3>(m0 - mp);
+  const double d0 = (qp - qm) * 0.25;
+  const double lim = 2. * fabs(d0);
+  const bool rawL = fabs(eLr) < lim, rawR = fabs(eRr) < lim;
+  const double eL1 = -copysign(mn(lim, fabs(eLr)), d0);
+  const double eR1 = +copysign(mn(lim, fabs(eRr)), d0);
+  const bool floorL = eL1 < -q0, floorR = eR1 < -q0;
+  const double eL2 = mx(eL1, -q0), eR2 = mx(eR1, -q0);
+  const double a = eR2 - eL2;
+  const double b = -3. * (eR2 + eL2);
+  int fix = 0;  // 0: none, 1: both zero, 2: eL = 2|eR|, 3: eR = 2|eL|
+  if ((fabs(a) < -b) && (q0 + a * a / (4. * b) + div_const<12>(b) < 0.)) {
+    if (eL2 * eR2 > 0.) fix = 1;
+    else if (eL2 > eR2) fix = 2;
+    else fix = 3;
+  }
+  const double eL3 = fix == 1 ? 0. : (fix == 2 ? 2. * fabs(eR2) : eL2);
+  const double eR3 = fix == 1 ? 0. : (fix == 3 ? 2. * fabs(eL2) : eR2);
+  const double sa = fabs(c);
+  const double k1 = (1. - 2. * sa) * (1. - sa);
+  const double k2 = sa * (sa - 1.);
+  const double F = (c > 0.) ? q0 + k1 * eR3 + k2 * eL3 : q0 + k1 * eL3 + k2 * eR3;
+  if (lamF == 0.) return F;
+  // reverse
+  const double lR3 = ((c > 0.) ? k1 : k2) * lamF, lL3 = ((c > 0.) ? k2 : k1) * lamF;
+  const double sgL2 = eL2 > 0. ? 1. : (eL2 < 0. ? -1. : 0.), sgR2 = eR2 > 0. ? 1. : (eR2 < 0. ? -1. : 0.);
+  double lL2, lR2;
+  if (fix == 0) { lL2 = lL3; lR2 = lR3; }
+  else if (fix == 1) { lL2 = 0.; lR2 = 0.; }
+  else if (fix == 2) { lL2 = 0.; lR2 = lR3 + 2. * sgR2 * lL3; }
+  else { lR2 = 0.; lL2 = lL3 + 2. * sgL2 * lR3; }
+  double lq0 = lamF;  // F's own q(u)
+  double lL1 = 0., lR1 = 0.;
+  if (floorL) lq0 -= lL2; else lL1 = lL2;
+  if (floorR) lq0 -= lR2; else lR1 = lR2;
+  const double sb = signbit(d0) ? -1. : 1.;
+  const double sd = d0 > 0. ? 1. : (d0 < 0. ? -1. : 0.);
+  double lLr = 0., lRr = 0., ld0 = 0.;
+  {  // eL1 = -copysign(mn(lim, |eLr|), d0)
+    const double av = rawL ? fabs(eLr) : lim;
+    const double la = -(av > 0. ? sb : 0.) * lL1;
+    if (rawL) lLr = (eLr > 0. ? 1. : (eLr < 0. ? -1. : 0.)) * la;
+    else ld0 += 2. * sd * la;
+  }
+  {  // eR1 = +copysign(mn(lim, |eRr|), d0)
+    const double av = rawR ? fabs(eRr) : lim;
+    const double la = (av > 0. ? sb : 0.) * lR1;
+    if (rawR) lRr = (eRr > 0. ? 1. : (eRr < 0. ? -1. : 0.)) * la;
+    else ld0 += 2. * sd * la;
+  }
+  double* lqu = lq + o * slq;
+  double* lmu = lm + o * slm;
+  const double a_m = .5 * lLr - .25 * ld0, a_0 = lq0 - .5 * (lLr + lRr), a_p = .5 * lRr + .25 * ld0;
+  if (a_m != 0.) sadd(lqu - slq, a_m);
+  if (a_0 != 0.) sadd(lqu, a_0);
+  if (a_p != 0.) sadd(lqu + slq, a_p);
+  const double b_m = lLr / 3., b_0 = (lRr - lLr) / 3., b_p = -lRr / 3.;
+  if (b_m != 0.) sadd(lmu - slm, b_m);
+  if (b_0 != 0.) sadd(lmu, b_0);
+  if (b_p != 0.) sadd(lmu + slm, b_p);
+  const double sg = c > 0. ? 1. : (c < 0. ? -1. : 0.);
+  const double dk1 = 4. * sa - 3., dk2 = 2. * sa - 1.;
+  lamc += sg * ((c > 0.) ? dk1 * eR3 + dk2 * eL3 : dk1 * eL3 + dk2 * eR3) * lamF;
+  return F;
+}
+
+// flux adjoint of the variant V of the mass sweeps (PPM_UNCONSTRAINED on
+// the C grid, PPM_NONNEGATIVE on the D grid)
 template <int V>
 __device__ __forceinline__ double flux_adj(const double* q, int sq, const double* mono, int sm, double c, double lamF,
                                            double* lq, int slq, double* lm, int slm, double& lamc) {
+  static_assert(V == PPM_UNC || V == PPM_NN, "the mass sweeps use PPM_UNCONSTRAINED or PPM_NONNEGATIVE");
   if constexpr (V == PPM_UNC) return flux_unc_adj(q, sq, mono, sm, c, lamF, lq, slq, lm, slm, lamc);
-  else return flux_pre_adj<V>(q, sq, mono, sm, c, lamF, lq, slq, lm, slm, lamc);
+  else return flux_nn_adj(q, sq, mono, sm, c, lamF, lq, slq, lm, slm, lamc);
 }
 
 // F = flux_con_pre(q, eL, eR, c) with precomputed PPM_CONSTRAINED edges
