@@ -110,6 +110,46 @@ __device__ __forceinline__ void region(int x0, int y0, F&& body) {
   }
 }
 
+// One stage's independent region loops as a single index space: the block's
+// threads share the whole stage evenly, where separate region() loops of
+// W*H a little above NT points each leave most threads idle in a last
+// partial pass.  regions(reg<W1, H1>(x1, y1, body1), reg<W2, H2>(...), ...).
+template <int W, int Hh, typename F>
+struct Reg {
+  static constexpr int N = W * Hh;
+  int x0, y0;
+  F body;
+  __device__ __forceinline__ void at(int idx) const {
+    const int y = idx / W;
+    body(x0 + idx - y * W, y0 + y);
+  }
+};
+template <int W, int Hh, typename F>
+__device__ __forceinline__ Reg<W, Hh, F> reg(int x0, int y0, F body) {
+  return Reg<W, Hh, F>{x0, y0, body};
+}
+template <typename R0, typename... Rs>
+__device__ __forceinline__ void reg_dispatch(int idx, const R0& r0, const Rs&... rs) {
+  if (idx < R0::N) r0.at(idx);
+  else if constexpr (sizeof...(Rs) > 0) reg_dispatch(idx - R0::N, rs...);
+}
+template <typename R>
+__device__ __forceinline__ void reg_loop(const R& r) {
+  for (int idx = threadIdx.x; idx < R::N; idx += NT) r.at(idx);
+}
+// MERGE = false runs the regions one after the other (separate loops), the
+// better schedule where the merged dispatch costs more registers than the
+// idle threads it saves.
+template <bool MERGE = true, typename... Rs>
+__device__ __forceinline__ void regions(const Rs&... rs) {
+  if constexpr (MERGE) {
+    constexpr int N = (Rs::N + ...);
+    for (int idx = threadIdx.x; idx < N; idx += NT) reg_dispatch(idx, rs...);
+  } else {
+    (reg_loop(rs), ...);
+  }
+}
+
 // Start of a TMA box whose first wanted column is i0, rounded down to a
 // 16-byte boundary of the tensor row.
 template <typename T>
@@ -212,19 +252,22 @@ __global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMa
   Sm<T> fyd = carve<T>(p, ox, oy, TX, TY + 1);
   Sm<T> fyp = carve<T>(p, ox, oy, TX, TY + 1);
 
+  // merged stage loops measured faster in FP32, slower in FP64
+  constexpr bool MG = std::is_same_v<T, float>;
   if constexpr (CGRID) {  // mod_sw_dyn.f90:109-117
-    region<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
+    regions<MG>(reg<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
       T ub = T(.5) * (T(su(x, y)) + T(su(x - 1, y)));
       suc(x, y) = T(.5) * (ub + T(.5) * (T(su(x, y + 1)) + T(su(x - 1, y + 1))));
-    });
-    region<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
+    }),
+            reg<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
       T vb = T(.5) * (T(sv(x, y)) + T(sv(x, y - 1)));
       svc(x, y) = T(.5) * (vb + T(.5) * (T(sv(x + 1, y)) + T(sv(x + 1, y - 1))));
-    });
+    }));
     __syncthreads();
   }
   // inner sweeps and Laplacians: mod_sw_dyn.f90:142-155,176-185 (C); 470-482,503-511 (D)
-  region<TX + 6, TY>(ox - 3, oy, [&](int x, int y) {
+  const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
+  regions<MG>(reg<TX + 6, TY>(ox - 3, oy, [&](int x, int y) {
     T cy0 = dtdx * svc(x, y), cy1 = dtdx * svc(x, y + 1);
     T den = T(1) / (T(1) - dtdy * (svc(x, y + 1) - svc(x, y)));
     const T d0 = T(sdp(x, y)), dm = T(sdp(x, y - 1)), dq = T(sdp(x, y + 1));
@@ -235,8 +278,8 @@ __global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMa
     f0 = (cy0 > T(0)) ? pm : p0;
     f1 = (cy1 > T(0)) ? p0 : pq;
     typ(x, y) = T(.5) * (p0 + den * (p0 - rA * (f1 - f0)));
-  });
-  region<TX, TY + 6>(ox, oy - 3, [&](int x, int y) {
+  }),
+          reg<TX, TY + 6>(ox, oy - 3, [&](int x, int y) {
     T cx0 = dtdx * suc(x, y), cx1 = dtdx * suc(x + 1, y);
     T den = T(1) / (T(1) - dtdx * (suc(x + 1, y) - suc(x, y)));
     const T d0 = T(sdp(x, y)), dm = T(sdp(x - 1, y)), dq = T(sdp(x + 1, y));
@@ -247,38 +290,35 @@ __global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMa
     f0 = (cx0 > T(0)) ? pm : p0;
     f1 = (cx1 > T(0)) ? p0 : pq;
     txp(x, y) = T(.5) * (p0 + den * (p0 - rA * (f1 - f0)));
-  });
-  {
-    const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
-    region<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
-      lpd(x, y) = T(-2.) * T(sdp(x, y)) * rdxy + (T(sdp(x + 1, y)) + T(sdp(x - 1, y))) * rdx2 +
-                  (T(sdp(x, y + 1)) + T(sdp(x, y - 1))) * rdy2;
-      lpp(x, y) = T(-2.) * T(spt(x, y)) * rdxy + (T(spt(x + 1, y)) + T(spt(x - 1, y))) * rdx2 +
-                  (T(spt(x, y + 1)) + T(spt(x, y - 1))) * rdy2;
-    });
-  }
+  }),
+          reg<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
+    lpd(x, y) = T(-2.) * T(sdp(x, y)) * rdxy + (T(sdp(x + 1, y)) + T(sdp(x - 1, y))) * rdx2 +
+                (T(sdp(x, y + 1)) + T(sdp(x, y - 1))) * rdy2;
+    lpp(x, y) = T(-2.) * T(spt(x, y)) * rdxy + (T(spt(x + 1, y)) + T(spt(x - 1, y))) * rdx2 +
+                (T(spt(x, y + 1)) + T(spt(x, y - 1))) * rdy2;
+  }));
   __syncthreads();
   // monotone slopes of the outer sweeps (ppm, :870-875)
-  region<TX + 4, TY>(ox - 2, oy, [&](int x, int y) {
+  regions<MG>(reg<TX + 4, TY>(ox - 2, oy, [&](int x, int y) {
     mxd(x, y) = slope_at(tyd.ptr(x, y), 1);
     mxp(x, y) = slope_at(typ.ptr(x, y), 1);
-  });
-  region<TX, TY + 4>(ox, oy - 2, [&](int x, int y) {
+  }),
+          reg<TX, TY + 4>(ox, oy - 2, [&](int x, int y) {
     myd(x, y) = slope_at(txd.ptr(x, y), TX);
     myp(x, y) = slope_at(txp.ptr(x, y), TX);
-  });
+  }));
   __syncthreads();
   // outer sweeps (PPM)
-  region<TX + 1, TY>(ox, oy, [&](int x, int y) {
+  regions<MG>(reg<TX + 1, TY>(ox, oy, [&](int x, int y) {
     T cx = dtdx * suc(x, y);
     fxd(x, y) = flux_pre<T, V>(tyd.ptr(x, y), 1, mxd.ptr(x, y), 1, cx) * cx;
     fxp(x, y) = flux_pre<T, V>(typ.ptr(x, y), 1, mxp.ptr(x, y), 1, cx);
-  });
-  region<TX, TY + 1>(ox, oy, [&](int x, int y) {
+  }),
+          reg<TX, TY + 1>(ox, oy, [&](int x, int y) {
     T cy = dtdx * svc(x, y);
     fyd(x, y) = flux_pre<T, V>(txd.ptr(x, y), TX, myd.ptr(x, y), TX, cy) * cy;
     fyp(x, y) = flux_pre<T, V>(txp.ptr(x, y), TX, myp.ptr(x, y), TX, cy);
-  });
+  }));
   __syncthreads();
 
   // updates, mod_sw_dyn.f90:163-172,193-202,230-237,258-267 (C); 490-499,519-528,555-562,582-591 (D)
@@ -403,64 +443,62 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
   Sm<T> mtV = carve<T>(p, ox - 1, oy, TX + 3, TY);          // slopes of tV along x
 
   // C-grid winds of this layer (first-loop values, mod_sw_dyn.f90:110-117)
-  region<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
+  // and A-grid winds of layer nlay (mod_sw_dyn.f90:110-125 at k = nlay)
+  regions(reg<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
     T ub = T(.5) * (sud(x, y) + sud(x - 1, y));
     uc1(x, y) = T(.5) * (ub + T(.5) * (sud(x, y + 1) + sud(x - 1, y + 1)));
     T vb = T(.5) * (svd(x, y) + svd(x, y - 1));
     vc1(x, y) = T(.5) * (vb + T(.5) * (svd(x + 1, y) + svd(x + 1, y - 1)));
-  });
-  // A-grid winds of layer nlay (mod_sw_dyn.f90:110-125 at k = nlay)
-  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
+  }),
+          reg<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
     T ub = T(.5) * (udL(x, y) + udL(x - 1, y));
     T ucl = T(.5) * (ub + T(.5) * (udL(x, y + 1) + udL(x - 1, y + 1)));
     uaL(x, y) = T(.5) * (ucl + T(.25) * (udL(x + 1, y) + udL(x, y) + udL(x + 1, y + 1) + udL(x, y + 1)));
     T vb = T(.5) * (vdL(x, y) + vdL(x, y - 1));
     T vcl = T(.5) * (vb + T(.5) * (vdL(x + 1, y) + vdL(x + 1, y - 1)));
     vaL(x, y) = T(.5) * (vcl + T(.25) * (vdL(x, y + 1) + vdL(x, y) + vdL(x + 1, y + 1) + vdL(x + 1, y)));
-  });
+  }));
   __syncthreads();
 
   const T f = T(c.coriolis);
   // vorticity (mod_sw_dyn.f90:319-323), slopes of the KE sweeps
-  region<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
+  regions(reg<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
     vor(x, y) = f - (uc1(x, y) - uc1(x, y - 1)) * rdy + (vc1(x, y) - vc1(x - 1, y)) * rdx;
-  });
-  region<TX + 1, TY + 4>(ox - 1, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(vc1.ptr(x, y), TX + 6); });
-  region<TX + 4, TY + 1>(ox - 2, oy - 1, [&](int x, int y) { mux(x, y) = slope_at(uc1.ptr(x, y), 1); });
+  }),
+          reg<TX + 1, TY + 4>(ox - 1, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(vc1.ptr(x, y), TX + 6); }),
+          reg<TX + 4, TY + 1>(ox - 2, oy - 1, [&](int x, int y) { mux(x, y) = slope_at(uc1.ptr(x, y), 1); }));
   __syncthreads();
 
-  // kinetic energy (:299-317): q(j) = vc(i, j+1), q(i) = uc(i+1, j)
-  region<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
+  // kinetic energy (:299-317): q(j) = vc(i, j+1), q(i) = uc(i+1, j); vorticity
+  // advection: inner sweeps and Laplacian (:344-367, 388-397)
+  const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
+  regions(reg<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
     T fy = flux_pre<T, PPM_UNC>(vc1.ptr(x, y + 1), TX + 6, mvy.ptr(x, y + 1), TX + 1, dtdy * vaL(x, y));
     T kv = vaL(x, y) * fy;
     T fx = flux_pre<T, PPM_UNC>(uc1.ptr(x + 1, y), 1, mux.ptr(x + 1, y), 1, dtdx * uaL(x, y));
     ke(x, y) = T(.5) * (kv + uaL(x, y) * fx);
-  });
-  // vorticity advection: inner sweeps and Laplacian (:344-367, 388-397)
-  region<TX, TY + 5>(ox, oy - 2, [&](int x, int y) {
+  }),
+          reg<TX, TY + 5>(ox, oy - 2, [&](int x, int y) {
     T c0 = dtdx * sud(x - 1, y), c1 = dtdx * sud(x, y);
     T den = T(1) / (T(1) - dtdx * (sud(x, y) - sud(x - 1, y)));
     T f0 = (c0 > T(0)) ? vor(x - 1, y) : vor(x, y);
     T f1 = (c1 > T(0)) ? vor(x, y) : vor(x + 1, y);
     tU(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
-  });
-  region<TX + 5, TY>(ox - 2, oy, [&](int x, int y) {
+  }),
+          reg<TX + 5, TY>(ox - 2, oy, [&](int x, int y) {
     T c0 = dtdx * svd(x, y - 1), c1 = dtdx * svd(x, y);
     T den = T(1) / (T(1) - dtdy * (svd(x, y) - svd(x, y - 1)));
     T f0 = (c0 > T(0)) ? vor(x, y - 1) : vor(x, y);
     T f1 = (c1 > T(0)) ? vor(x, y) : vor(x, y + 1);
     tV(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
-  });
-  {
-    const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
-    region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-      lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 +
-                  (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
-    });
-  }
+  }),
+          reg<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
+    lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 +
+                (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
+  }));
   __syncthreads();
-  region<TX, TY + 3>(ox, oy - 1, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); });
-  region<TX + 3, TY>(ox - 1, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); });
+  regions(reg<TX, TY + 3>(ox, oy - 1, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); }),
+          reg<TX + 3, TY>(ox - 1, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); }));
   __syncthreads();
 
   // uc, vc updates (:369-381, 399-411) with the PGF (:325-339)
