@@ -243,40 +243,44 @@ __device__ void vertical_ppm(PPMWork<LM>& w, int L, const double* var, const dou
   for (int k = 1; k <= L; ++k) w.curv[k] = 6. * var[k] - 3. * (w.top[k] + w.btm[k]);
 }
 
-// Contribution of source layer k to destination layer m, the body of the
-// pair loop of src/mod_remap.f90:188-280.  Returns the case tag(s).
-template <int LM>
-__device__ __forceinline__ int remap_pair(const PPMWork<LM>& w, const double* src_var, double* dst_var,
-                                          const double* sc, const double* dc, int k, int m) {
-  double dsrc = sc[k + 1] - sc[k];
-  double s1 = (dc[m] - sc[k]) / dsrc;
-  double s2 = (dc[m + 1] - sc[k]) / dsrc;
-  double integral_factor = dsrc / (dc[m + 1] - dc[m]);
+// Contribution of source layer k (edges btm, top, curvature cv, mean vk,
+// coordinates sk = coord(k), sk1 = coord(k+1)) to destination layer m
+// (coordinates d0 = coord(m), d1 = coord(m+1)), added to acc: the body of
+// the pair loop of src/mod_remap.f90:188-280.  Returns the case tag(s).
+__device__ __forceinline__ int pair_add(double& acc, double btm, double top, double cv, double vk, double sk,
+                                        double sk1, double d0, double d1) {
+  double dsrc = sk1 - sk;
+  double s1 = (d0 - sk) / dsrc;
+  double s2 = (d1 - sk) / dsrc;
+  double integral_factor = dsrc / (d1 - d0);
   int which = 0;
   double tmp3 = 2. * s1 * s1;
-  if (dc[m + 1] <= sc[k + 1] && sc[k + 1] < dc[m] && dc[m] < sc[k]) {
+  if (d1 <= sk1 && sk1 < d0 && d0 < sk) {
     double tmp1 = s1 - 1., tmp2 = s1 + 1.;
-    dst_var[m] = dst_var[m] + tmp1 / 6. * (3. * (w.btm[k] * tmp1 - w.top[k] * tmp2) + w.curv[k] * (tmp3 - tmp2)) *
-                                  integral_factor;
+    acc = acc + tmp1 / 6. * (3. * (btm * tmp1 - top * tmp2) + cv * (tmp3 - tmp2)) * integral_factor;
     which = 3;
   }
-  if (sc[k + 1] < dc[m + 1] && dc[m + 1] < sc[k] && sc[k] <= dc[m]) {
-    dst_var[m] = dst_var[m] + (s2 / 2.) * (w.btm[k] * (2. - s2) + s2 * (w.top[k] + w.curv[k] * (1. - C2_3 * s2))) *
-                                  integral_factor;
+  if (sk1 < d1 && d1 < sk && sk <= d0) {
+    acc = acc + (s2 / 2.) * (btm * (2. - s2) + s2 * (top + cv * (1. - C2_3 * s2))) * integral_factor;
     which = which * 10 + 4;
   }
-  if (dc[m + 1] <= sc[k + 1] && sc[k] <= dc[m]) {
-    dst_var[m] = dst_var[m] + src_var[k] * integral_factor;
+  if (d1 <= sk1 && sk <= d0) {
+    acc = acc + vk * integral_factor;
     which = which * 10 + 5;
   }
-  if (sc[k + 1] < dc[m + 1] && dc[m] < sc[k]) {
+  if (sk1 < d1 && d0 < sk) {
     double tmp1 = s1 + s2;
-    dst_var[m] = dst_var[m] + (s1 - s2) / 6. *
-                                  (3. * (w.btm[k] * (tmp1 - 2.) - w.top[k] * tmp1) + w.curv[k] * (tmp3 + tmp1 * (2. * s2 - 3.))) *
-                                  integral_factor;
+    acc = acc + (s1 - s2) / 6. * (3. * (btm * (tmp1 - 2.) - top * tmp1) + cv * (tmp3 + tmp1 * (2. * s2 - 3.))) *
+                    integral_factor;
     which = which * 10 + 6;
   }
   return which;
+}
+
+template <int LM>
+__device__ __forceinline__ int remap_pair(const PPMWork<LM>& w, const double* src_var, double* dst_var,
+                                          const double* sc, const double* dc, int k, int m) {
+  return pair_add(dst_var[m], w.btm[k], w.top[k], w.curv[k], src_var[k], sc[k], sc[k + 1], dc[m], dc[m + 1]);
 }
 
 // remap_column, src/mod_remap.f90:165-285.  When both coordinates are
@@ -331,9 +335,220 @@ __device__ void remap_column(PPMWork<LM>& w, int L, const double* src_var, doubl
   }
 }
 
+// ------------------------------------------------ streaming remap_column --
+// vertical_ppm + remap_column (src/mod_remap.f90:165-356) reorganised into
+// one descending and one ascending pass over the column, so that a column
+// keeps three stored arrays (the source coordinate, the interface values
+// before forward substitution, gam) instead of nine:
+//  * descending: the elimination of vertical_ppm (:296-309), fed level by
+//    level by the producer of the coordinate and of the remapped variable;
+//  * ascending: forward substitution (:311-313), boundary and monotonicity
+//    clamps (:316-334), the Huynh constraint (:339-352) and the curvature
+//    (:354) of layer k, produced when the pair loop (:188-280, visited as a
+//    monotone merge, see remap_column) first reaches layer k.
+// Every value comes from the same operations in the same order as in
+// vertical_ppm/remap_column above, so results and (k, m, case) sets are
+// identical; columns whose coordinates are not monotone take the
+// all-arrays path.
+
+// One column array, element k at p[k * s].
+struct ColArr {
+  double* p;
+  int s;
+  __device__ __forceinline__ double& operator[](int k) const { return p[k * s]; }
+};
+
+// Elimination sweep of vertical_ppm in descending k.  cnext() yields
+// coord(L+1), coord(L), ..., coord(1) and vnext() var(L), ..., var(1), one
+// call each in that order.  Stores lv (before forward substitution) for
+// levels 1..L+1, gam for 1..L and, with STORE_SC, the coordinate.  L >= 3.
+template <bool STORE_SC, typename FC, typename FV>
+__device__ __forceinline__ void ppm_eliminate(int L, FC&& cnext, FV&& vnext, ColArr sc, ColArr lv, ColArr gam) {
+  double c2 = cnext(), c1 = cnext(), c0 = cnext();  // coord(k+1), coord(k), coord(k-1)
+  if (STORE_SC) {
+    sc[L + 1] = c2;
+    sc[L] = c1;
+    sc[L - 1] = c0;
+  }
+  double v1 = vnext(), v0 = vnext();  // var(k), var(k-1)
+  double alpha = (c1 - c0) / (c2 - c1);
+  double beta = alpha * (.5 + alpha);
+  double lvk = (2. * alpha * (1. + alpha) * v1 + v0) / beta;
+  lv[L + 1] = lvk;
+  double g = (1. + alpha * (1.5 + alpha)) / beta;
+  gam[L] = g;
+  for (int k = L; k >= 2; --k) {
+    alpha = (c2 - c1) / (c1 - c0);
+    beta = 2. + 2. * alpha - g;
+    lvk = (3. * (v1 + alpha * v0) - lvk) / beta;
+    lv[k] = lvk;
+    g = alpha / beta;
+    gam[k - 1] = g;
+    if (k > 2) {
+      c2 = c1;
+      c1 = c0;
+      c0 = cnext();
+      if (STORE_SC) sc[k - 2] = c0;
+      v1 = v0;
+      v0 = vnext();
+    }
+  }
+  // v1 = var(2), v0 = var(1), lvk = lv(2), g = gam(1)
+  beta = 1. + alpha * (1.5 + alpha);
+  lv[1] = (2. * alpha * (1. + alpha) * v0 + v1 - beta * lvk) / (alpha * (.5 + alpha) - beta * g);
+}
+
+// Layer k's edges and curvature in ascending k from the eliminated column.
+template <typename FV>
+struct PPMLayers {
+  ColArr lv, gam;
+  int L;
+  const FV& var;  // var(k), k = 1..L
+  int k;
+  double lvf, lvc, vk, vk1, top, btm, curv;
+  __device__ __forceinline__ PPMLayers(ColArr lv_, ColArr gam_, int L_, const FV& v)
+      : lv(lv_), gam(gam_), L(L_), var(v), k(0) {
+    lvf = lv[1];
+    lvc = lvf;
+    vk1 = var(1);
+  }
+  __device__ __forceinline__ void next() {
+    ++k;
+    vk = vk1;
+    if (k < L) vk1 = var(k + 1);
+    const int j = k + 1;  // the level at the top of layer k
+    const double f = lv[j] - gam[k] * lvf;
+    double c = f;
+    if (j == L) {
+      c = mn(c, mx(vk1, vk));
+      c = mx(c, mn(vk1, vk));
+    }
+    if (j == 2) {
+      c = mn(c, mx(vk1, vk));
+      c = mx(c, mn(vk1, vk));
+    }
+    if (j >= 3 && j <= L) {
+      const double lo = mn(vk, vk1), hi = mx(vk, vk1);
+      if (j == L || gam[j + 1] * gam[j - 1] > 0) {
+        c = mn(c, hi);
+        c = mx(c, lo);
+      } else if (gam[j + 1] > 0) {
+        c = mx(c, lo);
+      } else {
+        c = mn(c, hi);
+      }
+    }
+    top = c;
+    btm = lvc;
+    if (k >= 3) {
+      const double gk1 = gam[k - 1];
+      double pmp1 = vk - 2. * gk1;
+      double lac1 = pmp1 + 1.5 * gam[k - 2];
+      top = mn(mx(top, mn3(vk, pmp1, lac1)), mx3(vk, pmp1, lac1));
+      pmp1 = vk + 2. * gam[k];
+      lac1 = pmp1 - 1.5 * gk1;
+      btm = mn(mx(btm, mn3(vk, pmp1, lac1)), mx3(vk, pmp1, lac1));
+    }
+    curv = 6. * vk - 3. * (top + btm);
+    lvf = f;
+    lvc = c;
+  }
+};
+
+// The pair loop as a monotone merge over the eliminated column: dst(m) for
+// m = 1..L in ascending order goes to put(m, value); dc(m) gives the
+// destination coordinate.  trace as in remap_column.
+template <typename FV, typename FD, typename FO>
+__device__ __forceinline__ void remap_merge(int L, ColArr sc, ColArr lv, ColArr gam, const FV& var, FD&& dc,
+                                            FO&& put, int* trace, long long ts) {
+  PPMLayers<FV> ly(lv, gam, L, var);
+  int k0 = 1;
+  double d0 = dc(1);
+  for (int m = 1; m <= L; ++m) {
+    const double d1 = dc(m + 1);
+    while (k0 <= L && sc[k0 + 1] >= d0) ++k0;
+    double acc = 0.;
+    int first = -1, last = -1, w0 = -1, w1 = -1, cnt = 0;
+    for (int k = k0; k <= L; ++k) {
+      const double sk = sc[k];
+      if (!(sk > d1)) break;
+      while (ly.k < k) ly.next();
+      const int which = pair_add(acc, ly.btm, ly.top, ly.curv, ly.vk, sk, sc[k + 1], d0, d1);
+      if (first < 0) {
+        first = k;
+        w0 = which;
+      }
+      last = k;
+      w1 = which;
+      ++cnt;
+    }
+    put(m, acc);
+    if (trace) {
+      int* t = trace + (long long)(m - 1) * 5 * ts;
+      t[0] = first;
+      t[ts] = last;
+      t[2 * ts] = w0;
+      t[3 * ts] = w1;
+      t[4 * ts] = cnt;
+    }
+    d0 = d1;
+  }
+}
+
 // Winds on the cell faces over [isd-1, ied+1]^2, src/mod_remap.f90:80-105.
 // The D-grid winds here still carry last step's halo (the remap runs before
-// the D-grid halo exchange), exactly as in the reference.
+// the D-grid halo exchange), exactly as in the reference.  Face column
+// (i, j), direction dir (0: u, columns (i, j-2..j+1); 1: v, (i-2..i+1, j)).
+// The all-arrays form, for columns with non-monotone coordinates.
+template <typename T, int LM>
+__device__ __noinline__ void remap_winds_full(const Geom& g, const RemapArgs& ra, const T* __restrict__ dp,
+                                              const T* __restrict__ f, T* __restrict__ r, int* tr, Status* st, int i,
+                                              int j, int dir) {
+  const int L = g.L;
+  double sc[LM + 2], dc[LM + 2], var[LM + 2], out[LM + 2];
+  PPMWork<LM> wk;
+  // a, b: the face's two neighbours (weight 7/12), c, d: the outer pair (1/12)
+  const long long oa = g.at(i, j);
+  const long long ob = dir == 0 ? g.at(i, j - 1) : g.at(i - 1, j);
+  const long long oc = dir == 0 ? g.at(i, j + 1) : g.at(i + 1, j);
+  const long long od = dir == 0 ? g.at(i, j - 2) : g.at(i - 2, j);
+  double psa = ra.ptop, psb = ra.ptop, psc = ra.ptop, psd = ra.ptop;
+  for (int k = L - 1; k >= 0; --k) {
+    const long long kk = (long long)k * g.S;
+    psa = psa + (double)dp[oa + kk];
+    psb = psb + (double)dp[ob + kk];
+    psc = psc + (double)dp[oc + kk];
+    psd = psd + (double)dp[od + kk];
+  }
+  double pa = ra.ptop, pb = ra.ptop, pc = ra.ptop, pd = ra.ptop;
+  for (int k = L + 1; k >= 1; --k) {
+    if (k <= L) {
+      long long kk = (long long)(k - 1) * g.S;
+      pa = pa + (double)dp[oa + kk];
+      pb = pb + (double)dp[ob + kk];
+      pc = pc + (double)dp[oc + kk];
+      pd = pd + (double)dp[od + kk];
+    }
+    sc[k] = C7_12 * (pa + pb) - C1_12 * (pc + pd);
+    double ta, tb, tc, td;
+    if (k <= L) {
+      double a = ra.ak[k - 1], b = ra.bk[k - 1];
+      ta = a + b * (psa - ra.ptop);
+      tb = a + b * (psb - ra.ptop);
+      tc = a + b * (psc - ra.ptop);
+      td = a + b * (psd - ra.ptop);
+    } else {
+      ta = tb = tc = td = ra.ptop;
+    }
+    dc[k] = C7_12 * (ta + tb) - C1_12 * (tc + td);
+  }
+  for (int k = 1; k <= L; ++k) var[k] = (double)f[oa + (long long)(k - 1) * g.S];
+  remap_column<LM>(wk, L, var, out, sc, dc, tr, 1, &st->fallback_pairs);
+  for (int k = 1; k <= L; ++k) r[oa + (long long)(k - 1) * g.S] = T(out[k]);
+}
+
+// One thread per face column and direction (blockIdx.y); three column
+// arrays of LM + 2 doubles per thread.
 template <typename T, int LM>
 __global__ void __launch_bounds__(64) k_remap_winds(Geom g, RemapArgs ra, const T* __restrict__ dp,
                                                     const T* __restrict__ ud, const T* __restrict__ vd,
@@ -343,72 +558,81 @@ __global__ void __launch_bounds__(64) k_remap_winds(Geom g, RemapArgs ra, const 
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= w * h) return;
   const int i = -1 + col % w, j = -1 + col / w;
+  const int dir = blockIdx.y;
   const int L = g.L;
-  double sc[LM + 2], dc[LM + 2], var[LM + 2], out[LM + 2];
-  PPMWork<LM> wk;
-  // surface pressures of the seven columns involved
-  const int cx[7] = {i, i, i, i, i - 2, i - 1, i + 1};
-  const int cy[7] = {j - 2, j - 1, j, j + 1, j, j, j};
-  double ps[7];
-  for (int q = 0; q < 7; ++q) {
-    long long o = g.at(cx[q], cy[q]);
-    double pl = ra.ptop;
-    for (int k = L - 1; k >= 0; --k) pl = pl + (double)dp[o + (long long)k * g.S];
-    ps[q] = pl;
-  }
-  for (int dir = 0; dir < 2; ++dir) {
-    // u: columns (i, j-2..j+1) -> q = 0..3 ; v: (i-2..i+1, j) -> q = 4, 5, 2, 6
-    const int qa = dir == 0 ? 2 : 2, qb = dir == 0 ? 1 : 5, qc = dir == 0 ? 3 : 6, qd = dir == 0 ? 0 : 4;
-    long long oa = g.at(cx[qa], cy[qa]), ob = g.at(cx[qb], cy[qb]), oc = g.at(cx[qc], cy[qc]), od = g.at(cx[qd], cy[qd]);
-    double pa = ra.ptop, pb = ra.ptop, pc = ra.ptop, pd = ra.ptop;
-    for (int k = L + 1; k >= 1; --k) {
-      if (k <= L) {
-        long long kk = (long long)(k - 1) * g.S;
-        pa = pa + (double)dp[oa + kk];
-        pb = pb + (double)dp[ob + kk];
-        pc = pc + (double)dp[oc + kk];
-        pd = pd + (double)dp[od + kk];
-      }
-      sc[k] = C7_12 * (pa + pb) - C1_12 * (pc + pd);
-      double ta, tb, tc, td;
-      if (k <= L) {
-        double a = ra.ak[k - 1], b = ra.bk[k - 1];
-        ta = a + b * (ps[qa] - ra.ptop);
-        tb = a + b * (ps[qb] - ra.ptop);
-        tc = a + b * (ps[qc] - ra.ptop);
-        td = a + b * (ps[qd] - ra.ptop);
-      } else {
-        ta = tb = tc = td = ra.ptop;
-      }
-      dc[k] = C7_12 * (ta + tb) - C1_12 * (tc + td);
+  const long long S = g.S;
+  const T* f = dir == 0 ? ud : vd;
+  T* r = dir == 0 ? urem : vrem;
+  int* tr = nullptr;
+  if (trace) tr = trace + ((long long)dir * h * w + (long long)(j + 1) * w + (i + 1)) * L * 5;  // [3][ny+2][nx+2][L][5]
+  double arr[3 * (LM + 2)];
+  const ColArr sc{arr, 1}, lv{arr + (LM + 2), 1}, gam{arr + 2 * (LM + 2), 1};
+  const long long oa = g.at(i, j);
+  const long long ob = dir == 0 ? g.at(i, j - 1) : g.at(i - 1, j);
+  const long long oc = dir == 0 ? g.at(i, j + 1) : g.at(i + 1, j);
+  const long long od = dir == 0 ? g.at(i, j - 2) : g.at(i - 2, j);
+  // source coordinate: running sums from the model top (the face
+  // interpolation of src/mod_remap.f90:84-85 of the levels of :42-44)
+  double pa = ra.ptop, pb = ra.ptop, pc = ra.ptop, pd = ra.ptop, prev = 0.;
+  int kc = L + 2, kv = L + 1;
+  bool mono = true;
+  auto cnext = [&]() {
+    --kc;
+    if (kc <= L) {
+      const long long kk = (long long)(kc - 1) * S;
+      pa = pa + (double)dp[oa + kk];
+      pb = pb + (double)dp[ob + kk];
+      pc = pc + (double)dp[oc + kk];
+      pd = pd + (double)dp[od + kk];
     }
-    const T* f = dir == 0 ? ud : vd;
-    long long o = g.at(i, j);
-    for (int k = 1; k <= L; ++k) var[k] = (double)f[o + (long long)(k - 1) * g.S];
-    int* tr = nullptr;
-    long long ts = 1;
-    if (trace) {
-      // layout [3][ny+2][nx+2][L][5]
-      tr = trace + ((long long)dir * h * w + (long long)(j + 1) * w + (i + 1)) * L * 5;
+    const double c = C7_12 * (pa + pb) - C1_12 * (pc + pd);
+    if (kc <= L) mono = mono && (prev <= c);
+    prev = c;
+    return c;
+  };
+  auto vnext = [&]() {
+    --kv;
+    return (double)f[oa + (long long)(kv - 1) * S];
+  };
+  ppm_eliminate<true>(L, cnext, vnext, sc, lv, gam);
+  // pa..pd now hold the surface pressures of the four columns
+  auto dc = [&](int k) {
+    double ta, tb, tc, td;
+    if (k <= L) {
+      const double a = ra.ak[k - 1], b = ra.bk[k - 1];
+      ta = a + b * (pa - ra.ptop);
+      tb = a + b * (pb - ra.ptop);
+      tc = a + b * (pc - ra.ptop);
+      td = a + b * (pd - ra.ptop);
+    } else {
+      ta = tb = tc = td = ra.ptop;
     }
-    remap_column<LM>(wk, L, var, out, sc, dc, tr, ts, &st->fallback_pairs);
-    T* r = dir == 0 ? urem : vrem;
-    for (int k = 1; k <= L; ++k) r[o + (long long)(k - 1) * g.S] = T(out[k]);
+    return C7_12 * (ta + tb) - C1_12 * (tc + td);
+  };
+  double dprev = dc(1);
+  for (int k = 2; k <= L + 1; ++k) {
+    const double d = dc(k);
+    mono = mono && (d <= dprev);
+    dprev = d;
   }
+  if (!mono) {
+    remap_winds_full<T, LM>(g, ra, dp, f, r, tr, st, i, j, dir);
+    return;
+  }
+  auto var = [&](int k) { return (double)f[oa + (long long)(k - 1) * S]; };
+  remap_merge(L, sc, lv, gam, var, dc, [&](int m, double v) { r[oa + (long long)(m - 1) * S] = T(v); }, tr, 1);
 }
 
 // Energy remap and potential-temperature recovery on the interior,
-// src/mod_remap.f90:42-78 (columns) and 111-161.
+// src/mod_remap.f90:42-78 (columns) and 111-161.  The all-arrays form, for
+// columns with non-monotone coordinates.
 template <typename T, int LM>
-__global__ void __launch_bounds__(64) k_remap_energy(Geom g, RemapArgs ra, const T* __restrict__ dp,
-                                                     const T* __restrict__ pt, const T* __restrict__ ud,
-                                                     const T* __restrict__ vd, const T* __restrict__ urem,
-                                                     const T* __restrict__ vrem, const double* __restrict__ gzs,
-                                                     T* __restrict__ dpo, T* __restrict__ pto, T* __restrict__ udo,
-                                                     T* __restrict__ vdo, int* trace, Status* st) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= g.nx * g.ny) return;
-  const int i = col % g.nx, j = col / g.nx;
+__device__ __noinline__ void remap_energy_full(const Geom& g, const RemapArgs& ra, const T* __restrict__ dp,
+                                               const T* __restrict__ pt, const T* __restrict__ ud,
+                                               const T* __restrict__ vd, const T* __restrict__ urem,
+                                               const T* __restrict__ vrem, const double* __restrict__ gzs,
+                                               T* __restrict__ dpo, T* __restrict__ pto, T* __restrict__ udo,
+                                               T* __restrict__ vdo, int* tr, Status* st, int i, int j) {
   const int L = g.L;
   const long long S = g.S;
   const long long o = g.at(i, j);
@@ -442,11 +666,6 @@ __global__ void __launch_bounds__(64) k_remap_energy(Geom g, RemapArgs ra, const
                  .125 * ((double)vd[ok - P] + (double)vd[ok + 1 - P] + (double)vd[ok + P] + (double)vd[ok + 1 + P]));
     en[k] = CV_DRY * (double)pt[ok] * lyk[k] + .5 * (gzv[k + 1] + gzv[k] + ua * ua + va * va);
   }
-  int* tr = nullptr;
-  if (trace) {
-    const int w = g.nx + 2, h = g.ny + 2;
-    tr = trace + ((long long)2 * h * w + (long long)(j + 1) * w + (i + 1)) * L * 5;
-  }
   remap_column<LM>(wk, L, en, er, plev, tpl, tr, 1, &st->fallback_pairs);
   double gzr = gzv[1];
   bool bad = false;
@@ -466,6 +685,109 @@ __global__ void __launch_bounds__(64) k_remap_energy(Geom g, RemapArgs ra, const
     vdo[ok] = vn;
     bad = bad || !(finite_(dpn) && finite_(tn) && finite_(un) && finite_(vn));
   }
+  flag_nonfinite(&st->nonfinite_remap, bad);
+}
+
+// One thread per interior column; four column arrays of LM + 2 doubles per
+// thread (levels, pkap then the eliminated interface values, energy, gam).
+template <typename T, int LM>
+__global__ void __launch_bounds__(64) k_remap_energy(Geom g, RemapArgs ra, const T* __restrict__ dp,
+                                                     const T* __restrict__ pt, const T* __restrict__ ud,
+                                                     const T* __restrict__ vd, const T* __restrict__ urem,
+                                                     const T* __restrict__ vrem, const double* __restrict__ gzs,
+                                                     T* __restrict__ dpo, T* __restrict__ pto, T* __restrict__ udo,
+                                                     T* __restrict__ vdo, int* trace, Status* st) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= g.nx * g.ny) return;
+  const int i = col % g.nx, j = col / g.nx;
+  const int L = g.L;
+  const long long S = g.S;
+  const long long o = g.at(i, j);
+  const int P = g.P;
+  int* tr = nullptr;
+  if (trace) {
+    const int w = g.nx + 2, h = g.ny + 2;
+    tr = trace + ((long long)2 * h * w + (long long)(j + 1) * w + (i + 1)) * L * 5;
+  }
+  double arr[4 * (LM + 2)];
+  const ColArr plev{arr, 1}, pk{arr + (LM + 2), 1}, en{arr + 2 * (LM + 2), 1}, gam{arr + 3 * (LM + 2), 1};
+  const ColArr lv = pk;  // pkap is dead once the energy is formed
+  // current levels and pkap (src/mod_remap.f90:42-54), downward
+  bool mono = true;
+  plev[L + 1] = ra.ptop;
+  pk[L + 1] = ra.pk_top;
+  double pl = ra.ptop;
+  for (int k = L; k >= 1; --k) {
+    const double pn = pl + (double)dp[o + (long long)(k - 1) * S];
+    mono = mono && (pl <= pn);
+    plev[k] = pn;
+    pk[k] = atm_pow(pn, KAPPA);
+    pl = pn;
+  }
+  const double ps = pl;
+  // gz (:70-75) and the total energy (:111-125), upward
+  {
+    double gz0 = gzs[o], pk0 = pk[1];
+    for (int k = 1; k <= L; ++k) {
+      const long long ok = o + (long long)(k - 1) * S;
+      const double pk1 = pk[k + 1];
+      const double ptk = (double)pt[ok];
+      const double gz1 = gz0 + CP_DRY * ptk * (pk0 - pk1);
+      const double plog = atm_log(pk1 / pk0);
+      const double lyk = (pk1 - pk0) / plog;
+      double ua = (.25 * ((double)ud[ok] + (double)ud[ok + P]) +
+                   .125 * ((double)ud[ok - 1] + (double)ud[ok - 1 + P] + (double)ud[ok + 1] + (double)ud[ok + 1 + P]));
+      double va = (.25 * ((double)vd[ok] + (double)vd[ok + 1]) +
+                   .125 * ((double)vd[ok - P] + (double)vd[ok + 1 - P] + (double)vd[ok + P] + (double)vd[ok + 1 + P]));
+      en[k] = CV_DRY * ptk * lyk + .5 * (gz1 + gz0 + ua * ua + va * va);
+      gz0 = gz1;
+      pk0 = pk1;
+    }
+  }
+  // target levels (:57-59)
+  auto tpl = [&](int k) { return k <= L ? ra.ak[k - 1] + ra.bk[k - 1] * (ps - ra.ptop) : ra.ptop; };
+  {
+    double tprev = tpl(1);
+    for (int k = 2; k <= L + 1; ++k) {
+      const double t = tpl(k);
+      mono = mono && (t <= tprev);
+      tprev = t;
+    }
+  }
+  if (!mono) {
+    remap_energy_full<T, LM>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, tr, st, i, j);
+    return;
+  }
+  int kc = L + 2, kv = L + 1;
+  ppm_eliminate<false>(L, [&]() { return plev[--kc]; }, [&]() { return en[--kv]; }, plev, lv, gam);
+  // remapped energy -> potential temperature (:127-161), upward
+  double gzr = gzs[o];
+  double tpl0 = tpl(1);
+  double tpk0 = atm_pow(tpl0, KAPPA);
+  bool bad = false;
+  auto put = [&](int m, double erm) {
+    const long long ok = o + (long long)(m - 1) * S;
+    const double tpl1 = tpl(m + 1);
+    const double tpk1 = m < L ? atm_pow(tpl1, KAPPA) : ra.pk_top;
+    const double plog = atm_log(tpk1 / tpk0);
+    const double tlyk = (tpk1 - tpk0) / plog;
+    double ua = (.25 * ((double)urem[ok] + (double)urem[ok + P]) +
+                 .125 * ((double)urem[ok - 1] + (double)urem[ok - 1 + P] + (double)urem[ok + 1] + (double)urem[ok + 1 + P]));
+    double va = (.25 * ((double)vrem[ok] + (double)vrem[ok + 1]) +
+                 .125 * ((double)vrem[ok - P] + (double)vrem[ok + 1 - P] + (double)vrem[ok + P] + (double)vrem[ok + 1 + P]));
+    double ptr = (erm - gzr - .5 * (ua * ua + va * va)) / (CV_DRY * tlyk + .5 * CP_DRY * (tpk0 - tpk1));
+    gzr = gzr + CP_DRY * ptr * (tpk0 - tpk1);
+    T dpn = T(tpl0 - tpl1);
+    T un = urem[ok], vn = vrem[ok], tn = T(ptr);
+    dpo[ok] = dpn;
+    pto[ok] = tn;
+    udo[ok] = un;
+    vdo[ok] = vn;
+    bad = bad || !(finite_(dpn) && finite_(tn) && finite_(un) && finite_(vn));
+    tpl0 = tpl1;
+    tpk0 = tpk1;
+  };
+  remap_merge(L, plev, lv, gam, [&](int k) { return en[k]; }, tpl, put, tr, 1);
   flag_nonfinite(&st->nonfinite_remap, bad);
 }
 

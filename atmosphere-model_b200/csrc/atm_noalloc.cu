@@ -52,7 +52,7 @@ cudaError_t launch(const atm::Geom& g, const atm::RemapArgs& ra, const double* d
                    const double* ud, const double* vd, const double* gzs, double* urem, double* vrem, double* dpo,
                    double* pto, double* udo, double* vdo, atm::Status* st, cudaStream_t s) {
   int nw = (g.nx + 2) * (g.ny + 2);
-  atm::k_remap_winds<double, LM><<<(nw + 63) / 64, 64, 0, s>>>(g, ra, dp, ud, vd, urem, vrem, nullptr, st);
+  atm::k_remap_winds<double, LM><<<dim3((nw + 63) / 64, 2), 64, 0, s>>>(g, ra, dp, ud, vd, urem, vrem, nullptr, st);
   int ne = g.nx * g.ny;
   atm::k_remap_energy<double, LM><<<(ne + 63) / 64, 64, 0, s>>>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto,
                                                                 udo, vdo, nullptr, st);
