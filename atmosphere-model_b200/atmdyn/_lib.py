@@ -17,6 +17,7 @@ CSRC = os.path.join(os.path.dirname(HERE), 'csrc')
 
 ATM_DP, ATM_PT, ATM_UD, ATM_VD, ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX = range(8)
 ATM_DPC, ATM_PTC, ATM_UC, ATM_VC = range(8, 12)
+ATM_TS = 12
 ATM_FP64, ATM_MIXED = 0, 1
 STATUS = {0: 'ATM_OK', 1: 'ATM_ERR_ARG', 2: 'ATM_ERR_CUDA', 3: 'ATM_ERR_STATE',
           4: 'ATM_ERR_NOMEM', 5: 'ATM_ERR_UNSUPPORTED', 6: 'ATM_ERR_TOO_LARGE'}
@@ -32,7 +33,8 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_adj_get_device', 'atm_adj_step', 'atm_adj_halo', 'atm_adj_cgrid_halo', 'atm_adj_cgrid_step',
            'atm_adj_dgrid_step', 'atm_adj_remap', 'atm_state_bytes', 'atm_state_save', 'atm_state_load',
            'atm_tape_bytes', 'atm_step_tape', 'atm_adj_step_tape', 'atm_output_enable', 'atm_output_reset',
-           'atm_accumulate_output', 'atm_output_read', 'atm_output_time')
+           'atm_accumulate_output', 'atm_output_read', 'atm_output_time', 'atm_physics_tendencies',
+           'atm_apply_physics', 'atm_physics_halo')
 ATM_ADJ_IN, ATM_ADJ_OUT = 0, 1
 
 # the entry points every build must export
@@ -114,6 +116,9 @@ def load():
         'atm_accumulate_output': ([vp, d], None),
         'atm_output_read': ([vp, i, P], None),
         'atm_output_time': ([vp, P], None),
+        'atm_physics_tendencies': ([vp], None),
+        'atm_apply_physics': ([vp, d], None),
+        'atm_physics_halo': ([vp], None),
     }
     for f, (args, res) in optional.items():
         if hasattr(lib, f):

@@ -14,12 +14,12 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import check, ATM_DP, ATM_PT, ATM_UD, ATM_VD, ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX
+from ._lib import check, ATM_DP, ATM_PT, ATM_UD, ATM_VD, ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX, ATM_TS
 
 HALO = 7
 FIELDS = {'dp': ATM_DP, 'pt': ATM_PT, 'ud': ATM_UD, 'vd': ATM_VD, 'gz': ATM_GZ,
           'plev': ATM_PLEV, 'pkap': ATM_PKAP, 'net_flux': ATM_NET_FLUX,
-          'dpc': 8, 'ptc': 9, 'uc': 10, 'vc': 11}
+          'dpc': 8, 'ptc': 9, 'uc': 10, 'vc': 11, 'ts': ATM_TS}
 _P = ctypes.POINTER(ctypes.c_double)
 
 
@@ -56,6 +56,8 @@ class Dycore:
         gz = np.zeros((st.nlay + 1, st.ny, st.nx))
         gz[0] = st.gzs
         self.upload(ATM_GZ, with_halo(gz))
+        if getattr(st, 'ts', None) is not None:
+            self.upload(ATM_TS, with_halo(np.asarray(st.ts, dtype=np.float64)[None]))
         check(self.lib.atm_init(self.ctx), self.ctx, 'atm_init')
 
     def close(self):
@@ -70,6 +72,8 @@ class Dycore:
             pass
 
     def levels(self, field):
+        if field == ATM_TS:
+            return 1
         return self.nlay + 1 if field in (ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX) else self.nlay
 
     def upload(self, field, a):
@@ -127,6 +131,16 @@ class Dycore:
         check(self.lib.atm_step(self.ctx, dt, int(remap), ctypes.byref(s) if check_stable else None),
               self.ctx, 'atm_step')
         return bool(s.value)
+
+    # column physics (src/mod_physics.f90)
+    def physics_tendencies(self):
+        check(self.lib.atm_physics_tendencies(self.ctx), self.ctx, 'atm_physics_tendencies')
+
+    def apply_physics(self, dt):
+        check(self.lib.atm_apply_physics(self.ctx, dt), self.ctx, 'atm_apply_physics')
+
+    def physics_halo(self):
+        check(self.lib.atm_physics_halo(self.ctx), self.ctx, 'atm_physics_halo')
 
     def mass(self):
         m = ctypes.c_double(0.)
@@ -204,9 +218,9 @@ class Dycore:
         check(self.lib.atm_accumulate_output(self.ctx, dt), self.ctx, 'atm_accumulate_output')
 
     def output_read(self, name):
-        """Mean over the interval of 'dp', 'pt', 'u', 'v' or 'nflx', (K, ny, nx)."""
-        which = {'dp': 0, 'pt': 1, 'u': 2, 'v': 3, 'nflx': 4}[name]
-        K = self.nlay + 1 if name == 'nflx' else self.nlay
+        """Mean over the interval of 'dp', 'pt', 'u', 'v', 'nflx' or 'ts', (K, ny, nx)."""
+        which = {'dp': 0, 'pt': 1, 'u': 2, 'v': 3, 'nflx': 4, 'ts': 5}[name]
+        K = self.nlay + 1 if name == 'nflx' else 1 if name == 'ts' else self.nlay
         out = np.empty((K, self.ny, self.nx))
         check(self.lib.atm_output_read(self.ctx, which, _ptr(out)), self.ctx, 'atm_output_read')
         return out

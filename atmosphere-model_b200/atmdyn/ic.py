@@ -58,6 +58,7 @@ class InitialState:
     nsteps: int = 100
     name: str = ''
     extra: dict = field(default_factory=dict)
+    ts: np.ndarray | None = None  # (ny, nx) surface temperature (the physics' only 2-D prognostic)
 
     @property
     def cells(self) -> int:

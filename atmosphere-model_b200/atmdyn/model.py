@@ -1,11 +1,13 @@
 """Host-side time loop of the dynamical core, mirroring the reference's
 ``run_model`` (src/mod_model.f90:91-199) and ``calculate_dt``
-(src/mod_model.f90:201-237) with radiation and physics switched off.
+(src/mod_model.f90:201-237) with radiation switched off.
 
 A *stepper* is anything with the reference's dycore entry points:
 ``cgrid_step(dt_half)``, ``cgrid_halo()``, ``dgrid_step(dt)``, ``remap()``,
-``dgrid_halo()`` and ``check_stability() -> bool``.  The CUDA library
-(:class:`atmdyn.Dycore`) is one; the CPU oracle used by the tests is another.
+``dgrid_halo()`` and ``check_stability() -> bool``, and, for a run with
+physics, ``physics_tendencies()``, ``apply_physics(dt)`` and
+``physics_halo()``.  The CUDA library (:class:`atmdyn.Dycore`) is one; the
+CPU oracle used by the tests is another.
 """
 from __future__ import annotations
 
@@ -86,13 +88,15 @@ class RunResult:
 
 
 def run_model(stepper, tc: TimeControl, max_steps: int | None = None,
-              on_step=None, accumulate=None, write=None) -> RunResult:
-    """The dycore part of ``run_model`` (mod_model.f90:112-193): each step is
-    C-grid half step, halo, D-grid step, remap if due, halo, stability
-    check, then ``accumulate(dt)`` (accumulate_output) and, when the
-    schedule says so, ``write(time_stamp)`` (write_output, stamped
-    .5 (previous_write_time + time) as the reference does).  Radiation
-    (net_flux) and physics tendencies are not computed."""
+              on_step=None, accumulate=None, write=None, physics: bool = False) -> RunResult:
+    """``run_model`` (mod_model.f90:112-193) without radiation: each step is
+    [physics tendencies when due], C-grid half step, halo, D-grid step,
+    [apply the physics tendencies], remap if due, halo, [physics halo],
+    stability check, then ``accumulate(dt)`` (accumulate_output) and, when
+    the schedule says so, ``write(time_stamp)`` (write_output, stamped
+    .5 (previous_write_time + time) as the reference does).  The bracketed
+    physics calls run when ``physics`` is true; the net flux (radiation)
+    is whatever the caller set (zero by default)."""
     sch = Schedule(tc)
     time = tc.t_initial
     n = 0
@@ -102,15 +106,22 @@ def run_model(stepper, tc: TimeControl, max_steps: int | None = None,
         sch.calculate_radiation_this_step = False
         n += 1
         dt = sch.calculate_dt(time)
-        sch.calculate_physics_this_step = False
+        if sch.calculate_physics_this_step:
+            if physics:
+                stepper.physics_tendencies()
+            sch.calculate_physics_this_step = False
         stepper.cgrid_step(dt / 2.0)
         stepper.cgrid_halo()
         stepper.dgrid_step(dt)
+        if physics:
+            stepper.apply_physics(dt)
         if sch.remap_this_step:
             stepper.remap()
             sch.remap_this_step = False
             remaps.append(n)
         stepper.dgrid_halo()
+        if physics:
+            stepper.physics_halo()
         stable = bool(stepper.check_stability())
         if not stable:
             break

@@ -9,8 +9,9 @@ the reference's time loop (src/mod_model.f90:112-199: schedule, C/D-grid
 steps, remap when due, halo fills, stability check), accumulates the
 output means on the device (src/mod_output.f90:94-142) and writes them to
 output.nc when an output interval ends, and writes the restart file at the
-end when the namelist asks for it.  Radiation and physics are not run (zero
-net flux and tendencies), so ts is carried through unchanged.
+end when the namelist asks for it.  The physics (src/mod_physics.f90: dry
+convective adjustment, surface heating) runs on the device when due;
+radiation is not run, so the net flux is zero and ts keeps its value.
 """
 from __future__ import annotations
 
@@ -48,19 +49,21 @@ def main(argv=None):
     def write(stamp):
         means = {n: dyn.output_read(n) for n in ('dp', 'pt', 'u', 'v', 'nflx')}
         if st.ts is not None:
-            means['ts'] = st.ts
+            means['ts'] = dyn.output_read('ts')[0]
         writer.write(stamp, means)
         dyn.output_reset()
         records.append(stamp)
 
-    res = run_model(dyn, tc, max_steps=args.max_steps, accumulate=dyn.accumulate_output, write=write)
+    res = run_model(dyn, tc, max_steps=args.max_steps, accumulate=dyn.accumulate_output, write=write,
+                    physics=True)
     writer.close()
     restart = None
     if cfg.save_restart_file and res.stable:
         restart = cfg.restart_filename if os.path.isabs(cfg.restart_filename) else os.path.join(
             base, cfg.restart_filename)
         os.makedirs(os.path.dirname(os.path.abspath(restart)), exist_ok=True)
-        write_restart(restart, st, dyn.state(), res.time, ts=st.ts, dtype=args.output_dtype)
+        ts = dyn.get('ts')[0] if st.ts is not None else None
+        write_restart(restart, st, dyn.state(), res.time, ts=ts, dtype=args.output_dtype)
     summary = {'steps': res.steps, 'time': res.time, 'stable': res.stable, 'remap_steps': res.remap_steps,
                'output_records': records, 'output': args.output, 'restart': restart}
     print(json.dumps(summary))

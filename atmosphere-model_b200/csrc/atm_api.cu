@@ -12,6 +12,7 @@
 
 #include "atmdyn.h"
 #include "atm_ops.h"
+#include "atm_physics.h"
 
 using atm::Geom;
 using atm::H;
@@ -45,8 +46,9 @@ __global__ void k_interior(Geom g, const A* __restrict__ src, B* __restrict__ ds
 // winds are the cell-centre averages .5 (ud(j) + ud(j+1)), .5 (vd(i) + vd(i+1)).
 template <typename T>
 __global__ void k_accumulate(Geom g, const T* __restrict__ dp, const T* __restrict__ pt, const T* __restrict__ ud,
-                             const T* __restrict__ vd, const double* __restrict__ nf, double dt, double* acc_dp,
-                             double* acc_pt, double* acc_u, double* acc_v, double* acc_nf) {
+                             const T* __restrict__ vd, const double* __restrict__ nf, const double* __restrict__ ts,
+                             double dt, double* acc_dp, double* acc_pt, double* acc_u, double* acc_v, double* acc_nf,
+                             double* acc_ts) {
   const long long n = (long long)g.nx * g.ny;
   const long long total = n * (g.L + 1);
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
@@ -61,6 +63,7 @@ __global__ void k_accumulate(Geom g, const T* __restrict__ dp, const T* __restri
       acc_v[q] = acc_v[q] + dt * .5 * ((double)vd[o] + (double)vd[o + 1]);
     }
     acc_nf[q] = acc_nf[q] + dt * (nf ? nf[o] : 0.);
+    if (k == 0) acc_ts[q] = acc_ts[q] + dt * ts[o];
   }
 }
 
@@ -117,8 +120,14 @@ struct atm_ctx {
   int slot_in = 0;
   // output accumulation (src/mod_output.f90:94-142): interior (nx, ny, K)
   // sums of dt * dp, pt, u, v (nlay levels) and net_flux (nlay+1 levels)
-  double* acc[5] = {nullptr};
+  double* acc[6] = {nullptr};
   double acc_time = 0.;
+  // column physics (src/mod_physics.f90): surface temperature ts (one
+  // level, allocated with the context) and the tendencies of pt, u, v on
+  // the A grid and of ts (allocated by the first atm_physics_tendencies)
+  double* ts = nullptr;
+  double *ph_pt = nullptr, *ph_u = nullptr, *ph_v = nullptr, *ph_ts = nullptr;
+  bool phys_ready = false;
   std::string err;
 };
 
@@ -146,6 +155,7 @@ int field_levels(const atm_ctx* c, int f) {
     case ATM_DP: case ATM_PT: case ATM_UD: case ATM_VD: return c->L;
     case ATM_DPC: case ATM_PTC: case ATM_UC: case ATM_VC: return c->L;
     case ATM_GZ: case ATM_PLEV: case ATM_PKAP: case ATM_NET_FLUX: return c->L + 1;
+    case ATM_TS: return 1;
     default: return -1;
   }
 }
@@ -177,6 +187,8 @@ void free_all(atm_ctx* c) {
   double* pl[] = {c->lam_pk, c->lam_gz, c->lam_pkb, c->lam_gzb, c->lam_ur, c->lam_vr};
   for (double* p : pl) cudaFree(p);
   for (double* p : c->acc) cudaFree(p);
+  double* ph[] = {c->ts, c->ph_pt, c->ph_u, c->ph_v, c->ph_ts};
+  for (double* p : ph) cudaFree(p);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_mass) cudaFreeHost(c->h_mass);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
@@ -199,10 +211,12 @@ const char* const STAGE_NAMES[] = {"c_mass",  "c_column", "c_mom",        "c_hal
                                    "d_mass",  "d_column", "d_corners",    "d_mom",       "remap_ring",
                                    "remap_winds", "remap_energy", "d_halo", "heating", "check",
                                    "adj_forward", "adj_remap", "adj_d_mom", "adj_d_column", "adj_d_mass",
-                                   "adj_c_column", "adj_c_mom", "adj_c_mass", "adj_halo"};
-constexpr int NSTAGE = 24;
+                                   "adj_c_column", "adj_c_mom", "adj_c_mass", "adj_halo",
+                                   "phys_tend", "phys_apply", "phys_halo"};
+constexpr int NSTAGE = 27;
 enum { S_CMASS, S_CCOL, S_CMOM, S_CHALO, S_DRING, S_DMASS, S_DCOL, S_DCORN, S_DMOM, S_RRING, S_RWIND, S_RENER,
-       S_DHALO, S_HEAT, S_CHECK, S_AFWD, S_ARMP, S_ADMOM, S_ADCOL, S_ADMASS, S_ACCOL, S_ACMOM, S_ACMASS, S_AHALO };
+       S_DHALO, S_HEAT, S_CHECK, S_AFWD, S_ARMP, S_ADMOM, S_ADCOL, S_ADMASS, S_ACCOL, S_ACMOM, S_ACMASS, S_AHALO,
+       S_PHYS_TEND, S_PHYS_APPLY, S_PHYS_HALO };
 
 // Brackets one stage (one kernel launch unless noted) with CUDA events on
 // the context's stream when profiling is on, and counts the launch.
@@ -305,6 +319,7 @@ int atm_create(atm_ctx** out, int nx, int ny, int nlay, double dx, double dy, co
   alloc((void**)&ctx->pkapb, lev);
   alloc((void**)&ctx->gzb, lev);
   alloc((void**)&ctx->stage, lev);
+  alloc((void**)&ctx->ts, level_elems(ctx) * 8);
   alloc((void**)&ctx->d_ak, (nlay + 1) * 8);
   alloc((void**)&ctx->d_bk, (nlay + 1) * 8);
   alloc((void**)&ctx->partial, MASS_BLOCKS * 8);
@@ -365,6 +380,8 @@ int atm_upload(atm_ctx* ctx, int field, const double* host) {
     CK(h2d_pitched(ctx, ctx->gz, host, 1));  // level 1: surface geopotential
   } else if (field == ATM_NET_FLUX) {
     return atm_set_net_flux(ctx, host);
+  } else if (field == ATM_TS) {
+    CK(h2d_pitched(ctx, ctx->ts, host, 1));
   } else {
     return fail(ctx, ATM_ERR_ARG, "field cannot be uploaded");
   }
@@ -425,6 +442,8 @@ int atm_download(atm_ctx* ctx, int field, double* host) {
       CK(ops.to_double(src, ctx->stage, ctx->geo.S * K, ctx->stream));
       CK(d2h_pitched(ctx, host, ctx->stage, K));
     }
+  } else if (field == ATM_TS) {
+    CK(d2h_pitched(ctx, host, ctx->ts, 1));
   } else if (field == ATM_NET_FLUX) {
     if (ctx->nf) {
       CK(d2h_pitched(ctx, host, ctx->nf, K));
@@ -476,6 +495,9 @@ int atm_init(atm_ctx* ctx) {
   CK(ctx->ops->ring(g, ctx->st[ctx->cur], nullptr, 4, ctx->L, false, ctx->stream));
   void* gz1[1] = {ctx->gz};
   CK(atm::ops_fp64.ring(g, gz1, nullptr, 1, 1, false, ctx->stream));
+  // and halo_exchange(ts) (src/mod_input.f90:251)
+  void* ts1[1] = {ctx->ts};
+  CK(atm::ops_fp64.ring(g, ts1, nullptr, 1, 1, false, ctx->stream));
   // model-top constants: pkap(nlay+1) and pkapb(nlay+1) = Ak(1)**kappa
   // (src/mod_input.f90:229-231, src/mod_sw_dyn.f90:991)
   k_fill<<<148, 256, 0, ctx->stream>>>(ctx->pkap + g.S * ctx->L, g.S, ctx->cst.pk_top);
@@ -1156,12 +1178,17 @@ int atm_state_load(atm_ctx* ctx, const void* dev) {
 // ------------------------------------------------------------ output ----
 extern "C" {
 
+namespace {
+// levels of an output accumulator: nlay (dp, pt, u, v), nlay + 1 (net
+// flux), 1 (ts)
+int out_levels(const atm_ctx* c, int which) { return which < ATM_OUT_NFLX ? c->L : which == ATM_OUT_NFLX ? c->L + 1 : 1; }
+}  // namespace
+
 int atm_output_enable(atm_ctx* ctx) {
   int r = require_init(ctx);
   if (r) return r;
-  const size_t lay = (size_t)ctx->nx * ctx->ny * ctx->L * 8, lev = (size_t)ctx->nx * ctx->ny * (ctx->L + 1) * 8;
-  for (int f = 0; f < 5; ++f) {
-    if (!ctx->acc[f]) CK(cudaMalloc((void**)&ctx->acc[f], f < 4 ? lay : lev));
+  for (int f = 0; f <= ATM_OUT_TS; ++f) {
+    if (!ctx->acc[f]) CK(cudaMalloc((void**)&ctx->acc[f], (size_t)ctx->nx * ctx->ny * out_levels(ctx, f) * 8));
   }
   return atm_output_reset(ctx);
 }
@@ -1169,8 +1196,8 @@ int atm_output_enable(atm_ctx* ctx) {
 int atm_output_reset(atm_ctx* ctx) {
   if (!ctx) return ATM_ERR_ARG;
   if (!ctx->acc[0]) return fail(ctx, ATM_ERR_STATE, "atm_output_enable has not been called");
-  const size_t lay = (size_t)ctx->nx * ctx->ny * ctx->L * 8, lev = (size_t)ctx->nx * ctx->ny * (ctx->L + 1) * 8;
-  for (int f = 0; f < 5; ++f) CK(cudaMemsetAsync(ctx->acc[f], 0, f < 4 ? lay : lev, ctx->stream));
+  for (int f = 0; f <= ATM_OUT_TS; ++f)
+    CK(cudaMemsetAsync(ctx->acc[f], 0, (size_t)ctx->nx * ctx->ny * out_levels(ctx, f) * 8, ctx->stream));
   ctx->acc_time = 0.;
   return ATM_OK;
 }
@@ -1183,13 +1210,14 @@ int atm_accumulate_output(atm_ctx* ctx, double dt) {
   const double* nf = ctx->heating ? ctx->nf : nullptr;
   if (ctx->ops->elem == 8)
     k_accumulate<double><<<1184, 256, 0, ctx->stream>>>(ctx->geo, (const double*)s[F_DP], (const double*)s[F_PT],
-                                                         (const double*)s[F_UD], (const double*)s[F_VD], nf, dt,
-                                                         ctx->acc[0], ctx->acc[1], ctx->acc[2], ctx->acc[3],
-                                                         ctx->acc[4]);
+                                                         (const double*)s[F_UD], (const double*)s[F_VD], nf, ctx->ts,
+                                                         dt, ctx->acc[0], ctx->acc[1], ctx->acc[2], ctx->acc[3],
+                                                         ctx->acc[4], ctx->acc[5]);
   else
     k_accumulate<float><<<1184, 256, 0, ctx->stream>>>(ctx->geo, (const float*)s[F_DP], (const float*)s[F_PT],
-                                                        (const float*)s[F_UD], (const float*)s[F_VD], nf, dt,
-                                                        ctx->acc[0], ctx->acc[1], ctx->acc[2], ctx->acc[3], ctx->acc[4]);
+                                                        (const float*)s[F_UD], (const float*)s[F_VD], nf, ctx->ts,
+                                                        dt, ctx->acc[0], ctx->acc[1], ctx->acc[2], ctx->acc[3],
+                                                        ctx->acc[4], ctx->acc[5]);
   CK(cudaGetLastError());
   ctx->launches += 1;
   ctx->acc_time = ctx->acc_time + dt;
@@ -1197,9 +1225,9 @@ int atm_accumulate_output(atm_ctx* ctx, double dt) {
 }
 
 int atm_output_read(atm_ctx* ctx, int which, double* host) {
-  if (!ctx || !host || which < 0 || which > 4) return ATM_ERR_ARG;
+  if (!ctx || !host || which < 0 || which > ATM_OUT_TS) return ATM_ERR_ARG;
   if (!ctx->acc[0]) return fail(ctx, ATM_ERR_STATE, "atm_output_enable has not been called");
-  const size_t n = (size_t)ctx->nx * ctx->ny * (which < 4 ? ctx->L : ctx->L + 1);
+  const size_t n = (size_t)ctx->nx * ctx->ny * out_levels(ctx, which);
   CK(cudaMemcpyAsync(host, ctx->acc[which], n * 8, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   // write_output (src/mod_output.f90:152): output_field / accumulation_time
@@ -1211,6 +1239,68 @@ int atm_output_read(atm_ctx* ctx, int which, double* host) {
 int atm_output_time(atm_ctx* ctx, double* t) {
   if (!ctx || !t) return ATM_ERR_ARG;
   *t = ctx->acc_time;
+  return ATM_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ physics ----
+extern "C" {
+
+int atm_physics_tendencies(atm_ctx* ctx) {
+  int r = require_init(ctx);
+  if (r) return r;
+  if (ctx->ops->elem != 8) return fail(ctx, ATM_ERR_UNSUPPORTED, "the physics needs an FP64 prognostic state");
+  if (!ctx->ph_pt) {
+    const size_t lay = level_elems(ctx) * ctx->L * 8;
+    bool ok = cudaMalloc((void**)&ctx->ph_pt, lay) == cudaSuccess && cudaMalloc((void**)&ctx->ph_u, lay) == cudaSuccess &&
+              cudaMalloc((void**)&ctx->ph_v, lay) == cudaSuccess &&
+              cudaMalloc((void**)&ctx->ph_ts, level_elems(ctx) * 8) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      double** ph[] = {&ctx->ph_pt, &ctx->ph_u, &ctx->ph_v, &ctx->ph_ts};
+      for (double** p : ph) {
+        cudaFree(*p);
+        *p = nullptr;
+      }
+      return fail(ctx, ATM_ERR_NOMEM, "physics tendencies");
+    }
+    CK(cudaMemsetAsync(ctx->ph_ts, 0, level_elems(ctx) * 8, ctx->stream));
+  }
+  void* const* s = ctx->st[ctx->cur];
+  atm::PhysicsArgs a{ctx->cst.ptop, ctx->cst.pk_top, (const double*)s[F_DP], (const double*)s[F_PT],
+                     (const double*)s[F_UD], (const double*)s[F_VD], ctx->gz, ctx->heating ? ctx->nf : nullptr,
+                     ctx->ph_pt, ctx->ph_u, ctx->ph_v, ctx->ph_ts};
+  {
+    Stage t(ctx, S_PHYS_TEND);
+    CK(atm::physics_tend(ctx->geo, a, ctx->stream));
+  }
+  ctx->phys_ready = true;
+  return ATM_OK;
+}
+
+int atm_apply_physics(atm_ctx* ctx, double dt) {
+  int r = require_init(ctx);
+  if (r) return r;
+  if (!ctx->phys_ready) return fail(ctx, ATM_ERR_STATE, "atm_physics_tendencies has not been called");
+  void* const* s = ctx->st[ctx->cur];
+  atm::PhysicsArgs a{ctx->cst.ptop, ctx->cst.pk_top, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                     ctx->ph_pt, ctx->ph_u, ctx->ph_v, ctx->ph_ts};
+  {
+    Stage t(ctx, S_PHYS_APPLY);
+    CK(atm::physics_apply(ctx->geo, dt, a, (double*)s[F_DP], (double*)s[F_PT], (double*)s[F_UD], (double*)s[F_VD],
+                          ctx->ts, ctx->stream));
+  }
+  ctx->flag_valid = false;
+  return ATM_OK;
+}
+
+int atm_physics_halo(atm_ctx* ctx) {
+  int r = require_init(ctx);
+  if (r) return r;
+  void* ts1[1] = {ctx->ts};
+  Stage t(ctx, S_PHYS_HALO);
+  CK(atm::ops_fp64.ring(ctx->geo, ts1, nullptr, 1, 1, false, ctx->stream));
   return ATM_OK;
 }
 

@@ -49,7 +49,9 @@ enum {
      module variables of the reference (src/mod_sw_dyn.f90:23-27), K = nlay;
      valid on the ranges cgrid_dynamics_step writes and, after
      atm_cgrid_halo, everywhere */
-  ATM_DPC = 8, ATM_PTC = 9, ATM_UC = 10, ATM_VC = 11
+  ATM_DPC = 8, ATM_PTC = 9, ATM_UC = 10, ATM_VC = 11,
+  ATM_TS = 12        /* surface temperature ts, K = 1 (mod_fields.f90:51); upload,
+                        download; the physics updates it (src/mod_physics.f90:172) */
 };
 
 /* forms */
@@ -85,7 +87,7 @@ int atm_create(atm_ctx** out, int nx, int ny, int nlay, double dx, double dy, co
                int precision, int flags);
 
 /* copy a field from / to a host (is:ie, js:je, 1:K) FP64 array.  Upload
-   accepts ATM_DP, ATM_PT, ATM_UD, ATM_VD and ATM_GZ (level 1 only).
+   accepts ATM_DP, ATM_PT, ATM_UD, ATM_VD, ATM_GZ (level 1 only) and ATM_TS.
    Download of ATM_PLEV / ATM_PKAP / ATM_GZ returns the column diagnostics
    recomputed from the current dp and pt (plev = Ak(1) + suffix sum of dp,
    pkap = plev**kappa, hydrostatic gz), on the whole array. */
@@ -93,8 +95,8 @@ int atm_upload(atm_ctx* ctx, int field, const double* host);
 int atm_download(atm_ctx* ctx, int field, double* host);
 
 /* initial_halo_exchange (src/mod_input.f90:247-252) of dp, pt, gz, ud, vd
-   and the set-up that needs gz (src/mod_sw_dyn.f90:990-996).  Call after
-   the uploads and before the first step. */
+   and ts, and the set-up that needs gz (src/mod_sw_dyn.f90:990-996).  Call
+   after the uploads and before the first step. */
 int atm_init(atm_ctx* ctx);
 
 /* cgrid_dynamics_step(dt) (src/mod_sw_dyn.f90:80-416); dt_half is the
@@ -254,16 +256,32 @@ int atm_state_bytes(atm_ctx* ctx, long long* bytes);
 int atm_state_save(atm_ctx* ctx, void* dev);
 int atm_state_load(atm_ctx* ctx, const void* dev);
 
+/* ---- column physics (src/mod_physics.f90), FP64 in both forms ----
+   atm_physics_tendencies: calculate_physics_tendencies (:27-79): A-grid
+   winds, plev / pkap / gz / playkap of the current state, the dry
+   convective adjustment (:81-176) on [isd-2, ied+2]^2 and the surface
+   heating from level 1 of the net flux set by atm_set_net_flux (zero when
+   none is set, :178-185).  The tendencies stay on the device until the next
+   call.  Called where run_model calls it: at the start of a step when the
+   physics is due (src/mod_model.f90:138-143).
+   atm_apply_physics(dt): apply_physics_tendencies (:187-211) to the
+   interior of dp, pt, ts, ud, vd, after the D-grid step of every step
+   (src/mod_model.f90:153-155); ATM_ERR_STATE before the first tendencies.
+   atm_physics_halo: physics_halo_exchange (:213-217), the periodic halo
+   of ts, after atm_dgrid_halo (src/mod_model.f90:165-166). */
+int atm_physics_tendencies(atm_ctx* ctx);
+int atm_apply_physics(atm_ctx* ctx, double dt);
+int atm_physics_halo(atm_ctx* ctx);
+
 /* ---- output accumulation on the device (accumulate_output / write_output,
    src/mod_output.f90:94-176) ----
-   atm_accumulate_output(ctx, dt) adds dt * (dp, pt, u, v, net_flux) of the
-   current state to device sums, with u, v the cell-centre averages of the
-   D-grid winds, exactly as the reference (whose compensated sum keeps no
-   compensation: plain FP64 adds); atm_output_read returns one mean (sum /
-   accumulated time) as a host (nlay or nlay+1, ny, nx) array, field
-   ATM_OUT_DP..ATM_OUT_NFLX; atm_output_reset starts a new interval.  The
-   surface temperature ts is a physics field and stays with the caller. */
-enum { ATM_OUT_DP = 0, ATM_OUT_PT = 1, ATM_OUT_U = 2, ATM_OUT_V = 3, ATM_OUT_NFLX = 4 };
+   atm_accumulate_output(ctx, dt) adds dt * (dp, pt, u, v, net_flux, ts) of
+   the current state to device sums, with u, v the cell-centre averages of
+   the D-grid winds, exactly as the reference (whose compensated sum keeps
+   no compensation: plain FP64 adds); atm_output_read returns one mean (sum /
+   accumulated time) as a host (nlay, nlay+1 or 1, ny, nx) array, field
+   ATM_OUT_DP..ATM_OUT_TS; atm_output_reset starts a new interval. */
+enum { ATM_OUT_DP = 0, ATM_OUT_PT = 1, ATM_OUT_U = 2, ATM_OUT_V = 3, ATM_OUT_NFLX = 4, ATM_OUT_TS = 5 };
 int atm_output_enable(atm_ctx* ctx);
 int atm_output_reset(atm_ctx* ctx);
 int atm_accumulate_output(atm_ctx* ctx, double dt);

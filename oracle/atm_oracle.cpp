@@ -286,6 +286,10 @@ struct StateT {
   // mod_sw_dyn module arrays
   A3<R> dpc, ptc, uc, vc, heating_rate, pkapb, gzb;
   Scratch<R> sc;
+  // mod_physics module arrays (tendencies on isd-2:ied+2, A-grid winds on
+  // is:ie) and the surface temperature ts (mod_fields.f90:51), 2-D arrays
+  // held as one-level 3-D arrays
+  A3<R> ts, ts_tend, dp_tend, pt_tend, u_tend, v_tend, ua, va;
   // mod_remap module arrays
   double top_pressure;
   A3<R> u_remap, v_remap, pt_remap, target_plev, target_pkap, target_playkap;
@@ -1095,6 +1099,7 @@ A3<R>* field_ptr(StateT<R>* s, int f) {
     case ORC_PTC: return &s->ptc;
     case ORC_UC: return &s->uc;
     case ORC_VC: return &s->vc;
+    case ORC_TS: return &s->ts;
     default: return nullptr;
   }
 }
@@ -1122,6 +1127,13 @@ bool setup_state(StateT<R>* s, int nx, int ny, int nlay, double dx, double dy, c
   for (A3<R>* a : {&s->dpc, &s->ptc, &s->uc, &s->vc, &s->heating_rate}) a->alloc(is, ie, js, je, 1, L);
   for (A3<R>* a : {&s->pkapb, &s->gzb}) a->alloc(is, ie, js, je, 1, L + 1);
   s->sc.alloc(is, ie, js, je);
+  // allocate_physics_arrays, mod_physics.f90:193-212; ts, mod_fields.f90:51
+  s->ts.alloc(is, ie, js, je, 1, 1);
+  s->ts_tend.alloc(s->isd - 2, s->ied + 2, s->jsd - 2, s->jed + 2, 1, 1);
+  for (A3<R>* a : {&s->dp_tend, &s->pt_tend, &s->u_tend, &s->v_tend})
+    a->alloc(s->isd - 2, s->ied + 2, s->jsd - 2, s->jed + 2, 1, L);
+  s->ua.alloc(is, ie, js, je, 1, L);
+  s->va.alloc(is, ie, js, je, 1, L);
   s->u_remap.alloc(s->isd - 1, s->ied + 1, s->jsd - 1, s->jed + 1, 1, L);
   s->v_remap.alloc(s->isd - 1, s->ied + 1, s->jsd - 1, s->jed + 1, 1, L);
   s->pt_remap.alloc(s->isd, s->ied, s->jsd, s->jed, 1, L);
@@ -1224,6 +1236,128 @@ void dgrid_halo(StateT<R>* s) {
   halo_exchange(s, f4, 4, s->nlay);
 }
 
+// ------------------------------------------------------------ physics ----
+// calculate_physics_tendencies, src/mod_physics.f90:27-79
+template <class R>
+void dry_convective_adjustment(StateT<R>* s);
+template <class R>
+void calculate_physics_tendencies(StateT<R>* s) {
+  const int L = s->nlay;
+  for (A3<R>* a : {&s->dp_tend, &s->pt_tend, &s->u_tend, &s->v_tend}) std::fill(a->v.begin(), a->v.end(), R(0.));
+  // A-grid winds (:39-47)
+  for (int j = s->js + 1; j <= s->je - 1; ++j)
+    for (int i = s->is + 1; i <= s->ie - 1; ++i)
+      for (int k = 1; k <= L; ++k) {
+        s->ua(i, j, k) = (.25 * (s->ud(i, j, k) + s->ud(i, j + 1, k)) +
+                          .125 * (s->ud(i - 1, j, k) + s->ud(i - 1, j + 1, k) + s->ud(i + 1, j, k) + s->ud(i + 1, j + 1, k)));
+        s->va(i, j, k) = (.25 * (s->vd(i, j, k) + s->vd(i + 1, j, k)) +
+                          .125 * (s->vd(i, j - 1, k) + s->vd(i + 1, j - 1, k) + s->vd(i, j + 1, k) + s->vd(i + 1, j + 1, k)));
+      }
+  // levels and pkap (:49-57)
+  for (int k = L; k >= 1; --k)
+    for (int j = s->js + 1; j <= s->je - 1; ++j)
+      for (int i = s->is + 1; i <= s->ie - 1; ++i) {
+        s->plev(i, j, k) = s->plev(i, j, k + 1) + s->dp(i, j, k);
+        s->pkap(i, j, k) = orc_pow_impl(s->plev(i, j, k), KAPPA);
+      }
+  // geopotential and layer-mean pkap (:59-71)
+  for (int k = 1; k <= L; ++k)
+    for (int j = s->js + 1; j <= s->je - 1; ++j)
+      for (int i = s->is + 1; i <= s->ie - 1; ++i) {
+        s->gz(i, j, k + 1) = s->gz(i, j, k) + CP_DRY * s->pt(i, j, k) * (s->pkap(i, j, k) - s->pkap(i, j, k + 1));
+        s->playkap(i, j, k) = (s->pkap(i, j, k + 1) - s->pkap(i, j, k)) /
+                              orc_log_impl(s->plev(i, j, k + 1) / s->plev(i, j, k)) / KAPPA;
+      }
+  dry_convective_adjustment(s);
+  // surface_heating (:178-185): heat capacity of 5 m of water, 41680*5 J/m^2/K
+  for (int j = s->jsd; j <= s->jed; ++j)
+    for (int i = s->isd; i <= s->ied; ++i) s->ts_tend(i, j, 1) = s->net_flux(i, j, 1) / 208400.;
+}
+
+// dry_convective_adjustment, src/mod_physics.f90:81-176
+template <class R>
+void dry_convective_adjustment(StateT<R>* s) {
+  const int L = s->nlay;
+  const double min_v2 = (double)1e-4f;  // a default-real literal (:86)
+  const double critical_richardson_number = .25;
+  const double mixing_timescale = 600.;
+  std::vector<R> energy(L + 1), u_adj(L + 1), v_adj(L + 1), gz_adj(L + 2), pt_adj(L + 1);
+  for (int j = s->jsd - 2; j <= s->jed + 2; ++j)
+    for (int i = s->isd - 2; i <= s->ied + 2; ++i) {
+      for (int k = 1; k <= L; ++k) {
+        energy[k] = CV_DRY * s->pt(i, j, k) * s->playkap(i, j, k) +
+                    .5 * (s->gz(i, j, k + 1) + s->gz(i, j, k) + s->ua(i, j, k) * s->ua(i, j, k) +
+                          s->va(i, j, k) * s->va(i, j, k));
+        u_adj[k] = s->ua(i, j, k);
+        v_adj[k] = s->va(i, j, k);
+      }
+      for (int k = 1; k <= L - 1; ++k) {
+        const R du = s->ua(i, j, k + 1) - s->ua(i, j, k), dv = s->va(i, j, k + 1) - s->va(i, j, k);
+        const R ri = (s->pt(i, j, k + 1) - s->pt(i, j, k)) *
+                     (s->dp(i, j, k) * (s->gz(i, j, k + 1) - s->gz(i, j, k)) +
+                      s->dp(i, j, k + 1) * (s->gz(i, j, k + 2) - s->gz(i, j, k + 1))) /
+                     ((s->dp(i, j, k) * s->pt(i, j, k) + s->dp(i, j, k + 1) * s->pt(i, j, k + 1)) *
+                      (du * du + dv * dv + min_v2));
+        if (ri < critical_richardson_number) {
+          const R q = ri / critical_richardson_number;
+          const R t = 1. - (q > 0. ? q : R(0.));  // max(0.0, q)
+          const R mixing_fraction = t * t * s->dp(i, j, k) * s->dp(i, j, k + 1) / (s->dp(i, j, k) + s->dp(i, j, k + 1));
+          R exchange = mixing_fraction * (u_adj[k] - u_adj[k + 1]);
+          u_adj[k] = u_adj[k] - exchange / s->dp(i, j, k);
+          u_adj[k + 1] = u_adj[k + 1] + exchange / s->dp(i, j, k + 1);
+          exchange = mixing_fraction * (v_adj[k] - v_adj[k + 1]);
+          v_adj[k] = v_adj[k] - exchange / s->dp(i, j, k);
+          v_adj[k + 1] = v_adj[k + 1] + exchange / s->dp(i, j, k + 1);
+          exchange = mixing_fraction * (energy[k] - energy[k + 1]);
+          energy[k] = energy[k] - exchange / s->dp(i, j, k);
+          energy[k + 1] = energy[k + 1] + exchange / s->dp(i, j, k + 1);
+        }
+      }
+      for (int k = 1; k <= L; ++k) {
+        s->u_tend(i, j, k) = s->u_tend(i, j, k) + (u_adj[k] - s->ua(i, j, k)) / mixing_timescale;
+        s->v_tend(i, j, k) = s->v_tend(i, j, k) + (v_adj[k] - s->va(i, j, k)) / mixing_timescale;
+      }
+      gz_adj[1] = s->gz(i, j, 1);
+      for (int k = 1; k <= L; ++k) {
+        pt_adj[k] = (energy[k] - gz_adj[k] - .5 * (u_adj[k] * u_adj[k] + v_adj[k] * v_adj[k])) /
+                    (CV_DRY * s->playkap(i, j, k) + .5 * CP_DRY * (s->pkap(i, j, k) - s->pkap(i, j, k + 1)));
+        gz_adj[k + 1] = gz_adj[k] + CP_DRY * pt_adj[k] * (s->pkap(i, j, k) - s->pkap(i, j, k + 1));
+      }
+      for (int k = 1; k <= L; ++k)
+        s->pt_tend(i, j, k) = s->pt_tend(i, j, k) + (pt_adj[k] - s->pt(i, j, k)) / mixing_timescale;
+    }
+}
+
+// apply_physics_tendencies, src/mod_physics.f90:187-211
+template <class R>
+void apply_physics_tendencies(StateT<R>* s, double dt) {
+  const int L = s->nlay;
+  for (int k = 1; k <= L; ++k)
+    for (int j = s->jsd; j <= s->jed; ++j)
+      for (int i = s->isd; i <= s->ied; ++i) s->dp(i, j, k) = s->dp(i, j, k) + dt * s->dp_tend(i, j, k);
+  for (int k = 1; k <= L; ++k)
+    for (int j = s->jsd; j <= s->jed; ++j)
+      for (int i = s->isd; i <= s->ied; ++i) s->pt(i, j, k) = s->pt(i, j, k) + dt * s->pt_tend(i, j, k);
+  for (int j = s->jsd; j <= s->jed; ++j)
+    for (int i = s->isd; i <= s->ied; ++i) s->ts(i, j, 1) = s->ts(i, j, 1) + dt * s->ts_tend(i, j, 1);
+  for (int j = s->jsd; j <= s->jed; ++j)
+    for (int i = s->isd; i <= s->ied; ++i)
+      for (int k = 1; k <= L; ++k) {
+        s->ud(i, j, k) = s->ud(i, j, k) + dt * (C7_12 * (s->u_tend(i, j, k) + s->u_tend(i, j - 1, k)) -
+                                                C1_12 * (s->u_tend(i, j + 1, k) + s->u_tend(i, j - 2, k)));
+        s->vd(i, j, k) = s->vd(i, j, k) + dt * (C7_12 * (s->v_tend(i, j, k) + s->v_tend(i - 1, j, k)) -
+                                                C1_12 * (s->v_tend(i + 1, j, k) + s->v_tend(i - 2, j, k)));
+      }
+}
+
+// physics_halo_exchange, src/mod_physics.f90:213-217 (the 2-D exchange of
+// mod_sync.f90:42-52 is the 3-D one on a single level)
+template <class R>
+void physics_halo(StateT<R>* s) {
+  A3<R>* f1[] = {&s->ts};
+  halo_exchange(s, f1, 1, 1);
+}
+
 }  // namespace
 
 extern "C" {
@@ -1254,6 +1388,9 @@ void orc_cgrid_halo(orc_state* s) { cgrid_halo<double>(s); }
 void orc_dgrid_step(orc_state* s, double dt) { dgrid_dynamics_step<double>(s, dt); }
 void orc_remap(orc_state* s) { perform_vertical_remapping<double>(s); }
 void orc_dgrid_halo(orc_state* s) { dgrid_halo<double>(s); }
+void orc_physics_tendencies(orc_state* s) { calculate_physics_tendencies<double>(s); }
+void orc_apply_physics(orc_state* s, double dt) { apply_physics_tendencies<double>(s, dt); }
+void orc_physics_halo(orc_state* s) { physics_halo<double>(s); }
 
 // mod_fields.f90:69-106
 int orc_check_stability(orc_state* s) {

@@ -3,9 +3,10 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This is a line-faithful FP64 restatement of the
  * reference's Fortran (src/mod_sw_dyn.f90, src/mod_remap.f90, the single-image
- * path of src/mod_sync.f90 / src/mod_tiles.f90, src/mod_fields.f90:69-106 and
- * the constants of src/mod_constants.f90).  It is the checker for the CUDA
- * library and the timed CPU baseline; no product code path may link or call it.
+ * path of src/mod_sync.f90 / src/mod_tiles.f90, src/mod_fields.f90:69-106,
+ * src/mod_physics.f90 and the constants of src/mod_constants.f90).  It is the
+ * checker for the CUDA library and the timed CPU baseline; no product code
+ * path may link or call it.
  *
  * PARITY UNPINNED: the reference is Fortran 2008 with coarrays and needs
  * gfortran + OpenCoarrays + netCDF-Fortran, none of which exist on this
@@ -34,7 +35,9 @@ enum {
   ORC_DP = 0, ORC_PT = 1, ORC_UD = 2, ORC_VD = 3,
   ORC_GZ = 4, ORC_PLEV = 5, ORC_PKAP = 6, ORC_NET_FLUX = 7,
   /* the C-grid half step's module arrays (private in mod_sw_dyn.f90:23-27) */
-  ORC_DPC = 8, ORC_PTC = 9, ORC_UC = 10, ORC_VC = 11
+  ORC_DPC = 8, ORC_PTC = 9, ORC_UC = 10, ORC_VC = 11,
+  /* surface temperature (mod_fields.f90:51), one level */
+  ORC_TS = 12
 };
 
 orc_state* orc_create(int nx, int ny, int nlay, double dx, double dy,
@@ -57,6 +60,12 @@ void orc_cgrid_halo(orc_state* s);
 void orc_dgrid_step(orc_state* s, double dt);
 void orc_remap(orc_state* s);
 void orc_dgrid_halo(orc_state* s);
+/* src/mod_physics.f90: calculate_physics_tendencies (:27-79, with
+   dry_convective_adjustment and surface_heating), apply_physics_tendencies
+   (:187-211), physics_halo_exchange (:213-217) */
+void orc_physics_tendencies(orc_state* s);
+void orc_apply_physics(orc_state* s, double dt);
+void orc_physics_halo(orc_state* s);
 int  orc_check_stability(orc_state* s);          /* 1 = all finite */
 double orc_mass(orc_state* s);                   /* sum of interior dp */
 

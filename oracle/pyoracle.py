@@ -12,7 +12,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 HALO = 7
-DP, PT, UD, VD, GZ, PLEV, PKAP, NET_FLUX, DPC, PTC, UC, VC = range(12)
+DP, PT, UD, VD, GZ, PLEV, PKAP, NET_FLUX, DPC, PTC, UC, VC, TS = range(13)
 
 _libs: dict = {}
 _P = ctypes.POINTER(ctypes.c_double)
@@ -44,6 +44,9 @@ def load(variant: str = 'portable'):
         getattr(lib, f).argtypes = vp
     lib.orc_cgrid_step.argtypes = vp + [ctypes.c_double]
     lib.orc_dgrid_step.argtypes = vp + [ctypes.c_double]
+    lib.orc_physics_tendencies.argtypes = vp
+    lib.orc_apply_physics.argtypes = vp + [ctypes.c_double]
+    lib.orc_physics_halo.argtypes = vp
     lib.orc_check_stability.argtypes = vp
     lib.orc_mass.argtypes = vp
     lib.orc_mass.restype = ctypes.c_double
@@ -80,7 +83,11 @@ class OracleModel:
         gz = np.zeros((st.nlay + 1, st.ny, st.nx))
         gz[0] = st.gzs
         self.set(GZ, gz)
+        if getattr(st, 'ts', None) is not None:
+            self.set(TS, np.asarray(st.ts)[None])
         self.lib.orc_init(self.s)
+        if getattr(st, 'ts', None) is not None:
+            self.physics_halo()  # initial_halo_exchange of ts (mod_input.f90:251)
         self._trace = None
 
     def __del__(self):
@@ -118,6 +125,18 @@ class OracleModel:
 
     def dgrid_halo(self):
         self.lib.orc_dgrid_halo(self.s)
+
+    def physics_tendencies(self):
+        self.lib.orc_physics_tendencies(self.s)
+
+    def apply_physics(self, dt):
+        self.lib.orc_apply_physics(self.s, dt)
+
+    def physics_halo(self):
+        self.lib.orc_physics_halo(self.s)
+
+    def set_net_flux(self, nf_halo):
+        self.set(NET_FLUX, nf_halo, halo=True)
 
     def check_stability(self):
         return bool(self.lib.orc_check_stability(self.s))

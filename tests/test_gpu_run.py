@@ -57,7 +57,7 @@ def test_run_from_reference_files(tmp_path):
 
     tc = model.TimeControl(dt_max=60.0, run_duration=600.0, dt_output=300.0, dt_radiation=10800.0,
                            dt_physics=300.0, dt_remap=240.0)
-    r = model.run_model(g, tc, on_step=on_step)
+    r = model.run_model(g, tc, on_step=on_step, physics=True)
     assert r.remap_steps == [4, 8]
     with netcdf_file(str(tmp_path / 'out' / 'restart.nc'), 'r', mmap=False) as nc:
         np.testing.assert_array_equal(nc.variables['dp'][:], g.get('dp'))

@@ -118,3 +118,79 @@ def test_portable_pow_log_accuracy():
 def test_literals_and_constants():
     assert ic.R_DRY == float(np.float32(287.052874))
     assert ic.KAPPA == ic.R_DRY / 1005.0
+
+
+# ------------------------------------------------------------- physics ----
+def physics_state(n=12, L=8, seed=3, unstable=True):
+    """Horizontally uniform layers (so the D-grid interpolation of a wind
+    tendency is the tendency itself) with sheared winds, and, when
+    unstable, potential temperature falling with height across layers 3-5."""
+    st = ic.bubble_case(n, n, L, 100e3, 100e3, amplitude=0.0, u0=0.0)
+    shear = np.linspace(-4.0, 6.0, L)[:, None, None]
+    st.u = np.broadcast_to(shear, st.u.shape).copy()
+    st.v = np.broadcast_to(-0.5 * shear, st.v.shape).copy()
+    if unstable:
+        st.pt = st.pt.copy()
+        st.pt[3] = st.pt[2] * (1 - 2e-3)
+        st.pt[4] = st.pt[2] * (1 - 4e-3)
+    st.ts = np.full((n, n), 288.0)
+    return st
+
+
+def test_physics_stable_column_leaves_winds_and_theta():
+    """Stable stratification with weak shear: no interface mixes, the wind
+    tendencies are exactly zero and theta only moves by the round-off of
+    its recovery from the energy (mod_physics.f90:146-166)."""
+    st = physics_state(unstable=False)
+    st.u = np.zeros_like(st.u)
+    st.v = np.zeros_like(st.v)
+    o = pyoracle.OracleModel(st)
+    before = o.state()
+    o.physics_tendencies()
+    o.apply_physics(600.0)
+    after = o.state()
+    np.testing.assert_array_equal(after['ud'], before['ud'])
+    np.testing.assert_array_equal(after['vd'], before['vd'])
+    np.testing.assert_array_equal(after['dp'], before['dp'])
+    assert np.max(np.abs(after['pt'] / before['pt'] - 1)) < 1e-12
+    np.testing.assert_array_equal(o.get(pyoracle.TS), 288.0)
+
+
+def test_physics_mixing_conserves_column_momentum():
+    """The exchange of mod_physics.f90:111-133 moves momentum between
+    layers k and k+1 in proportion to 1/dp, so sum(dp * du) over a column
+    vanishes."""
+    st = physics_state()
+    o = pyoracle.OracleModel(st)
+    before = o.state()
+    o.physics_tendencies()
+    o.apply_physics(600.0)  # one mixing timescale
+    after = o.state()
+    dp = before['dp']
+    du = after['ud'] - before['ud']
+    dv = after['vd'] - before['vd']
+    assert np.max(np.abs(du)) > 1e-3  # the unstable band mixed
+    scale = np.sum(dp * np.abs(du), axis=0)
+    assert np.max(np.abs(np.sum(dp * du, axis=0)) / scale) < 1e-12
+    assert np.max(np.abs(np.sum(dp * dv, axis=0)) / np.sum(dp * np.abs(dv), axis=0)) < 1e-12
+    assert np.max(np.abs(du[3:5])) > 1e-3  # the layers around the unstable interfaces
+
+
+def test_physics_surface_heating_and_ts_halo():
+    """ts_tend = net_flux(level 1) / 208400 (mod_physics.f90:178-185) on the
+    interior; physics_halo_exchange makes the halo the periodic image."""
+    st = physics_state(unstable=False)
+    o = pyoracle.OracleModel(st)
+    rng = np.random.default_rng(1)
+    nf = np.zeros((st.nlay + 1, st.ny + 2 * HALO, st.nx + 2 * HALO))
+    nf[0] = rng.normal(0, 100.0, nf[0].shape)
+    o.set_net_flux(nf)
+    o.physics_tendencies()
+    o.apply_physics(120.0)
+    ts = o.get(pyoracle.TS)[0]
+    np.testing.assert_array_equal(ts, 288.0 + 120.0 * (nf[0, HALO:-HALO, HALO:-HALO] / 208400.0))
+    o.physics_halo()
+    th = o.get(pyoracle.TS, halo=True)[0]
+    np.testing.assert_array_equal(th[:HALO, HALO:-HALO], th[st.ny:st.ny + HALO, HALO:-HALO])
+    np.testing.assert_array_equal(th[HALO:-HALO, :HALO], th[HALO:-HALO, st.nx:st.nx + HALO])
+    np.testing.assert_array_equal(th[:HALO, :HALO], th[st.ny:st.ny + HALO, st.nx:st.nx + HALO])
