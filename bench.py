@@ -64,6 +64,8 @@ WORDS = {
     'd_mom': (4, 2, 2),         # read ud, vd, uc, vc, pkapb, gzb; write ud, vd
     'remap_winds': (5, 0, 0),   # read dp, ud, vd; write u, v remapped
     'remap_energy': (10, 0, 0),  # read dp, pt, ud, vd, u, v remapped; write dp, pt, ud, vd
+    'phys_tend': (7, 0, 0),     # read dp, pt, ud, vd; write pt, u, v tendencies
+    'phys_apply': (11, 0, 0),   # read dp, pt, ud, vd and the three tendencies; write dp, pt, ud, vd
 }
 
 
@@ -282,6 +284,7 @@ def run_ours(args):
 
     adjoint = None if args.no_adjoint else adjoint_leg(args, torch, max_over_ranks, world)
     ensemble = None if (args.no_ensemble or world > 1) else ensemble_leg(args, torch)
+    physics = None if args.no_physics else physics_leg(args, torch, max_over_ranks, world, peak, peak_kind)
 
     # error of the mixed form against the FP64 form after the same steps
     err = {}
@@ -332,6 +335,8 @@ def run_ours(args):
         line['adjoint'] = adjoint
     if ensemble is not None:
         line['ensemble'] = ensemble
+    if physics is not None:
+        line['physics'] = physics
     if world == 1 and not args.no_cpu:
         threads = len(os.sched_getaffinity(0))
         v, t = cpu_sample_throughput(max(2, REMAP_EVERY // 2), 1, threads)
@@ -346,6 +351,75 @@ def run_ours(args):
 P0K = 1.0e5 ** (287.052874 / 1005.0)  # theta = pt * p0**kappa
 
 
+def physics_leg(args, torch, max_over_ranks, world, peak, peak_kind):
+    """The column physics (src/mod_physics.f90, FP64) on the headline
+    workload: calculate_physics_tendencies (k_physics_tend) and
+    apply_physics_tendencies (k_physics_apply), each launch timed with CUDA
+    events on the context's stream, and the FP64 restatement of the same two
+    routines on one host core on a 256 x 256 x 64 sample."""
+    from atmdyn import ic, Dycore
+    st = ic.jet_case(args.nx, args.nx, args.nlay, 25e3, 25e3, seed=0)
+    st.ts = np.full((st.ny, st.nx), 288.0)
+    cells = st.cells
+    dy = Dycore(st)
+    stream = torch.cuda.Stream()
+    dy.set_stream(stream.cuda_stream)
+    for _ in range(3):
+        dy.physics_tendencies()
+        dy.apply_physics(DT)
+        dy.physics_halo()
+    torch.cuda.synchronize()
+    reps = 8
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    dy.profile(True)
+    e0.record(stream)
+    for _ in range(reps):
+        dy.physics_tendencies()
+        dy.apply_physics(DT)
+        dy.physics_halo()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / reps
+    prof = dy.profile_read()
+    dy.profile(False)
+    dy.close()
+    del dy
+    torch.cuda.empty_cache()
+    kern = {}
+    for stage, (tms, cnt) in prof.items():
+        if cnt == 0:
+            continue
+        avg = tms / cnt
+        kern[stage] = {'ms_avg': round(avg, 4), 'launches': cnt}
+        b = kernel_bytes(stage, 'fp64', cells)
+        if b:
+            kern[stage].update({'algorithmic_bytes': b, 'gbs': round(b / (avg * 1e-3) / 1e9, 1),
+                                'frac_of_peak': round(b / (avg * 1e-3) / 1e9 / peak, 3)})
+    out = {'workload': 'jet %dx%dx%d, tendencies + application + ts halo per call' % (args.nx, args.nx, args.nlay),
+           'ms_per_call': ms, 'cells_per_s': world * cells / (ms * 1e-3), 'kernels': kern,
+           'peak_gbs': peak, 'peak_kind': peak_kind}
+    if world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+        import pyoracle
+        sm = ic.jet_case(SAMPLE_N, SAMPLE_N, args.nlay, 25e3, 25e3, seed=0)
+        sm.ts = np.full((sm.ny, sm.nx), 288.0)
+        o = pyoracle.OracleModel(sm)
+        o.physics_tendencies()
+        o.apply_physics(DT)
+        t0 = time.perf_counter()
+        n = 2
+        for _ in range(n):
+            o.physics_tendencies()
+            o.apply_physics(DT)
+            o.physics_halo()
+        t = time.perf_counter() - t0
+        out['cpu_baseline'] = {'value': sm.cells * n / t, 'unit': 'cells/s', 'cores': 1, 'kind': 'port',
+                               'sample': 'jet %dx%dx%d, %d calls after 1 warm-up' % (SAMPLE_N, SAMPLE_N,
+                                                                                     args.nlay, n)}
+    return out
+
+
 def adjoint_leg(args, torch, max_over_ranks, world):
     """fwd+adjoint through atmdyn.adjoint.integrate (checkpoints every
     ADJ_CKPT steps, tapes within a segment) on the headline workload, and
@@ -357,10 +431,12 @@ def adjoint_leg(args, torch, max_over_ranks, world):
     from atmdyn.adjoint import integrate, gaussian_mask
     out = {}
 
-    def timed(st, nsteps, remap_every, ckpt, reps):
+    def timed(st, nsteps, remap_every, ckpt, reps, dense=False):
         dyn = Dycore(st)
         dyn.adj_enable()
         mask = gaussian_mask(st, 300e3, device='cuda')
+        if dense:  # J = sum(theta^2): the adjoint is non-zero everywhere from the first reverse step
+            mask = torch.ones_like(mask)
         x = [torch.tensor(np.ascontiguousarray(a), device='cuda', requires_grad=True)
              for a in (st.dp, st.pt, st.u, st.v)]
 
@@ -406,12 +482,13 @@ def adjoint_leg(args, torch, max_over_ranks, world):
     st.dt = DT
     nsteps = args.adj_steps
     try:
-        dyn, x, _, _, J, (tf, tb, prof, launches, clocks) = timed(st, nsteps, REMAP_EVERY, ADJ_CKPT, 2)
+        dyn, x, _, _, J, (tf, tb, prof, launches, clocks) = timed(st, nsteps, REMAP_EVERY, ADJ_CKPT, 2,
+                                                                  dense=args.adj_dense)
         cells = st.cells
         out['value'] = world * cells * nsteps / ((tf + tb) * 1e-3)
         out['unit'] = 'cell-steps/s (forward + adjoint)'
-        out['workload'] = 'jet %dx%dx%d, %d steps, remap every %d, checkpoints every %d, J = sum(mask theta^2)' % (
-            args.nx, args.nx, args.nlay, nsteps, REMAP_EVERY, ADJ_CKPT)
+        out['workload'] = 'jet %dx%dx%d, %d steps, remap every %d, checkpoints every %d, J = sum(%stheta^2)' % (
+            args.nx, args.nx, args.nlay, nsteps, REMAP_EVERY, ADJ_CKPT, '' if args.adj_dense else 'mask ')
         out['forward_ms'] = tf
         out['backward_ms'] = tb
         out['backward_over_forward'] = tb / tf
@@ -420,6 +497,17 @@ def adjoint_leg(args, torch, max_over_ranks, world):
         out['clocks'] = clocks
         dyn.close()
         del dyn, x, J
+        torch.cuda.empty_cache()
+        if not args.adj_dense:
+            # the same run with an unmasked loss: no tile of the adjoint is zero
+            dyn, x, _, _, J, (tf, tb, prof, launches, clocks) = timed(st, nsteps, REMAP_EVERY, ADJ_CKPT, 1,
+                                                                      dense=True)
+            out['dense_loss'] = {'J': 'sum(theta^2) over the domain', 'forward_ms': tf, 'backward_ms': tb,
+                                 'backward_over_forward': tb / tf,
+                                 'value': world * st.cells * nsteps / ((tf + tb) * 1e-3), 'stages_ms': prof,
+                                 'clocks': clocks}
+            dyn.close()
+            del dyn, x, J
     except Exception as e:  # e.g. the tapes do not fit
         out['error'] = repr(e)[:300]
     torch.cuda.empty_cache()
@@ -447,7 +535,7 @@ def adjoint_leg(args, torch, max_over_ranks, world):
                 'per_direction': fd}
 
     st4 = ic.config(4)
-    dyn, x, final_theta, mask, J, (tf, tb, prof, launches, clocks) = timed(st4, st4.nsteps, st4.remap_every, 5, 1)
+    dyn, x, final_theta, mask, J, (tf, tb, prof4, launches, clocks) = timed(st4, st4.nsteps, st4.remap_every, 5, 1)
     gen = torch.Generator(device='cpu').manual_seed(4)
     fd_spec = fd_check(dyn, x, final_theta, mask, gen, (1e-6, 1e-3))
     dyn.close()
@@ -465,7 +553,7 @@ def adjoint_leg(args, torch, max_over_ranks, world):
     fd_generic = fd_check(dyn, x, final_theta, mask, gen, (1e-6,))
     out['differentiation_case'] = {
         'workload': 'jet 512x512x32 (seed 2), 20 steps, dt 30 s, remap every 5, checkpoints every 5',
-        'J': J.item(), 'forward_ms': tf, 'backward_ms': tb, 'backward_over_forward': tb / tf,
+        'J': J.item(), 'forward_ms': tf, 'backward_ms': tb, 'backward_over_forward': tb / tf, 'stages_ms': prof4,
         'cell_steps_per_s': st4.cells * st4.nsteps / ((tf + tb) * 1e-3),
         'fd_check': fd_spec,
         'fd_check_ties_broken': fd_generic,
@@ -616,6 +704,9 @@ def main():
     ap.add_argument('--adj-steps', type=int, default=16, help='steps of the timed forward + adjoint run')
     ap.add_argument('--no-ensemble', action='store_true', help='skip the batched-ensemble leg')
     ap.add_argument('--no-fdcheck', action='store_true', help='skip the differentiation case of the adjoint leg')
+    ap.add_argument('--no-physics', action='store_true', help='skip the column-physics leg')
+    ap.add_argument('--adj-dense', action='store_true',
+                    help='time the adjoint leg with the unmasked loss only (profiling of the dense adjoint)')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
