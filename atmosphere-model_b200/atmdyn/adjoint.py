@@ -10,7 +10,10 @@ adjoint steps in reverse order (``atm_adj_step_tape``: the CUDA adjoint
 kernels of the sweeps, the remap and the halo fills, with the limiter
 branches of the recomputed forward).
 :func:`integrate` chains segments of ``checkpoint_every`` steps, so memory
-grows with the number of checkpoints plus one segment of states.
+grows with the number of checkpoints plus one segment of states.  The
+last segment's forward records its tapes as it goes (the backward starts
+there and would recompute it at once), so its backward recomputes
+nothing; the peak memory is the same one segment of tapes.
 
 The step is the reference's time loop (src/mod_model.f90:146-177): C-grid
 half step, C-grid halo, D-grid step, vertical remap every ``remap_every``
@@ -54,20 +57,41 @@ def _download(dyn: Dycore, like):
     return outs
 
 
+def _record(dyn: Dycore, dt: float, remaps, like):
+    """Steps from the context's current state keeping, per step, the
+    initial state and the tape of its forward products."""
+    states, tapes = [], []
+    for r in remaps:
+        st = torch.empty(dyn.state_bytes() // 8, dtype=torch.float64, device=like.device)
+        dyn.state_save(st.data_ptr())
+        states.append(st)
+        tp = torch.empty(dyn.tape_bytes() // 8, dtype=torch.float64, device=like.device)
+        dyn.step_tape(dt, bool(r), tp.data_ptr())
+        tapes.append(tp)
+    return states, tapes
+
+
 class DycoreSegment(torch.autograd.Function):
     """(dp, pt, ud, vd) -> the state after ``len(remaps)`` steps of size dt;
-    remaps[i] says whether step i ends with the vertical remap."""
+    remaps[i] says whether step i ends with the vertical remap.  With
+    ``record`` the forward keeps every step's state and tape (the segment
+    the backward starts with) instead of a checkpoint."""
 
     @staticmethod
-    def forward(ctx, dyn: Dycore, dt: float, remaps, dp, pt, ud, vd):
+    def forward(ctx, dyn: Dycore, dt: float, remaps, record: bool, dp, pt, ud, vd):
         _bind_stream(dyn)
         _upload(dyn, (dp, pt, ud, vd))
-        ckpt = torch.empty(dyn.state_bytes() // 8, dtype=torch.float64, device=dp.device)
-        dyn.state_save(ckpt.data_ptr())
-        for r in remaps:
-            dyn.step(dt, remap=bool(r), check_stable=False)
-        outs = _download(dyn, dp)
         ctx.dyn, ctx.dt, ctx.remaps = dyn, dt, tuple(bool(r) for r in remaps)
+        if record:
+            ctx.trajectory = _record(dyn, dt, ctx.remaps, dp)
+            ckpt = torch.empty(0, dtype=torch.float64, device=dp.device)
+        else:
+            ctx.trajectory = None
+            ckpt = torch.empty(dyn.state_bytes() // 8, dtype=torch.float64, device=dp.device)
+            dyn.state_save(ckpt.data_ptr())
+            for r in ctx.remaps:
+                dyn.step(dt, remap=r, check_stable=False)
+        outs = _download(dyn, dp)
         ctx.save_for_backward(ckpt)
         ctx.mark_non_differentiable()
         return tuple(outs)
@@ -77,17 +101,14 @@ class DycoreSegment(torch.autograd.Function):
         dyn, dt, remaps = ctx.dyn, ctx.dt, ctx.remaps
         (ckpt,) = ctx.saved_tensors
         _bind_stream(dyn)
-        dyn.state_load(ckpt.data_ptr())
-        # recompute the segment, keeping every step's initial state and its
-        # forward products (C-grid fields, pre-remap state) on a tape
-        states, tapes = [], []
-        for r in remaps:
-            s = torch.empty_like(ckpt)
-            dyn.state_save(s.data_ptr())
-            states.append(s)
-            tp = torch.empty(dyn.tape_bytes() // 8, dtype=torch.float64, device=ckpt.device)
-            dyn.step_tape(dt, r, tp.data_ptr())
-            tapes.append(tp)
+        if ctx.trajectory is not None:
+            states, tapes = ctx.trajectory
+            ctx.trajectory = None
+        else:
+            # recompute the segment, keeping every step's initial state and
+            # its forward products (C-grid fields, pre-remap state) on a tape
+            dyn.state_load(ckpt.data_ptr())
+            states, tapes = _record(dyn, dt, remaps, ckpt)
         dyn.adj_zero()
         grads = [g if g is not None else torch.zeros_like(ckpt[:0]) for g in (gdp, gpt, gud, gvd)]
         for name, g in zip(FIELD_NAMES, grads):
@@ -96,6 +117,7 @@ class DycoreSegment(torch.autograd.Function):
         for s, tp, r in zip(reversed(states), reversed(tapes), reversed(remaps)):
             dyn.state_load(s.data_ptr())
             dyn.adj_step_tape(dt, r, tp.data_ptr())
+        del states, tapes
         dyn.adj_halo('out')  # the initial state's halo is the periodic image of its interior
         like = gdp if gdp is not None else (gpt if gpt is not None else (gud if gud is not None else gvd))
         outs = []
@@ -103,7 +125,7 @@ class DycoreSegment(torch.autograd.Function):
             o = torch.empty_like(like)
             dyn.adj_get_device('out', name, o.data_ptr())
             outs.append(o)
-        return (None, None, None, *outs)
+        return (None, None, None, None, *outs)
 
 
 def integrate(dyn: Dycore, fields, nsteps: int, dt: float, remap_every: int, checkpoint_every: int,
@@ -111,12 +133,13 @@ def integrate(dyn: Dycore, fields, nsteps: int, dt: float, remap_every: int, che
     """Advance (dp, pt, ud, vd) by nsteps with checkpoints every
     ``checkpoint_every`` steps; differentiable with respect to the inputs."""
     out = tuple(fields)
+    grad = torch.is_grad_enabled() and any(f.requires_grad for f in fields)
     s = first_step
     end = first_step + nsteps
     while s < end:
         n = min(checkpoint_every, end - s)
         remaps = [(q + 1) % remap_every == 0 for q in range(s, s + n)]
-        out = DycoreSegment.apply(dyn, dt, remaps, *out)
+        out = DycoreSegment.apply(dyn, dt, remaps, grad and s + n >= end, *out)
         s += n
     return out
 

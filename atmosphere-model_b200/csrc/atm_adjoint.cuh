@@ -680,7 +680,7 @@ template <int TX, int TY>
 struct CMomAdjL {
   using F = CMomL<double, TX, TY>;
   static constexpr size_t lam =
-      2 * box_bytes<double>(TX + 6, TY + 6) + 2 * box_bytes<double>(TX + 1, TY + 1) +  // uc1, vc1, uaL, vaL
+      2 * box_bytes<double>(TX + 6, TY + 6) +                                          // uc1, vc1
       box_bytes<double>(TX + 5, TY + 5) + box_bytes<double>(TX + 1, TY + 1) +          // vor, ke
       box_bytes<double>(TX, TY + 5) + box_bytes<double>(TX + 5, TY) +                  // tU, tV
       box_bytes<double>(TX + 1, TY + 1) +                                              // lap
@@ -688,12 +688,29 @@ struct CMomAdjL {
       box_bytes<double>(TX, TY + 3) + box_bytes<double>(TX + 3, TY) +                  // mtU, mtV
       2 * box_bytes<double>(TX + 7, TY + 7) + 2 * box_bytes<double>(TX + 3, TY + 3) +  // ud, vd (k, nlay)
       4 * box_bytes<double>(TX + 1, TY + 1);                                           // pkap, gz (k, k+1)
-  // the forward's ke and lap values are not needed by the reverse
+  // the forward's ke and lap values are not needed by the reverse, and
+  // the layer-nlay A-grid winds are recomputed where the reverse reads them
   static constexpr size_t bytes = F::bytes - 2 * box_bytes<double>(TX + 1, TY + 1) + lam;
 };
 
+// The layer-nlay A-grid winds at (x, y) from the layer-nlay D-grid winds
+// (src/mod_sw_dyn.f90:119-125), the operations of k_c_mom2.
+struct ALWinds {
+  double ua, va;
+};
+__device__ __forceinline__ ALWinds al_winds(const Sm<double>& udL, const Sm<double>& vdL, int x, int y) {
+  using T = double;
+  T ub = T(.5) * (udL(x, y) + udL(x - 1, y));
+  T ucl = T(.5) * (ub + T(.5) * (udL(x, y + 1) + udL(x - 1, y + 1)));
+  T vb = T(.5) * (vdL(x, y) + vdL(x, y - 1));
+  T vcl = T(.5) * (vb + T(.5) * (vdL(x + 1, y) + vdL(x + 1, y - 1)));
+  return ALWinds{T(.5) * (ucl + T(.25) * (udL(x + 1, y) + udL(x, y) + udL(x + 1, y + 1) + udL(x, y + 1))),
+                 T(.5) * (vcl + T(.25) * (vdL(x, y + 1) + vdL(x, y) + vdL(x + 1, y + 1) + vdL(x + 1, y)))};
+}
+
+// 3 CTAs per SM: shared memory (the layout above) and 85 registers a thread
 template <int TX, int TY>
-__global__ void __launch_bounds__(NTA, 1) k_c_mom_adj(const __grid_constant__ CUtensorMap m_ud,
+__global__ void __launch_bounds__(NTA, 3) k_c_mom_adj(const __grid_constant__ CUtensorMap m_ud,
                                                   const __grid_constant__ CUtensorMap m_vd,
                                                   const __grid_constant__ CUtensorMap m_udL,
                                                   const __grid_constant__ CUtensorMap m_vdL,
@@ -736,8 +753,6 @@ __global__ void __launch_bounds__(NTA, 1) k_c_mom_adj(const __grid_constant__ CU
   }
   Sm<T> uc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
   Sm<T> vc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
-  Sm<T> uaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<T> vaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
   Sm<T> vor = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
   Sm<T> tU = carve<T>(p, ox, oy - 2, TX, TY + 5);
   Sm<T> tV = carve<T>(p, ox - 2, oy, TX + 5, TY);
@@ -775,14 +790,6 @@ __global__ void __launch_bounds__(NTA, 1) k_c_mom_adj(const __grid_constant__ CU
     uc1(x, y) = T(.5) * (ub + T(.5) * (sud(x, y + 1) + sud(x - 1, y + 1)));
     T vb = T(.5) * (svd(x, y) + svd(x, y - 1));
     vc1(x, y) = T(.5) * (vb + T(.5) * (svd(x + 1, y) + svd(x + 1, y - 1)));
-  });
-  aregion<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
-    T ub = T(.5) * (udL(x, y) + udL(x - 1, y));
-    T ucl = T(.5) * (ub + T(.5) * (udL(x, y + 1) + udL(x - 1, y + 1)));
-    uaL(x, y) = T(.5) * (ucl + T(.25) * (udL(x + 1, y) + udL(x, y) + udL(x + 1, y + 1) + udL(x, y + 1)));
-    T vb = T(.5) * (vdL(x, y) + vdL(x, y - 1));
-    T vcl = T(.5) * (vb + T(.5) * (vdL(x + 1, y) + vdL(x + 1, y - 1)));
-    vaL(x, y) = T(.5) * (vcl + T(.25) * (vdL(x, y + 1) + vdL(x, y) + vdL(x + 1, y + 1) + vdL(x + 1, y)));
   });
   __syncthreads();
   const T f = c.coriolis;
@@ -879,7 +886,8 @@ __global__ void __launch_bounds__(NTA, 1) k_c_mom_adj(const __grid_constant__ CU
   aregion<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
     const double l = ake(x, y);
     if (l == 0.) return;
-    const T va = vaL(x, y), ua = uaL(x, y);
+    const ALWinds aw = al_winds(udL, vdL, x, y);
+    const T va = aw.va, ua = aw.ua;
     double lcy = 0., lcx = 0.;
     double fy = flux_unc_adj(vc1.ptr(x, y + 1), TX + 6, mvy.ptr(x, y + 1), TX + 1, dtdy * va, .5 * va * l,
                                       avc1.ptr(x, y + 1), TX + 6, amvy.ptr(x, y + 1), TX + 1, lcy);
