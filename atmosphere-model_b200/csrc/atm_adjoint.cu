@@ -36,7 +36,8 @@ cudaError_t adj_setup() {
   if ((e = smem_attr(k_mass_adj<TXA, TYA, true>, MassAdjL<TXA, TYA, true>::bytes))) return e;
   if ((e = smem_attr(k_mass_adj<TXA, TYA, false>, MassAdjL<TXA, TYA, false>::bytes))) return e;
   if ((e = smem_attr(k_c_mom_adj<TXA, TYM>, CMomAdjL<TXA, TYM>::bytes))) return e;
-  if ((e = smem_attr(k_d_mom_adj<TXA, TYM>, DMomAdjL<TXA, TYM>::bytes))) return e;
+  if ((e = smem_attr(k_d_mom_adj_ke<TXA, TYM>, DMomKeAdjL<TXA, TYM>::bytes))) return e;
+  if ((e = smem_attr(k_d_mom_adj_vf<TXA, TYM>, DMomVfAdjL<TXA, TYM>::bytes))) return e;
   return cudaSuccess;
 }
 
@@ -90,7 +91,12 @@ cudaError_t adj_d_mom(const Geom& g, const Consts& c, const double* ud, const do
       (e = tmap(uc, 8, g, g.L, Lay::WC, Lay::HC, &muc)) || (e = tmap(vc, 8, g, g.L, Lay::WC, Lay::HC, &mvc)) ||
       (e = tmap(pkapb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpb)) || (e = tmap(gzb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgb)))
     return e;
-  k_d_mom_adj<TXA, TYM><<<tiles_a(0, 0, g, TYM), NTA, DMomAdjL<TXA, TYM>::bytes, s>>>(
+  // the kinetic-energy chain and the rest, both adding into the same
+  // global adjoints
+  k_d_mom_adj_ke<TXA, TYM><<<tiles_a(0, 0, g, TYM), NTA, DMomKeAdjL<TXA, TYM>::bytes, s>>>(
+      mu, mv, muL, mvL, g, c, lam_udo, lam_vdo, lam_ud, lam_vd, lam_uc, lam_vc, timeout);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_d_mom_adj_vf<TXA, TYM><<<tiles_a(0, 0, g, TYM), NTA, DMomVfAdjL<TXA, TYM>::bytes, s>>>(
       mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c, lam_udo, lam_vdo, lam_ud, lam_vd, lam_uc, lam_vc, lam_pkb, lam_gzb,
       timeout);
   return cudaGetLastError();

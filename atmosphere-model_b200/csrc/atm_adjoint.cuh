@@ -986,35 +986,184 @@ __global__ void __launch_bounds__(NTA, 3) k_c_mom_adj(const __grid_constant__ CU
 // =================================================== D-momentum adjoint ====
 // Adjoint of k_d_mom2: ud, vd of layer k from the old ud, vd, uc, vc of
 // layers k and nlay and pkapb, gzb of levels k, k+1 (src/mod_sw_dyn.f90:634-771).
+// The reverse splits into two chains that share only the adjoints of the
+// inputs, which meet in global memory through the flush atomics: the
+// kinetic-energy flux (:639-657: its PPM sweeps of ud, vd with the layer-nlay
+// B-grid winds) and everything else (the vorticity-flux sweeps, the
+// divergence and vorticity damping, the PGF and the direct terms).  One
+// kernel each keeps the shared memory of a CTA small enough for 5 and 3
+// CTAs per SM where one kernel held 2.
+
+// the kinetic-energy chain: ud, vd and the layer-nlay C-grid winds
 template <int TX, int TY>
-struct DMomAdjL {
+struct DMomKeAdjL {
   using F = DMomL<double, TX, TY>;
-  // forward work arrays without aliasing (the reverse needs every one)
-  // (the divergence, its Laplacians, ke and lap values are not needed by the reverse)
-  static constexpr size_t fwd = box_bytes<double>(TX + 5, TY + 5) + 2 * box_bytes<double>(TX + 1, TY + 1) +
-                                box_bytes<double>(TX, TY + 5) + box_bytes<double>(TX + 5, TY) + F::slopes_ke +
-                                F::slopes_vf + F::edges_ke + F::edges_vf;
-  static constexpr size_t lam = box_bytes<double>(TX + 5, TY + 5) * 2 + box_bytes<double>(TX + 3, TY + 3) +
-                                4 * box_bytes<double>(TX + 1, TY + 1) + box_bytes<double>(TX, TY + 5) +
-                                box_bytes<double>(TX + 5, TY) + box_bytes<double>(TX + 1, TY + 1) + F::slopes_ke +
-                                F::slopes_vf + F::edges_ke + F::edges_vf + 2 * box_bytes<double>(TX + 6, TY + 6) +
-                                box_bytes<double>(TX + 1, TY + 5) + box_bytes<double>(TX + 5, TY + 1) +
-                                2 * box_bytes<double>(TX, TY) + 4 * box_bytes<double>(TX + 1, TY + 1);
+  static constexpr size_t boxes = 2 * tma_box_bytes(F::WU, F::HU, 8) + tma_box_bytes(F::WUL, F::HUL, 8) +
+                                  tma_box_bytes(F::WVL, F::HVL, 8);
+  static constexpr uint32_t tx_bytes = (uint32_t)((2 * F::WU * F::HU + F::WUL * F::HUL + F::WVL * F::HVL) * 8);
+  static constexpr size_t fwd = F::slopes_ke + F::edges_ke;
+  static constexpr size_t lam = box_bytes<double>(TX + 1, TY + 1) + F::edges_ke + F::slopes_ke +
+                                2 * box_bytes<double>(TX + 6, TY + 6) + box_bytes<double>(TX + 1, TY + 5) +
+                                box_bytes<double>(TX + 5, TY + 1);
+  static constexpr size_t bytes = boxes + fwd + lam + 128;
+};
+
+// the rest: all ten input boxes
+template <int TX, int TY>
+struct DMomVfAdjL {
+  using F = DMomL<double, TX, TY>;
+  static constexpr size_t fwd = box_bytes<double>(TX + 5, TY + 5) + box_bytes<double>(TX, TY + 5) +
+                                box_bytes<double>(TX + 5, TY) + F::slopes_vf + F::edges_vf;
+  static constexpr size_t lam = 2 * box_bytes<double>(TX + 5, TY + 5) + box_bytes<double>(TX + 3, TY + 3) +
+                                2 * box_bytes<double>(TX + 1, TY + 1) + box_bytes<double>(TX, TY + 5) +
+                                box_bytes<double>(TX + 5, TY) + F::slopes_vf + F::edges_vf +
+                                2 * box_bytes<double>(TX + 6, TY + 6) + box_bytes<double>(TX + 1, TY + 5) +
+                                box_bytes<double>(TX + 5, TY + 1) + 2 * box_bytes<double>(TX, TY) +
+                                4 * box_bytes<double>(TX + 1, TY + 1);
   static constexpr size_t bytes = F::boxes + fwd + lam + 128;
 };
 
 template <int TX, int TY>
-__global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CUtensorMap m_ud,
-                                                  const __grid_constant__ CUtensorMap m_vd,
-                                                  const __grid_constant__ CUtensorMap m_ucL,
-                                                  const __grid_constant__ CUtensorMap m_vcL,
-                                                  const __grid_constant__ CUtensorMap m_uc,
-                                                  const __grid_constant__ CUtensorMap m_vc,
-                                                  const __grid_constant__ CUtensorMap m_pkb,
-                                                  const __grid_constant__ CUtensorMap m_gzb, Geom g, Consts c,
-                                                  const double* __restrict__ lam_udo, const double* __restrict__ lam_vdo,
-                                                  double* lam_ud, double* lam_vd, double* lam_uc, double* lam_vc,
-                                                  double* lam_pkb, double* lam_gzb, int* timeout) {
+__global__ void __launch_bounds__(NTA, 4) k_d_mom_adj_ke(const __grid_constant__ CUtensorMap m_ud,
+                                                     const __grid_constant__ CUtensorMap m_vd,
+                                                     const __grid_constant__ CUtensorMap m_ucL,
+                                                     const __grid_constant__ CUtensorMap m_vcL, Geom g, Consts c,
+                                                     const double* __restrict__ lam_udo,
+                                                     const double* __restrict__ lam_vdo, double* lam_ud,
+                                                     double* lam_vd, double* lam_uc, double* lam_vc, int* timeout) {
+  using T = double;
+  using Lay = DMomL<T, TX, TY>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ok;
+  unsigned char* p = smem_base(smem);
+  const int k = blockIdx.z, L = g.L;
+  const int ox = blockIdx.x * TX, oy = blockIdx.y * TY;
+  const T dtdx = c.dtdx, dtdy = c.dtdy;
+  if (!tile_active<TX, TY>(lam_udo, lam_vdo, g, k, ox, oy, g.nx - 1, g.ny - 1, &s_ok)) return;
+
+  auto tbox = [&](int i0, int j0, int w, int h) {
+    Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
+    p += tma_box_bytes(w, h, sizeof(T));
+    return s;
+  };
+  Sm<T> sud = tbox(ox - 3, oy - 3, Lay::WU, Lay::HU);
+  Sm<T> svd = tbox(ox - 3, oy - 3, Lay::WU, Lay::HU);
+  Sm<T> ucL = tbox(ox, oy - 3, Lay::WUL, Lay::HUL);
+  Sm<T> vcL = tbox(ox - 3, oy, Lay::WVL, Lay::HVL);
+  {
+    const TmaBox boxes[4] = {{&m_ud, sud.p, sud.x0, sud.y0, k},
+                             {&m_vd, svd.p, svd.x0, svd.y0, k},
+                             {&m_ucL, ucL.p, ucL.x0, ucL.y0, L - 1},
+                             {&m_vcL, vcL.p, vcL.x0, vcL.y0, L - 1}};
+    if (!tma_fetch(boxes, DMomKeAdjL<TX, TY>::tx_bytes, &bar, timeout, &s_ok)) return;
+  }
+  Sm<T> mvy = carve<T>(p, ox, oy - 2, TX + 1, TY + 4);
+  Sm<T> mux = carve<T>(p, ox - 2, oy, TX + 4, TY + 1);
+  Sm<T> lvy = carve<T>(p, ox, oy - 1, TX + 1, TY + 2), rvy = carve<T>(p, ox, oy - 1, TX + 1, TY + 2);
+  Sm<T> lux = carve<T>(p, ox - 1, oy, TX + 2, TY + 1), rux = carve<T>(p, ox - 1, oy, TX + 2, TY + 1);
+  unsigned char* lam0 = p;
+  Sm<T> ake = carve<T>(p, ox, oy, TX + 1, TY + 1);
+  Sm<T> alvy = carve<T>(p, ox, oy - 1, TX + 1, TY + 2), arvy = carve<T>(p, ox, oy - 1, TX + 1, TY + 2);
+  Sm<T> alux = carve<T>(p, ox - 1, oy, TX + 2, TY + 1), arux = carve<T>(p, ox - 1, oy, TX + 2, TY + 1);
+  Sm<T> amvy = carve<T>(p, ox, oy - 2, TX + 1, TY + 4);
+  Sm<T> amux = carve<T>(p, ox - 2, oy, TX + 4, TY + 1);
+  Sm<T> asud = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
+  Sm<T> asvd = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
+  Sm<T> aucL = carve<T>(p, ox, oy - 3, TX + 1, TY + 5);
+  Sm<T> avcL = carve<T>(p, ox - 3, oy, TX + 5, TY + 1);
+  zero_smem(lam0, p);
+
+  // ---- forward recomputation (as k_d_mom2): slopes and edges of the KE sweeps
+  regions(reg<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(svd.ptr(x, y), Lay::WU); }),
+          reg<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { mux(x, y) = slope_at(sud.ptr(x, y), 1); }));
+  __syncthreads();
+  regions(reg<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
+    T eL, eR;
+    edges_pre<T, PPM_CON>(svd.ptr(x, y), Lay::WU, mvy.ptr(x, y), TX + 1, eL, eR);
+    lvy(x, y) = eL;
+    rvy(x, y) = eR;
+  }),
+          reg<TX + 2, TY + 1>(ox - 1, oy, [&](int x, int y) {
+    T eL, eR;
+    edges_pre<T, PPM_CON>(sud.ptr(x, y), 1, mux.ptr(x, y), 1, eL, eR);
+    lux(x, y) = eL;
+    rux(x, y) = eR;
+  }));
+  __syncthreads();
+
+  // ---- reverse: the kinetic-energy terms of the ud, vd updates (:665-679)
+  aregion<TX, TY>(ox, oy, [&](int x, int y) {
+    if (x >= g.nx || y >= g.ny) return;
+    const long long o = g.at(x, y, k);
+    const double lu = lam_udo[o], lv = lam_vdo[o];
+    if (lu != 0.) {
+      sadd(ake.ptr(x + 1, y), -dtdx * lu);
+      sadd(ake.ptr(x, y), dtdx * lu);
+    }
+    if (lv != 0.) {
+      sadd(ake.ptr(x, y + 1), -dtdy * lv);
+      sadd(ake.ptr(x, y), dtdy * lv);
+    }
+  });
+  __syncthreads();
+  // kinetic energy (:639-657) with the layer-nlay B-grid winds (:441-444),
+  // which the reverse recomputes where it reads them
+  aregion<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
+    const double l = ake(x, y);
+    if (l == 0.) return;
+    const T ub = T(.5) * (ucL(x, y) + ucL(x, y - 1));
+    const T vb = T(.5) * (vcL(x, y) + vcL(x - 1, y));
+    double lcy = 0., lcx = 0.;
+    double fy = flux_con_adj(svd.ptr(x, y), Lay::WU, lvy.ptr(x, y), rvy.ptr(x, y), TX + 1, dtdy * vb, .5 * vb * l,
+                             asvd.ptr(x, y), TX + 6, alvy.ptr(x, y), arvy.ptr(x, y), TX + 1, lcy);
+    double fx = flux_con_adj(sud.ptr(x, y), 1, lux.ptr(x, y), rux.ptr(x, y), 1, dtdx * ub, .5 * ub * l, asud.ptr(x, y), 1,
+                             alux.ptr(x, y), arux.ptr(x, y), 1, lcx);
+    const double lu = .5 * (.5 * fx * l + dtdx * lcx), lv = .5 * (.5 * fy * l + dtdy * lcy);
+    if (lu != 0.) {
+      sadd(aucL.ptr(x, y), lu);
+      sadd(aucL.ptr(x, y - 1), lu);
+    }
+    if (lv != 0.) {
+      sadd(avcL.ptr(x, y), lv);
+      sadd(avcL.ptr(x - 1, y), lv);
+    }
+  });
+  __syncthreads();
+  // edges of the KE sweeps
+  regions(reg<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
+    edges_con_adj(svd.ptr(x, y), Lay::WU, mvy.ptr(x, y), TX + 1, alvy(x, y), arvy(x, y), asvd.ptr(x, y), TX + 6,
+                  amvy.ptr(x, y), TX + 1);
+  }),
+          reg<TX + 2, TY + 1>(ox - 1, oy, [&](int x, int y) {
+    edges_con_adj(sud.ptr(x, y), 1, mux.ptr(x, y), 1, alux(x, y), arux(x, y), asud.ptr(x, y), 1, amux.ptr(x, y), 1);
+  }));
+  __syncthreads();
+  // slopes of the KE sweeps
+  regions(reg<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) {
+    slope_adj(svd.ptr(x, y), Lay::WU, amvy(x, y), asvd.ptr(x, y), TX + 6);
+  }),
+          reg<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { slope_adj(sud.ptr(x, y), 1, amux(x, y), asud.ptr(x, y), 1); }));
+  __syncthreads();
+  flush_box(asud, TX + 6, TY + 6, lam_ud, g, k);
+  flush_box(asvd, TX + 6, TY + 6, lam_vd, g, k);
+  flush_box(aucL, TX + 1, TY + 5, lam_uc, g, L - 1);
+  flush_box(avcL, TX + 5, TY + 1, lam_vc, g, L - 1);
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(NTA, 3) k_d_mom_adj_vf(const __grid_constant__ CUtensorMap m_ud,
+                                                     const __grid_constant__ CUtensorMap m_vd,
+                                                     const __grid_constant__ CUtensorMap m_ucL,
+                                                     const __grid_constant__ CUtensorMap m_vcL,
+                                                     const __grid_constant__ CUtensorMap m_uc,
+                                                     const __grid_constant__ CUtensorMap m_vc,
+                                                     const __grid_constant__ CUtensorMap m_pkb,
+                                                     const __grid_constant__ CUtensorMap m_gzb, Geom g, Consts c,
+                                                     const double* __restrict__ lam_udo,
+                                                     const double* __restrict__ lam_vdo, double* lam_ud,
+                                                     double* lam_vd, double* lam_uc, double* lam_vc, double* lam_pkb,
+                                                     double* lam_gzb, int* timeout) {
   using T = double;
   using Lay = DMomL<T, TX, TY>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1052,16 +1201,10 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
     if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
   }
   Sm<T> vor = carve<T>(p, ox - 3, oy - 3, TX + 5, TY + 5);
-  Sm<T> ubL = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> vbL = carve<T>(p, ox, oy, TX + 1, TY + 1);
   Sm<T> tU = carve<T>(p, ox, oy - 3, TX, TY + 5);
   Sm<T> tV = carve<T>(p, ox - 3, oy, TX + 5, TY);
-  Sm<T> mvy = carve<T>(p, ox, oy - 2, TX + 1, TY + 4);
-  Sm<T> mux = carve<T>(p, ox - 2, oy, TX + 4, TY + 1);
   Sm<T> mtU = carve<T>(p, ox, oy - 2, TX, TY + 3);
   Sm<T> mtV = carve<T>(p, ox - 2, oy, TX + 3, TY);
-  Sm<T> lvy = carve<T>(p, ox, oy - 1, TX + 1, TY + 2), rvy = carve<T>(p, ox, oy - 1, TX + 1, TY + 2);
-  Sm<T> lux = carve<T>(p, ox - 1, oy, TX + 2, TY + 1), rux = carve<T>(p, ox - 1, oy, TX + 2, TY + 1);
   Sm<T> ltU = carve<T>(p, ox, oy - 1, TX, TY + 1), rtU = carve<T>(p, ox, oy - 1, TX, TY + 1);
   Sm<T> ltV = carve<T>(p, ox - 1, oy, TX + 1, TY), rtV = carve<T>(p, ox - 1, oy, TX + 1, TY);
   unsigned char* lam0 = p;
@@ -1069,18 +1212,11 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
   Sm<T> adv0 = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
   Sm<T> adv2 = carve<T>(p, ox - 1, oy - 1, TX + 3, TY + 3);
   Sm<T> adv4 = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> aubL = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> avbL = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> ake = carve<T>(p, ox, oy, TX + 1, TY + 1);
   Sm<T> atU = carve<T>(p, ox, oy - 3, TX, TY + 5);
   Sm<T> atV = carve<T>(p, ox - 3, oy, TX + 5, TY);
   Sm<T> alap = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<T> amvy = carve<T>(p, ox, oy - 2, TX + 1, TY + 4);
-  Sm<T> amux = carve<T>(p, ox - 2, oy, TX + 4, TY + 1);
   Sm<T> amtU = carve<T>(p, ox, oy - 2, TX, TY + 3);
   Sm<T> amtV = carve<T>(p, ox - 2, oy, TX + 3, TY);
-  Sm<T> alvy = carve<T>(p, ox, oy - 1, TX + 1, TY + 2), arvy = carve<T>(p, ox, oy - 1, TX + 1, TY + 2);
-  Sm<T> alux = carve<T>(p, ox - 1, oy, TX + 2, TY + 1), arux = carve<T>(p, ox - 1, oy, TX + 2, TY + 1);
   Sm<T> altU = carve<T>(p, ox, oy - 1, TX, TY + 1), artU = carve<T>(p, ox, oy - 1, TX, TY + 1);
   Sm<T> altV = carve<T>(p, ox - 1, oy, TX + 1, TY), artV = carve<T>(p, ox - 1, oy, TX + 1, TY);
   Sm<T> asud = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
@@ -1095,65 +1231,48 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
   Sm<T> agb1 = carve<T>(p, ox, oy, TX + 1, TY + 1);
   zero_smem(lam0, p);
 
-  // ---- forward recomputation (as k_d_mom2)
+  // ---- forward recomputation (as k_d_mom2): vorticity and its flux sweeps
   const T f = c.coriolis;
   aregion<TX + 5, TY + 5>(ox - 3, oy - 3, [&](int x, int y) {
     vor(x, y) = f - (sud(x, y + 1) - sud(x, y)) * rdy + (svd(x + 1, y) - svd(x, y)) * rdx;
   });
-  aregion<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-    ubL(x, y) = T(.5) * (ucL(x, y) + ucL(x, y - 1));
-    vbL(x, y) = T(.5) * (vcL(x, y) + vcL(x - 1, y));
-  });
-  aregion<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(svd.ptr(x, y), Lay::WU); });
-  aregion<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { mux(x, y) = slope_at(sud.ptr(x, y), 1); });
   __syncthreads();
   const T rdx2 = c.rdx2, rdy2 = c.rdy2, rdxy = c.rdx2rdy2;
-  aregion<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
-    T eL, eR;
-    edges_pre<T, PPM_CON>(svd.ptr(x, y), Lay::WU, mvy.ptr(x, y), TX + 1, eL, eR);
-    lvy(x, y) = eL;
-    rvy(x, y) = eR;
-  });
-  aregion<TX + 2, TY + 1>(ox - 1, oy, [&](int x, int y) {
-    T eL, eR;
-    edges_pre<T, PPM_CON>(sud.ptr(x, y), 1, mux.ptr(x, y), 1, eL, eR);
-    lux(x, y) = eL;
-    rux(x, y) = eR;
-  });
-  aregion<TX, TY + 5>(ox, oy - 3, [&](int x, int y) {
+  regions(reg<TX, TY + 5>(ox, oy - 3, [&](int x, int y) {
     T c0 = dtdx * ucL(x, y), c1 = dtdx * ucL(x + 1, y);
     T den = T(1) / (T(1) - dtdx * (ucL(x + 1, y) - ucL(x, y)));
     T f0 = (c0 > T(0)) ? vor(x - 1, y) : vor(x, y);
     T f1 = (c1 > T(0)) ? vor(x, y) : vor(x + 1, y);
     tU(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
-  });
-  aregion<TX + 5, TY>(ox - 3, oy, [&](int x, int y) {
+  }),
+          reg<TX + 5, TY>(ox - 3, oy, [&](int x, int y) {
     T c0 = dtdx * vcL(x, y), c1 = dtdx * vcL(x, y + 1);
     T den = T(1) / (T(1) - dtdy * (vcL(x, y + 1) - vcL(x, y)));
     T f0 = (c0 > T(0)) ? vor(x, y - 1) : vor(x, y);
     T f1 = (c1 > T(0)) ? vor(x, y) : vor(x, y + 1);
     tV(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
-  });
+  }));
   __syncthreads();
   const T divdamp = c.divdamp;
-  aregion<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); });
-  aregion<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); });
+  regions(reg<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); }),
+          reg<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); }));
   __syncthreads();
-  aregion<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
+  regions(reg<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
     T eL, eR;
     edges_pre<T, PPM_CON>(tU.ptr(x, y), TX, mtU.ptr(x, y), TX, eL, eR);
     ltU(x, y) = eL;
     rtU(x, y) = eR;
-  });
-  aregion<TX + 1, TY>(ox - 1, oy, [&](int x, int y) {
+  }),
+          reg<TX + 1, TY>(ox - 1, oy, [&](int x, int y) {
     T eL, eR;
     edges_pre<T, PPM_CON>(tV.ptr(x, y), 1, mtV.ptr(x, y), 1, eL, eR);
     ltV(x, y) = eL;
     rtV(x, y) = eR;
-  });
+  }));
   __syncthreads();
 
-  // ---- reverse: ud, vd updates with the B-grid PGF (:665-679, 724-738, 755-769)
+  // ---- reverse: ud, vd updates without the KE terms, with the B-grid PGF
+  // (:665-679, 724-738, 755-769)
   const T vdx = c.vdx, vdy = c.vdy;
   aregion<TX, TY>(ox, oy, [&](int x, int y) {
     if (x >= g.nx || y >= g.ny) return;
@@ -1168,8 +1287,6 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
       sadd(asvc.ptr(x, y), dt * F * lu);
       sadd(alap.ptr(x, y), dt * vdy * lu);
       sadd(alap.ptr(x, y - 1), -dt * vdy * lu);
-      sadd(ake.ptr(x + 1, y), -dtdx * lu);
-      sadd(ake.ptr(x, y), dtdx * lu);
       sadd(adv4.ptr(x + 1, y), dtdx * lu);
       sadd(adv4.ptr(x, y), -dtdx * lu);
       PgfAdj a = pgf_adj(pb0(x + 1, y), pb1(x, y), gb0(x, y), gb1(x + 1, y), pb0(x, y), pb1(x + 1, y), gb1(x, y),
@@ -1192,8 +1309,6 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
       sadd(asuc.ptr(x, y), -dt * F * lv);
       sadd(alap.ptr(x, y), -dt * vdx * lv);
       sadd(alap.ptr(x - 1, y), dt * vdx * lv);
-      sadd(ake.ptr(x, y + 1), -dtdy * lv);
-      sadd(ake.ptr(x, y), dtdy * lv);
       sadd(adv4.ptr(x, y + 1), dtdy * lv);
       sadd(adv4.ptr(x, y), -dtdy * lv);
       PgfAdj a = pgf_adj(pb0(x, y + 1), pb1(x, y), gb0(x, y), gb1(x, y + 1), pb0(x, y), pb1(x, y + 1), gb1(x, y),
@@ -1209,28 +1324,17 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
     }
   });
   __syncthreads();
-  // edges of the vorticity-flux sweeps; kinetic energy (:639-657);
-  // del^4 (:695-702, gather); Laplacian of the vorticity (:712-721, gather)
-  aregion<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
-    edges_con_adj(tU.ptr(x, y), TX, mtU.ptr(x, y), TX, altU(x, y), artU(x, y), atU.ptr(x, y), TX, amtU.ptr(x, y), TX);
-  });
-  aregion<TX + 1, TY>(ox - 1, oy, [&](int x, int y) {
-    edges_con_adj(tV.ptr(x, y), 1, mtV.ptr(x, y), 1, altV(x, y), artV(x, y), atV.ptr(x, y), 1, amtV.ptr(x, y), 1);
-  });
-  aregion<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-    const double l = ake(x, y);
-    if (l == 0.) return;
-    const T vb = vbL(x, y), ub = ubL(x, y);
-    double lcy = 0., lcx = 0.;
-    double fy = flux_con_adj(svd.ptr(x, y), Lay::WU, lvy.ptr(x, y), rvy.ptr(x, y), TX + 1, dtdy * vb, .5 * vb * l,
-                             asvd.ptr(x, y), TX + 6, alvy.ptr(x, y), arvy.ptr(x, y), TX + 1, lcy);
-    double fx = flux_con_adj(sud.ptr(x, y), 1, lux.ptr(x, y), rux.ptr(x, y), 1, dtdx * ub, .5 * ub * l, asud.ptr(x, y), 1,
-                             alux.ptr(x, y), arux.ptr(x, y), 1, lcx);
-    avbL(x, y) += .5 * fy * l + dtdy * lcy;
-    aubL(x, y) += .5 * fx * l + dtdx * lcx;
-  });
+  // edges of the vorticity-flux sweeps; del^4 (:695-702, gather); Laplacian
+  // of the vorticity (:712-721, gather)
   auto in4 = [&](int x, int y) { return x >= ox && x <= ox + TX && y >= oy && y <= oy + TY; };
-  aregion<TX + 3, TY + 3>(ox - 1, oy - 1, [&](int x, int y) {
+  auto inP = [&](int x, int y) { return x >= ox - 1 && x <= ox + TX - 1 && y >= oy - 1 && y <= oy + TY - 1; };
+  regions(reg<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
+    edges_con_adj(tU.ptr(x, y), TX, mtU.ptr(x, y), TX, altU(x, y), artU(x, y), atU.ptr(x, y), TX, amtU.ptr(x, y), TX);
+  }),
+          reg<TX + 1, TY>(ox - 1, oy, [&](int x, int y) {
+    edges_con_adj(tV.ptr(x, y), 1, mtV.ptr(x, y), 1, altV(x, y), artV(x, y), atV.ptr(x, y), 1, amtV.ptr(x, y), 1);
+  }),
+          reg<TX + 3, TY + 3>(ox - 1, oy - 1, [&](int x, int y) {
     double a = 0.;
     if (in4(x, y)) a += -2. * rdxy * adv4(x, y);
     if (in4(x - 1, y)) a += rdx2 * adv4(x - 1, y);
@@ -1238,9 +1342,8 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
     if (in4(x, y - 1)) a += rdy2 * adv4(x, y - 1);
     if (in4(x, y + 1)) a += rdy2 * adv4(x, y + 1);
     adv2(x, y) = divdamp * a;
-  });
-  auto inP = [&](int x, int y) { return x >= ox - 1 && x <= ox + TX - 1 && y >= oy - 1 && y <= oy + TY - 1; };
-  aregion<TX + 3, TY + 3>(ox - 2, oy - 2, [&](int x, int y) {
+  }),
+          reg<TX + 3, TY + 3>(ox - 2, oy - 2, [&](int x, int y) {
     double a = 0.;
     if (inP(x, y)) a += -2. * rdxy * alap(x, y);
     if (inP(x - 1, y)) a += rdx2 * alap(x - 1, y);
@@ -1248,21 +1351,13 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
     if (inP(x, y - 1)) a += rdy2 * alap(x, y - 1);
     if (inP(x, y + 1)) a += rdy2 * alap(x, y + 1);
     avor(x, y) += a;
-  });
+  }));
   __syncthreads();
-  // slopes of the vorticity-flux sweeps; edges of the KE sweeps; del^2 of
-  // the divergence (gather); layer-nlay B-grid winds (:441-444)
-  aregion<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { slope_adj(tU.ptr(x, y), TX, amtU(x, y), atU.ptr(x, y), TX); });
-  aregion<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { slope_adj(tV.ptr(x, y), 1, amtV(x, y), atV.ptr(x, y), 1); });
-  aregion<TX + 1, TY + 2>(ox, oy - 1, [&](int x, int y) {
-    edges_con_adj(svd.ptr(x, y), Lay::WU, mvy.ptr(x, y), TX + 1, alvy(x, y), arvy(x, y), asvd.ptr(x, y), TX + 6,
-                       amvy.ptr(x, y), TX + 1);
-  });
-  aregion<TX + 2, TY + 1>(ox - 1, oy, [&](int x, int y) {
-    edges_con_adj(sud.ptr(x, y), 1, mux.ptr(x, y), 1, alux(x, y), arux(x, y), asud.ptr(x, y), 1, amux.ptr(x, y), 1);
-  });
+  // slopes of the vorticity-flux sweeps; del^2 of the divergence (gather)
   auto in2 = [&](int x, int y) { return x >= ox - 1 && x <= ox + TX + 1 && y >= oy - 1 && y <= oy + TY + 1; };
-  aregion<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
+  regions(reg<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { slope_adj(tU.ptr(x, y), TX, amtU(x, y), atU.ptr(x, y), TX); }),
+          reg<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { slope_adj(tV.ptr(x, y), 1, amtV(x, y), atV.ptr(x, y), 1); }),
+          reg<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
     double a = 0.;
     if (in2(x, y)) a += -2. * rdxy * adv2(x, y);
     if (in2(x - 1, y)) a += rdx2 * adv2(x - 1, y);
@@ -1270,25 +1365,10 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
     if (in2(x, y - 1)) a += rdy2 * adv2(x, y - 1);
     if (in2(x, y + 1)) a += rdy2 * adv2(x, y + 1);
     adv0(x, y) = a;
-  });
-  aregion<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-    const double lu = .5 * aubL(x, y), lv = .5 * avbL(x, y);
-    if (lu != 0.) {
-      sadd(aucL.ptr(x, y), lu);
-      sadd(aucL.ptr(x, y - 1), lu);
-    }
-    if (lv != 0.) {
-      sadd(avcL.ptr(x, y), lv);
-      sadd(avcL.ptr(x - 1, y), lv);
-    }
-  });
+  }));
   __syncthreads();
-  // slopes of the KE sweeps; inner vorticity sweeps (:704-722, 740-753); divergence (:682-685)
-  aregion<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) {
-    slope_adj(svd.ptr(x, y), Lay::WU, amvy(x, y), asvd.ptr(x, y), TX + 6);
-  });
-  aregion<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { slope_adj(sud.ptr(x, y), 1, amux(x, y), asud.ptr(x, y), 1); });
-  aregion<TX, TY + 5>(ox, oy - 3, [&](int x, int y) {
+  // inner vorticity sweeps (:704-722, 740-753); divergence (:682-685)
+  regions(reg<TX, TY + 5>(ox, oy - 3, [&](int x, int y) {
     const double l = atU(x, y);
     if (l == 0.) return;
     const T w0 = ucL(x, y), w1 = ucL(x + 1, y);
@@ -1300,8 +1380,8 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
       sadd(aucL.ptr(x + 1, y), lw);
       sadd(aucL.ptr(x, y), -lw);
     }
-  });
-  aregion<TX + 5, TY>(ox - 3, oy, [&](int x, int y) {
+  }),
+          reg<TX + 5, TY>(ox - 3, oy, [&](int x, int y) {
     const double l = atV(x, y);
     if (l == 0.) return;
     const T w0 = vcL(x, y), w1 = vcL(x, y + 1);
@@ -1313,15 +1393,15 @@ __global__ void __launch_bounds__(NTA, 1) k_d_mom_adj(const __grid_constant__ CU
       sadd(avcL.ptr(x, y + 1), lw);
       sadd(avcL.ptr(x, y), -lw);
     }
-  });
-  aregion<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
+  }),
+          reg<TX + 5, TY + 5>(ox - 2, oy - 2, [&](int x, int y) {
     const double l = adv0(x, y);
     if (l == 0.) return;
     sadd(asud.ptr(x, y), rdx * l);
     sadd(asud.ptr(x - 1, y), -rdx * l);
     sadd(asvd.ptr(x, y), rdy * l);
     sadd(asvd.ptr(x, y - 1), -rdy * l);
-  });
+  }));
   __syncthreads();
   // vorticity (:659-663)
   aregion<TX + 5, TY + 5>(ox - 3, oy - 3, [&](int x, int y) {

@@ -872,7 +872,7 @@ int adj_d(atm_ctx* ctx, double dt, const void* const* so, const void* const* sn,
   CK(cudaMemsetAsync(ctx->lam_pkb, 0, lev, ctx->stream));
   CK(cudaMemsetAsync(ctx->lam_gzb, 0, lev, ctx->stream));
   {
-    Stage t(ctx, S_ADMOM);
+    Stage t(ctx, S_ADMOM, 2);
     CK(atm::adj_d_mom(g, k, o[F_UD], o[F_VD], cg[C_UC], cg[C_VC], ctx->pkapb, ctx->gzb, lout[F_UD], lout[F_VD],
                       lin[F_UD], lin[F_VD], ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], ctx->lam_pkb, ctx->lam_gzb,
                       &ctx->status->tma_timeout, ctx->stream));
