@@ -9,15 +9,10 @@
 namespace atm {
 namespace {
 
-// tile of the mass adjoints (TXA x TYA) and of the momentum adjoints
-// (TXA x TYM)
-#ifndef ATM_ADJ_TYA
-#define ATM_ADJ_TYA 8
-#endif
-#ifndef ATM_ADJ_TYM
-#define ATM_ADJ_TYM 4
-#endif
-constexpr int TXA = 32, TYA = ATM_ADJ_TYA, TYM = ATM_ADJ_TYM;
+// tiles of the adjoints, measured: C-grid mass TXA x TYC (3 CTAs per SM),
+// D-grid mass TXA x TYA (2 CTAs per SM; 32 x 4 is no faster there), the
+// momentum adjoints TXA x TYM
+constexpr int TXA = 32, TYC = 4, TYA = 8, TYM = 4;
 
 inline dim3 tiles_a(int lo, int hi, const Geom& g, int ty) {
   int w = g.nx - lo + hi, h = g.ny - lo + hi;
@@ -33,7 +28,7 @@ cudaError_t smem_attr(K kernel, size_t bytes) {
 
 cudaError_t adj_setup() {
   cudaError_t e;
-  if ((e = smem_attr(k_mass_adj<TXA, TYA, true>, MassAdjL<TXA, TYA, true>::bytes))) return e;
+  if ((e = smem_attr(k_mass_adj<TXA, TYC, true>, MassAdjL<TXA, TYC, true>::bytes))) return e;
   if ((e = smem_attr(k_mass_adj<TXA, TYA, false>, MassAdjL<TXA, TYA, false>::bytes))) return e;
   if ((e = smem_attr(k_c_mom_adj<TXA, TYM>, CMomAdjL<TXA, TYM>::bytes))) return e;
   if ((e = smem_attr(k_d_mom_adj_ke<TXA, TYM>, DMomKeAdjL<TXA, TYM>::bytes))) return e;
@@ -47,11 +42,11 @@ cudaError_t adj_mass(const Geom& g, const Consts& c, const double* dp, const dou
   CUtensorMap md, mp, mu, mv;
   cudaError_t e;
   if (cgrid) {
-    using Lay = MassL<double, TXA, TYA, true>;
+    using Lay = MassL<double, TXA, TYC, true>;
     if ((e = tmap(dp, 8, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, 8, g, g.L, Lay::WD, Lay::HD, &mp)) ||
         (e = tmap(u, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, 8, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
-    k_mass_adj<TXA, TYA, true><<<tiles_a(lo, hi, g, TYA), NTA, MassAdjL<TXA, TYA, true>::bytes, s>>>(
+    k_mass_adj<TXA, TYC, true><<<tiles_a(lo, hi, g, TYC), NTA, MassAdjL<TXA, TYC, true>::bytes, s>>>(
         md, mp, mu, mv, g, c, lam_dpo, lam_pto, lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
   } else {
     using Lay = MassL<double, TXA, TYA, false>;

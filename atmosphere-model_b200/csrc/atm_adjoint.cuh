@@ -383,7 +383,7 @@ struct MassAdjL {
 };
 
 template <int TX, int TY, bool CGRID>
-__global__ void __launch_bounds__(NTA, 2) k_mass_adj(const __grid_constant__ CUtensorMap m_dp,
+__global__ void __launch_bounds__(NTA, 3) k_mass_adj(const __grid_constant__ CUtensorMap m_dp,
                                                  const __grid_constant__ CUtensorMap m_pt,
                                                  const __grid_constant__ CUtensorMap m_u,
                                                  const __grid_constant__ CUtensorMap m_v, Geom g, Consts c,
