@@ -28,8 +28,9 @@ cudaError_t smem_attr(K kernel, size_t bytes) {
 
 cudaError_t adj_setup() {
   cudaError_t e;
-  if ((e = smem_attr(k_mass_adj<TXA, TYC, true>, MassAdjL<TXA, TYC, true>::bytes))) return e;
-  if ((e = smem_attr(k_mass_adj<TXA, TYA, false>, MassAdjL<TXA, TYA, false>::bytes))) return e;
+  if ((e = smem_attr(k_mass_adj1<TXA, TYC, true>, MassAdj1L<TXA, TYC, true>::bytes))) return e;
+  if ((e = smem_attr(k_mass_adj<TXA, TYA, false, true>, MassAdjBL<TXA, TYA, false>::bytes))) return e;
+  if ((e = smem_attr(k_mass_adj<TXA, TYA, false, false>, MassAdjBL<TXA, TYA, false>::bytes))) return e;
   if ((e = smem_attr(k_c_mom_adj<TXA, TYM>, CMomAdjL<TXA, TYM>::bytes))) return e;
   if ((e = smem_attr(k_d_mom_adj_ke<TXA, TYM>, DMomKeAdjL<TXA, TYM>::bytes))) return e;
   if ((e = smem_attr(k_d_mom_adj_vf<TXA, TYM>, DMomVfAdjL<TXA, TYM>::bytes))) return e;
@@ -37,24 +38,32 @@ cudaError_t adj_setup() {
 }
 
 cudaError_t adj_mass(const Geom& g, const Consts& c, const double* dp, const double* pt, const double* u,
-                     const double* v, const double* lam_dpo, const double* lam_pto, double* lam_dp, double* lam_pt,
-                     double* lam_u, double* lam_v, int lo, int hi, int* timeout, bool cgrid, cudaStream_t s) {
+                     const double* v, const double* dpo, const double* pto, const double* lam_dpo,
+                     const double* lam_pto, double* lam_dp, double* lam_pt, double* lam_u, double* lam_v, int lo,
+                     int hi, int* timeout, bool cgrid, cudaStream_t s) {
   CUtensorMap md, mp, mu, mv;
   cudaError_t e;
-  if (cgrid) {
+  if (cgrid) {  // one kernel (the update recomputed from the fluxes)
     using Lay = MassL<double, TXA, TYC, true>;
     if ((e = tmap(dp, 8, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, 8, g, g.L, Lay::WD, Lay::HD, &mp)) ||
         (e = tmap(u, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, 8, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
-    k_mass_adj<TXA, TYC, true><<<tiles_a(lo, hi, g, TYC), NTA, MassAdjL<TXA, TYC, true>::bytes, s>>>(
+    (void)dpo;
+    (void)pto;
+    k_mass_adj1<TXA, TYC, true><<<tiles_a(lo, hi, g, TYC), NTA, MassAdj1L<TXA, TYC, true>::bytes, s>>>(
         md, mp, mu, mv, g, c, lam_dpo, lam_pto, lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
-  } else {
+  } else {  // the x branch (with the direct terms) and the y branch, both adding into the same global adjoints
     using Lay = MassL<double, TXA, TYA, false>;
+    constexpr size_t bytes = MassAdjBL<TXA, TYA, false>::bytes;
     if ((e = tmap(dp, 8, g, g.L, Lay::WD, Lay::HD, &md)) || (e = tmap(pt, 8, g, g.L, Lay::WD, Lay::HD, &mp)) ||
         (e = tmap(u, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, 8, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
-    k_mass_adj<TXA, TYA, false><<<tiles_a(lo, hi, g, TYA), NTA, MassAdjL<TXA, TYA, false>::bytes, s>>>(
-        md, mp, mu, mv, g, c, lam_dpo, lam_pto, lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
+    const dim3 grid = tiles_a(lo, hi, g, TYA);
+    k_mass_adj<TXA, TYA, false, true><<<grid, NTA, bytes, s>>>(md, mp, mu, mv, g, c, dpo, pto, lam_dpo, lam_pto,
+                                                                lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_mass_adj<TXA, TYA, false, false><<<grid, NTA, bytes, s>>>(md, mp, mu, mv, g, c, dpo, pto, lam_dpo, lam_pto,
+                                                                 lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
   }
   return cudaGetLastError();
 }

@@ -369,8 +369,309 @@ __device__ __forceinline__ void flush_box(const Sm<double>& a, int w, int h, dou
 // ======================================================== mass adjoint ====
 // Adjoint of k_mass2 (C grid: dpc, ptc from dp, pt, ud, vd; D grid: dp, pt
 // from dp, pt, uc, vc), src/mod_sw_dyn.f90:94-270 and 439-600 (heating off).
+// The update's adjoint needs only the new dp and pt (read from the step's
+// outputs), so the reverse splits by sweep direction into two kernels that
+// meet in global memory through the flush atomics: the x branch (inner
+// y-sweep, its slopes, the outer x fluxes, the x terms of the damping, and
+// the direct dependence of the new dp, pt on the old) and the y branch.
+// Each holds about two thirds of the shared memory one kernel needed (3
+// CTAs per SM on 32 x 8 tiles instead of 2); the D grid uses the split, the
+// C grid the one-kernel form below.
 template <int TX, int TY, bool CGRID>
-struct MassAdjL {
+struct MassAdjBL {
+  using F = MassL<double, TX, TY, CGRID>;
+  static constexpr int UW = CGRID ? TX + 2 : TX + 1, UH = CGRID ? TY + 7 : TY + 6;
+  static constexpr int VW = CGRID ? TX + 7 : TX + 6, VH = CGRID ? TY + 2 : TY + 1;
+  static constexpr size_t cwinds = CGRID ? box_bytes<double>(TX + 1, TY + 6) + box_bytes<double>(TX + 6, TY + 1) : 0;
+  // the larger of the two branches (the y branch's arrays are the x
+  // branch's transposed, up to the row padding)
+  static constexpr size_t inner = box_bytes<double>(TX + 6, TY) > box_bytes<double>(TX, TY + 6)
+                                      ? box_bytes<double>(TX + 6, TY) : box_bytes<double>(TX, TY + 6);
+  static constexpr size_t slope = box_bytes<double>(TX + 4, TY) > box_bytes<double>(TX, TY + 4)
+                                      ? box_bytes<double>(TX + 4, TY) : box_bytes<double>(TX, TY + 4);
+  static constexpr size_t flux = box_bytes<double>(TX + 1, TY) > box_bytes<double>(TX, TY + 1)
+                                     ? box_bytes<double>(TX + 1, TY) : box_bytes<double>(TX, TY + 1);
+  static constexpr size_t fwd = cwinds + 2 * inner + box_bytes<double>(TX + 2, TY + 2) + 2 * slope + 2 * flux;
+  static constexpr size_t lam = 2 * box_bytes<double>(TX, TY) + 2 * box_bytes<double>(TX + 2, TY + 2) + 2 * slope +
+                                2 * inner + cwinds + 2 * box_bytes<double>(TX + 6, TY + 6) +
+                                box_bytes<double>(UW, UH) + box_bytes<double>(VW, VH);
+  static constexpr size_t bytes = F::boxes + fwd + lam + 128;
+};
+
+// XB: the x branch (and the direct terms); !XB: the y branch.  dpo, pto: the
+// new dp and pt the forward wrote (outputs over [lo, n-1+hi]^2).
+template <int TX, int TY, bool CGRID, bool XB>
+__global__ void __launch_bounds__(NTA, 3) k_mass_adj(const __grid_constant__ CUtensorMap m_dp,
+                                                 const __grid_constant__ CUtensorMap m_pt,
+                                                 const __grid_constant__ CUtensorMap m_u,
+                                                 const __grid_constant__ CUtensorMap m_v, Geom g, Consts c,
+                                                 const double* __restrict__ dpo, const double* __restrict__ pto,
+                                                 const double* __restrict__ lam_dpo, const double* __restrict__ lam_pto,
+                                                 double* lam_dp, double* lam_pt, double* lam_u, double* lam_v, int lo,
+                                                 int hi, int* timeout) {
+  using T = double;
+  using Lay = MassL<T, TX, TY, CGRID>;
+  using ALay = MassAdjBL<TX, TY, CGRID>;
+  constexpr int V = CGRID ? PPM_UNC : PPM_NN;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ok;
+  unsigned char* p = smem_base(smem);
+  const int k = blockIdx.z;
+  const int ox = lo + blockIdx.x * TX, oy = lo + blockIdx.y * TY;
+  const T dtdx = c.dtdx, dtdy = c.dtdy, rA = c.rA;
+  if (!tile_active<TX, TY>(lam_dpo, lam_pto, g, k, ox, oy, g.nx - 1 + hi, g.ny - 1 + hi, &s_ok)) return;
+
+  auto tbox = [&](int i0, int j0, int w, int h) {
+    Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
+    p += tma_box_bytes(w, h, sizeof(T));
+    return s;
+  };
+  Sm<T> sdp = tbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
+  Sm<T> spt = tbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
+  Sm<T> su = CGRID ? tbox(ox - 1, oy - 3, Lay::WU, Lay::HU) : tbox(ox, oy - 3, Lay::WU, Lay::HU);
+  Sm<T> sv = CGRID ? tbox(ox - 3, oy - 1, Lay::WV, Lay::HV) : tbox(ox - 3, oy, Lay::WV, Lay::HV);
+  {
+    const TmaBox boxes[4] = {{&m_dp, sdp.p, sdp.x0, sdp.y0, k},
+                             {&m_pt, spt.p, spt.x0, spt.y0, k},
+                             {&m_u, su.p, su.x0, su.y0, k},
+                             {&m_v, sv.p, sv.x0, sv.y0, k}};
+    if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
+  }
+  Sm<T> suc = su, svc = sv;
+  if (CGRID) {
+    suc = carve<T>(p, ox, oy - 3, TX + 1, TY + 6);
+    svc = carve<T>(p, ox - 3, oy, TX + 6, TY + 1);
+  }
+  // the branch's inner sweeps (x branch: the y-sweeps tyd, typ on
+  // [ox-3, ox+TX+2] x [oy, oy+TY); y branch: the x-sweeps txd, txp), their
+  // slopes along the outer direction, and its outer fluxes
+  constexpr int IW = XB ? TX + 6 : TX, IH = XB ? TY : TY + 6;
+  constexpr int MW = XB ? TX + 4 : TX, MH = XB ? TY : TY + 4;
+  constexpr int FW = XB ? TX + 1 : TX, FH = XB ? TY : TY + 1;
+  const int ix = XB ? ox - 3 : ox, iy = XB ? oy : oy - 3;
+  const int mx = XB ? ox - 2 : ox, my = XB ? oy : oy - 2;
+  constexpr int SO = XB ? 1 : IW;  // stride along the outer direction in the inner arrays
+  constexpr int SM_ = XB ? 1 : MW;
+  Sm<T> tid = carve<T>(p, ix, iy, IW, IH);
+  Sm<T> tip = carve<T>(p, ix, iy, IW, IH);
+  Sm<T> lpp = carve<T>(p, ox - 1, oy - 1, TX + 2, TY + 2);
+  Sm<T> mid = carve<T>(p, mx, my, MW, MH);
+  Sm<T> mip = carve<T>(p, mx, my, MW, MH);
+  Sm<T> fod = carve<T>(p, ox, oy, FW, FH);
+  Sm<T> fop = carve<T>(p, ox, oy, FW, FH);
+  // adjoints
+  unsigned char* lam0 = p;
+  Sm<T> Lv = carve<T>(p, ox, oy, TX, TY);
+  Sm<T> Lq = carve<T>(p, ox, oy, TX, TY);
+  Sm<T> alpd = carve<T>(p, ox - 1, oy - 1, TX + 2, TY + 2);
+  Sm<T> alpp = carve<T>(p, ox - 1, oy - 1, TX + 2, TY + 2);
+  Sm<T> amid = carve<T>(p, mx, my, MW, MH);
+  Sm<T> amip = carve<T>(p, mx, my, MW, MH);
+  Sm<T> atid = carve<T>(p, ix, iy, IW, IH);
+  Sm<T> atip = carve<T>(p, ix, iy, IW, IH);
+  Sm<T> asuc{}, asvc{};
+  if (CGRID) {
+    asuc = carve<T>(p, ox, oy - 3, TX + 1, TY + 6);
+    asvc = carve<T>(p, ox - 3, oy, TX + 6, TY + 1);
+  }
+  Sm<T> asdp = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
+  Sm<T> aspt = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
+  Sm<T> asu = CGRID ? carve<T>(p, ox - 1, oy - 3, ALay::UW, ALay::UH) : carve<T>(p, ox, oy - 3, ALay::UW, ALay::UH);
+  Sm<T> asv = CGRID ? carve<T>(p, ox - 3, oy - 1, ALay::VW, ALay::VH) : carve<T>(p, ox - 3, oy, ALay::VW, ALay::VH);
+  if (!CGRID) {
+    asuc = asu;
+    asvc = asv;
+  }
+  zero_smem(lam0, p);
+
+  // ---- forward recomputation (as k_mass2)
+  if (CGRID) {  // mod_sw_dyn.f90:109-117
+    regions(reg<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
+      T ub = T(.5) * (su(x, y) + su(x - 1, y));
+      suc(x, y) = T(.5) * (ub + T(.5) * (su(x, y + 1) + su(x - 1, y + 1)));
+    }),
+            reg<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
+      T vb = T(.5) * (sv(x, y) + sv(x, y - 1));
+      svc(x, y) = T(.5) * (vb + T(.5) * (sv(x + 1, y) + sv(x + 1, y - 1)));
+    }));
+    __syncthreads();
+  }
+  const T rdx2 = c.rdx2, rdy2 = c.rdy2, rdxy = c.rdx2rdy2;
+  regions(reg<IW, IH>(ix, iy, [&](int x, int y) {
+    if constexpr (XB) {
+      T cy0 = dtdx * svc(x, y), cy1 = dtdx * svc(x, y + 1);
+      T den = T(1) / (T(1) - dtdy * (svc(x, y + 1) - svc(x, y)));
+      T f0 = (cy0 > T(0)) ? sdp(x, y - 1) : sdp(x, y);
+      T f1 = (cy1 > T(0)) ? sdp(x, y) : sdp(x, y + 1);
+      tid(x, y) = T(.5) * (sdp(x, y) + den * (sdp(x, y) - rA * (f1 - f0)));
+      f0 = (cy0 > T(0)) ? spt(x, y - 1) : spt(x, y);
+      f1 = (cy1 > T(0)) ? spt(x, y) : spt(x, y + 1);
+      tip(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
+    } else {
+      T cx0 = dtdx * suc(x, y), cx1 = dtdx * suc(x + 1, y);
+      T den = T(1) / (T(1) - dtdx * (suc(x + 1, y) - suc(x, y)));
+      T f0 = (cx0 > T(0)) ? sdp(x - 1, y) : sdp(x, y);
+      T f1 = (cx1 > T(0)) ? sdp(x, y) : sdp(x + 1, y);
+      tid(x, y) = T(.5) * (sdp(x, y) + den * (sdp(x, y) - rA * (f1 - f0)));
+      f0 = (cx0 > T(0)) ? spt(x - 1, y) : spt(x, y);
+      f1 = (cx1 > T(0)) ? spt(x, y) : spt(x + 1, y);
+      tip(x, y) = T(.5) * (spt(x, y) + den * (spt(x, y) - rA * (f1 - f0)));
+    }
+  }),
+          reg<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
+    lpp(x, y) = T(-2.) * spt(x, y) * rdxy + (spt(x + 1, y) + spt(x - 1, y)) * rdx2 +
+                (spt(x, y + 1) + spt(x, y - 1)) * rdy2;
+  }));
+  __syncthreads();
+  aregion<MW, MH>(mx, my, [&](int x, int y) {
+    mid(x, y) = slope_at(tid.ptr(x, y), SO);
+    mip(x, y) = slope_at(tip.ptr(x, y), SO);
+  });
+  __syncthreads();
+  aregion<FW, FH>(ox, oy, [&](int x, int y) {
+    T cw = dtdx * (XB ? suc(x, y) : svc(x, y));
+    fod(x, y) = flux_pre<T, V>(tid.ptr(x, y), SO, mid.ptr(x, y), SM_, cw) * cw;
+    fop(x, y) = flux_pre<T, V>(tip.ptr(x, y), SO, mip.ptr(x, y), SM_, cw);
+  });
+  __syncthreads();
+
+  // ---- reverse
+  const int xhi = g.nx - 1 + hi, yhi = g.ny - 1 + hi;
+  const T dxv = dtdx * c.vdx, dyv = dtdy * c.vdy, vdx = c.vdx, vdy = c.vdy;
+  // updates (:163-172,193-202,230-237,258-267 / :490-499,519-528,555-562,582-591):
+  // Lv = adjoint of the new dp, Lq = adjoint of the numerator of the new pt
+  aregion<TX, TY>(ox, oy, [&](int x, int y) {
+    double lv = 0., lq = 0.;
+    if (x <= xhi && y <= yhi) {
+      const long long o = g.at(x, y, k);
+      const double v = dpo[o], qv = pto[o];  // the new dp and pt = q / v
+      const double lpo = lam_pto[o];
+      lq = lpo / v;
+      lv = lam_dpo[o] - qv / v * lpo;
+      if (XB) {
+        asdp(x, y) += lv + spt(x, y) * lq;
+        aspt(x, y) += sdp(x, y) * lq;
+      }
+    }
+    Lv(x, y) = lv;
+    Lq(x, y) = lq;
+  });
+  __syncthreads();
+  auto inT = [&](int x, int y) { return x >= ox && x < ox + TX && y >= oy && y < oy + TY; };
+  auto LV = [&](int x, int y) { return inT(x, y) ? Lv(x, y) : 0.; };
+  auto LQ = [&](int x, int y) { return inT(x, y) ? Lq(x, y) : 0.; };
+  // the branch's terms of the Laplacians' adjoints (gather), and the outer
+  // PPM sweep (:156-161,186-191 / :484-489,513-518)
+  regions(reg<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
+    double a = 0.;
+    if constexpr (XB) {
+      alpd(x, y) = dxv * (2. * LV(x, y) - LV(x - 1, y) - LV(x + 1, y));
+      if (inT(x - 1, y)) a -= fod(x, y) * Lq(x - 1, y);
+      if (inT(x, y)) a += (fod(x + 1, y) + fod(x, y)) * Lq(x, y);
+      if (inT(x + 1, y)) a -= fod(x + 1, y) * Lq(x + 1, y);
+      alpp(x, y) = vdx * a;
+    } else {
+      alpd(x, y) = dyv * (2. * LV(x, y) - LV(x, y - 1) - LV(x, y + 1));
+      if (inT(x, y - 1)) a -= fod(x, y) * Lq(x, y - 1);
+      if (inT(x, y)) a += (fod(x, y + 1) + fod(x, y)) * Lq(x, y);
+      if (inT(x, y + 1)) a -= fod(x, y + 1) * Lq(x, y + 1);
+      alpp(x, y) = vdy * a;
+    }
+  }),
+          reg<FW, FH>(ox, oy, [&](int x, int y) {
+    const int xm = XB ? x - 1 : x, ym = XB ? y : y - 1;  // the upstream cell of the face
+    const double ql = LQ(xm, ym), qr = LQ(x, y);
+    const double lfd = (LV(x, y) - LV(xm, ym)) + (fop(x, y) + (XB ? vdx : vdy) * (lpp(x, y) - lpp(xm, ym))) * (qr - ql);
+    const double lfp = fod(x, y) * (qr - ql);
+    if (lfd == 0. && lfp == 0.) return;
+    const T cw = dtdx * (XB ? suc(x, y) : svc(x, y));
+    double lc = 0.;
+    double Fl = flux_adj<V>(tid.ptr(x, y), SO, mid.ptr(x, y), SM_, cw, lfd * cw, atid.ptr(x, y), SO, amid.ptr(x, y),
+                            SM_, lc);
+    lc += lfd * Fl;
+    flux_adj<V>(tip.ptr(x, y), SO, mip.ptr(x, y), SM_, cw, lfp, atip.ptr(x, y), SO, amip.ptr(x, y), SM_, lc);
+    if (XB) asuc(x, y) += dtdx * lc;
+    else asvc(x, y) += dtdx * lc;
+  }));
+  __syncthreads();
+  // slopes (:870-875) and the Laplacians (:148-153,178-183 / :476-481,505-510)
+  auto inL = [&](int x, int y) { return x >= ox - 1 && x < ox + TX + 1 && y >= oy - 1 && y < oy + TY + 1; };
+  regions(reg<MW, MH>(mx, my, [&](int x, int y) {
+    slope_adj(tid.ptr(x, y), SO, amid(x, y), atid.ptr(x, y), SO);
+    slope_adj(tip.ptr(x, y), SO, amip(x, y), atip.ptr(x, y), SO);
+  }),
+          reg<TX + 4, TY + 4>(ox - 2, oy - 2, [&](int x, int y) {
+    double ad = 0., ap = 0.;
+    if (inL(x, y)) { ad += -2. * rdxy * alpd(x, y); ap += -2. * rdxy * alpp(x, y); }
+    if (inL(x - 1, y)) { ad += rdx2 * alpd(x - 1, y); ap += rdx2 * alpp(x - 1, y); }
+    if (inL(x + 1, y)) { ad += rdx2 * alpd(x + 1, y); ap += rdx2 * alpp(x + 1, y); }
+    if (inL(x, y - 1)) { ad += rdy2 * alpd(x, y - 1); ap += rdy2 * alpp(x, y - 1); }
+    if (inL(x, y + 1)) { ad += rdy2 * alpd(x, y + 1); ap += rdy2 * alpp(x, y + 1); }
+    asdp(x, y) += ad;
+    aspt(x, y) += ap;
+  }));
+  __syncthreads();
+  // inner sweeps (:142-147,176-177,210-216,238-243 / :470-475,503-504,531-536,563-568)
+  aregion<IW, IH>(ix, iy, [&](int x, int y) {
+    const double ld = atid(x, y), lp = atip(x, y);
+    if (ld == 0. && lp == 0.) return;
+    double lden = 0.;
+    if constexpr (XB) {
+      const T w0 = svc(x, y), w1 = svc(x, y + 1);
+      const T cy0 = dtdx * w0, cy1 = dtdx * w1;
+      const T den = T(1) / (T(1) - dtdy * (w1 - w0));
+      inner_adj(sdp.ptr(x, y), sdp.w, cy0, cy1, den, rA, ld, asdp.ptr(x, y), TX + 6, lden);
+      inner_adj(spt.ptr(x, y), spt.w, cy0, cy1, den, rA, lp, aspt.ptr(x, y), TX + 6, lden);
+      const double lw = dtdy * den * den * lden;
+      if (lw != 0.) {
+        sadd(asvc.ptr(x, y + 1), lw);
+        sadd(asvc.ptr(x, y), -lw);
+      }
+    } else {
+      const T w0 = suc(x, y), w1 = suc(x + 1, y);
+      const T cx0 = dtdx * w0, cx1 = dtdx * w1;
+      const T den = T(1) / (T(1) - dtdx * (w1 - w0));
+      inner_adj(sdp.ptr(x, y), 1, cx0, cx1, den, rA, ld, asdp.ptr(x, y), 1, lden);
+      inner_adj(spt.ptr(x, y), 1, cx0, cx1, den, rA, lp, aspt.ptr(x, y), 1, lden);
+      const double lw = dtdx * den * den * lden;
+      if (lw != 0.) {
+        sadd(asuc.ptr(x + 1, y), lw);
+        sadd(asuc.ptr(x, y), -lw);
+      }
+    }
+  });
+  __syncthreads();
+  if (CGRID) {  // C-grid winds from the D-grid winds (:109-117)
+    regions(reg<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
+      const double l = .25 * asuc(x, y);
+      if (l == 0.) return;
+      sadd(asu.ptr(x, y), l);
+      sadd(asu.ptr(x - 1, y), l);
+      sadd(asu.ptr(x, y + 1), l);
+      sadd(asu.ptr(x - 1, y + 1), l);
+    }),
+            reg<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
+      const double l = .25 * asvc(x, y);
+      if (l == 0.) return;
+      sadd(asv.ptr(x, y), l);
+      sadd(asv.ptr(x, y - 1), l);
+      sadd(asv.ptr(x + 1, y), l);
+      sadd(asv.ptr(x + 1, y - 1), l);
+    }));
+    __syncthreads();
+  }
+  flush_box(asdp, TX + 6, TY + 6, lam_dp, g, k);
+  flush_box(aspt, TX + 6, TY + 6, lam_pt, g, k);
+  flush_box(asu, ALay::UW, ALay::UH, lam_u, g, k);
+  flush_box(asv, ALay::VW, ALay::VH, lam_v, g, k);
+}
+
+// The mass adjoint in one kernel (both branches, the update recomputed from
+// the fluxes), used on the C grid: there the halo-wide output range and the
+// C-grid winds each branch would recompute make two kernels slower.
+template <int TX, int TY, bool CGRID>
+struct MassAdj1L {
   using F = MassL<double, TX, TY, CGRID>;
   static constexpr int UW = CGRID ? TX + 2 : TX + 1, UH = CGRID ? TY + 7 : TY + 6;
   static constexpr int VW = CGRID ? TX + 7 : TX + 6, VH = CGRID ? TY + 2 : TY + 1;
@@ -383,7 +684,7 @@ struct MassAdjL {
 };
 
 template <int TX, int TY, bool CGRID>
-__global__ void __launch_bounds__(NTA, 3) k_mass_adj(const __grid_constant__ CUtensorMap m_dp,
+__global__ void __launch_bounds__(NTA, 3) k_mass_adj1(const __grid_constant__ CUtensorMap m_dp,
                                                  const __grid_constant__ CUtensorMap m_pt,
                                                  const __grid_constant__ CUtensorMap m_u,
                                                  const __grid_constant__ CUtensorMap m_v, Geom g, Consts c,
@@ -392,7 +693,7 @@ __global__ void __launch_bounds__(NTA, 3) k_mass_adj(const __grid_constant__ CUt
                                                  int hi, int* timeout) {
   using T = double;
   using Lay = MassL<T, TX, TY, CGRID>;
-  using ALay = MassAdjL<TX, TY, CGRID>;
+  using ALay = MassAdj1L<TX, TY, CGRID>;
   constexpr int V = CGRID ? PPM_UNC : PPM_NN;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;

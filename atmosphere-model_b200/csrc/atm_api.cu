@@ -851,7 +851,8 @@ int adj_c(atm_ctx* ctx, double dt_half, void* const* s, double* const* lin, cons
   }
   {
     Stage t(ctx, S_ACMASS);
-    CK(atm::adj_mass(g, k, sd[F_DP], sd[F_PT], sd[F_UD], sd[F_VD], ctx->lam_cg[C_DPC], ctx->lam_cg[C_PTC], lin[F_DP],
+    CK(atm::adj_mass(g, k, sd[F_DP], sd[F_PT], sd[F_UD], sd[F_VD], cg[C_DPC], cg[C_PTC], ctx->lam_cg[C_DPC],
+                     ctx->lam_cg[C_PTC], lin[F_DP],
                      lin[F_PT], lin[F_UD], lin[F_VD], -2, 2, &ctx->status->tma_timeout, true, ctx->stream));
   }
   return ATM_OK;
@@ -883,8 +884,9 @@ int adj_d(atm_ctx* ctx, double dt, const void* const* so, const void* const* sn,
     CK(atm::adj_column(g, k, n[F_DP], n[F_PT], ctx->lam_pk, ctx->lam_gz, lout[F_DP], lout[F_PT], -2, 2, ctx->stream));
   }
   {
-    Stage t(ctx, S_ADMASS);
-    CK(atm::adj_mass(g, k, o[F_DP], o[F_PT], cg[C_UC], cg[C_VC], lout[F_DP], lout[F_PT], lin[F_DP], lin[F_PT],
+    Stage t(ctx, S_ADMASS, 2);
+    CK(atm::adj_mass(g, k, o[F_DP], o[F_PT], cg[C_UC], cg[C_VC], n[F_DP], n[F_PT], lout[F_DP], lout[F_PT], lin[F_DP],
+                     lin[F_PT],
                      ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], -3, 3, &ctx->status->tma_timeout, false, ctx->stream));
   }
   {

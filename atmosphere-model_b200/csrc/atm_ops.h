@@ -61,9 +61,11 @@ cudaError_t device_div_check(unsigned long long n, unsigned long long seed, unsi
 // ---- FP64 adjoint (atm_adjoint.cu); lam_* are adjoint fields laid out like
 // the fields they belong to, accumulated with +=
 cudaError_t adj_setup();
+// dpo, pto: the new dp and pt the forward sweep wrote
 cudaError_t adj_mass(const Geom&, const Consts&, const double* dp, const double* pt, const double* u, const double* v,
-                     const double* lam_dpo, const double* lam_pto, double* lam_dp, double* lam_pt, double* lam_u,
-                     double* lam_v, int lo, int hi, int* timeout, bool cgrid, cudaStream_t);
+                     const double* dpo, const double* pto, const double* lam_dpo, const double* lam_pto, double* lam_dp,
+                     double* lam_pt, double* lam_u, double* lam_v, int lo, int hi, int* timeout, bool cgrid,
+                     cudaStream_t);
 cudaError_t adj_c_mom(const Geom&, const Consts&, const double* ud, const double* vd, const double* pkap,
                       const double* gz, const double* lam_uc, const double* lam_vc, double* lam_ud, double* lam_vd,
                       double* lam_pk, double* lam_gz, int* timeout, cudaStream_t);
