@@ -119,7 +119,7 @@ cudaError_t adj_column(const Geom& g, const Consts& c, const double* dp, const d
 cudaError_t adj_corners(const Geom& g, const double* lam_pkb, const double* lam_gzb, double* lam_pk, double* lam_gz,
                         cudaStream_t s) {
   const int n = (g.nx + 4) * (g.ny + 4);
-  k_corners_adj<<<(n + 255) / 256, 256, 0, s>>>(g, lam_pkb, lam_gzb, lam_pk, lam_gz);
+  k_corners_adj<<<dim3((n + 255) / 256, g.L), 256, 0, s>>>(g, lam_pkb, lam_gzb, lam_pk, lam_gz);
   return cudaGetLastError();
 }
 

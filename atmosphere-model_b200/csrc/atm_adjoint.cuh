@@ -1779,28 +1779,32 @@ __global__ void __launch_bounds__(128) k_column_adj(Geom g, Consts c, const doub
 // [-2, nx+1]^2 feeds: pkapb(l) -> pkap(l) and gzb(l+1) -> gz(l+1), l < nlay.
 __global__ void k_corners_adj(Geom g, const double* __restrict__ lam_pkb, const double* __restrict__ lam_gzb,
                               double* lam_pk, double* lam_gz) {
+  // one thread per point and level (blockIdx.y): the 16-point gathers of a
+  // block's row of points hit L1, and every level runs in parallel
   const int w = g.nx + 4, h = g.ny + 4;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= w * h) return;
   const int x = -2 + idx % w, y = -2 + idx / w;
+  const int l = blockIdx.y;
   const double a[4] = {-C1_12, C7_12, C7_12, -C1_12};
   const double b[4] = {-C1_32, C9_32, C9_32, -C1_32};
-  for (int l = 0; l < g.L; ++l) {
-    double sp = 0., sg = 0.;
-    for (int dy = -2; dy <= 1; ++dy) {
-      const int cy = y - dy;
-      if (cy < 0 || cy > g.ny) continue;
-      for (int dx = -2; dx <= 1; ++dx) {
-        const int cx = x - dx;
-        if (cx < 0 || cx > g.nx) continue;
-        const double wt = a[dx + 2] * b[dy + 2] + b[dx + 2] * a[dy + 2];
-        sp += wt * lam_pkb[g.at(cx, cy, l)];
-        sg += wt * lam_gzb[g.at(cx, cy, l + 1)];
-      }
+  const double* pkb = lam_pkb + (long long)l * g.S;
+  const double* gzb = lam_gzb + (long long)(l + 1) * g.S;
+  double sp = 0., sg = 0.;
+  for (int dy = -2; dy <= 1; ++dy) {
+    const int cy = y - dy;
+    if (cy < 0 || cy > g.ny) continue;
+    const long long row = g.at(0, cy);
+    for (int dx = -2; dx <= 1; ++dx) {
+      const int cx = x - dx;
+      if (cx < 0 || cx > g.nx) continue;
+      const double wt = a[dx + 2] * b[dy + 2] + b[dx + 2] * a[dy + 2];
+      sp += wt * pkb[row + cx];
+      sg += wt * gzb[row + cx];
     }
-    lam_pk[g.at(x, y, l)] += sp;
-    lam_gz[g.at(x, y, l + 1)] += sg;
   }
+  lam_pk[g.at(x, y, l)] += sp;
+  lam_gz[g.at(x, y, l + 1)] += sg;
 }
 
 // ======================================================= halo adjoints ====
