@@ -754,6 +754,20 @@ int atm_device_div_check(long long n, long long seed, long long* mismatches) {
   return rc;
 }
 
+int atm_device_wait_check(int max_polls, int* timed_out) {
+  if (max_polls <= 0 || max_polls > 100000 || !timed_out) return ATM_ERR_ARG;
+  int* d = nullptr;
+  if (cudaMalloc((void**)&d, 4) != cudaSuccess) return ATM_ERR_NOMEM;
+  int rc = ATM_OK;
+  int h = -1;
+  if (cudaMemset(d, 0xff, 4) != cudaSuccess || atm::device_wait_timeout(max_polls, d, 0) != cudaSuccess ||
+      cudaMemcpy(&h, d, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = ATM_ERR_CUDA;
+  cudaFree(d);
+  *timed_out = h;
+  return rc;
+}
+
 int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_out, int n) {
   if (n <= 0 || !x || !pow_out || !log_out) return ATM_ERR_ARG;
   double *dx = nullptr, *dp = nullptr, *dl = nullptr;

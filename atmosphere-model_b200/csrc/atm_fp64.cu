@@ -51,6 +51,26 @@ cudaError_t device_div_check(unsigned long long n, unsigned long long seed, unsi
   return cudaGetLastError();
 }
 
+// The bounded wait of the TMA loads, made to run out: one thread arms an
+// mbarrier for 16 bytes of transactions that no copy ever brings (no copy
+// is issued) and waits on it with mbar_wait's poll limit, as tma_fetch
+// does; it must come back with the failure recorded in *flag.
+static __global__ void k_wait_timeout(int max_polls, int* flag) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    mbar_expect_tx(&bar, 16);
+    const bool ok = mbar_wait(&bar, 0, max_polls);
+    *flag = ok ? 0 : 1;
+  }
+}
+
+cudaError_t device_wait_timeout(int max_polls, int* flag, cudaStream_t s) {
+  k_wait_timeout<<<1, 32, 0, s>>>(max_polls, flag);
+  return cudaGetLastError();
+}
+
 cudaError_t device_pow_log(const double* x, double y, double* p, double* l, int n, cudaStream_t s) {
   k_pow_log<<<(n + 255) / 256, 256, 0, s>>>(x, y, p, l, n);
   return cudaGetLastError();

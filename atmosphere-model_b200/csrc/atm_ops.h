@@ -57,6 +57,8 @@ cudaError_t device_pow_log(const double* x, double y, double* p, double* l, int 
 
 // count of arguments where div_const<3>/<12> differs from IEEE division (tests)
 cudaError_t device_div_check(unsigned long long n, unsigned long long seed, unsigned long long* bad, cudaStream_t);
+// the TMA loads' bounded mbarrier wait on a barrier nothing completes: *flag = 1 when it gave up
+cudaError_t device_wait_timeout(int max_polls, int* flag, cudaStream_t);
 
 // ---- FP64 adjoint (atm_adjoint.cu); lam_* are adjoint fields laid out like
 // the fields they belong to, accumulated with +=

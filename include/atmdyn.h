@@ -203,6 +203,13 @@ int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, const double* 
    integers) for which the FP64 form's FMA-corrected division by the
    constants 3 and 12 differs from IEEE division (expected: 0) */
 int atm_device_div_check(long long n, long long seed, long long* mismatches);
+/* failure-detection check of the tile kernels' bounded wait: a kernel arms
+   an mbarrier for transactions that never arrive (no copy is issued) and
+   waits with the poll limit the TMA loads use, here max_polls polls of at
+   most ~1 us (1..100000); *timed_out = 1 when the wait gave up and the
+   kernel returned, as a tile kernel then does (it records
+   Status.tma_timeout, which atm_check_stability reports as an error). */
+int atm_device_wait_check(int max_polls, int* timed_out);
 
 /* ---- adjoint of the FP64 step (the gradient work; no reference counterpart) ----
    Hand-written reverse mode of cgrid_dynamics_step, dgrid_dynamics_step

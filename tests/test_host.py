@@ -34,6 +34,10 @@ def test_create_rejects_bad_arguments_without_touching_the_gpu():
         rc = lib.atm_create(ctypes.byref(ctx), nx, ny, nl, 1e3, 1e3, ak.ctypes.data_as(P), bk.ctypes.data_as(P),
                             9.8, 1e-4, 0.1, 0.0, prec, 0)
         assert rc == 1
+    # the wait check's poll limit is bounded before any launch
+    t = ctypes.c_int(-1)
+    for polls in (0, -5, 100001):
+        assert lib.atm_device_wait_check(polls, ctypes.byref(t)) == 1 and t.value == -1
 
 
 def test_schedule_matches_calculate_dt():
