@@ -316,8 +316,8 @@ def run_ours(args):
                      'traffic': (TRAFFIC_PER_CELL_FP64[dom_name] * cells if dom_name in TRAFFIC_PER_CELL_FP64
                                  else None),
                      'traffic_unit': 'bytes per launch (ncu DRAM read + write per cell, scaled by cells)',
-                     'note': 'the FP64 sweeps are bound by FP64 instruction issue, not HBM (ncu: 60 % issue, '
-                             '29 % FP64 pipe, DRAM traffic = algorithmic bytes)'},
+                     'note': 'the FP64 sweeps are bound by instruction issue, not HBM (ncu: issue 54-68 %, '
+                             'FP64 pipe 32-44 %, DRAM traffic = algorithmic bytes)'},
         'e2e': f64.get('e2e'),
         'e2e_resident': f64.get('e2e_resident'),
         'gpu_launches': f64['gpu_launches'],
