@@ -530,8 +530,14 @@ def adjoint_leg(args, torch, max_over_ranks, world):
                 ad = torch.dot(grad, d).item()
                 fd.append({'eps': eps, 'adjoint': ad, 'central_difference': fdv,
                            'rel_diff': abs(fdv - ad) / max(abs(ad), 1e-300)})
-        return {'directions_per_eps': 8,
+        gnorm = float(grad.norm().item())
+        # |FD - AD| / |grad J| for unit directions: the error on the scale of
+        # the gradient (a direction with a small derivative inflates rel_diff)
+        return {'directions_per_eps': 8, 'grad_norm': gnorm,
                 'max_rel_diff': {str(e): max(f['rel_diff'] for f in fd if f['eps'] == e) for e in eps_list},
+                'max_abs_diff_over_grad_norm': {str(e): max(abs(f['central_difference'] - f['adjoint'])
+                                                            for f in fd if f['eps'] == e) / gnorm
+                                                for e in eps_list},
                 'per_direction': fd}
 
     st4 = ic.config(4)
