@@ -8,10 +8,10 @@ idle.  :class:`Ensemble` therefore
 * spreads the members over several CUDA streams, balanced by cell count
   (longest-processing-time first), so kernels of different members run
   concurrently on the 148 SMs;
-* captures one remap cycle of every member (``remap_every`` steps, the
-  remap on the last) into a single CUDA graph: the forks and joins across
-  the streams become graph edges, and advancing the whole ensemble by a
-  cycle is one graph launch.
+* captures remap cycles of every member (``remap_every`` steps, the remap
+  on the last; one cycle up to a whole run) into a single CUDA graph: the
+  forks and joins across the streams become graph edges, and advancing the
+  whole ensemble by the captured steps is one graph launch.
 
 Every member is a full :class:`Dycore` (FP64 or mixed form) whose kernels
 are those of a single domain; the graph changes only how they are launched,
@@ -70,16 +70,19 @@ class Ensemble:
             for st, d in zip(self.members, self.dyn):
                 d.step(st.dt, remap=self.steps_done % st.remap_every == 0, check_stable=False)
 
-    def capture(self, remap_every: int):
+    def capture(self, remap_every: int, cycles: int | None = None):
         """Capture remap cycles of every member into one CUDA graph (the
         members must share remap_every, and capture starts right after a
         remap).  A step and a remap each swap a member's two time levels;
-        the graph holds an even number of swaps (one cycle when
-        remap_every is odd, two otherwise) so that each replay starts from
-        the buffers the capture started from."""
+        the graph holds an even number of swaps (cycles defaults to one
+        cycle when remap_every is odd, two otherwise, and must be even when
+        remap_every is even) so that each replay starts from the buffers
+        the capture started from."""
         assert all(st.remap_every == remap_every for st in self.members)
         assert self.steps_done % remap_every == 0
-        cycles = 1 if (remap_every + 1) % 2 == 0 else 2
+        unit = 1 if (remap_every + 1) % 2 == 0 else 2
+        cycles = unit if cycles is None else cycles
+        assert cycles >= 1 and cycles % unit == 0
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         cap = torch.cuda.Stream()

@@ -980,8 +980,15 @@ __global__ void __launch_bounds__(NTA, 3) k_mass_adj1(const __grid_constant__ CU
 template <int TX, int TY>
 struct CMomAdjL {
   using F = CMomL<double, TX, TY>;
+  // the forward values the reverse reads (the layer-nlay A-grid winds are
+  // recomputed where the reverse reads them; ke and lap are not needed)
+  static constexpr size_t fwd = 2 * box_bytes<double>(TX + 6, TY + 6) +                       // uc1, vc1
+                                box_bytes<double>(TX + 5, TY + 5) +                           // vor
+                                box_bytes<double>(TX, TY + 5) + box_bytes<double>(TX + 5, TY) +  // tU, tV
+                                box_bytes<double>(TX + 1, TY + 4) + box_bytes<double>(TX + 4, TY + 1) +  // mvy, mux
+                                box_bytes<double>(TX, TY + 3) + box_bytes<double>(TX + 3, TY);  // mtU, mtV
   static constexpr size_t lam =
-      2 * box_bytes<double>(TX + 6, TY + 6) +                                          // uc1, vc1
+      2 * box_bytes<double>(TX + 6, TY + 6) + 2 * box_bytes<double>(TX + 1, TY + 1) +  // uc1, vc1, uaL, vaL
       box_bytes<double>(TX + 5, TY + 5) + box_bytes<double>(TX + 1, TY + 1) +          // vor, ke
       box_bytes<double>(TX, TY + 5) + box_bytes<double>(TX + 5, TY) +                  // tU, tV
       box_bytes<double>(TX + 1, TY + 1) +                                              // lap
@@ -989,25 +996,9 @@ struct CMomAdjL {
       box_bytes<double>(TX, TY + 3) + box_bytes<double>(TX + 3, TY) +                  // mtU, mtV
       2 * box_bytes<double>(TX + 7, TY + 7) + 2 * box_bytes<double>(TX + 3, TY + 3) +  // ud, vd (k, nlay)
       4 * box_bytes<double>(TX + 1, TY + 1);                                           // pkap, gz (k, k+1)
-  // the forward's ke and lap values are not needed by the reverse, and
-  // the layer-nlay A-grid winds are recomputed where the reverse reads them
-  static constexpr size_t bytes = F::bytes - 2 * box_bytes<double>(TX + 1, TY + 1) + lam;
+  static constexpr size_t bytes = F::boxes + fwd + lam + 128;
 };
 
-// The layer-nlay A-grid winds at (x, y) from the layer-nlay D-grid winds
-// (src/mod_sw_dyn.f90:119-125), the operations of k_c_mom2.
-struct ALWinds {
-  double ua, va;
-};
-__device__ __forceinline__ ALWinds al_winds(const Sm<double>& udL, const Sm<double>& vdL, int x, int y) {
-  using T = double;
-  T ub = T(.5) * (udL(x, y) + udL(x - 1, y));
-  T ucl = T(.5) * (ub + T(.5) * (udL(x, y + 1) + udL(x - 1, y + 1)));
-  T vb = T(.5) * (vdL(x, y) + vdL(x, y - 1));
-  T vcl = T(.5) * (vb + T(.5) * (vdL(x + 1, y) + vdL(x + 1, y - 1)));
-  return ALWinds{T(.5) * (ucl + T(.25) * (udL(x + 1, y) + udL(x, y) + udL(x + 1, y + 1) + udL(x, y + 1))),
-                 T(.5) * (vcl + T(.25) * (vdL(x, y + 1) + vdL(x, y) + vdL(x + 1, y + 1) + vdL(x + 1, y)))};
-}
 
 // 3 CTAs per SM: shared memory (the layout above) and 85 registers a thread
 template <int TX, int TY>
@@ -1187,8 +1178,8 @@ __global__ void __launch_bounds__(NTA, 3) k_c_mom_adj(const __grid_constant__ CU
   aregion<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
     const double l = ake(x, y);
     if (l == 0.) return;
-    const ALWinds aw = al_winds(udL, vdL, x, y);
-    const T va = aw.va, ua = aw.ua;
+    T ua, va;
+    al_winds<T>(udL, vdL, x, y, ua, va);
     double lcy = 0., lcx = 0.;
     double fy = flux_unc_adj(vc1.ptr(x, y + 1), TX + 6, mvy.ptr(x, y + 1), TX + 1, dtdy * va, .5 * va * l,
                                       avc1.ptr(x, y + 1), TX + 6, amvy.ptr(x, y + 1), TX + 1, lcy);

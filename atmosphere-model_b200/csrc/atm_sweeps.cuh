@@ -376,13 +376,28 @@ struct CMomL {
       (uint32_t)((WU * HU + WV * HV + 2 * WL * HL) * sizeof(S) + 4 * WP * HP * sizeof(double));
   static constexpr size_t boxes = tma_box_bytes(WU, HU, sizeof(S)) + tma_box_bytes(WV, HV, sizeof(S)) +
                                   2 * tma_box_bytes(WL, HL, sizeof(S)) + 4 * tma_box_bytes(WP, HP, 8);
-  static constexpr size_t work = 2 * box_bytes<T>(TX + 6, TY + 6) + 2 * box_bytes<T>(TX + 1, TY + 1) +
-                                 box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 1, TY + 1) +
-                                 box_bytes<T>(TX, TY + 5) + box_bytes<T>(TX + 5, TY) + box_bytes<T>(TX + 1, TY + 1) +
-                                 box_bytes<T>(TX + 1, TY + 4) + box_bytes<T>(TX + 4, TY + 1) +
-                                 box_bytes<T>(TX, TY + 3) + box_bytes<T>(TX + 3, TY);
+  // slopes of the KE sweeps, later of the vorticity-flux sweeps (one buffer)
+  static constexpr size_t slopes_ke = box_bytes<T>(TX + 1, TY + 4) + box_bytes<T>(TX + 4, TY + 1);
+  static constexpr size_t slopes_vf = box_bytes<T>(TX, TY + 3) + box_bytes<T>(TX + 3, TY);
+  static constexpr size_t slopes = slopes_ke > slopes_vf ? slopes_ke : slopes_vf;
+  static constexpr size_t work = 2 * box_bytes<T>(TX + 6, TY + 6) +                  // uc1, vc1
+                                 box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 1, TY + 1) +  // vor, ke
+                                 box_bytes<T>(TX, TY + 5) + box_bytes<T>(TX + 5, TY) +  // tU, tV
+                                 box_bytes<T>(TX + 1, TY + 1) + slopes;               // lap, slopes
   static constexpr size_t bytes = boxes + work + 128;
 };
+
+// The layer-nlay A-grid winds at (x, y) from the layer-nlay D-grid winds
+// (src/mod_sw_dyn.f90:110-125 at k = nlay), recomputed where they are read.
+template <typename T, typename A>
+__device__ __forceinline__ void al_winds(const A& udL, const A& vdL, int x, int y, T& ua, T& va) {
+  T ub = T(.5) * (udL(x, y) + udL(x - 1, y));
+  T ucl = T(.5) * (ub + T(.5) * (udL(x, y + 1) + udL(x - 1, y + 1)));
+  ua = T(.5) * (ucl + T(.25) * (udL(x + 1, y) + udL(x, y) + udL(x + 1, y + 1) + udL(x, y + 1)));
+  T vb = T(.5) * (vdL(x, y) + vdL(x, y - 1));
+  T vcl = T(.5) * (vb + T(.5) * (vdL(x + 1, y) + vdL(x + 1, y - 1)));
+  va = T(.5) * (vcl + T(.25) * (vdL(x, y + 1) + vdL(x, y) + vdL(x + 1, y + 1) + vdL(x + 1, y)));
+}
 
 template <typename T, int TX, int TY, typename S = T, typename C = T>
 __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorMap m_ud,
@@ -430,34 +445,28 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
   }
   Sm<T> uc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
   Sm<T> vc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
-  Sm<T> uaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
-  Sm<T> vaL = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
   Sm<T> vor = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
   Sm<T> ke = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
   Sm<T> tU = carve<T>(p, ox, oy - 2, TX, TY + 5);
   Sm<T> tV = carve<T>(p, ox - 2, oy, TX + 5, TY);
   Sm<T> lap = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> mvy = carve<T>(p, ox - 1, oy - 2, TX + 1, TY + 4);  // slopes of vc1 along y
-  Sm<T> mux = carve<T>(p, ox - 2, oy - 1, TX + 4, TY + 1);  // slopes of uc1 along x
-  Sm<T> mtU = carve<T>(p, ox, oy - 1, TX, TY + 3);          // slopes of tU along y
-  Sm<T> mtV = carve<T>(p, ox - 1, oy, TX + 3, TY);          // slopes of tV along x
+  // the KE sweeps' slopes are dead before the vorticity-flux sweeps' ones
+  // are written (a __syncthreads apart): they share memory
+  unsigned char* ps = p;
+  Sm<T> mvy = carve<T>(ps, ox - 1, oy - 2, TX + 1, TY + 4);  // slopes of vc1 along y
+  Sm<T> mux = carve<T>(ps, ox - 2, oy - 1, TX + 4, TY + 1);  // slopes of uc1 along x
+  ps = p;
+  Sm<T> mtU = carve<T>(ps, ox, oy - 1, TX, TY + 3);          // slopes of tU along y
+  Sm<T> mtV = carve<T>(ps, ox - 1, oy, TX + 3, TY);          // slopes of tV along x
+  p += Lay::slopes;
 
   // C-grid winds of this layer (first-loop values, mod_sw_dyn.f90:110-117)
-  // and A-grid winds of layer nlay (mod_sw_dyn.f90:110-125 at k = nlay)
-  regions(reg<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
+  region<TX + 6, TY + 6>(ox - 3, oy - 3, [&](int x, int y) {
     T ub = T(.5) * (sud(x, y) + sud(x - 1, y));
     uc1(x, y) = T(.5) * (ub + T(.5) * (sud(x, y + 1) + sud(x - 1, y + 1)));
     T vb = T(.5) * (svd(x, y) + svd(x, y - 1));
     vc1(x, y) = T(.5) * (vb + T(.5) * (svd(x + 1, y) + svd(x + 1, y - 1)));
-  }),
-          reg<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
-    T ub = T(.5) * (udL(x, y) + udL(x - 1, y));
-    T ucl = T(.5) * (ub + T(.5) * (udL(x, y + 1) + udL(x - 1, y + 1)));
-    uaL(x, y) = T(.5) * (ucl + T(.25) * (udL(x + 1, y) + udL(x, y) + udL(x + 1, y + 1) + udL(x, y + 1)));
-    T vb = T(.5) * (vdL(x, y) + vdL(x, y - 1));
-    T vcl = T(.5) * (vb + T(.5) * (vdL(x + 1, y) + vdL(x + 1, y - 1)));
-    vaL(x, y) = T(.5) * (vcl + T(.25) * (vdL(x, y + 1) + vdL(x, y) + vdL(x + 1, y + 1) + vdL(x + 1, y)));
-  }));
+  });
   __syncthreads();
 
   const T f = T(c.coriolis);
@@ -473,10 +482,12 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
   // advection: inner sweeps and Laplacian (:344-367, 388-397)
   const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
   regions(reg<TX + 1, TY + 1>(ox - 1, oy - 1, [&](int x, int y) {
-    T fy = flux_pre<T, PPM_UNC>(vc1.ptr(x, y + 1), TX + 6, mvy.ptr(x, y + 1), TX + 1, dtdy * vaL(x, y));
-    T kv = vaL(x, y) * fy;
-    T fx = flux_pre<T, PPM_UNC>(uc1.ptr(x + 1, y), 1, mux.ptr(x + 1, y), 1, dtdx * uaL(x, y));
-    ke(x, y) = T(.5) * (kv + uaL(x, y) * fx);
+    T ua, va;  // A-grid winds of layer nlay (mod_sw_dyn.f90:110-125 at k = nlay)
+    al_winds<T>(udL, vdL, x, y, ua, va);
+    T fy = flux_pre<T, PPM_UNC>(vc1.ptr(x, y + 1), TX + 6, mvy.ptr(x, y + 1), TX + 1, dtdy * va);
+    T kv = va * fy;
+    T fx = flux_pre<T, PPM_UNC>(uc1.ptr(x + 1, y), 1, mux.ptr(x + 1, y), 1, dtdx * ua);
+    ke(x, y) = T(.5) * (kv + ua * fx);
   }),
           reg<TX, TY + 5>(ox, oy - 2, [&](int x, int y) {
     T c0 = dtdx * sud(x - 1, y), c1 = dtdx * sud(x, y);

@@ -39,3 +39,21 @@ def test_graph_replay_matches_eager(precision):
     assert a.stable() and b.stable()
     a.close()
     b.close()
+
+
+def test_whole_run_as_one_graph_matches_eager():
+    """Four remap cycles (20 steps) captured as one graph and replayed as
+    one launch."""
+    a = Ensemble(members(), 'mixed', nstreams=3)
+    b = Ensemble(members(), 'mixed', nstreams=3)
+    a.step_eager(25)
+    b.step_eager(5)
+    b.capture(5, cycles=4)
+    assert b.cycle == 20
+    b.replay(1)
+    torch.cuda.synchronize()
+    for da, db in zip(a.dyn, b.dyn):
+        for f in ('dp', 'pt', 'ud', 'vd'):
+            np.testing.assert_array_equal(da.get(f, halo=True), db.get(f, halo=True))
+    a.close()
+    b.close()
