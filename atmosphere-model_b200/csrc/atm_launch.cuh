@@ -15,12 +15,13 @@ using T = ATM_FORM_T;  // sweep arithmetic
 using S = double;      // prognostic state (dp, pt, ud, vd), both forms
 using C = T;           // C-grid fields (dpc, ptc, uc, vc)
 // Tile of each sweep kernel (TX x TY_*), measured per kernel and form on
-// B200 at 1024x1024x64 (32x4, 32x8, 32x16 and 64x8 tried): smaller tiles
-// hold more CTAs per SM, taller ones recompute less halo.
+// B200 at 1024x1024x64 (heights 3 to 16 and 64x8 tried, with the CTAs per
+// SM each layout's register budget is set for): smaller tiles hold more
+// CTAs per SM, taller ones recompute less halo.
 constexpr bool FP64_FORM = std::is_same_v<T, double>;
 constexpr int TX = 32;
 constexpr int TY_CMASS = FP64_FORM ? 4 : 16;
-constexpr int TY_DMASS = FP64_FORM ? 8 : 16;
+constexpr int TY_DMASS = FP64_FORM ? 6 : 16;
 constexpr int TY_CMOM = 8;
 constexpr int TY_DMOM = 4;
 

@@ -184,10 +184,14 @@ struct MassL {
       2 * box_bytes<T>(TX + 4, TY) + 2 * box_bytes<T>(TX, TY + 4) +               // slopes
       2 * box_bytes<T>(TX + 1, TY) + 2 * box_bytes<T>(TX, TY + 1);                // fluxes
   static constexpr size_t bytes = boxes + work + 128;
+  // CTAs per SM the register budget is set for (measured): FP64 C grid 6
+  // on 32 x 4 tiles (40 registers), FP64 D grid 5 on 32 x 6 tiles (48
+  // registers); the FP32 sweeps keep the compiler's choice
+  static constexpr int min_blocks = !std::is_same_v<T, double> ? 1 : CGRID ? 6 : 5;
 };
 
 template <typename T, int TX, int TY, bool CGRID, typename S = T, typename C = T>
-__global__ void __launch_bounds__(NT) k_mass2(const __grid_constant__ CUtensorMap m_dp,
+__global__ void __launch_bounds__(NT, MassL<T, TX, TY, CGRID, S, C>::min_blocks) k_mass2(const __grid_constant__ CUtensorMap m_dp,
                                               const __grid_constant__ CUtensorMap m_pt,
                                               const __grid_constant__ CUtensorMap m_u,
                                               const __grid_constant__ CUtensorMap m_v, Geom g, Consts c,
