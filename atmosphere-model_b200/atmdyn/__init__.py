@@ -9,6 +9,6 @@ conditions (:mod:`atmdyn.ic`) and the namelist reader (:mod:`atmdyn.namelist`).
 """
 from . import ic, model  # noqa: F401
 from ._lib import AtmError, load, build  # noqa: F401
-from .dycore import Dycore, device_pow_log, subtiles  # noqa: F401
+from .dycore import Dycore, device_pow_log  # noqa: F401
 
 __version__ = '0.1'

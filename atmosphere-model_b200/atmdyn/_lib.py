@@ -34,7 +34,7 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_adj_dgrid_step', 'atm_adj_remap', 'atm_state_bytes', 'atm_state_save', 'atm_state_load',
            'atm_tape_bytes', 'atm_step_tape', 'atm_adj_step_tape', 'atm_output_enable', 'atm_output_reset',
            'atm_accumulate_output', 'atm_output_read', 'atm_output_time', 'atm_physics_tendencies',
-           'atm_apply_physics', 'atm_physics_halo', 'atm_device_wait_check', 'atm_set_subtiles')
+           'atm_apply_physics', 'atm_physics_halo', 'atm_device_wait_check')
 ATM_ADJ_IN, ATM_ADJ_OUT = 0, 1
 
 # the entry points every build must export
@@ -120,7 +120,6 @@ def load():
         'atm_apply_physics': ([vp, d], None),
         'atm_physics_halo': ([vp], None),
         'atm_device_wait_check': ([i, ctypes.POINTER(i)], None),
-        'atm_set_subtiles': ([i], None),
     }
     for f, (args, res) in optional.items():
         if hasattr(lib, f):

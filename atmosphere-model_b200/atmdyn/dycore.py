@@ -10,7 +10,6 @@ memory layout of the reference's Fortran arrays.
 """
 from __future__ import annotations
 
-import contextlib
 import ctypes
 import numpy as np
 
@@ -302,18 +301,6 @@ class Dycore:
 
     def state_load(self, ptr):
         check(self.lib.atm_state_load(self.ctx, ctypes.c_void_p(ptr)), self.ctx, 'atm_state_load')
-
-
-@contextlib.contextmanager
-def subtiles(n: int):
-    """Within the block, the strip kernels march through n sub-tiles per
-    block (0 = the library's choice, restored on exit); atm_set_subtiles."""
-    lib = _lib.load()
-    check(lib.atm_set_subtiles(int(n)), None, 'atm_set_subtiles')
-    try:
-        yield
-    finally:
-        check(lib.atm_set_subtiles(0), None, 'atm_set_subtiles')
 
 
 def device_pow_log(x, y):

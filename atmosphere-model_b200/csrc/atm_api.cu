@@ -251,10 +251,6 @@ int require_init(atm_ctx* c) {
 
 }  // namespace
 
-namespace atm {
-int subtiles_override = 0;
-}
-
 extern "C" {
 
 const char* atm_version(void) { return "libatmdyn 0.1 (sm_100a)"; }
@@ -730,12 +726,6 @@ int atm_profile_read(atm_ctx* ctx, double* ms, int* count, int nstage) {
 }
 
 const char* atm_profile_stage(int i) { return (i >= 0 && i < NSTAGE) ? STAGE_NAMES[i] : nullptr; }
-
-int atm_set_subtiles(int n) {
-  if (n < 0 || n > 64) return ATM_ERR_ARG;
-  atm::subtiles_override = n;
-  return ATM_OK;
-}
 
 int atm_launch_count(atm_ctx* ctx, long long* n) {
   if (!ctx || !n) return ATM_ERR_ARG;

@@ -3,8 +3,6 @@
 // (T = float), which each define ATM_FORM_T and ATM_OPS_NAME.
 #pragma once
 
-#include <algorithm>
-
 #include "atm_kernels.cuh"
 #include "atm_ops.h"
 #include "atm_sweeps.cuh"
@@ -32,24 +30,6 @@ inline dim3 tiles(int lo, int hi, const Geom& g, int layers, int ty) {
   return dim3((w + TX - 1) / TX, (h + ty - 1) / ty, layers);
 }
 
-// Blocks of a strip kernel (one block marches through nsub sub-tiles in y):
-// nsub is as large as keeps about four waves of blocks on the device's SMs,
-// at most 8 (beyond that the rows a strip's first sub-tile adds are under
-// 1/8 of its work), and 1 on small domains; atm_set_subtiles fixes it.
-inline dim3 strips(int lo, int hi, const Geom& g, int layers, int ty, int& nsub) {
-  static const int sms = [] {
-    int dev = 0, n = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    return n;
-  }();
-  dim3 t = tiles(lo, hi, g, layers, ty);
-  const long long blocks = (long long)t.x * t.y * t.z, waves = 4LL * sms * 8;
-  nsub = subtiles_override > 0 ? subtiles_override
-                               : (int)std::min<long long>(8, std::max<long long>(1, blocks / waves));
-  t.y = (t.y + nsub - 1) / nsub;
-  return t;
-}
-
 template <typename K>
 cudaError_t smem_attr(K kernel, size_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -74,26 +54,24 @@ cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt,
   cudaError_t e;
   if (cgrid) {  // state in, C-grid fields out
     using Lay = MassL<T, TX, TY_CMASS, true, S, C>;
-    int nsub;
-    dim3 grid = strips(lo, hi, g, g.L, TY_CMASS, nsub);
+    dim3 grid = tiles(lo, hi, g, g.L, TY_CMASS);
     constexpr int eu = sizeof(typename Lay::UB);
     if ((e = tmap(dp, sizeof(S), g, g.L, Lay::WD, Lay::HD, &md)) ||
         (e = tmap(pt, sizeof(S), g, g.L, Lay::WD, Lay::HD, &mp)) || (e = tmap(u, eu, g, g.L, Lay::WU, Lay::HU, &mu)) ||
         (e = tmap(v, eu, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
     k_mass2<T, TX, TY_CMASS, true, S, C><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (C*)dpo,
-                                                                       (C*)pto, lo, hi, nsub, nonfinite, timeout);
+                                                                       (C*)pto, lo, hi, nonfinite, timeout);
   } else {  // state and C-grid winds in, state out
     using Lay = MassL<T, TX, TY_DMASS, false, S, C>;
-    int nsub;
-    dim3 grid = strips(lo, hi, g, g.L, TY_DMASS, nsub);
+    dim3 grid = tiles(lo, hi, g, g.L, TY_DMASS);
     constexpr int eu = sizeof(typename Lay::UB);
     if ((e = tmap(dp, sizeof(S), g, g.L, Lay::WD, Lay::HD, &md)) ||
         (e = tmap(pt, sizeof(S), g, g.L, Lay::WD, Lay::HD, &mp)) || (e = tmap(u, eu, g, g.L, Lay::WU, Lay::HU, &mu)) ||
         (e = tmap(v, eu, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
     k_mass2<T, TX, TY_DMASS, false, S, C><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (S*)dpo,
-                                                                        (S*)pto, lo, hi, nsub, nonfinite, timeout);
+                                                                        (S*)pto, lo, hi, nonfinite, timeout);
   }
   return cudaGetLastError();
 }

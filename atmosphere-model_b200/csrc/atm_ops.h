@@ -59,9 +59,6 @@ cudaError_t device_pow_log(const double* x, double y, double* p, double* l, int 
 cudaError_t device_div_check(unsigned long long n, unsigned long long seed, unsigned long long* bad, cudaStream_t);
 // the TMA loads' bounded mbarrier wait on a barrier nothing completes: *flag = 1 when it gave up
 cudaError_t device_wait_timeout(int max_polls, int* flag, cudaStream_t);
-// Sub-tiles per block of the strip kernels when positive (atm_set_subtiles);
-// 0 chooses from the grid.
-extern int subtiles_override;
 
 // ---- FP64 adjoint (atm_adjoint.cu); lam_* are adjoint fields laid out like
 // the fields they belong to, accumulated with +=

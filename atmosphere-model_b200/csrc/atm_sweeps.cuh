@@ -119,8 +119,6 @@ struct Reg {
   static constexpr int N = W * Hh;
   int x0, y0;
   F body;
-  __host__ __device__ static constexpr int size() { return N; }
-  __device__ __forceinline__ static int start() { return threadIdx.x; }
   __device__ __forceinline__ void at(int idx) const {
     const int y = idx / W;
     body(x0 + idx - y * W, y0 + y);
@@ -130,43 +128,14 @@ template <int W, int Hh, typename F>
 __device__ __forceinline__ Reg<W, Hh, F> reg(int x0, int y0, F body) {
   return Reg<W, Hh, F>{x0, y0, body};
 }
-// The thread's index, read anew at every call: a loop over sub-tiles then
-// recomputes each thread's points per stage instead of keeping them all
-// live across the loop.
-__device__ __forceinline__ int tid_fresh() {
-  int t;
-  asm volatile("mov.u32 %0, %%tid.x;" : "=r"(t));
-  return t;
-}
-// A region of W columns and a run-time number of rows h (used by the strip
-// kernels).
-template <int W, typename F>
-struct RowReg {
-  int x0, y0, n;
-  F body;
-  __device__ __forceinline__ int size() const { return n; }
-  __device__ __forceinline__ static int start() { return tid_fresh(); }
-  __device__ __forceinline__ void at(int idx) const {
-    const int y = idx / W;
-    body(x0 + idx - y * W, y0 + y);
-  }
-};
-template <int W, typename F>
-__device__ __forceinline__ RowReg<W, F> reg(int x0, int y0, int h, F body) {
-  return RowReg<W, F>{x0, y0, W * h, body};
-}
 template <typename R0, typename... Rs>
 __device__ __forceinline__ void reg_dispatch(int idx, const R0& r0, const Rs&... rs) {
-  if (idx < r0.size()) r0.at(idx);
-  else if constexpr (sizeof...(Rs) > 0) reg_dispatch(idx - r0.size(), rs...);
+  if (idx < R0::N) r0.at(idx);
+  else if constexpr (sizeof...(Rs) > 0) reg_dispatch(idx - R0::N, rs...);
 }
 template <typename R>
 __device__ __forceinline__ void reg_loop(const R& r) {
-  for (int idx = r.start(); idx < r.size(); idx += NT) r.at(idx);
-}
-template <typename R0, typename... Rs>
-__device__ __forceinline__ const R0& first_of(const R0& r0, const Rs&...) {
-  return r0;
+  for (int idx = threadIdx.x; idx < R::N; idx += NT) r.at(idx);
 }
 // MERGE = false runs the regions one after the other (separate loops), the
 // better schedule where the merged dispatch costs more registers than the
@@ -174,75 +143,11 @@ __device__ __forceinline__ const R0& first_of(const R0& r0, const Rs&...) {
 template <bool MERGE = true, typename... Rs>
 __device__ __forceinline__ void regions(const Rs&... rs) {
   if constexpr (MERGE) {
-    const int N = (rs.size() + ...);
-    for (int idx = first_of(rs...).start(); idx < N; idx += NT) reg_dispatch(idx, rs...);
+    constexpr int N = (Rs::N + ...);
+    for (int idx = threadIdx.x; idx < N; idx += NT) reg_dispatch(idx, rs...);
   } else {
     (reg_loop(rs), ...);
   }
-}
-
-// ------------------------------------------------------ strips of tiles ----
-// A block that marches through a strip of sub-tiles in y keeps, in every
-// intermediate box that a later stage reads with a y halo, the rows that
-// the next sub-tile shares with this one, instead of recomputing them.  A
-// box of a stage whose rows are [oy + a, oy + TY + b) on the sub-tile at oy
-// computes them all on the strip's first sub-tile and only the TY new rows
-// [oy + b, oy + TY + b) on the others; between sub-tiles its last b - a rows
-// move to the top (Roll).  The values are those a fresh tile computes: each
-// row is a function of the same inputs.
-struct Rows {
-  int y0, h;
-};
-template <int TYS>
-__device__ __forceinline__ Rows rows_of(int oy, bool first, int a, int b) {
-  return first ? Rows{oy + a, TYS + b - a} : Rows{oy + b, TYS};
-}
-// rows [TYS, TYS + K) of a box of pitch W move to rows [0, K), in passes of
-// at most TYS rows (pass q: rows TYS + q*TYS .. to q*TYS ..), so that a
-// pass's source and destination rows never overlap
-template <int W, int K, int TYS, typename T>
-struct Roll {
-  static constexpr int PASSES = (K + TYS - 1) / TYS, SHIFT = W * TYS;
-  T* p;
-  __host__ __device__ static constexpr int off(int q) { return q * W * TYS; }
-  __host__ __device__ static constexpr int n(int q) {
-    return q < PASSES ? W * ((K - q * TYS) < TYS ? (K - q * TYS) : TYS) : 0;
-  }
-};
-template <int K, int TYS, int W, typename T>
-__device__ __forceinline__ Roll<W, K, TYS, T> roll(const Sm<T>& s) {
-  return Roll<W, K, TYS, T>{s.p};
-}
-template <int Q, typename R0, typename... Rs>
-__device__ __forceinline__ void roll_elem(int idx, const R0& r0, const Rs&... rs) {
-  constexpr int n0 = R0::n(Q);
-  if (idx < n0) {
-    const int d = R0::off(Q) + idx;
-    r0.p[d] = r0.p[d + R0::SHIFT];
-  } else if constexpr (sizeof...(Rs) > 0) {
-    roll_elem<Q>(idx - n0, rs...);
-  }
-}
-template <int Q, int QN, typename... Rs>
-__device__ __forceinline__ void roll_pass(const Rs&... rs) {
-  if constexpr (Q < QN) {
-    if constexpr (Q > 0) __syncthreads();
-    constexpr int N = (Rs::n(Q) + ...);
-    for (int idx = tid_fresh(); idx < N; idx += NT) roll_elem<Q>(idx, rs...);
-    roll_pass<Q + 1, QN>(rs...);
-  }
-}
-template <typename... Rs>
-__host__ __device__ constexpr int max_passes() {
-  int m = 0;
-  ((m = Rs::PASSES > m ? Rs::PASSES : m), ...);
-  return m;
-}
-// The caller synchronises the block before (last reads of the boxes) and
-// after (first writes of the next sub-tile).
-template <typename... Rs>
-__device__ __forceinline__ void roll_rows(const Rs&... rs) {
-  roll_pass<0, max_passes<Rs...>()>(rs...);
 }
 
 // Start of a TMA box whose first wanted column is i0, rounded down to a
@@ -281,11 +186,10 @@ struct MassL {
   static constexpr size_t bytes = boxes + work + 128;
   // CTAs per SM the register budget is set for (measured): FP64 C grid 6
   // on 32 x 4 tiles (40 registers), FP64 D grid 5 on 32 x 6 tiles (48
-  // registers); FP32 the CTAs their shared memory holds (3 C grid, 4 D grid)
-  static constexpr int min_blocks = !std::is_same_v<T, double> ? (CGRID ? 3 : 4) : CGRID ? 6 : 5;
+  // registers); the FP32 sweeps keep the compiler's choice
+  static constexpr int min_blocks = !std::is_same_v<T, double> ? 1 : CGRID ? 6 : 5;
 };
 
-// One block per strip of nsub sub-tiles of TX x TY (in y) of one layer.
 template <typename T, int TX, int TY, bool CGRID, typename S = T, typename C = T>
 __global__ void __launch_bounds__(NT, MassL<T, TX, TY, CGRID, S, C>::min_blocks) k_mass2(const __grid_constant__ CUtensorMap m_dp,
                                               const __grid_constant__ CUtensorMap m_pt,
@@ -294,7 +198,7 @@ __global__ void __launch_bounds__(NT, MassL<T, TX, TY, CGRID, S, C>::min_blocks)
                                               const double* __restrict__ heat,
                                               std::conditional_t<CGRID, C, S>* __restrict__ dpo,
                                               std::conditional_t<CGRID, C, S>* __restrict__ pto, int lo, int hi,
-                                              int nsub, int* nonfinite, int* timeout) {
+                                              int* nonfinite, int* timeout) {
   using Lay = MassL<T, TX, TY, CGRID, S, C>;
   using UB = typename Lay::UB;
   using O = std::conditional_t<CGRID, C, S>;
@@ -304,8 +208,7 @@ __global__ void __launch_bounds__(NT, MassL<T, TX, TY, CGRID, S, C>::min_blocks)
   __shared__ int s_ok;
   unsigned char* p = smem_base(smem);
   const int k = blockIdx.z;
-  const int ox = lo + blockIdx.x * TX, oy0 = lo + blockIdx.y * (TY * nsub);
-  const int xhi = g.nx - 1 + hi, yhi = g.ny - 1 + hi;
+  const int ox = lo + blockIdx.x * TX, oy = lo + blockIdx.y * TY;
   const T dt = T(c.dt), dtdx = T(c.dtdx), dtdy = T(c.dtdy), rA = T(c.rA);
 
   auto sbox = [&](int i0, int j0, int w, int h) {
@@ -318,188 +221,151 @@ __global__ void __launch_bounds__(NT, MassL<T, TX, TY, CGRID, S, C>::min_blocks)
     p += tma_box_bytes(w, h, sizeof(UB));
     return s;
   };
-  // box origins are those of the strip's first sub-tile; every sub-tile
-  // moves them to its own rows
-  Sm<S> sdp = sbox(ox - 3, oy0 - 3, Lay::WD, Lay::HD);
-  Sm<S> spt = sbox(ox - 3, oy0 - 3, Lay::WD, Lay::HD);
-  Sm<UB> su = CGRID ? ubox(ox - 1, oy0 - 3, Lay::WU, Lay::HU) : ubox(ox, oy0 - 3, Lay::WU, Lay::HU);
-  Sm<UB> sv = CGRID ? ubox(ox - 3, oy0 - 1, Lay::WV, Lay::HV) : ubox(ox - 3, oy0, Lay::WV, Lay::HV);
+  Sm<S> sdp = sbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
+  Sm<S> spt = sbox(ox - 3, oy - 3, Lay::WD, Lay::HD);
+  Sm<UB> su = CGRID ? ubox(ox - 1, oy - 3, Lay::WU, Lay::HU) : ubox(ox, oy - 3, Lay::WU, Lay::HU);
+  Sm<UB> sv = CGRID ? ubox(ox - 3, oy - 1, Lay::WV, Lay::HV) : ubox(ox - 3, oy, Lay::WV, Lay::HV);
+  {
+    const TmaBox boxes[4] = {{&m_dp, sdp.p, sdp.x0, sdp.y0, k},
+                             {&m_pt, spt.p, spt.x0, spt.y0, k},
+                             {&m_u, su.p, su.x0, su.y0, k},
+                             {&m_v, sv.p, sv.x0, sv.y0, k}};
+    if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
+  }
   // C-grid winds: built from the D-grid winds (C step) or the loaded boxes (D step)
   Sm<T> suc, svc;
   if constexpr (CGRID) {
-    suc = carve<T>(p, ox, oy0 - 3, TX + 1, TY + 6);
-    svc = carve<T>(p, ox - 3, oy0, TX + 6, TY + 1);
+    suc = carve<T>(p, ox, oy - 3, TX + 1, TY + 6);
+    svc = carve<T>(p, ox - 3, oy, TX + 6, TY + 1);
+  } else {
+    suc = su;
+    svc = sv;
   }
-  Sm<T> tyd = carve<T>(p, ox - 3, oy0, TX + 6, TY);
-  Sm<T> typ = carve<T>(p, ox - 3, oy0, TX + 6, TY);
-  Sm<T> txd = carve<T>(p, ox, oy0 - 3, TX, TY + 6);
-  Sm<T> txp = carve<T>(p, ox, oy0 - 3, TX, TY + 6);
-  Sm<T> lpd = carve<T>(p, ox - 1, oy0 - 1, TX + 2, TY + 2);
-  Sm<T> lpp = carve<T>(p, ox - 1, oy0 - 1, TX + 2, TY + 2);
-  Sm<T> mxd = carve<T>(p, ox - 2, oy0, TX + 4, TY);
-  Sm<T> mxp = carve<T>(p, ox - 2, oy0, TX + 4, TY);
-  Sm<T> myd = carve<T>(p, ox, oy0 - 2, TX, TY + 4);
-  Sm<T> myp = carve<T>(p, ox, oy0 - 2, TX, TY + 4);
-  Sm<T> fxd = carve<T>(p, ox, oy0, TX + 1, TY);
-  Sm<T> fxp = carve<T>(p, ox, oy0, TX + 1, TY);
-  Sm<T> fyd = carve<T>(p, ox, oy0, TX, TY + 1);
-  Sm<T> fyp = carve<T>(p, ox, oy0, TX, TY + 1);
+  Sm<T> tyd = carve<T>(p, ox - 3, oy, TX + 6, TY);
+  Sm<T> typ = carve<T>(p, ox - 3, oy, TX + 6, TY);
+  Sm<T> txd = carve<T>(p, ox, oy - 3, TX, TY + 6);
+  Sm<T> txp = carve<T>(p, ox, oy - 3, TX, TY + 6);
+  Sm<T> lpd = carve<T>(p, ox - 1, oy - 1, TX + 2, TY + 2);
+  Sm<T> lpp = carve<T>(p, ox - 1, oy - 1, TX + 2, TY + 2);
+  Sm<T> mxd = carve<T>(p, ox - 2, oy, TX + 4, TY);
+  Sm<T> mxp = carve<T>(p, ox - 2, oy, TX + 4, TY);
+  Sm<T> myd = carve<T>(p, ox, oy - 2, TX, TY + 4);
+  Sm<T> myp = carve<T>(p, ox, oy - 2, TX, TY + 4);
+  Sm<T> fxd = carve<T>(p, ox, oy, TX + 1, TY);
+  Sm<T> fxp = carve<T>(p, ox, oy, TX + 1, TY);
+  Sm<T> fyd = carve<T>(p, ox, oy, TX, TY + 1);
+  Sm<T> fyp = carve<T>(p, ox, oy, TX, TY + 1);
 
   // merged stage loops measured faster in FP32, slower in FP64
   constexpr bool MG = std::is_same_v<T, float>;
-  bool bad = false;
-  for (int j = 0; j < nsub; ++j) {
-    const int oy = oy0 + j * TY;
-    if (oy > yhi) break;
-    const bool first = j == 0;
-    if (!first) {
-      // the rows this sub-tile shares with the last one move to the top
-      __syncthreads();
-      if constexpr (CGRID)
-        roll_rows(roll<6, TY, TX + 1>(suc), roll<1, TY, TX + 6>(svc), roll<6, TY, TX>(txd), roll<6, TY, TX>(txp),
-                  roll<2, TY, TX + 2>(lpd), roll<2, TY, TX + 2>(lpp), roll<4, TY, TX>(myd), roll<4, TY, TX>(myp),
-                  roll<1, TY, TX>(fyd), roll<1, TY, TX>(fyp));
-      else
-        roll_rows(roll<6, TY, TX>(txd), roll<6, TY, TX>(txp), roll<2, TY, TX + 2>(lpd), roll<2, TY, TX + 2>(lpp),
-                  roll<4, TY, TX>(myd), roll<4, TY, TX>(myp), roll<1, TY, TX>(fyd), roll<1, TY, TX>(fyp));
-    }
-    sdp.y0 = oy - 3;
-    spt.y0 = oy - 3;
-    su.y0 = oy - 3;
-    sv.y0 = CGRID ? oy - 1 : oy;
-    {
-      const TmaBox boxes[4] = {{&m_dp, sdp.p, sdp.x0, sdp.y0, k},
-                               {&m_pt, spt.p, spt.x0, spt.y0, k},
-                               {&m_u, su.p, su.x0, su.y0, k},
-                               {&m_v, sv.p, sv.x0, sv.y0, k}};
-      if (!tma_fetch_round(boxes, Lay::tx_bytes, &bar, j, timeout, &s_ok)) return;
-    }
-    if constexpr (CGRID) {
-      suc.y0 = oy - 3;
-      svc.y0 = oy;
-    } else {
-      suc = su;
-      svc = sv;
-    }
-    tyd.y0 = typ.y0 = oy;
-    txd.y0 = txp.y0 = oy - 3;
-    lpd.y0 = lpp.y0 = oy - 1;
-    mxd.y0 = mxp.y0 = oy;
-    myd.y0 = myp.y0 = oy - 2;
-    fxd.y0 = fxp.y0 = oy;
-    fyd.y0 = fyp.y0 = oy;
-    // rows per stage: [oy + a, oy + TY + b) on the first sub-tile, the new ones after
-    const Rows r_uc = rows_of<TY>(oy, first, -3, 3), r_vc = rows_of<TY>(oy, first, 0, 1);
-    const Rows r_tx = rows_of<TY>(oy, first, -3, 3), r_lp = rows_of<TY>(oy, first, -1, 1);
-    const Rows r_my = rows_of<TY>(oy, first, -2, 2), r_fy = rows_of<TY>(oy, first, 0, 1);
-
-    if constexpr (CGRID) {  // mod_sw_dyn.f90:109-117
-      regions<MG>(reg<TX + 1>(ox, r_uc.y0, r_uc.h, [&](int x, int y) {
-        T ub = T(.5) * (T(su(x, y)) + T(su(x - 1, y)));
-        suc(x, y) = T(.5) * (ub + T(.5) * (T(su(x, y + 1)) + T(su(x - 1, y + 1))));
-      }),
-                  reg<TX + 6>(ox - 3, r_vc.y0, r_vc.h, [&](int x, int y) {
-        T vb = T(.5) * (T(sv(x, y)) + T(sv(x, y - 1)));
-        svc(x, y) = T(.5) * (vb + T(.5) * (T(sv(x + 1, y)) + T(sv(x + 1, y - 1))));
-      }));
-      __syncthreads();
-    }
-    // inner sweeps and Laplacians: mod_sw_dyn.f90:142-155,176-185 (C); 470-482,503-511 (D)
-    const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
-    regions<MG>(reg<TX + 6>(ox - 3, oy, TY, [&](int x, int y) {
-      T cy0 = dtdx * svc(x, y), cy1 = dtdx * svc(x, y + 1);
-      T den = T(1) / (T(1) - dtdy * (svc(x, y + 1) - svc(x, y)));
-      const T d0 = T(sdp(x, y)), dm = T(sdp(x, y - 1)), dq = T(sdp(x, y + 1));
-      T f0 = (cy0 > T(0)) ? dm : d0;
-      T f1 = (cy1 > T(0)) ? d0 : dq;
-      tyd(x, y) = T(.5) * (d0 + den * (d0 - rA * (f1 - f0)));
-      const T p0 = T(spt(x, y)), pm = T(spt(x, y - 1)), pq = T(spt(x, y + 1));
-      f0 = (cy0 > T(0)) ? pm : p0;
-      f1 = (cy1 > T(0)) ? p0 : pq;
-      typ(x, y) = T(.5) * (p0 + den * (p0 - rA * (f1 - f0)));
+  if constexpr (CGRID) {  // mod_sw_dyn.f90:109-117
+    regions<MG>(reg<TX + 1, TY + 6>(ox, oy - 3, [&](int x, int y) {
+      T ub = T(.5) * (T(su(x, y)) + T(su(x - 1, y)));
+      suc(x, y) = T(.5) * (ub + T(.5) * (T(su(x, y + 1)) + T(su(x - 1, y + 1))));
     }),
-                reg<TX>(ox, r_tx.y0, r_tx.h, [&](int x, int y) {
-      T cx0 = dtdx * suc(x, y), cx1 = dtdx * suc(x + 1, y);
-      T den = T(1) / (T(1) - dtdx * (suc(x + 1, y) - suc(x, y)));
-      const T d0 = T(sdp(x, y)), dm = T(sdp(x - 1, y)), dq = T(sdp(x + 1, y));
-      T f0 = (cx0 > T(0)) ? dm : d0;
-      T f1 = (cx1 > T(0)) ? d0 : dq;
-      txd(x, y) = T(.5) * (d0 + den * (d0 - rA * (f1 - f0)));
-      const T p0 = T(spt(x, y)), pm = T(spt(x - 1, y)), pq = T(spt(x + 1, y));
-      f0 = (cx0 > T(0)) ? pm : p0;
-      f1 = (cx1 > T(0)) ? p0 : pq;
-      txp(x, y) = T(.5) * (p0 + den * (p0 - rA * (f1 - f0)));
-    }),
-                reg<TX + 2>(ox - 1, r_lp.y0, r_lp.h, [&](int x, int y) {
-      lpd(x, y) = T(-2.) * T(sdp(x, y)) * rdxy + (T(sdp(x + 1, y)) + T(sdp(x - 1, y))) * rdx2 +
-                  (T(sdp(x, y + 1)) + T(sdp(x, y - 1))) * rdy2;
-      lpp(x, y) = T(-2.) * T(spt(x, y)) * rdxy + (T(spt(x + 1, y)) + T(spt(x - 1, y))) * rdx2 +
-                  (T(spt(x, y + 1)) + T(spt(x, y - 1))) * rdy2;
+            reg<TX + 6, TY + 1>(ox - 3, oy, [&](int x, int y) {
+      T vb = T(.5) * (T(sv(x, y)) + T(sv(x, y - 1)));
+      svc(x, y) = T(.5) * (vb + T(.5) * (T(sv(x + 1, y)) + T(sv(x + 1, y - 1))));
     }));
     __syncthreads();
-    // monotone slopes of the outer sweeps (ppm, :870-875)
-    regions<MG>(reg<TX + 4>(ox - 2, oy, TY, [&](int x, int y) {
-      mxd(x, y) = slope_at(tyd.ptr(x, y), 1);
-      mxp(x, y) = slope_at(typ.ptr(x, y), 1);
-    }),
-                reg<TX>(ox, r_my.y0, r_my.h, [&](int x, int y) {
-      myd(x, y) = slope_at(txd.ptr(x, y), TX);
-      myp(x, y) = slope_at(txp.ptr(x, y), TX);
-    }));
-    __syncthreads();
-    // outer sweeps (PPM)
-    regions<MG>(reg<TX + 1>(ox, oy, TY, [&](int x, int y) {
-      T cx = dtdx * suc(x, y);
-      fxd(x, y) = flux_pre<T, V>(tyd.ptr(x, y), 1, mxd.ptr(x, y), 1, cx) * cx;
-      fxp(x, y) = flux_pre<T, V>(typ.ptr(x, y), 1, mxp.ptr(x, y), 1, cx);
-    }),
-                reg<TX>(ox, r_fy.y0, r_fy.h, [&](int x, int y) {
-      T cy = dtdx * svc(x, y);
-      fyd(x, y) = flux_pre<T, V>(txd.ptr(x, y), TX, myd.ptr(x, y), TX, cy) * cy;
-      fyp(x, y) = flux_pre<T, V>(txp.ptr(x, y), TX, myp.ptr(x, y), TX, cy);
-    }));
-    __syncthreads();
-
-    // updates, mod_sw_dyn.f90:163-172,193-202,230-237,258-267 (C); 490-499,519-528,555-562,582-591 (D)
-    const T dxv = dtdx * T(c.vdx), dyv = dtdy * T(c.vdy), vdx = T(c.vdx), vdy = T(c.vdy);
-    regions<false>(reg<TX>(ox, oy, TY, [&](int x, int y) {
-      if (x > xhi || y > yhi) return;
-      O vo, qo;
-      if constexpr (std::is_same_v<S, T>) {  // the reference's operations, in order
-        T d = sdp(x, y);
-        T v = d - (fxd(x + 1, y) - fxd(x, y) + dxv * (lpd(x + 1, y) - T(2.) * lpd(x, y) + lpd(x - 1, y)));
-        v = v - (fyd(x, y + 1) - fyd(x, y) + dyv * (lpd(x, y + 1) - T(2.) * lpd(x, y) + lpd(x, y - 1)));
-        T q = d * spt(x, y) - (fxp(x + 1, y) * fxd(x + 1, y) - fxp(x, y) * fxd(x, y) +
-                               vdx * ((lpp(x + 1, y) - lpp(x, y)) * fxd(x + 1, y) - (lpp(x, y) - lpp(x - 1, y)) * fxd(x, y)));
-        q = q - (fyp(x, y + 1) * fyd(x, y + 1) - fyp(x, y) * fyd(x, y) +
-                 vdy * ((lpp(x, y + 1) - lpp(x, y)) * fyd(x, y + 1) - (lpp(x, y) - lpp(x, y - 1)) * fyd(x, y)));
-        if (heat) q = q + dt * d * T(heat[g.at(x, y, k)]);
-        q = q / v;
-        vo = O(v);
-        qo = O(q);
-      } else {
-        // the same update in flux form: interface fluxes (advective plus
-        // vorticity-damping) in the sweep type, their differences applied to
-        // the state's type, so that mass and dp*pt telescope in S
-        auto Fx = [&](int xx) { return fxd(xx, y) + dxv * (lpd(xx, y) - lpd(xx - 1, y)); };
-        auto Fy = [&](int yy) { return fyd(x, yy) + dyv * (lpd(x, yy) - lpd(x, yy - 1)); };
-        auto Hx = [&](int xx) { return (fxp(xx, y) + vdx * (lpp(xx, y) - lpp(xx - 1, y))) * fxd(xx, y); };
-        auto Hy = [&](int yy) { return (fyp(x, yy) + vdy * (lpp(x, yy) - lpp(x, yy - 1))) * fyd(x, yy); };
-        const S d = sdp(x, y);
-        const S v = d - ((S(Fx(x + 1)) - S(Fx(x))) + (S(Fy(y + 1)) - S(Fy(y))));
-        S q = d * spt(x, y) - ((S(Hx(x + 1)) - S(Hx(x))) + (S(Hy(y + 1)) - S(Hy(y))));
-        if (heat) q = q + S(c.dt) * d * S(heat[g.at(x, y, k)]);
-        q = q / v;
-        vo = O(v);
-        qo = O(q);
-      }
-      long long o = g.at(x, y, k);
-      dpo[o] = vo;
-      pto[o] = qo;
-      bool inside = x >= 0 && x < g.nx && y >= 0 && y < g.ny;
-      bad = bad || (inside && !(finite_(vo) && finite_(qo)));
-    }));
   }
+  // inner sweeps and Laplacians: mod_sw_dyn.f90:142-155,176-185 (C); 470-482,503-511 (D)
+  const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
+  regions<MG>(reg<TX + 6, TY>(ox - 3, oy, [&](int x, int y) {
+    T cy0 = dtdx * svc(x, y), cy1 = dtdx * svc(x, y + 1);
+    T den = T(1) / (T(1) - dtdy * (svc(x, y + 1) - svc(x, y)));
+    const T d0 = T(sdp(x, y)), dm = T(sdp(x, y - 1)), dq = T(sdp(x, y + 1));
+    T f0 = (cy0 > T(0)) ? dm : d0;
+    T f1 = (cy1 > T(0)) ? d0 : dq;
+    tyd(x, y) = T(.5) * (d0 + den * (d0 - rA * (f1 - f0)));
+    const T p0 = T(spt(x, y)), pm = T(spt(x, y - 1)), pq = T(spt(x, y + 1));
+    f0 = (cy0 > T(0)) ? pm : p0;
+    f1 = (cy1 > T(0)) ? p0 : pq;
+    typ(x, y) = T(.5) * (p0 + den * (p0 - rA * (f1 - f0)));
+  }),
+          reg<TX, TY + 6>(ox, oy - 3, [&](int x, int y) {
+    T cx0 = dtdx * suc(x, y), cx1 = dtdx * suc(x + 1, y);
+    T den = T(1) / (T(1) - dtdx * (suc(x + 1, y) - suc(x, y)));
+    const T d0 = T(sdp(x, y)), dm = T(sdp(x - 1, y)), dq = T(sdp(x + 1, y));
+    T f0 = (cx0 > T(0)) ? dm : d0;
+    T f1 = (cx1 > T(0)) ? d0 : dq;
+    txd(x, y) = T(.5) * (d0 + den * (d0 - rA * (f1 - f0)));
+    const T p0 = T(spt(x, y)), pm = T(spt(x - 1, y)), pq = T(spt(x + 1, y));
+    f0 = (cx0 > T(0)) ? pm : p0;
+    f1 = (cx1 > T(0)) ? p0 : pq;
+    txp(x, y) = T(.5) * (p0 + den * (p0 - rA * (f1 - f0)));
+  }),
+          reg<TX + 2, TY + 2>(ox - 1, oy - 1, [&](int x, int y) {
+    lpd(x, y) = T(-2.) * T(sdp(x, y)) * rdxy + (T(sdp(x + 1, y)) + T(sdp(x - 1, y))) * rdx2 +
+                (T(sdp(x, y + 1)) + T(sdp(x, y - 1))) * rdy2;
+    lpp(x, y) = T(-2.) * T(spt(x, y)) * rdxy + (T(spt(x + 1, y)) + T(spt(x - 1, y))) * rdx2 +
+                (T(spt(x, y + 1)) + T(spt(x, y - 1))) * rdy2;
+  }));
+  __syncthreads();
+  // monotone slopes of the outer sweeps (ppm, :870-875)
+  regions<MG>(reg<TX + 4, TY>(ox - 2, oy, [&](int x, int y) {
+    mxd(x, y) = slope_at(tyd.ptr(x, y), 1);
+    mxp(x, y) = slope_at(typ.ptr(x, y), 1);
+  }),
+          reg<TX, TY + 4>(ox, oy - 2, [&](int x, int y) {
+    myd(x, y) = slope_at(txd.ptr(x, y), TX);
+    myp(x, y) = slope_at(txp.ptr(x, y), TX);
+  }));
+  __syncthreads();
+  // outer sweeps (PPM)
+  regions<MG>(reg<TX + 1, TY>(ox, oy, [&](int x, int y) {
+    T cx = dtdx * suc(x, y);
+    fxd(x, y) = flux_pre<T, V>(tyd.ptr(x, y), 1, mxd.ptr(x, y), 1, cx) * cx;
+    fxp(x, y) = flux_pre<T, V>(typ.ptr(x, y), 1, mxp.ptr(x, y), 1, cx);
+  }),
+          reg<TX, TY + 1>(ox, oy, [&](int x, int y) {
+    T cy = dtdx * svc(x, y);
+    fyd(x, y) = flux_pre<T, V>(txd.ptr(x, y), TX, myd.ptr(x, y), TX, cy) * cy;
+    fyp(x, y) = flux_pre<T, V>(txp.ptr(x, y), TX, myp.ptr(x, y), TX, cy);
+  }));
+  __syncthreads();
+
+  // updates, mod_sw_dyn.f90:163-172,193-202,230-237,258-267 (C); 490-499,519-528,555-562,582-591 (D)
+  const int xhi = g.nx - 1 + hi, yhi = g.ny - 1 + hi;
+  const T dxv = dtdx * T(c.vdx), dyv = dtdy * T(c.vdy), vdx = T(c.vdx), vdy = T(c.vdy);
+  bool bad = false;
+  region<TX, TY>(ox, oy, [&](int x, int y) {
+    if (x > xhi || y > yhi) return;
+    O vo, qo;
+    if constexpr (std::is_same_v<S, T>) {  // the reference's operations, in order
+      T d = sdp(x, y);
+      T v = d - (fxd(x + 1, y) - fxd(x, y) + dxv * (lpd(x + 1, y) - T(2.) * lpd(x, y) + lpd(x - 1, y)));
+      v = v - (fyd(x, y + 1) - fyd(x, y) + dyv * (lpd(x, y + 1) - T(2.) * lpd(x, y) + lpd(x, y - 1)));
+      T q = d * spt(x, y) - (fxp(x + 1, y) * fxd(x + 1, y) - fxp(x, y) * fxd(x, y) +
+                             vdx * ((lpp(x + 1, y) - lpp(x, y)) * fxd(x + 1, y) - (lpp(x, y) - lpp(x - 1, y)) * fxd(x, y)));
+      q = q - (fyp(x, y + 1) * fyd(x, y + 1) - fyp(x, y) * fyd(x, y) +
+               vdy * ((lpp(x, y + 1) - lpp(x, y)) * fyd(x, y + 1) - (lpp(x, y) - lpp(x, y - 1)) * fyd(x, y)));
+      if (heat) q = q + dt * d * T(heat[g.at(x, y, k)]);
+      q = q / v;
+      vo = O(v);
+      qo = O(q);
+    } else {
+      // the same update in flux form: interface fluxes (advective plus
+      // vorticity-damping) in the sweep type, their differences applied to
+      // the state's type, so that mass and dp*pt telescope in S
+      auto Fx = [&](int xx) { return fxd(xx, y) + dxv * (lpd(xx, y) - lpd(xx - 1, y)); };
+      auto Fy = [&](int yy) { return fyd(x, yy) + dyv * (lpd(x, yy) - lpd(x, yy - 1)); };
+      auto Hx = [&](int xx) { return (fxp(xx, y) + vdx * (lpp(xx, y) - lpp(xx - 1, y))) * fxd(xx, y); };
+      auto Hy = [&](int yy) { return (fyp(x, yy) + vdy * (lpp(x, yy) - lpp(x, yy - 1))) * fyd(x, yy); };
+      const S d = sdp(x, y);
+      const S v = d - ((S(Fx(x + 1)) - S(Fx(x))) + (S(Fy(y + 1)) - S(Fy(y))));
+      S q = d * spt(x, y) - ((S(Hx(x + 1)) - S(Hx(x))) + (S(Hy(y + 1)) - S(Hy(y))));
+      if (heat) q = q + S(c.dt) * d * S(heat[g.at(x, y, k)]);
+      q = q / v;
+      vo = O(v);
+      qo = O(q);
+    }
+    long long o = g.at(x, y, k);
+    dpo[o] = vo;
+    pto[o] = qo;
+    bool inside = x >= 0 && x < g.nx && y >= 0 && y < g.ny;
+    bad = bad || (inside && !(finite_(vo) && finite_(qo)));
+  });
   if (nonfinite) flag_nonfinite(nonfinite, bad);
 }
 

@@ -108,32 +108,4 @@ __device__ __forceinline__ bool tma_fetch(const TmaBox (&boxes)[N], uint32_t byt
   return *s_ok != 0;
 }
 
-// The same for a block that loads several rounds of boxes on one barrier
-// (a strip of sub-tiles): round r (from 0) initialises the barrier when r is
-// 0 and waits for the phase of parity r & 1.  The caller synchronises the
-// block between its last read of the previous round's boxes and this call.
-template <int N>
-__device__ __forceinline__ bool tma_fetch_round(const TmaBox (&boxes)[N], uint32_t bytes, uint64_t* bar, int round,
-                                                int* timeout_flag, int* s_ok) {
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    if (round == 0) {
-      mbar_init(bar, 1);
-      fence_mbar_init();
-    }
-    mbar_expect_tx(bar, bytes);
-#pragma unroll
-    for (int b = 0; b < N; ++b)
-      tma_load_3d(boxes[b].dst, boxes[b].map, boxes[b].i0 + H + XOFF, boxes[b].j0 + H, boxes[b].k, bar);
-    const uint32_t parity = (uint32_t)round & 1u;
-    bool ok = mbar_wait(bar, parity, 1000000);  // about one second at most
-    if (!ok) {
-      if (timeout_flag) atomicOr(timeout_flag, 1);
-      mbar_wait(bar, parity, 1000000);
-    }
-    *s_ok = ok ? 1 : 0;
-  }
-  __syncthreads();
-  return *s_ok != 0;
-}
-
 }  // namespace atm

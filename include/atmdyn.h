@@ -165,13 +165,6 @@ int atm_profile(atm_ctx* ctx, int enable);
 int atm_profile_read(atm_ctx* ctx, double* ms, int* count, int nstage);
 const char* atm_profile_stage(int i);
 int atm_launch_count(atm_ctx* ctx, long long* n);
-/* The mass sweeps run one block per strip of sub-tiles in y, keeping the
-   stencil rows that neighbouring sub-tiles share; the library picks the
-   sub-tiles per strip from the grid (1 on small domains).  A positive n
-   fixes it for every later launch of the process (0 = automatic again),
-   so that tests reach strips, and ragged last strips, on small domains.
-   Results do not depend on it.  Returns ATM_ERR_ARG outside 0..64. */
-int atm_set_subtiles(int n);
 
 /* the portable x**y and log(x) the FP64 form evaluates on the device, on n
    host values (accuracy and bit-identity tests) */

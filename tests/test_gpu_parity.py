@@ -7,7 +7,7 @@ so every comparison here is bit-exact: max |difference| == 0.
 import numpy as np
 import pytest
 
-from atmdyn import ic, model, Dycore, device_pow_log, subtiles
+from atmdyn import ic, model, Dycore, device_pow_log
 import pyoracle
 
 pytestmark = pytest.mark.gpu
@@ -44,18 +44,14 @@ def test_device_pow_log_bit_identical_to_host():
     _assert_same(l_dev, pyoracle.log_array(x), 'log')
 
 
-# strip: sub-tiles per block of the mass sweeps (0 = the library's choice,
-# one on these small domains; 3 gives strips with a ragged last one)
-@pytest.mark.parametrize('strip', [0, 3])
 @pytest.mark.parametrize('case', ['bubble', 'jet', 'ragged'])
-def test_cgrid_step_bit_exact(case, strip):
+def test_cgrid_step_bit_exact(case):
     st = {'bubble': _bubble(), 'jet': _jet(), 'ragged': _bubble(37, 23, 7)}[case]
     dt = st.dt
     g = Dycore(st)
     o = pyoracle.OracleModel(st)
-    with subtiles(strip):
-        g.cgrid_step(dt / 2)
-    o.cgrid_step(dt / 2)
+    for a in (g, o):
+        a.cgrid_step(dt / 2)
     nx, ny = st.nx, st.ny
     sl2 = (slice(None), slice(HALO - 2, HALO + ny + 2), slice(HALO - 2, HALO + nx + 2))
     sl0 = (slice(None), slice(HALO, HALO + ny), slice(HALO, HALO + nx))
@@ -69,18 +65,16 @@ def test_cgrid_step_bit_exact(case, strip):
         _assert_same(g.get(name, halo=True), o.get(f, halo=True), name + ' after halo')
 
 
-@pytest.mark.parametrize('strip', [0, 3])
 @pytest.mark.parametrize('case', ['bubble', 'jet', 'ragged'])
-def test_dgrid_step_and_remap_bit_exact(case, strip):
+def test_dgrid_step_and_remap_bit_exact(case):
     st = {'bubble': _bubble(), 'jet': _jet(), 'ragged': _bubble(37, 23, 7)}[case]
     dt = st.dt
     g = Dycore(st)
     o = pyoracle.OracleModel(st)
-    with subtiles(strip):
-        for a in (g, o):
-            a.cgrid_step(dt / 2)
-            a.cgrid_halo()
-            a.dgrid_step(dt)
+    for a in (g, o):
+        a.cgrid_step(dt / 2)
+        a.cgrid_halo()
+        a.dgrid_step(dt)
     # the whole arrays, halo included, as the reference leaves them
     for name, f in (('dp', pyoracle.DP), ('pt', pyoracle.PT), ('ud', pyoracle.UD), ('vd', pyoracle.VD)):
         _assert_same(g.get(name, halo=True), o.get(f, halo=True), name + ' after D step')
@@ -105,29 +99,12 @@ def test_bubble_100_steps_bit_exact_and_mass():
     g = Dycore(st)
     o = pyoracle.OracleModel(st, threads=4)
     m0 = g.mass()
-    with subtiles(2):
-        rg = model.run_model(g, tc)
+    rg = model.run_model(g, tc)
     ro = model.run_model(o, tc)
     assert rg.stable and ro.stable and rg.steps == ro.steps == 100 and rg.remap_steps == ro.remap_steps
     for name, f in (('dp', pyoracle.DP), ('pt', pyoracle.PT), ('ud', pyoracle.UD), ('vd', pyoracle.VD)):
         _assert_same(g.get(name, halo=True), o.get(f, halo=True), name)
     assert abs(g.mass() - m0) / m0 <= 1e-13
-
-
-def test_step_at_strip_size_bit_exact():
-    """A domain large enough that the library itself runs the mass sweeps
-    as strips of several sub-tiles (160 x 160 x 64): one step with remap."""
-    st = _jet(160, 160, 64, seed=3)
-    g = Dycore(st)
-    o = pyoracle.OracleModel(st, threads=8)
-    for a in (g, o):
-        a.cgrid_step(st.dt / 2)
-        a.cgrid_halo()
-        a.dgrid_step(st.dt)
-        a.remap()
-        a.dgrid_halo()
-    for name, f in (('dp', pyoracle.DP), ('pt', pyoracle.PT), ('ud', pyoracle.UD), ('vd', pyoracle.VD)):
-        _assert_same(g.get(name, halo=True), o.get(f, halo=True), name)
 
 
 def test_division_by_constants_is_ieee_division():
