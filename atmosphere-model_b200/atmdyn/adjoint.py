@@ -5,10 +5,10 @@ prognostic interior (dp, pt, ud, vd as float64 CUDA tensors of shape
 (nlay, ny, nx)) through a segment of steps with libatmdyn.  Its forward
 keeps only the segment's initial state (a checkpoint).  Its backward
 restores that state, recomputes the segment once keeping each step's
-initial state and forward products (``atm_step_tape``), and then runs the
-adjoint steps in reverse order (``atm_adj_step_tape``: the CUDA adjoint
-kernels of the sweeps, the remap and the halo fills, with the limiter
-branches of the recomputed forward).
+tape (``atm_step_tape``: its initial state and forward products), and then
+runs the adjoint steps in reverse order from the tapes
+(``atm_adj_step_tape``: the CUDA adjoint kernels of the sweeps, the remap
+and the halo fills, with the limiter branches of the recomputed forward).
 :func:`integrate` chains segments of ``checkpoint_every`` steps, so memory
 grows with the number of checkpoints plus one segment of states.  The
 last segment's forward records its tapes as it goes (the backward starts
@@ -58,24 +58,21 @@ def _download(dyn: Dycore, like):
 
 
 def _record(dyn: Dycore, dt: float, remaps, like):
-    """Steps from the context's current state keeping, per step, the
-    initial state and the tape of its forward products."""
-    states, tapes = [], []
+    """Steps from the context's current state keeping, per step, its tape
+    (the initial state and the forward products the adjoint step reads)."""
+    tapes = []
     for r in remaps:
-        st = torch.empty(dyn.state_bytes() // 8, dtype=torch.float64, device=like.device)
-        dyn.state_save(st.data_ptr())
-        states.append(st)
         tp = torch.empty(dyn.tape_bytes() // 8, dtype=torch.float64, device=like.device)
         dyn.step_tape(dt, bool(r), tp.data_ptr())
         tapes.append(tp)
-    return states, tapes
+    return tapes
 
 
 class DycoreSegment(torch.autograd.Function):
     """(dp, pt, ud, vd) -> the state after ``len(remaps)`` steps of size dt;
     remaps[i] says whether step i ends with the vertical remap.  With
-    ``record`` the forward keeps every step's state and tape (the segment
-    the backward starts with) instead of a checkpoint."""
+    ``record`` the forward keeps every step's tape (the segment the
+    backward starts with) instead of a checkpoint."""
 
     @staticmethod
     def forward(ctx, dyn: Dycore, dt: float, remaps, record: bool, dp, pt, ud, vd):
@@ -102,22 +99,21 @@ class DycoreSegment(torch.autograd.Function):
         (ckpt,) = ctx.saved_tensors
         _bind_stream(dyn)
         if ctx.trajectory is not None:
-            states, tapes = ctx.trajectory
+            tapes = ctx.trajectory
             ctx.trajectory = None
         else:
-            # recompute the segment, keeping every step's initial state and
-            # its forward products (C-grid fields, pre-remap state) on a tape
+            # recompute the segment, keeping every step's tape (initial
+            # state, C-grid fields, pre-remap state, corner pkap and gz)
             dyn.state_load(ckpt.data_ptr())
-            states, tapes = _record(dyn, dt, remaps, ckpt)
+            tapes = _record(dyn, dt, remaps, ckpt)
         dyn.adj_zero()
         grads = [g if g is not None else torch.zeros_like(ckpt[:0]) for g in (gdp, gpt, gud, gvd)]
         for name, g in zip(FIELD_NAMES, grads):
             if g.numel():
                 dyn.adj_set_device('out', name, g.detach().contiguous().data_ptr())
-        for s, tp, r in zip(reversed(states), reversed(tapes), reversed(remaps)):
-            dyn.state_load(s.data_ptr())
+        for tp, r in zip(reversed(tapes), reversed(remaps)):
             dyn.adj_step_tape(dt, r, tp.data_ptr())
-        del states, tapes
+        del tapes
         dyn.adj_halo('out')  # the initial state's halo is the periodic image of its interior
         like = gdp if gdp is not None else (gpt if gpt is not None else (gud if gud is not None else gvd))
         outs = []

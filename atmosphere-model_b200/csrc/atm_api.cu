@@ -1072,12 +1072,12 @@ int atm_adj_remap(atm_ctx* ctx) {
 
 namespace {
 
-// the reverse of one step given its forward products: cgf = C-grid fields
-// after the C-grid halo, s1 = the state after the D-grid step (before the
-// remap); pkapb, gzb must hold the D step's values
-int adj_step_given(atm_ctx* ctx, double dt, int do_remap, const void* const* cgf, const void* const* s1) {
+// the reverse of one step given its forward products: s0 = the state before
+// the step, cgf = C-grid fields after the C-grid halo, s1 = the state after
+// the D-grid step (before the remap); pkapb, gzb must hold the D step's values
+int adj_step_given(atm_ctx* ctx, double dt, int do_remap, const void* const* s0, const void* const* cgf,
+                   const void* const* s1) {
   const Geom& g = ctx->geo;
-  const void* const* s0 = (const void* const*)ctx->st[ctx->cur];
   if (do_remap) {
     CK(zero_fields(ctx, slot_fields(ctx, ATM_ADJ_IN), 4, ctx->L));
     int r = adj_r(ctx, s1, slot_fields(ctx, ATM_ADJ_OUT), slot_fields(ctx, ATM_ADJ_IN));
@@ -1092,12 +1092,18 @@ int adj_step_given(atm_ctx* ctx, double dt, int do_remap, const void* const* cgf
     Stage t(ctx, S_AHALO);
     CK(atm::adj_ring_fold(g, ctx->lam_cg, 4, ctx->L, ctx->stream));
   }
-  if ((r = adj_c(ctx, dt / 2., ctx->st[ctx->cur], slot_fields(ctx, ATM_ADJ_IN), cgf))) return r;
+  if ((r = adj_c(ctx, dt / 2., const_cast<void* const*>(s0), slot_fields(ctx, ATM_ADJ_IN), cgf))) return r;
   ctx->slot_in = 1 - ctx->slot_in;
   return ATM_OK;
 }
 
 size_t field_bytes(const atm_ctx* c) { return (size_t)c->L * c->geo.S * 8; }
+size_t level_bytes(const atm_ctx* c) { return (size_t)(c->L + 1) * c->geo.S * 8; }
+
+// Tape of one step: the C-grid fields after their halo (4 fields), the
+// state after the D-grid step (4), the state before the step (4), then the
+// D step's pkapb and gzb (L + 1 levels each).
+constexpr int TAPE_CG = 0, TAPE_S1 = 4, TAPE_S0 = 8, TAPE_FIELDS = 12;
 
 }  // namespace
 
@@ -1118,12 +1124,13 @@ int atm_adj_step(atm_ctx* ctx, double dt, int do_remap) {
     CK(ctx->ops->ring_cg(g, ctx->cg, nullptr, 4, ctx->L, false, ctx->stream));
     if ((r = fwd_d(ctx, dt, ctx->st[cur], ctx->st[nxt]))) return r;
   }
-  return adj_step_given(ctx, dt, do_remap, (const void* const*)ctx->cg, (const void* const*)ctx->st[nxt]);
+  return adj_step_given(ctx, dt, do_remap, (const void* const*)ctx->st[cur], (const void* const*)ctx->cg,
+                        (const void* const*)ctx->st[nxt]);
 }
 
 int atm_tape_bytes(atm_ctx* ctx, long long* bytes) {
   if (!ctx || !bytes) return ATM_ERR_ARG;
-  *bytes = 8LL * (long long)field_bytes(ctx);
+  *bytes = (long long)(TAPE_FIELDS * field_bytes(ctx) + 2 * level_bytes(ctx));
   return ATM_OK;
 }
 
@@ -1132,14 +1139,20 @@ int atm_step_tape(atm_ctx* ctx, double dt, int do_remap, void* tape) {
   if (r) return r;
   if (ctx->precision != ATM_FP64) return fail(ctx, ATM_ERR_UNSUPPORTED, "tapes are defined for the FP64 form");
   if (!tape) return ATM_ERR_ARG;
-  const size_t fb = field_bytes(ctx);
+  const size_t fb = field_bytes(ctx), lb = level_bytes(ctx);
   char* t = (char*)tape;
+  for (int i = 0; i < 4; ++i)
+    CK(cudaMemcpyAsync(t + (TAPE_S0 + i) * fb, ctx->st[ctx->cur][i], fb, cudaMemcpyDeviceToDevice, ctx->stream));
   if ((r = atm_cgrid_step(ctx, dt / 2.))) return r;
   if ((r = atm_cgrid_halo(ctx))) return r;
-  for (int i = 0; i < 4; ++i) CK(cudaMemcpyAsync(t + i * fb, ctx->cg[i], fb, cudaMemcpyDeviceToDevice, ctx->stream));
+  for (int i = 0; i < 4; ++i)
+    CK(cudaMemcpyAsync(t + (TAPE_CG + i) * fb, ctx->cg[i], fb, cudaMemcpyDeviceToDevice, ctx->stream));
   if ((r = atm_dgrid_step(ctx, dt))) return r;
   for (int i = 0; i < 4; ++i)
-    CK(cudaMemcpyAsync(t + (4 + i) * fb, ctx->st[ctx->cur][i], fb, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(t + (TAPE_S1 + i) * fb, ctx->st[ctx->cur][i], fb, cudaMemcpyDeviceToDevice, ctx->stream));
+  char* tb = t + TAPE_FIELDS * fb;
+  CK(cudaMemcpyAsync(tb, ctx->pkapb, lb, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(tb + lb, ctx->gzb, lb, cudaMemcpyDeviceToDevice, ctx->stream));
   if (do_remap && (r = atm_remap(ctx))) return r;
   return atm_dgrid_halo(ctx);
 }
@@ -1149,21 +1162,27 @@ int atm_adj_step_tape(atm_ctx* ctx, double dt, int do_remap, const void* tape) {
   if (r) return r;
   if (!tape) return ATM_ERR_ARG;
   const Geom& g = ctx->geo;
-  const size_t fb = field_bytes(ctx);
+  const size_t fb = field_bytes(ctx), lb = level_bytes(ctx);
   const char* t = (const char*)tape;
-  const void* cgf[4] = {t, t + fb, t + 2 * fb, t + 3 * fb};
-  const void* s1[4] = {t + 4 * fb, t + 5 * fb, t + 6 * fb, t + 7 * fb};
+  const void *cgf[4], *s1[4], *s0[4];
+  for (int i = 0; i < 4; ++i) {
+    cgf[i] = t + (TAPE_CG + i) * fb;
+    s1[i] = t + (TAPE_S1 + i) * fb;
+    s0[i] = t + (TAPE_S0 + i) * fb;
+  }
   {
     Stage st(ctx, S_AHALO);
     CK(atm::adj_ring_fold(g, slot_fields(ctx, ATM_ADJ_OUT), 4, ctx->L, ctx->stream));
   }
-  {  // pkapb, gzb of the D step from its new dp, pt
-    Stage st(ctx, S_AFWD, 2);
-    atm::Consts k = step_consts(ctx, dt);
-    CK(ctx->ops->column(g, k, s1[F_DP], s1[F_PT], ctx->ops->elem, ctx->pkap, ctx->gz, -2, 2, nullptr, ctx->stream));
-    CK(atm::corners(g, ctx->pkap, ctx->gz, ctx->pkapb, ctx->gzb, 1, 0, ctx->L, ctx->stream));
-  }
-  return adj_step_given(ctx, dt, do_remap, cgf, s1);
+  // the D step's pkapb, gzb are read from the tape for this reverse step
+  double* const pkapb = ctx->pkapb;
+  double* const gzb = ctx->gzb;
+  ctx->pkapb = (double*)(t + TAPE_FIELDS * fb);
+  ctx->gzb = (double*)(t + TAPE_FIELDS * fb + lb);
+  const int r2 = adj_step_given(ctx, dt, do_remap, s0, cgf, s1);
+  ctx->pkapb = pkapb;
+  ctx->gzb = gzb;
+  return r2;
 }
 
 int atm_state_bytes(atm_ctx* ctx, long long* bytes) {

@@ -241,9 +241,11 @@ int atm_adj_get_device(atm_ctx* ctx, int slot, int field, double* dev);
 int atm_adj_step(atm_ctx* ctx, double dt, int do_remap);
 /* the same with the step's forward products recorded by atm_step_tape
    instead of recomputed: atm_step_tape advances the state like atm_step
-   and writes the C-grid fields (after their halo) and the pre-remap state
-   into a device buffer of atm_tape_bytes bytes; atm_adj_step_tape reverses
-   that step from the restored state before it (atm_state_load) */
+   and writes the state before the step, the C-grid fields (after their
+   halo), the pre-remap state and the D step's corner pkap and gz into a
+   device buffer of atm_tape_bytes bytes; atm_adj_step_tape reverses that
+   step from the tape alone (the context's state is neither read nor
+   changed) */
 int atm_tape_bytes(atm_ctx* ctx, long long* bytes);
 int atm_step_tape(atm_ctx* ctx, double dt, int do_remap, void* tape);
 int atm_adj_step_tape(atm_ctx* ctx, double dt, int do_remap, const void* tape);
