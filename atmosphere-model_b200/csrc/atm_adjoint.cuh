@@ -1870,17 +1870,26 @@ __global__ void k_ring_copy_adj(Geom g, double* d0, double* d1, double* d2, doub
 // substitution, limited interface values), the same layer pairs are
 // visited, and the adjoints flow back to the source values and to both
 // coordinates.
+// The column arrays of the adjoint of vertical_ppm: the forward's lvs (after
+// the elimination), lvb (after the back substitution), lvc (limited) and
+// gam, and the adjoints.  The monotone path forms each layer's edges and
+// curvature on the fly (PPMLayers); RemapAdjFull also stores them, for the
+// all-pairs path of non-monotone coordinates.
 template <int LM>
 struct RemapAdjWork {
-  double gam[LM + 2], lvs[LM + 2], lvb[LM + 2], lvc[LM + 2], top[LM + 2], btm[LM + 2], curv[LM + 2];
+  double gam[LM + 2], lvs[LM + 2], lvb[LM + 2], lvc[LM + 2];
   double LL[LM + 2], Lgam[LM + 2], Ltop[LM + 2], Lbtm[LM + 2];
 };
-
-// vertical_ppm (src/mod_remap.f90:287-356) keeping lvs (after the
-// elimination), lvb (after the back substitution) and lvc (limited);
-// the operations are those of vertical_ppm in atm_kernels.cuh.
 template <int LM>
-__device__ void vppm_record(RemapAdjWork<LM>& w, int L, const double* var, const double* coord) {
+struct RemapAdjFull : RemapAdjWork<LM> {
+  double top[LM + 2], btm[LM + 2], curv[LM + 2];
+};
+
+// vertical_ppm (src/mod_remap.f90:287-356) keeping lvs, lvb, lvc, the
+// edges and the curvature; the operations are those of vertical_ppm in
+// atm_kernels.cuh.
+template <int LM>
+__device__ void vppm_record(RemapAdjFull<LM>& w, int L, const double* var, const double* coord) {
   double* gam = w.gam;
   double* lv = w.lvs;
   double alpha, beta;
@@ -2093,18 +2102,19 @@ __device__ void vppm_adj(RemapAdjWork<LM>& w, int L, const double* var, const do
   }
 }
 
-// adjoint of one pair's contribution (remap_pair): adds to Ltop/Lbtm (with
-// the curvature folded in), Lsrc, Lsc, Ldc
+// adjoint of one pair's contribution (remap_pair) given source layer k's
+// edges, curvature and value: adds to Ltop/Lbtm (with the curvature folded
+// in), Lsrc, Lsc, Ldc
 template <int LM>
-__device__ __forceinline__ void remap_pair_adj(RemapAdjWork<LM>& w, const double* src_var, double ldst, const double* sc,
-                                               const double* dc, int k, int m, double* Lsrc, double* Lsc, double* Ldc) {
+__device__ __forceinline__ void remap_pair_adj(RemapAdjWork<LM>& w, double btm, double top, double curv, double vk,
+                                               double ldst, const double* sc, const double* dc, int k, int m,
+                                               double* Lsrc, double* Lsc, double* Ldc) {
   const double dsrc = sc[k + 1] - sc[k];
   const double s1 = (dc[m] - sc[k]) / dsrc;
   const double s2 = (dc[m + 1] - sc[k]) / dsrc;
   const double ddst = dc[m + 1] - dc[m];
   const double IF = dsrc / ddst;
   const double tmp3 = 2. * s1 * s1;
-  const double btm = w.btm[k], top = w.top[k], curv = w.curv[k];
   double Ls1 = 0., Ls2 = 0., LIF = 0., Lb = 0., Lt = 0., Lcv = 0.;
   if (dc[m + 1] <= sc[k + 1] && sc[k + 1] < dc[m] && dc[m] < sc[k]) {
     const double t1 = s1 - 1., t2 = s1 + 1.;
@@ -2127,7 +2137,7 @@ __device__ __forceinline__ void remap_pair_adj(RemapAdjWork<LM>& w, const double
   }
   if (dc[m + 1] <= sc[k + 1] && sc[k] <= dc[m]) {
     Lsrc[k] += IF * ldst;
-    LIF += src_var[k] * ldst;
+    LIF += vk * ldst;
   }
   if (sc[k + 1] < dc[m + 1] && dc[m] < sc[k]) {
     const double t1 = s1 + s2;
@@ -2153,33 +2163,81 @@ __device__ __forceinline__ void remap_pair_adj(RemapAdjWork<LM>& w, const double
   Lsc[k + 1] += Ldsrc;
 }
 
-// Adjoint of remap_column: given the adjoint Ldst of the remapped values,
-// adds to Lsrc (source values), Lsc (source coordinate), Ldc (target).
+// All-pairs adjoint of remap_column for coordinates that are not monotone
+// (every source layer against every target layer, as the reference loops),
+// with its own column arrays.
 template <int LM>
-__device__ void remap_column_adj(RemapAdjWork<LM>& w, int L, const double* src_var, const double* Ldst, const double* sc,
-                                 const double* dc, double* Lsrc, double* Lsc, double* Ldc) {
+__device__ __noinline__ void remap_column_adj_full(int L, const double* src_var, const double* Ldst, const double* sc,
+                                                   const double* dc, double* Lsrc, double* Lsc, double* Ldc) {
+  RemapAdjFull<LM> w;
   vppm_record<LM>(w, L, src_var, sc);
   for (int k = 0; k <= L + 1; ++k) {
     w.Ltop[k] = 0.;
     w.Lbtm[k] = 0.;
   }
+  for (int k = 1; k <= L; ++k)
+    for (int m = 1; m <= L; ++m) {
+      if (sc[k + 1] >= dc[m] || sc[k] <= dc[m + 1] || Ldst[m] == 0.) continue;
+      remap_pair_adj<LM>(w, w.btm[k], w.top[k], w.curv[k], src_var[k], Ldst[m], sc, dc, k, m, Lsrc, Lsc, Ldc);
+    }
+  vppm_adj<LM>(w, L, src_var, sc, Lsrc, Lsc);
+}
+
+// Adjoint of remap_column: given the adjoint Ldst of the remapped values,
+// adds to Lsrc (source values), Lsc (source coordinate), Ldc (target).
+// Monotone coordinates (the usual case): the elimination of vertical_ppm
+// as the forward's streaming remap does it (ppm_eliminate), then the pairs
+// in the forward merge's order with each source layer's edges and curvature
+// formed as the merge reaches it (PPMLayers, which also yields the back
+// substituted and limited interface values the reverse of vertical_ppm
+// reads); the same operations as vertical_ppm, so the same values.
+template <int LM>
+__device__ void remap_column_adj(RemapAdjWork<LM>& w, int L, const double* src_var, const double* Ldst, const double* sc,
+                                 const double* dc, double* Lsrc, double* Lsc, double* Ldc) {
   bool mono = true;
   for (int k = 1; k <= L; ++k) mono = mono && (sc[k + 1] <= sc[k]) && (dc[k + 1] <= dc[k]);
-  if (mono) {
-    int k0 = 1;
-    for (int m = 1; m <= L; ++m) {
-      while (k0 <= L && sc[k0 + 1] >= dc[m]) ++k0;
-      if (Ldst[m] == 0.) continue;
-      for (int k = k0; k <= L && sc[k] > dc[m + 1]; ++k) remap_pair_adj<LM>(w, src_var, Ldst[m], sc, dc, k, m, Lsrc, Lsc, Ldc);
-    }
-  } else {
-    for (int k = 1; k <= L; ++k)
-      for (int m = 1; m <= L; ++m) {
-        if (sc[k + 1] >= dc[m] || sc[k] <= dc[m + 1] || Ldst[m] == 0.) continue;
-        remap_pair_adj<LM>(w, src_var, Ldst[m], sc, dc, k, m, Lsrc, Lsc, Ldc);
-      }
+  if (!mono) {
+    remap_column_adj_full<LM>(L, src_var, Ldst, sc, dc, Lsrc, Lsc, Ldc);
+    return;
   }
+  const ColArr csc{const_cast<double*>(sc), 1}, clv{w.lvs, 1}, cgam{w.gam, 1};
+  {
+    int kc = L + 2, kv = L + 1;
+    ppm_eliminate<false>(L, [&]() { return sc[--kc]; }, [&]() { return src_var[--kv]; }, csc, clv, cgam);
+  }
+  for (int k = 0; k <= L + 1; ++k) {
+    w.Ltop[k] = 0.;
+    w.Lbtm[k] = 0.;
+  }
+  auto var = [&](int k) { return src_var[k]; };
+  PPMLayers<decltype(var)> ly(clv, cgam, L, var);
+  w.lvb[1] = ly.lvf;
+  w.lvc[1] = ly.lvc;
+  auto advance = [&]() {  // to the next layer; its top interface values
+    ly.next();
+    w.lvb[ly.k + 1] = ly.lvf;
+    w.lvc[ly.k + 1] = ly.lvc;
+  };
+  int k0 = 1;
+  for (int m = 1; m <= L; ++m) {
+    while (k0 <= L && sc[k0 + 1] >= dc[m]) ++k0;
+    if (Ldst[m] == 0.) continue;
+    for (int k = k0; k <= L && sc[k] > dc[m + 1]; ++k) {
+      while (ly.k < k) advance();
+      remap_pair_adj<LM>(w, ly.btm, ly.top, ly.curv, ly.vk, Ldst[m], sc, dc, k, m, Lsrc, Lsc, Ldc);
+    }
+  }
+  while (ly.k < L) advance();
   vppm_adj<LM>(w, L, src_var, sc, Lsrc, Lsc);
+}
+
+// remap_column of the energy for coordinates that are not monotone, with
+// its own column arrays
+template <int LM>
+__device__ __noinline__ void remap_energy_pairs(int L, const double* en, double* er, const double* plev,
+                                                const double* tpl) {
+  PPMWork<LM> wf;
+  remap_column<LM>(wf, L, en, er, plev, tpl, nullptr, 1, nullptr);
 }
 
 // Adjoint of k_remap_energy (src/mod_remap.f90:42-78, 111-161) on the
@@ -2204,11 +2262,10 @@ __global__ void __launch_bounds__(64) k_remap_energy_adj(Geom g, RemapArgs ra, c
   const long long S = g.S;
   const long long o = g.at(i, j);
   const int P = g.P;
-  double plev[LM + 2], pk[LM + 2], tpl[LM + 2], tpk[LM + 2], gzv[LM + 2];
-  double en[LM + 2], er[LM + 2], ptr[LM + 2];
-  double Lplev[LM + 2], Ltpl[LM + 2], Lpk[LM + 2], Ltpk[LM + 2], Len[LM + 2], Ler[LM + 2];
+  double plev[LM + 2], pk[LM + 2], tpl[LM + 2], tpk[LM + 2];
+  double en[LM + 2], ptr[LM + 2];
+  double Lplev[LM + 2], Ltpl[LM + 2], Lpk[LM + 2], Ltpk[LM + 2], Ler[LM + 2];
   RemapAdjWork<LM> wk;
-  PPMWork<LM> wf;
   // ud = urem and vd = vrem (:156-161); the column's energy and pressure
   // adjoints are zero unless its new dp or pt carry an adjoint
   bool any = false;
@@ -2237,27 +2294,41 @@ __global__ void __launch_bounds__(64) k_remap_energy_adj(Geom g, RemapArgs ra, c
     double plog = atm_log(tpk[k + 1] / tpk[k]);
     tlyk[k] = (tpk[k + 1] - tpk[k]) / plog;
   }
-  gzv[1] = gzs[o];
-  for (int k = 1; k <= L; ++k) gzv[k + 1] = gzv[k] + CP_DRY * pt[o + (long long)(k - 1) * S] * (pk[k] - pk[k + 1]);
-  for (int k = 1; k <= L; ++k) {
-    long long ok = o + (long long)(k - 1) * S;
-    double ua = (.25 * (ud[ok] + ud[ok + P]) + .125 * (ud[ok - 1] + ud[ok - 1 + P] + ud[ok + 1] + ud[ok + 1 + P]));
-    double va = (.25 * (vd[ok] + vd[ok + 1]) + .125 * (vd[ok - P] + vd[ok + 1 - P] + vd[ok + P] + vd[ok + 1 + P]));
-    en[k] = CV_DRY * pt[ok] * lyk[k] + .5 * (gzv[k + 1] + gzv[k] + ua * ua + va * va);
-  }
-  remap_column<LM>(wf, L, en, er, plev, tpl, nullptr, 1, nullptr);
   {
-    double gzr = gzv[1];
+    double gz0 = gzs[o];  // gz(k), streamed upward
     for (int k = 1; k <= L; ++k) {
       long long ok = o + (long long)(k - 1) * S;
+      const double gz1 = gz0 + CP_DRY * pt[ok] * (pk[k] - pk[k + 1]);
+      double ua = (.25 * (ud[ok] + ud[ok + P]) + .125 * (ud[ok - 1] + ud[ok - 1 + P] + ud[ok + 1] + ud[ok + 1 + P]));
+      double va = (.25 * (vd[ok] + vd[ok + 1]) + .125 * (vd[ok - P] + vd[ok + 1 - P] + vd[ok + P] + vd[ok + 1 + P]));
+      en[k] = CV_DRY * pt[ok] * lyk[k] + .5 * (gz1 + gz0 + ua * ua + va * va);
+      gz0 = gz1;
+    }
+  }
+  {
+    // the remapped energy er(m), ascending, and the recovered pt (:127-150)
+    double gzr = gzs[o];
+    auto put = [&](int m, double erm) {
+      long long ok = o + (long long)(m - 1) * S;
       double ua = (.25 * (urem[ok] + urem[ok + P]) + .125 * (urem[ok - 1] + urem[ok - 1 + P] + urem[ok + 1] + urem[ok + 1 + P]));
       double va = (.25 * (vrem[ok] + vrem[ok + 1]) + .125 * (vrem[ok - P] + vrem[ok + 1 - P] + vrem[ok + P] + vrem[ok + 1 + P]));
-      ptr[k] = (er[k] - gzr - .5 * (ua * ua + va * va)) / (CV_DRY * tlyk[k] + .5 * CP_DRY * (tpk[k] - tpk[k + 1]));
-      gzr = gzr + CP_DRY * ptr[k] * (tpk[k] - tpk[k + 1]);
+      ptr[m] = (erm - gzr - .5 * (ua * ua + va * va)) / (CV_DRY * tlyk[m] + .5 * CP_DRY * (tpk[m] - tpk[m + 1]));
+      gzr = gzr + CP_DRY * ptr[m] * (tpk[m] - tpk[m + 1]);
+    };
+    bool mono = true;
+    for (int k = 1; k <= L; ++k) mono = mono && (plev[k + 1] <= plev[k]) && (tpl[k + 1] <= tpl[k]);
+    if (mono) {  // the forward's streaming remap (the energy kernel's path)
+      const ColArr cpl{plev, 1}, clv{wk.lvs, 1}, cgam{wk.gam, 1};
+      int kc = L + 2, kv = L + 1;
+      ppm_eliminate<false>(L, [&]() { return plev[--kc]; }, [&]() { return en[--kv]; }, cpl, clv, cgam);
+      remap_merge(L, cpl, clv, cgam, [&](int k) { return en[k]; }, [&](int k) { return tpl[k]; }, put, nullptr, 1);
+    } else {  // all pairs, into Ler as scratch (it is cleared below)
+      remap_energy_pairs<LM>(L, en, Ler, plev, tpl);
+      for (int m = 1; m <= L; ++m) put(m, Ler[m]);
     }
   }
   for (int k = 0; k <= L + 1; ++k) {
-    Lplev[k] = 0.; Ltpl[k] = 0.; Lpk[k] = 0.; Ltpk[k] = 0.; Len[k] = 0.; Ler[k] = 0.;
+    Lplev[k] = 0.; Ltpl[k] = 0.; Lpk[k] = 0.; Ltpk[k] = 0.; Ler[k] = 0.;
   }
   // outputs: dp = tpl(k) - tpl(k+1) (:156-161)
   for (int k = 1; k <= L; ++k) {
@@ -2330,7 +2401,7 @@ __global__ void __launch_bounds__(64) k_remap_energy_adj(Geom g, RemapArgs ra, c
       const double lg = log(pk[k + 1] / pk[k]);
       Lpk[k + 1] += ly * (1. - lyk[k] / pk[k + 1]) / lg;
       Lpk[k] += ly * (-1. + lyk[k] / pk[k]) / lg;
-      Len[k] = le;  // .5 (gz(k+1) + gz(k)) and the kinetic energy
+      // the adjoint of en(k) (Lsrc(k)) also reaches .5 (gz(k+1) + gz(k)) and the kinetic energy
       const double ua = (.25 * (ud[ok] + ud[ok + P]) + .125 * (ud[ok - 1] + ud[ok - 1 + P] + ud[ok + 1] + ud[ok + 1 + P]));
       const double va = (.25 * (vd[ok] + vd[ok + 1]) + .125 * (vd[ok - P] + vd[ok + 1 - P] + vd[ok + P] + vd[ok + 1 + P]));
       const double lu = ua * le, lv = va * le;
@@ -2355,8 +2426,8 @@ __global__ void __launch_bounds__(64) k_remap_energy_adj(Geom g, RemapArgs ra, c
     double lz = 0.;
     for (int k = L; k >= 1; --k) {
       long long ok = o + (long long)(k - 1) * S;
-      lz += .5 * Len[k];  // gz(k+1)
-      if (k + 1 <= L) lz += .5 * Len[k + 1];  // gz(k+1) is also the lower level of layer k+1
+      lz += .5 * Lsrc[k];  // gz(k+1)
+      if (k + 1 <= L) lz += .5 * Lsrc[k + 1];  // gz(k+1) is also the lower level of layer k+1
       Lpt[k] += CP_DRY * (pk[k] - pk[k + 1]) * lz;
       Lpk[k] += CP_DRY * pt[ok] * lz;
       Lpk[k + 1] -= CP_DRY * pt[ok] * lz;

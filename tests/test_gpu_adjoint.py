@@ -122,6 +122,27 @@ def test_remap_dot_product():
     assert rel(lhs, rhs) <= TOL, (lhs, rhs)
 
 
+def test_remap_dot_product_non_monotone_columns():
+    """Columns whose source pressure is not monotone (one layer of negative
+    thickness) take the all-pairs path of the remap and of its adjoint."""
+    st = generic_state(seed=6)
+    for j, i in ((3, 5), (10, 20), (17, 31)):
+        st.dp[2, j, i] = -0.3 * st.dp[2, j, i]
+    rng = np.random.default_rng(7)
+    g = Dycore(st)
+    g.adj_enable()
+    v = {n: rand(rng, st, n) for n in NAMES}
+    t = tlm_from_gpu(g, st, v)
+    t.remap()
+    w = {n: rand(rng, st, n) for n in NAMES}
+    lhs = sum(np.sum(w[n] * t.get(STATE[n], halo=True)[1]) for n in NAMES)
+    for n in NAMES:
+        g.adj_set('out', n, w[n])
+    g.adj_remap()
+    rhs = sum(np.sum(v[n] * g.adj_get('in', n)) for n in NAMES)
+    assert rel(lhs, rhs) <= TOL, (lhs, rhs)
+
+
 def test_halo_dot_products():
     st = generic_state(seed=6)
     rng = np.random.default_rng(7)
