@@ -124,7 +124,7 @@ cudaError_t d_mom(const Geom& g, const Consts& c, const void* ud, const void* vd
       (e = tmap(pkapb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpb)) || (e = tmap(gzb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgb)))
     return e;
   k_d_mom2<T, TX, TY_DMOM, S, C><<<tiles(0, 0, g, g.L, TY_DMOM), NT, Lay::bytes, s>>>(
-      mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c, (S*)udo, (S*)vdo, nonfinite, timeout);
+      mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c, (const S*)ud, (const S*)vd, (S*)udo, (S*)vdo, nonfinite, timeout);
   return cudaGetLastError();
 }
 

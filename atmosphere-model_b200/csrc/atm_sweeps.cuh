@@ -547,18 +547,33 @@ struct DMomL {
   static constexpr int WVL = tma_width<T>(TX + 5), HVL = TY + 1;     // vc layer nlay: x [ox-3, ox+TX+1], y [oy, oy+TY]
   static constexpr int WC = tma_width<T>(TX), HC = TY;               // uc, vc of the layer at the outputs
   static constexpr int WP = tma_width<double>(TX + 1), HP = TY + 1;  // pkapb, gzb
+  // all ten input boxes at once (the adjoint kernels' layouts)
   static constexpr uint32_t tx_bytes = (uint32_t)(2 * WU * HU * sizeof(S) +
                                                    (WUL * HUL + WVL * HVL + 2 * WC * HC) * sizeof(T) +
                                                    4 * WP * HP * sizeof(double));
-  // the state's ud, vd as sweep-type copies when the types differ
-  static constexpr size_t conv = std::is_same_v<S, T> ? 0 : 2 * box_bytes<T>(TX + 6, TY + 6);
   static constexpr size_t boxes = 2 * tma_box_bytes(WU, HU, sizeof(S)) + tma_box_bytes(WUL, HUL, sizeof(T)) +
                                   tma_box_bytes(WVL, HVL, sizeof(T)) + 2 * tma_box_bytes(WC, HC, sizeof(T)) +
                                   4 * tma_box_bytes(WP, HP, 8);
-  static constexpr size_t work =
-      box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 3, TY + 3) +
-      4 * box_bytes<T>(TX + 1, TY + 1) + box_bytes<T>(TX, TY + 5) + box_bytes<T>(TX + 5, TY) +
-      box_bytes<T>(TX + 1, TY + 1);
+  // The FP64 forward loads ud, vd and the C-grid winds first (tx_main) and
+  // the PGF boxes pkapb, gzb (tx_pgf) later, into the ud, vd boxes, which
+  // the stages after the kinetic energy do not read (its update reads the
+  // cell's ud, vd from global memory): 34 KB, 6 CTAs per SM instead of 5.
+  // The mixed form, at 6 CTAs by its registers already, loads all ten at once.
+  static constexpr bool LATE_PGF = std::is_same_v<S, T>;
+  static constexpr uint32_t tx_main =
+      (uint32_t)(2 * WU * HU * sizeof(S) + (WUL * HUL + WVL * HVL + 2 * WC * HC) * sizeof(T));
+  static constexpr uint32_t tx_pgf = (uint32_t)(4 * WP * HP * sizeof(double));
+  static constexpr size_t boxes_main = 2 * tma_box_bytes(WU, HU, sizeof(S)) + tma_box_bytes(WUL, HUL, sizeof(T)) +
+                                       tma_box_bytes(WVL, HVL, sizeof(T)) + 2 * tma_box_bytes(WC, HC, sizeof(T));
+  static_assert(4 * tma_box_bytes(WP, HP, 8) <= 2 * tma_box_bytes(WU, HU, sizeof(S)),
+                "the PGF boxes fit where the ud, vd boxes were");
+  // the state's ud, vd as sweep-type copies when the types differ
+  static constexpr size_t conv = std::is_same_v<S, T> ? 0 : 2 * box_bytes<T>(TX + 6, TY + 6);
+  // vor (later ke and dv4), dv0, dv2, tU, tV, lap
+  static_assert(2 * box_bytes<T>(TX + 1, TY + 1) <= box_bytes<T>(TX + 5, TY + 5), "ke, dv4 fit where vor was");
+  static constexpr size_t work = box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 5, TY + 5) +
+                                 box_bytes<T>(TX + 3, TY + 3) + box_bytes<T>(TX, TY + 5) + box_bytes<T>(TX + 5, TY) +
+                                 box_bytes<T>(TX + 1, TY + 1);
   // slopes of the KE sweeps, later of the vorticity-flux sweeps (one buffer)
   static constexpr size_t slopes_ke = box_bytes<T>(TX + 1, TY + 4) + box_bytes<T>(TX + 4, TY + 1);
   static constexpr size_t slopes_vf = box_bytes<T>(TX, TY + 3) + box_bytes<T>(TX + 3, TY);
@@ -567,7 +582,7 @@ struct DMomL {
   static constexpr size_t edges_ke = 2 * box_bytes<T>(TX + 1, TY + 2) + 2 * box_bytes<T>(TX + 2, TY + 1);
   static constexpr size_t edges_vf = 2 * box_bytes<T>(TX, TY + 1) + 2 * box_bytes<T>(TX + 1, TY);
   static constexpr size_t edges = edges_ke > edges_vf ? edges_ke : edges_vf;
-  static constexpr size_t bytes = boxes + conv + work + slopes + edges + 128;
+  static constexpr size_t bytes = (LATE_PGF ? boxes_main : boxes) + conv + work + slopes + edges + 128;
 };
 
 template <typename T, int TX, int TY, typename S = T, typename C = T>
@@ -579,11 +594,12 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
                                                const __grid_constant__ CUtensorMap m_vc,
                                                const __grid_constant__ CUtensorMap m_pkb,
                                                const __grid_constant__ CUtensorMap m_gzb, Geom g, Consts c,
+                                               const S* __restrict__ ud, const S* __restrict__ vd,
                                                S* __restrict__ udo, S* __restrict__ vdo, int* nonfinite,
                                                int* timeout) {
   using Lay = DMomL<T, TX, TY, S, C>;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar, bar_pgf;
   __shared__ int s_ok;
   unsigned char* p = smem_base(smem);
   const int k = blockIdx.z, L = g.L;
@@ -594,11 +610,6 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
   auto tbox = [&](int i0, int j0, int w, int h) {
     Sm<T> s{reinterpret_cast<T*>(p), tma_x0<T>(i0), j0, w};
     p += tma_box_bytes(w, h, sizeof(T));
-    return s;
-  };
-  auto dbox = [&](int i0, int j0, int w, int h) {
-    Sm<double> s{reinterpret_cast<double*>(p), tma_x0<double>(i0), j0, w};
-    p += tma_box_bytes(w, h, 8);
     return s;
   };
   auto sbox = [&](int i0, int j0, int w, int h) {
@@ -612,11 +623,25 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
   Sm<T> vcL = tbox(ox - 3, oy, Lay::WVL, Lay::HVL);
   Sm<T> suc = tbox(ox, oy, Lay::WC, Lay::HC);
   Sm<T> svc = tbox(ox, oy, Lay::WC, Lay::HC);
-  Sm<double> pb0 = dbox(ox, oy, Lay::WP, Lay::HP);
-  Sm<double> pb1 = dbox(ox, oy, Lay::WP, Lay::HP);
-  Sm<double> gb0 = dbox(ox, oy, Lay::WP, Lay::HP);
-  Sm<double> gb1 = dbox(ox, oy, Lay::WP, Lay::HP);
-  {
+  // the PGF boxes: in the ud, vd boxes, loaded later (FP64), or after the
+  // C-grid winds and loaded with the rest
+  unsigned char* pq = Lay::LATE_PGF ? reinterpret_cast<unsigned char*>(bud.p) : p;
+  auto qbox = [&]() {
+    Sm<double> s{reinterpret_cast<double*>(pq), tma_x0<double>(ox), oy, Lay::WP};
+    pq += tma_box_bytes(Lay::WP, Lay::HP, 8);
+    return s;
+  };
+  const Sm<double> pb0 = qbox();
+  const Sm<double> pb1 = qbox();
+  const Sm<double> gb0 = qbox();
+  const Sm<double> gb1 = qbox();
+  if constexpr (Lay::LATE_PGF) {
+    const TmaBox boxes[6] = {{&m_ud, bud.p, bud.x0, bud.y0, k},      {&m_vd, bvd.p, bvd.x0, bvd.y0, k},
+                             {&m_ucL, ucL.p, ucL.x0, ucL.y0, L - 1}, {&m_vcL, vcL.p, vcL.x0, vcL.y0, L - 1},
+                             {&m_uc, suc.p, suc.x0, suc.y0, k},      {&m_vc, svc.p, svc.x0, svc.y0, k}};
+    if (!tma_fetch(boxes, Lay::tx_main, &bar, timeout, &s_ok)) return;
+  } else {
+    p = pq;
     const TmaBox boxes[10] = {
         {&m_ud, bud.p, bud.x0, bud.y0, k},       {&m_vd, bvd.p, bvd.x0, bvd.y0, k},
         {&m_ucL, ucL.p, ucL.x0, ucL.y0, L - 1},  {&m_vcL, vcL.p, vcL.x0, vcL.y0, L - 1},
@@ -641,12 +666,12 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
     __syncthreads();
   }
   Sm<T> vor = carve<T>(p, ox - 3, oy - 3, TX + 5, TY + 5);
+  // ke and dv4 are written after the last read of vor (a __syncthreads apart)
+  unsigned char* pk = reinterpret_cast<unsigned char*>(vor.p);
+  Sm<T> ke = carve<T>(pk, ox, oy, TX + 1, TY + 1);
+  Sm<T> dv4 = carve<T>(pk, ox, oy, TX + 1, TY + 1);
   Sm<T> dv0 = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
   Sm<T> dv2 = carve<T>(p, ox - 1, oy - 1, TX + 3, TY + 3);
-  Sm<T> dv4 = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> ubL = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> vbL = carve<T>(p, ox, oy, TX + 1, TY + 1);
-  Sm<T> ke = carve<T>(p, ox, oy, TX + 1, TY + 1);
   Sm<T> tU = carve<T>(p, ox, oy - 3, TX, TY + 5);
   Sm<T> tV = carve<T>(p, ox - 3, oy, TX + 5, TY);
   Sm<T> lap = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
@@ -668,16 +693,11 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
   p += Lay::edges;
 
   const T f = T(c.coriolis);
-  // vorticity (:659-663), divergence (:682-685), layer-nlay B-grid winds (:441-444),
-  // slopes of the KE sweeps
+  // vorticity (:659-663), divergence (:682-685), slopes of the KE sweeps
   region<TX + 5, TY + 5>(ox - 3, oy - 3, [&](int x, int y) {
     vor(x, y) = f - (sud(x, y + 1) - sud(x, y)) * rdy + (svd(x + 1, y) - svd(x, y)) * rdx;
     int xd = x + 1, yd = y + 1;
     dv0(xd, yd) = rdx * (sud(xd, yd) - sud(xd - 1, yd)) + rdy * (svd(xd, yd) - svd(xd, yd - 1));
-  });
-  region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-    ubL(x, y) = T(.5) * (ucL(x, y) + ucL(x, y - 1));
-    vbL(x, y) = T(.5) * (vcL(x, y) + vcL(x - 1, y));
   });
   region<TX + 1, TY + 4>(ox, oy - 2, [&](int x, int y) { mvy(x, y) = slope_at(svd.ptr(x, y), WQ); });
   region<TX + 4, TY + 1>(ox - 2, oy, [&](int x, int y) { mux(x, y) = slope_at(sud.ptr(x, y), 1); });
@@ -719,13 +739,15 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
     lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 + (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
   });
   __syncthreads();
-  // kinetic energy with PPM_CONSTRAINED (:639-657), del^4 (:695-702),
-  // slopes of the vorticity-flux sweeps
+  // kinetic energy with PPM_CONSTRAINED (:639-657) and the layer-nlay
+  // B-grid winds (:441-444), del^4 (:695-702), slopes of the vorticity-flux sweeps
   region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
-    T fy = flux_con_pre<T>(svd.ptr(x, y), WQ, lvy.ptr(x, y), rvy.ptr(x, y), TX + 1, dtdy * vbL(x, y));
-    T kv = vbL(x, y) * fy;
-    T fx = flux_con_pre<T>(sud.ptr(x, y), 1, lux.ptr(x, y), rux.ptr(x, y), 1, dtdx * ubL(x, y));
-    ke(x, y) = T(.5) * (kv + ubL(x, y) * fx);
+    const T ubL = T(.5) * (ucL(x, y) + ucL(x, y - 1));
+    const T vbL = T(.5) * (vcL(x, y) + vcL(x - 1, y));
+    T fy = flux_con_pre<T>(svd.ptr(x, y), WQ, lvy.ptr(x, y), rvy.ptr(x, y), TX + 1, dtdy * vbL);
+    T kv = vbL * fy;
+    T fx = flux_con_pre<T>(sud.ptr(x, y), 1, lux.ptr(x, y), rux.ptr(x, y), 1, dtdx * ubL);
+    ke(x, y) = T(.5) * (kv + ubL * fx);
   });
   const T divdamp = T(c.divdamp);
   region<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
@@ -735,6 +757,11 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
   region<TX, TY + 3>(ox, oy - 2, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); });
   region<TX + 3, TY>(ox - 2, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); });
   __syncthreads();
+  if constexpr (Lay::LATE_PGF) {  // the ud, vd boxes are read no more: the PGF boxes go there
+    const TmaBox boxes[4] = {{&m_pkb, pb0.p, pb0.x0, pb0.y0, k}, {&m_pkb, pb1.p, pb1.x0, pb1.y0, k + 1},
+                             {&m_gzb, gb0.p, gb0.x0, gb0.y0, k}, {&m_gzb, gb1.p, gb1.x0, gb1.y0, k + 1}};
+    tma_issue(boxes, Lay::tx_pgf, &bar_pgf);
+  }
   region<TX, TY + 1>(ox, oy - 1, [&](int x, int y) {
     T eL, eR;
     edges_pre<T, PPM_CON>(tU.ptr(x, y), TX, mtU.ptr(x, y), TX, eL, eR);
@@ -747,9 +774,14 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
     ltV(x, y) = eL;
     rtV(x, y) = eR;
   });
-  __syncthreads();
+  if constexpr (Lay::LATE_PGF) {
+    if (!tma_wait(&bar_pgf, timeout, &s_ok)) return;
+  } else {
+    __syncthreads();
+  }
 
-  // ud, vd updates (:724-738, 755-769) with the B-grid PGF (:665-679)
+  // ud, vd updates (:724-738, 755-769) with the B-grid PGF (:665-679); the
+  // state's ud, vd of the cell from global memory (FP64) or its box
   const T vdx = T(c.vdx), vdy = T(c.vdy);
   bool bad = false;
   region<TX, TY>(ox, oy, [&](int x, int y) {
@@ -762,11 +794,12 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
                  (pb0(x, y + 1) - pb1(x, y) + pb0(x, y) - pb1(x, y + 1));
     T fy = flux_con_pre<T>(tU.ptr(x, y), TX, ltU.ptr(x, y), rtU.ptr(x, y), TX, dtdx * vcL(x, y));
     T fx = flux_con_pre<T>(tV.ptr(x, y), 1, ltV.ptr(x, y), rtV.ptr(x, y), 1, dtdx * ucL(x, y));
+    const long long o = g.at(x, y, k);
     S u, v;
     if constexpr (std::is_same_v<S, T>) {  // the reference's operations, in order
-      u = sud(x, y) + dt * (svc(x, y) * fy + vdy * (lap(x, y) - lap(x, y - 1))) -
+      u = ud[o] + dt * (svc(x, y) * fy + vdy * (lap(x, y) - lap(x, y - 1))) -
           dtdx * (ke(x + 1, y) - ke(x, y) - dv4(x + 1, y) + dv4(x, y) - T(pgx));
-      v = svd(x, y) - dt * (suc(x, y) * fx + vdx * (lap(x, y) - lap(x - 1, y))) -
+      v = vd[o] - dt * (suc(x, y) * fx + vdx * (lap(x, y) - lap(x - 1, y))) -
           dtdy * (ke(x, y + 1) - ke(x, y) - dv4(x, y + 1) + dv4(x, y) - T(pgy));
     } else {  // the tendency in the sweep type added to the state's type
       const T du = dt * (svc(x, y) * fy + vdy * (lap(x, y) - lap(x, y - 1))) -
@@ -776,7 +809,6 @@ __global__ void __launch_bounds__(NT) k_d_mom2(const __grid_constant__ CUtensorM
       u = bud(x, y) + S(du);
       v = bvd(x, y) + S(dv);
     }
-    long long o = g.at(x, y, k);
     udo[o] = u;
     vdo[o] = v;
     bad = bad || !(finite_(u) && finite_(v));

@@ -108,4 +108,34 @@ __device__ __forceinline__ bool tma_fetch(const TmaBox (&boxes)[N], uint32_t byt
   return *s_ok != 0;
 }
 
+// The same split in two, for boxes loaded into shared memory that the block
+// has finished reading (the caller synchronises the block before the
+// issue), so that the copies overlap the block's next stage: tma_issue
+// (thread 0 only) initialises bar and issues the boxes; tma_wait waits for
+// them as tma_fetch does.
+template <int N>
+__device__ __forceinline__ void tma_issue(const TmaBox (&boxes)[N], uint32_t bytes, uint64_t* bar) {
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    mbar_expect_tx(bar, bytes);
+#pragma unroll
+    for (int b = 0; b < N; ++b)
+      tma_load_3d(boxes[b].dst, boxes[b].map, boxes[b].i0 + H + XOFF, boxes[b].j0 + H, boxes[b].k, bar);
+  }
+}
+__device__ __forceinline__ bool tma_wait(uint64_t* bar, int* timeout_flag, int* s_ok) {
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    bool ok = mbar_wait(bar, 0, 1000000);  // about one second at most
+    if (!ok) {
+      if (timeout_flag) atomicOr(timeout_flag, 1);
+      mbar_wait(bar, 0, 1000000);
+    }
+    *s_ok = ok ? 1 : 0;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
 }  // namespace atm

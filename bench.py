@@ -239,6 +239,16 @@ def run_ours(args):
             n += 1
             return dy.step(DT, remap=(n % REMAP_EVERY == 0), check_stable=True)
 
+        # every kernel of the step, the remap's included, launches once before
+        # the warm-up (first-launch costs such as module loading stay out of
+        # the timed region whatever W is): one step with remap from a saved
+        # copy of the state, which is then restored
+        saved = torch.empty(dy.state_bytes() // 8, dtype=torch.float64, device='cuda')
+        dy.state_save(saved.data_ptr())
+        dy.step(DT, remap=True, check_stable=False)
+        dy.state_load(saved.data_ptr())
+        dy.sync()
+        del saved
         for _ in range(W):
             one()
         barrier()
