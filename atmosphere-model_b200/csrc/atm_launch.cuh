@@ -106,8 +106,8 @@ cudaError_t c_mom(const Geom& g, const Consts& c, const void* ud, const void* vd
       (e = tmap(ud, es, g, g.L, Lay::WL, Lay::HL, &muL)) || (e = tmap(vd, es, g, g.L, Lay::WL, Lay::HL, &mvL)) ||
       (e = tmap(pkap, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpk)) || (e = tmap(gz, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgz)))
     return e;
-  k_c_mom2<T, TX, TY_CMOM, S, C><<<tiles(0, 0, g, g.L, TY_CMOM), NT, Lay::bytes, s>>>(mu, mv, muL, mvL, mpk, mgz, g,
-                                                                                      c, (C*)uc, (C*)vc, timeout);
+  k_c_mom2<T, TX, TY_CMOM, S, C><<<tiles(0, 0, g, g.L, TY_CMOM), NT, Lay::bytes, s>>>(
+      mu, mv, muL, mvL, mpk, mgz, g, c, (const S*)ud, (const S*)vd, (C*)uc, (C*)vc, timeout);
   return cudaGetLastError();
 }
 

@@ -376,10 +376,25 @@ struct CMomL {
   static constexpr int WV = tma_width<S>(TX + 7), HV = TY + 7;   // vd box x in [ox-3, ox+TX+3]
   static constexpr int WL = tma_width<S>(TX + 3), HL = TY + 3;   // layer-nlay ud, vd
   static constexpr int WP = tma_width<double>(TX + 1), HP = TY + 1;  // pkap, gz at k and k+1
+  // all eight input boxes at once (the adjoint kernel's layout)
   static constexpr uint32_t tx_bytes =
       (uint32_t)((WU * HU + WV * HV + 2 * WL * HL) * sizeof(S) + 4 * WP * HP * sizeof(double));
   static constexpr size_t boxes = tma_box_bytes(WU, HU, sizeof(S)) + tma_box_bytes(WV, HV, sizeof(S)) +
                                   2 * tma_box_bytes(WL, HL, sizeof(S)) + 4 * tma_box_bytes(WP, HP, 8);
+  // The forward loads ud, vd and the layer-nlay winds first (tx_main) and
+  // the PGF boxes pkap, gz (tx_pgf) after the kinetic-energy stage, three
+  // into the ud, vd boxes and one into the layer-nlay ud box, which no later
+  // stage reads (the update reads the cell's ud, vd from global memory);
+  // the Laplacian of the vorticity is formed a stage later, into the
+  // layer-nlay vd box.
+  static constexpr uint32_t tx_main = (uint32_t)((WU * HU + WV * HV + 2 * WL * HL) * sizeof(S));
+  static constexpr uint32_t tx_pgf = (uint32_t)(4 * WP * HP * sizeof(double));
+  static constexpr size_t boxes_main = tma_box_bytes(WU, HU, sizeof(S)) + tma_box_bytes(WV, HV, sizeof(S)) +
+                                       2 * tma_box_bytes(WL, HL, sizeof(S));
+  static_assert(3 * tma_box_bytes(WP, HP, 8) <= tma_box_bytes(WU, HU, sizeof(S)) + tma_box_bytes(WV, HV, sizeof(S)),
+                "three PGF boxes fit where the ud, vd boxes were");
+  static_assert(tma_box_bytes(WP, HP, 8) <= tma_box_bytes(WL, HL, sizeof(S)), "one PGF box fits in a layer-nlay box");
+  static_assert(box_bytes<T>(TX + 1, TY + 1) <= tma_box_bytes(WL, HL, sizeof(S)), "lap fits in a layer-nlay box");
   // slopes of the KE sweeps, later of the vorticity-flux sweeps (one buffer)
   static constexpr size_t slopes_ke = box_bytes<T>(TX + 1, TY + 4) + box_bytes<T>(TX + 4, TY + 1);
   static constexpr size_t slopes_vf = box_bytes<T>(TX, TY + 3) + box_bytes<T>(TX + 3, TY);
@@ -387,8 +402,8 @@ struct CMomL {
   static constexpr size_t work = 2 * box_bytes<T>(TX + 6, TY + 6) +                  // uc1, vc1
                                  box_bytes<T>(TX + 5, TY + 5) + box_bytes<T>(TX + 1, TY + 1) +  // vor, ke
                                  box_bytes<T>(TX, TY + 5) + box_bytes<T>(TX + 5, TY) +  // tU, tV
-                                 box_bytes<T>(TX + 1, TY + 1) + slopes;               // lap, slopes
-  static constexpr size_t bytes = boxes + work + 128;
+                                 slopes;                                              // slopes
+  static constexpr size_t bytes = boxes_main + work + 128;
 };
 
 // The layer-nlay A-grid winds at (x, y) from the layer-nlay D-grid winds
@@ -410,10 +425,11 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
                                                const __grid_constant__ CUtensorMap m_vdL,
                                                const __grid_constant__ CUtensorMap m_pk,
                                                const __grid_constant__ CUtensorMap m_gz, Geom g, Consts c,
+                                               const S* __restrict__ ud, const S* __restrict__ vd,
                                                C* __restrict__ uc, C* __restrict__ vc, int* timeout) {
   using Lay = CMomL<T, TX, TY, S>;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar, bar_pgf;
   __shared__ int s_ok;
   unsigned char* p = smem_base(smem);
   const int k = blockIdx.z, L = g.L;
@@ -426,34 +442,41 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
     p += tma_box_bytes(w, h, sizeof(S));
     return s;
   };
-  auto dbox = [&](int i0, int j0, int w, int h) {
-    Sm<double> s{reinterpret_cast<double*>(p), tma_x0<double>(i0), j0, w};
-    p += tma_box_bytes(w, h, 8);
-    return s;
-  };
   Sm<S> bud = tbox(ox - 4, oy - 3, Lay::WU, Lay::HU);
   Sm<S> bvd = tbox(ox - 3, oy - 4, Lay::WV, Lay::HV);
   Sm<S> budL = tbox(ox - 2, oy - 2, Lay::WL, Lay::HL);
   Sm<S> bvdL = tbox(ox - 2, oy - 2, Lay::WL, Lay::HL);
   const SmAs<S, T> sud{bud}, svd{bvd}, udL{budL}, vdL{bvdL};
-  Sm<double> pk0 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
-  Sm<double> pk1 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
-  Sm<double> gz0 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
-  Sm<double> gz1 = dbox(ox - 1, oy - 1, Lay::WP, Lay::HP);
   {
-    const TmaBox boxes[8] = {{&m_ud, bud.p, bud.x0, bud.y0, k},     {&m_vd, bvd.p, bvd.x0, bvd.y0, k},
-                             {&m_udL, budL.p, budL.x0, budL.y0, L - 1}, {&m_vdL, bvdL.p, bvdL.x0, bvdL.y0, L - 1},
-                             {&m_pk, pk0.p, pk0.x0, pk0.y0, k},      {&m_pk, pk1.p, pk1.x0, pk1.y0, k + 1},
-                             {&m_gz, gz0.p, gz0.x0, gz0.y0, k},      {&m_gz, gz1.p, gz1.x0, gz1.y0, k + 1}};
-    if (!tma_fetch(boxes, Lay::tx_bytes, &bar, timeout, &s_ok)) return;
+    const TmaBox boxes[4] = {{&m_ud, bud.p, bud.x0, bud.y0, k},
+                             {&m_vd, bvd.p, bvd.x0, bvd.y0, k},
+                             {&m_udL, budL.p, budL.x0, budL.y0, L - 1},
+                             {&m_vdL, bvdL.p, bvdL.x0, bvdL.y0, L - 1}};
+    if (!tma_fetch(boxes, Lay::tx_main, &bar, timeout, &s_ok)) return;
   }
+  // the PGF boxes, loaded after the kinetic energy: three where ud, vd
+  // were, one where the layer-nlay ud was
+  unsigned char* pq = reinterpret_cast<unsigned char*>(bud.p);
+  auto qbox = [&](unsigned char*& q) {
+    Sm<double> s{reinterpret_cast<double*>(q), tma_x0<double>(ox - 1), oy - 1, Lay::WP};
+    q += tma_box_bytes(Lay::WP, Lay::HP, 8);
+    return s;
+  };
+  const Sm<double> pk0 = qbox(pq);
+  const Sm<double> pk1 = qbox(pq);
+  const Sm<double> gz0 = qbox(pq);
+  unsigned char* pl = reinterpret_cast<unsigned char*>(budL.p);
+  const Sm<double> gz1 = qbox(pl);
+  // the Laplacian of the vorticity, formed after the kinetic energy, where
+  // the layer-nlay vd was
+  unsigned char* plap = reinterpret_cast<unsigned char*>(bvdL.p);
+  Sm<T> lap = carve<T>(plap, ox, oy, TX + 1, TY + 1);
   Sm<T> uc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
   Sm<T> vc1 = carve<T>(p, ox - 3, oy - 3, TX + 6, TY + 6);
   Sm<T> vor = carve<T>(p, ox - 2, oy - 2, TX + 5, TY + 5);
   Sm<T> ke = carve<T>(p, ox - 1, oy - 1, TX + 1, TY + 1);
   Sm<T> tU = carve<T>(p, ox, oy - 2, TX, TY + 5);
   Sm<T> tV = carve<T>(p, ox - 2, oy, TX + 5, TY);
-  Sm<T> lap = carve<T>(p, ox, oy, TX + 1, TY + 1);
   // the KE sweeps' slopes are dead before the vorticity-flux sweeps' ones
   // are written (a __syncthreads apart): they share memory
   unsigned char* ps = p;
@@ -506,15 +529,20 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
     T f0 = (c0 > T(0)) ? vor(x, y - 1) : vor(x, y);
     T f1 = (c1 > T(0)) ? vor(x, y) : vor(x, y + 1);
     tV(x, y) = T(.5) * (vor(x, y) + den * (vor(x, y) - rA * (f1 - f0)));
-  }),
+  }));
+  __syncthreads();
+  {  // ud, vd and the layer-nlay winds are read no more: the PGF boxes go there
+    const TmaBox boxes[4] = {{&m_pk, pk0.p, pk0.x0, pk0.y0, k}, {&m_pk, pk1.p, pk1.x0, pk1.y0, k + 1},
+                             {&m_gz, gz0.p, gz0.x0, gz0.y0, k}, {&m_gz, gz1.p, gz1.x0, gz1.y0, k + 1}};
+    tma_issue(boxes, Lay::tx_pgf, &bar_pgf);
+  }
+  regions(reg<TX, TY + 3>(ox, oy - 1, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); }),
+          reg<TX + 3, TY>(ox - 1, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); }),
           reg<TX + 1, TY + 1>(ox, oy, [&](int x, int y) {
     lap(x, y) = T(-2.) * vor(x, y) * rdxy + (vor(x + 1, y) + vor(x - 1, y)) * rdx2 +
                 (vor(x, y + 1) + vor(x, y - 1)) * rdy2;
   }));
-  __syncthreads();
-  regions(reg<TX, TY + 3>(ox, oy - 1, [&](int x, int y) { mtU(x, y) = slope_at(tU.ptr(x, y), TX); }),
-          reg<TX + 3, TY>(ox - 1, oy, [&](int x, int y) { mtV(x, y) = slope_at(tV.ptr(x, y), 1); }));
-  __syncthreads();
+  if (!tma_wait(&bar_pgf, timeout, &s_ok)) return;
 
   // uc, vc updates (:369-381, 399-411) with the PGF (:325-339)
   const T vdx = T(c.vdx), vdy = T(c.vdy);
@@ -526,13 +554,14 @@ __global__ void __launch_bounds__(NT) k_c_mom2(const __grid_constant__ CUtensorM
     double pgy = ((pk0(x, y) - pk1(x, y - 1)) * (gz0(x, y - 1) - gz1(x, y)) +
                   (pk0(x, y - 1) - pk1(x, y)) * (gz1(x, y - 1) - gz0(x, y))) /
                  (pk0(x, y) - pk1(x, y - 1) + pk0(x, y - 1) - pk1(x, y));
-    T fy = flux_pre<T, PPM_UNC>(tU.ptr(x, y + 1), TX, mtU.ptr(x, y + 1), TX, dtdx * svd(x, y));
-    T u = uc1(x, y) + dt * (svd(x, y) * fy + vdy * (lap(x, y + 1) - lap(x, y))) -
+    const long long o = g.at(x, y, k);
+    const T udx = T(ud[o]), vdx_ = T(vd[o]);  // the cell's ud, vd (their boxes hold the PGF now)
+    T fy = flux_pre<T, PPM_UNC>(tU.ptr(x, y + 1), TX, mtU.ptr(x, y + 1), TX, dtdx * vdx_);
+    T u = uc1(x, y) + dt * (vdx_ * fy + vdy * (lap(x, y + 1) - lap(x, y))) -
           dtdx * (ke(x, y) - ke(x - 1, y) - T(pgx));
-    T fx = flux_pre<T, PPM_UNC>(tV.ptr(x + 1, y), 1, mtV.ptr(x + 1, y), 1, dtdx * sud(x, y));
-    T v = vc1(x, y) - dt * (sud(x, y) * fx + vdx * (lap(x + 1, y) - lap(x, y))) -
+    T fx = flux_pre<T, PPM_UNC>(tV.ptr(x + 1, y), 1, mtV.ptr(x + 1, y), 1, dtdx * udx);
+    T v = vc1(x, y) - dt * (udx * fx + vdx * (lap(x + 1, y) - lap(x, y))) -
           dtdy * (ke(x, y) - ke(x, y - 1) - T(pgy));
-    long long o = g.at(x, y, k);
     uc[o] = C(u);
     vc[o] = C(v);
   });
