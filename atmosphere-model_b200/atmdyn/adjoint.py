@@ -57,13 +57,19 @@ def _download(dyn: Dycore, like):
     return outs
 
 
-def _record(dyn: Dycore, dt: float, remaps, like):
+def _record(dyn: Dycore, dt: float, remaps, like, final_state: bool = True):
     """Steps from the context's current state keeping, per step, its tape
-    (the initial state and the forward products the adjoint step reads)."""
+    (the initial state and the forward products the adjoint step reads).
+    Without ``final_state`` the last step stops before its remap: its tape
+    holds the pre-remap state the remap's adjoint needs (the adjoint step
+    is told separately that the step remapped), and the remapped state
+    itself, the segment's output, is not wanted (a backward's recompute)."""
     tapes = []
-    for r in remaps:
+    n = len(remaps)
+    for i, r in enumerate(remaps):
         tp = torch.empty(dyn.tape_bytes() // 8, dtype=torch.float64, device=like.device)
-        dyn.step_tape(dt, bool(r), tp.data_ptr())
+        remap = bool(r) and (final_state or i + 1 < n)
+        dyn.step_tape(dt, remap, tp.data_ptr())
         tapes.append(tp)
     return tapes
 
@@ -105,7 +111,7 @@ class DycoreSegment(torch.autograd.Function):
             # recompute the segment, keeping every step's tape (initial
             # state, C-grid fields, pre-remap state, corner pkap and gz)
             dyn.state_load(ckpt.data_ptr())
-            tapes = _record(dyn, dt, remaps, ckpt)
+            tapes = _record(dyn, dt, remaps, ckpt, final_state=False)
         dyn.adj_zero()
         grads = [g if g is not None else torch.zeros_like(ckpt[:0]) for g in (gdp, gpt, gud, gvd)]
         for name, g in zip(FIELD_NAMES, grads):
