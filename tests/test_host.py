@@ -123,3 +123,35 @@ def test_ensemble_balance():
     loads = [sum(s for s, k in zip(sizes, b) if k == j) for j in range(3)]
     assert max(loads) <= sum(sizes) / 3 + max(sizes)
     assert b[1] != b[5]  # the two largest members run on different streams
+
+
+class _TapeRecorder:
+    """Stands in for a Dycore in the tape recording of atmdyn.adjoint."""
+
+    def __init__(self):
+        self.calls = []
+
+    def tape_bytes(self):
+        return 64
+
+    def step_tape(self, dt, remap, ptr):
+        self.calls.append(bool(remap))
+
+
+def test_recompute_stops_before_the_last_remap_only():
+    """A backward's recompute (final_state=False) skips the remap of the
+    segment's last step only, whose tape already holds the pre-remap state;
+    the forward's recording keeps every remap (its final state is the
+    segment's output)."""
+    torch = pytest.importorskip('torch')
+    from atmdyn.adjoint import _record
+    like = torch.zeros(1, dtype=torch.float64)
+    remaps = [False, True, False, True]
+    for final_state, want in ((True, remaps), (False, [False, True, False, False])):
+        dyn = _TapeRecorder()
+        tapes = _record(dyn, 30.0, remaps, like, final_state=final_state)
+        assert dyn.calls == want
+        assert len(tapes) == len(remaps) and all(t.numel() == 8 for t in tapes)
+    dyn = _TapeRecorder()
+    _record(dyn, 30.0, [False, False], like, final_state=False)
+    assert dyn.calls == [False, False]
