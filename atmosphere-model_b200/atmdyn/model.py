@@ -88,7 +88,8 @@ class RunResult:
 
 
 def run_model(stepper, tc: TimeControl, max_steps: int | None = None,
-              on_step=None, accumulate=None, write=None, physics: bool = False) -> RunResult:
+              on_step=None, accumulate=None, write=None, physics: bool = False,
+              before_remap=None) -> RunResult:
     """``run_model`` (mod_model.f90:112-193) without radiation: each step is
     [physics tendencies when due], C-grid half step, halo, D-grid step,
     [apply the physics tendencies], remap if due, halo, [physics halo],
@@ -96,7 +97,9 @@ def run_model(stepper, tc: TimeControl, max_steps: int | None = None,
     the schedule says so, ``write(time_stamp)`` (write_output, stamped
     .5 (previous_write_time + time) as the reference does).  The bracketed
     physics calls run when ``physics`` is true; the net flux (radiation)
-    is whatever the caller set (zero by default)."""
+    is whatever the caller set (zero by default).  ``before_remap(n)``, when
+    given, runs just before the remap of step n (the tests arm the remap's
+    pair trace there)."""
     sch = Schedule(tc)
     time = tc.t_initial
     n = 0
@@ -116,6 +119,8 @@ def run_model(stepper, tc: TimeControl, max_steps: int | None = None,
         if physics:
             stepper.apply_physics(dt)
         if sch.remap_this_step:
+            if before_remap is not None:
+                before_remap(n)
             stepper.remap()
             sch.remap_this_step = False
             remaps.append(n)

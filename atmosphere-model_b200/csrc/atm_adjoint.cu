@@ -40,7 +40,7 @@ cudaError_t adj_setup() {
 cudaError_t adj_mass(const Geom& g, const Consts& c, const double* dp, const double* pt, const double* u,
                      const double* v, const double* dpo, const double* pto, const double* lam_dpo,
                      const double* lam_pto, double* lam_dp, double* lam_pt, double* lam_u, double* lam_v, int lo,
-                     int hi, int* timeout, bool cgrid, cudaStream_t s) {
+                     int hi, int* timeout, bool cgrid, cudaStream_t s, int parts) {
   CUtensorMap md, mp, mu, mv;
   cudaError_t e;
   if (cgrid) {  // one kernel (the update recomputed from the fluxes)
@@ -59,11 +59,13 @@ cudaError_t adj_mass(const Geom& g, const Consts& c, const double* dp, const dou
         (e = tmap(u, 8, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(v, 8, g, g.L, Lay::WV, Lay::HV, &mv)))
       return e;
     const dim3 grid = tiles_a(lo, hi, g, TYA);
-    k_mass_adj<TXA, TYA, false, true><<<grid, NTA, bytes, s>>>(md, mp, mu, mv, g, c, dpo, pto, lam_dpo, lam_pto,
-                                                                lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
+    if (parts & 1)
+      k_mass_adj<TXA, TYA, false, true><<<grid, NTA, bytes, s>>>(md, mp, mu, mv, g, c, dpo, pto, lam_dpo, lam_pto,
+                                                                  lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_mass_adj<TXA, TYA, false, false><<<grid, NTA, bytes, s>>>(md, mp, mu, mv, g, c, dpo, pto, lam_dpo, lam_pto,
-                                                                 lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
+    if (parts & 2)
+      k_mass_adj<TXA, TYA, false, false><<<grid, NTA, bytes, s>>>(md, mp, mu, mv, g, c, dpo, pto, lam_dpo, lam_pto,
+                                                                   lam_dp, lam_pt, lam_u, lam_v, lo, hi, timeout);
   }
   return cudaGetLastError();
 }
@@ -86,7 +88,7 @@ cudaError_t adj_c_mom(const Geom& g, const Consts& c, const double* ud, const do
 cudaError_t adj_d_mom(const Geom& g, const Consts& c, const double* ud, const double* vd, const double* uc,
                       const double* vc, const double* pkapb, const double* gzb, const double* lam_udo,
                       const double* lam_vdo, double* lam_ud, double* lam_vd, double* lam_uc, double* lam_vc,
-                      double* lam_pkb, double* lam_gzb, int* timeout, cudaStream_t s) {
+                      double* lam_pkb, double* lam_gzb, int* timeout, cudaStream_t s, int parts) {
   using Lay = DMomL<double, TXA, TYM>;
   CUtensorMap mu, mv, muL, mvL, muc, mvc, mpb, mgb;
   cudaError_t e;
@@ -97,12 +99,14 @@ cudaError_t adj_d_mom(const Geom& g, const Consts& c, const double* ud, const do
     return e;
   // the kinetic-energy chain and the rest, both adding into the same
   // global adjoints
-  k_d_mom_adj_ke<TXA, TYM><<<tiles_a(0, 0, g, TYM), NTA, DMomKeAdjL<TXA, TYM>::bytes, s>>>(
-      mu, mv, muL, mvL, g, c, lam_udo, lam_vdo, lam_ud, lam_vd, lam_uc, lam_vc, timeout);
+  if (parts & 1)
+    k_d_mom_adj_ke<TXA, TYM><<<tiles_a(0, 0, g, TYM), NTA, DMomKeAdjL<TXA, TYM>::bytes, s>>>(
+        mu, mv, muL, mvL, g, c, lam_udo, lam_vdo, lam_ud, lam_vd, lam_uc, lam_vc, timeout);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_d_mom_adj_vf<TXA, TYM><<<tiles_a(0, 0, g, TYM), NTA, DMomVfAdjL<TXA, TYM>::bytes, s>>>(
-      mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c, lam_udo, lam_vdo, lam_ud, lam_vd, lam_uc, lam_vc, lam_pkb, lam_gzb,
-      timeout);
+  if (parts & 2)
+    k_d_mom_adj_vf<TXA, TYM><<<tiles_a(0, 0, g, TYM), NTA, DMomVfAdjL<TXA, TYM>::bytes, s>>>(
+        mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c, lam_udo, lam_vdo, lam_ud, lam_vd, lam_uc, lam_vc, lam_pkb,
+        lam_gzb, timeout);
   return cudaGetLastError();
 }
 

@@ -210,13 +210,13 @@ cudaError_t d2h_pitched(atm_ctx* c, double* host, const double* dev, int K) {
 const char* const STAGE_NAMES[] = {"c_mass",  "c_column", "c_mom",        "c_halo",      "d_ring",
                                    "d_mass",  "d_column", "d_corners",    "d_mom",       "remap_ring",
                                    "remap_winds", "remap_energy", "d_halo", "heating", "check",
-                                   "adj_forward", "adj_remap", "adj_d_mom", "adj_d_column", "adj_d_mass",
+                                   "adj_forward", "adj_remap", "adj_d_mom_ke", "adj_d_column", "adj_d_mass_x",
                                    "adj_c_column", "adj_c_mom", "adj_c_mass", "adj_halo",
-                                   "phys_tend", "phys_apply", "phys_halo"};
-constexpr int NSTAGE = 27;
+                                   "phys_tend", "phys_apply", "phys_halo", "adj_d_mom_vf", "adj_d_mass_y"};
+constexpr int NSTAGE = 29;
 enum { S_CMASS, S_CCOL, S_CMOM, S_CHALO, S_DRING, S_DMASS, S_DCOL, S_DCORN, S_DMOM, S_RRING, S_RWIND, S_RENER,
        S_DHALO, S_HEAT, S_CHECK, S_AFWD, S_ARMP, S_ADMOM, S_ADCOL, S_ADMASS, S_ACCOL, S_ACMOM, S_ACMASS, S_AHALO,
-       S_PHYS_TEND, S_PHYS_APPLY, S_PHYS_HALO };
+       S_PHYS_TEND, S_PHYS_APPLY, S_PHYS_HALO, S_ADMOM_VF, S_ADMASS_Y };
 
 // Brackets one stage (one kernel launch unless noted) with CUDA events on
 // the context's stream when profiling is on, and counts the launch.
@@ -886,22 +886,25 @@ int adj_d(atm_ctx* ctx, double dt, const void* const* so, const void* const* sn,
   CK(cudaMemsetAsync(ctx->lam_gz, 0, lev, ctx->stream));
   CK(cudaMemsetAsync(ctx->lam_pkb, 0, lev, ctx->stream));
   CK(cudaMemsetAsync(ctx->lam_gzb, 0, lev, ctx->stream));
-  {
-    Stage t(ctx, S_ADMOM, 2);
+  // the kinetic-energy chain and the rest of the D-momentum reverse, each
+  // its own kernel and profiled stage
+  for (int part = 1; part <= 2; ++part) {
+    Stage t(ctx, part == 1 ? S_ADMOM : S_ADMOM_VF);
     CK(atm::adj_d_mom(g, k, o[F_UD], o[F_VD], cg[C_UC], cg[C_VC], ctx->pkapb, ctx->gzb, lout[F_UD], lout[F_VD],
                       lin[F_UD], lin[F_VD], ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], ctx->lam_pkb, ctx->lam_gzb,
-                      &ctx->status->tma_timeout, ctx->stream));
+                      &ctx->status->tma_timeout, ctx->stream, part));
   }
   {
     Stage t(ctx, S_ADCOL, 2);
     CK(atm::adj_corners(g, ctx->lam_pkb, ctx->lam_gzb, ctx->lam_pk, ctx->lam_gz, ctx->stream));
     CK(atm::adj_column(g, k, n[F_DP], n[F_PT], ctx->lam_pk, ctx->lam_gz, lout[F_DP], lout[F_PT], -2, 2, ctx->stream));
   }
-  {
-    Stage t(ctx, S_ADMASS, 2);
+  // the x and the y branch of the D-grid mass reverse
+  for (int part = 1; part <= 2; ++part) {
+    Stage t(ctx, part == 1 ? S_ADMASS : S_ADMASS_Y);
     CK(atm::adj_mass(g, k, o[F_DP], o[F_PT], cg[C_UC], cg[C_VC], n[F_DP], n[F_PT], lout[F_DP], lout[F_PT], lin[F_DP],
-                     lin[F_PT],
-                     ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], -3, 3, &ctx->status->tma_timeout, false, ctx->stream));
+                     lin[F_PT], ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], -3, 3, &ctx->status->tma_timeout, false,
+                     ctx->stream, part));
   }
   {
     Stage t(ctx, S_AHALO);

@@ -63,7 +63,8 @@ cudaError_t launch(const atm::Geom& g, const atm::RemapArgs& ra, const double* d
 
 extern "C" int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, const double* bk, const double* dp,
                                  const double* pt, const double* ud, const double* vd, const double* gzs,
-                                 double* dp_out, double* pt_out, double* ud_out, double* vd_out, void* stream) {
+                                 double* dp_out, double* pt_out, double* ud_out, double* vd_out, void* stream,
+                                 int* stable, int* fallback_columns) {
   if (nx < atm::H || ny < atm::H || nlay < 3 || nlay > atm::MAX_LAYERS || !ak || !bk || !dp || !pt || !ud || !vd ||
       !gzs || !dp_out || !pt_out || !ud_out || !vd_out)
     return ATM_ERR_ARG;
@@ -113,5 +114,15 @@ extern "C" int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, con
   else
     e = launch<atm::MAX_LAYERS>(g, ra, dp - o, pt - o, ud - o, vd - o, gzs - o, urem - o, vrem - o, dp_out - o,
                                 pt_out - o, ud_out - o, vd_out - o, st, s);
-  return e == cudaSuccess ? ATM_OK : ATM_ERR_CUDA;
+  if (e != cudaSuccess) return ATM_ERR_CUDA;
+  if (!stable && !fallback_columns) return ATM_OK;
+  // the report: wait for the remap, then read the status words the kernels
+  // raised (into a stack copy: nothing is allocated)
+  atm::Status h{};
+  if (cudaMemcpyAsync(&h, st, sizeof(atm::Status), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return ATM_ERR_CUDA;
+  if (stable) *stable = h.nonfinite_remap ? 0 : 1;
+  if (fallback_columns) *fallback_columns = h.fallback_pairs;
+  return ATM_OK;
 }

@@ -63,18 +63,20 @@ cudaError_t device_wait_timeout(int max_polls, int* flag, cudaStream_t);
 // ---- FP64 adjoint (atm_adjoint.cu); lam_* are adjoint fields laid out like
 // the fields they belong to, accumulated with +=
 cudaError_t adj_setup();
-// dpo, pto: the new dp and pt the forward sweep wrote
+// dpo, pto: the new dp and pt the forward sweep wrote; parts (D grid): 1
+// the x branch, 2 the y branch, 3 both (the C grid is one kernel)
 cudaError_t adj_mass(const Geom&, const Consts&, const double* dp, const double* pt, const double* u, const double* v,
                      const double* dpo, const double* pto, const double* lam_dpo, const double* lam_pto, double* lam_dp,
                      double* lam_pt, double* lam_u, double* lam_v, int lo, int hi, int* timeout, bool cgrid,
-                     cudaStream_t);
+                     cudaStream_t, int parts = 3);
 cudaError_t adj_c_mom(const Geom&, const Consts&, const double* ud, const double* vd, const double* pkap,
                       const double* gz, const double* lam_uc, const double* lam_vc, double* lam_ud, double* lam_vd,
                       double* lam_pk, double* lam_gz, int* timeout, cudaStream_t);
+// parts: 1 the kinetic-energy chain, 2 the rest, 3 both
 cudaError_t adj_d_mom(const Geom&, const Consts&, const double* ud, const double* vd, const double* uc,
                       const double* vc, const double* pkapb, const double* gzb, const double* lam_udo,
                       const double* lam_vdo, double* lam_ud, double* lam_vd, double* lam_uc, double* lam_vc,
-                      double* lam_pkb, double* lam_gzb, int* timeout, cudaStream_t);
+                      double* lam_pkb, double* lam_gzb, int* timeout, cudaStream_t, int parts = 3);
 cudaError_t adj_column(const Geom&, const Consts&, const double* dp, const double* pt, const double* lam_pk,
                        const double* lam_gz, double* lam_dp, double* lam_pt, int lo, int hi, cudaStream_t);
 cudaError_t adj_corners(const Geom&, const double* lam_pkb, const double* lam_gzb, double* lam_pk, double* lam_gz,

@@ -1,28 +1,32 @@
 #!/usr/bin/env python
-"""Throughput of the dynamical-core step on B200: cell-steps/s.
+"""Throughput of the dynamical-core step and its gradient on B200:
+cell-steps/s of forward + adjoint.
 
 One step is one model step of run_model (src/mod_model.f90:146-177): the
 C-grid half step, its halo fill, the D-grid step, the vertical remap when
-due (every 8 steps) and the D-grid halo fill, then the stability check.
-One cell-step is one interior (i, j, k) cell advanced by one such step.
+due (every 8 steps) and the D-grid halo fill.  One cell-step is one
+interior (i, j, k) cell advanced by one such step.
 
 Workload: the seeded zonal-jet case at 1024 x 1024 x 64 (dx = 25 km,
 dt = 30 s, remap every 8 steps), synthetic data from atmdyn.ic.jet_case.
-The headline ``value`` is the FP64 form (the reference's arithmetic,
-bit-identical to the FP64 restatement); the mixed-precision form is
-measured on the same workload and reported under ``forms``, and the
-gradient (forward with checkpoints + hand-written adjoint, through the
-torch.autograd binding) under ``adjoint``: fwd+adjoint cell-steps/s on the
-same workload, the backward/forward time ratio, and the finite-difference
-check of the 512 x 512 x 32 differentiation case.
+The headline ``value`` is forward + adjoint of the FP64 form through the
+torch.autograd binding: K steps forward with checkpoints every 8 steps,
+J = sum(theta^2) over the final state (every tile of the adjoint active),
+and the hand-written adjoint back to the initial state, per (K cells x
+steps) / (forward + backward time).  Beside it: the FP64 and mixed forward
+forms (``forms``), the masked loss of the differentiation case and its
+finite-difference check (``adjoint``), the batched ensemble, the column
+physics, and CPU baselines of the reference algorithm (the FP64
+restatement: forward plus its tangent-linear model, which stands in for a
+reverse pass since the reference has no derivative code).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 With N > 1 (torchrun) every rank advances its own replica of the domain
 (the path shards, but one domain fits one GPU; replicas only) and the time
 is the maximum over ranks.  ``--impl reference`` times the reference's CPU
-algorithm (the FP64 restatement) on the host cores, on a 256 x 256 x 64
-sample of the same case.
+algorithm (the FP64 restatement, forward + tangent-linear pass) on the
+host cores, on a 256 x 256 x 64 sample of the same case.
 """
 from __future__ import annotations
 
@@ -77,7 +81,7 @@ def kernel_bytes(stage, form, cells):
 
 # DRAM bytes per interior cell and launch measured by ncu on the FP64 form
 # (dram__bytes_read.sum + dram__bytes_write.sum, jet 512x512x32, scaled by
-# cells; the profile summary in profiles/ gives the command)
+# cells)
 TRAFFIC_PER_CELL_FP64 = {'c_mass': 48.3, 'c_mom': 48.3, 'd_mass': 48.4, 'd_mom': 66.2, 'c_column': 31.4,
                          'd_column': 31.4}
 
@@ -145,33 +149,62 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_sample_throughput(steps, warmup, threads):
-    """The FP64 restatement of the reference on the host cores."""
+def cpu_grad_throughput(n, steps, warmup, threads):
+    """The FP64 restatement of the reference on the host cores, on the jet
+    case at n x n x NLAY (remap every REMAP_EVERY steps, counted from the
+    first warm-up step): ``steps`` steps of the forward and ``steps`` steps
+    of its tangent-linear model (dual numbers: the forward values and one
+    directional derivative), after ``warmup`` untimed steps of each.  The
+    reference has no derivative code; one tangent-linear pass stands in for
+    the reverse pass of the GPU's forward + adjoint.  Returns the forward +
+    derivative rate and the forward-only rate, cell-steps/s."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import pyoracle
     from atmdyn import ic
-    st = ic.jet_case(SAMPLE_N, SAMPLE_N, NLAY, 25e3, 25e3, seed=0)
+    st = ic.jet_case(n, n, NLAY, 25e3, 25e3, seed=0)
+    rng = np.random.default_rng(0)
     o = pyoracle.OracleModel(st, threads=threads)
-    n = 0
+    tl = pyoracle.TLMModel(st, {'pt': rng.normal(0, 1e-3, st.pt.shape)}, threads=threads)
 
-    def one():
-        nonlocal n
-        n += 1
-        o.cgrid_step(DT / 2.)
-        o.cgrid_halo()
-        o.dgrid_step(DT)
-        if n % REMAP_EVERY == 0:
-            o.remap()
-        o.dgrid_halo()
-        return o.check_stability()
+    def run(m, first, count):
+        for q in range(first, first + count):
+            m.cgrid_step(DT / 2.)
+            m.cgrid_halo()
+            m.dgrid_step(DT)
+            if (q + 1) % REMAP_EVERY == 0:
+                m.remap()
+            m.dgrid_halo()
+        assert m.check_stability()
 
-    for _ in range(warmup):
-        one()
+    run(o, 0, warmup)
+    run(tl, 0, warmup)
     t0 = time.perf_counter()
-    for _ in range(steps):
-        one()
-    t = time.perf_counter() - t0
-    return st.cells * steps / t, t
+    run(o, warmup, steps)
+    tf = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    run(tl, warmup, steps)
+    tt = time.perf_counter() - t0
+    remaps = sum(1 for q in range(warmup, warmup + steps) if (q + 1) % REMAP_EVERY == 0)
+    return {'value': st.cells * steps / (tf + tt), 'forward_only': st.cells * steps / tf,
+            'forward_s': tf, 'tangent_linear_s': tt, 'remaps': remaps}
+
+
+def cpu_baseline_lines(steps, warmup):
+    """All host cores on the 256^2 sample (the reference arm's workload) and
+    one core on a 128^2 sample (8 steps with one remap)."""
+    threads = len(os.sched_getaffinity(0))
+    a = cpu_grad_throughput(SAMPLE_N, steps, warmup, threads)
+    one = cpu_grad_throughput(SAMPLE_N // 2, REMAP_EVERY, 1, 1)
+    out = {'value': a['value'], 'unit': 'cell-steps/s', 'cores': threads, 'kind': 'port',
+           'sample': 'jet %dx%dx%d, %d steps forward + %d steps tangent-linear (%d remaps) after %d warm-up each' % (
+               SAMPLE_N, SAMPLE_N, NLAY, steps, steps, a['remaps'], warmup),
+           'forward_only': a['forward_only'],
+           'single_core': {'value': one['value'], 'unit': 'cell-steps/s', 'cores': 1, 'kind': 'port',
+                           'forward_only': one['forward_only'],
+                           'sample': 'jet %dx%dx%d, %d steps forward + %d tangent-linear (%d remap) after 1 '
+                                     'warm-up each' % (SAMPLE_N // 2, SAMPLE_N // 2, NLAY, REMAP_EVERY,
+                                                       REMAP_EVERY, one['remaps'])}}
+    return out
 
 
 def run_reference(args):
@@ -180,17 +213,21 @@ def run_reference(args):
         return
     threads = len(os.sched_getaffinity(0))
     steps, warmup = args.steps, args.warmup
-    v, t = cpu_sample_throughput(steps, warmup, threads)
+    r = cpu_grad_throughput(SAMPLE_N, steps, warmup, threads)
+    v = r['value']
     line = {
         'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'cell-steps/s', 'n_gpus': args.gpus,
-        'steps': steps, 'warmup': warmup, 'ms_per_step': 1000 * t / steps, 'higher_is_better': True,
-        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+        'steps': steps, 'warmup': warmup, 'ms_per_step': 1000 * (r['forward_s'] + r['tangent_linear_s']) / steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
         'data': 'synthetic (seeded jet case)',
-        'config': {'workload': 'jet case, the reference algorithm on the host cores, sample %dx%dx%d per step' % (
-            SAMPLE_N, SAMPLE_N, NLAY), 'nx': SAMPLE_N, 'ny': SAMPLE_N, 'nlay': NLAY, 'remap_every': REMAP_EVERY},
+        'config': {'workload': 'jet case, forward + derivative pass of the reference algorithm on the host cores, '
+                               'sample %dx%dx%d per step' % (SAMPLE_N, SAMPLE_N, NLAY),
+                   'nx': SAMPLE_N, 'ny': SAMPLE_N, 'nlay': NLAY, 'remap_every': REMAP_EVERY},
         'cpu_baseline': {'value': v, 'unit': 'cell-steps/s', 'cores': threads, 'kind': 'port',
-                         'sample': 'jet %dx%dx%d, %d steps after %d warm-up (1/16 of the 1024^2 domain)' % (
-                             SAMPLE_N, SAMPLE_N, NLAY, steps, warmup)},
+                         'sample': 'jet %dx%dx%d, %d steps forward + %d steps tangent-linear (%d remaps) after %d '
+                                   'warm-up each (1/16 of the 1024^2 domain)' % (
+                                       SAMPLE_N, SAMPLE_N, NLAY, steps, steps, r['remaps'], warmup),
+                         'forward_only': r['forward_only']},
         'e2e': {'value': v, 'unit': 'cell-steps/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
     print(json.dumps(line), flush=True)
@@ -292,6 +329,7 @@ def run_ours(args):
         del dy
         torch.cuda.empty_cache()
 
+    grad = grad_leg(args, torch, barrier, max_over_ranks, world, peak, peak_kind)
     adjoint = None if args.no_adjoint else adjoint_leg(args, torch, max_over_ranks, world)
     ensemble = None if (args.no_ensemble or world > 1) else ensemble_leg(args, torch)
     physics = None if args.no_physics else physics_leg(args, torch, max_over_ranks, world, peak, peak_kind)
@@ -309,36 +347,40 @@ def run_ours(args):
         return
     f64 = results['fp64'] if 'fp64' in results else next(iter(results.values()))
     mixed = results.get('mixed') if 'fp64' in results else None
-    dom = max(f64['kernels'].items(), key=lambda kv: kv[1]['ms_avg'] * kv[1]['launches'])
-    dom_name, dom_k = dom
-    achieved = dom_k.get('gbs', 0.0)
+    # the forward's dominant kernel, for the forward forms' own roofline
+    fdom_name, fdom_k = max(f64['kernels'].items(), key=lambda kv: kv[1]['ms_avg'] * kv[1]['launches'])
+    fwd_roofline = {'bound': 'hbm', 'kernel': fdom_name, 'achieved': fdom_k.get('gbs', 0.0), 'peak': peak,
+                    'unit': 'GB/s', 'frac': fdom_k.get('gbs', 0.0) / peak, 'peak_kind': peak_kind,
+                    'traffic': (TRAFFIC_PER_CELL_FP64[fdom_name] * cells if fdom_name in TRAFFIC_PER_CELL_FP64
+                                else None)}
     line = {
-        'metric': METRIC, 'value': f64['value'], 'unit': 'cell-steps/s', 'n_gpus': world, 'steps': K, 'warmup': W,
-        'ms_per_step': f64['ms_per_step'], 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'metric': METRIC, 'value': grad['value'], 'unit': 'cell-steps/s', 'n_gpus': world, 'steps': K, 'warmup': W,
+        'ms_per_step': grad['ms_per_step'], 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f64', 'data': 'synthetic (seeded jet case, atmdyn.ic.jet_case)',
-        'config': {'workload': 'jet %dx%dx%d, dx=25 km, dt=30 s, remap every %d steps, FP64 form' % (
-            args.nx, args.nx, args.nlay, REMAP_EVERY), 'nx': args.nx, 'ny': args.nx, 'nlay': args.nlay,
-            'remap_every': REMAP_EVERY,
-            'l2': 'inputs larger than L2 (each prognostic field is 552 MB)',
-            'parallelism': 'replicas' if world > 1 else 'single GPU'},
-        'roofline': {'bound': 'hbm', 'kernel': dom_name, 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                     'frac': achieved / peak, 'peak_kind': peak_kind,
-                     'traffic': (TRAFFIC_PER_CELL_FP64[dom_name] * cells if dom_name in TRAFFIC_PER_CELL_FP64
-                                 else None),
-                     'traffic_unit': 'bytes per launch (ncu DRAM read + write per cell, scaled by cells)',
-                     'note': 'the FP64 sweeps are bound by instruction issue, not HBM (ncu: issue 54-68 %, '
-                             'FP64 pipe 32-44 %, DRAM traffic = algorithmic bytes)'},
-        'e2e': f64.get('e2e'),
-        'e2e_resident': f64.get('e2e_resident'),
-        'gpu_launches': f64['gpu_launches'],
-        'clocks': clocks,
-        'kernels': f64['kernels'],
+        'config': {'workload': 'jet %dx%dx%d, dx=25 km, dt=30 s, remap every %d steps, FP64 form: %d steps forward '
+                               '(checkpoints every %d) + adjoint of J = sum(theta^2) at the final step' % (
+                                   args.nx, args.nx, args.nlay, REMAP_EVERY, K, ADJ_CKPT),
+                   'nx': args.nx, 'ny': args.nx, 'nlay': args.nlay, 'remap_every': REMAP_EVERY,
+                   'checkpoint_every': ADJ_CKPT,
+                   'l2': 'inputs larger than L2 (each prognostic field is 552 MB)',
+                   'parallelism': 'replicas' if world > 1 else 'single GPU'},
+        'roofline': grad['roofline'],
+        'e2e': grad['e2e'],
+        'gpu_launches': grad['gpu_launches'],
+        'clocks': grad['clocks'],
+        'kernels': grad['kernels'],
+        'forward_ms': grad['forward_ms'], 'backward_ms': grad['backward_ms'],
+        'backward_over_forward': grad['backward_ms'] / grad['forward_ms'],
         'forms': {
-            'fp64': {'value': f64['value'], 'ms_per_step': f64['ms_per_step'], 'stable': f64['stable']},
+            'fp64': {'value': f64['value'], 'unit': 'cell-steps/s (forward)', 'ms_per_step': f64['ms_per_step'],
+                     'stable': f64['stable'], 'roofline': fwd_roofline, 'kernels': f64['kernels'],
+                     'e2e': f64.get('e2e'), 'e2e_resident': f64.get('e2e_resident'),
+                     'gpu_launches': f64['gpu_launches'], 'clocks': clocks},
         },
     }
     if mixed:
-        line['forms']['mixed'] = {'value': mixed['value'], 'ms_per_step': mixed['ms_per_step'],
+        line['forms']['mixed'] = {'value': mixed['value'], 'unit': 'cell-steps/s (forward)',
+                                  'ms_per_step': mixed['ms_per_step'],
                                   'stable': mixed['stable'], 'speedup_vs_fp64': mixed['value'] / f64['value'],
                                   'err_vs_fp64_after_%d_steps' % (K + W): err, 'kernels': mixed['kernels']}
     if adjoint is not None:
@@ -348,11 +390,7 @@ def run_ours(args):
     if physics is not None:
         line['physics'] = physics
     if world == 1 and not args.no_cpu:
-        threads = len(os.sched_getaffinity(0))
-        v, t = cpu_sample_throughput(max(2, REMAP_EVERY // 2), 1, threads)
-        line['cpu_baseline'] = {'value': v, 'unit': 'cell-steps/s', 'cores': threads, 'kind': 'port',
-                                'sample': 'jet %dx%dx%d, %d steps after 1 warm-up (1/16 of the domain)' % (
-                                    SAMPLE_N, SAMPLE_N, NLAY, max(2, REMAP_EVERY // 2))}
+        line['cpu_baseline'] = cpu_baseline_lines(K, W)
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -430,10 +468,141 @@ def physics_leg(args, torch, max_over_ranks, world, peak, peak_kind):
     return out
 
 
+# Algorithmic HBM words per interior cell and launch of the adjoint
+# kernels: the forward inputs the kernel recomputes from, the output
+# adjoints it reads, and a read and a write of every adjoint it adds into
+# (layer-nlay slabs excluded, as for the forward).
+ADJ_WORDS = {
+    'adj_c_mass': 14,    # dp, pt, ud, vd; lam dpc, ptc; += lam dp, pt, ud, vd
+    'adj_c_mom': 14,     # ud, vd, pkap, gz; lam uc, vc; += lam ud, vd, pkap, gz
+    'adj_d_mom_ke': 8,   # ud, vd; lam ud, vd (out); += lam ud, vd (in)
+    'adj_d_mom_vf': 20,  # ud, vd, uc, vc, pkapb, gzb; lam ud, vd (out); += lam ud, vd, uc, vc, pkapb, gzb
+    'adj_d_mass_x': 16,  # dp, pt, uc, vc, new dp, pt; lam dp, pt (out); += lam dp, pt, uc, vc
+    'adj_d_mass_y': 16,
+}
+# DRAM bytes per interior cell and launch of the adjoint kernels measured by
+# ncu (dram__bytes_read.sum + dram__bytes_write.sum, dense adjoint of the
+# jet at 512x512x32, scaled by cells)
+TRAFFIC_PER_CELL_ADJ = {}
+
+
+def grad_leg(args, torch, barrier, max_over_ranks, world, peak, peak_kind):
+    """The headline: the gradient of J = sum(theta^2) over the final state
+    (theta = pt p0**kappa) with respect to the initial dp, pt, ud, vd,
+    through atmdyn.adjoint.integrate (FP64 form, checkpoints every ADJ_CKPT
+    steps, the last segment's tapes recorded by its forward).  W steps of
+    forward + adjoint untimed, then exactly K steps timed (forward and
+    backward separately, CUDA events on torch's current stream, which the
+    library is bound to); one more identical pass with per-launch events for
+    the per-kernel breakdown and the roofline of the dominant kernel; one
+    pass end to end from and to pinned host memory."""
+    from atmdyn import ic, Dycore
+    from atmdyn.adjoint import integrate
+    K, W = args.steps, args.warmup
+    st = ic.jet_case(args.nx, args.nx, args.nlay, 25e3, 25e3, seed=0)
+    st.dt = DT
+    cells = st.cells
+    dyn = Dycore(st)
+    dyn.adj_enable()
+    inputs = [torch.tensor(np.ascontiguousarray(a), device='cuda') for a in (st.dp, st.pt, st.u, st.v)]
+
+    def fwd_bwd(nsteps, x, events=None):
+        if events:
+            events[0].record()
+        y = integrate(dyn, x, nsteps, DT, REMAP_EVERY, ADJ_CKPT)
+        J = ((y[1] * P0K) ** 2).sum()
+        if events:
+            events[1].record()
+        J.backward()
+        if events:
+            events[2].record()
+        return J
+
+    def fresh():
+        return [t.clone().requires_grad_(True) for t in inputs]
+
+    fwd_bwd(W, fresh())  # warm-up: W steps forward + adjoint
+    torch.cuda.synchronize()
+    x = fresh()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    barrier()
+    l0 = dyn.launch_count()
+    clk = Clocks()
+    J = fwd_bwd(K, x, ev)
+    barrier()
+    clocks = clk.stop()
+    launches = dyn.launch_count() - l0
+    tf = max_over_ranks(ev[0].elapsed_time(ev[1]))
+    tb = max_over_ranks(ev[1].elapsed_time(ev[2]))
+    gnorm = float(sum(float(xx.grad.norm()) ** 2 for xx in x) ** .5)
+    # the same pass with per-launch events (stage breakdown, roofline)
+    del x
+    x = fresh()
+    torch.cuda.synchronize()
+    dyn.profile(True)
+    fwd_bwd(K, x)
+    torch.cuda.synchronize()
+    prof = dyn.profile_read()
+    dyn.profile(False)
+    del x
+    kern = {}
+    for stage, (tms, cnt) in prof.items():
+        if cnt == 0:
+            continue
+        avg = tms / cnt
+        kern[stage] = {'ms_avg': round(avg, 4), 'launches': cnt, 'share': round(tms / max(tf + tb, 1e-9), 4)}
+        words = ADJ_WORDS.get(stage)
+        b = words * 8 * cells if words else kernel_bytes(stage, 'fp64', cells)
+        if b:
+            kern[stage]['algorithmic_bytes'] = b
+            kern[stage]['gbs'] = round(b / (avg * 1e-3) / 1e9, 1)
+    # dominant kernel: the single-kernel stage with the largest total time
+    single = {k: v for k, v in kern.items() if k in ADJ_WORDS or k in WORDS}
+    dom_name, dom = max(single.items(), key=lambda kv: kv[1]['ms_avg'] * kv[1]['launches'])
+    achieved = dom.get('gbs', 0.0)
+    roofline = {'bound': 'hbm', 'kernel': dom_name, 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                'frac': achieved / peak, 'peak_kind': peak_kind,
+                'traffic': (TRAFFIC_PER_CELL_ADJ[dom_name] * cells if dom_name in TRAFFIC_PER_CELL_ADJ else
+                            TRAFFIC_PER_CELL_FP64[dom_name] * cells if dom_name in TRAFFIC_PER_CELL_FP64 else None),
+                'traffic_unit': 'bytes per launch (ncu DRAM read + write per cell, scaled by cells)',
+                'algorithmic_bytes_per_launch': dom.get('algorithmic_bytes'),
+                'ms_per_launch': dom['ms_avg'], 'launches': dom['launches']}
+    # end to end: the inputs from pinned host memory, the loss and the four
+    # gradients back to pinned host memory, inside the timed region
+    host_in = [torch.empty(t.shape, dtype=torch.float64, pin_memory=True) for t in inputs]
+    host_out = [torch.empty(t.shape, dtype=torch.float64, pin_memory=True) for t in inputs]
+    for h, t in zip(host_in, inputs):
+        h.copy_(t)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record()
+    x = [torch.empty_like(t).copy_(h, non_blocking=True).requires_grad_(True) for t, h in zip(inputs, host_in)]
+    J2 = fwd_bwd(K, x)
+    for h, xx in zip(host_out, x):
+        h.copy_(xx.grad, non_blocking=True)
+    j_host = J2.item()
+    e1.record()
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    nbytes = sum(h.numel() * 8 for h in host_in)
+    e2e = {'value': world * cells * K / (ms_e2e * 1e-3), 'unit': 'cell-steps/s', 'h2d_bytes_per_step': nbytes / K,
+           'd2h_bytes_per_step': (nbytes + 8) / K, 'steps': K,
+           'how': 'one pass of K steps: dp, pt, ud, vd copied from pinned host memory, forward + adjoint through '
+                  'atmdyn.adjoint.integrate, J and the four gradients copied back to pinned host memory',
+           'same_gradient_as_device_timed': bool(abs(j_host - J.item()) <= 1e-12 * abs(J.item()))}
+    dyn.close()
+    del dyn, x, J, J2
+    torch.cuda.empty_cache()
+    return {'value': world * cells * K / ((tf + tb) * 1e-3), 'ms_per_step': (tf + tb) / K, 'forward_ms': tf,
+            'backward_ms': tb, 'gpu_launches': launches, 'clocks': clocks, 'kernels': kern, 'roofline': roofline,
+            'e2e': e2e, 'grad_norm': gnorm}
+
+
 def adjoint_leg(args, torch, max_over_ranks, world):
-    """fwd+adjoint through atmdyn.adjoint.integrate (checkpoints every
-    ADJ_CKPT steps, tapes within a segment) on the headline workload, and
-    the finite-difference check of the differentiation case: 512 x 512 x 32
+    """fwd+adjoint through atmdyn.adjoint.integrate with the masked loss of
+    the differentiation case on the headline workload, and the timing and
+    finite-difference check of the differentiation case itself: 512 x 512 x 32
     jet (seed 2), 20 steps, checkpoints every 5, J = sum(mask theta^2) at
     the final step with a 300 km Gaussian mask at mid-domain, central
     differences with eps = 1e-6 along 8 seeded random unit directions."""
@@ -487,37 +656,23 @@ def adjoint_leg(args, torch, max_over_ranks, world):
                 best = (tf, tb, None, dyn.launch_count() - l0, clocks)
         return dyn, x, final_theta, mask, J, best
 
-    # headline workload
+    # the headline workload with the masked loss of the differentiation case
+    # (a loss over a sub-domain: tiles outside its domain of dependence skip)
     st = ic.jet_case(args.nx, args.nx, args.nlay, 25e3, 25e3, seed=0)
     st.dt = DT
-    nsteps = args.adj_steps
+    nsteps = args.steps
     try:
-        dyn, x, _, _, J, (tf, tb, prof, launches, clocks) = timed(st, nsteps, REMAP_EVERY, ADJ_CKPT, 2,
-                                                                  dense=args.adj_dense)
+        dyn, x, _, _, J, (tf, tb, prof, launches, clocks) = timed(st, nsteps, REMAP_EVERY, ADJ_CKPT, 1)
         cells = st.cells
-        out['value'] = world * cells * nsteps / ((tf + tb) * 1e-3)
-        out['unit'] = 'cell-steps/s (forward + adjoint)'
-        out['workload'] = 'jet %dx%dx%d, %d steps, remap every %d, checkpoints every %d, J = sum(%stheta^2)' % (
-            args.nx, args.nx, args.nlay, nsteps, REMAP_EVERY, ADJ_CKPT, '' if args.adj_dense else 'mask ')
-        out['forward_ms'] = tf
-        out['backward_ms'] = tb
-        out['backward_over_forward'] = tb / tf
-        out['stages_ms'] = prof
-        out['gpu_launches'] = launches
-        out['clocks'] = clocks
+        out['masked_loss'] = {
+            'value': world * cells * nsteps / ((tf + tb) * 1e-3), 'unit': 'cell-steps/s (forward + adjoint)',
+            'workload': 'jet %dx%dx%d, %d steps, remap every %d, checkpoints every %d, J = sum(mask theta^2), '
+                        '300 km Gaussian mask' % (args.nx, args.nx, args.nlay, nsteps, REMAP_EVERY, ADJ_CKPT),
+            'forward_ms': tf, 'backward_ms': tb, 'backward_over_forward': tb / tf, 'stages_ms': prof,
+            'gpu_launches': launches, 'clocks': clocks}
         dyn.close()
         del dyn, x, J
         torch.cuda.empty_cache()
-        if not args.adj_dense:
-            # the same run with an unmasked loss: no tile of the adjoint is zero
-            dyn, x, _, _, J, (tf, tb, prof, launches, clocks) = timed(st, nsteps, REMAP_EVERY, ADJ_CKPT, 1,
-                                                                      dense=True)
-            out['dense_loss'] = {'J': 'sum(theta^2) over the domain', 'forward_ms': tf, 'backward_ms': tb,
-                                 'backward_over_forward': tb / tf,
-                                 'value': world * st.cells * nsteps / ((tf + tb) * 1e-3), 'stages_ms': prof,
-                                 'clocks': clocks}
-            dyn.close()
-            del dyn, x, J
     except Exception as e:  # e.g. the tapes do not fit
         out['error'] = repr(e)[:300]
     torch.cuda.empty_cache()
@@ -721,13 +876,11 @@ def main():
     ap.add_argument('--nlay', type=int, default=NLAY)
     ap.add_argument('--forms', default='fp64,mixed')
     ap.add_argument('--no-e2e', action='store_true')
-    ap.add_argument('--no-adjoint', action='store_true', help='skip the forward + adjoint leg')
-    ap.add_argument('--adj-steps', type=int, default=16, help='steps of the timed forward + adjoint run')
+    ap.add_argument('--no-adjoint', action='store_true',
+                    help='skip the masked-loss and differentiation-case legs of the adjoint')
     ap.add_argument('--no-ensemble', action='store_true', help='skip the batched-ensemble leg')
     ap.add_argument('--no-fdcheck', action='store_true', help='skip the differentiation case of the adjoint leg')
     ap.add_argument('--no-physics', action='store_true', help='skip the column-physics leg')
-    ap.add_argument('--adj-dense', action='store_true',
-                    help='time the adjoint leg with the unmasked loss only (profiling of the dense adjoint)')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

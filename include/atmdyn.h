@@ -6,8 +6,8 @@
  * interface of mod_sw_dyn / mod_remap / mod_sync, whose routines take only
  * dt and work on module-global arrays (src/mod_fields.f90:16-37).  Each
  * entry point below replaces one of those routines; the Fortran host binds
- * them through ISO_C_BINDING with the same call order
- * as run_model (src/mod_model.f90:146-177).
+ * them through ISO_C_BINDING with the same call order as run_model
+ * (src/mod_model.f90:146-177).
  *
  * Conventions
  *  - Every function returns an int status: ATM_OK (0) or an ATM_ERR_* code;
@@ -194,10 +194,21 @@ int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_o
    other threads) race and must be serialised by the caller.  The first
    call on a device looks up the array's device address
    (cudaGetSymbolAddress) with that device current; make that first call
-   before any stream capture. */
+   before any stream capture.  The address is kept for the life of the
+   process: a cudaDeviceReset unloads the array, and the entry point must
+   not be called on that device afterwards.
+   stable and fallback_columns (either may be NULL) report what
+   atm_check_stability and atm_remap_trace report for atm_remap: when
+   either is non-NULL the call waits for the remap to finish on stream,
+   stores 1 in *stable when every remapped value is finite (0 otherwise) and
+   the number of columns whose coordinates were not monotone (the
+   all-pairs search) in *fallback_columns.  When both are NULL the call
+   stays asynchronous and reports no non-finite result: the caller checks
+   the outputs itself. */
 int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, const double* bk, const double* dp,
                       const double* pt, const double* ud, const double* vd, const double* gzs,
-                      double* dp_out, double* pt_out, double* ud_out, double* vd_out, void* stream);
+                      double* dp_out, double* pt_out, double* ud_out, double* vd_out, void* stream,
+                      int* stable, int* fallback_columns);
 
 /* the number of the n pseudo-random FP64 arguments (all exponents, plus
    integers) for which the FP64 form's FMA-corrected division by the

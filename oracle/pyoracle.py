@@ -149,6 +149,10 @@ class OracleModel:
         self.lib.orc_set_remap_trace(self.s, self._trace.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
         return self._trace
 
+    def disable_trace(self):
+        self.lib.orc_set_remap_trace(self.s, None)
+        self._trace = None
+
     def state(self):
         return {name: self.get(f) for name, f in (('dp', DP), ('pt', PT), ('ud', UD), ('vd', VD))}
 

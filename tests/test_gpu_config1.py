@@ -1,0 +1,143 @@
+"""The warm-bubble configuration at its stated size: 128 x 128 x 20, dx = dy =
+50 km, dt = 60 s, vertical remap every 5 steps, 100 steps, with the
+reference's time loop (src/mod_model.f90:146-177).
+
+Three comparisons of the CUDA library's FP64 form:
+* against the oracle with the portable pow/log the library shares: every
+  field bit for bit after 100 steps, the remap's (k, m, case) pair sets of
+  steps 5 and 100 identical, total mass conserved to 1e-13;
+* against the oracle with the C library's pow/log (the arithmetic a
+  gfortran build of the reference uses): the distance after 100 steps is
+  bounded by the problem's own sensitivity, measured here as the distance
+  between two oracle runs whose initial potential temperature differs in
+  the last bit at half of the points; mass to 1e-13 in both;
+* the remap's pair sets against the C-library oracle: identical on a case
+  whose source and target interfaces are apart (a jet after 5 steps); in
+  the bubble case the resting pure-sigma start puts source and target
+  interfaces on top of each other, and there the sets may differ only by
+  zero-width pairs (first or last source layer moved by one).
+"""
+import copy
+import os
+
+import numpy as np
+import pytest
+
+from atmdyn import ic, model, Dycore
+import pyoracle
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = (('dp', pyoracle.DP), ('pt', pyoracle.PT), ('ud', pyoracle.UD), ('vd', pyoracle.VD))
+THREADS = max(1, min(16, os.cpu_count() or 1))
+
+
+def _run(stepper, st, trace_steps=()):
+    """run_model over the configuration's schedule; pair traces of the
+    remaps of the given steps, {step: trace}."""
+    tc = model.schedule_for(st.dt, st.nsteps, st.remap_every)
+    traces = {}
+    armed = []
+
+    def before_remap(n):
+        if n not in trace_steps:
+            return
+        if isinstance(stepper, Dycore):
+            traces[n] = stepper.remap_trace()[0]
+        else:
+            traces[n] = stepper.enable_trace()
+            armed.append(n)
+
+    def on_step(n, time):
+        if armed:
+            stepper.disable_trace()
+            armed.clear()
+
+    r = model.run_model(stepper, tc, before_remap=before_remap, on_step=on_step)
+    assert r.stable and r.steps == st.nsteps
+    return r, {n: t.copy() for n, t in traces.items()}
+
+
+def _relmax(a, b):
+    return np.abs(a - b).max() / np.abs(a).max()
+
+
+@pytest.fixture(scope='module')
+def config1_runs():
+    st = ic.config(1)
+    assert (st.nx, st.ny, st.nlay, st.dx, st.dt, st.remap_every, st.nsteps) == (128, 128, 20, 50e3, 60.0, 5, 100)
+    g = Dycore(st, 'fp64')
+    m0 = g.mass()
+    rg, tg = _run(g, st, (5, 100))
+    gpu = {n: g.get(n, halo=True) for n, _ in FIELDS}
+    gpu_mass = (g.mass() - m0) / m0
+    g.close()
+    runs = {'gpu': (rg, tg, gpu, gpu_mass)}
+    for variant in ('portable', 'libm'):
+        o = pyoracle.OracleModel(st, threads=THREADS, variant=variant)
+        m0 = o.mass()
+        r, t = _run(o, st, (5, 100))
+        runs[variant] = (r, t, {n: o.get(f, halo=True) for n, f in FIELDS}, (o.mass() - m0) / m0)
+    # the sensitivity of the problem itself: the last bit of pt at half the points
+    st1 = copy.deepcopy(st)
+    rng = np.random.default_rng(5)
+    st1.pt = np.where(rng.random(st1.pt.shape) < 0.5, np.nextafter(st1.pt, np.inf), st1.pt)
+    o = pyoracle.OracleModel(st1, threads=THREADS)
+    r, t = _run(o, st1)
+    runs['ulp'] = (r, t, {n: o.get(f, halo=True) for n, f in FIELDS}, None)
+    return runs
+
+
+def test_config1_bit_exact_against_oracle(config1_runs):
+    rg, tg, gpu, gpu_mass = config1_runs['gpu']
+    ro, to, orc, orc_mass = config1_runs['portable']
+    assert rg.remap_steps == ro.remap_steps == list(range(5, 101, 5))
+    for name, _ in FIELDS:
+        a, b = gpu[name], orc[name]
+        assert np.array_equal(a, b), '%s differs from the oracle after 100 steps (max %g)' % (
+            name, np.abs(a - b).max())
+    for n in (5, 100):
+        np.testing.assert_array_equal(tg[n], to[n], err_msg='remap pair sets of step %d' % n)
+    assert abs(gpu_mass) <= 1e-13 and abs(orc_mass) <= 1e-13
+
+
+def test_config1_against_libm_arithmetic(config1_runs):
+    _, tg, gpu, gpu_mass = config1_runs['gpu']
+    _, tl, libm, libm_mass = config1_runs['libm']
+    _, _, orc, _ = config1_runs['portable']
+    _, _, ulp, _ = config1_runs['ulp']
+    assert abs(libm_mass) <= 1e-13 and abs(gpu_mass) <= 1e-13
+    dist = {}
+    for name, _ in FIELDS:
+        d_libm = _relmax(libm[name], gpu[name])
+        d_ulp = _relmax(orc[name], ulp[name])
+        dist[name] = (d_libm, d_ulp)
+        # at the problem's own sensitivity to a last-bit change of the input
+        assert d_libm <= 2.0 * d_ulp + 1e-14, (name, d_libm, d_ulp)
+    # the thickness stays well inside the north-star bound
+    assert dist['dp'][0] <= 1e-11, dist
+    print('relative max-norm distance after 100 steps (C-library pow/log, last-bit input change):',
+          {k: '%.1e / %.1e' % v for k, v in dist.items()})
+    # pair sets of the first remap: equal except zero-width pairs at
+    # coincident source and target interfaces
+    a, b = tg[5].astype(np.int64), tl[5].astype(np.int64)
+    differ = (a != b).any(-1)
+    assert differ.mean() < 0.01
+    d = np.abs(a - b)
+    assert d[..., 0].max() <= 1 and d[..., 1].max() <= 1 and d[..., 4].max() <= 2
+
+
+def test_remap_pair_sets_match_libm_arithmetic_apart_from_ties():
+    """A jet after 5 steps: source and target interfaces are apart, and the
+    (k, m, case) sets of the GPU equal those of the C-library oracle."""
+    st = ic.jet_case(128, 128, 20, 50e3, 50e3, seed=0)
+    st.dt, st.remap_every, st.nsteps = 60.0, 5, 5
+    g = Dycore(st, 'fp64')
+    _, tg = _run(g, st, (5,))
+    gpu = {n: g.get(n) for n, _ in FIELDS}
+    g.close()
+    o = pyoracle.OracleModel(st, threads=THREADS, variant='libm')
+    _, tl = _run(o, st, (5,))
+    np.testing.assert_array_equal(tg[5], tl[5])
+    for name, f in FIELDS:
+        assert _relmax(gpu[name], o.get(f)) <= 1e-11, name

@@ -114,3 +114,38 @@ def test_division_by_constants_is_ieee_division():
     bad = ctypes.c_longlong(-1)
     assert lib.atm_device_div_check(400_000_000, 12345, ctypes.byref(bad)) == 0
     assert bad.value == 0
+
+
+def _ridged(nx=24, ny=20, L=8, layer=3):
+    """A state whose face-interpolated interface pressures are not monotone:
+    in one layer the thickness alternates thin, thin, thick, thick along y
+    (and along x), so that at some faces the outer pair of the (7/12, -1/12)
+    interpolation (src/mod_remap.f90:84-100) outweighs the inner pair."""
+    st = _bubble(nx, ny, L)
+    thin, thick = 400.0, 9000.0
+    jy = (np.arange(ny) % 4)[:, None]
+    ix = (np.arange(nx) % 4)[None, :]
+    pat = np.where((jy == 1) | (jy == 2), thin, thick) * 0.5 + np.where((ix == 1) | (ix == 2), thin, thick) * 0.5
+    st.dp = st.dp.copy()
+    st.dp[layer] = pat
+    st.u = st.u + 0.5 * np.sin(np.arange(nx) * 0.7)[None, None, :]
+    st.v = st.v + 0.3 * np.cos(np.arange(ny) * 0.9)[None, :, None]
+    return st
+
+
+def test_remap_all_pairs_branch_bit_exact():
+    """Columns with non-monotone coordinates take the reference's all-pairs
+    loop (src/mod_remap.f90:176-283); the forward result and the (k, m,
+    case) sets match the oracle there too."""
+    st = _ridged()
+    g = Dycore(st)
+    o = pyoracle.OracleModel(st)
+    trace_o = o.enable_trace()
+    trace_g, fallback = g.remap_trace()
+    for a in (g, o):
+        a.remap()
+    assert fallback.value > 0, 'no column took the all-pairs branch'
+    for name, f in (('dp', pyoracle.DP), ('pt', pyoracle.PT), ('ud', pyoracle.UD), ('vd', pyoracle.VD)):
+        _assert_same(g.get(name, halo=True), o.get(f, halo=True), name + ' after remap')
+    np.testing.assert_array_equal(trace_g, trace_o)
+    g.close()
