@@ -5,7 +5,9 @@ C-grid and D-grid flux-form semi-Lagrangian sweeps with PPM, the vertical
 PPM remap and the periodic halo fill) behind the C ABI of include/atmdyn.h.
 This package is its host side: the ctypes binding (:mod:`atmdyn.dycore`),
 the time loop of the reference (:mod:`atmdyn.model`), seeded initial
-conditions (:mod:`atmdyn.ic`) and the namelist reader (:mod:`atmdyn.namelist`).
+conditions (:mod:`atmdyn.ic`), the namelist and netCDF-3 file formats
+(:mod:`atmdyn.io`), the autograd binding of the adjoint
+(:mod:`atmdyn.adjoint`) and the batched ensemble (:mod:`atmdyn.ensemble`).
 """
 from . import ic, model  # noqa: F401
 from ._lib import AtmError, load, build  # noqa: F401

@@ -865,6 +865,57 @@ def e2e_runs(dy, st, K, stream, torch, max_over_ranks, world):
     return out[0], out[1]
 
 
+def probe_remap_adjoint(args):
+    """A small case for ncu captures of the remap adjoint kernels (nothing
+    is timed here): a jet at nx x nx x nlay, two forward steps, then three
+    calls of the remap adjoint with a dense seeded output adjoint."""
+    import torch
+    torch.cuda.set_device(0)
+    from atmdyn import ic, Dycore
+    from atmdyn.dycore import HALO
+    st = ic.jet_case(args.nx, args.nx, args.nlay, 25e3, 25e3, seed=0)
+    g = Dycore(st)
+    for _ in range(2):
+        g.step(DT, remap=False, check_stable=False)
+    g.adj_enable()
+    rng = np.random.default_rng(7)
+    shape = (st.nlay, st.ny + 2 * HALO, st.nx + 2 * HALO)
+    for n in ('dp', 'pt', 'ud', 'vd'):
+        g.adj_set('out', n, rng.normal(0, 1, shape))
+    for _ in range(3):
+        g.adj_remap()
+    g.sync()
+    g.close()
+    print('remap adjoint probe done: %dx%dx%d' % (args.nx, args.nx, args.nlay))
+
+
+def probe_steps(args):
+    """A small case for ncu captures of the step kernels (nothing is timed
+    here): the forward forms, or the forward + adjoint of the headline loss."""
+    import torch
+    torch.cuda.set_device(0)
+    from atmdyn import ic, Dycore
+    st = ic.jet_case(args.nx, args.nx, args.nlay, 25e3, 25e3, seed=0)
+    if args.probe == 'forward':
+        for form in args.forms.split(','):
+            dy = Dycore(st, form)
+            for n in range(args.warmup + args.steps):
+                dy.step(DT, remap=(n + 1) % REMAP_EVERY == 0, check_stable=False)
+            assert dy.check_stability()
+            dy.close()
+    else:
+        from atmdyn.adjoint import integrate
+        dyn = Dycore(st)
+        dyn.adj_enable()
+        x = [torch.tensor(np.ascontiguousarray(a), device='cuda', requires_grad=True)
+             for a in (st.dp, st.pt, st.u, st.v)]
+        y = integrate(dyn, x, args.steps, DT, REMAP_EVERY, ADJ_CKPT)
+        ((y[1] * P0K) ** 2).sum().backward()
+        torch.cuda.synchronize()
+        dyn.close()
+    print('probe done: %s %dx%dx%d' % (args.probe, args.nx, args.nx, args.nlay))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -881,9 +932,20 @@ def main():
     ap.add_argument('--no-ensemble', action='store_true', help='skip the batched-ensemble leg')
     ap.add_argument('--no-fdcheck', action='store_true', help='skip the differentiation case of the adjoint leg')
     ap.add_argument('--no-physics', action='store_true', help='skip the column-physics leg')
+    ap.add_argument('--probe', choices=['remap_adj', 'forward', 'adjoint'], default=None,
+                    help='profiling case instead of the benchmark, on a jet at --nx x --nx x --nlay: remap_adj = '
+                         'two steps, then three calls of the remap adjoint with a dense random output adjoint; '
+                         'forward = --warmup + --steps steps of each form in --forms (remap every 8); adjoint = '
+                         '--steps steps forward + adjoint of J = sum(theta^2) (checkpoints every 8)')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.probe == 'remap_adj':
+        probe_remap_adjoint(args)
+        return
+    if args.probe in ('forward', 'adjoint'):
+        probe_steps(args)
+        return
     if args.impl == 'reference':
         run_reference(args)
     else:

@@ -125,3 +125,62 @@ def test_differentiation_case_dot_product():
     J.backward()
     rhs = sum(np.sum(v[n] * xx.grad.cpu().numpy()) for n, xx in zip(NAMES, x))
     assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs)), (lhs, rhs)
+
+
+def _dot_product_case(st, nsteps, remap_every, ckpt, seed):
+    rng = np.random.default_rng(seed)
+    v = {n: rng.normal(0, SCALE[n], (st.nlay, st.ny, st.nx)) for n in NAMES}
+    w = {n: rng.normal(0, SCALE[n], (st.nlay, st.ny, st.nx)) for n in NAMES}
+    t = pyoracle.TLMModel(st, v, threads=8)
+    for s in range(nsteps):
+        t.cgrid_step(st.dt / 2)
+        t.cgrid_halo()
+        t.dgrid_step(st.dt)
+        if (s + 1) % remap_every == 0:
+            t.remap()
+        t.dgrid_halo()
+    lhs = sum(np.sum(w[n] * t.get(STATE[n])[1]) for n in NAMES)
+    del t
+    dyn = Dycore(st)
+    dyn.adj_enable()
+    x = tensors(st)
+    y = integrate(dyn, x, nsteps, st.dt, remap_every, ckpt)
+    J = sum((torch.tensor(w[n], device='cuda') * yy).sum() for n, yy in zip(NAMES, y))
+    J.backward()
+    rhs = sum(np.sum(v[n] * xx.grad.cpu().numpy()) for n, xx in zip(NAMES, x))
+    dyn.close()
+    return lhs, rhs
+
+
+@pytest.mark.parametrize('member', [5, 7])
+def test_ensemble_member_adjoint_dot_product(member):
+    """Two members of the batched ensemble (seed 3) of different grid sizes
+    and layer counts (64^2 x 48 and 128^2 x 64 jets), with their own time
+    steps and remap interval: the gradient the ensemble leg computes for
+    them (20 steps, checkpoints every 5) passes the dot-product test against
+    the tangent-linear oracle."""
+    st = ic.ensemble_members(8, seed=3)[member]
+    assert (st.nx, st.nlay) == {5: (64, 48), 7: (128, 64)}[member]
+    lhs, rhs = _dot_product_case(st, 20, st.remap_every, 5, seed=20 + member)
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs)), (st.name, lhs, rhs)
+
+
+def test_gradient_run_to_run_spread():
+    """The adjoint kernels add the adjoints of overlapping tile halos into
+    global memory with atomics, so the order of those additions, and with it
+    the last bits of the gradient, can change from run to run.  Two
+    gradients of the same loss differ by at most 1e-12 of the gradient's
+    norm (20 steps of the noisy jet, loss over every cell)."""
+    st = small_jet(noisy=True)
+    dyn = Dycore(st)
+    dyn.adj_enable()
+    grads = []
+    for _ in range(2):
+        x = tensors(st)
+        y = integrate(dyn, x, 20, st.dt, 5, 5)
+        ((y[1] * P0K) ** 2).sum().backward()
+        grads.append(torch.cat([xx.grad.flatten() for xx in x]))
+    dyn.close()
+    spread = ((grads[0] - grads[1]).norm() / grads[0].norm()).item()
+    print('relative run-to-run spread of the gradient: %.2e' % spread)
+    assert spread <= 1e-12, spread
