@@ -4,9 +4,8 @@
 #pragma once
 
 #include "atm_kernels.cuh"
+#include "atm_march.cuh"
 #include "atm_ops.h"
-#include "atm_sweeps.cuh"
-#include "atm_tmap.h"
 
 namespace atm {
 namespace {
@@ -14,65 +13,34 @@ namespace {
 using T = ATM_FORM_T;  // sweep arithmetic
 using S = double;      // prognostic state (dp, pt, ud, vd), both forms
 using C = T;           // C-grid fields (dpc, ptc, uc, vc)
-// Tile of each sweep kernel (TX x TY_*), measured per kernel and form on
-// B200 at 1024x1024x64 (heights 3 to 16 and 64x8 tried, with the CTAs per
-// SM each layout's register budget is set for): smaller tiles hold more
-// CTAs per SM, taller ones recompute less halo.
-constexpr bool FP64_FORM = std::is_same_v<T, double>;
-constexpr int TX = 32;
-constexpr int TY_CMASS = FP64_FORM ? 4 : 16;
-constexpr int TY_DMASS = FP64_FORM ? 6 : 16;
-constexpr int TY_CMOM = 8;
-constexpr int TY_DMOM = 4;
+// Strip height (output rows a warp walks through) of each column-marching
+// sweep: 6 warm-up rows per strip are recomputed halo, more strips per
+// layer fill the GPU.
+constexpr int TYS_MASS = 64;
+constexpr int TYS_CMOM = 64;
+constexpr int TYS_DMOM = 64;
 
-inline dim3 tiles(int lo, int hi, const Geom& g, int layers, int ty) {
+inline dim3 strips(int lo, int hi, const Geom& g, int tys) {
   int w = g.nx - lo + hi, h = g.ny - lo + hi;
-  return dim3((w + TX - 1) / TX, (h + ty - 1) / ty, layers);
+  return dim3((w + MOUT * MWARPS - 1) / (MOUT * MWARPS), (h + tys - 1) / tys, g.L);
 }
 
-template <typename K>
-cudaError_t smem_attr(K kernel, size_t bytes) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
-
-cudaError_t setup() {
-  cudaError_t e;
-  if ((e = smem_attr(k_mass2<T, TX, TY_CMASS, true, S, C>, MassL<T, TX, TY_CMASS, true, S, C>::bytes)) != cudaSuccess)
-    return e;
-  if ((e = smem_attr(k_mass2<T, TX, TY_DMASS, false, S, C>, MassL<T, TX, TY_DMASS, false, S, C>::bytes)) !=
-      cudaSuccess)
-    return e;
-  if ((e = smem_attr(k_c_mom2<T, TX, TY_CMOM, S, C>, CMomL<T, TX, TY_CMOM, S>::bytes)) != cudaSuccess) return e;
-  if ((e = smem_attr(k_d_mom2<T, TX, TY_DMOM, S, C>, DMomL<T, TX, TY_DMOM, S, C>::bytes)) != cudaSuccess) return e;
-  return cudaSuccess;
-}
+// the column-marching sweeps need no shared memory: nothing to set up
+cudaError_t setup() { return cudaSuccess; }
 
 cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt, const void* u, const void* v,
                  const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, int* timeout, bool cgrid,
                  cudaStream_t s) {
-  CUtensorMap md, mp, mu, mv;
-  cudaError_t e;
-  if (cgrid) {  // state in, C-grid fields out
-    using Lay = MassL<T, TX, TY_CMASS, true, S, C>;
-    dim3 grid = tiles(lo, hi, g, g.L, TY_CMASS);
-    constexpr int eu = sizeof(typename Lay::UB);
-    if ((e = tmap(dp, sizeof(S), g, g.L, Lay::WD, Lay::HD, &md)) ||
-        (e = tmap(pt, sizeof(S), g, g.L, Lay::WD, Lay::HD, &mp)) || (e = tmap(u, eu, g, g.L, Lay::WU, Lay::HU, &mu)) ||
-        (e = tmap(v, eu, g, g.L, Lay::WV, Lay::HV, &mv)))
-      return e;
-    k_mass2<T, TX, TY_CMASS, true, S, C><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (C*)dpo,
-                                                                       (C*)pto, lo, hi, nonfinite, timeout);
-  } else {  // state and C-grid winds in, state out
-    using Lay = MassL<T, TX, TY_DMASS, false, S, C>;
-    dim3 grid = tiles(lo, hi, g, g.L, TY_DMASS);
-    constexpr int eu = sizeof(typename Lay::UB);
-    if ((e = tmap(dp, sizeof(S), g, g.L, Lay::WD, Lay::HD, &md)) ||
-        (e = tmap(pt, sizeof(S), g, g.L, Lay::WD, Lay::HD, &mp)) || (e = tmap(u, eu, g, g.L, Lay::WU, Lay::HU, &mu)) ||
-        (e = tmap(v, eu, g, g.L, Lay::WV, Lay::HV, &mv)))
-      return e;
-    k_mass2<T, TX, TY_DMASS, false, S, C><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (S*)dpo,
-                                                                        (S*)pto, lo, hi, nonfinite, timeout);
-  }
+  (void)timeout;
+  const dim3 grid = strips(lo, hi, g, TYS_MASS);
+  if (cgrid)  // state in, C-grid fields out
+    k_mass_m<T, TYS_MASS, true, S, C><<<grid, MW * MWARPS, 0, s>>>(g, c, (const S*)dp, (const S*)pt, (const S*)u,
+                                                                    (const S*)v, heat, (C*)dpo, (C*)pto, lo, hi,
+                                                                    nonfinite);
+  else  // state and C-grid winds in, state out
+    k_mass_m<T, TYS_MASS, false, S, C><<<grid, MW * MWARPS, 0, s>>>(g, c, (const S*)dp, (const S*)pt, (const C*)u,
+                                                                     (const C*)v, heat, (S*)dpo, (S*)pto, lo, hi,
+                                                                     nonfinite);
   return cudaGetLastError();
 }
 
@@ -98,33 +66,18 @@ cudaError_t heating(const Geom& g, const Consts& c, const void* dpl, int es, con
 
 cudaError_t c_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const double* pkap, const double* gz,
                   void* uc, void* vc, int* timeout, cudaStream_t s) {
-  using Lay = CMomL<T, TX, TY_CMOM, S>;
-  constexpr int es = sizeof(S);
-  CUtensorMap mu, mv, muL, mvL, mpk, mgz;
-  cudaError_t e;
-  if ((e = tmap(ud, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, es, g, g.L, Lay::WV, Lay::HV, &mv)) ||
-      (e = tmap(ud, es, g, g.L, Lay::WL, Lay::HL, &muL)) || (e = tmap(vd, es, g, g.L, Lay::WL, Lay::HL, &mvL)) ||
-      (e = tmap(pkap, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpk)) || (e = tmap(gz, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgz)))
-    return e;
-  k_c_mom2<T, TX, TY_CMOM, S, C><<<tiles(0, 0, g, g.L, TY_CMOM), NT, Lay::bytes, s>>>(
-      mu, mv, muL, mvL, mpk, mgz, g, c, (const S*)ud, (const S*)vd, (C*)uc, (C*)vc, timeout);
+  (void)timeout;
+  k_c_mom_m<T, TYS_CMOM, S, C><<<strips(0, 0, g, TYS_CMOM), MW * MWARPS, 0, s>>>(g, c, (const S*)ud, (const S*)vd,
+                                                                                pkap, gz, (C*)uc, (C*)vc);
   return cudaGetLastError();
 }
 
 cudaError_t d_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const void* uc, const void* vc,
                   const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, int* timeout,
                   cudaStream_t s) {
-  using Lay = DMomL<T, TX, TY_DMOM, S, C>;
-  constexpr int es = sizeof(S), ec = sizeof(C);
-  CUtensorMap mu, mv, muL, mvL, muc, mvc, mpb, mgb;
-  cudaError_t e;
-  if ((e = tmap(ud, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, es, g, g.L, Lay::WU, Lay::HU, &mv)) ||
-      (e = tmap(uc, ec, g, g.L, Lay::WUL, Lay::HUL, &muL)) || (e = tmap(vc, ec, g, g.L, Lay::WVL, Lay::HVL, &mvL)) ||
-      (e = tmap(uc, ec, g, g.L, Lay::WC, Lay::HC, &muc)) || (e = tmap(vc, ec, g, g.L, Lay::WC, Lay::HC, &mvc)) ||
-      (e = tmap(pkapb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpb)) || (e = tmap(gzb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgb)))
-    return e;
-  k_d_mom2<T, TX, TY_DMOM, S, C><<<tiles(0, 0, g, g.L, TY_DMOM), NT, Lay::bytes, s>>>(
-      mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c, (const S*)ud, (const S*)vd, (S*)udo, (S*)vdo, nonfinite, timeout);
+  (void)timeout;
+  k_d_mom_m<T, TYS_DMOM, S, C><<<strips(0, 0, g, TYS_DMOM), MW * MWARPS, 0, s>>>(
+      g, c, (const S*)ud, (const S*)vd, (const C*)uc, (const C*)vc, pkapb, gzb, (S*)udo, (S*)vdo, nonfinite);
   return cudaGetLastError();
 }
 
