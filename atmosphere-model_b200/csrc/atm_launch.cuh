@@ -6,6 +6,7 @@
 #include "atm_kernels.cuh"
 #include "atm_march.cuh"
 #include "atm_ops.h"
+#include "atm_remap_warp.cuh"
 
 namespace atm {
 namespace {
@@ -13,6 +14,7 @@ namespace {
 using T = ATM_FORM_T;  // sweep arithmetic
 using S = double;      // prognostic state (dp, pt, ud, vd), both forms
 using C = T;           // C-grid fields (dpc, ptc, uc, vc)
+constexpr bool FP64_FORM = std::is_same_v<T, double>;
 // Strip height (output rows a warp walks through) of each column-marching
 // sweep: 6 warm-up rows per strip are recomputed halo, more strips per
 // layer fill the GPU.
@@ -125,8 +127,35 @@ cudaError_t remap_energy_lm(const Geom& g, const RemapArgs& ra, const void* dp, 
   return cudaGetLastError();
 }
 
+// The mixed form remaps with the warp-cooperative kernels (its sums in a
+// different association); the FP64 form, and any remap whose pair trace is
+// requested, with the sequential ones.
+template <int LPL>
+cudaError_t remap_winds_wl(const Geom& g, const RemapArgs& ra, const void* dp, const void* ud, const void* vd,
+                           void* urem, void* vrem, Status* st, cudaStream_t s) {
+  const long long warps = 2LL * (g.nx + 2) * (g.ny + 2);
+  k_remap_winds_w<LPL><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(g, ra, (const double*)dp, (const double*)ud,
+                                                                    (const double*)vd, (double*)urem, (double*)vrem, st);
+  return cudaGetLastError();
+}
+template <int LPL>
+cudaError_t remap_energy_wl(const Geom& g, const RemapArgs& ra, const void* dp, const void* pt, const void* ud,
+                            const void* vd, const void* urem, const void* vrem, const double* gzs, void* dpo,
+                            void* pto, void* udo, void* vdo, Status* st, cudaStream_t s) {
+  const long long warps = (long long)g.nx * g.ny;
+  k_remap_energy_w<LPL><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(
+      g, ra, (const double*)dp, (const double*)pt, (const double*)ud, (const double*)vd, (const double*)urem,
+      (const double*)vrem, gzs, (double*)dpo, (double*)pto, (double*)udo, (double*)vdo, st);
+  return cudaGetLastError();
+}
+
 cudaError_t remap_winds(const Geom& g, const RemapArgs& ra, const void* dp, const void* ud, const void* vd, void* urem,
                         void* vrem, int* trace, Status* st, cudaStream_t s) {
+  if (!FP64_FORM && !trace) {
+    if (g.L <= 32) return remap_winds_wl<1>(g, ra, dp, ud, vd, urem, vrem, st, s);
+    if (g.L <= 64) return remap_winds_wl<2>(g, ra, dp, ud, vd, urem, vrem, st, s);
+    return remap_winds_wl<4>(g, ra, dp, ud, vd, urem, vrem, st, s);
+  }
   if (g.L <= 32) return remap_winds_lm<32>(g, ra, dp, ud, vd, urem, vrem, trace, st, s);
   if (g.L <= 64) return remap_winds_lm<64>(g, ra, dp, ud, vd, urem, vrem, trace, st, s);
   return remap_winds_lm<MAX_LAYERS>(g, ra, dp, ud, vd, urem, vrem, trace, st, s);
@@ -135,6 +164,11 @@ cudaError_t remap_winds(const Geom& g, const RemapArgs& ra, const void* dp, cons
 cudaError_t remap_energy(const Geom& g, const RemapArgs& ra, const void* dp, const void* pt, const void* ud,
                          const void* vd, const void* urem, const void* vrem, const double* gzs, void* dpo, void* pto,
                          void* udo, void* vdo, int* trace, Status* st, cudaStream_t s) {
+  if (!FP64_FORM && !trace) {
+    if (g.L <= 32) return remap_energy_wl<1>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, st, s);
+    if (g.L <= 64) return remap_energy_wl<2>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, st, s);
+    return remap_energy_wl<4>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, st, s);
+  }
   if (g.L <= 32) return remap_energy_lm<32>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, trace, st, s);
   if (g.L <= 64) return remap_energy_lm<64>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, trace, st, s);
   return remap_energy_lm<MAX_LAYERS>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, trace, st, s);
