@@ -25,6 +25,10 @@ constexpr int MW = 32;              // lanes (columns) of a strip
 constexpr int MXH = 3;              // halo columns on each side
 constexpr int MOUT = MW - 2 * MXH;  // output columns of a strip
 constexpr int MWARPS = 4;           // independent strips (warps) per block
+// blocks per SM the register budget of the marching kernels is set for
+#ifndef ATM_MARCH_MINB
+#define ATM_MARCH_MINB 1
+#endif
 
 template <typename T>
 __device__ __forceinline__ T shfl_at(T v, int src) {
@@ -134,7 +138,7 @@ struct MassM {
 };
 
 template <typename T, int TYS, bool CGRID, typename S, typename C>
-__global__ void __launch_bounds__(MW * MWARPS) k_mass_m(Geom g, Consts c, const S* __restrict__ dp,
+__global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_mass_m(Geom g, Consts c, const S* __restrict__ dp,
                                                          const S* __restrict__ pt,
                                                          const typename MassM<T, CGRID, S, C>::UB* __restrict__ u,
                                                          const typename MassM<T, CGRID, S, C>::UB* __restrict__ v,
@@ -324,7 +328,7 @@ __global__ void __launch_bounds__(MW * MWARPS) k_mass_m(Geom g, Consts c, const 
 // pressure-gradient force (:325-339) and the vorticity-flux updates of uc
 // and vc (:344-412).  Outputs on the interior; strips of TYS rows.
 template <typename T, int TYS, typename S, typename C>
-__global__ void __launch_bounds__(MW * MWARPS) k_c_mom_m(Geom g, Consts c, const S* __restrict__ ud,
+__global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_c_mom_m(Geom g, Consts c, const S* __restrict__ ud,
                                                           const S* __restrict__ vd, const double* __restrict__ pkap,
                                                           const double* __restrict__ gz, C* __restrict__ uc,
                                                           C* __restrict__ vc) {
@@ -477,7 +481,7 @@ __global__ void __launch_bounds__(MW * MWARPS) k_c_mom_m(Geom g, Consts c, const
 // (:682-702) and the vorticity-flux updates (:708-769).  Outputs on the
 // interior; strips of TYS rows.
 template <typename T, int TYS, typename S, typename C>
-__global__ void __launch_bounds__(MW * MWARPS) k_d_mom_m(Geom g, Consts c, const S* __restrict__ ud,
+__global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_d_mom_m(Geom g, Consts c, const S* __restrict__ ud,
                                                           const S* __restrict__ vd, const C* __restrict__ uc,
                                                           const C* __restrict__ vc, const double* __restrict__ pkapb,
                                                           const double* __restrict__ gzb, S* __restrict__ udo,
@@ -545,8 +549,9 @@ __global__ void __launch_bounds__(MW * MWARPS) k_d_mom_m(Geom g, Consts c, const
       const T cR = shfl_dn(cu1, 1);
       const T c0 = dtdx * cu1, c1 = dtdx * cR;
       const T den = T(1) / (T(1) - dtdx * (cR - cu1));
-      const T f0 = (c0 > T(0)) ? shfl_up(w1, 1) : w1;
-      const T f1 = (c1 > T(0)) ? w1 : shfl_dn(w1, 1);
+      const T wl = shfl_up(w1, 1), wr = shfl_dn(w1, 1);  // every lane takes part in the shuffles
+      const T f0 = (c0 > T(0)) ? wl : w1;
+      const T f1 = (c1 > T(0)) ? w1 : wr;
       t4 = t3; t3 = t2; t2 = t1;
       t1 = T(.5) * (w1 + den * (w1 - rA * (f1 - f0)));
     }
