@@ -4,7 +4,6 @@
 #define ATM_FORM_T double
 #define ATM_OPS_NAME ops_fp64
 #include "atm_launch.cuh"
-#include "atm_tma.cuh"
 
 namespace atm {
 

@@ -6,7 +6,8 @@
 #include "atm_kernels.cuh"
 #include "atm_march.cuh"
 #include "atm_ops.h"
-#include "atm_remap_warp.cuh"
+#include "atm_sweeps.cuh"
+#include "atm_tmap.h"
 
 namespace atm {
 namespace {
@@ -14,35 +15,85 @@ namespace {
 using T = ATM_FORM_T;  // sweep arithmetic
 using S = double;      // prognostic state (dp, pt, ud, vd), both forms
 using C = T;           // C-grid fields (dpc, ptc, uc, vc)
+// Tile of each sweep kernel (TX x TY_*), measured per kernel and form on
+// B200 at 1024x1024x64 (heights 3 to 16 and 64x8 tried, with the CTAs per
+// SM each layout's register budget is set for): smaller tiles hold more
+// CTAs per SM, taller ones recompute less halo.
 constexpr bool FP64_FORM = std::is_same_v<T, double>;
-// Strip height (output rows a warp walks through) of each column-marching
-// sweep: 6 warm-up rows per strip are recomputed halo, more strips per
-// layer fill the GPU.
-constexpr int TYS_MASS = 64;
-constexpr int TYS_CMOM = 64;
-constexpr int TYS_DMOM = 64;
+constexpr int TX = 32;
+constexpr int TY_CMASS = FP64_FORM ? 4 : 16;
+constexpr int TY_DMASS = FP64_FORM ? 6 : 16;
+constexpr int TY_CMOM = 8;
+constexpr int TY_DMOM = 4;
+// The mixed form runs its C-grid momentum, D-grid mass and D-grid momentum
+// sweeps as column-marching kernels (atm_march.cuh), measured faster than
+// its tiles there (B200, 1024x1024x64: 2.83 / 2.01 / 2.82 ms against 3.01 /
+// 2.66 / 4.05); its C-grid mass sweep (2.70 ms against 2.94) and every
+// FP64 sweep (13 FP64 sweep-ms against 29 marching: at 136-174 registers
+// a thread the marching kernels hold too few warps to hide FP64 latency)
+// keep the tiles.
+constexpr bool MARCH = !FP64_FORM;
+// strip height (output rows a warp walks through) of the marching sweeps
+constexpr int TYS = 64;
 
 inline dim3 strips(int lo, int hi, const Geom& g, int tys) {
   int w = g.nx - lo + hi, h = g.ny - lo + hi;
   return dim3((w + MOUT * MWARPS - 1) / (MOUT * MWARPS), (h + tys - 1) / tys, g.L);
 }
 
-// the column-marching sweeps need no shared memory: nothing to set up
-cudaError_t setup() { return cudaSuccess; }
+inline dim3 tiles(int lo, int hi, const Geom& g, int layers, int ty) {
+  int w = g.nx - lo + hi, h = g.ny - lo + hi;
+  return dim3((w + TX - 1) / TX, (h + ty - 1) / ty, layers);
+}
+
+template <typename K>
+cudaError_t smem_attr(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t setup() {
+  cudaError_t e;
+  if ((e = smem_attr(k_mass2<T, TX, TY_CMASS, true, S, C>, MassL<T, TX, TY_CMASS, true, S, C>::bytes)) != cudaSuccess)
+    return e;
+  if ((e = smem_attr(k_mass2<T, TX, TY_DMASS, false, S, C>, MassL<T, TX, TY_DMASS, false, S, C>::bytes)) !=
+      cudaSuccess)
+    return e;
+  if constexpr (!MARCH) {
+    if ((e = smem_attr(k_c_mom2<T, TX, TY_CMOM, S, C>, CMomL<T, TX, TY_CMOM, S>::bytes)) != cudaSuccess) return e;
+    if ((e = smem_attr(k_d_mom2<T, TX, TY_DMOM, S, C>, DMomL<T, TX, TY_DMOM, S, C>::bytes)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
 
 cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt, const void* u, const void* v,
                  const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, int* timeout, bool cgrid,
                  cudaStream_t s) {
-  (void)timeout;
-  const dim3 grid = strips(lo, hi, g, TYS_MASS);
-  if (cgrid)  // state in, C-grid fields out
-    k_mass_m<T, TYS_MASS, true, S, C><<<grid, MW * MWARPS, 0, s>>>(g, c, (const S*)dp, (const S*)pt, (const S*)u,
-                                                                    (const S*)v, heat, (C*)dpo, (C*)pto, lo, hi,
-                                                                    nonfinite);
-  else  // state and C-grid winds in, state out
-    k_mass_m<T, TYS_MASS, false, S, C><<<grid, MW * MWARPS, 0, s>>>(g, c, (const S*)dp, (const S*)pt, (const C*)u,
-                                                                     (const C*)v, heat, (S*)dpo, (S*)pto, lo, hi,
-                                                                     nonfinite);
+  CUtensorMap md, mp, mu, mv;
+  cudaError_t e;
+  if (cgrid) {  // state in, C-grid fields out
+    using Lay = MassL<T, TX, TY_CMASS, true, S, C>;
+    dim3 grid = tiles(lo, hi, g, g.L, TY_CMASS);
+    constexpr int eu = sizeof(typename Lay::UB);
+    if ((e = tmap(dp, sizeof(S), g, g.L, Lay::WD, Lay::HD, &md)) ||
+        (e = tmap(pt, sizeof(S), g, g.L, Lay::WD, Lay::HD, &mp)) || (e = tmap(u, eu, g, g.L, Lay::WU, Lay::HU, &mu)) ||
+        (e = tmap(v, eu, g, g.L, Lay::WV, Lay::HV, &mv)))
+      return e;
+    k_mass2<T, TX, TY_CMASS, true, S, C><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (C*)dpo,
+                                                                       (C*)pto, lo, hi, nonfinite, timeout);
+  } else if constexpr (MARCH) {  // state and C-grid winds in, state out
+    k_mass_m<T, TYS, false, S, C><<<strips(lo, hi, g, TYS), MW * MWARPS, 0, s>>>(
+        g, c, (const S*)dp, (const S*)pt, (const C*)u, (const C*)v, heat, (S*)dpo, (S*)pto, lo, hi, nonfinite);
+  } else {
+    using Lay = MassL<T, TX, TY_DMASS, false, S, C>;
+    dim3 grid = tiles(lo, hi, g, g.L, TY_DMASS);
+    constexpr int eu = sizeof(typename Lay::UB);
+    if ((e = tmap(dp, sizeof(S), g, g.L, Lay::WD, Lay::HD, &md)) ||
+        (e = tmap(pt, sizeof(S), g, g.L, Lay::WD, Lay::HD, &mp)) || (e = tmap(u, eu, g, g.L, Lay::WU, Lay::HU, &mu)) ||
+        (e = tmap(v, eu, g, g.L, Lay::WV, Lay::HV, &mv)))
+      return e;
+    k_mass2<T, TX, TY_DMASS, false, S, C><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (S*)dpo,
+                                                                        (S*)pto, lo, hi, nonfinite, timeout);
+  }
   return cudaGetLastError();
 }
 
@@ -68,18 +119,43 @@ cudaError_t heating(const Geom& g, const Consts& c, const void* dpl, int es, con
 
 cudaError_t c_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const double* pkap, const double* gz,
                   void* uc, void* vc, int* timeout, cudaStream_t s) {
-  (void)timeout;
-  k_c_mom_m<T, TYS_CMOM, S, C><<<strips(0, 0, g, TYS_CMOM), MW * MWARPS, 0, s>>>(g, c, (const S*)ud, (const S*)vd,
-                                                                                pkap, gz, (C*)uc, (C*)vc);
+  if constexpr (MARCH) {
+    k_c_mom_m<T, TYS, S, C><<<strips(0, 0, g, TYS), MW * MWARPS, 0, s>>>(g, c, (const S*)ud, (const S*)vd, pkap, gz,
+                                                                          (C*)uc, (C*)vc);
+    return cudaGetLastError();
+  }
+  using Lay = CMomL<T, TX, TY_CMOM, S>;
+  constexpr int es = sizeof(S);
+  CUtensorMap mu, mv, muL, mvL, mpk, mgz;
+  cudaError_t e;
+  if ((e = tmap(ud, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, es, g, g.L, Lay::WV, Lay::HV, &mv)) ||
+      (e = tmap(ud, es, g, g.L, Lay::WL, Lay::HL, &muL)) || (e = tmap(vd, es, g, g.L, Lay::WL, Lay::HL, &mvL)) ||
+      (e = tmap(pkap, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpk)) || (e = tmap(gz, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgz)))
+    return e;
+  k_c_mom2<T, TX, TY_CMOM, S, C><<<tiles(0, 0, g, g.L, TY_CMOM), NT, Lay::bytes, s>>>(
+      mu, mv, muL, mvL, mpk, mgz, g, c, (const S*)ud, (const S*)vd, (C*)uc, (C*)vc, timeout);
   return cudaGetLastError();
 }
 
 cudaError_t d_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const void* uc, const void* vc,
                   const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, int* timeout,
                   cudaStream_t s) {
-  (void)timeout;
-  k_d_mom_m<T, TYS_DMOM, S, C><<<strips(0, 0, g, TYS_DMOM), MW * MWARPS, 0, s>>>(
-      g, c, (const S*)ud, (const S*)vd, (const C*)uc, (const C*)vc, pkapb, gzb, (S*)udo, (S*)vdo, nonfinite);
+  if constexpr (MARCH) {
+    k_d_mom_m<T, TYS, S, C><<<strips(0, 0, g, TYS), MW * MWARPS, 0, s>>>(
+        g, c, (const S*)ud, (const S*)vd, (const C*)uc, (const C*)vc, pkapb, gzb, (S*)udo, (S*)vdo, nonfinite);
+    return cudaGetLastError();
+  }
+  using Lay = DMomL<T, TX, TY_DMOM, S, C>;
+  constexpr int es = sizeof(S), ec = sizeof(C);
+  CUtensorMap mu, mv, muL, mvL, muc, mvc, mpb, mgb;
+  cudaError_t e;
+  if ((e = tmap(ud, es, g, g.L, Lay::WU, Lay::HU, &mu)) || (e = tmap(vd, es, g, g.L, Lay::WU, Lay::HU, &mv)) ||
+      (e = tmap(uc, ec, g, g.L, Lay::WUL, Lay::HUL, &muL)) || (e = tmap(vc, ec, g, g.L, Lay::WVL, Lay::HVL, &mvL)) ||
+      (e = tmap(uc, ec, g, g.L, Lay::WC, Lay::HC, &muc)) || (e = tmap(vc, ec, g, g.L, Lay::WC, Lay::HC, &mvc)) ||
+      (e = tmap(pkapb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mpb)) || (e = tmap(gzb, 8, g, g.L + 1, Lay::WP, Lay::HP, &mgb)))
+    return e;
+  k_d_mom2<T, TX, TY_DMOM, S, C><<<tiles(0, 0, g, g.L, TY_DMOM), NT, Lay::bytes, s>>>(
+      mu, mv, muL, mvL, muc, mvc, mpb, mgb, g, c, (const S*)ud, (const S*)vd, (S*)udo, (S*)vdo, nonfinite, timeout);
   return cudaGetLastError();
 }
 
@@ -127,35 +203,8 @@ cudaError_t remap_energy_lm(const Geom& g, const RemapArgs& ra, const void* dp, 
   return cudaGetLastError();
 }
 
-// The mixed form remaps with the warp-cooperative kernels (its sums in a
-// different association); the FP64 form, and any remap whose pair trace is
-// requested, with the sequential ones.
-template <int LPL>
-cudaError_t remap_winds_wl(const Geom& g, const RemapArgs& ra, const void* dp, const void* ud, const void* vd,
-                           void* urem, void* vrem, Status* st, cudaStream_t s) {
-  const long long warps = 2LL * (g.nx + 2) * (g.ny + 2);
-  k_remap_winds_w<LPL><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(g, ra, (const double*)dp, (const double*)ud,
-                                                                    (const double*)vd, (double*)urem, (double*)vrem, st);
-  return cudaGetLastError();
-}
-template <int LPL>
-cudaError_t remap_energy_wl(const Geom& g, const RemapArgs& ra, const void* dp, const void* pt, const void* ud,
-                            const void* vd, const void* urem, const void* vrem, const double* gzs, void* dpo,
-                            void* pto, void* udo, void* vdo, Status* st, cudaStream_t s) {
-  const long long warps = (long long)g.nx * g.ny;
-  k_remap_energy_w<LPL><<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(
-      g, ra, (const double*)dp, (const double*)pt, (const double*)ud, (const double*)vd, (const double*)urem,
-      (const double*)vrem, gzs, (double*)dpo, (double*)pto, (double*)udo, (double*)vdo, st);
-  return cudaGetLastError();
-}
-
 cudaError_t remap_winds(const Geom& g, const RemapArgs& ra, const void* dp, const void* ud, const void* vd, void* urem,
                         void* vrem, int* trace, Status* st, cudaStream_t s) {
-  if (!FP64_FORM && !trace) {
-    if (g.L <= 32) return remap_winds_wl<1>(g, ra, dp, ud, vd, urem, vrem, st, s);
-    if (g.L <= 64) return remap_winds_wl<2>(g, ra, dp, ud, vd, urem, vrem, st, s);
-    return remap_winds_wl<4>(g, ra, dp, ud, vd, urem, vrem, st, s);
-  }
   if (g.L <= 32) return remap_winds_lm<32>(g, ra, dp, ud, vd, urem, vrem, trace, st, s);
   if (g.L <= 64) return remap_winds_lm<64>(g, ra, dp, ud, vd, urem, vrem, trace, st, s);
   return remap_winds_lm<MAX_LAYERS>(g, ra, dp, ud, vd, urem, vrem, trace, st, s);
@@ -164,11 +213,6 @@ cudaError_t remap_winds(const Geom& g, const RemapArgs& ra, const void* dp, cons
 cudaError_t remap_energy(const Geom& g, const RemapArgs& ra, const void* dp, const void* pt, const void* ud,
                          const void* vd, const void* urem, const void* vrem, const double* gzs, void* dpo, void* pto,
                          void* udo, void* vdo, int* trace, Status* st, cudaStream_t s) {
-  if (!FP64_FORM && !trace) {
-    if (g.L <= 32) return remap_energy_wl<1>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, st, s);
-    if (g.L <= 64) return remap_energy_wl<2>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, st, s);
-    return remap_energy_wl<4>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, st, s);
-  }
   if (g.L <= 32) return remap_energy_lm<32>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, trace, st, s);
   if (g.L <= 64) return remap_energy_lm<64>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, trace, st, s);
   return remap_energy_lm<MAX_LAYERS>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, trace, st, s);

@@ -11,8 +11,12 @@
 // barrier: the warps of a block are independent.
 //
 // The stage formulas, index shifts and evaluation order are those of the
-// tile kernels (atm_sweeps.cuh) and of the reference, so the FP64 results
-// are bit-identical to them.
+// tile kernels (atm_sweeps.cuh) and of the reference, so FP64 instances
+// are bit-identical to them (checked by the parity tests).  The mixed form
+// launches its C-momentum, D-mass and D-momentum sweeps as marching
+// kernels; in FP64 the tiles are faster (the marching FP64 sweeps execute
+// about as many instructions per cell, at 140-174 registers a thread and
+// 17 % warps active), so the FP64 form keeps them.
 #pragma once
 
 #include <type_traits>
@@ -138,22 +142,21 @@ struct MassM {
 };
 
 template <typename T, int TYS, bool CGRID, typename S, typename C>
-__global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_mass_m(Geom g, Consts c, const S* __restrict__ dp,
+__device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* __restrict__ dp,
                                                          const S* __restrict__ pt,
                                                          const typename MassM<T, CGRID, S, C>::UB* __restrict__ u,
                                                          const typename MassM<T, CGRID, S, C>::UB* __restrict__ v,
                                                          const double* __restrict__ heat,
                                                          typename MassM<T, CGRID, S, C>::O* __restrict__ dpo,
                                                          typename MassM<T, CGRID, S, C>::O* __restrict__ pto, int lo,
-                                                         int hi, int* nonfinite) {
+                                                         int hi, int* nonfinite, int sx, int sy, int k) {
   using UB = typename MassM<T, CGRID, S, C>::UB;
   using O = typename MassM<T, CGRID, S, C>::O;
   constexpr int V = CGRID ? PPM_UNC : PPM_NN;
   constexpr bool SAME = std::is_same_v<S, T>;
   const int lane = threadIdx.x & (MW - 1);
-  const int ox = lo + (blockIdx.x * MWARPS + (threadIdx.x >> 5)) * MOUT;
-  const int oy = lo + blockIdx.y * TYS;
-  const int k = blockIdx.z;
+  const int ox = lo + sx * MOUT;
+  const int oy = lo + sy * TYS;
   const int xhi = g.nx - 1 + hi, yhi = g.ny - 1 + hi;
   if (ox > xhi) return;  // the whole warp is past the region
   const int x = ox - MXH + lane;
@@ -321,6 +324,20 @@ __global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_mass_m(Geom g, 
   if (nonfinite) flag_nonfinite(nonfinite, bad);
 }
 
+// one warp per strip: blockIdx.x * MWARPS + warp across x, blockIdx.y
+// across y, blockIdx.z the layer
+template <typename T, int TYS, bool CGRID, typename S, typename C>
+__global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_mass_m(Geom g, Consts c, const S* __restrict__ dp,
+                                                         const S* __restrict__ pt,
+                                                         const typename MassM<T, CGRID, S, C>::UB* __restrict__ u,
+                                                         const typename MassM<T, CGRID, S, C>::UB* __restrict__ v,
+                                                         const double* __restrict__ heat,
+                                                         typename MassM<T, CGRID, S, C>::O* __restrict__ dpo,
+                                                         typename MassM<T, CGRID, S, C>::O* __restrict__ pto, int lo,
+                                                         int hi, int* nonfinite) {
+  mass_strip<T, TYS, CGRID, S, C>(g, c, dp, pt, u, v, heat, dpo, pto, lo, hi, nonfinite, blockIdx.x * MWARPS + (threadIdx.x >> 5), blockIdx.y, blockIdx.z);
+}
+
 // ======================================================== C-grid momentum ==
 // The C-grid momentum update of one layer (src/mod_sw_dyn.f90:294-414), as
 // k_c_mom2: kinetic energy from PPM fluxes of the C-grid winds with the
@@ -328,15 +345,15 @@ __global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_mass_m(Geom g, 
 // pressure-gradient force (:325-339) and the vorticity-flux updates of uc
 // and vc (:344-412).  Outputs on the interior; strips of TYS rows.
 template <typename T, int TYS, typename S, typename C>
-__global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_c_mom_m(Geom g, Consts c, const S* __restrict__ ud,
+__device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* __restrict__ ud,
                                                           const S* __restrict__ vd, const double* __restrict__ pkap,
                                                           const double* __restrict__ gz, C* __restrict__ uc,
-                                                          C* __restrict__ vc) {
+                                                          C* __restrict__ vc, int sx, int sy, int k) {
   constexpr int UNC = PPM_UNC;
   const int lane = threadIdx.x & (MW - 1);
-  const int ox = (blockIdx.x * MWARPS + (threadIdx.x >> 5)) * MOUT;
-  const int oy = blockIdx.y * TYS;
-  const int k = blockIdx.z, L = g.L;
+  const int ox = sx * MOUT;
+  const int oy = sy * TYS;
+  const int L = g.L;
   if (ox >= g.nx) return;  // the whole warp is past the region
   const int x = ox - MXH + lane;
   const bool out_lane = lane >= MXH && lane < MXH + MOUT && x < g.nx;
@@ -473,6 +490,16 @@ __global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_c_mom_m(Geom g,
   }
 }
 
+// one warp per strip: blockIdx.x * MWARPS + warp across x, blockIdx.y
+// across y, blockIdx.z the layer
+template <typename T, int TYS, typename S, typename C>
+__global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_c_mom_m(Geom g, Consts c, const S* __restrict__ ud,
+                                                          const S* __restrict__ vd, const double* __restrict__ pkap,
+                                                          const double* __restrict__ gz, C* __restrict__ uc,
+                                                          C* __restrict__ vc) {
+  c_mom_strip<T, TYS, S, C>(g, c, ud, vd, pkap, gz, uc, vc, blockIdx.x * MWARPS + (threadIdx.x >> 5), blockIdx.y, blockIdx.z);
+}
+
 // ======================================================== D-grid momentum ==
 // The D-grid momentum update of one layer (src/mod_sw_dyn.f90:634-771), as
 // k_d_mom2: kinetic energy from constrained-PPM fluxes of ud, vd with the
@@ -481,16 +508,16 @@ __global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_c_mom_m(Geom g,
 // (:682-702) and the vorticity-flux updates (:708-769).  Outputs on the
 // interior; strips of TYS rows.
 template <typename T, int TYS, typename S, typename C>
-__global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_d_mom_m(Geom g, Consts c, const S* __restrict__ ud,
+__device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* __restrict__ ud,
                                                           const S* __restrict__ vd, const C* __restrict__ uc,
                                                           const C* __restrict__ vc, const double* __restrict__ pkapb,
                                                           const double* __restrict__ gzb, S* __restrict__ udo,
-                                                          S* __restrict__ vdo, int* nonfinite) {
+                                                          S* __restrict__ vdo, int* nonfinite, int sx, int sy, int k) {
   constexpr int CON = PPM_CON;
   const int lane = threadIdx.x & (MW - 1);
-  const int ox = (blockIdx.x * MWARPS + (threadIdx.x >> 5)) * MOUT;
-  const int oy = blockIdx.y * TYS;
-  const int k = blockIdx.z, L = g.L;
+  const int ox = sx * MOUT;
+  const int oy = sy * TYS;
+  const int L = g.L;
   if (ox >= g.nx) return;  // the whole warp is past the region
   const int x = ox - MXH + lane;
   const bool out_lane = lane >= MXH && lane < MXH + MOUT && x < g.nx;
@@ -620,6 +647,17 @@ __global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_d_mom_m(Geom g,
     pb0y = pb0n; pb1y = pb1n; gb0y = gb0n; gb1y = gb1n;
   }
   flag_nonfinite(nonfinite, bad);
+}
+
+// one warp per strip: blockIdx.x * MWARPS + warp across x, blockIdx.y
+// across y, blockIdx.z the layer
+template <typename T, int TYS, typename S, typename C>
+__global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_d_mom_m(Geom g, Consts c, const S* __restrict__ ud,
+                                                          const S* __restrict__ vd, const C* __restrict__ uc,
+                                                          const C* __restrict__ vc, const double* __restrict__ pkapb,
+                                                          const double* __restrict__ gzb, S* __restrict__ udo,
+                                                          S* __restrict__ vdo, int* nonfinite) {
+  d_mom_strip<T, TYS, S, C>(g, c, ud, vd, uc, vc, pkapb, gzb, udo, vdo, nonfinite, blockIdx.x * MWARPS + (threadIdx.x >> 5), blockIdx.y, blockIdx.z);
 }
 
 }  // namespace atm

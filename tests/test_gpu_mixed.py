@@ -52,38 +52,3 @@ def test_mixed_form_is_deterministic():
     for f in ('dp', 'pt', 'ud', 'vd'):
         np.testing.assert_array_equal(a[f], b[f], err_msg=f)
 
-
-def _remap_state(kind, nlay):
-    if kind == 'ridged':  # some face coordinates not monotone: the sequential all-pairs path
-        st = ic.bubble_case(24, 20, nlay, 266e3, 266e3, radius=200e3)
-        pat = (np.where(np.isin(np.arange(st.ny) % 4, (1, 2)), 400.0, 9000.0)[:, None] * 0.5 +
-               np.where(np.isin(np.arange(st.nx) % 4, (1, 2)), 400.0, 9000.0)[None, :] * 0.5)
-        st.dp = st.dp.copy()
-        st.dp[3] = pat
-        return st
-    st = ic.jet_case(48, 40, nlay, 100e3, 100e3, width=600e3, seed=3)
-    rng = np.random.default_rng(nlay)
-    st.dp = st.dp * (1 + rng.uniform(-0.3, 0.3, st.dp.shape))  # source and target interfaces apart
-    st.pt = st.pt * (1 + rng.normal(0, 1e-3, st.pt.shape))
-    st.v = st.v + rng.normal(0, 1.0, st.v.shape)
-    return st
-
-
-@pytest.mark.parametrize('kind,nlay', [('jet', 20), ('jet', 64), ('jet', 100), ('ridged', 8)])
-def test_warp_remap_matches_sequential_remap(kind, nlay):
-    """The mixed form remaps with the warp-cooperative kernels (one warp per
-    column, scans with shuffles); the FP64 form with the sequential ones.
-    On the same FP64 state one remap of each agrees to rounding: the sums
-    are associated differently."""
-    st = _remap_state(kind, nlay)
-    out = {}
-    for form in ('fp64', 'mixed'):
-        g = Dycore(st, form)
-        g.remap()
-        assert g.check_stability()
-        out[form] = {f: g.get(f, halo=True) for f in ('dp', 'pt', 'ud', 'vd')}
-        g.close()
-    for f in ('dp', 'pt', 'ud', 'vd'):
-        a, b = out['fp64'][f], out['mixed'][f]
-        rel = np.abs(a - b).max() / np.abs(a).max()
-        assert rel <= 1e-11, (f, rel)
