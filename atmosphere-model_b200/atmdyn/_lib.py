@@ -34,7 +34,10 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_adj_dgrid_step', 'atm_adj_remap', 'atm_state_bytes', 'atm_state_save', 'atm_state_load',
            'atm_tape_bytes', 'atm_step_tape', 'atm_adj_step_tape', 'atm_output_enable', 'atm_output_reset',
            'atm_accumulate_output', 'atm_output_read', 'atm_output_time', 'atm_physics_tendencies',
-           'atm_apply_physics', 'atm_physics_halo', 'atm_device_wait_check')
+           'atm_apply_physics', 'atm_physics_halo', 'atm_device_wait_check',
+           'atm_ensemble_create', 'atm_ensemble_set_strips', 'atm_ensemble_set_stream', 'atm_ensemble_prepare',
+           'atm_ensemble_run', 'atm_ensemble_status', 'atm_ensemble_blocks', 'atm_ensemble_destroy',
+           'atm_ensemble_barrier_check')
 ATM_ADJ_IN, ATM_ADJ_OUT = 0, 1
 
 # the entry points every build must export
@@ -120,6 +123,15 @@ def load():
         'atm_apply_physics': ([vp, d], None),
         'atm_physics_halo': ([vp], None),
         'atm_device_wait_check': ([i, ctypes.POINTER(i)], None),
+        'atm_ensemble_create': ([ctypes.POINTER(vp), ctypes.POINTER(vp), P, i], None),
+        'atm_ensemble_set_strips': ([vp, i, i], None),
+        'atm_ensemble_set_stream': ([vp, vp], None),
+        'atm_ensemble_prepare': ([vp], None),
+        'atm_ensemble_run': ([vp, i, i], None),
+        'atm_ensemble_status': ([vp, ctypes.POINTER(i)], None),
+        'atm_ensemble_blocks': ([vp, ctypes.POINTER(i)], None),
+        'atm_ensemble_destroy': ([vp], None),
+        'atm_ensemble_barrier_check': ([ctypes.c_longlong, ctypes.POINTER(i)], None),
     }
     for f, (args, res) in optional.items():
         if hasattr(lib, f):

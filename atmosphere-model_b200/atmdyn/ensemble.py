@@ -16,13 +16,25 @@ idle.  :class:`Ensemble` therefore
 Every member is a full :class:`Dycore` (FP64 or mixed form) whose kernels
 are those of a single domain; the graph changes only how they are launched,
 so the results are bit-identical to stepping the members one by one.
+
+For the mixed form, :meth:`Ensemble.run_persistent` and
+:meth:`Ensemble.capture_persistent` advance every member with ONE launch of
+the library's persistent kernel (``atm_ensemble_*``): each stage of a step
+is a queue of warp-sized work items over all members, the stages are
+separated by bounded grid-wide barriers, and each member's sweeps use the
+strip height of an autotuned table keyed on its grid size
+(:meth:`Ensemble.autotune`).  The results are again bit-identical to
+stepping the members one by one.
 """
 from __future__ import annotations
 
+import ctypes
 import heapq
 
+import numpy as np
 import torch
 
+from . import _lib
 from .dycore import Dycore
 
 
@@ -54,8 +66,119 @@ class Ensemble:
 
     def close(self):
         self.graph = None
+        if getattr(self, 'ens', None) is not None:
+            _lib.load().atm_ensemble_destroy(self.ens)
+            self.ens = None
         for d in self.dyn:
             d.close()
+
+    # ---- the persistent kernel (mixed form)
+    def _ens(self):
+        if getattr(self, 'ens', None) is None:
+            lib = _lib.load()
+            n = len(self.dyn)
+            ctxs = (ctypes.c_void_p * n)(*[d.ctx.value for d in self.dyn])
+            dts = np.ascontiguousarray([st.dt for st in self.members], dtype=np.float64)
+            h = ctypes.c_void_p()
+            _lib.check(lib.atm_ensemble_create(ctypes.byref(h), ctxs, dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               n), None, 'atm_ensemble_create')
+            self.ens = h
+            self.strips = {}
+        return self.ens
+
+    def set_strips(self, table):
+        """Strip height of the marching sweeps per member grid size, {nx: rows}."""
+        lib = _lib.load()
+        e = self._ens()
+        for i, st in enumerate(self.members):
+            rows = table.get(st.nx, 64)
+            _lib.check(lib.atm_ensemble_set_strips(e, i, rows), None, 'atm_ensemble_set_strips')
+        self.strips = dict(table)
+
+    def _prepare(self, stream):
+        lib = _lib.load()
+        e = self._ens()
+        _lib.check(lib.atm_ensemble_set_stream(e, ctypes.c_void_p(stream)), None, 'atm_ensemble_set_stream')
+        torch.cuda.synchronize()
+        _lib.check(lib.atm_ensemble_prepare(e), None, 'atm_ensemble_prepare')
+
+    def run_persistent(self, nsteps: int, remap_every: int):
+        """One launch of the persistent kernel: nsteps steps of every member
+        from the current one (which must follow a remap when remap_every > 0,
+        as the remap is due after every remap_every-th step of the launch)."""
+        assert remap_every == 0 or self.steps_done % remap_every == 0
+        lib = _lib.load()
+        stream = torch.cuda.current_stream()
+        self._prepare(stream.cuda_stream)
+        _lib.check(lib.atm_ensemble_run(self.ens, nsteps, remap_every), None, 'atm_ensemble_run')
+        self.steps_done += nsteps
+
+    def barrier_timed_out(self):
+        v = ctypes.c_int(0)
+        _lib.check(_lib.load().atm_ensemble_status(self._ens(), ctypes.byref(v)), None, 'atm_ensemble_status')
+        return bool(v.value)
+
+    def capture_persistent(self, remap_every: int, cycles: int):
+        """The persistent launch of cycles remap cycles as a CUDA graph (one
+        kernel node): each replay advances every member by remap_every *
+        cycles steps.  The launch must swap the time levels an even number of
+        times: (remap_every + 1) * cycles even."""
+        assert self.steps_done % remap_every == 0 and ((remap_every + 1) * cycles) % 2 == 0
+        lib = _lib.load()
+        cap = torch.cuda.Stream()
+        self._prepare(cap.cuda_stream)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=cap):
+            _lib.check(lib.atm_ensemble_run(self.ens, remap_every * cycles, remap_every), None, 'atm_ensemble_run')
+        self.graph = g
+        self.cycle = remap_every * cycles
+        return g
+
+    def autotune(self, rows=(16, 32, 64), steps: int = 2, reps: int = 2):
+        """The strip height of each grid size's members: for each size (in
+        turn, the others at their best so far) the fastest of ``rows`` over
+        ``steps`` steps of the persistent kernel without remap, timed on the
+        device; the members' states are restored afterwards.  Returns the
+        table {nx: rows}."""
+        assert steps % 2 == 0  # the time levels come back where they were
+        saved = []
+        for d in self.dyn:
+            buf = torch.empty(d.state_bytes() // 8, dtype=torch.float64, device='cuda')
+            d.state_save(buf.data_ptr())
+            saved.append(buf)
+        torch.cuda.synchronize()
+        lib = _lib.load()
+        table = {st.nx: 64 for st in self.members}
+        done = self.steps_done
+        timings = {}
+        for nx in sorted(table):
+            best = None
+            for r in rows:
+                trial = dict(table)
+                trial[nx] = r
+                self.set_strips(trial)
+                ms = []
+                for _ in range(reps):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    self._prepare(torch.cuda.current_stream().cuda_stream)
+                    e0.record()
+                    _lib.check(lib.atm_ensemble_run(self.ens, steps, 0), None, 'atm_ensemble_run')
+                    e1.record()
+                    torch.cuda.synchronize()
+                    ms.append(e0.elapsed_time(e1))
+                t = min(ms)
+                timings[(nx, r)] = t
+                if best is None or t < best[0]:
+                    best = (t, r)
+            table[nx] = best[1]
+        for d, buf in zip(self.dyn, saved):
+            d.state_load(buf.data_ptr())
+        torch.cuda.synchronize()
+        self.steps_done = done
+        self.set_strips(table)
+        self.autotune_ms = timings
+        return table
 
     def _cycle(self, remap_every):
         for _ in range(remap_every):

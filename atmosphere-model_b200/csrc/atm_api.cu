@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "atmdyn.h"
+#include "atm_ensemble.cuh"
 #include "atm_ops.h"
 #include "atm_physics.h"
 
@@ -1340,6 +1341,213 @@ int atm_physics_halo(atm_ctx* ctx) {
   Stage t(ctx, S_PHYS_HALO);
   CK(atm::ops_fp64.ring(ctx->geo, ts1, nullptr, 1, 1, false, ctx->stream));
   return ATM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------- persistent ensemble --
+// Config 5: many members of the mixed form advanced in one cooperative
+// launch of the persistent kernel (atm_ensemble.cuh).
+struct atm_ens {
+  std::vector<atm_ctx*> m;
+  std::vector<double> dt;
+  std::vector<int> tys;
+  atm::EnsMember* d_members = nullptr;
+  long long* d_off = nullptr;
+  unsigned* d_bar = nullptr;  // arrival count, generation
+  int* d_err = nullptr;
+  int* h_err = nullptr;  // pinned
+  int blocks = 0;
+  long long timeout_ns = 2000000000LL;
+  cudaStream_t stream = nullptr;
+  bool prepared = false;
+  int pending_flips = 0;  // time-level swaps of the launches since the last prepare
+};
+
+namespace {
+
+int ens_free(atm_ens* e) {
+  if (!e) return ATM_ERR_ARG;
+  cudaFree(e->d_members);
+  cudaFree(e->d_off);
+  cudaFree(e->d_bar);
+  cudaFree(e->d_err);
+  if (e->h_err) cudaFreeHost(e->h_err);
+  delete e;
+  return ATM_OK;
+}
+
+// the members' descriptors and the stage work prefix sums, to the device
+int ens_upload(atm_ens* e) {
+  const int n = (int)e->m.size();
+  std::vector<atm::EnsMember> hm(n);
+  std::vector<long long> off((size_t)atm::E_NSTAGE * (n + 1), 0);
+  for (int i = 0; i < n; ++i) {
+    atm_ctx* c = e->m[i];
+    atm::EnsMember& d = hm[i];
+    d.g = c->geo;
+    d.cc = step_consts(c, e->dt[i] / 2.);
+    d.cd = step_consts(c, e->dt[i]);
+    d.ra = remap_args(c);
+    for (int t = 0; t < 2; ++t)
+      for (int f = 0; f < 4; ++f) d.st[t][f] = c->st[t][f];
+    for (int f = 0; f < 4; ++f) d.cg[f] = c->cg[f];
+    d.pkap = c->pkap;
+    d.gz = c->gz;
+    d.pkapb = c->pkapb;
+    d.gzb = c->gzb;
+    d.urem = c->urem;
+    d.vrem = c->vrem;
+    d.status = c->status;
+    d.cur0 = c->cur;
+    d.tys = e->tys[i];
+  }
+  for (int s = 0; s < atm::E_NSTAGE; ++s)
+    for (int i = 0; i < n; ++i)
+      off[(size_t)s * (n + 1) + i + 1] = off[(size_t)s * (n + 1) + i] + atm::ens_items(hm[i].g, s, hm[i].tys);
+  if (cudaMemcpy(e->d_members, hm.data(), sizeof(atm::EnsMember) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(e->d_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return ATM_ERR_CUDA;
+  return ATM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int atm_ensemble_create(atm_ens** out, atm_ctx* const* members, const double* dts, int n) {
+  if (!out || !members || !dts || n <= 0) return ATM_ERR_ARG;
+  *out = nullptr;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return ATM_ERR_CUDA;
+  for (int i = 0; i < n; ++i) {
+    atm_ctx* c = members[i];
+    // the kernel holds the mixed form's sweeps, remaps at most 64 layers
+    // and has no radiative heating term
+    if (!c || !c->initialized || c->precision != ATM_MIXED || c->heating || c->L > 64 || c->device != dev ||
+        !(dts[i] > 0.))
+      return ATM_ERR_ARG;
+  }
+  atm_ens* e = new atm_ens();
+  e->m.assign(members, members + n);
+  e->dt.assign(dts, dts + n);
+  e->tys.assign(n, 64);
+  e->stream = members[0]->stream;
+  e->blocks = atm::ensemble_max_blocks();
+  const size_t off_bytes = sizeof(long long) * atm::E_NSTAGE * (n + 1);
+  if (e->blocks <= 0 || cudaMalloc((void**)&e->d_members, sizeof(atm::EnsMember) * n) != cudaSuccess ||
+      cudaMalloc((void**)&e->d_off, off_bytes) != cudaSuccess ||
+      cudaMalloc((void**)&e->d_bar, 2 * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc((void**)&e->d_err, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost((void**)&e->h_err, sizeof(int)) != cudaSuccess) {
+    ens_free(e);
+    return ATM_ERR_NOMEM;
+  }
+  *out = e;
+  return ATM_OK;
+}
+
+int atm_ensemble_set_strips(atm_ens* e, int member, int rows) {
+  if (!e || member < 0 || member >= (int)e->m.size() || (rows != 16 && rows != 32 && rows != 64)) return ATM_ERR_ARG;
+  e->tys[member] = rows;
+  e->prepared = false;
+  return ATM_OK;
+}
+
+int atm_ensemble_set_stream(atm_ens* e, void* stream) {
+  if (!e) return ATM_ERR_ARG;
+  e->stream = (cudaStream_t)stream;
+  return ATM_OK;
+}
+
+int atm_ensemble_prepare(atm_ens* e) {
+  if (!e) return ATM_ERR_ARG;
+  for (atm_ctx* c : e->m)
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return ATM_ERR_CUDA;
+  if (cudaStreamSynchronize(e->stream) != cudaSuccess) return ATM_ERR_CUDA;
+  int r = ens_upload(e);
+  if (r) return r;
+  e->prepared = true;
+  e->pending_flips = 0;
+  return ATM_OK;
+}
+
+int atm_ensemble_run(atm_ens* e, int nsteps, int remap_every) {
+  if (!e || nsteps <= 0 || remap_every < 0) return ATM_ERR_ARG;
+  if (!e->prepared) return ATM_ERR_STATE;
+  // each launch starts from the time levels recorded at prepare: the
+  // launches since then must have swapped them an even number of times
+  if (e->pending_flips % 2) return ATM_ERR_STATE;
+  const int n = (int)e->m.size();
+  const int remaps = remap_every > 0 ? nsteps / remap_every : 0;
+  if (cudaMemsetAsync(e->d_bar, 0, 2 * sizeof(unsigned), e->stream) != cudaSuccess ||
+      cudaMemsetAsync(e->d_err, 0, sizeof(int), e->stream) != cudaSuccess)
+    return ATM_ERR_CUDA;
+  for (atm_ctx* c : e->m)
+    if (cudaMemsetAsync(&c->status->nonfinite_step, 0, 2 * sizeof(int), e->stream) != cudaSuccess) return ATM_ERR_CUDA;
+  atm::EnsPlan p{e->d_members, e->d_off, n, nsteps, remap_every, e->d_bar, (unsigned)e->blocks, e->d_err,
+                 e->timeout_ns};
+  if (atm::ensemble_launch(p, e->blocks, e->stream) != cudaSuccess) return ATM_ERR_CUDA;
+  const int flips = nsteps + remaps;
+  e->pending_flips += flips;
+  for (atm_ctx* c : e->m) {
+    c->cur ^= (flips & 1);
+    c->flag_valid = false;  // the stability check reads the state itself
+    c->launches += 1;
+  }
+  return ATM_OK;
+}
+
+int atm_ensemble_status(atm_ens* e, int* barrier_timed_out) {
+  if (!e || !barrier_timed_out) return ATM_ERR_ARG;
+  if (cudaMemcpyAsync(e->h_err, e->d_err, sizeof(int), cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
+      cudaStreamSynchronize(e->stream) != cudaSuccess)
+    return ATM_ERR_CUDA;
+  *barrier_timed_out = *e->h_err;
+  return ATM_OK;
+}
+
+int atm_ensemble_blocks(atm_ens* e, int* blocks) {
+  if (!e || !blocks) return ATM_ERR_ARG;
+  *blocks = e->blocks;
+  return ATM_OK;
+}
+
+int atm_ensemble_destroy(atm_ens* e) {
+  if (!e) return ATM_ERR_ARG;
+  cudaStreamSynchronize(e->stream);
+  return ens_free(e);
+}
+
+int atm_ensemble_barrier_check(long long timeout_ns, int* timed_out) {
+  if (timeout_ns <= 0 || timeout_ns > 2000000000LL || !timed_out) return ATM_ERR_ARG;
+  const int blocks = atm::ensemble_max_blocks();
+  if (blocks <= 0) return ATM_ERR_CUDA;
+  long long* d_off = nullptr;
+  unsigned* d_bar = nullptr;
+  int* d_err = nullptr;
+  int rc = ATM_OK;
+  int h = 0;
+  if (cudaMalloc((void**)&d_off, sizeof(long long) * atm::E_NSTAGE) != cudaSuccess ||
+      cudaMalloc((void**)&d_bar, 2 * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc((void**)&d_err, sizeof(int)) != cudaSuccess) {
+    rc = ATM_ERR_NOMEM;
+  } else if (cudaMemset(d_off, 0, sizeof(long long) * atm::E_NSTAGE) != cudaSuccess ||
+             cudaMemset(d_bar, 0, 2 * sizeof(unsigned)) != cudaSuccess || cudaMemset(d_err, 0, sizeof(int)) != cudaSuccess) {
+    rc = ATM_ERR_CUDA;
+  } else {
+    // no members, one step: the first barrier waits for one block more than
+    // the grid holds, so its wait runs out in every block
+    atm::EnsPlan p{nullptr, d_off, 0, 1, 0, d_bar, (unsigned)blocks + 1, d_err, timeout_ns};
+    if (atm::ensemble_launch(p, blocks, 0) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = ATM_ERR_CUDA;
+  }
+  cudaFree(d_off);
+  cudaFree(d_bar);
+  cudaFree(d_err);
+  *timed_out = h;
+  return rc;
 }
 
 }  // extern "C"

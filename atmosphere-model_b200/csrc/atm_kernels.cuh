@@ -58,12 +58,12 @@ __device__ __forceinline__ bool finite_(float v) { return isfinite(v); }
 // written), so no shared memory limits the occupancy.  The next layer's dp
 // is loaded one iteration ahead so that its latency overlaps atm_pow.
 template <typename T>
-__global__ void __launch_bounds__(128) k_column(Geom g, Consts c, const T* __restrict__ dpl, const T* __restrict__ ptl,
-                                                double* __restrict__ pkap, double* __restrict__ gz, int lo, int hi,
-                                                double* __restrict__ plev_out) {
+__device__ __forceinline__ void column_at(const Geom& g, const Consts& c, const T* __restrict__ dpl,
+                                          const T* __restrict__ ptl, double* __restrict__ pkap,
+                                          double* __restrict__ gz, int lo, int hi, double* __restrict__ plev_out,
+                                          int col) {
   const int w = g.nx - lo + hi;
   const int hgt = g.ny - lo + hi;
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= w * hgt) return;
   const int x = lo + col % w, y = lo + col / w;
   const long long o = g.at(x, y);
@@ -90,6 +90,14 @@ __global__ void __launch_bounds__(128) k_column(Geom g, Consts c, const T* __res
     gz[o + (long long)(k + 1) * S] = z;
     pk0 = pk1;
   }
+}
+
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_column(Geom g, Consts c, const T* __restrict__ dpl, const T* __restrict__ ptl,
+                                                double* __restrict__ pkap, double* __restrict__ gz, int lo, int hi,
+                                                double* __restrict__ plev_out) {
+  column_at<T>(g, c, dpl, ptl, pkap, gz, lo, hi, plev_out, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Heating rate of the layer from the radiative net flux,
@@ -133,10 +141,10 @@ __device__ __forceinline__ double corner(const double* q, long long o, int P) {
   return out;
 }
 
-static __global__ void k_corners(Geom g, const double* __restrict__ pkap, const double* __restrict__ gz,
-                          double* __restrict__ pkapb, double* __restrict__ gzb, int with_pkap, int lev0, int nlev) {
+__device__ __forceinline__ void corner_at(const Geom& g, const double* __restrict__ pkap, const double* __restrict__ gz,
+                                          double* __restrict__ pkapb, double* __restrict__ gzb, int with_pkap, int lev0,
+                                          int nlev, int idx) {
   const int w = g.nx + 1, h = g.ny + 1;
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= w * h) return;
   const int x = idx % w, y = idx / w;
   for (int l = lev0; l < lev0 + nlev; ++l) {
@@ -147,17 +155,22 @@ static __global__ void k_corners(Geom g, const double* __restrict__ pkap, const 
   }
 }
 
+static __global__ void k_corners(Geom g, const double* __restrict__ pkap, const double* __restrict__ gz,
+                          double* __restrict__ pkapb, double* __restrict__ gzb, int with_pkap, int lev0, int nlev) {
+  corner_at(g, pkap, gz, pkapb, gzb, with_pkap, lev0, nlev, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // =============================================================== halos ====
 // Periodic fill of the 7-wide ring (the single-image halo_exchange,
 // src/mod_sync.f90:67-217): every ring point takes the value of its
 // periodic image in the interior.  With copy = true the ring of src is
 // copied to dst instead (the ring of a new time level keeps the old ring).
+// ring point idx of level k of one field f (src: the copy's source)
 template <typename T, bool COPY>
-__global__ void k_ring(Geom g, T* f0, T* f1, T* f2, T* f3, const T* s0, const T* s1, const T* s2, const T* s3, int K) {
+__device__ __forceinline__ void ring_at(const Geom& g, T* f, const T* s, int idx, int k) {
   const int wide = g.nx + 2 * H;
   const int nband = 2 * H * wide;
   const int nring = nband + 2 * H * g.ny;
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= nring) return;
   int x, y;
   if (idx < nband) {
@@ -170,11 +183,6 @@ __global__ void k_ring(Geom g, T* f0, T* f1, T* f2, T* f3, const T* s0, const T*
     int cc = q % (2 * H);
     x = cc < H ? cc - H : g.nx + (cc - H);
   }
-  const int k = blockIdx.y;
-  if (k >= K) return;
-  const int fld = blockIdx.z;
-  T* f = fld == 0 ? f0 : fld == 1 ? f1 : fld == 2 ? f2 : f3;
-  const T* s = fld == 0 ? s0 : fld == 1 ? s1 : fld == 2 ? s2 : s3;
   long long o = g.at(x, y, k);
   if (COPY) {
     f[o] = s[o];
@@ -183,6 +191,16 @@ __global__ void k_ring(Geom g, T* f0, T* f1, T* f2, T* f3, const T* s0, const T*
     int ys = y < 0 ? y + g.ny : (y >= g.ny ? y - g.ny : y);
     f[o] = f[g.at(xs, ys, k)];
   }
+}
+
+template <typename T, bool COPY>
+__global__ void k_ring(Geom g, T* f0, T* f1, T* f2, T* f3, const T* s0, const T* s1, const T* s2, const T* s3, int K) {
+  const int k = blockIdx.y;
+  if (k >= K) return;
+  const int fld = blockIdx.z;
+  T* f = fld == 0 ? f0 : fld == 1 ? f1 : fld == 2 ? f2 : f3;
+  const T* s = fld == 0 ? s0 : fld == 1 ? s1 : fld == 2 ? s2 : s3;
+  ring_at<T, COPY>(g, f, s, blockIdx.x * blockDim.x + threadIdx.x, k);
 }
 
 // ========================================================= vertical remap ==
@@ -549,16 +567,15 @@ __device__ __noinline__ void remap_winds_full(const Geom& g, const RemapArgs& ra
 
 // One thread per face column and direction (blockIdx.y); three column
 // arrays of LM + 2 doubles per thread.
+// face column col of direction dir (0: u, 1: v)
 template <typename T, int LM>
-__global__ void __launch_bounds__(64) k_remap_winds(Geom g, RemapArgs ra, const T* __restrict__ dp,
-                                                    const T* __restrict__ ud, const T* __restrict__ vd,
-                                                    T* __restrict__ urem, T* __restrict__ vrem, int* trace,
-                                                    Status* st) {
+__device__ __forceinline__ void remap_winds_at(const Geom& g, const RemapArgs& ra, const T* __restrict__ dp,
+                                               const T* __restrict__ ud, const T* __restrict__ vd,
+                                               T* __restrict__ urem, T* __restrict__ vrem, int* trace, Status* st,
+                                               int col, int dir) {
   const int w = g.nx + 2, h = g.ny + 2;
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= w * h) return;
   const int i = -1 + col % w, j = -1 + col / w;
-  const int dir = blockIdx.y;
   const int L = g.L;
   const long long S = g.S;
   const T* f = dir == 0 ? ud : vd;
@@ -621,6 +638,14 @@ __global__ void __launch_bounds__(64) k_remap_winds(Geom g, RemapArgs ra, const 
   }
   auto var = [&](int k) { return (double)f[oa + (long long)(k - 1) * S]; };
   remap_merge(L, sc, lv, gam, var, dc, [&](int m, double v) { r[oa + (long long)(m - 1) * S] = T(v); }, tr, 1);
+}
+
+template <typename T, int LM>
+__global__ void __launch_bounds__(64) k_remap_winds(Geom g, RemapArgs ra, const T* __restrict__ dp,
+                                                    const T* __restrict__ ud, const T* __restrict__ vd,
+                                                    T* __restrict__ urem, T* __restrict__ vrem, int* trace,
+                                                    Status* st) {
+  remap_winds_at<T, LM>(g, ra, dp, ud, vd, urem, vrem, trace, st, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
 
 // Energy remap and potential-temperature recovery on the interior,
@@ -690,14 +715,14 @@ __device__ __noinline__ void remap_energy_full(const Geom& g, const RemapArgs& r
 
 // One thread per interior column; four column arrays of LM + 2 doubles per
 // thread (levels, pkap then the eliminated interface values, energy, gam).
+// interior column col
 template <typename T, int LM>
-__global__ void __launch_bounds__(64) k_remap_energy(Geom g, RemapArgs ra, const T* __restrict__ dp,
-                                                     const T* __restrict__ pt, const T* __restrict__ ud,
-                                                     const T* __restrict__ vd, const T* __restrict__ urem,
-                                                     const T* __restrict__ vrem, const double* __restrict__ gzs,
-                                                     T* __restrict__ dpo, T* __restrict__ pto, T* __restrict__ udo,
-                                                     T* __restrict__ vdo, int* trace, Status* st) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void remap_energy_at(const Geom& g, const RemapArgs& ra, const T* __restrict__ dp,
+                                                const T* __restrict__ pt, const T* __restrict__ ud,
+                                                const T* __restrict__ vd, const T* __restrict__ urem,
+                                                const T* __restrict__ vrem, const double* __restrict__ gzs,
+                                                T* __restrict__ dpo, T* __restrict__ pto, T* __restrict__ udo,
+                                                T* __restrict__ vdo, int* trace, Status* st, int col) {
   if (col >= g.nx * g.ny) return;
   const int i = col % g.nx, j = col / g.nx;
   const int L = g.L;
@@ -789,6 +814,17 @@ __global__ void __launch_bounds__(64) k_remap_energy(Geom g, RemapArgs ra, const
   };
   remap_merge(L, plev, lv, gam, [&](int k) { return en[k]; }, tpl, put, tr, 1);
   flag_nonfinite(&st->nonfinite_remap, bad);
+}
+
+template <typename T, int LM>
+__global__ void __launch_bounds__(64) k_remap_energy(Geom g, RemapArgs ra, const T* __restrict__ dp,
+                                                     const T* __restrict__ pt, const T* __restrict__ ud,
+                                                     const T* __restrict__ vd, const T* __restrict__ urem,
+                                                     const T* __restrict__ vrem, const double* __restrict__ gzs,
+                                                     T* __restrict__ dpo, T* __restrict__ pto, T* __restrict__ udo,
+                                                     T* __restrict__ vdo, int* trace, Status* st) {
+  remap_energy_at<T, LM>(g, ra, dp, pt, ud, vd, urem, vrem, gzs, dpo, pto, udo, vdo, trace, st,
+                         blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ============================================================ reductions ===

@@ -25,14 +25,20 @@ constexpr int TY_CMASS = FP64_FORM ? 4 : 16;
 constexpr int TY_DMASS = FP64_FORM ? 6 : 16;
 constexpr int TY_CMOM = 8;
 constexpr int TY_DMOM = 4;
-// The mixed form runs its C-grid momentum, D-grid mass and D-grid momentum
-// sweeps as column-marching kernels (atm_march.cuh), measured faster than
-// its tiles there (B200, 1024x1024x64: 2.83 / 2.01 / 2.82 ms against 3.01 /
-// 2.66 / 4.05); its C-grid mass sweep (2.70 ms against 2.94) and every
-// FP64 sweep (13 FP64 sweep-ms against 29 marching: at 136-174 registers
-// a thread the marching kernels hold too few warps to hide FP64 latency)
-// keep the tiles.
-constexpr bool MARCH = !FP64_FORM;
+// The mixed form (ATM_MARCH_SWEEPS) runs its four sweeps as column-marching
+// kernels (atm_march.cuh): measured on B200 at 1024x1024x64 against its
+// tiles, C momentum 2.83 / D mass 2.01 / D momentum 2.82 ms against 3.01 /
+// 2.66 / 4.05, and C mass 2.94 against 2.70 (kept marching so that the
+// persistent ensemble kernel, which has only the marching sweeps, is
+// bit-identical to it).  The FP64 form keeps the tiles: its marching
+// sweeps took 29.1 ms a step against 17.4 (at 136-174 registers a thread
+// they hold too few warps to hide the FP64 latency, and they execute about
+// as many instructions per cell).
+#ifdef ATM_MARCH_SWEEPS
+constexpr bool MARCH = true;
+#else
+constexpr bool MARCH = false;
+#endif
 // strip height (output rows a warp walks through) of the marching sweeps
 constexpr int TYS = 64;
 
@@ -68,6 +74,17 @@ cudaError_t setup() {
 cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt, const void* u, const void* v,
                  const double* heat, void* dpo, void* pto, int lo, int hi, int* nonfinite, int* timeout, bool cgrid,
                  cudaStream_t s) {
+#ifdef ATM_MARCH_SWEEPS
+  if constexpr (MARCH) {
+    if (cgrid)  // state in, C-grid fields out
+      k_mass_m<T, TYS, true, S, C><<<strips(lo, hi, g, TYS), MW * MWARPS, 0, s>>>(
+          g, c, (const S*)dp, (const S*)pt, (const S*)u, (const S*)v, heat, (C*)dpo, (C*)pto, lo, hi, nonfinite);
+    else  // state and C-grid winds in, state out
+      k_mass_m<T, TYS, false, S, C><<<strips(lo, hi, g, TYS), MW * MWARPS, 0, s>>>(
+          g, c, (const S*)dp, (const S*)pt, (const C*)u, (const C*)v, heat, (S*)dpo, (S*)pto, lo, hi, nonfinite);
+    return cudaGetLastError();
+  }
+#endif
   CUtensorMap md, mp, mu, mv;
   cudaError_t e;
   if (cgrid) {  // state in, C-grid fields out
@@ -80,9 +97,6 @@ cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt,
       return e;
     k_mass2<T, TX, TY_CMASS, true, S, C><<<grid, NT, Lay::bytes, s>>>(md, mp, mu, mv, g, c, heat, (C*)dpo,
                                                                        (C*)pto, lo, hi, nonfinite, timeout);
-  } else if constexpr (MARCH) {  // state and C-grid winds in, state out
-    k_mass_m<T, TYS, false, S, C><<<strips(lo, hi, g, TYS), MW * MWARPS, 0, s>>>(
-        g, c, (const S*)dp, (const S*)pt, (const C*)u, (const C*)v, heat, (S*)dpo, (S*)pto, lo, hi, nonfinite);
   } else {
     using Lay = MassL<T, TX, TY_DMASS, false, S, C>;
     dim3 grid = tiles(lo, hi, g, g.L, TY_DMASS);
@@ -119,11 +133,13 @@ cudaError_t heating(const Geom& g, const Consts& c, const void* dpl, int es, con
 
 cudaError_t c_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const double* pkap, const double* gz,
                   void* uc, void* vc, int* timeout, cudaStream_t s) {
+#ifdef ATM_MARCH_SWEEPS
   if constexpr (MARCH) {
     k_c_mom_m<T, TYS, S, C><<<strips(0, 0, g, TYS), MW * MWARPS, 0, s>>>(g, c, (const S*)ud, (const S*)vd, pkap, gz,
                                                                           (C*)uc, (C*)vc);
     return cudaGetLastError();
   }
+#endif
   using Lay = CMomL<T, TX, TY_CMOM, S>;
   constexpr int es = sizeof(S);
   CUtensorMap mu, mv, muL, mvL, mpk, mgz;
@@ -140,11 +156,13 @@ cudaError_t c_mom(const Geom& g, const Consts& c, const void* ud, const void* vd
 cudaError_t d_mom(const Geom& g, const Consts& c, const void* ud, const void* vd, const void* uc, const void* vc,
                   const double* pkapb, const double* gzb, void* udo, void* vdo, int* nonfinite, int* timeout,
                   cudaStream_t s) {
+#ifdef ATM_MARCH_SWEEPS
   if constexpr (MARCH) {
     k_d_mom_m<T, TYS, S, C><<<strips(0, 0, g, TYS), MW * MWARPS, 0, s>>>(
         g, c, (const S*)ud, (const S*)vd, (const C*)uc, (const C*)vc, pkapb, gzb, (S*)udo, (S*)vdo, nonfinite);
     return cudaGetLastError();
   }
+#endif
   using Lay = DMomL<T, TX, TY_DMOM, S, C>;
   constexpr int es = sizeof(S), ec = sizeof(C);
   CUtensorMap mu, mv, muL, mvL, muc, mvc, mpb, mgb;

@@ -93,6 +93,12 @@ cudaError_t adj_remap_winds(const Geom&, const RemapArgs&, const double* dp, con
                             const double* lam_ur, const double* lam_vr, double* lam_dp, double* lam_ud, double* lam_vd,
                             cudaStream_t);
 
+// the persistent ensemble kernel of the mixed form (atm_ensemble.cuh): its
+// largest cooperative grid on the current device, and one launch of a plan
+struct EnsPlan;
+int ensemble_max_blocks();
+cudaError_t ensemble_launch(const EnsPlan& plan, int blocks, cudaStream_t);
+
 // largest number of layers the vertical remap supports
 constexpr int MAX_LAYERS = 128;
 

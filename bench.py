@@ -740,9 +740,10 @@ def adjoint_leg(args, torch, max_over_ranks, world):
 def ensemble_leg(args, torch):
     """The batched ensemble: 64 members of uneven sizes (grids from
     {64, 128, 256, 512}^2, layers from {20, 32, 48, 64}, bubble or jet,
-    seed 3), mixed form, remap every 5 steps, 100 steps: the whole run
-    captured over 8 streams as one CUDA graph and replayed as one launch,
-    against launching the members one by one on one stream; then the
+    seed 3), mixed form, remap every 5 steps, 100 steps: as one launch of
+    the persistent kernel captured in a CUDA graph (strip heights autotuned
+    per grid size), as the per-member kernels captured over 8 streams in
+    one graph, and launching the members one by one on one stream; then the
     gradient of J = sum(mask theta^2) of 8 members (FP64 form, 20 steps,
     checkpoints every 5)."""
     from atmdyn import ic
@@ -785,6 +786,32 @@ def ensemble_leg(args, torch):
                     'stable': ens.stable()}
     out['one_stream_eager'] = {'cell_steps_per_s': out['cells'] / t_seq, 'ms_per_step': 1e3 * t_seq}
     out['graph_speedup'] = out['graph']['cell_steps_per_s'] / out['one_stream_eager']['cell_steps_per_s']
+    ens.close()
+    del ens
+    torch.cuda.empty_cache()
+    # the persistent kernel: strip heights autotuned per grid size, then the
+    # 100 steps as ONE cooperative launch captured in a CUDA graph
+    ens = Ensemble(members, 'mixed', nstreams=1)
+    ens.step_eager(5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    table = ens.autotune(steps=2, reps=2)
+    t_tune = time.perf_counter() - t0
+    ens.capture_persistent(5, cycles=nsteps // 5)
+    ens.replay(1)  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.replay(1)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out['persistent'] = {'cell_steps_per_s': out['cells'] * nsteps / (ms * 1e-3), 'ms_per_step': ms / nsteps,
+                         'steps': nsteps, 'kernel_launches': 1, 'graph_launches': 1,
+                         'strip_rows_by_grid': {str(k): v for k, v in sorted(table.items())},
+                         'autotune_s': t_tune, 'barrier_timed_out': ens.barrier_timed_out(),
+                         'stable': ens.stable()}
+    out['persistent_speedup_vs_stream_graph'] = out['persistent']['cell_steps_per_s'] / out['graph']['cell_steps_per_s']
     ens.close()
     del ens
     torch.cuda.empty_cache()

@@ -210,6 +210,41 @@ int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, const double* 
                       double* dp_out, double* pt_out, double* ud_out, double* vd_out, void* stream,
                       int* stable, int* fallback_columns);
 
+/* ---- persistent ensemble (config 5; no counterpart in the reference) ----
+   Many independent domains of the mixed form (members of uneven sizes, each
+   a context made by atm_create/atm_init) advanced together by ONE
+   cooperative launch of a persistent kernel: every stage of a step is a
+   work queue of warp-sized items over all members, and the stages are
+   separated by grid-wide barriers whose waits are bounded (about two
+   seconds; a wait that runs out raises the status word read by
+   atm_ensemble_status and ends the launch).  Members hold at most 64
+   layers, use no net flux, live on the current device; dts gives each
+   member's time step.  A member's results are bit-identical to stepping it
+   alone with atm_step.
+   atm_ensemble_prepare copies the members' descriptors (their current time
+   levels and strip heights) to the device; call it after changing a
+   member outside the ensemble and before stream capture.
+   atm_ensemble_run enqueues one launch of nsteps steps on the ensemble's
+   stream (the first member's unless set), the remap after every
+   remap_every-th step counted from the launch (0: none); successive launches
+   after one prepare must each swap the time levels an even number of times
+   (nsteps + nsteps / remap_every even), so that a captured launch can be
+   replayed.  atm_ensemble_set_strips sets a member's strip height of the
+   marching sweeps (16, 32 or 64 rows; default 64).
+   atm_ensemble_barrier_check launches the kernel with no members and a
+   barrier that waits for one block more than the grid holds: *timed_out
+   reports that the bounded wait ran out and the launch ended. */
+typedef struct atm_ens atm_ens;
+int atm_ensemble_create(atm_ens** out, atm_ctx* const* members, const double* dts, int n);
+int atm_ensemble_set_strips(atm_ens* e, int member, int rows);
+int atm_ensemble_set_stream(atm_ens* e, void* stream);
+int atm_ensemble_prepare(atm_ens* e);
+int atm_ensemble_run(atm_ens* e, int nsteps, int remap_every);
+int atm_ensemble_status(atm_ens* e, int* barrier_timed_out);
+int atm_ensemble_blocks(atm_ens* e, int* blocks);
+int atm_ensemble_destroy(atm_ens* e);
+int atm_ensemble_barrier_check(long long timeout_ns, int* timed_out);
+
 /* the number of the n pseudo-random FP64 arguments (all exponents, plus
    integers) for which the FP64 form's FMA-corrected division by the
    constants 3 and 12 differs from IEEE division (expected: 0) */

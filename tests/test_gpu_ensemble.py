@@ -57,3 +57,75 @@ def test_whole_run_as_one_graph_matches_eager():
             np.testing.assert_array_equal(da.get(f, halo=True), db.get(f, halo=True))
     a.close()
     b.close()
+
+
+def _fields(ens):
+    return [{f: d.get(f, halo=True) for f in ('dp', 'pt', 'ud', 'vd')} for d in ens.dyn]
+
+
+def _assert_same(a, b):
+    for fa, fb in zip(a, b):
+        for f in fa:
+            np.testing.assert_array_equal(fa[f], fb[f], err_msg=f)
+
+
+@pytest.mark.parametrize('strips', [None, {32: 16, 48: 32, 40: 16, 64: 64, 24: 32}])
+def test_persistent_kernel_matches_eager(strips):
+    """One launch of the persistent kernel advances every member (uneven
+    sizes and layer counts) by 10 steps with two remaps, bit for bit as
+    stepping the members one by one, whatever the strip heights."""
+    a = Ensemble(members(), 'mixed', nstreams=3)
+    b = Ensemble(members(), 'mixed', nstreams=3)
+    a.step_eager(10)
+    if strips:
+        b.set_strips(strips)
+    b.run_persistent(10, 5)
+    torch.cuda.synchronize()
+    assert not b.barrier_timed_out()
+    _assert_same(_fields(a), _fields(b))
+    assert a.stable() and b.stable()
+    a.close()
+    b.close()
+
+
+def test_persistent_launch_as_graph_replays():
+    """Two remap cycles as one persistent launch captured in a CUDA graph,
+    replayed twice: 20 steps, bit-identical to eager stepping."""
+    a = Ensemble(members(), 'mixed', nstreams=3)
+    b = Ensemble(members(), 'mixed', nstreams=3)
+    a.step_eager(20)
+    b.capture_persistent(5, cycles=2)
+    b.replay(2)
+    torch.cuda.synchronize()
+    assert b.steps_done == 20
+    assert not b.barrier_timed_out()
+    _assert_same(_fields(a), _fields(b))
+    a.close()
+    b.close()
+
+
+def test_autotune_keeps_the_state():
+    """The strip-height autotuner times trial launches and restores every
+    member's state afterwards."""
+    b = Ensemble(members(), 'mixed', nstreams=3)
+    before = _fields(b)
+    table = b.autotune(steps=2, reps=1)
+    assert set(table) == {st.nx for st in b.members} and set(table.values()) <= {16, 32, 64}
+    _assert_same(before, _fields(b))
+    b.close()
+
+
+def test_persistent_barrier_wait_runs_out():
+    """The grid barrier's wait is bounded: a launch whose barrier waits for
+    one block more than the grid holds ends with the timeout status instead
+    of hanging, and the device keeps working."""
+    import ctypes
+    from atmdyn import load
+    lib = load()
+    out = ctypes.c_int(0)
+    assert lib.atm_ensemble_barrier_check(5_000_000, ctypes.byref(out)) == 0
+    assert out.value == 1
+    a = Ensemble(members()[:2], 'mixed', nstreams=1)
+    a.run_persistent(5, 5)
+    assert not a.barrier_timed_out() and a.stable()
+    a.close()
