@@ -111,6 +111,10 @@ __device__ __forceinline__ bool ens_barrier(const EnsPlan& p) {
     } else {
       const long long t0 = global_ns();
       while (*gen == g0) {
+        if (*(volatile int*)p.err != 0) {  // another block's wait ran out: leave at once
+          ok = false;
+          break;
+        }
         if (global_ns() - t0 > p.timeout_ns) {
           ok = false;
           atomicOr(p.err, 1);
