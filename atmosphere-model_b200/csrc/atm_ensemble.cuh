@@ -271,7 +271,7 @@ __device__ __forceinline__ void ens_item(int stage, const EnsMember& M, int cur,
 // The run: p.nsteps steps of every member, the remap on steps whose number
 // (counted from 1 at the launch) is a multiple of p.remap_every.
 template <typename T, typename S, typename C>
-__global__ void __launch_bounds__(MW * MWARPS) k_ensemble(EnsPlan p) {
+__global__ void __launch_bounds__(MW * MWARPS, 3) k_ensemble(EnsPlan p) {
   const long long nwarps = (long long)gridDim.x * MWARPS;
   const long long gw = (long long)blockIdx.x * MWARPS + (threadIdx.x >> 5);
   int flip = 0;  // swaps of the time levels so far (the same for every member)

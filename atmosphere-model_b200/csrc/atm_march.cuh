@@ -29,9 +29,11 @@ constexpr int MW = 32;              // lanes (columns) of a strip
 constexpr int MXH = 3;              // halo columns on each side
 constexpr int MOUT = MW - 2 * MXH;  // output columns of a strip
 constexpr int MWARPS = 4;           // independent strips (warps) per block
-// blocks per SM the register budget of the marching kernels is set for
+// blocks per SM the register budget of the marching kernels is set for: 4
+// (16 warps), which the FP32 sweeps reach without spilling (at most 128
+// registers; the C-momentum sweep would take 131 and fall to 3 blocks)
 #ifndef ATM_MARCH_MINB
-#define ATM_MARCH_MINB 1
+#define ATM_MARCH_MINB 4
 #endif
 
 template <typename T>
@@ -189,18 +191,33 @@ __device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* __restrict
   }
   bool bad = false;
   const int jend = min(oy + TYS, yhi + 1) + 3;
+  S dn_p = fdp(x, oy - 3), pn_p = fpt(x, oy - 3);
+  UB ua_p = CGRID ? fu(x, oy - 2) : fu(x, oy - 3), ub_p = CGRID ? fu(x - 1, oy - 2) : UB(0);
+  UB va_p = fv(x, oy - 5), vb_p = CGRID ? fv(x + 1, oy - 5) : UB(0);
   for (int j = oy - 3; j < jend; ++j) {
     // ---- row j: inputs, C-grid u, the inner x sweep (mod_sw_dyn.f90:109-117, 176-185; 503-511)
-    const T dn = T(fdp(x, j)), pn = T(fpt(x, j));
+    const S d_upd = fdp(x, j - 3), p_upd = fpt(x, j - 3);  // the update's state values of row j-3
+    const T dn = T(dn_p), pn = T(pn_p);
+    const UB ua_c = ua_p, ub_c = ub_p, va_c = va_p, vb_c = vb_p;
+    dn_p = fdp(x, j + 1);
+    pn_p = fpt(x, j + 1);
+    if constexpr (CGRID) {
+      ua_p = fu(x, j + 2);
+      ub_p = fu(x - 1, j + 2);
+      vb_p = fv(x + 1, j - 1);
+    } else {
+      ua_p = fu(x, j + 1);
+    }
+    va_p = fv(x, j - 1);
     T ucn;
     if constexpr (CGRID) {
-      const T a = T(fu(x, j + 1)), b = T(fu(x - 1, j + 1));
+      const T a = T(ua_c), b = T(ub_c);
       const T ub = T(.5) * (su_x + su_xm);
       ucn = T(.5) * (ub + T(.5) * (a + b));
       su_x = a;
       su_xm = b;
     } else {
-      ucn = T(fu(x, j));
+      ucn = T(ua_c);
     }
     const T ucR = shfl_dn(ucn, 1);
     const T dL = shfl_up(dn, 1), dR = shfl_dn(dn, 1);
@@ -228,13 +245,13 @@ __device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* __restrict
     // C-grid v of row j-2 (:109-117)
     T vcn;
     if constexpr (CGRID) {
-      const T a = T(fv(x, j - 2)), b = T(fv(x + 1, j - 2));
+      const T a = T(va_c), b = T(vb_c);
       const T vb = T(.5) * (a + sv_x);
       vcn = T(.5) * (vb + T(.5) * (b + sv_xp));
       sv_x = a;
       sv_xp = b;
     } else {
-      vcn = T(fv(x, j - 2));
+      vcn = T(va_c);
     }
     vc1 = vc0;
     vc0 = vcn;
@@ -308,9 +325,9 @@ __device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* __restrict
       const T Fy0 = fy1 + dyv * (ld1 - ld2), Fy1 = fy0 + dyv * (ld0 - ld1);
       const T Hx0 = (fxp + vdx * (lq1 - qxm)) * fxd, Hx1 = (fxp1 + vdx * (qxp - lq1)) * fxd1;
       const T Hy0 = (fq1 + vdy * (lq1 - lq2)) * fy1, Hy1 = (fq0 + vdy * (lq0 - lq1)) * fy0;
-      const S d = fdp(x, y);
+      const S d = d_upd;
       const S vv = d - ((S(Fx1) - S(Fx0)) + (S(Fy1) - S(Fy0)));
-      S q = d * fpt(x, y) - ((S(Hx1) - S(Hx0)) + (S(Hy1) - S(Hy0)));
+      S q = d * p_upd - ((S(Hx1) - S(Hx0)) + (S(Hy1) - S(Hy0)));
       if (heat) q = q + S(c.dt) * d * S(heat[o]);
       q = q / vv;
       vo = O(vv);
@@ -384,11 +401,19 @@ __device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* __restric
   // layer-nlay ud at row y and vd at rows y-1, y of the first kinetic-energy row y = oy-1
   T uL1 = T(fuL(x, oy - 1)), vL2 = T(fvL(x, oy - 2)), vL1 = T(fvL(x, oy - 1));
   const int jend = min(oy + TYS, g.ny) + 3;
+  S un_p = fud(x, oy - 2), unm_p = fud(x - 1, oy - 2), vn_p = fvd(x, oy - 3), vnp_p = fvd(x + 1, oy - 3);
   for (int j = oy - 3; j < jend; ++j) {
+    // loads of row y = j-3 issued before this row's work
+    const double pk0 = fpk0(x, j - 3), pk1 = fpk1(x, j - 3), gz0 = fgz0(x, j - 3), gz1 = fgz1(x, j - 3);
+    const S uL0_r = fuL(x, j - 2), vL0_r = fvL(x, j - 2);
     // ---- row j: C-grid winds of the layer (:110-117), vorticity (:319-323),
     // inner x sweep of the vorticity (:353-367)
-    const T un = T(fud(x, j + 1)), unm = T(fud(x - 1, j + 1));
-    const T vn = T(fvd(x, j)), vnp = T(fvd(x + 1, j));
+    const T un = T(un_p), unm = T(unm_p);
+    const T vn = T(vn_p), vnp = T(vnp_p);
+    un_p = fud(x, j + 2);
+    unm_p = fud(x - 1, j + 2);
+    vn_p = fvd(x, j + 1);
+    vnp_p = fvd(x + 1, j + 1);
     const T ucn = T(.5) * (T(.5) * (u_x + u_xm) + T(.5) * (un + unm));
     const T vcn = T(.5) * (T(.5) * (vn + v_x) + T(.5) * (vnp + v_xp));
     const T vor = f - (ucn - a0) * rdy + (vcn - shfl_up(vcn, 1)) * rdx;
@@ -420,7 +445,7 @@ __device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* __restric
     if (y < oy - 1) continue;  // warm-up rows (warp-uniform)
     // ---- row y: kinetic energy (:299-317) with the layer-nlay A-grid winds
     // (:110-125 at k = nlay), recomputed where they are read
-    const T uL0 = T(fuL(x, y + 1)), vL0 = T(fvL(x, y + 1));
+    const T uL0 = T(uL0_r), vL0 = T(vL0_r);
     T ken;
     {
       const T ub = T(.5) * (uL1 + shfl_up(uL1, 1));
@@ -447,7 +472,6 @@ __device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* __restric
     vL1 = vL0;
     ke1 = ke0;
     ke0 = ken;
-    const double pk0 = fpk0(x, y), pk1 = fpk1(x, y), gz0 = fgz0(x, y), gz1 = fgz1(x, y);
     const double pk0l = shfl_up(pk0, 1), pk1l = shfl_up(pk1, 1), gz0l = shfl_up(gz0, 1), gz1l = shfl_up(gz1, 1);
     const double pk0d = pk0m, pk1d = pk1m, gz0d = gz0m, gz1d = gz1m;  // row y-1
     pk0m = pk0; pk1m = pk1; gz0m = gz0; gz1m = gz1;
@@ -551,17 +575,28 @@ __device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* __restric
   double pb0y = 0, pb1y = 0, gb0y = 0, gb1y = 0;                // pkapb, gzb at k, k+1, row j-3
   bool bad = false;
   const int jend = min(oy + TYS, g.ny) + 3;
+  S sn_p = fud(x, oy - 2), vn_p = fvd(x, oy - 2);
+  C cu_p = fuL(x, oy - 3), cv_p = fvL(x, oy - 4);
   for (int j = oy - 2; j < jend; ++j) {
+    // loads of rows j-2 (pressure terms) and j-3 (the update) issued before this row's work
+    const double pb0n = fpb0(x, j - 2), pb1n = fpb1(x, j - 2), gb0n = fgb0(x, j - 2), gb1n = fgb1(x, j - 2);
+    const C svc_r = fvc(x, j - 3), suc_r = fuc(x, j - 3);
+    const S uo_r = fud(x, j - 3), vo_r = fvd(x, j - 3);
     // ---- row j inputs; vorticity of row j-1 (:659-663), divergence of row j (:682-685)
-    const T sn = T(fud(x, j)), vn = T(fvd(x, j));
+    const T sn = T(sn_p), vn = T(vn_p);
+    const C cu_c = cu_p, cv_c = cv_p;
+    sn_p = fud(x, j + 1);
+    vn_p = fvd(x, j + 1);
+    cu_p = fuL(x, j);
+    cv_p = fvL(x, j - 1);
     const T vorn = f - (sn - s0) * rdy + (shfl_dn(v0, 1) - v0) * rdx;
     const T dvn = rdx * (sn - shfl_up(sn, 1)) + rdy * (vn - v0);
     s2 = s1; s1 = s0; s0 = sn;
     v3 = v2; v2 = v1; v1 = v0; v0 = vn;
     w4 = w3; w3 = w2; w2 = w1; w1 = vorn;
     q2 = q1; q1 = q0; q0 = dvn;
-    cu3 = cu2; cu2 = cu1; cu1 = T(fuL(x, j - 1));
-    cv3 = cv2; cv2 = T(fvL(x, j - 2));
+    cu3 = cu2; cu2 = cu1; cu1 = T(cu_c);
+    cv3 = cv2; cv2 = T(cv_c);
     // monotone slope of vd at row j-1, its edges at row j-2 (:870-911)
     mv3 = mv2; mv2 = mv1; mv1 = slope_v(v2, v1, v0);
     lv3 = lv2; rv3 = rv2;
@@ -603,7 +638,6 @@ __device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* __restric
       ke3 = ke2;
       ke2 = T(.5) * (kv + ubL * fx);
     }
-    const double pb0n = fpb0(x, j - 2), pb1n = fpb1(x, j - 2), gb0n = fgb0(x, j - 2), gb1n = fgb1(x, j - 2);
     const int y = j - 3;
     if (y >= oy) {
       // ---- row y: inner y sweep of the vorticity (:744-753), its x slopes and
@@ -628,16 +662,16 @@ __device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* __restric
         const double pgx = ((pb0r - pb1y) * (gb0y - gb1r) + (pb0y - pb1r) * (gb1y - gb0r)) / (pb0r - pb1y + pb0y - pb1r);
         const double pgy = ((pb0n - pb1y) * (gb0y - gb1n) + (pb0y - pb1n) * (gb1y - gb0n)) / (pb0n - pb1y + pb0y - pb1n);
         const long long o = g.at(x, y, k);
-        const T svc = T(fvc(x, y)), suc = T(fuc(x, y));
+        const T svc = T(svc_r), suc = T(suc_r);
         S u, v;
         if constexpr (std::is_same_v<S, T>) {  // the reference's operations, in order
-          u = ud[o] + dt * (svc * fy + vdy * (lp3 - lp4)) - dtdx * (ke_r - ke3 - dd_r + dd3 - T(pgx));
-          v = vd[o] - dt * (suc * fx + vdx * (lp3 - lp_l)) - dtdy * (ke2 - ke3 - dd2 + dd3 - T(pgy));
+          u = uo_r + dt * (svc * fy + vdy * (lp3 - lp4)) - dtdx * (ke_r - ke3 - dd_r + dd3 - T(pgx));
+          v = vo_r - dt * (suc * fx + vdx * (lp3 - lp_l)) - dtdy * (ke2 - ke3 - dd2 + dd3 - T(pgy));
         } else {  // the tendency in the sweep type added to the state's type
           const T du = dt * (svc * fy + vdy * (lp3 - lp4)) - dtdx * (ke_r - ke3 - dd_r + dd3 - T(pgx));
           const T dv = -dt * (suc * fx + vdx * (lp3 - lp_l)) - dtdy * (ke2 - ke3 - dd2 + dd3 - T(pgy));
-          u = ud[o] + S(du);
-          v = vd[o] + S(dv);
+          u = uo_r + S(du);
+          v = vo_r + S(dv);
         }
         udo[o] = u;
         vdo[o] = v;
