@@ -91,7 +91,7 @@ class Ensemble:
         lib = _lib.load()
         e = self._ens()
         for i, st in enumerate(self.members):
-            rows = table.get(st.nx, 64)
+            rows = table.get(st.nx, 32)
             _lib.check(lib.atm_ensemble_set_strips(e, i, rows), None, 'atm_ensemble_set_strips')
         self.strips = dict(table)
 
@@ -148,7 +148,7 @@ class Ensemble:
             saved.append(buf)
         torch.cuda.synchronize()
         lib = _lib.load()
-        table = {st.nx: 64 for st in self.members}
+        table = {st.nx: 32 for st in self.members}
         done = self.steps_done
         timings = {}
         for nx in sorted(table):

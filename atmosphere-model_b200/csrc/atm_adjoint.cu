@@ -2,10 +2,7 @@
 // --fmad=false like the FP64 form: the adjoint kernels recompute the
 // forward's intermediates with the forward's exact operations, so every
 // limiter and upwind branch is taken as in the forward step.
-#include <algorithm>
-
 #include "atm_adjoint.cuh"
-#include "atm_remap_wadj.cuh"
 #include "atm_ops.h"
 #include "atm_tmap.h"
 
@@ -173,35 +170,14 @@ cudaError_t adj_remap_energy(const Geom& g, const RemapArgs& ra, const double* d
                                          lam_dp, lam_pt, lam_ud, lam_vd, lam_ur, lam_vr, s);
 }
 
-// the warp-cooperative wind remap adjoint (atm_remap_wadj.cuh): a grid of
-// resident blocks walking the groups of face columns
-template <int LM>
-static cudaError_t winds_adj_warp(const Geom& g, const RemapArgs& ra, const double* dp, const double* ud,
-                                  const double* vd, const double* lam_ur, const double* lam_vr, double* lam_dp,
-                                  double* lam_ud, double* lam_vd, cudaStream_t s) {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaError_t e;
-  if ((e = cudaGetDevice(&dev)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) ||
-      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rwa::k_remap_winds_adj_w<LM>, 32 * rwa::NWB, 0)))
-    return e;
-  const long long nq = 2LL * (g.nx + 2) * (g.ny + 2);
-  const long long groups = (nq + rwa::G - 1) / rwa::G;
-  const long long need = (groups + rwa::NWB - 1) / rwa::NWB;
-  const int blocks = (int)std::min<long long>(need, (long long)sms * std::max(per_sm, 1));
-  rwa::k_remap_winds_adj_w<LM><<<blocks, 32 * rwa::NWB, 0, s>>>(g, ra, dp, ud, vd, lam_ur, lam_vr, lam_dp, lam_ud,
-                                                                  lam_vd);
-  return cudaGetLastError();
-}
-
 cudaError_t adj_remap_winds(const Geom& g, const RemapArgs& ra, const double* dp, const double* ud, const double* vd,
                             const double* lam_ur, const double* lam_vr, double* lam_dp, double* lam_ud, double* lam_vd,
                             cudaStream_t s) {
-  if (g.L <= 32) return winds_adj_warp<32>(g, ra, dp, ud, vd, lam_ur, lam_vr, lam_dp, lam_ud, lam_vd, s);
-  if (g.L <= 64) return winds_adj_warp<64>(g, ra, dp, ud, vd, lam_ur, lam_vr, lam_dp, lam_ud, lam_vd, s);
-  // deeper columns: a thread per face column, both directions
   const int n = (g.nx + 2) * (g.ny + 2);
-  k_remap_winds_adj<MAX_LAYERS><<<(n + 63) / 64, 64, 0, s>>>(g, ra, dp, ud, vd, lam_ur, lam_vr, lam_dp, lam_ud,
-                                                             lam_vd);
+  const int nb = (n + 63) / 64;
+  if (g.L <= 32) k_remap_winds_adj<32><<<nb, 64, 0, s>>>(g, ra, dp, ud, vd, lam_ur, lam_vr, lam_dp, lam_ud, lam_vd);
+  else if (g.L <= 64) k_remap_winds_adj<64><<<nb, 64, 0, s>>>(g, ra, dp, ud, vd, lam_ur, lam_vr, lam_dp, lam_ud, lam_vd);
+  else k_remap_winds_adj<MAX_LAYERS><<<nb, 64, 0, s>>>(g, ra, dp, ud, vd, lam_ur, lam_vr, lam_dp, lam_ud, lam_vd);
   return cudaGetLastError();
 }
 

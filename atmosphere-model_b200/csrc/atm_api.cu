@@ -1431,7 +1431,7 @@ int atm_ensemble_create(atm_ens** out, atm_ctx* const* members, const double* dt
   atm_ens* e = new atm_ens();
   e->m.assign(members, members + n);
   e->dt.assign(dts, dts + n);
-  e->tys.assign(n, 64);
+  e->tys.assign(n, 32);
   e->stream = members[0]->stream;
   e->blocks = atm::ensemble_max_blocks();
   const size_t off_bytes = sizeof(long long) * atm::E_NSTAGE * (n + 1);

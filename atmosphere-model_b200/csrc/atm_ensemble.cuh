@@ -18,6 +18,9 @@
 //
 // The per-member strip height of the marching sweeps (16, 32 or 64 rows)
 // comes from the plan (an autotuned table keyed on the member's grid size).
+// Fields written by one stage are read by later stages of the same launch,
+// so every stage reads with plain (coherent) loads, never through the
+// read-only data path; the barrier's fences order the writes before them.
 // The stage bodies are the single-domain kernels' device functions, so a
 // member's results are bit-identical to stepping it alone.
 #pragma once
@@ -158,7 +161,7 @@ template <typename T, typename S, typename C, int TYS>
 __device__ __noinline__ void ens_cmass(const EnsMember& M, int cur, long long li) {
   ens_strip_item<TYS>(M.g, -2, 2, li, [&](int sx, int sy, int k) {
     void* const* so = M.st[cur];
-    mass_strip<T, TYS, true, S, C>(M.g, M.cc, (const S*)so[0], (const S*)so[1], (const S*)so[2], (const S*)so[3],
+    mass_strip<T, TYS, true, S, C, false>(M.g, M.cc, (const S*)so[0], (const S*)so[1], (const S*)so[2], (const S*)so[3],
                                    nullptr, (C*)M.cg[0], (C*)M.cg[1], -2, 2, nullptr, sx, sy, k);
   });
 }
@@ -166,7 +169,7 @@ template <typename T, typename S, typename C, int TYS>
 __device__ __noinline__ void ens_cmom(const EnsMember& M, int cur, long long li) {
   ens_strip_item<TYS>(M.g, 0, 0, li, [&](int sx, int sy, int k) {
     void* const* so = M.st[cur];
-    c_mom_strip<T, TYS, S, C>(M.g, M.cc, (const S*)so[2], (const S*)so[3], M.pkap, M.gz, (C*)M.cg[2], (C*)M.cg[3],
+    c_mom_strip<T, TYS, S, C, false>(M.g, M.cc, (const S*)so[2], (const S*)so[3], M.pkap, M.gz, (C*)M.cg[2], (C*)M.cg[3],
                               sx, sy, k);
   });
 }
@@ -175,7 +178,7 @@ __device__ __noinline__ void ens_dmass(const EnsMember& M, int cur, long long li
   ens_strip_item<TYS>(M.g, -3, 3, li, [&](int sx, int sy, int k) {
     void* const* so = M.st[cur];
     void* const* sn = M.st[cur ^ 1];
-    mass_strip<T, TYS, false, S, C>(M.g, M.cd, (const S*)so[0], (const S*)so[1], (const C*)M.cg[2], (const C*)M.cg[3],
+    mass_strip<T, TYS, false, S, C, false>(M.g, M.cd, (const S*)so[0], (const S*)so[1], (const C*)M.cg[2], (const C*)M.cg[3],
                                     nullptr, (S*)sn[0], (S*)sn[1], -3, 3, &M.status->nonfinite_step, sx, sy, k);
   });
 }
@@ -184,7 +187,7 @@ __device__ __noinline__ void ens_dmom(const EnsMember& M, int cur, long long li)
   ens_strip_item<TYS>(M.g, 0, 0, li, [&](int sx, int sy, int k) {
     void* const* so = M.st[cur];
     void* const* sn = M.st[cur ^ 1];
-    d_mom_strip<T, TYS, S, C>(M.g, M.cd, (const S*)so[2], (const S*)so[3], (const C*)M.cg[2], (const C*)M.cg[3],
+    d_mom_strip<T, TYS, S, C, false>(M.g, M.cd, (const S*)so[2], (const S*)so[3], (const C*)M.cg[2], (const C*)M.cg[3],
                               M.pkapb, M.gzb, (S*)sn[2], (S*)sn[3], &M.status->nonfinite_step, sx, sy, k);
   });
 }

@@ -58,9 +58,9 @@ __device__ __forceinline__ bool finite_(float v) { return isfinite(v); }
 // written), so no shared memory limits the occupancy.  The next layer's dp
 // is loaded one iteration ahead so that its latency overlaps atm_pow.
 template <typename T>
-__device__ __forceinline__ void column_at(const Geom& g, const Consts& c, const T* __restrict__ dpl,
-                                          const T* __restrict__ ptl, double* __restrict__ pkap,
-                                          double* __restrict__ gz, int lo, int hi, double* __restrict__ plev_out,
+__device__ __forceinline__ void column_at(const Geom& g, const Consts& c, const T* dpl,
+                                          const T* ptl, double* pkap,
+                                          double* gz, int lo, int hi, double* plev_out,
                                           int col) {
   const int w = g.nx - lo + hi;
   const int hgt = g.ny - lo + hi;
@@ -141,8 +141,8 @@ __device__ __forceinline__ double corner(const double* q, long long o, int P) {
   return out;
 }
 
-__device__ __forceinline__ void corner_at(const Geom& g, const double* __restrict__ pkap, const double* __restrict__ gz,
-                                          double* __restrict__ pkapb, double* __restrict__ gzb, int with_pkap, int lev0,
+__device__ __forceinline__ void corner_at(const Geom& g, const double* pkap, const double* gz,
+                                          double* pkapb, double* gzb, int with_pkap, int lev0,
                                           int nlev, int idx) {
   const int w = g.nx + 1, h = g.ny + 1;
   if (idx >= w * h) return;
@@ -519,8 +519,8 @@ __device__ __forceinline__ void remap_merge(int L, ColArr sc, ColArr lv, ColArr 
 // (i, j), direction dir (0: u, columns (i, j-2..j+1); 1: v, (i-2..i+1, j)).
 // The all-arrays form, for columns with non-monotone coordinates.
 template <typename T, int LM>
-__device__ __noinline__ void remap_winds_full(const Geom& g, const RemapArgs& ra, const T* __restrict__ dp,
-                                              const T* __restrict__ f, T* __restrict__ r, int* tr, Status* st, int i,
+__device__ __noinline__ void remap_winds_full(const Geom& g, const RemapArgs& ra, const T* dp,
+                                              const T* f, T* r, int* tr, Status* st, int i,
                                               int j, int dir) {
   const int L = g.L;
   double sc[LM + 2], dc[LM + 2], var[LM + 2], out[LM + 2];
@@ -569,9 +569,9 @@ __device__ __noinline__ void remap_winds_full(const Geom& g, const RemapArgs& ra
 // arrays of LM + 2 doubles per thread.
 // face column col of direction dir (0: u, 1: v)
 template <typename T, int LM>
-__device__ __forceinline__ void remap_winds_at(const Geom& g, const RemapArgs& ra, const T* __restrict__ dp,
-                                               const T* __restrict__ ud, const T* __restrict__ vd,
-                                               T* __restrict__ urem, T* __restrict__ vrem, int* trace, Status* st,
+__device__ __forceinline__ void remap_winds_at(const Geom& g, const RemapArgs& ra, const T* dp,
+                                               const T* ud, const T* vd,
+                                               T* urem, T* vrem, int* trace, Status* st,
                                                int col, int dir) {
   const int w = g.nx + 2, h = g.ny + 2;
   if (col >= w * h) return;
@@ -652,12 +652,12 @@ __global__ void __launch_bounds__(64) k_remap_winds(Geom g, RemapArgs ra, const 
 // src/mod_remap.f90:42-78 (columns) and 111-161.  The all-arrays form, for
 // columns with non-monotone coordinates.
 template <typename T, int LM>
-__device__ __noinline__ void remap_energy_full(const Geom& g, const RemapArgs& ra, const T* __restrict__ dp,
-                                               const T* __restrict__ pt, const T* __restrict__ ud,
-                                               const T* __restrict__ vd, const T* __restrict__ urem,
-                                               const T* __restrict__ vrem, const double* __restrict__ gzs,
-                                               T* __restrict__ dpo, T* __restrict__ pto, T* __restrict__ udo,
-                                               T* __restrict__ vdo, int* tr, Status* st, int i, int j) {
+__device__ __noinline__ void remap_energy_full(const Geom& g, const RemapArgs& ra, const T* dp,
+                                               const T* pt, const T* ud,
+                                               const T* vd, const T* urem,
+                                               const T* vrem, const double* gzs,
+                                               T* dpo, T* pto, T* udo,
+                                               T* vdo, int* tr, Status* st, int i, int j) {
   const int L = g.L;
   const long long S = g.S;
   const long long o = g.at(i, j);
@@ -717,12 +717,12 @@ __device__ __noinline__ void remap_energy_full(const Geom& g, const RemapArgs& r
 // thread (levels, pkap then the eliminated interface values, energy, gam).
 // interior column col
 template <typename T, int LM>
-__device__ __forceinline__ void remap_energy_at(const Geom& g, const RemapArgs& ra, const T* __restrict__ dp,
-                                                const T* __restrict__ pt, const T* __restrict__ ud,
-                                                const T* __restrict__ vd, const T* __restrict__ urem,
-                                                const T* __restrict__ vrem, const double* __restrict__ gzs,
-                                                T* __restrict__ dpo, T* __restrict__ pto, T* __restrict__ udo,
-                                                T* __restrict__ vdo, int* trace, Status* st, int col) {
+__device__ __forceinline__ void remap_energy_at(const Geom& g, const RemapArgs& ra, const T* dp,
+                                                const T* pt, const T* ud,
+                                                const T* vd, const T* urem,
+                                                const T* vrem, const double* gzs,
+                                                T* dpo, T* pto, T* udo,
+                                                T* vdo, int* trace, Status* st, int col) {
   if (col >= g.nx * g.ny) return;
   const int i = col % g.nx, j = col / g.nx;
   const int L = g.L;

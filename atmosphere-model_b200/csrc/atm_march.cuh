@@ -117,19 +117,24 @@ __device__ __forceinline__ float slope_v(float qm, float q0, float qp) {
 }
 
 // Row accessor of one level of a stored field: value at (x, y) of the
-// level, zero outside the stored (halo-padded) array.
-template <typename E>
+// level, zero outside the stored (halo-padded) array.  RO: no thread writes
+// the field during the launch, so it is read through the read-only data
+// path; the persistent ensemble kernel, whose later stages read what earlier
+// stages of the same launch wrote, uses plain (coherent) loads.
+template <typename E, bool RO = true>
 struct Lev {
-  const E* __restrict__ p;  // element (0, 0) of the level
+  const E* p;  // element (0, 0) of the level
   int P, nx, ny;
   __device__ __forceinline__ E operator()(int x, int y) const {
     if (x < -H || x >= nx + H || y < -H || y >= ny + H) return E(0);
-    return __ldg(p + (long long)y * P + x);
+    const E* a = p + (long long)y * P + x;
+    if constexpr (RO) return __ldg(a);
+    else return *a;
   }
 };
-template <typename E>
-__device__ __forceinline__ Lev<E> level(const E* f, const Geom& g, int k) {
-  return Lev<E>{f + g.at(0, 0, k), g.P, g.nx, g.ny};
+template <bool RO = true, typename E>
+__device__ __forceinline__ Lev<E, RO> level(const E* f, const Geom& g, int k) {
+  return Lev<E, RO>{f + g.at(0, 0, k), g.P, g.nx, g.ny};
 }
 
 // ---------------------------------------------------------------- mass ----
@@ -143,14 +148,14 @@ struct MassM {
   using O = std::conditional_t<CGRID, C, S>;   // outputs
 };
 
-template <typename T, int TYS, bool CGRID, typename S, typename C>
-__device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* __restrict__ dp,
-                                                         const S* __restrict__ pt,
-                                                         const typename MassM<T, CGRID, S, C>::UB* __restrict__ u,
-                                                         const typename MassM<T, CGRID, S, C>::UB* __restrict__ v,
-                                                         const double* __restrict__ heat,
-                                                         typename MassM<T, CGRID, S, C>::O* __restrict__ dpo,
-                                                         typename MassM<T, CGRID, S, C>::O* __restrict__ pto, int lo,
+template <typename T, int TYS, bool CGRID, typename S, typename C, bool RO = true>
+__device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* dp,
+                                                         const S* pt,
+                                                         const typename MassM<T, CGRID, S, C>::UB* u,
+                                                         const typename MassM<T, CGRID, S, C>::UB* v,
+                                                         const double* heat,
+                                                         typename MassM<T, CGRID, S, C>::O* dpo,
+                                                         typename MassM<T, CGRID, S, C>::O* pto, int lo,
                                                          int hi, int* nonfinite, int sx, int sy, int k) {
   using UB = typename MassM<T, CGRID, S, C>::UB;
   using O = typename MassM<T, CGRID, S, C>::O;
@@ -166,8 +171,8 @@ __device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* __restrict
   const T dt = T(c.dt), dtdx = T(c.dtdx), dtdy = T(c.dtdy), rA = T(c.rA);
   const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
   const T dxv = dtdx * T(c.vdx), dyv = dtdy * T(c.vdy), vdx = T(c.vdx), vdy = T(c.vdy);
-  const Lev<S> fdp = level(dp, g, k), fpt = level(pt, g, k);
-  const Lev<UB> fu = level(u, g, k), fv = level(v, g, k);
+  const auto fdp = level<RO>(dp, g, k), fpt = level<RO>(pt, g, k);
+  const auto fu = level<RO>(u, g, k), fv = level<RO>(v, g, k);
 
   // register windows of the column, named by their row offset from the
   // newest row j of the current iteration
@@ -361,11 +366,11 @@ __global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_mass_m(Geom g, 
 // layer-nlay A-grid winds (:299-317), absolute vorticity (:319-323), the
 // pressure-gradient force (:325-339) and the vorticity-flux updates of uc
 // and vc (:344-412).  Outputs on the interior; strips of TYS rows.
-template <typename T, int TYS, typename S, typename C>
-__device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* __restrict__ ud,
-                                                          const S* __restrict__ vd, const double* __restrict__ pkap,
-                                                          const double* __restrict__ gz, C* __restrict__ uc,
-                                                          C* __restrict__ vc, int sx, int sy, int k) {
+template <typename T, int TYS, typename S, typename C, bool RO = true>
+__device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* ud,
+                                                          const S* vd, const double* pkap,
+                                                          const double* gz, C* uc,
+                                                          C* vc, int sx, int sy, int k) {
   constexpr int UNC = PPM_UNC;
   const int lane = threadIdx.x & (MW - 1);
   const int ox = sx * MOUT;
@@ -378,10 +383,10 @@ __device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* __restric
   const T rdx = T(c.rdx), rdy = T(c.rdy), f = T(c.coriolis);
   const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
   const T vdx = T(c.vdx), vdy = T(c.vdy);
-  const Lev<S> fud = level(ud, g, k), fvd = level(vd, g, k);
-  const Lev<S> fuL = level(ud, g, L - 1), fvL = level(vd, g, L - 1);
-  const Lev<double> fpk0 = level(pkap, g, k), fpk1 = level(pkap, g, k + 1);
-  const Lev<double> fgz0 = level(gz, g, k), fgz1 = level(gz, g, k + 1);
+  const auto fud = level<RO>(ud, g, k), fvd = level<RO>(vd, g, k);
+  const auto fuL = level<RO>(ud, g, L - 1), fvL = level<RO>(vd, g, L - 1);
+  const auto fpk0 = level<RO>(pkap, g, k), fpk1 = level<RO>(pkap, g, k + 1);
+  const auto fgz0 = level<RO>(gz, g, k), fgz1 = level<RO>(gz, g, k + 1);
 
   // register windows of the column, named by their row offset from the
   // newest row j of the iteration
@@ -531,12 +536,12 @@ __global__ void __launch_bounds__(MW * MWARPS, ATM_MARCH_MINB) k_c_mom_m(Geom g,
 // B-grid pressure-gradient force (:665-679), del^4 divergence damping
 // (:682-702) and the vorticity-flux updates (:708-769).  Outputs on the
 // interior; strips of TYS rows.
-template <typename T, int TYS, typename S, typename C>
-__device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* __restrict__ ud,
-                                                          const S* __restrict__ vd, const C* __restrict__ uc,
-                                                          const C* __restrict__ vc, const double* __restrict__ pkapb,
-                                                          const double* __restrict__ gzb, S* __restrict__ udo,
-                                                          S* __restrict__ vdo, int* nonfinite, int sx, int sy, int k) {
+template <typename T, int TYS, typename S, typename C, bool RO = true>
+__device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* ud,
+                                                          const S* vd, const C* uc,
+                                                          const C* vc, const double* pkapb,
+                                                          const double* gzb, S* udo,
+                                                          S* vdo, int* nonfinite, int sx, int sy, int k) {
   constexpr int CON = PPM_CON;
   const int lane = threadIdx.x & (MW - 1);
   const int ox = sx * MOUT;
@@ -549,11 +554,11 @@ __device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* __restric
   const T rdx = T(c.rdx), rdy = T(c.rdy), f = T(c.coriolis);
   const T rdx2 = T(c.rdx2), rdy2 = T(c.rdy2), rdxy = T(c.rdx2rdy2);
   const T vdx = T(c.vdx), vdy = T(c.vdy), divdamp = T(c.divdamp);
-  const Lev<S> fud = level(ud, g, k), fvd = level(vd, g, k);
-  const Lev<C> fuL = level(uc, g, L - 1), fvL = level(vc, g, L - 1);
-  const Lev<C> fuc = level(uc, g, k), fvc = level(vc, g, k);
-  const Lev<double> fpb0 = level(pkapb, g, k), fpb1 = level(pkapb, g, k + 1);
-  const Lev<double> fgb0 = level(gzb, g, k), fgb1 = level(gzb, g, k + 1);
+  const auto fud = level<RO>(ud, g, k), fvd = level<RO>(vd, g, k);
+  const auto fuL = level<RO>(uc, g, L - 1), fvL = level<RO>(vc, g, L - 1);
+  const auto fuc = level<RO>(uc, g, k), fvc = level<RO>(vc, g, k);
+  const auto fpb0 = level<RO>(pkapb, g, k), fpb1 = level<RO>(pkapb, g, k + 1);
+  const auto fgb0 = level<RO>(gzb, g, k), fgb1 = level<RO>(gzb, g, k + 1);
 
   // register windows of the column, named by their row offset from the
   // newest row j of the iteration

@@ -483,7 +483,8 @@ ADJ_WORDS = {
 # DRAM bytes per interior cell and launch of the adjoint kernels measured by
 # ncu (dram__bytes_read.sum + dram__bytes_write.sum, dense adjoint of the
 # jet at 512x512x32, scaled by cells)
-TRAFFIC_PER_CELL_ADJ = {}
+TRAFFIC_PER_CELL_ADJ = {'adj_c_mass': 113.3, 'adj_c_mom': 114.2, 'adj_d_mass_x': 130.9, 'adj_d_mass_y': 131.1,
+                        'adj_d_mom_ke': 64.7, 'adj_d_mom_vf': 165.2}
 
 
 def grad_leg(args, torch, barrier, max_over_ranks, world, peak, peak_kind):

@@ -230,7 +230,7 @@ int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, const double* 
    after one prepare must each swap the time levels an even number of times
    (nsteps + nsteps / remap_every even), so that a captured launch can be
    replayed.  atm_ensemble_set_strips sets a member's strip height of the
-   marching sweeps (16, 32 or 64 rows; default 64).
+   marching sweeps (16, 32 or 64 rows; default 32).
    atm_ensemble_barrier_check launches the kernel with no members and a
    barrier that waits for one block more than the grid holds: *timed_out
    reports that the bounded wait ran out and the launch ended. */
