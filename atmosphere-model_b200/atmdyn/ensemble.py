@@ -113,6 +113,21 @@ class Ensemble:
         _lib.check(lib.atm_ensemble_run(self.ens, nsteps, remap_every), None, 'atm_ensemble_run')
         self.steps_done += nsteps
 
+    STAGES = ('c_mass', 'c_column', 'c_mom', 'c_halo', 'd_ring', 'd_mass', 'd_column', 'd_corners', 'd_mom',
+              'remap_ring', 'remap_winds', 'remap_energy', 'd_halo')
+
+    def profile_persistent(self, enable=True):
+        """Per-stage timing of the following persistent launches (block 0's
+        clock between barrier exits)."""
+        _lib.check(_lib.load().atm_ensemble_profile(self._ens(), int(enable)), None, 'atm_ensemble_profile')
+
+    def persistent_stage_ms(self):
+        """{stage: milliseconds summed over the launches since profiling began}."""
+        out = (ctypes.c_double * len(self.STAGES))()
+        _lib.check(_lib.load().atm_ensemble_stage_ms(self._ens(), out, len(self.STAGES)), None,
+                   'atm_ensemble_stage_ms')
+        return {n: out[i] for i, n in enumerate(self.STAGES)}
+
     def barrier_timed_out(self):
         v = ctypes.c_int(0)
         _lib.check(_lib.load().atm_ensemble_status(self._ens(), ctypes.byref(v)), None, 'atm_ensemble_status')

@@ -1362,6 +1362,7 @@ struct atm_ens {
   cudaStream_t stream = nullptr;
   bool prepared = false;
   int pending_flips = 0;  // time-level swaps of the launches since the last prepare
+  unsigned long long* d_stage = nullptr;  // per-stage nanoseconds while profiling
 };
 
 namespace {
@@ -1372,6 +1373,7 @@ int ens_free(atm_ens* e) {
   cudaFree(e->d_off);
   cudaFree(e->d_bar);
   cudaFree(e->d_err);
+  cudaFree(e->d_stage);
   if (e->h_err) cudaFreeHost(e->h_err);
   delete e;
   return ATM_OK;
@@ -1486,7 +1488,7 @@ int atm_ensemble_run(atm_ens* e, int nsteps, int remap_every) {
   for (atm_ctx* c : e->m)
     if (cudaMemsetAsync(&c->status->nonfinite_step, 0, 2 * sizeof(int), e->stream) != cudaSuccess) return ATM_ERR_CUDA;
   atm::EnsPlan p{e->d_members, e->d_off, n, nsteps, remap_every, e->d_bar, (unsigned)e->blocks, e->d_err,
-                 e->timeout_ns};
+                 e->timeout_ns, e->d_stage};
   if (atm::ensemble_launch(p, e->blocks, e->stream) != cudaSuccess) return ATM_ERR_CUDA;
   const int flips = nsteps + remaps;
   e->pending_flips += flips;
@@ -1504,6 +1506,33 @@ int atm_ensemble_status(atm_ens* e, int* barrier_timed_out) {
       cudaStreamSynchronize(e->stream) != cudaSuccess)
     return ATM_ERR_CUDA;
   *barrier_timed_out = *e->h_err;
+  return ATM_OK;
+}
+
+int atm_ensemble_profile(atm_ens* e, int enable) {
+  if (!e) return ATM_ERR_ARG;
+  if (!enable) {
+    cudaFree(e->d_stage);
+    e->d_stage = nullptr;
+    return ATM_OK;
+  }
+  if (!e->d_stage && cudaMalloc((void**)&e->d_stage, atm::E_NSTAGE * sizeof(unsigned long long)) != cudaSuccess) {
+    e->d_stage = nullptr;
+    return ATM_ERR_NOMEM;
+  }
+  return cudaMemsetAsync(e->d_stage, 0, atm::E_NSTAGE * sizeof(unsigned long long), e->stream) == cudaSuccess
+             ? ATM_OK
+             : ATM_ERR_CUDA;
+}
+
+int atm_ensemble_stage_ms(atm_ens* e, double* ms, int n) {
+  if (!e || !ms || n < atm::E_NSTAGE) return ATM_ERR_ARG;
+  if (!e->d_stage) return ATM_ERR_STATE;
+  unsigned long long h[atm::E_NSTAGE];
+  if (cudaStreamSynchronize(e->stream) != cudaSuccess ||
+      cudaMemcpy(h, e->d_stage, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return ATM_ERR_CUDA;
+  for (int i = 0; i < atm::E_NSTAGE; ++i) ms[i] = (double)h[i] * 1e-6;
   return ATM_OK;
 }
 
@@ -1538,7 +1567,7 @@ int atm_ensemble_barrier_check(long long timeout_ns, int* timed_out) {
   } else {
     // no members, one step: the first barrier waits for one block more than
     // the grid holds, so its wait runs out in every block
-    atm::EnsPlan p{nullptr, d_off, 0, 1, 0, d_bar, (unsigned)blocks + 1, d_err, timeout_ns};
+    atm::EnsPlan p{nullptr, d_off, 0, 1, 0, d_bar, (unsigned)blocks + 1, d_err, timeout_ns, nullptr};
     if (atm::ensemble_launch(p, blocks, 0) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
         cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
       rc = ATM_ERR_CUDA;

@@ -57,6 +57,7 @@ struct EnsPlan {
   unsigned expect;       // blocks a barrier waits for (the grid; one more makes every barrier run out)
   int* err;              // raised when a barrier wait ran out
   long long timeout_ns;  // limit of one barrier wait
+  unsigned long long* stage_ns;  // optional: nanoseconds between barrier exits, summed per stage (block 0's clock)
 };
 
 __host__ __device__ inline long long ens_div_up(long long a, long long b) { return (a + b - 1) / b; }
@@ -278,6 +279,8 @@ __global__ void __launch_bounds__(MW * MWARPS, 3) k_ensemble(EnsPlan p) {
   const long long nwarps = (long long)gridDim.x * MWARPS;
   const long long gw = (long long)blockIdx.x * MWARPS + (threadIdx.x >> 5);
   int flip = 0;  // swaps of the time levels so far (the same for every member)
+  const bool timer = p.stage_ns != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
+  long long tprev = timer ? global_ns() : 0;
   for (int s = 0; s < p.nsteps; ++s) {
     const bool remap = p.remap_every > 0 && (s + 1) % p.remap_every == 0;
     for (int stage = 0; stage < E_NSTAGE; ++stage) {
@@ -291,6 +294,11 @@ __global__ void __launch_bounds__(MW * MWARPS, 3) k_ensemble(EnsPlan p) {
       }
       if (stage == E_DMOM || stage == E_RENER) flip ^= 1;
       if (!ens_barrier(p)) return;
+      if (timer) {
+        const long long t = global_ns();
+        atomicAdd(p.stage_ns + stage, (unsigned long long)(t - tprev));
+        tprev = t;
+      }
     }
   }
 }

@@ -55,13 +55,15 @@ __device__ __forceinline__ bool finite_(float v) { return isfinite(v); }
 // hydrostatic gz from the bottom (src/mod_sw_dyn.f90:276-292 and 606-626).
 // One thread per column over [lo, n-1+hi]^2.  The downward pass writes
 // pkap; the upward pass reads it back (from L2: a block's columns were just
-// written), so no shared memory limits the occupancy.  The next layer's dp
-// is loaded one iteration ahead so that its latency overlaps atm_pow.
+// written), so no shared memory limits the occupancy.  Both passes load
+// eight levels at a time before using them, so that a thread keeps eight
+// loads in flight (the persistent ensemble kernel runs this at a quarter of
+// the column kernel's occupancy) and the eight atm_pow calls of a batch,
+// independent once the running sum is formed, overlap.
 template <typename T>
-__device__ __forceinline__ void column_at(const Geom& g, const Consts& c, const T* dpl,
-                                          const T* ptl, double* pkap,
-                                          double* gz, int lo, int hi, double* plev_out,
-                                          int col) {
+__device__ __forceinline__ void column_at(const Geom& g, const Consts& c, const T* dpl, const T* ptl, double* pkap,
+                                          double* gz, int lo, int hi, double* plev_out, int col) {
+  constexpr int B = 8;  // levels whose loads are in flight together
   const int w = g.nx - lo + hi;
   const int hgt = g.ny - lo + hi;
   if (col >= w * hgt) return;
@@ -71,27 +73,40 @@ __device__ __forceinline__ void column_at(const Geom& g, const Consts& c, const 
   const int L = g.L;
   double plev = c.ptop;
   if (plev_out) plev_out[o + (long long)L * S] = plev;
-  double dnext = (double)dpl[o + (long long)(L - 1) * S];
-  for (int k = L - 1; k >= 0; --k) {
-    const double d = dnext;
-    if (k > 0) dnext = (double)dpl[o + (long long)(k - 1) * S];
-    plev = plev + d;
-    if (plev_out) plev_out[o + (long long)k * S] = plev;
-    pkap[o + (long long)k * S] = atm_pow(plev, KAPPA);
+  for (int k0 = L - 1; k0 >= 0; k0 -= B) {
+    T dv[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) dv[u] = k0 - u >= 0 ? dpl[o + (long long)(k0 - u) * S] : T(0);
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int k = k0 - u;
+      if (k < 0) break;
+      plev = plev + (double)dv[u];
+      if (plev_out) plev_out[o + (long long)k * S] = plev;
+      pkap[o + (long long)k * S] = atm_pow(plev, KAPPA);
+    }
   }
   double z = gz[o];
   double pk0 = pkap[o];
-  double ptn = (double)ptl[o];
-  for (int k = 0; k < L; ++k) {
-    const double pk1 = k + 1 < L ? pkap[o + (long long)(k + 1) * S] : c.pk_top;
-    const double pt = ptn;
-    if (k + 1 < L) ptn = (double)ptl[o + (long long)(k + 1) * S];
-    z = z + CP_DRY * pt * (pk0 - pk1);
-    gz[o + (long long)(k + 1) * S] = z;
-    pk0 = pk1;
+  for (int k0 = 0; k0 < L; k0 += B) {
+    double pk[B];
+    T pv[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int k = k0 + u;
+      pk[u] = k + 1 < L ? pkap[o + (long long)(k + 1) * S] : c.pk_top;
+      pv[u] = k < L ? ptl[o + (long long)k * S] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int k = k0 + u;
+      if (k >= L) break;
+      z = z + CP_DRY * (double)pv[u] * (pk0 - pk[u]);
+      gz[o + (long long)(k + 1) * S] = z;
+      pk0 = pk[u];
+    }
   }
 }
-
 
 template <typename T>
 __global__ void __launch_bounds__(128) k_column(Geom g, Consts c, const T* __restrict__ dpl, const T* __restrict__ ptl,

@@ -242,6 +242,15 @@ int atm_ensemble_prepare(atm_ens* e);
 int atm_ensemble_run(atm_ens* e, int nsteps, int remap_every);
 int atm_ensemble_status(atm_ens* e, int* barrier_timed_out);
 int atm_ensemble_blocks(atm_ens* e, int* blocks);
+/* atm_ensemble_profile(e, 1) zeroes and enables per-stage timing of the
+   following launches (block 0 reads the global timer at every barrier exit;
+   0 disables it); atm_ensemble_stage_ms writes, for each of the 13 stages in
+   step order (C mass, C column, C momentum, C halo, D ring copy, D mass,
+   D column, corners, D momentum, remap ring copy, wind remap, energy remap,
+   D halo), the milliseconds between the exit of the barrier before it and
+   its own, summed over the timed launches (n >= 13). */
+int atm_ensemble_profile(atm_ens* e, int enable);
+int atm_ensemble_stage_ms(atm_ens* e, double* ms, int n);
 int atm_ensemble_destroy(atm_ens* e);
 int atm_ensemble_barrier_check(long long timeout_ns, int* timed_out);
 

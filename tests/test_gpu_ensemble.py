@@ -129,3 +129,23 @@ def test_persistent_barrier_wait_runs_out():
     a.run_persistent(5, 5)
     assert not a.barrier_timed_out() and a.stable()
     a.close()
+
+
+def test_persistent_stage_profile():
+    """Per-stage timing of a persistent launch: every stage that ran has a
+    positive time, the remap stages run only on remap steps, and the stages
+    add up to about the launch's own duration."""
+    b = Ensemble(members(), 'mixed', nstreams=1)
+    b.run_persistent(2, 0)
+    b.profile_persistent(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.run_persistent(4, 0)  # no remap
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = b.persistent_stage_ms()
+    assert all(st[s] > 0 for s in st if not s.startswith('remap'))
+    assert all(st[s] == 0 for s in ('remap_ring', 'remap_winds', 'remap_energy'))
+    assert 0.5 * ms < sum(st.values()) <= 1.05 * ms + 0.05
+    b.close()
