@@ -67,8 +67,10 @@ __host__ __device__ inline void ens_strips(const Geom& g, int lo, int hi, int ty
   sxn = (int)ens_div_up(g.nx - lo + hi, MOUT);
   syn = (int)ens_div_up(g.ny - lo + hi, tys);
 }
+// ring points of one level and field in a warp item: ENS_RING_R per lane
+constexpr int ENS_RING_R = 8;
 __host__ __device__ inline int ens_ring_chunks(const Geom& g) {
-  return (int)ens_div_up(2 * H * (g.nx + 2 * H) + 2 * H * g.ny, 32);
+  return (int)ens_div_up(2 * H * (g.nx + 2 * H) + 2 * H * g.ny, 32 * ENS_RING_R);
 }
 
 // warp items of a member in a stage
@@ -254,12 +256,12 @@ __device__ __forceinline__ void ens_item(int stage, const EnsMember& M, int cur,
     case E_RRING:
     case E_DHALO: {
       const int chunks = ens_ring_chunks(g);
-      const int idx = (int)(li % chunks) * 32 + lane;
+      const int idx = (int)(li % chunks) * 32 * ENS_RING_R + lane;
       const int k = (int)((li / chunks) % g.L);
       const int f = (int)(li / ((long long)chunks * g.L));
-      if (stage == E_CHALO) ring_at<C, false>(g, (C*)M.cg[f], nullptr, idx, k);
-      else if (stage == E_DHALO) ring_at<S, false>(g, (S*)M.st[cur][f], nullptr, idx, k);
-      else ring_at<S, true>(g, (S*)M.st[cur ^ 1][f], (const S*)M.st[cur][f], idx, k);  // new level keeps the old ring
+      if (stage == E_CHALO) ring_batch<C, false, ENS_RING_R>(g, (C*)M.cg[f], nullptr, idx, k);
+      else if (stage == E_DHALO) ring_batch<S, false, ENS_RING_R>(g, (S*)M.st[cur][f], nullptr, idx, k);
+      else ring_batch<S, true, ENS_RING_R>(g, (S*)M.st[cur ^ 1][f], (const S*)M.st[cur][f], idx, k);  // new level keeps the old ring
       break;
     }
     case E_RWIND:

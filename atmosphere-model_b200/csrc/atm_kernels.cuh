@@ -156,17 +156,28 @@ __device__ __forceinline__ double corner(const double* q, long long o, int P) {
   return out;
 }
 
-__device__ __forceinline__ void corner_at(const Geom& g, const double* pkap, const double* gz,
-                                          double* pkapb, double* gzb, int with_pkap, int lev0,
-                                          int nlev, int idx) {
+__device__ __forceinline__ void corner_at(const Geom& g, const double* pkap, const double* gz, double* pkapb,
+                                          double* gzb, int with_pkap, int lev0, int nlev, int idx) {
+  constexpr int B = 4;  // levels whose loads are issued before their stores
   const int w = g.nx + 1, h = g.ny + 1;
   if (idx >= w * h) return;
   const int x = idx % w, y = idx / w;
-  for (int l = lev0; l < lev0 + nlev; ++l) {
-    long long o = g.at(x, y, l);
-    if (with_pkap) pkapb[o] = corner(pkap, o, g.P);
-    long long o1 = g.at(x, y, l + (with_pkap ? 1 : 0));
-    gzb[o1] = corner(gz, o1, g.P);
+  for (int l0 = lev0; l0 < lev0 + nlev; l0 += B) {
+    double pb[B], zb[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int l = l0 + u;
+      if (l >= lev0 + nlev) break;
+      if (with_pkap) pb[u] = corner(pkap, g.at(x, y, l), g.P);
+      zb[u] = corner(gz, g.at(x, y, l + (with_pkap ? 1 : 0)), g.P);
+    }
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int l = l0 + u;
+      if (l >= lev0 + nlev) break;
+      if (with_pkap) pkapb[g.at(x, y, l)] = pb[u];
+      gzb[g.at(x, y, l + (with_pkap ? 1 : 0))] = zb[u];
+    }
   }
 }
 
@@ -181,23 +192,30 @@ static __global__ void k_corners(Geom g, const double* __restrict__ pkap, const 
 // periodic image in the interior.  With copy = true the ring of src is
 // copied to dst instead (the ring of a new time level keeps the old ring).
 // ring point idx of level k of one field f (src: the copy's source)
-template <typename T, bool COPY>
-__device__ __forceinline__ void ring_at(const Geom& g, T* f, const T* s, int idx, int k) {
+// Ring point idx (the halo bands of ring_at) of a level: its (x, y); false
+// past the ring.
+__device__ __forceinline__ bool ring_xy(const Geom& g, int idx, int& x, int& y) {
   const int wide = g.nx + 2 * H;
   const int nband = 2 * H * wide;
   const int nring = nband + 2 * H * g.ny;
-  if (idx >= nring) return;
-  int x, y;
+  if (idx >= nring) return false;
   if (idx < nband) {
-    int r = idx / wide;
+    const int r = idx / wide;
     y = r < H ? r - H : g.ny + (r - H);
     x = idx % wide - H;
   } else {
-    int q = idx - nband;
+    const int q = idx - nband;
     y = q / (2 * H);
-    int cc = q % (2 * H);
+    const int cc = q % (2 * H);
     x = cc < H ? cc - H : g.nx + (cc - H);
   }
+  return true;
+}
+
+template <typename T, bool COPY>
+__device__ __forceinline__ void ring_at(const Geom& g, T* f, const T* s, int idx, int k) {
+  int x, y;
+  if (!ring_xy(g, idx, x, y)) return;
   long long o = g.at(x, y, k);
   if (COPY) {
     f[o] = s[o];
@@ -206,6 +224,33 @@ __device__ __forceinline__ void ring_at(const Geom& g, T* f, const T* s, int idx
     int ys = y < 0 ? y + g.ny : (y >= g.ny ? y - g.ny : y);
     f[o] = f[g.at(xs, ys, k)];
   }
+}
+
+// R ring points idx0, idx0 + 32, ... of a level: all loads issued before the
+// stores (the ring's sources are interior points, which no store of the
+// pass touches)
+template <typename T, bool COPY, int R>
+__device__ __forceinline__ void ring_batch(const Geom& g, T* f, const T* s, int idx0, int k) {
+  T v[R];
+  long long od[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    int x, y;
+    od[r] = -1;
+    v[r] = T(0);
+    if (!ring_xy(g, idx0 + 32 * r, x, y)) continue;
+    od[r] = g.at(x, y, k);
+    if (COPY) {
+      v[r] = s[od[r]];
+    } else {
+      const int xs = x < 0 ? x + g.nx : (x >= g.nx ? x - g.nx : x);
+      const int ys = y < 0 ? y + g.ny : (y >= g.ny ? y - g.ny : y);
+      v[r] = f[g.at(xs, ys, k)];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    if (od[r] >= 0) f[od[r]] = v[r];
 }
 
 template <typename T, bool COPY>
