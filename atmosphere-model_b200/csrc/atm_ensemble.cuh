@@ -249,7 +249,7 @@ __device__ __forceinline__ void ens_item(int stage, const EnsMember& M, int cur,
       break;
     }
     case E_DCORN:
-      corner_at(g, M.pkap, M.gz, M.pkapb, M.gzb, 1, 0, g.L, (int)(li * 32 + lane));
+      corner_at<4>(g, M.pkap, M.gz, M.pkapb, M.gzb, 1, 0, g.L, (int)(li * 32 + lane));
       break;
     case E_CHALO:
     case E_DRING:

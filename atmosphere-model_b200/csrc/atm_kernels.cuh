@@ -156,9 +156,12 @@ __device__ __forceinline__ double corner(const double* q, long long o, int P) {
   return out;
 }
 
+// B levels' loads are issued before their stores: 1 in the corner kernel
+// (measured fastest there), 4 in the persistent ensemble kernel, whose
+// pointers carry no no-alias promise and which runs at lower occupancy.
+template <int B = 1>
 __device__ __forceinline__ void corner_at(const Geom& g, const double* pkap, const double* gz, double* pkapb,
                                           double* gzb, int with_pkap, int lev0, int nlev, int idx) {
-  constexpr int B = 4;  // levels whose loads are issued before their stores
   const int w = g.nx + 1, h = g.ny + 1;
   if (idx >= w * h) return;
   const int x = idx % w, y = idx / w;
