@@ -119,10 +119,6 @@ struct atm_ctx {
   double *lam_pk = nullptr, *lam_gz = nullptr, *lam_pkb = nullptr, *lam_gzb = nullptr;
   double *lam_ur = nullptr, *lam_vr = nullptr;
   int slot_in = 0;
-  // a second stream for the independent halves of the D-step reverse
-  // (forked from and joined back into the context's stream by events)
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // output accumulation (src/mod_output.f90:94-142): interior (nx, ny, K)
   // sums of dt * dp, pt, u, v (nlay levels) and net_flux (nlay+1 levels)
   double* acc[6] = {nullptr};
@@ -197,9 +193,6 @@ void free_all(atm_ctx* c) {
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_mass) cudaFreeHost(c->h_mass);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
-  if (c->side) cudaStreamDestroy(c->side);
-  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-  if (c->ev_join) cudaEventDestroy(c->ev_join);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
 }
 
@@ -894,46 +887,26 @@ int adj_d(atm_ctx* ctx, double dt, const void* const* so, const void* const* sn,
   CK(cudaMemsetAsync(ctx->lam_gz, 0, lev, ctx->stream));
   CK(cudaMemsetAsync(ctx->lam_pkb, 0, lev, ctx->stream));
   CK(cudaMemsetAsync(ctx->lam_gzb, 0, lev, ctx->stream));
-  // The kinetic-energy chain and the rest of the D-momentum reverse, and
-  // below the x and the y branch of the D-grid mass reverse: each pair reads
-  // the same inputs and adds into the same adjoints with atomics, so the two
-  // kernels run concurrently (the first on the side stream) and fill each
-  // other's barrier and latency stalls; profiled runs keep them in turn so
-  // that each stage is timed alone.
-  auto both = [&](int st1, int st2, auto&& launch) -> int {
-    if (ctx->prof || !ctx->side) {
-      for (int part = 1; part <= 2; ++part) {
-        Stage t(ctx, part == 1 ? st1 : st2);
-        CK(launch(ctx->stream, part));
-      }
-      return ATM_OK;
-    }
-    CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
-    CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
-    CK(launch(ctx->side, 1));
-    CK(launch(ctx->stream, 2));
-    CK(cudaEventRecord(ctx->ev_join, ctx->side));
-    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
-    ctx->launches += 2;
-    return ATM_OK;
-  };
-  int rc = both(S_ADMOM, S_ADMOM_VF, [&](cudaStream_t st, int part) {
-    return atm::adj_d_mom(g, k, o[F_UD], o[F_VD], cg[C_UC], cg[C_VC], ctx->pkapb, ctx->gzb, lout[F_UD], lout[F_VD],
-                          lin[F_UD], lin[F_VD], ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], ctx->lam_pkb, ctx->lam_gzb,
-                          &ctx->status->tma_timeout, st, part);
-  });
-  if (rc != ATM_OK) return rc;
+  // the kinetic-energy chain and the rest of the D-momentum reverse, each
+  // its own kernel and profiled stage
+  for (int part = 1; part <= 2; ++part) {
+    Stage t(ctx, part == 1 ? S_ADMOM : S_ADMOM_VF);
+    CK(atm::adj_d_mom(g, k, o[F_UD], o[F_VD], cg[C_UC], cg[C_VC], ctx->pkapb, ctx->gzb, lout[F_UD], lout[F_VD],
+                      lin[F_UD], lin[F_VD], ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], ctx->lam_pkb, ctx->lam_gzb,
+                      &ctx->status->tma_timeout, ctx->stream, part));
+  }
   {
     Stage t(ctx, S_ADCOL, 2);
     CK(atm::adj_corners(g, ctx->lam_pkb, ctx->lam_gzb, ctx->lam_pk, ctx->lam_gz, ctx->stream));
     CK(atm::adj_column(g, k, n[F_DP], n[F_PT], ctx->lam_pk, ctx->lam_gz, lout[F_DP], lout[F_PT], -2, 2, ctx->stream));
   }
-  rc = both(S_ADMASS, S_ADMASS_Y, [&](cudaStream_t st, int part) {
-    return atm::adj_mass(g, k, o[F_DP], o[F_PT], cg[C_UC], cg[C_VC], n[F_DP], n[F_PT], lout[F_DP], lout[F_PT],
-                         lin[F_DP], lin[F_PT], ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], -3, 3, &ctx->status->tma_timeout,
-                         false, st, part);
-  });
-  if (rc != ATM_OK) return rc;
+  // the x and the y branch of the D-grid mass reverse
+  for (int part = 1; part <= 2; ++part) {
+    Stage t(ctx, part == 1 ? S_ADMASS : S_ADMASS_Y);
+    CK(atm::adj_mass(g, k, o[F_DP], o[F_PT], cg[C_UC], cg[C_VC], n[F_DP], n[F_PT], lout[F_DP], lout[F_PT], lin[F_DP],
+                     lin[F_PT], ctx->lam_cg[C_UC], ctx->lam_cg[C_VC], -3, 3, &ctx->status->tma_timeout, false,
+                     ctx->stream, part));
+  }
   {
     Stage t(ctx, S_AHALO);
     CK(atm::adj_ring_copy(g, lout, lin, ctx->L, 3, 0, ctx->stream));
@@ -994,12 +967,6 @@ int atm_adj_enable(atm_ctx* ctx) {
   alloc(&ctx->lam_gzb, lev);
   alloc(&ctx->lam_ur, lay);
   alloc(&ctx->lam_vr, lay);
-  if (ok && (cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
-             cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-             cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess)) {
-    cudaGetLastError();
-    return fail(ctx, ATM_ERR_CUDA, "adjoint stream set-up failed");
-  }
   if (!ok) {
     cudaGetLastError();
     return fail(ctx, ATM_ERR_NOMEM, "adjoint fields do not fit on the device");
