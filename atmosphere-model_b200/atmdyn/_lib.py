@@ -37,7 +37,8 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_apply_physics', 'atm_physics_halo', 'atm_device_wait_check',
            'atm_ensemble_create', 'atm_ensemble_set_strips', 'atm_ensemble_set_stream', 'atm_ensemble_prepare',
            'atm_ensemble_run', 'atm_ensemble_status', 'atm_ensemble_blocks', 'atm_ensemble_destroy',
-           'atm_ensemble_barrier_check', 'atm_ensemble_profile', 'atm_ensemble_stage_ms')
+           'atm_ensemble_barrier_check', 'atm_ensemble_profile', 'atm_ensemble_stage_ms',
+           'atm_ensemble_set_schedule')
 ATM_ADJ_IN, ATM_ADJ_OUT = 0, 1
 
 # the entry points every build must export
@@ -131,6 +132,7 @@ def load():
         'atm_ensemble_status': ([vp, ctypes.POINTER(i)], None),
         'atm_ensemble_blocks': ([vp, ctypes.POINTER(i)], None),
         'atm_ensemble_profile': ([vp, i], None),
+        'atm_ensemble_set_schedule': ([vp, i], None),
         'atm_ensemble_stage_ms': ([vp, ctypes.POINTER(ctypes.c_double), i], None),
         'atm_ensemble_destroy': ([vp], None),
         'atm_ensemble_barrier_check': ([ctypes.c_longlong, ctypes.POINTER(i)], None),

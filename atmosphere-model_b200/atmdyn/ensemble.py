@@ -19,12 +19,14 @@ so the results are bit-identical to stepping the members one by one.
 
 For the mixed form, :meth:`Ensemble.run_persistent` and
 :meth:`Ensemble.capture_persistent` advance every member with ONE launch of
-the library's persistent kernel (``atm_ensemble_*``): each stage of a step
-is a queue of warp-sized work items over all members, the stages are
-separated by bounded grid-wide barriers, and each member's sweeps use the
-strip height of an autotuned table keyed on its grid size
-(:meth:`Ensemble.autotune`).  The results are again bit-identical to
-stepping the members one by one.
+the library's persistent kernel (``atm_ensemble_*``): the stages of every
+step are queues of warp-sized work items; by default each member advances
+through them on its own (a per-member ticket, so the stages of different
+members overlap), or, with :meth:`Ensemble.set_schedule` (False), all
+members take each stage together between bounded grid-wide barriers.  Each
+member's sweeps use the strip height of an autotuned table keyed on its
+grid size (:meth:`Ensemble.autotune`).  The results are again bit-identical
+to stepping the members one by one.
 """
 from __future__ import annotations
 
@@ -112,6 +114,13 @@ class Ensemble:
         self._prepare(stream.cuda_stream)
         _lib.check(lib.atm_ensemble_run(self.ens, nsteps, remap_every), None, 'atm_ensemble_run')
         self.steps_done += nsteps
+
+    def set_schedule(self, dataflow: bool = True):
+        """Schedule of the persistent kernel: dataflow (members advance on
+        their own, stages of different members overlap) or a grid barrier
+        after every stage."""
+        _lib.check(_lib.load().atm_ensemble_set_schedule(self._ens(), int(bool(dataflow))), None,
+                   'atm_ensemble_set_schedule')
 
     STAGES = ('c_mass', 'c_column', 'c_mom', 'c_halo', 'd_ring', 'd_mass', 'd_column', 'd_corners', 'd_mom',
               'remap_ring', 'remap_winds', 'remap_energy', 'd_halo')

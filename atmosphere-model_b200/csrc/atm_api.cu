@@ -1363,6 +1363,11 @@ struct atm_ens {
   bool prepared = false;
   int pending_flips = 0;  // time-level swaps of the launches since the last prepare
   unsigned long long* d_stage = nullptr;  // per-stage nanoseconds while profiling
+  // dataflow schedule: per-member phase tickets and completion counts, the
+  // finished-member count
+  int dataflow = 1;
+  unsigned long long* d_tk = nullptr;
+  unsigned* d_dn = nullptr;
 };
 
 namespace {
@@ -1374,6 +1379,8 @@ int ens_free(atm_ens* e) {
   cudaFree(e->d_bar);
   cudaFree(e->d_err);
   cudaFree(e->d_stage);
+  cudaFree(e->d_tk);
+  cudaFree(e->d_dn);
   if (e->h_err) cudaFreeHost(e->h_err);
   delete e;
   return ATM_OK;
@@ -1441,6 +1448,8 @@ int atm_ensemble_create(atm_ens** out, atm_ctx* const* members, const double* dt
       cudaMalloc((void**)&e->d_off, off_bytes) != cudaSuccess ||
       cudaMalloc((void**)&e->d_bar, 2 * sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc((void**)&e->d_err, sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&e->d_tk, sizeof(unsigned long long) * n) != cudaSuccess ||
+      cudaMalloc((void**)&e->d_dn, sizeof(unsigned) * (n + 1)) != cudaSuccess ||
       cudaMallocHost((void**)&e->h_err, sizeof(int)) != cudaSuccess) {
     ens_free(e);
     return ATM_ERR_NOMEM;
@@ -1483,12 +1492,16 @@ int atm_ensemble_run(atm_ens* e, int nsteps, int remap_every) {
   const int n = (int)e->m.size();
   const int remaps = remap_every > 0 ? nsteps / remap_every : 0;
   if (cudaMemsetAsync(e->d_bar, 0, 2 * sizeof(unsigned), e->stream) != cudaSuccess ||
-      cudaMemsetAsync(e->d_err, 0, sizeof(int), e->stream) != cudaSuccess)
+      cudaMemsetAsync(e->d_err, 0, sizeof(int), e->stream) != cudaSuccess ||
+      cudaMemsetAsync(e->d_tk, 0, sizeof(unsigned long long) * n, e->stream) != cudaSuccess ||
+      cudaMemsetAsync(e->d_dn, 0, sizeof(unsigned) * (n + 1), e->stream) != cudaSuccess)
     return ATM_ERR_CUDA;
+  // per-stage timing needs the stage barriers
   for (atm_ctx* c : e->m)
     if (cudaMemsetAsync(&c->status->nonfinite_step, 0, 2 * sizeof(int), e->stream) != cudaSuccess) return ATM_ERR_CUDA;
+  const int dataflow = e->dataflow && !e->d_stage;
   atm::EnsPlan p{e->d_members, e->d_off, n, nsteps, remap_every, e->d_bar, (unsigned)e->blocks, e->d_err,
-                 e->timeout_ns, e->d_stage};
+                 e->timeout_ns, e->d_stage, dataflow, e->d_tk, e->d_dn, e->d_dn + n};
   if (atm::ensemble_launch(p, e->blocks, e->stream) != cudaSuccess) return ATM_ERR_CUDA;
   const int flips = nsteps + remaps;
   e->pending_flips += flips;
@@ -1506,6 +1519,12 @@ int atm_ensemble_status(atm_ens* e, int* barrier_timed_out) {
       cudaStreamSynchronize(e->stream) != cudaSuccess)
     return ATM_ERR_CUDA;
   *barrier_timed_out = *e->h_err;
+  return ATM_OK;
+}
+
+int atm_ensemble_set_schedule(atm_ens* e, int dataflow) {
+  if (!e || (dataflow != 0 && dataflow != 1)) return ATM_ERR_ARG;
+  e->dataflow = dataflow;
   return ATM_OK;
 }
 
@@ -1567,7 +1586,8 @@ int atm_ensemble_barrier_check(long long timeout_ns, int* timed_out) {
   } else {
     // no members, one step: the first barrier waits for one block more than
     // the grid holds, so its wait runs out in every block
-    atm::EnsPlan p{nullptr, d_off, 0, 1, 0, d_bar, (unsigned)blocks + 1, d_err, timeout_ns, nullptr};
+    atm::EnsPlan p{nullptr, d_off, 0, 1, 0, d_bar, (unsigned)blocks + 1, d_err, timeout_ns, nullptr, 0,
+                   nullptr, nullptr, nullptr};
     if (atm::ensemble_launch(p, blocks, 0) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
         cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
       rc = ATM_ERR_CUDA;

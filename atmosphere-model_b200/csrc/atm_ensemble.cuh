@@ -58,6 +58,13 @@ struct EnsPlan {
   int* err;              // raised when a barrier wait ran out
   long long timeout_ns;  // limit of one barrier wait
   unsigned long long* stage_ns;  // optional: nanoseconds between barrier exits, summed per stage (block 0's clock)
+  // dataflow schedule (used when dataflow != 0): per member, the phase
+  // ticket (phase << 32 | next item to claim) and the items done in the
+  // phase; the count of members that finished the launch
+  int dataflow;
+  unsigned long long* tk;
+  unsigned* dn;
+  unsigned* fin;
 };
 
 __host__ __device__ inline long long ens_div_up(long long a, long long b) { return (a + b - 1) / b; }
@@ -274,12 +281,129 @@ __device__ __forceinline__ void ens_item(int stage, const EnsMember& M, int cur,
   }
 }
 
+// Phase ph of a launch (the stages of all steps in order, 10 per step and 13
+// on a remap step): its stage and the parity of the time-level swaps before
+// it (a swap follows the D-grid momentum sweep and the energy remap).
+__device__ __forceinline__ void ens_phase(int ph, int R, int& stage, int& flip) {
+  constexpr int kStep[10] = {E_CMASS, E_CCOL, E_CMOM, E_CHALO, E_DRING, E_DMASS, E_DCOL, E_DCORN, E_DMOM, E_DHALO};
+  if (R <= 0) {
+    const int s = ph / 10, j = ph - 10 * (ph / 10);
+    stage = kStep[j];
+    flip = (s + (j == 9 ? 1 : 0)) & 1;
+    return;
+  }
+  const int per = 10 * R + 3;  // phases of a remap cycle
+  const int c = ph / per, q = ph - per * c;
+  const int base = c * (R + 1);  // swaps of the earlier cycles
+  if (q < 10 * (R - 1)) {
+    const int s = q / 10, j = q - 10 * s;
+    stage = kStep[j];
+    flip = (base + s + (j == 9 ? 1 : 0)) & 1;
+  } else {
+    const int j = q - 10 * (R - 1);  // the remap step: all 13 stages in order
+    stage = j;
+    flip = (base + (R - 1) + (j > E_DMOM ? 1 : 0) + (j > E_RENER ? 1 : 0)) & 1;
+  }
+}
+
+__device__ __forceinline__ long long ens_count(const EnsPlan& p, int stage, int m) {
+  const long long* off = p.off + (long long)stage * (p.nm + 1);
+  return off[m + 1] - off[m];
+}
+
+// Dataflow schedule: no grid barrier.  Each member advances through its
+// phases on its own: a warp claims the next item of any member whose
+// current phase has items left (an atomic add on the member's ticket), runs
+// it, and the warp completing a phase's last item opens the member's next
+// phase.  So the compute-bound sweeps of some members overlap the
+// memory-bound column, corner, ring and remap passes of others.  Writes of
+// a phase are released by a fence before its completion count and acquired
+// by a fence after the claim of a later phase's item.  A warp that finds
+// no work for longer than the plan's limit raises the error word and
+// leaves; the others leave at their next idle check.
+template <typename T, typename S, typename C>
+__device__ __forceinline__ void ens_dataflow(const EnsPlan& p, long long gw) {
+  const int lane = threadIdx.x & 31;
+  const int R = p.remap_every;
+  const int P = p.nsteps * 10 + (R > 0 ? (p.nsteps / R) * 3 : 0);
+  int start = (int)(gw % p.nm);
+  long long idle0 = global_ns();
+  while (true) {
+    int m = -1, ph = 0;
+    long long item = 0;
+    if (lane == 0) {
+      for (int t = 0; t < p.nm; ++t) {
+        int mm = start + t;
+        if (mm >= p.nm) mm -= p.nm;
+        const unsigned long long tk = *(volatile unsigned long long*)(p.tk + mm);
+        const int ph0 = (int)(tk >> 32);
+        if (ph0 >= P) continue;
+        int st0, fl0;
+        ens_phase(ph0, R, st0, fl0);
+        if ((long long)(tk & 0xffffffffull) >= ens_count(p, st0, mm)) continue;
+        const unsigned long long old = atomicAdd(p.tk + mm, 1ull);
+        const int ph1 = (int)(old >> 32);
+        if (ph1 >= P) continue;
+        int st1, fl1;
+        ens_phase(ph1, R, st1, fl1);
+        const long long it1 = (long long)(old & 0xffffffffull);
+        if (it1 >= ens_count(p, st1, mm)) continue;
+        m = mm;
+        ph = ph1;
+        item = it1;
+        break;
+      }
+    }
+    m = __shfl_sync(0xffffffffu, m, 0);
+    if (m < 0) {
+      int stop = 0;
+      if (lane == 0) {
+        if (*(volatile unsigned*)p.fin >= (unsigned)p.nm || *(volatile int*)p.err != 0) {
+          stop = 1;
+        } else if (global_ns() - idle0 > p.timeout_ns) {
+          atomicOr(p.err, 1);
+          stop = 1;
+        } else {
+          __nanosleep(256);
+        }
+      }
+      if (__shfl_sync(0xffffffffu, stop, 0)) return;
+      continue;
+    }
+    ph = __shfl_sync(0xffffffffu, ph, 0);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    idle0 = global_ns();
+    start = m;
+    __threadfence();  // acquire: the member's earlier phases
+    int stage, flip;
+    ens_phase(ph, R, stage, flip);
+    const EnsMember& M = p.m[m];
+    ens_item<T, S, C>(stage, M, M.cur0 ^ flip, item);
+    __threadfence();  // release: this item's writes
+    __syncwarp();
+    if (lane == 0) {
+      const unsigned done = atomicAdd(p.dn + m, 1u) + 1u;
+      if ((long long)done == ens_count(p, stage, m)) {
+        atomicExch(p.dn + m, 0u);
+        __threadfence();
+        if (ph + 1 >= P) atomicAdd(p.fin, 1u);
+        atomicExch(p.tk + m, (unsigned long long)(ph + 1) << 32);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // The run: p.nsteps steps of every member, the remap on steps whose number
 // (counted from 1 at the launch) is a multiple of p.remap_every.
 template <typename T, typename S, typename C>
 __global__ void __launch_bounds__(MW * MWARPS, 3) k_ensemble(EnsPlan p) {
   const long long nwarps = (long long)gridDim.x * MWARPS;
   const long long gw = (long long)blockIdx.x * MWARPS + (threadIdx.x >> 5);
+  if (p.dataflow) {
+    if (p.nm > 0) ens_dataflow<T, S, C>(p, gw);
+    return;
+  }
   int flip = 0;  // swaps of the time levels so far (the same for every member)
   const bool timer = p.stage_ns != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
   long long tprev = timer ? global_ns() : 0;

@@ -231,7 +231,7 @@ int atm_remap_noalloc(int nx, int ny, int nlay, const double* ak, const double* 
    (nsteps + nsteps / remap_every even), so that a captured launch can be
    replayed.  atm_ensemble_set_strips sets a member's strip height of the
    marching sweeps (16, 32 or 64 rows; default 32).
-   atm_ensemble_barrier_check launches the kernel with no members and a
+   atm_ensemble_barrier_check launches the barrier schedule with no members and a
    barrier that waits for one block more than the grid holds: *timed_out
    reports that the bounded wait ran out and the launch ended. */
 typedef struct atm_ens atm_ens;
@@ -250,6 +250,14 @@ int atm_ensemble_blocks(atm_ens* e, int* blocks);
    D halo), the milliseconds between the exit of the barrier before it and
    its own, summed over the timed launches (n >= 13). */
 int atm_ensemble_profile(atm_ens* e, int enable);
+/* The schedule of the following launches: 1 (default) dataflow -- no grid
+   barrier; each member advances through its stages on its own, a warp
+   claiming the next item of any member whose current stage has items left
+   (an atomic ticket per member), so the stages of different members
+   overlap; an idle wait longer than the limit raises the status word.
+   0: every stage of every member, then a grid barrier.  Profiled launches
+   (atm_ensemble_profile) use the barriers. */
+int atm_ensemble_set_schedule(atm_ens* e, int dataflow);
 int atm_ensemble_stage_ms(atm_ens* e, double* ms, int n);
 int atm_ensemble_destroy(atm_ens* e);
 int atm_ensemble_barrier_check(long long timeout_ns, int* timed_out);

@@ -70,15 +70,18 @@ def _assert_same(a, b):
 
 
 @pytest.mark.parametrize('strips', [None, {32: 16, 48: 32, 40: 16, 64: 64, 24: 32}])
-def test_persistent_kernel_matches_eager(strips):
+@pytest.mark.parametrize('dataflow', [True, False])
+def test_persistent_kernel_matches_eager(strips, dataflow):
     """One launch of the persistent kernel advances every member (uneven
     sizes and layer counts) by 10 steps with two remaps, bit for bit as
-    stepping the members one by one, whatever the strip heights."""
+    stepping the members one by one, whatever the strip heights, with the
+    dataflow schedule and with the stage barriers."""
     a = Ensemble(members(), 'mixed', nstreams=3)
     b = Ensemble(members(), 'mixed', nstreams=3)
     a.step_eager(10)
     if strips:
         b.set_strips(strips)
+    b.set_schedule(dataflow)
     b.run_persistent(10, 5)
     torch.cuda.synchronize()
     assert not b.barrier_timed_out()
@@ -89,8 +92,9 @@ def test_persistent_kernel_matches_eager(strips):
 
 
 def test_persistent_launch_as_graph_replays():
-    """Two remap cycles as one persistent launch captured in a CUDA graph,
-    replayed twice: 20 steps, bit-identical to eager stepping."""
+    """Two remap cycles as one persistent launch (dataflow schedule)
+    captured in a CUDA graph, replayed twice: 20 steps, bit-identical to
+    eager stepping."""
     a = Ensemble(members(), 'mixed', nstreams=3)
     b = Ensemble(members(), 'mixed', nstreams=3)
     a.step_eager(20)
@@ -148,4 +152,24 @@ def test_persistent_stage_profile():
     assert all(st[s] > 0 for s in st if not s.startswith('remap'))
     assert all(st[s] == 0 for s in ('remap_ring', 'remap_winds', 'remap_energy'))
     assert 0.5 * ms < sum(st.values()) <= 1.05 * ms + 0.05
+    b.close()
+
+
+def test_dataflow_odd_step_counts():
+    """The dataflow schedule's phase arithmetic: a launch whose remap cycle
+    does not divide its step count (7 steps, remap every 3: remaps after
+    steps 3 and 6, none after step 7) and a launch without remap, bit-
+    identical to eager stepping."""
+    a = Ensemble(members(), 'mixed', nstreams=3)
+    b = Ensemble(members(), 'mixed', nstreams=3)
+    for n in range(1, 9):
+        for st, d in zip(a.members, a.dyn):
+            d.step(st.dt, remap=(n <= 7 and n % 3 == 0), check_stable=False)
+    b.set_schedule(True)
+    b.run_persistent(7, 3)  # 7 steps and 2 remaps: 9 swaps of the time levels
+    b.run_persistent(1, 0)  # one step more: 10 swaps
+    torch.cuda.synchronize()
+    assert not b.barrier_timed_out()
+    _assert_same(_fields(a), _fields(b))
+    a.close()
     b.close()
