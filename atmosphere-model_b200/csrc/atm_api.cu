@@ -1365,7 +1365,7 @@ struct atm_ens {
   unsigned long long* d_stage = nullptr;  // per-stage nanoseconds while profiling
   // dataflow schedule: per-member phase tickets and completion counts, the
   // finished-member count
-  int dataflow = 1;
+  int dataflow = 0;
   unsigned long long* d_tk = nullptr;
   unsigned* d_dn = nullptr;
 };

@@ -250,12 +250,12 @@ int atm_ensemble_blocks(atm_ens* e, int* blocks);
    D halo), the milliseconds between the exit of the barrier before it and
    its own, summed over the timed launches (n >= 13). */
 int atm_ensemble_profile(atm_ens* e, int enable);
-/* The schedule of the following launches: 1 (default) dataflow -- no grid
-   barrier; each member advances through its stages on its own, a warp
-   claiming the next item of any member whose current stage has items left
-   (an atomic ticket per member), so the stages of different members
-   overlap; an idle wait longer than the limit raises the status word.
-   0: every stage of every member, then a grid barrier.  Profiled launches
+/* The schedule of the following launches: 0 (default) every stage of every
+   member, then a grid barrier; 1 dataflow -- no grid barrier: each member
+   advances through its stages on its own, a warp claiming the next item of
+   any member whose current stage has items left (an atomic ticket per
+   member), so the stages of different members overlap; an idle wait longer
+   than the limit raises the status word.  Profiled launches
    (atm_ensemble_profile) use the barriers. */
 int atm_ensemble_set_schedule(atm_ens* e, int dataflow);
 int atm_ensemble_stage_ms(atm_ens* e, double* ms, int n);

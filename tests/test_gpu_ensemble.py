@@ -98,6 +98,7 @@ def test_persistent_launch_as_graph_replays():
     a = Ensemble(members(), 'mixed', nstreams=3)
     b = Ensemble(members(), 'mixed', nstreams=3)
     a.step_eager(20)
+    b.set_schedule(True)
     b.capture_persistent(5, cycles=2)
     b.replay(2)
     torch.cuda.synchronize()
