@@ -149,6 +149,30 @@ def dist_setup():
     return world, rank, local
 
 
+class Ranks:
+    """Rank coordination of a run: a barrier, and the maximum of a device
+    time over the ranks (every rank takes the same collective steps in the
+    same order).  One rank: no collective."""
+
+    def __init__(self, world, device):
+        self.world, self.device = world, device
+
+    def barrier(self):
+        import torch
+        if self.world > 1:
+            torch.distributed.barrier()
+        if self.device.type == 'cuda':
+            torch.cuda.synchronize()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+
 def cpu_grad_throughput(n, steps, warmup, threads):
     """The FP64 restatement of the reference on the host cores, on the jet
     case at n x n x NLAY (remap every REMAP_EVERY steps, counted from the
@@ -249,17 +273,8 @@ def run_ours(args):
     K, W = args.steps, args.warmup
     peak, peak_kind = load_peaks()
 
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device='cuda')
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(world, torch.device('cuda', torch.cuda.current_device()))
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     results = {}
     states = {}
