@@ -8,19 +8,24 @@
 // D-grid column, corner interpolation, D-grid momentum sweep, [ring copy,
 // wind remap, energy remap], D-grid halo fill.  A stage's work is a queue
 // of warp-sized items over all members -- a (member, layer, strip) of a
-// marching sweep, or 32 consecutive columns / points of the column, corner,
-// ring and remap passes -- which the resident warps take in turn, so small
-// and large members share the GPU within each stage.  Stages are separated
-// by a grid-wide barrier whose wait is bounded: a block that waits longer
-// than the plan's limit raises the error word and returns, and every other
-// block returns at its next barrier, so a failed barrier ends the launch
-// instead of hanging it.
+// marching sweep, 32 consecutive columns or corners, or 8 x 32 ring points
+// of a level -- which the resident warps take in turn, so small and large
+// members share the GPU within each stage.  Two schedules:
+//  * barrier (default): every member takes a stage together, and stages are
+//    separated by a grid-wide barrier whose wait is bounded: a block that
+//    waits longer than the plan's limit raises the error word and returns,
+//    and every other block returns at its next barrier or as soon as it
+//    sees the error, so a failed barrier ends the launch instead of hanging
+//    it;
+//  * dataflow: no grid barrier; each member advances through its stages on
+//    its own (ens_dataflow), so the stages of different members overlap.
 //
 // The per-member strip height of the marching sweeps (16, 32 or 64 rows)
 // comes from the plan (an autotuned table keyed on the member's grid size).
 // Fields written by one stage are read by later stages of the same launch,
 // so every stage reads with plain (coherent) loads, never through the
-// read-only data path; the barrier's fences order the writes before them.
+// read-only data path; the fences of the barrier (or of the dataflow
+// tickets) order the writes before them.
 // The stage bodies are the single-domain kernels' device functions, so a
 // member's results are bit-identical to stepping it alone.
 #pragma once

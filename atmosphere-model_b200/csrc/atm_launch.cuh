@@ -26,14 +26,13 @@ constexpr int TY_DMASS = FP64_FORM ? 6 : 16;
 constexpr int TY_CMOM = 8;
 constexpr int TY_DMOM = 4;
 // The mixed form (ATM_MARCH_SWEEPS) runs its four sweeps as column-marching
-// kernels (atm_march.cuh): measured on B200 at 1024x1024x64 against its
-// tiles, C momentum 2.83 / D mass 2.01 / D momentum 2.82 ms against 3.01 /
-// 2.66 / 4.05, and C mass 2.94 against 2.70 (kept marching so that the
-// persistent ensemble kernel, which has only the marching sweeps, is
-// bit-identical to it).  The FP64 form keeps the tiles: its marching
-// sweeps took 29.1 ms a step against 17.4 (at 136-174 registers a thread
-// they hold too few warps to hide the FP64 latency, and they execute about
-// as many instructions per cell).
+// kernels (atm_march.cuh): measured on B200 at 1024x1024x64, C mass 1.79 /
+// C momentum 2.21 / D mass 1.84 / D momentum 2.43 ms against its tiles'
+// 2.70 / 3.01 / 2.66 / 4.05 (and the persistent ensemble kernel, which has
+// only the marching sweeps, is bit-identical to it).  The FP64 form keeps
+// the tiles: its marching sweeps took 29.1 ms a step against 17.4 (at
+// 136-174 registers a thread they hold too few warps to hide the FP64
+// latency, and they execute about as many instructions per cell).
 #ifdef ATM_MARCH_SWEEPS
 constexpr bool MARCH = true;
 #else

@@ -10,13 +10,19 @@
 // neighbouring lanes by warp shuffles.  No shared memory and no block-wide
 // barrier: the warps of a block are independent.
 //
+// Each iteration loads the inputs of the next row before working on the
+// current one, so that the loads' latency overlaps a row of arithmetic.
+//
 // The stage formulas, index shifts and evaluation order are those of the
 // tile kernels (atm_sweeps.cuh) and of the reference, so FP64 instances
-// are bit-identical to them (checked by the parity tests).  The mixed form
-// launches its C-momentum, D-mass and D-momentum sweeps as marching
-// kernels; in FP64 the tiles are faster (the marching FP64 sweeps execute
-// about as many instructions per cell, at 140-174 registers a thread and
-// 17 % warps active), so the FP64 form keeps them.
+// are bit-identical to them (the oracle's parity tests passed with the
+// FP64 form built on these kernels).  The mixed form launches its four
+// sweeps as marching kernels; in FP64 the tiles are faster (the marching
+// FP64 sweeps execute about as many instructions per cell, at 140-174
+// registers a thread and 17 % warps active), so the FP64 form keeps them.
+// The persistent ensemble kernel runs the same strip functions with plain
+// loads (RO = false), as it reads fields that it wrote earlier in the same
+// launch.
 #pragma once
 
 #include <type_traits>
