@@ -28,12 +28,6 @@ cudaError_t smem_attr(K kernel, size_t bytes) {
 
 cudaError_t adj_setup() {
   cudaError_t e;
-  // the remap adjoints keep their column arrays in local memory and use no
-  // shared memory: all of the SM's L1/shared capacity as L1
-  for (const void* k : {(const void*)k_remap_winds_adj<32>, (const void*)k_remap_winds_adj<64>,
-                        (const void*)k_remap_winds_adj<MAX_LAYERS>, (const void*)k_remap_energy_adj<32>,
-                        (const void*)k_remap_energy_adj<64>, (const void*)k_remap_energy_adj<MAX_LAYERS>})
-    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 0))) return e;
   if ((e = smem_attr(k_mass_adj1<TXA, TYC, true>, MassAdj1L<TXA, TYC, true>::bytes))) return e;
   if ((e = smem_attr(k_mass_adj<TXA, TYA, false, true>, MassAdjBL<TXA, TYA, false>::bytes))) return e;
   if ((e = smem_attr(k_mass_adj<TXA, TYA, false, false>, MassAdjBL<TXA, TYA, false>::bytes))) return e;

@@ -58,19 +58,8 @@ cudaError_t smem_attr(K kernel, size_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-// The column-local remap kernels keep their column arrays in local memory
-// and use no shared memory: all of the SM's L1/shared capacity as L1.
-template <typename K>
-cudaError_t l1_max(K kernel) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-}
-
 cudaError_t setup() {
   cudaError_t e;
-  if ((e = l1_max(k_remap_winds<S, 32>)) || (e = l1_max(k_remap_winds<S, 64>)) ||
-      (e = l1_max(k_remap_winds<S, MAX_LAYERS>)) || (e = l1_max(k_remap_energy<S, 32>)) ||
-      (e = l1_max(k_remap_energy<S, 64>)) || (e = l1_max(k_remap_energy<S, MAX_LAYERS>)))
-    return e;
   if ((e = smem_attr(k_mass2<T, TX, TY_CMASS, true, S, C>, MassL<T, TX, TY_CMASS, true, S, C>::bytes)) != cudaSuccess)
     return e;
   if ((e = smem_attr(k_mass2<T, TX, TY_DMASS, false, S, C>, MassL<T, TX, TY_DMASS, false, S, C>::bytes)) !=
