@@ -55,12 +55,20 @@ __device__ __forceinline__ T shfl_up(T v, int d) {
   return __shfl_up_sync(0xffffffffu, v, d);
 }
 
+// a * b + c.  The mixed form's translation unit is compiled without
+// contraction (so that every kernel inlining these functions rounds them
+// alike), and its FP32 arithmetic asks for its fused operations here; in
+// FP64 the unfused expression, whose value equals the formula as written
+// (an IEEE sum does not depend on the order of its two operands).
+__device__ __forceinline__ float fmadd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmadd(double a, double b, double c) { return a * b + c; }
+
 // Edge anomalies of a cell from its value and neighbours (qm, q0, qp) and
 // their monotone slopes (mm, m0, mp): the operations of edges_pre.
 template <typename T, int V>
 __device__ __forceinline__ void edges_v(T qm, T q0, T qp, T mm, T m0, T mp, T& eL, T& eR) {
-  eL = (qm - q0) * T(0.5) + div_const<3>(mm - m0);
-  eR = (qp - q0) * T(0.5) + div_const<3>(m0 - mp);
+  eL = fmadd(qm - q0, T(0.5), div_const<3>(mm - m0));
+  eR = fmadd(qp - q0, T(0.5), div_const<3>(m0 - mp));
   if (V == PPM_CON || V == PPM_NN) {
     const T d0 = (qp - qm) * T(0.25);
     const T lim = T(2) * fab(d0);
@@ -91,11 +99,11 @@ __device__ __forceinline__ void edges_v(T qm, T q0, T qp, T mm, T m0, T mp, T& e
 template <typename T, int V>
 __device__ __forceinline__ T flux_v(T c, T qm, T q0, T qp, T mm, T m0, T mp) {
   const T sa = fab(c);
-  const T k1 = (T(1) - T(2) * sa) * (T(1) - sa);
+  const T k1 = fmadd(T(-2), sa, T(1)) * (T(1) - sa);
   const T k2 = sa * (sa - T(1));
   T eL, eR;
   edges_v<T, V>(qm, q0, qp, mm, m0, mp, eL, eR);
-  return (c > T(0)) ? q0 + k1 * eR + k2 * eL : q0 + k1 * eL + k2 * eR;
+  return (c > T(0)) ? fmadd(k2, eL, fmadd(k1, eR, q0)) : fmadd(k2, eR, fmadd(k1, eL, q0));
 }
 
 // Flux with the edge values of the upwind candidates given (PPM_CONSTRAINED):
@@ -106,9 +114,9 @@ __device__ __forceinline__ T flux_con_v(T c, T qm, T q0, T eLm, T eRm, T eL0, T 
   if ((T(3) * fab(eL0 + eR0) > fab(eL0 - eR0)) && (T(3) * fab(eLm + eRm) > fab(eLm - eRm)))
     return (c > T(0)) ? qm : q0;
   const T sa = fab(c);
-  const T k1 = (T(1) - T(2) * sa) * (T(1) - sa);
+  const T k1 = fmadd(T(-2), sa, T(1)) * (T(1) - sa);
   const T k2 = sa * (sa - T(1));
-  return (c > T(0)) ? qm + k1 * eRm + k2 * eLm : q0 + k1 * eL0 + k2 * eR0;
+  return (c > T(0)) ? fmadd(k2, eLm, fmadd(k1, eRm, qm)) : fmadd(k2, eR0, fmadd(k1, eL0, q0));
 }
 
 __device__ __forceinline__ double slope_v(double qm, double q0, double qp) {
@@ -236,13 +244,13 @@ __device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* dp,
     T txn, tpn;
     {
       const T cx0 = dtdx * ucn, cx1 = dtdx * ucR;
-      const T den = T(1) / (T(1) - dtdx * (ucR - ucn));
+      const T den = T(1) / fmadd(-dtdx, ucR - ucn, T(1));
       T f0 = (cx0 > T(0)) ? dL : dn;
       T f1 = (cx1 > T(0)) ? dn : dR;
-      txn = T(.5) * (dn + den * (dn - rA * (f1 - f0)));
+      txn = T(.5) * fmadd(den, fmadd(-rA, f1 - f0, dn), dn);
       f0 = (cx0 > T(0)) ? pL : pn;
       f1 = (cx1 > T(0)) ? pn : pR;
-      tpn = T(.5) * (pn + den * (pn - rA * (f1 - f0)));
+      tpn = T(.5) * fmadd(den, fmadd(-rA, f1 - f0, pn), pn);
     }
     // shift the windows to the new row
     d4 = d3; d3 = d2; d2 = d1; d1 = d0; d0 = dn;
@@ -283,8 +291,8 @@ __device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* dp,
       const T pl = shfl_up(p2, 1), pr = shfl_dn(p2, 1);
       ld2 = ld1; ld1 = ld0;
       lq2 = lq1; lq1 = lq0;
-      ld0 = T(-2.) * d2 * rdxy + (dr + dl) * rdx2 + (d1 + d3) * rdy2;
-      lq0 = T(-2.) * p2 * rdxy + (pr + pl) * rdx2 + (p1 + p3) * rdy2;
+      ld0 = fmadd(d1 + d3, rdy2, fmadd(dr + dl, rdx2, T(-2.) * d2 * rdxy));
+      lq0 = fmadd(p1 + p3, rdy2, fmadd(pr + pl, rdx2, T(-2.) * p2 * rdxy));
     }
     const int y = j - 3;
     if (y < oy) continue;  // warm-up rows of the strip (warp-uniform)
@@ -292,13 +300,13 @@ __device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* dp,
     T tyd, typ;
     {
       const T cy0 = dtdx * vc1, cy1 = dtdx * vc0;
-      const T den = T(1) / (T(1) - dtdy * (vc0 - vc1));
+      const T den = T(1) / fmadd(-dtdy, vc0 - vc1, T(1));
       T f0 = (cy0 > T(0)) ? d4 : d3;
       T f1 = (cy1 > T(0)) ? d3 : d2;
-      tyd = T(.5) * (d3 + den * (d3 - rA * (f1 - f0)));
+      tyd = T(.5) * fmadd(den, fmadd(-rA, f1 - f0, d3), d3);
       f0 = (cy0 > T(0)) ? p4 : p3;
       f1 = (cy1 > T(0)) ? p3 : p2;
-      typ = T(.5) * (p3 + den * (p3 - rA * (f1 - f0)));
+      typ = T(.5) * fmadd(den, fmadd(-rA, f1 - f0, p3), p3);
     }
     const T mxd = slope_v(shfl_up(tyd, 1), tyd, shfl_dn(tyd, 1));
     const T mxp = slope_v(shfl_up(typ, 1), typ, shfl_dn(typ, 1));
@@ -332,10 +340,10 @@ __device__ __forceinline__ void mass_strip(Geom g, Consts c, const S* dp,
       // the same update in flux form: interface fluxes (advective plus
       // vorticity-damping) in the sweep type, their differences applied to
       // the state's type, so that mass and dp*pt telescope in S
-      const T Fx0 = fxd + dxv * (ld1 - lxm), Fx1 = fxd1 + dxv * (lxp - ld1);
-      const T Fy0 = fy1 + dyv * (ld1 - ld2), Fy1 = fy0 + dyv * (ld0 - ld1);
-      const T Hx0 = (fxp + vdx * (lq1 - qxm)) * fxd, Hx1 = (fxp1 + vdx * (qxp - lq1)) * fxd1;
-      const T Hy0 = (fq1 + vdy * (lq1 - lq2)) * fy1, Hy1 = (fq0 + vdy * (lq0 - lq1)) * fy0;
+      const T Fx0 = fmadd(dxv, ld1 - lxm, fxd), Fx1 = fmadd(dxv, lxp - ld1, fxd1);
+      const T Fy0 = fmadd(dyv, ld1 - ld2, fy1), Fy1 = fmadd(dyv, ld0 - ld1, fy0);
+      const T Hx0 = fmadd(vdx, lq1 - qxm, fxp) * fxd, Hx1 = fmadd(vdx, qxp - lq1, fxp1) * fxd1;
+      const T Hy0 = fmadd(vdy, lq1 - lq2, fq1) * fy1, Hy1 = fmadd(vdy, lq0 - lq1, fq0) * fy0;
       const S d = d_upd;
       const S vv = d - ((S(Fx1) - S(Fx0)) + (S(Fy1) - S(Fy0)));
       S q = d * p_upd - ((S(Hx1) - S(Hx0)) + (S(Hy1) - S(Hy0)));
@@ -427,15 +435,15 @@ __device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* ud,
     vnp_p = fvd(x + 1, j + 1);
     const T ucn = T(.5) * (T(.5) * (u_x + u_xm) + T(.5) * (un + unm));
     const T vcn = T(.5) * (T(.5) * (vn + v_x) + T(.5) * (vnp + v_xp));
-    const T vor = f - (ucn - a0) * rdy + (vcn - shfl_up(vcn, 1)) * rdx;
+    const T vor = fmadd(vcn - shfl_up(vcn, 1), rdx, fmadd(-(ucn - a0), rdy, f));
     const T vl = shfl_up(vor, 1), vr = shfl_dn(vor, 1);
     T tun;
     {
       const T c0 = dtdx * u_xm, c1 = dtdx * u_x;
-      const T den = T(1) / (T(1) - dtdx * (u_x - u_xm));
+      const T den = T(1) / fmadd(-dtdx, u_x - u_xm, T(1));
       const T f0 = (c0 > T(0)) ? vl : vor;
       const T f1 = (c1 > T(0)) ? vor : vr;
-      tun = T(.5) * (vor + den * (vor - rA * (f1 - f0)));
+      tun = T(.5) * fmadd(den, fmadd(-rA, f1 - f0, vor), vor);
     }
     uw3 = uw2; uw2 = uw1; uw1 = uw0; uw0 = u_x;
     u_x = un;
@@ -451,7 +459,7 @@ __device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* ud,
     mt4 = mt3; mt3 = mt2; mt2 = mt1; mt1 = slope_v(t2, t1, t0);
     // Laplacian of the vorticity at row j-2
     lp1 = lp0;
-    lp0 = T(-2.) * w2 * rdxy + (shfl_dn(w2, 1) + shfl_up(w2, 1)) * rdx2 + (w1 + w3) * rdy2;
+    lp0 = fmadd(w1 + w3, rdy2, fmadd(shfl_dn(w2, 1) + shfl_up(w2, 1), rdx2, T(-2.) * w2 * rdxy));
     const int y = j - 3;
     if (y < oy - 1) continue;  // warm-up rows (warp-uniform)
     // ---- row y: kinetic energy (:299-317) with the layer-nlay A-grid winds
@@ -476,7 +484,7 @@ __device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* ud,
       const int s0 = lane + ((cx > T(0)) ? 0 : 1);  // the upwind cell's lane
       const T fx = flux_v<T, UNC>(cx, shfl_at(a3, s0 - 1), shfl_at(a3, s0), shfl_at(a3, s0 + 1),
                                   shfl_at(mux, s0 - 1), shfl_at(mux, s0), shfl_at(mux, s0 + 1));
-      ken = T(.5) * (kv + ua * fx);
+      ken = T(.5) * fmadd(ua, fx, kv);
     }
     uL1 = uL0;
     vL2 = vL1;
@@ -491,10 +499,10 @@ __device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* ud,
     T tvn;
     {
       const T c0 = dtdx * vw4, c1 = dtdx * vw3;
-      const T den = T(1) / (T(1) - dtdy * (vw3 - vw4));
+      const T den = T(1) / fmadd(-dtdy, vw3 - vw4, T(1));
       const T f0 = (c0 > T(0)) ? w4 : w3;
       const T f1 = (c1 > T(0)) ? w3 : w2;
-      tvn = T(.5) * (w3 + den * (w3 - rA * (f1 - f0)));
+      tvn = T(.5) * fmadd(den, fmadd(-rA, f1 - f0, w3), w3);
     }
     const T mtv = slope_v(shfl_up(tvn, 1), tvn, shfl_dn(tvn, 1));
     const T ke_l = shfl_up(ke0, 1);
@@ -517,8 +525,8 @@ __device__ __forceinline__ void c_mom_strip(Geom g, Consts c, const S* ud,
       fy = flux_v<T, UNC>(cy, up ? t4 : t3, up ? t3 : t2, up ? t2 : t1, up ? mt4 : mt3, up ? mt3 : mt2,
                           up ? mt2 : mt1);
     }
-    const T u = a3 + dt * (vdx_ * fy + vdy * (lp0 - lp1)) - dtdx * (ke0 - ke_l - T(pgx));
-    const T v = b3 - dt * (udx * fx + vdx * (lp_r - lp1)) - dtdy * (ke0 - ke1 - T(pgy));
+    const T u = fmadd(-dtdx, ke0 - ke_l - T(pgx), fmadd(dt, fmadd(vdy, lp0 - lp1, vdx_ * fy), a3));
+    const T v = fmadd(-dtdy, ke0 - ke1 - T(pgy), fmadd(-dt, fmadd(vdx, lp_r - lp1, udx * fx), b3));
     const long long o = g.at(x, y, k);
     uc[o] = C(u);
     vc[o] = C(v);
@@ -600,8 +608,8 @@ __device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* ud,
     vn_p = fvd(x, j + 1);
     cu_p = fuL(x, j);
     cv_p = fvL(x, j - 1);
-    const T vorn = f - (sn - s0) * rdy + (shfl_dn(v0, 1) - v0) * rdx;
-    const T dvn = rdx * (sn - shfl_up(sn, 1)) + rdy * (vn - v0);
+    const T vorn = fmadd(shfl_dn(v0, 1) - v0, rdx, fmadd(-(sn - s0), rdy, f));
+    const T dvn = fmadd(rdy, vn - v0, rdx * (sn - shfl_up(sn, 1)));
     s2 = s1; s1 = s0; s0 = sn;
     v3 = v2; v2 = v1; v1 = v0; v0 = vn;
     w4 = w3; w3 = w2; w2 = w1; w1 = vorn;
@@ -614,26 +622,26 @@ __device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* ud,
     edges_v<T, CON>(v3, v2, v1, mv3, mv2, mv1, lv2, rv2);
     // del^2 of the divergence at row j-1 (:688-692), del^4 at row j-2 (:695-702)
     e3 = e2; e2 = e1;
-    e1 = T(-2.) * q1 * rdxy + (shfl_dn(q1, 1) + shfl_up(q1, 1)) * rdx2 + (q0 + q2) * rdy2;
+    e1 = fmadd(q0 + q2, rdy2, fmadd(shfl_dn(q1, 1) + shfl_up(q1, 1), rdx2, T(-2.) * q1 * rdxy));
     dd3 = dd2;
-    dd2 = divdamp * (T(-2.) * e2 * rdxy + (shfl_dn(e2, 1) + shfl_up(e2, 1)) * rdx2 + (e1 + e3) * rdy2);
+    dd2 = divdamp * (fmadd(e1 + e3, rdy2, fmadd(shfl_dn(e2, 1) + shfl_up(e2, 1), rdx2, T(-2.) * e2 * rdxy)));
     // inner x sweep of the vorticity at row j-1 with the layer-nlay Courant numbers (:708-722)
     {
       const T cR = shfl_dn(cu1, 1);
       const T c0 = dtdx * cu1, c1 = dtdx * cR;
-      const T den = T(1) / (T(1) - dtdx * (cR - cu1));
+      const T den = T(1) / fmadd(-dtdx, cR - cu1, T(1));
       const T wl = shfl_up(w1, 1), wr = shfl_dn(w1, 1);  // every lane takes part in the shuffles
       const T f0 = (c0 > T(0)) ? wl : w1;
       const T f1 = (c1 > T(0)) ? w1 : wr;
       t4 = t3; t3 = t2; t2 = t1;
-      t1 = T(.5) * (w1 + den * (w1 - rA * (f1 - f0)));
+      t1 = T(.5) * fmadd(den, fmadd(-rA, f1 - f0, w1), w1);
     }
     mt4 = mt3; mt3 = mt2; mt2 = slope_v(t3, t2, t1);
     lt4 = lt3; rt4 = rt3;
     edges_v<T, CON>(t4, t3, t2, mt4, mt3, mt2, lt3, rt3);
     // Laplacian of the vorticity at row j-2
     lp4 = lp3; lp3 = lp2;
-    lp2 = T(-2.) * w2 * rdxy + (shfl_dn(w2, 1) + shfl_up(w2, 1)) * rdx2 + (w1 + w3) * rdy2;
+    lp2 = fmadd(w1 + w3, rdy2, fmadd(shfl_dn(w2, 1) + shfl_up(w2, 1), rdx2, T(-2.) * w2 * rdxy));
     // kinetic energy of row j-2 with PPM_CONSTRAINED (:639-657) and the
     // layer-nlay B-grid winds (:441-444)
     {
@@ -647,7 +655,7 @@ __device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* ud,
       edges_v<T, CON>(sl, s2, sr, shfl_up(mux, 1), mux, shfl_dn(mux, 1), lux, rux);
       const T fx = flux_con_v(dtdx * ubL, sl, s2, shfl_up(lux, 1), shfl_up(rux, 1), lux, rux);
       ke3 = ke2;
-      ke2 = T(.5) * (kv + ubL * fx);
+      ke2 = T(.5) * fmadd(ubL, fx, kv);
     }
     const int y = j - 3;
     if (y >= oy) {
@@ -656,10 +664,10 @@ __device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* ud,
       T tv;
       {
         const T c0 = dtdx * cv3, c1 = dtdx * cv2;
-        const T den = T(1) / (T(1) - dtdy * (cv2 - cv3));
+        const T den = T(1) / fmadd(-dtdy, cv2 - cv3, T(1));
         const T f0 = (c0 > T(0)) ? w4 : w3;
         const T f1 = (c1 > T(0)) ? w3 : w2;
-        tv = T(.5) * (w3 + den * (w3 - rA * (f1 - f0)));
+        tv = T(.5) * fmadd(den, fmadd(-rA, f1 - f0, w3), w3);
       }
       const T tl = shfl_up(tv, 1), tr = shfl_dn(tv, 1);
       const T mtv = slope_v(tl, tv, tr);
@@ -679,8 +687,8 @@ __device__ __forceinline__ void d_mom_strip(Geom g, Consts c, const S* ud,
           u = uo_r + dt * (svc * fy + vdy * (lp3 - lp4)) - dtdx * (ke_r - ke3 - dd_r + dd3 - T(pgx));
           v = vo_r - dt * (suc * fx + vdx * (lp3 - lp_l)) - dtdy * (ke2 - ke3 - dd2 + dd3 - T(pgy));
         } else {  // the tendency in the sweep type added to the state's type
-          const T du = dt * (svc * fy + vdy * (lp3 - lp4)) - dtdx * (ke_r - ke3 - dd_r + dd3 - T(pgx));
-          const T dv = -dt * (suc * fx + vdx * (lp3 - lp_l)) - dtdy * (ke2 - ke3 - dd2 + dd3 - T(pgy));
+          const T du = fmadd(-dtdx, ke_r - ke3 - dd_r + dd3 - T(pgx), dt * fmadd(vdy, lp3 - lp4, svc * fy));
+          const T dv = fmadd(-dtdy, ke2 - ke3 - dd2 + dd3 - T(pgy), -dt * fmadd(vdx, lp3 - lp_l, suc * fx));
           u = uo_r + S(du);
           v = vo_r + S(dv);
         }
