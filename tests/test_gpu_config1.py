@@ -114,7 +114,7 @@ def test_config1_against_libm_arithmetic(config1_runs):
         dist[name] = (d_libm, d_ulp)
         # at the problem's own sensitivity to a last-bit change of the input
         assert d_libm <= 2.0 * d_ulp + 1e-14, (name, d_libm, d_ulp)
-    # the thickness stays well inside the north-star bound
+    # the thickness stays within the 1e-11 relative max-norm target
     assert dist['dp'][0] <= 1e-11, dist
     print('relative max-norm distance after 100 steps (C-library pow/log, last-bit input change):',
           {k: '%.1e / %.1e' % v for k, v in dist.items()})

@@ -2,9 +2,9 @@
 
 * Total mass: the sweeps' tendencies are applied in flux form to the FP64
   state, so sum(dp) telescopes and changes only by FP64 round-off: within
-  1e-12 (the north star's bound) at steps 50, 100 and 200.
+  1e-12 (the target bound) at steps 50, 100 and 200.
 * Error on a 512 x 512 x 64 jet (dt 30 s, remap every 8), relative L2
-  against the FP64 form: dp, pt and ud within the north star's 1e-5 at
+  against the FP64 form: dp, pt and ud within the target 1e-5 at
   steps 50, 100 and 200; vd (whose norm is the small perturbation of a
   zonal jet, amplified by its instability) within 1e-5 at step 50, and at
   steps 100 and 200 within 2e-5 and 1e-4 (measured 1.1e-5 at step 100),
