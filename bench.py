@@ -231,6 +231,16 @@ def cpu_baseline_lines(steps, warmup):
     return out
 
 
+def headline_config(nx, nlay, steps, world):
+    """The workload of the headline, the same in both arms' lines."""
+    return {'workload': 'jet %dx%dx%d, dx=25 km, dt=30 s, remap every %d steps, FP64 form: %d steps forward '
+                        '(checkpoints every %d) + adjoint of J = sum(theta^2) at the final step' % (
+                            nx, nx, nlay, REMAP_EVERY, steps, ADJ_CKPT),
+            'nx': nx, 'ny': nx, 'nlay': nlay, 'remap_every': REMAP_EVERY, 'checkpoint_every': ADJ_CKPT,
+            'l2': 'inputs larger than L2 (each prognostic field is 552 MB)',
+            'parallelism': 'replicas' if world > 1 else 'single GPU'}
+
+
 def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
@@ -244,9 +254,7 @@ def run_reference(args):
         'steps': steps, 'warmup': warmup, 'ms_per_step': 1000 * (r['forward_s'] + r['tangent_linear_s']) / steps,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
         'data': 'synthetic (seeded jet case)',
-        'config': {'workload': 'jet case, forward + derivative pass of the reference algorithm on the host cores, '
-                               'sample %dx%dx%d per step' % (SAMPLE_N, SAMPLE_N, NLAY),
-                   'nx': SAMPLE_N, 'ny': SAMPLE_N, 'nlay': NLAY, 'remap_every': REMAP_EVERY},
+        'config': headline_config(args.nx, args.nlay, steps, world),
         'cpu_baseline': {'value': v, 'unit': 'cell-steps/s', 'cores': threads, 'kind': 'port',
                          'sample': 'jet %dx%dx%d, %d steps forward + %d steps tangent-linear (%d remaps) after %d '
                                    'warm-up each (1/16 of the 1024^2 domain)' % (
@@ -372,13 +380,7 @@ def run_ours(args):
         'metric': METRIC, 'value': grad['value'], 'unit': 'cell-steps/s', 'n_gpus': world, 'steps': K, 'warmup': W,
         'ms_per_step': grad['ms_per_step'], 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f64', 'data': 'synthetic (seeded jet case, atmdyn.ic.jet_case)',
-        'config': {'workload': 'jet %dx%dx%d, dx=25 km, dt=30 s, remap every %d steps, FP64 form: %d steps forward '
-                               '(checkpoints every %d) + adjoint of J = sum(theta^2) at the final step' % (
-                                   args.nx, args.nx, args.nlay, REMAP_EVERY, K, ADJ_CKPT),
-                   'nx': args.nx, 'ny': args.nx, 'nlay': args.nlay, 'remap_every': REMAP_EVERY,
-                   'checkpoint_every': ADJ_CKPT,
-                   'l2': 'inputs larger than L2 (each prognostic field is 552 MB)',
-                   'parallelism': 'replicas' if world > 1 else 'single GPU'},
+        'config': headline_config(args.nx, args.nlay, K, world),
         'roofline': grad['roofline'],
         'e2e': grad['e2e'],
         'gpu_launches': grad['gpu_launches'],
