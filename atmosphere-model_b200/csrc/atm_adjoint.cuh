@@ -25,6 +25,10 @@ namespace atm {
 
 // threads per block of the adjoint tile kernels
 constexpr int NTA = 256;
+// The adjoint kernels also run the forward's merged region loops
+// (regions() of atm_sweeps.cuh), which stride by NT: a block of any other
+// size would visit some points twice and double their accumulations.
+static_assert(NTA == NT, "adjoint blocks must have the forward kernels' NT threads");
 
 // add to a shared-memory adjoint (p points into shared memory): a reduction
 // in the shared state space, not a generic-address atomic
