@@ -38,14 +38,33 @@ constexpr bool MARCH = true;
 #else
 constexpr bool MARCH = false;
 #endif
-// strip height (output rows a warp walks through) of the marching sweeps;
-// at 1024x1024x64 the momentum sweeps took 2.71 / 2.74 ms at 32 rows, 2.83 /
-// 2.83 at 64 and 2.95 / 2.95 at 128 (the mass sweeps the same at each)
-constexpr int TYS = 32;
+// strip height (output rows a warp walks through) of the marching sweeps,
+// chosen per launch: 128 rows where that grid still fills eight waves of
+// resident blocks, else 32.  Measured on B200 (ms a step, mixed form, rows
+// 32 / 64 / 96 / 128 / 256): 11.46 / 11.10 / 11.03 / 10.96 / 11.25 at
+// 1024x1024x64 and 3.14 / 3.13 / 3.20 / 3.30 / 3.80 at 512x512x64, where 128
+// rows leave 2.2 waves and the tail dominates.
+constexpr int TYS_TALL = 128, TYS_SHORT = 32;
 
 inline dim3 strips(int lo, int hi, const Geom& g, int tys) {
   int w = g.nx - lo + hi, h = g.ny - lo + hi;
   return dim3((w + MOUT * MWARPS - 1) / (MOUT * MWARPS), (h + tys - 1) / tys, g.L);
+}
+
+inline bool tall_strips(int lo, int hi, const Geom& g) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    sms = 148;
+  dim3 b = strips(lo, hi, g, TYS_TALL);
+  return (long long)b.x * b.y * b.z >= 8LL * sms * ATM_MARCH_MINB;
+}
+
+// calls f(std::integral_constant<int, rows>) with the strip height picked above
+template <typename F>
+cudaError_t with_rows(int lo, int hi, const Geom& g, F&& f) {
+  if (tall_strips(lo, hi, g)) f(std::integral_constant<int, TYS_TALL>{});
+  else f(std::integral_constant<int, TYS_SHORT>{});
+  return cudaGetLastError();
 }
 
 inline dim3 tiles(int lo, int hi, const Geom& g, int layers, int ty) {
@@ -77,13 +96,15 @@ cudaError_t mass(const Geom& g, const Consts& c, const void* dp, const void* pt,
                  cudaStream_t s) {
 #ifdef ATM_MARCH_SWEEPS
   if constexpr (MARCH) {
-    if (cgrid)  // state in, C-grid fields out
-      k_mass_m<T, TYS, true, S, C><<<strips(lo, hi, g, TYS), MW * MWARPS, 0, s>>>(
-          g, c, (const S*)dp, (const S*)pt, (const S*)u, (const S*)v, heat, (C*)dpo, (C*)pto, lo, hi, nonfinite);
-    else  // state and C-grid winds in, state out
-      k_mass_m<T, TYS, false, S, C><<<strips(lo, hi, g, TYS), MW * MWARPS, 0, s>>>(
-          g, c, (const S*)dp, (const S*)pt, (const C*)u, (const C*)v, heat, (S*)dpo, (S*)pto, lo, hi, nonfinite);
-    return cudaGetLastError();
+    return with_rows(lo, hi, g, [&](auto rows) {
+      constexpr int R = decltype(rows)::value;
+      if (cgrid)  // state in, C-grid fields out
+        k_mass_m<T, R, true, S, C><<<strips(lo, hi, g, R), MW * MWARPS, 0, s>>>(
+            g, c, (const S*)dp, (const S*)pt, (const S*)u, (const S*)v, heat, (C*)dpo, (C*)pto, lo, hi, nonfinite);
+      else  // state and C-grid winds in, state out
+        k_mass_m<T, R, false, S, C><<<strips(lo, hi, g, R), MW * MWARPS, 0, s>>>(
+            g, c, (const S*)dp, (const S*)pt, (const C*)u, (const C*)v, heat, (S*)dpo, (S*)pto, lo, hi, nonfinite);
+    });
   }
 #endif
   CUtensorMap md, mp, mu, mv;
@@ -136,9 +157,11 @@ cudaError_t c_mom(const Geom& g, const Consts& c, const void* ud, const void* vd
                   void* uc, void* vc, int* timeout, cudaStream_t s) {
 #ifdef ATM_MARCH_SWEEPS
   if constexpr (MARCH) {
-    k_c_mom_m<T, TYS, S, C><<<strips(0, 0, g, TYS), MW * MWARPS, 0, s>>>(g, c, (const S*)ud, (const S*)vd, pkap, gz,
-                                                                          (C*)uc, (C*)vc);
-    return cudaGetLastError();
+    return with_rows(0, 0, g, [&](auto rows) {
+      constexpr int R = decltype(rows)::value;
+      k_c_mom_m<T, R, S, C><<<strips(0, 0, g, R), MW * MWARPS, 0, s>>>(g, c, (const S*)ud, (const S*)vd, pkap, gz,
+                                                                        (C*)uc, (C*)vc);
+    });
   }
 #endif
   using Lay = CMomL<T, TX, TY_CMOM, S>;
@@ -159,9 +182,11 @@ cudaError_t d_mom(const Geom& g, const Consts& c, const void* ud, const void* vd
                   cudaStream_t s) {
 #ifdef ATM_MARCH_SWEEPS
   if constexpr (MARCH) {
-    k_d_mom_m<T, TYS, S, C><<<strips(0, 0, g, TYS), MW * MWARPS, 0, s>>>(
-        g, c, (const S*)ud, (const S*)vd, (const C*)uc, (const C*)vc, pkapb, gzb, (S*)udo, (S*)vdo, nonfinite);
-    return cudaGetLastError();
+    return with_rows(0, 0, g, [&](auto rows) {
+      constexpr int R = decltype(rows)::value;
+      k_d_mom_m<T, R, S, C><<<strips(0, 0, g, R), MW * MWARPS, 0, s>>>(
+          g, c, (const S*)ud, (const S*)vd, (const C*)uc, (const C*)vc, pkapb, gzb, (S*)udo, (S*)vdo, nonfinite);
+    });
   }
 #endif
   using Lay = DMomL<T, TX, TY_DMOM, S, C>;
