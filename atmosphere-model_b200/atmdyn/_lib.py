@@ -20,7 +20,7 @@ ATM_DPC, ATM_PTC, ATM_UC, ATM_VC = range(8, 12)
 ATM_TS = 12
 ATM_FP64, ATM_MIXED = 0, 1
 STATUS = {0: 'ATM_OK', 1: 'ATM_ERR_ARG', 2: 'ATM_ERR_CUDA', 3: 'ATM_ERR_STATE',
-          4: 'ATM_ERR_NOMEM', 5: 'ATM_ERR_UNSUPPORTED', 6: 'ATM_ERR_TOO_LARGE'}
+          4: 'ATM_ERR_NOMEM', 5: 'ATM_ERR_UNSUPPORTED', 6: 'ATM_ERR_TOO_LARGE', 7: 'ATM_ERR_RANGE'}
 
 # every entry point of include/atmdyn.h
 EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_step', 'atm_cgrid_halo',
@@ -38,7 +38,8 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_ensemble_create', 'atm_ensemble_set_strips', 'atm_ensemble_set_stream', 'atm_ensemble_prepare',
            'atm_ensemble_run', 'atm_ensemble_status', 'atm_ensemble_blocks', 'atm_ensemble_destroy',
            'atm_ensemble_barrier_check', 'atm_ensemble_profile', 'atm_ensemble_stage_ms',
-           'atm_ensemble_set_schedule')
+           'atm_ensemble_set_schedule', 'atm_set_gas_optics', 'atm_set_cell_coordinates',
+           'atm_radiative_heating', 'atm_radiation_halo')
 ATM_ADJ_IN, ATM_ADJ_OUT = 0, 1
 
 # the entry points every build must export
@@ -47,6 +48,25 @@ CORE = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_step'
         'atm_sync', 'atm_destroy', 'atm_last_error', 'atm_set_stream')
 
 _lib = None
+
+
+class GasOpticsC(ctypes.Structure):
+    """atm_gas_optics of include/atmdyn.h."""
+    _fields_ = [('n_g', ctypes.c_int), ('n_p', ctypes.c_int), ('n_t', ctypes.c_int), ('n_planck', ctypes.c_int)] + \
+        [(n, ctypes.POINTER(ctypes.c_double)) for n in
+         ('pressures', 'temperatures', 'sw_absorption', 'sw_scattering', 'lw_absorption', 'planck_temperatures',
+          'planck', 'irradiance_fraction')]
+
+
+def gas_optics_struct(go):
+    """An atm_gas_optics over the arrays of a :class:`atmdyn.gas_optics.GasOptics`
+    (which must outlive the struct)."""
+    P = ctypes.POINTER(ctypes.c_double)
+    n_p, n_t = go.temperatures.shape
+    return GasOpticsC(go.n_g, n_p, n_t, go.planck_temperatures.shape[0],
+                      *[getattr(go, n).ctypes.data_as(P) for n in
+                        ('pressures', 'temperatures', 'sw_absorption', 'sw_scattering', 'lw_absorption',
+                         'planck_temperatures', 'planck', 'irradiance_fraction')])
 
 
 class AtmError(RuntimeError):
@@ -136,6 +156,10 @@ def load():
         'atm_ensemble_stage_ms': ([vp, ctypes.POINTER(ctypes.c_double), i], None),
         'atm_ensemble_destroy': ([vp], None),
         'atm_ensemble_barrier_check': ([ctypes.c_longlong, ctypes.POINTER(i)], None),
+        'atm_set_gas_optics': ([vp, ctypes.POINTER(GasOpticsC)], None),
+        'atm_set_cell_coordinates': ([vp, P, P], None),
+        'atm_radiative_heating': ([vp, d, d, d, d], None),
+        'atm_radiation_halo': ([vp], None),
     }
     for f, (args, res) in optional.items():
         if hasattr(lib, f):

@@ -77,6 +77,8 @@ class Dycore:
         return self.nlay + 1 if field in (ATM_GZ, ATM_PLEV, ATM_PKAP, ATM_NET_FLUX) else self.nlay
 
     def upload(self, field, a):
+        if isinstance(field, str):
+            field = FIELDS[field]
         a = np.ascontiguousarray(a, dtype=np.float64)
         check(self.lib.atm_upload(self.ctx, field, _ptr(a)), self.ctx, 'atm_upload')
 
@@ -141,6 +143,36 @@ class Dycore:
 
     def physics_halo(self):
         check(self.lib.atm_physics_halo(self.ctx), self.ctx, 'atm_physics_halo')
+
+    # radiation (src/mod_radiation.f90)
+    def set_radiation(self, go, xc=None, yc=None):
+        """Upload the gas-optics tables (:class:`atmdyn.gas_optics.GasOptics`)
+        and the cell-centre axes the solar irradiance depends on (default:
+        the state's, see :func:`atmdyn.ic.cell_axes`)."""
+        from .ic import cell_axes
+        self._go = go.validate()
+        check(self.lib.atm_set_gas_optics(self.ctx, ctypes.byref(_lib.gas_optics_struct(self._go))), self.ctx,
+              'atm_set_gas_optics')
+        if xc is None or yc is None:
+            xc, yc = cell_axes(self.st)
+        xc = np.ascontiguousarray(xc, dtype=np.float64)
+        yc = np.ascontiguousarray(yc, dtype=np.float64)
+        assert xc.shape == (self.nx,) and yc.shape == (self.ny,)
+        check(self.lib.atm_set_cell_coordinates(self.ctx, _ptr(xc), _ptr(yc)), self.ctx, 'atm_set_cell_coordinates')
+
+    def radiative_heating(self, time=0.0, solar_zenith_angle=None, surface_albedo=None, surface_emissivity=None):
+        """calculate_radiative_heating (src/mod_radiation.f90:41-156): the
+        net flux of the current state; the parameters default to the
+        reference's fixed values.  Raises AtmError (ATM_ERR_RANGE) where the
+        reference stops on a lookup outside its tables."""
+        from . import gas_optics as g
+        sza = g.SOLAR_ZENITH_ANGLE if solar_zenith_angle is None else solar_zenith_angle
+        alb = g.SURFACE_ALBEDO if surface_albedo is None else surface_albedo
+        emi = g.SURFACE_EMISSIVITY if surface_emissivity is None else surface_emissivity
+        check(self.lib.atm_radiative_heating(self.ctx, time, sza, alb, emi), self.ctx, 'atm_radiative_heating')
+
+    def radiation_halo(self):
+        check(self.lib.atm_radiation_halo(self.ctx), self.ctx, 'atm_radiation_halo')
 
     def mass(self):
         m = ctypes.c_double(0.)

@@ -29,6 +29,12 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_PATH = os.path.join(HERE, '_tables', 'ecckd_climate16.npz')
 
+# the reference's fixed radiation parameters (src/mod_radiation.f90:107-109;
+# .3 and .99 are default-real literals)
+SOLAR_ZENITH_ANGLE = 0.0
+SURFACE_ALBEDO = float(np.float32(.3))
+SURFACE_EMISSIVITY = float(np.float32(.99))
+
 
 @dataclass
 class GasOptics:

@@ -59,10 +59,26 @@ class InitialState:
     name: str = ''
     extra: dict = field(default_factory=dict)
     ts: np.ndarray | None = None  # (ny, nx) surface temperature (the physics' only 2-D prognostic)
+    xc: np.ndarray | None = None  # (nx,) cell-centre x axis of the initial file (default: see cell_axes)
+    yc: np.ndarray | None = None  # (ny,)
 
     @property
     def cells(self) -> int:
         return self.nx * self.ny * self.nlay
+
+
+def cell_axes(st):
+    """The cell-centre axes (xc, yc): the state's own (read from its initial
+    file), else the reference generator's, centred on the domain
+    (scripts/ic_generator.py:20-22: linspace((dx-Lx)/2, (Lx-dx)/2, nx))."""
+    xc, yc = getattr(st, 'xc', None), getattr(st, 'yc', None)
+    if xc is None:
+        lx = st.nx * st.dx
+        xc = np.linspace((st.dx - lx) / 2, (lx - st.dx) / 2, st.nx)
+    if yc is None:
+        ly = st.ny * st.dy
+        yc = np.linspace((st.dy - ly) / 2, (ly - st.dy) / 2, st.ny)
+    return np.asarray(xc, dtype=np.float64), np.asarray(yc, dtype=np.float64)
 
 
 def sigma_coordinate(nlay: int, ptop: float = 1.0e4):

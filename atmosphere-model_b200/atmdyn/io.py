@@ -29,7 +29,7 @@ from dataclasses import dataclass, field
 import numpy as np
 from scipy.io import netcdf_file
 
-from .ic import InitialState
+from .ic import InitialState, cell_axes
 from .model import TimeControl, NEVER
 
 
@@ -227,6 +227,7 @@ def read_initial(path: str, config: Config | None = None) -> InitialState:
     st = InitialState(nx, ny, nlay, float(dx), float(dy), ak, bk, f['dp'], f['pt'], f['u'], f['v'], gzs)
     st.t_initial = t0
     st.ts = ts
+    st.xc, st.yc = xc, yc  # the radiation's cell radius (src/mod_input.f90:233-243)
     if config is not None:
         st.gravity, st.coriolis = config.gravity, config.coriolis
         st.divdamp, st.vortdamp = config.divdamp, config.vortdamp
@@ -243,8 +244,8 @@ def write_initial(path: str, st: InitialState, ts=None, t0: float = 0.0):
         for n, size in (('xc', st.nx), ('yc', st.ny), ('xf', st.nx), ('yf', st.ny), ('lay', st.nlay),
                         ('lev', st.nlay + 1)):
             nc.createDimension(n, size)
-        axes = {'xc': (np.arange(st.nx) + .5) * st.dx, 'xf': np.arange(st.nx) * st.dx,
-                'yc': (np.arange(st.ny) + .5) * st.dy, 'yf': np.arange(st.ny) * st.dy,
+        xc, yc = cell_axes(st)  # the generator's axes (scripts/ic_generator.py:20-24)
+        axes = {'xc': xc, 'xf': xc - st.dx / 2, 'yc': yc, 'yf': yc - st.dy / 2,
                 'lay': np.arange(1, st.nlay + 1), 'lev': np.arange(1, st.nlay + 2)}
         for n, v in axes.items():
             nc.createVariable(n, 'f8', (n,))[:] = v

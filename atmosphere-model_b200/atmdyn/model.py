@@ -1,12 +1,13 @@
 """Host-side time loop of the dynamical core, mirroring the reference's
 ``run_model`` (src/mod_model.f90:91-199) and ``calculate_dt``
-(src/mod_model.f90:201-237) with radiation switched off.
+(src/mod_model.f90:201-237).
 
 A *stepper* is anything with the reference's dycore entry points:
 ``cgrid_step(dt_half)``, ``cgrid_halo()``, ``dgrid_step(dt)``, ``remap()``,
 ``dgrid_halo()`` and ``check_stability() -> bool``, and, for a run with
 physics, ``physics_tendencies()``, ``apply_physics(dt)`` and
-``physics_halo()``.  The CUDA library (:class:`atmdyn.Dycore`) is one; the
+``physics_halo()``, and for a run with radiation ``radiative_heating(time)``
+and ``radiation_halo()``.  The CUDA library (:class:`atmdyn.Dycore`) is one; the
 CPU oracle used by the tests is another.
 """
 from __future__ import annotations
@@ -89,15 +90,17 @@ class RunResult:
 
 def run_model(stepper, tc: TimeControl, max_steps: int | None = None,
               on_step=None, accumulate=None, write=None, physics: bool = False,
-              before_remap=None) -> RunResult:
-    """``run_model`` (mod_model.f90:112-193) without radiation: each step is
-    [physics tendencies when due], C-grid half step, halo, D-grid step,
+              before_remap=None, radiation: bool = False) -> RunResult:
+    """``run_model`` (mod_model.f90:112-193): each step is [radiative
+    heating and its halo when due], [physics tendencies when due], C-grid
+    half step, halo, D-grid step,
     [apply the physics tendencies], remap if due, halo, [physics halo],
     stability check, then ``accumulate(dt)`` (accumulate_output) and, when
     the schedule says so, ``write(time_stamp)`` (write_output, stamped
     .5 (previous_write_time + time) as the reference does).  The bracketed
-    physics calls run when ``physics`` is true; the net flux (radiation)
-    is whatever the caller set (zero by default).  ``before_remap(n)``, when
+    physics calls run when ``physics`` is true, the radiation when
+    ``radiation`` is true (at the first step and every dt_radiation);
+    without it the net flux is whatever the caller set (zero by default).  ``before_remap(n)``, when
     given, runs just before the remap of step n (the tests arm the remap's
     pair trace there)."""
     sch = Schedule(tc)
@@ -106,7 +109,11 @@ def run_model(stepper, tc: TimeControl, max_steps: int | None = None,
     stable = True
     remaps = []
     while time < sch.t_final:
-        sch.calculate_radiation_this_step = False
+        if sch.calculate_radiation_this_step:        # mod_model.f90:117-127
+            if radiation:
+                stepper.radiative_heating(time)
+                stepper.radiation_halo()
+            sch.calculate_radiation_this_step = False
         n += 1
         dt = sch.calculate_dt(time)
         if sch.calculate_physics_this_step:

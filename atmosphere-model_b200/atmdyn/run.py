@@ -1,7 +1,7 @@
 """Run the dynamical core from the reference's own files.
 
     python -m atmdyn.run [config.nml] [--precision fp64|mixed] [--output output/output.nc]
-                         [--max-steps N] [--output-dtype f4|f8]
+                         [--max-steps N] [--output-dtype f4|f8] [--gas-optics tables.npz | --no-radiation]
 
 Reads the namelist (src/mod_config.f90:27-99) and the initial-conditions
 file it names (src/mod_input.f90:21-228), steps the CUDA library through
@@ -10,8 +10,12 @@ steps, remap when due, halo fills, stability check), accumulates the
 output means on the device (src/mod_output.f90:94-142) and writes them to
 output.nc when an output interval ends, and writes the restart file at the
 end when the namelist asks for it.  The physics (src/mod_physics.f90: dry
-convective adjustment, surface heating) runs on the device when due;
-radiation is not run, so the net flux is zero and ts keeps its value.
+convective adjustment, surface heating) and the radiation
+(src/mod_radiation.f90: two-stream shortwave and longwave over 16 g-points)
+run on the device when due.  The radiation needs the gas-optics tables
+(:mod:`atmdyn.gas_optics`): ``--gas-optics`` names an ``.npz``, else the
+package's default tables are used; without tables (or with
+``--no-radiation``) the net flux stays zero.
 """
 from __future__ import annotations
 
@@ -19,6 +23,7 @@ import argparse
 import json
 import os
 
+from . import gas_optics
 from .dycore import Dycore
 from .io import read_config, read_initial, OutputWriter, write_restart
 from .model import run_model, TimeControl
@@ -31,6 +36,8 @@ def main(argv=None):
     ap.add_argument('--output', default='output/output.nc')
     ap.add_argument('--output-dtype', default='f4', choices=['f4', 'f8'])
     ap.add_argument('--max-steps', type=int, default=None)
+    ap.add_argument('--gas-optics', default=None, help='gas-optics tables (.npz, atmdyn.gas_optics.save)')
+    ap.add_argument('--no-radiation', action='store_true')
     args = ap.parse_args(argv)
     cfg = read_config(args.config)
     base = os.path.dirname(os.path.abspath(args.config))
@@ -41,6 +48,11 @@ def main(argv=None):
                      dt_radiation=t.dt_radiation, dt_physics=t.dt_physics, dt_remap=t.dt_remap,
                      t_initial=st.t_initial)
     dyn = Dycore(st, args.precision)
+    go = None
+    if not args.no_radiation:
+        go = gas_optics.load(args.gas_optics) if args.gas_optics else gas_optics.load_default()
+    if go is not None:
+        dyn.set_radiation(go)
     dyn.output_enable()
     os.makedirs(os.path.dirname(os.path.abspath(args.output)), exist_ok=True)
     writer = OutputWriter(args.output, st, dtype=args.output_dtype)
@@ -55,7 +67,7 @@ def main(argv=None):
         records.append(stamp)
 
     res = run_model(dyn, tc, max_steps=args.max_steps, accumulate=dyn.accumulate_output, write=write,
-                    physics=True)
+                    physics=True, radiation=go is not None)
     writer.close()
     restart = None
     if cfg.save_restart_file and res.stable:
@@ -65,7 +77,8 @@ def main(argv=None):
         ts = dyn.get('ts')[0] if st.ts is not None else None
         write_restart(restart, st, dyn.state(), res.time, ts=ts, dtype=args.output_dtype)
     summary = {'steps': res.steps, 'time': res.time, 'stable': res.stable, 'remap_steps': res.remap_steps,
-               'output_records': records, 'output': args.output, 'restart': restart}
+               'output_records': records, 'output': args.output, 'restart': restart,
+               'radiation': go is not None}
     print(json.dumps(summary))
     dyn.close()
     return summary

@@ -5,6 +5,7 @@
 // point enqueues kernels on the context's stream.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -14,6 +15,7 @@
 #include "atm_ensemble.cuh"
 #include "atm_ops.h"
 #include "atm_physics.h"
+#include "atm_radiation.h"
 
 using atm::Geom;
 using atm::H;
@@ -129,6 +131,12 @@ struct atm_ctx {
   double* ts = nullptr;
   double *ph_pt = nullptr, *ph_u = nullptr, *ph_v = nullptr, *ph_ts = nullptr;
   bool phys_ready = false;
+  // radiation (src/mod_radiation.f90): the gas-optics tables in one device
+  // block (pointers in rad), the distance of each cell centre from the
+  // origin (ny, nx) (src/mod_input.f90:233-243)
+  double* rad_block = nullptr;
+  atm::RadTables rad{};
+  double* radius = nullptr;
   std::string err;
 };
 
@@ -188,7 +196,7 @@ void free_all(atm_ctx* c) {
   double* pl[] = {c->lam_pk, c->lam_gz, c->lam_pkb, c->lam_gzb, c->lam_ur, c->lam_vr};
   for (double* p : pl) cudaFree(p);
   for (double* p : c->acc) cudaFree(p);
-  double* ph[] = {c->ts, c->ph_pt, c->ph_u, c->ph_v, c->ph_ts};
+  double* ph[] = {c->ts, c->ph_pt, c->ph_u, c->ph_v, c->ph_ts, c->rad_block, c->radius};
   for (double* p : ph) cudaFree(p);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_mass) cudaFreeHost(c->h_mass);
@@ -213,11 +221,12 @@ const char* const STAGE_NAMES[] = {"c_mass",  "c_column", "c_mom",        "c_hal
                                    "remap_winds", "remap_energy", "d_halo", "heating", "check",
                                    "adj_forward", "adj_remap", "adj_d_mom_ke", "adj_d_column", "adj_d_mass_x",
                                    "adj_c_column", "adj_c_mom", "adj_c_mass", "adj_halo",
-                                   "phys_tend", "phys_apply", "phys_halo", "adj_d_mom_vf", "adj_d_mass_y"};
-constexpr int NSTAGE = 29;
+                                   "phys_tend", "phys_apply", "phys_halo", "adj_d_mom_vf", "adj_d_mass_y",
+                                   "radiation", "radiation_halo"};
+constexpr int NSTAGE = 31;
 enum { S_CMASS, S_CCOL, S_CMOM, S_CHALO, S_DRING, S_DMASS, S_DCOL, S_DCORN, S_DMOM, S_RRING, S_RWIND, S_RENER,
        S_DHALO, S_HEAT, S_CHECK, S_AFWD, S_ARMP, S_ADMOM, S_ADCOL, S_ADMASS, S_ACCOL, S_ACMOM, S_ACMASS, S_AHALO,
-       S_PHYS_TEND, S_PHYS_APPLY, S_PHYS_HALO, S_ADMOM_VF, S_ADMASS_Y };
+       S_PHYS_TEND, S_PHYS_APPLY, S_PHYS_HALO, S_ADMOM_VF, S_ADMASS_Y, S_RAD, S_RAD_HALO };
 
 // Brackets one stage (one kernel launch unless noted) with CUDA events on
 // the context's stream when profiling is on, and counts the launch.
@@ -466,12 +475,8 @@ int atm_download(atm_ctx* ctx, int field, double* host) {
   return ATM_OK;
 }
 
-int atm_set_net_flux(atm_ctx* ctx, const double* host) {
-  if (!ctx) return ATM_ERR_ARG;
-  if (!host) {
-    ctx->heating = false;
-    return ATM_OK;
-  }
+// net_flux and the heating term it feeds, allocated (zero) on first use
+static int ensure_net_flux(atm_ctx* ctx) {
   const size_t lev = level_elems(ctx) * (ctx->L + 1) * 8;
   if (!ctx->nf) {
     CK(cudaMalloc((void**)&ctx->nf, lev));
@@ -481,6 +486,17 @@ int atm_set_net_flux(atm_ctx* ctx, const double* host) {
     CK(cudaMalloc((void**)&ctx->heat, lev));
     CK(cudaMemset(ctx->heat, 0, lev));
   }
+  return ATM_OK;
+}
+
+int atm_set_net_flux(atm_ctx* ctx, const double* host) {
+  if (!ctx) return ATM_ERR_ARG;
+  if (!host) {
+    ctx->heating = false;
+    return ATM_OK;
+  }
+  int r = ensure_net_flux(ctx);
+  if (r) return r;
   CK(h2d_pitched(ctx, ctx->nf, host, ctx->L + 1));
   ctx->heating = true;
   return ATM_OK;
@@ -1340,6 +1356,120 @@ int atm_physics_halo(atm_ctx* ctx) {
   void* ts1[1] = {ctx->ts};
   Stage t(ctx, S_PHYS_HALO);
   CK(atm::ops_fp64.ring(ctx->geo, ts1, nullptr, 1, 1, false, ctx->stream));
+  return ATM_OK;
+}
+
+int atm_set_gas_optics(atm_ctx* ctx, const atm_gas_optics* t) {
+  if (!ctx || !t) return ATM_ERR_ARG;
+  if (t->n_g < 1 || t->n_p < 2 || t->n_t < 2 || t->n_planck < 2 || t->n_g > 4096 || t->n_p > 4096 ||
+      t->n_t > 4096 || t->n_planck > 65536)
+    return fail(ctx, ATM_ERR_ARG, "atm_set_gas_optics: table sizes out of range");
+  const size_t ng = t->n_g, np = t->n_p, nt = t->n_t, npl = t->n_planck;
+  const double* src[8] = {t->pressures,    t->temperatures, t->sw_absorption, t->sw_scattering,
+                          t->lw_absorption, t->planck_temperatures, t->planck, t->irradiance_fraction};
+  const size_t len[8] = {np, np * nt, ng * np * nt, ng, ng * np * nt, npl, ng * npl, ng};
+  for (const double* p : src)
+    if (!p) return fail(ctx, ATM_ERR_ARG, "atm_set_gas_optics: null table");
+  // the lookups search these axes (mod_gas_optics.f90:4556-4609)
+  auto ascending = [](const double* x, size_t n) {
+    for (size_t q = 1; q < n; ++q)
+      if (!(x[q] > x[q - 1])) return false;
+    return true;
+  };
+  bool ok = ascending(t->pressures, np) && ascending(t->planck_temperatures, npl);
+  for (size_t p = 0; p < np && ok; ++p) ok = ascending(t->temperatures + p * nt, nt);
+  if (!ok) return fail(ctx, ATM_ERR_ARG, "atm_set_gas_optics: lookup axes must be strictly ascending");
+  size_t total = 0;
+  for (size_t n : len) total += n;
+  std::vector<double> h(total);
+  size_t off[8];
+  for (int q = 0, at = 0; q < 8; at += (int)len[q], ++q) {
+    off[q] = (size_t)at;
+    std::memcpy(h.data() + at, src[q], len[q] * 8);
+  }
+  if (ctx->rad_block) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->rad_block);
+    ctx->rad_block = nullptr;
+  }
+  if (cudaMalloc((void**)&ctx->rad_block, total * 8) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->rad_block = nullptr;
+    return fail(ctx, ATM_ERR_NOMEM, "gas-optics tables");
+  }
+  CK(cudaMemcpyAsync(ctx->rad_block, h.data(), total * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  double* b = ctx->rad_block;
+  ctx->rad = atm::RadTables{(int)ng,     (int)np,       (int)nt,       (int)npl,      b + off[0], b + off[1],
+                            b + off[2],  b + off[3],    b + off[4],    b + off[5],    b + off[6], b + off[7]};
+  return ATM_OK;
+}
+
+int atm_set_cell_coordinates(atm_ctx* ctx, const double* xc, const double* yc) {
+  if (!ctx || !xc || !yc) return ATM_ERR_ARG;
+  const int nx = ctx->nx, ny = ctx->ny;
+  // radius = sqrt(xc**2 + yc**2), summed as init_prognostic_fields does (src/mod_input.f90:233-243)
+  std::vector<double> r((size_t)nx * ny);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      double v = xc[i] * xc[i];
+      v = v + yc[j] * yc[j];
+      r[(size_t)j * nx + i] = std::sqrt(v);
+    }
+  if (!ctx->radius && cudaMalloc((void**)&ctx->radius, r.size() * 8) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->radius = nullptr;
+    return fail(ctx, ATM_ERR_NOMEM, "cell radius");
+  }
+  CK(cudaMemcpyAsync(ctx->radius, r.data(), r.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATM_OK;
+}
+
+int atm_radiative_heating(atm_ctx* ctx, double time, double solar_zenith_angle, double surface_albedo,
+                          double surface_emissivity) {
+  (void)time;  // solar_irradiance does not depend on it (src/mod_solar.f90:26-35)
+  int r = require_init(ctx);
+  if (r) return r;
+  if (ctx->ops->elem != 8) return fail(ctx, ATM_ERR_UNSUPPORTED, "the radiation needs an FP64 prognostic state");
+  if (!ctx->rad_block) return fail(ctx, ATM_ERR_STATE, "atm_set_gas_optics has not been called");
+  if (!ctx->radius) return fail(ctx, ATM_ERR_STATE, "atm_set_cell_coordinates has not been called");
+  if ((r = ensure_net_flux(ctx))) return r;
+  void* const* s = ctx->st[ctx->cur];
+  CK(cudaMemsetAsync(&ctx->status->radiation_range, 0, sizeof(int), ctx->stream));
+  atm::RadArgs a{ctx->cst.ptop,
+                 ctx->cst.pk_top,
+                 ctx->cst.gravity,
+                 std::cos(solar_zenith_angle),
+                 surface_albedo,
+                 surface_emissivity,
+                 (const double*)s[F_DP],
+                 (const double*)s[F_PT],
+                 ctx->ts,
+                 ctx->radius,
+                 ctx->nf,
+                 &ctx->status->radiation_range};
+  {
+    Stage t(ctx, S_RAD);
+    CK(atm::radiative_heating(ctx->geo, ctx->rad, a, ctx->stream));
+  }
+  ctx->heating = true;
+  CK(cudaMemcpyAsync(ctx->h_status, ctx->status, sizeof(atm::Status), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->h_status->radiation_range)
+    return fail(ctx, ATM_ERR_RANGE,
+                "radiation: a layer pressure or temperature is outside the gas-optics tables "
+                "(the reference stops there: src/mod_gas_optics.f90:4562-4566,4589-4594)");
+  return ATM_OK;
+}
+
+int atm_radiation_halo(atm_ctx* ctx) {
+  int r = require_init(ctx);
+  if (r) return r;
+  if (!ctx->nf) return fail(ctx, ATM_ERR_STATE, "no net flux to exchange");
+  void* nf1[1] = {ctx->nf};
+  Stage t(ctx, S_RAD_HALO);
+  CK(atm::ops_fp64.ring(ctx->geo, nf1, nullptr, 1, ctx->L + 1, false, ctx->stream));
   return ATM_OK;
 }
 

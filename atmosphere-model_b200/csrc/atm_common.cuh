@@ -61,6 +61,7 @@ struct Status {
   int nonfinite_check;  // standalone stability check
   int fallback_pairs;   // columns whose remap used the all-pairs search
   int tma_timeout;      // a TMA tile load did not complete within its wait limit
+  int radiation_range;  // a radiation table lookup left its table
 };
 
 // Hybrid coordinate of the vertical remap (src/mod_remap.f90:57-71).

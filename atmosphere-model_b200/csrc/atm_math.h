@@ -166,6 +166,15 @@ ATM_HD double atm_log(double x) {
   return hi;
 }
 
+// exp(x): the radiation's transmittances (src/mod_radiation.f90:214,216,
+// 300); 0 below the smallest subnormal, +inf above the largest double
+ATM_HD double atm_exp(double x) {
+  if (x != x) return x;
+  if (x > 709.78) return HUGE_VAL;
+  if (x < -745.0) return 0.0;
+  return atm_math::exp_dd(x, 0.0);
+}
+
 // x**y for x > 0 (the only case the dynamical core needs); x == 0 gives
 // 0 (y > 0) or +inf (y < 0), negative x gives NaN
 ATM_HD double atm_pow(double x, double y) {

@@ -26,15 +26,15 @@ struct RadTables {
 struct RadArgs {
   double ptop, pk_top;           // plev(nlay+1) and pkap(nlay+1) (mod_input.f90:229-231)
   double gravity;
-  double mu0;                    // cos(solar_zenith_angle) (mod_radiation.f90:176)
-  double albedo, emissivity;     // surface_albedo, surface_emissivity (:109-110)
+  double mu0;                    // cos(solar_zenith_angle) (mod_radiation.f90:174)
+  double albedo, emissivity;     // surface_albedo, surface_emissivity (:108-109)
   const double *dp, *pt, *ts;    // state fields (pitched, with halo)
   const double* radius;          // [ny][nx], distance of each cell centre from the origin
   double* nf;                    // net_flux (pitched, nlay + 1 levels)
   int* range_error;              // set when a lookup leaves its table (the reference stops there)
 };
 
-// calculate_radiative_heating (src/mod_radiation.f90:41-154) on the interior
+// calculate_radiative_heating (src/mod_radiation.f90:41-156) on the interior
 cudaError_t radiative_heating(const Geom& g, const RadTables& t, const RadArgs& a, cudaStream_t s);
 
 }  // namespace atm

@@ -68,7 +68,8 @@ enum {
   ATM_ERR_STATE = 3,     /* call out of order (e.g. a step before atm_init) */
   ATM_ERR_NOMEM = 4,     /* device allocation failed */
   ATM_ERR_UNSUPPORTED = 5,
-  ATM_ERR_TOO_LARGE = 6  /* atm_remap_noalloc: the domain needs more than its fixed scratch */
+  ATM_ERR_TOO_LARGE = 6, /* atm_remap_noalloc: the domain needs more than its fixed scratch */
+  ATM_ERR_RANGE = 7      /* atm_radiative_heating: a lookup outside the gas-optics tables */
 };
 
 /* flags for atm_create */
@@ -344,6 +345,55 @@ int atm_state_load(atm_ctx* ctx, const void* dev);
 int atm_physics_tendencies(atm_ctx* ctx);
 int atm_apply_physics(atm_ctx* ctx, double dt);
 int atm_physics_halo(atm_ctx* ctx);
+
+/* ---- radiation (src/mod_radiation.f90, src/mod_gas_optics.f90,
+   src/mod_solar.f90), FP64 in both forms ----
+   The correlated-k tables, which the reference compiles in as parameter
+   arrays, are an input: arrays in the reference's index order flattened
+   from the last Fortran index (temperatures[p][t] is temperatures(t, p) of
+   mod_gas_optics.f90:50-132, sw_absorption[g][p][t] is
+   shortwave_absorption_lut(t, p, g) of :143-1841, lw_absorption likewise of
+   :1870-3568, planck[g][t] is planckian_lut(t, g) of :3623-4549;
+   sw_scattering is rayleigh_scattering_lut (:1852-1857), irradiance_fraction
+   that of mod_solar.f90:16-23).  atm_set_gas_optics copies them to the
+   device (strictly ascending axes required). */
+typedef struct {
+  int n_g, n_p, n_t, n_planck;        /* 16, 53, 6, 231 in the reference */
+  const double* pressures;            /* [n_p], Pa */
+  const double* temperatures;         /* [n_p][n_t], K */
+  const double* sw_absorption;        /* [n_g][n_p][n_t], m2/kg */
+  const double* sw_scattering;        /* [n_g], m2/kg */
+  const double* lw_absorption;        /* [n_g][n_p][n_t], m2/kg */
+  const double* planck_temperatures;  /* [n_planck], K */
+  const double* planck;               /* [n_g][n_planck] */
+  const double* irradiance_fraction;  /* [n_g] */
+} atm_gas_optics;
+
+/* the reference's fixed radiation parameters (mod_radiation.f90:107-109;
+   .3 and .99 are default-real literals) */
+#define ATM_SOLAR_ZENITH_ANGLE 0.0
+#define ATM_SURFACE_ALBEDO ((double)0.3f)
+#define ATM_SURFACE_EMISSIVITY ((double)0.99f)
+
+int atm_set_gas_optics(atm_ctx* ctx, const atm_gas_optics* tables);
+/* the cell-centre axes xc[nx], yc[ny] of the initial file; the solar
+   irradiance of a column depends on radius = sqrt(xc^2 + yc^2)
+   (src/mod_input.f90:233-243, src/mod_solar.f90:26-35) */
+int atm_set_cell_coordinates(atm_ctx* ctx, const double* xc, const double* yc);
+/* calculate_radiative_heating(time) (src/mod_radiation.f90:41-156): net_flux
+   on the interior from the current dp, pt and ts: layer pressures and
+   temperatures, then per g-point a shortwave and a longwave two-stream
+   solution closed by the adding method.  The heating term and the surface
+   heating use it from then on (as after atm_set_net_flux).  Called where
+   run_model calls it: at the start of a step when radiation is due
+   (src/mod_model.f90:117-127).  Synchronises the stream; ATM_ERR_RANGE when
+   a layer pressure or temperature lies outside the tables (where the
+   reference stops).
+   atm_radiation_halo: radiation_halo_exchange (:400-404), the periodic halo
+   of net_flux. */
+int atm_radiative_heating(atm_ctx* ctx, double time, double solar_zenith_angle, double surface_albedo,
+                          double surface_emissivity);
+int atm_radiation_halo(atm_ctx* ctx);
 
 /* ---- output accumulation on the device (accumulate_output / write_output,
    src/mod_output.f90:94-176) ----

@@ -105,6 +105,22 @@ void tlm_set_threads(orc_tlm* s, int nthreads);
 void orc_pow_array(const double* x, double y, double* out, int n);
 void orc_log_array(const double* x, double* out, int n);
 
+/* radiation (src/mod_radiation.f90:41-398, src/mod_gas_optics.f90,
+   src/mod_solar.f90), atm_oracle_radiation.cpp.  Tables in the layout of
+   include/atmdyn.h's atm_gas_optics; fields interior-only, i fastest:
+   dp, pt (nlay, ny, nx), ts (ny, nx), net_flux out (nlay + 1, ny, nx).
+   Returns 0, 1 when a lookup leaves a table (where the reference stops),
+   2 on bad sizes. */
+typedef struct {
+  int n_g, n_p, n_t, n_planck;
+  const double *pressures, *temperatures, *sw_absorption, *sw_scattering, *lw_absorption, *planck_temperatures,
+      *planck, *irradiance_fraction;
+} orc_gas_optics;
+int orc_radiative_heating(int nx, int ny, int nlay, const double* dp, const double* pt, const double* ts,
+                          const double* xc, const double* yc, double ptop, double gravity,
+                          const orc_gas_optics* go, double sza, double surface_albedo,
+                          double surface_emissivity, double* net_flux, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

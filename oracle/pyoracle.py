@@ -55,6 +55,8 @@ def load(variant: str = 'portable'):
     lib.orc_set_remap_trace.argtypes = vp + [ctypes.POINTER(ctypes.c_int32)]
     lib.orc_pow_array.argtypes = [_P, ctypes.c_double, _P, ctypes.c_int]
     lib.orc_log_array.argtypes = [_P, _P, ctypes.c_int]
+    lib.orc_radiative_heating.argtypes = [ctypes.c_int] * 3 + [_P] * 5 + [ctypes.c_double] * 2 + \
+        [ctypes.c_void_p] + [ctypes.c_double] * 3 + [_P, ctypes.c_int]
     _libs[variant] = lib
     return lib
 
@@ -77,6 +79,7 @@ class OracleModel:
         if not self.s:
             raise ValueError('orc_create rejected the configuration')
         self.lib.orc_set_threads(self.s, threads)
+        self.threads, self.variant = threads, variant
         self.lib.orc_set_poison(self.s, int(poison))
         for f, a in ((DP, st.dp), (PT, st.pt), (UD, st.u), (VD, st.v)):
             self.set(f, a)
@@ -138,6 +141,19 @@ class OracleModel:
     def set_net_flux(self, nf_halo):
         self.set(NET_FLUX, nf_halo, halo=True)
 
+    # radiation (the stepper interface of run_model)
+    def set_radiation(self, go, xc, yc, threads=None, **params):
+        self._rad = (go, xc, yc, threads or self.threads, params)
+
+    def radiative_heating(self, time=0.0):
+        go, xc, yc, threads, params = self._rad
+        ts = self.get(TS)[0]
+        self._nf = radiative_heating(go, self.get(DP), self.get(PT), ts, xc, yc, float(self.st.ak[0]),
+                                     self.st.gravity, threads=threads, variant=self.variant, **params)
+
+    def radiation_halo(self):
+        self.set_net_flux(periodic_halo(self._nf))
+
     def check_stability(self):
         return bool(self.lib.orc_check_stability(self.s))
 
@@ -155,6 +171,47 @@ class OracleModel:
 
     def state(self):
         return {name: self.get(f) for name, f in (('dp', DP), ('pt', PT), ('ud', UD), ('vd', VD))}
+
+
+def periodic_halo(a):
+    """(K, ny, nx) interior -> (K, ny+14, nx+14) with the periodic halo
+    (the single-image halo_exchange, src/mod_sync.f90:67-217)."""
+    K, ny, nx = a.shape
+    iy = (np.arange(-HALO, ny + HALO)) % ny
+    ix = (np.arange(-HALO, nx + HALO)) % nx
+    return np.ascontiguousarray(a[:, iy][:, :, ix])
+
+
+class RadiationRangeError(ValueError):
+    """A layer pressure or temperature outside the gas-optics tables (the
+    reference stops there)."""
+
+
+def radiative_heating(go, dp, pt, ts, xc, yc, ptop, gravity, solar_zenith_angle=0.0,
+                      surface_albedo=float(np.float32(.3)), surface_emissivity=float(np.float32(.99)),
+                      threads=1, variant='portable'):
+    """calculate_radiative_heating of the oracle: net_flux (nlay+1, ny, nx)
+    from interior dp, pt (nlay, ny, nx), ts (ny, nx) and the cell axes."""
+    lib = load(variant)
+    nlay, ny, nx = dp.shape
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (dp, pt, ts, xc, yc)]
+    tabs = [np.ascontiguousarray(getattr(go, n), dtype=np.float64) for n in
+            ('pressures', 'temperatures', 'sw_absorption', 'sw_scattering', 'lw_absorption',
+             'planck_temperatures', 'planck', 'irradiance_fraction')]
+
+    class _GO(ctypes.Structure):
+        _fields_ = [('n_g', ctypes.c_int), ('n_p', ctypes.c_int), ('n_t', ctypes.c_int),
+                    ('n_planck', ctypes.c_int)] + [('p%d' % q, _P) for q in range(8)]
+    st = _GO(tabs[3].shape[0], tabs[0].shape[0], tabs[1].shape[1], tabs[5].shape[0], *[_ptr(t) for t in tabs])
+    out = np.zeros((nlay + 1, ny, nx))
+    rc = lib.orc_radiative_heating(nx, ny, nlay, *[_ptr(a) for a in arrs], float(ptop), float(gravity),
+                                   ctypes.cast(ctypes.byref(st), ctypes.c_void_p), float(solar_zenith_angle),
+                                   float(surface_albedo), float(surface_emissivity), _ptr(out), int(threads))
+    if rc == 1:
+        raise RadiationRangeError('a layer pressure or temperature is outside the gas-optics tables')
+    if rc:
+        raise ValueError('orc_radiative_heating rejected the sizes')
+    return out
 
 
 def pow_array(x, y, variant='portable'):

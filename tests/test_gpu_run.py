@@ -1,12 +1,13 @@
 """The run driver from the reference's files: namelist + initial file ->
 the CUDA library through the reference's time loop -> output.nc and the
 restart file.  The final state equals stepping the same initial state
-directly (bit for bit), and each output record is the interval mean."""
+directly (bit for bit, with the radiation when the package has its
+gas-optics tables), and each output record is the interval mean."""
 import numpy as np
 import pytest
 from scipy.io import netcdf_file
 
-from atmdyn import ic, Dycore, model
+from atmdyn import ic, Dycore, model, gas_optics
 from atmdyn.io import write_initial, read_initial
 from atmdyn.run import main
 
@@ -46,6 +47,10 @@ def test_run_from_reference_files(tmp_path):
     st2 = read_initial(str(tmp_path / 'init.nc'))
     st2.gravity, st2.coriolis, st2.divdamp, st2.vortdamp = 9.807, 1e-4, 0.15, 0.005
     g = Dycore(st2)
+    go = gas_optics.load_default()
+    assert summary['radiation'] == (go is not None)
+    if go is not None:
+        g.set_radiation(go)
     means = []
     acc = {'dp': 0.}
 
@@ -57,7 +62,7 @@ def test_run_from_reference_files(tmp_path):
 
     tc = model.TimeControl(dt_max=60.0, run_duration=600.0, dt_output=300.0, dt_radiation=10800.0,
                            dt_physics=300.0, dt_remap=240.0)
-    r = model.run_model(g, tc, on_step=on_step, physics=True)
+    r = model.run_model(g, tc, on_step=on_step, physics=True, radiation=go is not None)
     assert r.remap_steps == [4, 8]
     with netcdf_file(str(tmp_path / 'out' / 'restart.nc'), 'r', mmap=False) as nc:
         np.testing.assert_array_equal(nc.variables['dp'][:], g.get('dp'))
