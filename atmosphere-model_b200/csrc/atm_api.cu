@@ -1362,7 +1362,7 @@ int atm_physics_halo(atm_ctx* ctx) {
 int atm_set_gas_optics(atm_ctx* ctx, const atm_gas_optics* t) {
   if (!ctx || !t) return ATM_ERR_ARG;
   if (t->n_g < 1 || t->n_p < 2 || t->n_t < 2 || t->n_planck < 2 || t->n_g > 4096 || t->n_p > 4096 ||
-      t->n_t > 4096 || t->n_planck > 65536)
+      t->n_t > 255 || t->n_planck > 65536)
     return fail(ctx, ATM_ERR_ARG, "atm_set_gas_optics: table sizes out of range");
   const size_t ng = t->n_g, np = t->n_p, nt = t->n_t, npl = t->n_planck;
   const double* src[8] = {t->pressures,    t->temperatures, t->sw_absorption, t->sw_scattering,

@@ -37,31 +37,46 @@ __device__ __forceinline__ int first_not_below(const double* __restrict__ xs, in
   return lo;
 }
 
-// lookup_1d (mod_gas_optics.f90:4556-4579); outside the table the
-// reference stops (:4562-4566): the kernel flags it and returns NaN
-__device__ double lookup_1d(double x, const double* __restrict__ xs, const double* __restrict__ ys, int n,
-                            bool& bad) {
+// lookup_1d (mod_gas_optics.f90:4556-4579) split in two: the bracket
+// (where the reference's scan stops; outside the table the reference stops,
+// :4562-4566, and the kernel flags it) and the interpolation at a known
+// bracket.  The pressures, temperatures and level temperatures are the
+// same for every g-point, so each column finds its brackets once.
+__device__ __forceinline__ int bracket(double x, const double* __restrict__ xs, int n, bool& bad) {
   if (x < xs[0] || x > xs[n - 1] || x != x) {
     bad = true;
-    return __longlong_as_double(0x7ff8000000000000LL);
+    return 1;
   }
-  const int k = first_not_below(xs, n, x);
+  return first_not_below(xs, n, x);  // 0 only where x == xs[0], which interp_at returns exactly
+}
+__device__ __forceinline__ double interp_at(double x, const double* __restrict__ xs, const double* __restrict__ ys,
+                                            int k) {
   if (x == xs[k]) return ys[k];
   return (ys[k] * (xs[k - 1] - x) + ys[k - 1] * (x - xs[k])) / (xs[k - 1] - xs[k]);
 }
 
-// lookup_pT_table (mod_gas_optics.f90:4581-4609) for table[p][t] of one g-point
-__device__ double lookup_pt(const RadTables& tb, double p, double t, const double* __restrict__ table, bool& bad) {
+// lookup_pT_table (mod_gas_optics.f90:4581-4609): the brackets of one layer
+// packed as kp | kt1 << 16 | kt2 << 24 (pressure; temperature in rows kp
+// and kp - 1; kt2 unused when p is a grid pressure; atm_set_gas_optics
+// keeps n_p below 2^16 and n_t below 2^8)
+__device__ __forceinline__ unsigned bracket_pt(const RadTables& tb, double p, double t, bool& bad) {
   const int np = tb.np, nt = tb.nt;
   if (p < tb.pressures[0] || p > tb.pressures[np - 1] || p != p) {
     bad = true;
-    return __longlong_as_double(0x7ff8000000000000LL);
+    return 1u | 1u << 16 | 1u << 24;
   }
-  const int k = first_not_below(tb.pressures, np, p);
-  if (p == tb.pressures[k]) return lookup_1d(t, tb.temps + k * nt, table + k * nt, nt, bad);
-  const double t1 = lookup_1d(t, tb.temps + k * nt, table + k * nt, nt, bad);
-  const double t2 = lookup_1d(t, tb.temps + (k - 1) * nt, table + (k - 1) * nt, nt, bad);
-  return (t1 * (tb.pressures[k - 1] - p) + t2 * (p - tb.pressures[k])) / (tb.pressures[k - 1] - tb.pressures[k]);
+  const int kp = first_not_below(tb.pressures, np, p);
+  const int kt1 = bracket(t, tb.temps + kp * nt, nt, bad);
+  const int kt2 = p == tb.pressures[kp] ? 1 : bracket(t, tb.temps + (kp - 1) * nt, nt, bad);
+  return (unsigned)kp | (unsigned)kt1 << 16 | (unsigned)kt2 << 24;
+}
+__device__ __forceinline__ double lookup_pt_at(const RadTables& tb, double p, double t,
+                                               const double* __restrict__ table, unsigned code) {
+  const int nt = tb.nt, kp = code & 0xffff, kt1 = (code >> 16) & 0xff, kt2 = code >> 24;
+  const double t1 = interp_at(t, tb.temps + kp * nt, table + kp * nt, kt1);
+  if (p == tb.pressures[kp]) return t1;
+  const double t2 = interp_at(t, tb.temps + (kp - 1) * nt, table + (kp - 1) * nt, kt2);
+  return (t1 * (tb.pressures[kp - 1] - p) + t2 * (p - tb.pressures[kp])) / (tb.pressures[kp - 1] - tb.pressures[kp]);
 }
 
 // delta_eddington_rescaling (mod_radiation.f90:383-398)
@@ -81,19 +96,27 @@ struct Column {
   double beam[LM + 2];                                  // solar_beam
 };
 
-// calculate_fluxes (mod_radiation.f90:349-381): the upward sweep of albedo
-// and emission, then the downward sweep of the fluxes, each level's pair
-// handed to emit(k, flux_up, flux_dn) from the top down
+// calculate_fluxes (mod_radiation.f90:349-381) in two halves.  The upward
+// sweep (:357-363) at layer k: beta(k), albedo(k+1), emission_up(k+1), the
+// last two carried in registers; the longwave runs it inside its layer loop
+// (both go upward), so its upward sources are never stored.
+template <int LM>
+__device__ __forceinline__ void adding_up(Column<LM>& c, int k, double R, double T, double su, double sd,
+                                          double& alb, double& em) {
+  const double beta = 1. / (1. - R * alb);
+  const double alb1 = R + (T * T) * beta * alb;
+  const double em1 = su + T * beta * (em + sd * alb);
+  c.beta[k] = beta;
+  c.alb[k + 1] = alb1;
+  c.em[k + 1] = em1;
+  alb = alb1;
+  em = em1;
+}
+
+// the downward sweep (:365-380), each level's pair handed to
+// emit(k, flux_up, flux_dn) from the top down
 template <int LM, typename Emit>
-__device__ __forceinline__ void adding(Column<LM>& c, int L, double toa_dn, double sfc_up, double sfc_albedo,
-                                       Emit emit) {
-  c.alb[1] = sfc_albedo;
-  c.em[1] = sfc_up;
-  for (int k = 1; k <= L; ++k) {
-    c.beta[k] = 1. / (1. - c.R[k] * c.alb[k]);
-    c.alb[k + 1] = c.R[k] + (c.T[k] * c.T[k]) * c.beta[k] * c.alb[k];
-    c.em[k + 1] = c.su[k] + c.T[k] * c.beta[k] * (c.em[k] + c.sd[k] * c.alb[k]);
-  }
+__device__ __forceinline__ void adding_down(const Column<LM>& c, int L, double toa_dn, Emit emit) {
   double fdn = toa_dn;
   emit(L + 1, c.alb[L + 1] * toa_dn + c.em[L + 1], fdn);
   for (int k = L + 1; k >= 2; --k) {
@@ -107,12 +130,12 @@ __device__ __forceinline__ void adding(Column<LM>& c, int L, double toa_dn, doub
 // layer), then calculate_fluxes; the beam is added to the downward flux.
 template <int LM>
 __device__ void shortwave(const RadTables& tb, int g, int L, const double* play, const double* dm, const double* tlay,
-                          double irradiance, double mu0, double sfc_albedo, Column<LM>& c, double* up, double* dn,
-                          bool& bad) {
+                          const unsigned* code, double irradiance, double mu0, double sfc_albedo, Column<LM>& c,
+                          double* up, double* dn) {
   const double* tab = tb.sw_abs + (long long)g * tb.np * tb.nt;
   c.beam[L + 1] = mu0 * irradiance;
   for (int k = L; k >= 1; --k) {
-    const double k_abs = lookup_pt(tb, play[k], tlay[k], tab, bad);
+    const double k_abs = lookup_pt_at(tb, play[k], tlay[k], tab, code[k]);
     const double k_sca = tb.sw_sca[g];
     const double k_ext = k_abs + k_sca;
     double tau = k_ext * dm[k];
@@ -158,7 +181,11 @@ __device__ void shortwave(const RadTables& tb, int g, int L, const double* play,
     c.R[k] = tmp1 * gamma2 * (1. - e_2minus);
     c.T[k] = 2. * tmp1 * lambda * e_minus;
   }
-  adding(c, L, c.beam[L + 1], 0., sfc_albedo, [&](int k, double fu, double fd) {
+  double alb = sfc_albedo, em = 0.;
+  c.alb[1] = alb;
+  c.em[1] = em;
+  for (int k = 1; k <= L; ++k) adding_up(c, k, c.R[k], c.T[k], c.su[k], c.sd[k], alb, em);
+  adding_down(c, L, c.beam[L + 1], [&](int k, double fu, double fd) {
     up[k] = up[k] + fu;
     dn[k] = dn[k] + (fd + c.beam[k]);
   });
@@ -168,14 +195,17 @@ __device__ void shortwave(const RadTables& tb, int g, int L, const double* play,
 // scattering, a Planck source linear in optical depth
 template <int LM>
 __device__ void longwave(const RadTables& tb, int g, int L, const double* play, const double* dm, const double* tlay,
-                         const double* tlev, double ts, double emissivity, Column<LM>& c, double* up, double* dn,
-                         bool& bad) {
+                         const double* tlev, const unsigned* code, const int* kb, double ts, int kbs,
+                         double emissivity, Column<LM>& c, double* up, double* dn) {
   const double* tab = tb.lw_abs + (long long)g * tb.np * tb.nt;
   const double* plk = tb.plk + (long long)g * tb.npl;
-  const double surface_planckian = lookup_1d(ts, tb.plk_t, plk, tb.npl, bad);
-  double lp_k = lookup_1d(tlev[1], tb.plk_t, plk, tb.npl, bad);
+  const double surface_planckian = interp_at(ts, tb.plk_t, plk, kbs);
+  double lp_k = interp_at(tlev[1], tb.plk_t, plk, kb[1]);
+  double alb = 1. - emissivity, em = emissivity * PI_F * surface_planckian;  // calculate_fluxes' arguments (:345)
+  c.alb[1] = alb;
+  c.em[1] = em;
   for (int k = 1; k <= L; ++k) {
-    const double k_abs = lookup_pt(tb, play[k], tlay[k], tab, bad);
+    const double k_abs = lookup_pt_at(tb, play[k], tlay[k], tab, code[k]);
     const double k_sca = 0.;
     const double k_ext = k_abs + k_sca;
     double tau = k_ext * dm[k];
@@ -189,16 +219,20 @@ __device__ void longwave(const RadTables& tb, int g, int L, const double* play, 
     const double e_minus = atm_exp(-(lambda * tau));
     const double e_2minus = e_minus * e_minus;
     double tmp1 = 1. / (lambda + gamma1 + (lambda - gamma1) * e_2minus);
-    c.R[k] = tmp1 * gamma2 * (1. - e_2minus);
-    c.T[k] = 2. * tmp1 * lambda * e_minus;
-    const double lp_k1 = lookup_1d(tlev[k + 1], tb.plk_t, plk, tb.npl, bad);
-    const double pdiff = (1. + c.R[k] - c.T[k]) * (lp_k - lp_k1) / (tau * (gamma1 + gamma2));
-    tmp1 = 1. - c.R[k];
-    c.su[k] = PI_F * (tmp1 * lp_k1 - c.T[k] * lp_k + pdiff);
-    c.sd[k] = PI_F * (tmp1 * lp_k - c.T[k] * lp_k1 - pdiff);
+    const double R = tmp1 * gamma2 * (1. - e_2minus);
+    const double T = 2. * tmp1 * lambda * e_minus;
+    const double lp_k1 = interp_at(tlev[k + 1], tb.plk_t, plk, kb[k + 1]);
+    const double pdiff = (1. + R - T) * (lp_k - lp_k1) / (tau * (gamma1 + gamma2));
+    tmp1 = 1. - R;
+    const double su = PI_F * (tmp1 * lp_k1 - T * lp_k + pdiff);
+    const double sd = PI_F * (tmp1 * lp_k - T * lp_k1 - pdiff);
+    c.R[k] = R;
+    c.T[k] = T;
+    c.sd[k] = sd;
     lp_k = lp_k1;
+    adding_up(c, k, R, T, su, sd, alb, em);
   }
-  adding(c, L, 0., emissivity * PI_F * surface_planckian, 1. - emissivity, [&](int k, double fu, double fd) {
+  adding_down(c, L, 0., [&](int k, double fu, double fd) {
     up[k] = up[k] + fu;
     dn[k] = dn[k] + fd;
   });
@@ -214,7 +248,7 @@ __device__ void longwave(const RadTables& tb, int g, int L, const double* play, 
 // halo exchange that follows replaces: the interior is computed here and
 // atm_radiation_halo fills the halo.
 template <int LM>
-__global__ void __launch_bounds__(128) k_radiation(Geom g, RadTables tb, RadArgs a) {
+__global__ void __launch_bounds__(128, 8) k_radiation(Geom g, RadTables tb, RadArgs a) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= g.nx * g.ny) return;
   const int i = col % g.nx, j = col / g.nx;
@@ -254,12 +288,19 @@ __global__ void __launch_bounds__(128) k_radiation(Geom g, RadTables tb, RadArgs
   const double r = a.radius[col] / SOLAR_SCALE;
   const double irradiance = SOLAR_BASE * (1. + SOLAR_PEAK / (1. + r * r));
   const double ts = a.ts[o];
+  // the table brackets of every layer and level, shared by the g-points
   bool bad = false;
+  unsigned code[LM + 1];
+  int kb[LM + 2];
+  for (int k = 1; k <= L; ++k) code[k] = bracket_pt(tb, play[k], tlay[k], bad);
+  for (int k = 1; k <= L + 1; ++k) kb[k] = bracket(tlev[k], tb.plk_t, tb.npl, bad);
+  const int kbs = bracket(ts, tb.plk_t, tb.npl, bad);
   Column<LM> c;
-  for (int gp = 0; gp < tb.ng; ++gp) {
-    shortwave<LM>(tb, gp, L, play, dm, tlay, tb.frac[gp] * irradiance, a.mu0, a.albedo, c, usw, dsw, bad);
-    longwave<LM>(tb, gp, L, play, dm, tlay, tlev, ts, a.emissivity, c, ulw, dlw, bad);
-  }
+  if (!bad)
+    for (int gp = 0; gp < tb.ng; ++gp) {
+      shortwave<LM>(tb, gp, L, play, dm, tlay, code, tb.frac[gp] * irradiance, a.mu0, a.albedo, c, usw, dsw);
+      longwave<LM>(tb, gp, L, play, dm, tlay, tlev, code, kb, ts, kbs, a.emissivity, c, ulw, dlw);
+    }
   for (int k = 1; k <= L + 1; ++k) a.nf[o + (long long)(k - 1) * S] = (dsw[k] + dlw[k]) - (usw[k] + ulw[k]);
   if (bad) atomicOr(a.range_error, 1);
 }

@@ -16,7 +16,7 @@ and the hand-written adjoint back to the initial state, per (K cells x
 steps) / (forward + backward time).  Beside it: the FP64 and mixed forward
 forms (``forms``), the masked loss of the differentiation case and its
 finite-difference check (``adjoint``), the batched ensemble, the column
-physics, and CPU baselines of the reference algorithm (the FP64
+physics, the radiation, and CPU baselines of the reference algorithm (the FP64
 restatement: forward plus its tangent-linear model, which stands in for a
 reverse pass since the reference has no derivative code).
 
@@ -356,6 +356,7 @@ def run_ours(args):
     adjoint = None if args.no_adjoint else adjoint_leg(args, torch, max_over_ranks, world)
     ensemble = None if (args.no_ensemble or world > 1) else ensemble_leg(args, torch)
     physics = None if args.no_physics else physics_leg(args, torch, max_over_ranks, world, peak, peak_kind)
+    radiation = None if args.no_radiation else radiation_leg(args, torch, max_over_ranks, world)
 
     # error of the mixed form against the FP64 form after the same steps
     err = {}
@@ -406,6 +407,8 @@ def run_ours(args):
         line['ensemble'] = ensemble
     if physics is not None:
         line['physics'] = physics
+    if radiation is not None:
+        line['radiation'] = radiation
     if world == 1 and not args.no_cpu:
         line['cpu_baseline'] = cpu_baseline_lines(K, W)
     print(json.dumps(line), flush=True)
@@ -483,6 +486,84 @@ def physics_leg(args, torch, max_over_ranks, world, peak, peak_kind):
                                'sample': 'jet %dx%dx%d, %d calls after 1 warm-up' % (SAMPLE_N, SAMPLE_N,
                                                                                      args.nlay, n)}
     return out
+
+
+def radiation_leg(args, torch, max_over_ranks, world):
+    """The radiation (src/mod_radiation.f90, FP64) on the headline workload:
+    calculate_radiative_heating (k_radiation: per column the layer
+    temperatures, then 16 g-points of shortwave and longwave two-stream
+    solutions closed by the adding method) and the net-flux halo, timed with
+    CUDA events on the context's stream; the reference's tables when the
+    package build extracted them, else synthetic ones of the same shapes.
+    The FP64 restatement of the same routine runs on a 64 x 64 sample of
+    columns on one host core and on all of them."""
+    from atmdyn import ic, Dycore, gas_optics
+    go = gas_optics.load_default()
+    tables = 'reference (extracted)' if go is not None else 'synthetic'
+    go = go or gas_optics.synthetic(0)
+    st = ic.jet_case(args.nx, args.nx, args.nlay, 25e3, 25e3, seed=0)
+    st.ts = np.full((st.ny, st.nx), 288.0)
+    cols = st.nx * st.ny
+    dy = Dycore(st)
+    dy.set_radiation(go)
+    stream = torch.cuda.Stream()
+    dy.set_stream(stream.cuda_stream)
+    dy.radiative_heating()
+    torch.cuda.synchronize()
+    reps = 3
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    dy.profile(True)
+    e0.record(stream)
+    for _ in range(reps):
+        dy.radiative_heating()
+        dy.radiation_halo()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / reps
+    prof = dy.profile_read()
+    dy.profile(False)
+    dy.close()
+    del dy
+    torch.cuda.empty_cache()
+    kern = {k: {'ms_avg': round(t / c, 4), 'launches': c} for k, (t, c) in prof.items() if c}
+    ng = go.n_g
+    out = {'workload': 'jet %dx%dx%d, %d g-points, tables: %s; one call + net-flux halo' % (
+               args.nx, args.nx, args.nlay, ng, tables),
+           'ms_per_call': ms, 'columns_per_s': world * cols / (ms * 1e-3),
+           'layer_gpoints_per_s': world * cols * args.nlay * ng / (ms * 1e-3), 'kernels': kern}
+    if world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+        import pyoracle
+        n = 64
+        sm = ic.jet_case(n, n, args.nlay, 25e3, 25e3, seed=0)
+        ts = np.full((n, n), 288.0)
+        xc, yc = ic.cell_axes(sm)
+        threads = len(os.sched_getaffinity(0))
+        base = {}
+        for cores in sorted({1, threads}):
+            t0 = time.perf_counter()
+            pyoracle.radiative_heating(go, sm.dp, sm.pt, ts, xc, yc, sm.ak[0], sm.gravity, threads=cores)
+            base[cores] = n * n / (time.perf_counter() - t0)
+        out['cpu_baseline'] = [{'value': v, 'unit': 'columns/s', 'cores': c, 'kind': 'port',
+                                'sample': 'jet %dx%dx%d, one call' % (n, n, args.nlay)} for c, v in base.items()]
+    return out
+
+
+def probe_radiation(args):
+    """A small case for ncu captures of the radiation kernel (nothing is
+    timed here): a jet at nx x nx x nlay, three calls."""
+    import torch
+    torch.cuda.set_device(0)
+    from atmdyn import ic, Dycore, gas_optics
+    st = ic.jet_case(args.nx, args.nx, args.nlay, 25e3, 25e3, seed=0)
+    st.ts = np.full((st.ny, st.nx), 288.0)
+    dy = Dycore(st)
+    dy.set_radiation(gas_optics.load_default() or gas_optics.synthetic(0))
+    for _ in range(3):
+        dy.radiative_heating()
+    dy.close()
+    print('radiation probe done: %dx%dx%d' % (args.nx, args.nx, args.nlay))
 
 
 # Algorithmic HBM words per interior cell and launch of the adjoint
@@ -977,16 +1058,21 @@ def main():
     ap.add_argument('--no-ensemble', action='store_true', help='skip the batched-ensemble leg')
     ap.add_argument('--no-fdcheck', action='store_true', help='skip the differentiation case of the adjoint leg')
     ap.add_argument('--no-physics', action='store_true', help='skip the column-physics leg')
-    ap.add_argument('--probe', choices=['remap_adj', 'forward', 'adjoint'], default=None,
+    ap.add_argument('--no-radiation', action='store_true', help='skip the radiation leg')
+    ap.add_argument('--probe', choices=['remap_adj', 'forward', 'adjoint', 'radiation'], default=None,
                     help='profiling case instead of the benchmark, on a jet at --nx x --nx x --nlay: remap_adj = '
                          'two steps, then three calls of the remap adjoint with a dense random output adjoint; '
                          'forward = --warmup + --steps steps of each form in --forms (remap every 8); adjoint = '
-                         '--steps steps forward + adjoint of J = sum(theta^2) (checkpoints every 8)')
+                         '--steps steps forward + adjoint of J = sum(theta^2) (checkpoints every 8); radiation = '
+                         'three calls of the radiation')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.probe == 'remap_adj':
         probe_remap_adjoint(args)
+        return
+    if args.probe == 'radiation':
+        probe_radiation(args)
         return
     if args.probe in ('forward', 'adjoint'):
         probe_steps(args)

@@ -358,7 +358,7 @@ int atm_physics_halo(atm_ctx* ctx);
    that of mod_solar.f90:16-23).  atm_set_gas_optics copies them to the
    device (strictly ascending axes required). */
 typedef struct {
-  int n_g, n_p, n_t, n_planck;        /* 16, 53, 6, 231 in the reference */
+  int n_g, n_p, n_t, n_planck;        /* 16, 53, 6, 231 in the reference; n_t <= 255 */
   const double* pressures;            /* [n_p], Pa */
   const double* temperatures;         /* [n_p][n_t], K */
   const double* sw_absorption;        /* [n_g][n_p][n_t], m2/kg */
