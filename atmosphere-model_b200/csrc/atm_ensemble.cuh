@@ -228,9 +228,10 @@ template <typename S, int LM>
 __device__ __noinline__ void ens_rener(const EnsMember& M, int src, long long idx) {
   void* const* s = M.st[src];
   void* const* d = M.st[src ^ 1];
-  remap_energy_at<S, LM>(M.g, M.ra, (const S*)s[0], (const S*)s[1], (const S*)s[2], (const S*)s[3],
-                         (const S*)M.urem, (const S*)M.vrem, M.gz, (S*)d[0], (S*)d[1], (S*)d[2], (S*)d[3], nullptr,
-                         M.status, (int)idx);
+  // the persistent kernel serves the mixed form only (atm_ensemble_create)
+  remap_energy_at<S, LM, DevicePow>(M.g, M.ra, (const S*)s[0], (const S*)s[1], (const S*)s[2], (const S*)s[3],
+                                    (const S*)M.urem, (const S*)M.vrem, M.gz, (S*)d[0], (S*)d[1], (S*)d[2], (S*)d[3],
+                                    nullptr, M.status, (int)idx);
 }
 template <typename S, int LM>
 __device__ __forceinline__ void ens_remap(int stage, const EnsMember& M, int src, long long idx) {
@@ -252,12 +253,12 @@ __device__ __forceinline__ void ens_item(int stage, const EnsMember& M, int cur,
       else ens_sweep<T, S, C, 64>(stage, M, cur, li);
       break;
     case E_CCOL:
-      column_at<C>(g, M.cc, (const C*)M.cg[0], (const C*)M.cg[1], M.pkap, M.gz, -2, 2, nullptr,
+      column_at<C, FormPow<T>>(g, M.cc, (const C*)M.cg[0], (const C*)M.cg[1], M.pkap, M.gz, -2, 2, nullptr,
                    (int)(li * 32 + lane));
       break;
     case E_DCOL: {
       void* const* sn = M.st[cur ^ 1];
-      column_at<S>(g, M.cd, (const S*)sn[0], (const S*)sn[1], M.pkap, M.gz, -2, 2, nullptr, (int)(li * 32 + lane));
+      column_at<S, FormPow<T>>(g, M.cd, (const S*)sn[0], (const S*)sn[1], M.pkap, M.gz, -2, 2, nullptr, (int)(li * 32 + lane));
       break;
     }
     case E_DCORN:

@@ -137,10 +137,10 @@ cudaError_t column(const Geom& g, const Consts& c, const void* dpl, const void* 
                    int lo, int hi, double* plev, cudaStream_t s) {
   int n = (g.nx - lo + hi) * (g.ny - lo + hi);
   if (es == 8)
-    k_column<double><<<(n + 127) / 128, 128, 0, s>>>(g, c, (const double*)dpl, (const double*)ptl, pkap, gz, lo, hi,
+    k_column<double, FormPow<T>><<<(n + 127) / 128, 128, 0, s>>>(g, c, (const double*)dpl, (const double*)ptl, pkap, gz, lo, hi,
                                                      plev);
   else
-    k_column<float><<<(n + 127) / 128, 128, 0, s>>>(g, c, (const float*)dpl, (const float*)ptl, pkap, gz, lo, hi,
+    k_column<float, FormPow<T>><<<(n + 127) / 128, 128, 0, s>>>(g, c, (const float*)dpl, (const float*)ptl, pkap, gz, lo, hi,
                                                     plev);
   return cudaGetLastError();
 }
@@ -241,7 +241,7 @@ cudaError_t remap_energy_lm(const Geom& g, const RemapArgs& ra, const void* dp, 
                             const void* vd, const void* urem, const void* vrem, const double* gzs, void* dpo,
                             void* pto, void* udo, void* vdo, int* trace, Status* st, cudaStream_t s) {
   int n = g.nx * g.ny;
-  k_remap_energy<S, LM><<<(n + 63) / 64, 64, 0, s>>>(g, ra, (const S*)dp, (const S*)pt, (const S*)ud, (const S*)vd,
+  k_remap_energy<S, LM, FormPow<T>><<<(n + 63) / 64, 64, 0, s>>>(g, ra, (const S*)dp, (const S*)pt, (const S*)ud, (const S*)vd,
                                                      (const S*)urem, (const S*)vrem, gzs, (S*)dpo, (S*)pto, (S*)udo,
                                                      (S*)vdo, trace, st);
   return cudaGetLastError();
