@@ -39,7 +39,7 @@ EXPORTS = ('atm_create', 'atm_upload', 'atm_download', 'atm_init', 'atm_cgrid_st
            'atm_ensemble_run', 'atm_ensemble_status', 'atm_ensemble_blocks', 'atm_ensemble_destroy',
            'atm_ensemble_barrier_check', 'atm_ensemble_profile', 'atm_ensemble_stage_ms',
            'atm_ensemble_set_schedule', 'atm_set_gas_optics', 'atm_set_cell_coordinates',
-           'atm_radiative_heating', 'atm_radiation_halo')
+           'atm_radiative_heating', 'atm_radiation_halo', 'atm_device_kappa_pow')
 ATM_ADJ_IN, ATM_ADJ_OUT = 0, 1
 
 # the entry points every build must export
@@ -160,6 +160,7 @@ def load():
         'atm_set_cell_coordinates': ([vp, P, P], None),
         'atm_radiative_heating': ([vp, d, d, d, d], None),
         'atm_radiation_halo': ([vp], None),
+        'atm_device_kappa_pow': ([P, P, i], None),
     }
     for f, (args, res) in optional.items():
         if hasattr(lib, f):

@@ -804,6 +804,22 @@ int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_o
   return rc;
 }
 
+int atm_device_kappa_pow(const double* x, double* out, int n) {
+  if (n <= 0 || !x || !out) return ATM_ERR_ARG;
+  double *dx = nullptr, *dy = nullptr;
+  const size_t b = (size_t)n * 8;
+  if (cudaMalloc((void**)&dx, b) != cudaSuccess || cudaMalloc((void**)&dy, b) != cudaSuccess) {
+    cudaFree(dx); cudaFree(dy);
+    return ATM_ERR_NOMEM;
+  }
+  int rc = ATM_OK;
+  if (cudaMemcpy(dx, x, b, cudaMemcpyHostToDevice) != cudaSuccess || atm::device_kappa_pow(dx, dy, n, 0) != cudaSuccess ||
+      cudaMemcpy(out, dy, b, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = ATM_ERR_CUDA;
+  cudaFree(dx); cudaFree(dy);
+  return rc;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------- adjoint ----

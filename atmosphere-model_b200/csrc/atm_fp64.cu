@@ -5,12 +5,18 @@
 #define ATM_OPS_NAME ops_fp64
 #include "atm_launch.cuh"
 
+#ifndef ATM_CORNER_CHUNK
+#define ATM_CORNER_CHUNK 8
+#endif
+
 namespace atm {
 
 cudaError_t corners(const Geom& g, const double* pkap, const double* gz, double* pkapb, double* gzb, int with_pkap,
                     int lev0, int nlev, cudaStream_t s) {
   int n = (g.nx + 1) * (g.ny + 1);
-  k_corners<<<(n + 255) / 256, 256, 0, s>>>(g, pkap, gz, pkapb, gzb, with_pkap, lev0, nlev);
+  const int chunk = ATM_CORNER_CHUNK;
+  k_corners<<<dim3((n + 255) / 256, (nlev + chunk - 1) / chunk), 256, 0, s>>>(g, pkap, gz, pkapb, gzb, with_pkap,
+                                                                             lev0, nlev, chunk);
   return cudaGetLastError();
 }
 

@@ -12,6 +12,7 @@
 #include <type_traits>
 
 #include "atm_common.cuh"
+#include "atm_kappa_tables.h"
 
 namespace atm {
 
@@ -64,16 +65,37 @@ __device__ __forceinline__ bool finite_(float v) { return isfinite(v); }
 // independent once the running sum is formed, overlap.
 // plev**kappa and the log of a pkap ratio in the column and remap kernels.
 // PortablePow is atm_math.h's (bit-identical on host and device: the FP64
-// form and its oracle); DevicePow is the device library's exp(kappa log p)
-// and log, a few ulp from the exact value and cheaper (the mixed form,
-// whose error is its FP32 sweeps'; measured at 1024x1024x64: a column pass
-// 0.63 -> 0.45 ms, the energy remap 4.88 -> 4.62 ms).
+// form and its oracle).  DevicePow serves the mixed form, whose error is its
+// FP32 sweeps': p**kappa = 2^(kappa e) F_j**kappa (1 + r)**kappa from the
+// tables of atm_kappa_tables.h and a degree-7 binomial series (within 3 ulp;
+// outside p in [2^-126, 2^128) the device library's exp(kappa log p)) and the
+// device library's log.  Measured at 1024x1024x64: a column pass 0.63 ms
+// with the portable pow, 0.45 with exp(kappa log p).
 struct PortablePow {
-  __device__ static double pow(double x, double y) { return atm_pow(x, y); }
+  __device__ static double kappa(double x) { return atm_pow(x, KAPPA); }
   __device__ static double log(double x) { return atm_log(x); }
 };
+static_assert(KAPPA == ATM_KAP_KAPPA, "atm_kappa_tables.h was generated for another kappa");
+static __device__ const double d_kap_e[] = {ATM_KAP_E_VALUES};
+static __device__ const double d_kap_f[] = {ATM_KAP_F_VALUES};
+static __device__ const double d_kap_invf[] = {ATM_KAP_INVF_VALUES};
 struct DevicePow {
-  __device__ static double pow(double x, double y) { return ::exp(y * ::log(x)); }
+  __device__ static double kappa(double x) {
+    const long long b = __double_as_longlong(x);
+    const int e = (int)((b >> 52) & 0x7ff) - 1023;
+    if (b < 0 || e < ATM_KAP_E_FIRST || e > ATM_KAP_E_LAST) return ::exp(KAPPA * ::log(x));
+    const int j = (int)((b >> 45) & 127);
+    const double m = __longlong_as_double((b & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
+    const double r = m * __ldg(d_kap_invf + j) - 1.0;
+    double q = ::fma(r, ATM_KAP_C7, ATM_KAP_C6);
+    q = ::fma(r, q, ATM_KAP_C5);
+    q = ::fma(r, q, ATM_KAP_C4);
+    q = ::fma(r, q, ATM_KAP_C3);
+    q = ::fma(r, q, ATM_KAP_C2);
+    q = ::fma(r, q, ATM_KAP_C1);
+    const double t = __ldg(d_kap_e + (e - ATM_KAP_E_FIRST)) * __ldg(d_kap_f + j);
+    return ::fma(t, q * r, t);
+  }
   __device__ static double log(double x) { return ::log(x); }
 };
 // the one a form with sweep type T uses
@@ -103,7 +125,7 @@ __device__ __forceinline__ void column_at(const Geom& g, const Consts& c, const 
       if (k < 0) break;
       plev = plev + (double)dv[u];
       if (plev_out) plev_out[o + (long long)k * S] = plev;
-      pkap[o + (long long)k * S] = PW::pow(plev, KAPPA);
+      pkap[o + (long long)k * S] = PW::kappa(plev);
     }
   }
   double z = gz[o];
@@ -204,9 +226,15 @@ __device__ __forceinline__ void corner_at(const Geom& g, const double* pkap, con
   }
 }
 
+// blockIdx.y selects a chunk of `chunk` levels (8: 0.67 ms at 1024x1024x64,
+// against 0.72 / 0.67 / 0.68 / 0.73 at 1 / 4 / 16 / 64), so that more threads share
+// the levels' independent loads
 static __global__ void k_corners(Geom g, const double* __restrict__ pkap, const double* __restrict__ gz,
-                          double* __restrict__ pkapb, double* __restrict__ gzb, int with_pkap, int lev0, int nlev) {
-  corner_at(g, pkap, gz, pkapb, gzb, with_pkap, lev0, nlev, blockIdx.x * blockDim.x + threadIdx.x);
+                          double* __restrict__ pkapb, double* __restrict__ gzb, int with_pkap, int lev0, int nlev,
+                          int chunk) {
+  const int l0 = lev0 + blockIdx.y * chunk;
+  const int n = min(chunk, lev0 + nlev - l0);
+  if (n > 0) corner_at(g, pkap, gz, pkapb, gzb, with_pkap, l0, n, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // =============================================================== halos ====
@@ -755,7 +783,7 @@ __device__ __noinline__ void remap_energy_full(const Geom& g, const RemapArgs& r
   pk[L + 1] = ra.pk_top;
   for (int k = L; k >= 1; --k) {
     plev[k] = plev[k + 1] + (double)dp[o + (long long)(k - 1) * S];
-    pk[k] = PW::pow(plev[k], KAPPA);
+    pk[k] = PW::kappa(plev[k]);
     double plog = PW::log(pk[k + 1] / pk[k]);
     lyk[k] = (pk[k + 1] - pk[k]) / plog;
   }
@@ -763,7 +791,7 @@ __device__ __noinline__ void remap_energy_full(const Geom& g, const RemapArgs& r
   tpk[L + 1] = ra.pk_top;
   for (int k = L; k >= 1; --k) {
     tpl[k] = ra.ak[k - 1] + ra.bk[k - 1] * (plev[1] - ra.ptop);
-    tpk[k] = PW::pow(tpl[k], KAPPA);
+    tpk[k] = PW::kappa(tpl[k]);
     double plog = PW::log(tpk[k + 1] / tpk[k]);
     tlyk[k] = (tpk[k + 1] - tpk[k]) / plog;
   }
@@ -833,7 +861,7 @@ __device__ __forceinline__ void remap_energy_at(const Geom& g, const RemapArgs& 
     const double pn = pl + (double)dp[o + (long long)(k - 1) * S];
     mono = mono && (pl <= pn);
     plev[k] = pn;
-    pk[k] = PW::pow(pn, KAPPA);
+    pk[k] = PW::kappa(pn);
     pl = pn;
   }
   const double ps = pl;
@@ -875,12 +903,12 @@ __device__ __forceinline__ void remap_energy_at(const Geom& g, const RemapArgs& 
   // remapped energy -> potential temperature (:127-161), upward
   double gzr = gzs[o];
   double tpl0 = tpl(1);
-  double tpk0 = PW::pow(tpl0, KAPPA);
+  double tpk0 = PW::kappa(tpl0);
   bool bad = false;
   auto put = [&](int m, double erm) {
     const long long ok = o + (long long)(m - 1) * S;
     const double tpl1 = tpl(m + 1);
-    const double tpk1 = m < L ? PW::pow(tpl1, KAPPA) : ra.pk_top;
+    const double tpk1 = m < L ? PW::kappa(tpl1) : ra.pk_top;
     const double plog = PW::log(tpk1 / tpk0);
     const double tlyk = (tpk1 - tpk0) / plog;
     double ua = (.25 * ((double)urem[ok] + (double)urem[ok + P]) +

@@ -22,6 +22,17 @@ int ensemble_max_blocks() {
   return sms * per_sm;
 }
 
+static __global__ void k_kappa_pow(const double* x, double* out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = DevicePow::kappa(x[i]);
+}
+
+// p**kappa as the mixed form's column and remap kernels evaluate it
+cudaError_t device_kappa_pow(const double* x, double* out, int n, cudaStream_t s) {
+  k_kappa_pow<<<(n + 255) / 256, 256, 0, s>>>(x, out, n);
+  return cudaGetLastError();
+}
+
 cudaError_t ensemble_launch(const EnsPlan& plan, int blocks, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);

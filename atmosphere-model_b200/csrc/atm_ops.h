@@ -54,6 +54,8 @@ cudaError_t corners(const Geom&, const double* pkap, const double* gz, double* p
 
 // x**y and log(x) of the portable math on the device (tests)
 cudaError_t device_pow_log(const double* x, double y, double* p, double* l, int n, cudaStream_t);
+// p**kappa as the mixed form evaluates it (atm_mixed.cu)
+cudaError_t device_kappa_pow(const double* x, double* out, int n, cudaStream_t);
 
 // count of arguments where div_const<3>/<12> differs from IEEE division (tests)
 cudaError_t device_div_check(unsigned long long n, unsigned long long seed, unsigned long long* bad, cudaStream_t);

@@ -1,4 +1,5 @@
-"""Generate atm_math_tables.h: the constant tables of the portable log/exp.
+"""Generate atm_math_tables.h: the constant tables of the portable log/exp
+(and, with --kappa, atm_kappa_tables.h: those of the mixed form's p**kappa).
 
 The tables follow the table-driven method of P. T. P. Tang ("Table-driven
 implementation of the exponential function in IEEE floating-point
@@ -8,6 +9,15 @@ Every entry is computed here with Python's decimal module at 60 significant
 digits and rounded to nearest double, so the header is reproducible:
 
     python gen_math_tables.py > atm_math_tables.h
+    python gen_math_tables.py --kappa > atm_kappa_tables.h
+
+p**kappa for the fixed kappa = R_dry / cp_dry of the dynamical core (the
+double the C code computes, R_dry the single-precision literal
+287.052874): with p = 2^e m, m in [1, 2), and F_j = 1 + (2j + 1)/256 the
+midpoint of the j-th of 128 mantissa intervals, p**kappa = 2^(kappa e)
+F_j**kappa (1 + r)**kappa with r = m / F_j - 1, |r| < 1/256; the first two
+factors are tables (e in [-126, 127], j in [0, 128)), the third the
+binomial series to r^7 (truncation below 1e-18).
 """
 from decimal import Decimal, getcontext
 from fractions import Fraction
@@ -92,5 +102,32 @@ def main():
     print('\n'.join(out))
 
 
+def kappa_main():
+    r_dry = float(__import__('numpy').float32(287.052874))
+    kappa = r_dry / 1005.0  # the double the C code forms
+    k = Decimal(kappa)
+    ln2 = Decimal(2).ln()
+    out = ['// Generated by gen_math_tables.py --kappa; do not edit.', '#pragma once',
+           '#define ATM_KAP_E_FIRST (-126)', '#define ATM_KAP_E_LAST 127', '#define ATM_KAP_KAPPA %s' % h(kappa)]
+
+    def arr(name, vals):
+        body = ', \\\n  '.join(h(v) for v in vals)
+        return '#define %s \\\n  %s' % (name, body)
+    out.append(arr('ATM_KAP_E_VALUES', [dec_to_double((k * e * ln2).exp()) for e in range(-126, 128)]))
+    fs = [Fraction(256 + 2 * j + 1, 256) for j in range(128)]
+    out.append(arr('ATM_KAP_F_VALUES', [dec_to_double((k * (Decimal(f.numerator) / Decimal(f.denominator)).ln()).exp())
+                                        for f in fs]))
+    out.append(arr('ATM_KAP_INVF_VALUES', [float(1 / f) for f in fs]))
+    c = Decimal(1)
+    for n in range(1, 8):
+        c = c * (k - n + 1) / n  # binomial(kappa, n)
+        out.append('#define ATM_KAP_C%d %s' % (n, h(dec_to_double(c))))
+    print('\n'.join(out))
+
+
 if __name__ == '__main__':
-    main()
+    import sys
+    if '--kappa' in sys.argv:
+        kappa_main()
+    else:
+        main()

@@ -170,6 +170,10 @@ int atm_launch_count(atm_ctx* ctx, long long* n);
 /* the portable x**y and log(x) the FP64 form evaluates on the device, on n
    host values (accuracy and bit-identity tests) */
 int atm_device_pow_log(const double* x, double y, double* pow_out, double* log_out, int n);
+/* p**kappa (kappa = R_dry / cp_dry) as the mixed form's column and remap
+   kernels evaluate it on the device (a table method, within a few ulp), on n
+   host values (accuracy tests) */
+int atm_device_kappa_pow(const double* x, double* out, int n);
 
 /* ---- vertical remap without allocation (no counterpart in the reference) ----
    perform_vertical_remapping (src/mod_remap.f90:27-163) for callers that

@@ -68,3 +68,32 @@ def test_mixed_form_is_deterministic():
     for f in ('dp', 'pt', 'ud', 'vd'):
         np.testing.assert_array_equal(a[f], b[f], err_msg=f)
 
+
+
+def test_kappa_power_accuracy():
+    """p**kappa as the mixed form's column and remap kernels evaluate it
+    (the table method of atm_kappa_tables.h): within 3 ulp of the exact
+    power on pressures and on powers of two across the table's range;
+    outside it the device library's exp(kappa log p), finite and within
+    |kappa log p| ulp (up to 213 at the smallest subnormal)."""
+    import ctypes
+    from decimal import Decimal, getcontext
+    from fractions import Fraction
+    from atmdyn import _lib
+    lib = _lib.load()
+    getcontext().prec = 50
+    rng = np.random.default_rng(0)
+    x = np.concatenate([rng.uniform(1.0, 2.0e5, 3000), 2.0 ** rng.uniform(-125, 127, 1000),
+                        [1e-300, 5e-324, 1e300, 1.0, 2.0, 1e5]])
+    out = np.empty_like(x)
+    P = ctypes.POINTER(ctypes.c_double)
+    assert lib.atm_device_kappa_pow(x.ctypes.data_as(P), out.ctypes.data_as(P), x.size) == 0
+    kappa = float(np.float32(287.052874)) / 1005.0
+    worst = 0.0
+    for xi, yi in zip(x[:4000], out[:4000]):
+        ref = Fraction(Decimal(float(xi)) ** Decimal(kappa))
+        worst = max(worst, float(abs(Fraction(float(yi)) - ref) / Fraction(np.spacing(float(ref)))))
+    assert worst <= 3.0, worst
+    assert np.all(np.isfinite(out[4000:])) and np.all(out[4000:] > 0)
+    np.testing.assert_allclose(out[4000:], x[4000:] ** kappa, rtol=5e-14)
+

@@ -155,3 +155,16 @@ def test_recompute_stops_before_the_last_remap_only():
     dyn = _TapeRecorder()
     _record(dyn, 30.0, [False, False], like, final_state=False)
     assert dyn.calls == [False, False]
+
+
+def test_math_tables_reproducible():
+    """atm_math_tables.h and atm_kappa_tables.h are what their generator writes."""
+    import subprocess
+    import sys
+    import os
+    here = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'atmosphere-model_b200', 'csrc')
+    for args, name in (([], 'atm_math_tables.h'), (['--kappa'], 'atm_kappa_tables.h')):
+        got = subprocess.run([sys.executable, 'gen_math_tables.py'] + args, cwd=here, check=True,
+                             capture_output=True, text=True).stdout
+        with open(os.path.join(here, name)) as f:
+            assert got == f.read(), name
