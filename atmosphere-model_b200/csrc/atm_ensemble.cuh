@@ -221,7 +221,7 @@ __device__ __noinline__ void ens_rwind(const EnsMember& M, int src, long long id
   void* const* s = M.st[src];
   const long long wh = (long long)(g.nx + 2) * (g.ny + 2);
   if (idx >= 2 * wh) return;
-  remap_winds_at<S, LM>(g, M.ra, (const S*)s[0], (const S*)s[2], (const S*)s[3], (S*)M.urem, (S*)M.vrem, nullptr,
+  remap_winds_at<S, LM, float>(g, M.ra, (const S*)s[0], (const S*)s[2], (const S*)s[3], (S*)M.urem, (S*)M.vrem, nullptr,
                         M.status, (int)(idx % wh), (int)(idx / wh));
 }
 template <typename S, int LM>

@@ -481,18 +481,38 @@ __device__ void remap_column(PPMWork<LM>& w, int L, const double* src_var, doubl
 // all-arrays path.
 
 // One column array, element k at p[k * s].
-struct ColArr {
+// A column array of element type E read and written as doubles (k * s
+// apart).  The mixed form keeps the PPM interface values and elimination
+// coefficients of its wind remap in FP32 (half the local-memory traffic of
+// the thread's column arrays); every other column array is FP64.
+template <typename E>
+struct ColArrT {
+  E* p;
+  int s;
+  struct Ref {
+    E* q;
+    __device__ __forceinline__ operator double() const { return (double)*q; }
+    __device__ __forceinline__ Ref& operator=(double v) {
+      *q = (E)v;
+      return *this;
+    }
+  };
+  __device__ __forceinline__ Ref operator[](int k) const { return Ref{p + k * s}; }
+};
+template <>
+struct ColArrT<double> {
   double* p;
   int s;
   __device__ __forceinline__ double& operator[](int k) const { return p[k * s]; }
 };
+using ColArr = ColArrT<double>;
 
 // Elimination sweep of vertical_ppm in descending k.  cnext() yields
 // coord(L+1), coord(L), ..., coord(1) and vnext() var(L), ..., var(1), one
 // call each in that order.  Stores lv (before forward substitution) for
 // levels 1..L+1, gam for 1..L and, with STORE_SC, the coordinate.  L >= 3.
-template <bool STORE_SC, typename FC, typename FV>
-__device__ __forceinline__ void ppm_eliminate(int L, FC&& cnext, FV&& vnext, ColArr sc, ColArr lv, ColArr gam) {
+template <bool STORE_SC, typename FC, typename FV, typename LA = ColArr>
+__device__ __forceinline__ void ppm_eliminate(int L, FC&& cnext, FV&& vnext, ColArr sc, LA lv, LA gam) {
   double c2 = cnext(), c1 = cnext(), c0 = cnext();  // coord(k+1), coord(k), coord(k-1)
   if (STORE_SC) {
     sc[L + 1] = c2;
@@ -528,14 +548,14 @@ __device__ __forceinline__ void ppm_eliminate(int L, FC&& cnext, FV&& vnext, Col
 }
 
 // Layer k's edges and curvature in ascending k from the eliminated column.
-template <typename FV>
+template <typename FV, typename LA = ColArr>
 struct PPMLayers {
-  ColArr lv, gam;
+  LA lv, gam;
   int L;
   const FV& var;  // var(k), k = 1..L
   int k;
   double lvf, lvc, vk, vk1, top, btm, curv;
-  __device__ __forceinline__ PPMLayers(ColArr lv_, ColArr gam_, int L_, const FV& v)
+  __device__ __forceinline__ PPMLayers(LA lv_, LA gam_, int L_, const FV& v)
       : lv(lv_), gam(gam_), L(L_), var(v), k(0) {
     lvf = lv[1];
     lvc = lvf;
@@ -587,10 +607,10 @@ struct PPMLayers {
 // The pair loop as a monotone merge over the eliminated column: dst(m) for
 // m = 1..L in ascending order goes to put(m, value); dc(m) gives the
 // destination coordinate.  trace as in remap_column.
-template <typename FV, typename FD, typename FO>
-__device__ __forceinline__ void remap_merge(int L, ColArr sc, ColArr lv, ColArr gam, const FV& var, FD&& dc,
+template <typename FV, typename FD, typename FO, typename LA = ColArr>
+__device__ __forceinline__ void remap_merge(int L, ColArr sc, LA lv, LA gam, const FV& var, FD&& dc,
                                             FO&& put, int* trace, long long ts) {
-  PPMLayers<FV> ly(lv, gam, L, var);
+  PPMLayers<FV, LA> ly(lv, gam, L, var);
   int k0 = 1;
   double d0 = dc(1);
   for (int m = 1; m <= L; ++m) {
@@ -677,9 +697,10 @@ __device__ __noinline__ void remap_winds_full(const Geom& g, const RemapArgs& ra
 }
 
 // One thread per face column and direction (blockIdx.y); three column
-// arrays of LM + 2 doubles per thread.
+// arrays of LM + 2 per thread: the coordinate in FP64, the eliminated
+// interface values and coefficients in E (FP64, or FP32 in the mixed form).
 // face column col of direction dir (0: u, 1: v)
-template <typename T, int LM>
+template <typename T, int LM, typename E = double>
 __device__ __forceinline__ void remap_winds_at(const Geom& g, const RemapArgs& ra, const T* dp,
                                                const T* ud, const T* vd,
                                                T* urem, T* vrem, int* trace, Status* st,
@@ -693,8 +714,10 @@ __device__ __forceinline__ void remap_winds_at(const Geom& g, const RemapArgs& r
   T* r = dir == 0 ? urem : vrem;
   int* tr = nullptr;
   if (trace) tr = trace + ((long long)dir * h * w + (long long)(j + 1) * w + (i + 1)) * L * 5;  // [3][ny+2][nx+2][L][5]
-  double arr[3 * (LM + 2)];
-  const ColArr sc{arr, 1}, lv{arr + (LM + 2), 1}, gam{arr + 2 * (LM + 2), 1};
+  double sca[LM + 2];
+  E lva[LM + 2], gama[LM + 2];
+  const ColArr sc{sca, 1};
+  const ColArrT<E> lv{lva, 1}, gam{gama, 1};
   const long long oa = g.at(i, j);
   const long long ob = dir == 0 ? g.at(i, j - 1) : g.at(i - 1, j);
   const long long oc = dir == 0 ? g.at(i, j + 1) : g.at(i + 1, j);
@@ -755,12 +778,13 @@ __device__ __forceinline__ void remap_winds_at(const Geom& g, const RemapArgs& r
 // local memory either way): more columns in flight hide more of the local
 // memory latency (measured at 1024x1024x64: 4.67 ms against 5.88 at the
 // compiler's own budget, 5.34 at 24 blocks, 7.05 at 32).
-template <typename T, int LM>
+template <typename T, int LM, typename E = double>
 __global__ void __launch_bounds__(64, 16) k_remap_winds(Geom g, RemapArgs ra, const T* __restrict__ dp,
                                                     const T* __restrict__ ud, const T* __restrict__ vd,
                                                     T* __restrict__ urem, T* __restrict__ vrem, int* trace,
                                                     Status* st) {
-  remap_winds_at<T, LM>(g, ra, dp, ud, vd, urem, vrem, trace, st, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
+  remap_winds_at<T, LM, E>(g, ra, dp, ud, vd, urem, vrem, trace, st, blockIdx.x * blockDim.x + threadIdx.x,
+                           blockIdx.y);
 }
 
 // Energy remap and potential-temperature recovery on the interior,

@@ -232,7 +232,7 @@ template <int LM>
 cudaError_t remap_winds_lm(const Geom& g, const RemapArgs& ra, const void* dp, const void* ud, const void* vd,
                            void* urem, void* vrem, int* trace, Status* st, cudaStream_t s) {
   int n = (g.nx + 2) * (g.ny + 2);
-  k_remap_winds<S, LM><<<dim3((n + 63) / 64, 2), 64, 0, s>>>(g, ra, (const S*)dp, (const S*)ud, (const S*)vd, (S*)urem,
+  k_remap_winds<S, LM, T><<<dim3((n + 63) / 64, 2), 64, 0, s>>>(g, ra, (const S*)dp, (const S*)ud, (const S*)vd, (S*)urem,
                                                     (S*)vrem, trace, st);
   return cudaGetLastError();
 }
