@@ -3,8 +3,8 @@ restatement, bit for bit: net fluxes of one call at three layer counts
 (the kernel's 32-, 64- and 128-level instances) on the reference's tables
 and on synthetic ones, with noisy surface temperatures and cell axes off
 the origin; both forms; the net-flux halo; the table-range stop and the
-context after it; and whole runs with radiation and physics in the time
-loop."""
+context after it; whole runs with radiation and physics in the time
+loop; and sampled columns of the benchmark's 1024 x 1024 x 64 domain."""
 import numpy as np
 import pytest
 
@@ -133,3 +133,27 @@ def test_run_with_radiation_and_physics(precision):
         else:
             assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), n
     g.close()
+
+
+def test_full_size_sampled_columns():
+    """At the benchmark's size (jet 1024 x 1024 x 64, the reference's tables
+    when present): the net flux of 8 x 8 sampled columns (a sub-grid of the
+    domain, so that their cell axes are a subset of the domain's) is
+    bit-identical to the oracle's on the same columns."""
+    go = tables()[-1][1]
+    st = ic.jet_case(1024, 1024, 64, 25e3, 25e3, seed=0)
+    rng = np.random.default_rng(5)
+    st.ts = 288.0 + rng.normal(0, 2.0, (st.ny, st.nx))
+    xc, yc = ic.cell_axes(st)
+    dy = Dycore(st)
+    dy.set_radiation(go, xc, yc)
+    dy.radiative_heating()
+    nf = dy.get('net_flux')
+    ii = np.sort(rng.choice(st.nx, 8, replace=False))
+    jj = np.sort(rng.choice(st.ny, 8, replace=False))
+    dp, pt, ts = dy.get('dp'), dy.get('pt'), dy.get('ts')[0]
+    sub = np.ix_(jj, ii)
+    want = pyoracle.radiative_heating(go, dp[:, sub[0], sub[1]], pt[:, sub[0], sub[1]], ts[sub], xc[ii], yc[jj],
+                                      st.ak[0], st.gravity)
+    np.testing.assert_array_equal(nf[:, sub[0], sub[1]], want)
+    dy.close()
