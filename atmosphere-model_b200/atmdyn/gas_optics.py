@@ -110,9 +110,16 @@ def from_fortran(gas_optics_f90: str, solar_f90: str) -> GasOptics:
     mod_solar.f90 (the parameter arrays of mod_gas_optics.f90:25-132,
     143-1841, 1852-1857, 1870-3568, 3579-4549 and mod_solar.f90:16-23)."""
     with open(gas_optics_f90) as f:
-        a = _arrays(f.read())
+        go_text = f.read()
     with open(solar_f90) as f:
-        a.update(_arrays(f.read()))
+        solar_text = f.read()
+    return from_fortran_text(go_text, solar_text)
+
+
+def from_fortran_text(gas_optics_src: str, solar_src: str) -> GasOptics:
+    """:func:`from_fortran` on the two files' contents."""
+    a = _arrays(gas_optics_src)
+    a.update(_arrays(solar_src))
     missing = [n for n in _NAMES if n not in a]
     if missing:
         raise ValueError('arrays not found: %s' % ', '.join(missing))

@@ -17,12 +17,10 @@ KAPPA = ic.KAPPA
 F32 = lambda x: float(np.float32(x))  # noqa: E731
 
 
-def test_fortran_reader(tmp_path):
+def test_fortran_reader():
     """Default-real literals are rounded to single precision, d exponents
     and kind suffixes stay double; reshape order (t, p, g) -> [g][p][t];
     continuation lines and comments are skipped."""
-    src = tmp_path / 'mod_gas_optics.f90'
-    sol = tmp_path / 'mod_solar.f90'
     body = ['   real(rk), parameter :: pressures(n_pressures) = [ &',
             '      1.0e+00, 1.0e+05] ! Pa',
             '   real(rk), parameter :: &',
@@ -42,10 +40,9 @@ def test_fortran_reader(tmp_path):
              '      real(rk), parameter :: &',
              '         planckian_lut(n_planckian_temperatures, n_g_points) = reshape( &',
              '         [1., 2., 3., 4., 5., 6.], (/n_planckian_temperatures, n_g_points/))']
-    src.write_text('\n'.join(body) + '\n')
-    sol.write_text('   real(rk), parameter :: irradiance_fraction(n_g_points) = &\n'
-                   '                          [0.3, 0.7]\n')
-    go = gas_optics.from_fortran(str(src), str(sol))
+    solar = ('   real(rk), parameter :: irradiance_fraction(n_g_points) = &\n'
+             '                          [0.3, 0.7]\n')
+    go = gas_optics.from_fortran_text('\n'.join(body) + '\n', solar)
     assert go.sw_absorption.shape == (2, 2, 2) and go.planck.shape == (2, 3)
     assert go.sw_absorption[0, 0, 1] == F32(0.2) and go.sw_absorption[0, 1, 0] == F32(0.3)
     assert go.sw_absorption[1, 0, 0] == 0.5 and go.sw_absorption[1, 0, 1] == 0.6  # double literals
@@ -237,3 +234,40 @@ def test_portable_math_against_libm():
     scale = np.abs(a).max()
     assert np.abs(a - b).max() <= 1e-12 * scale
     assert np.all(np.isfinite(a))
+
+
+def test_gas_optics_struct_matches_header():
+    """The ctypes atm_gas_optics has the fields of include/atmdyn.h's struct,
+    in its order and with its types."""
+    import os
+    import re
+    import ctypes
+    from atmdyn import _lib
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with open(os.path.join(here, 'include', 'atmdyn.h')) as f:
+        h = f.read()
+    body = re.search(r'typedef struct \{(.*?)\} atm_gas_optics;', h, re.S).group(1)
+    decl = [(t.strip(), [n.strip(' *') for n in names.split(',')])
+            for t, names in re.findall(r'^\s*(int|const double\*)\s+([^;]+);', body, re.M)]
+    fields = [(n, t) for t, ns in decl for n in ns]
+    got = _lib.GasOpticsC._fields_
+    assert [n for n, _ in fields] == [n for n, _ in got]
+    for (n, t), (_, ct) in zip(fields, got):
+        assert (ct is ctypes.c_int) == (t == 'int'), n
+    go = gas_optics.synthetic(0)
+    st = _lib.gas_optics_struct(go)
+    assert (st.n_g, st.n_p, st.n_t, st.n_planck) == (16, 53, 6, 231)
+    assert ctypes.addressof(st.planck.contents) == go.planck.ctypes.data
+
+
+def test_gas_optics_validation():
+    """Tables with a descending axis or mismatched shapes are rejected."""
+    go = gas_optics.synthetic(0)
+    bad = gas_optics.GasOptics(**{f: getattr(go, f).copy() for f in go.__dataclass_fields__})
+    bad.pressures = bad.pressures[::-1].copy()
+    with pytest.raises(ValueError, match='ascending'):
+        bad.validate()
+    bad = gas_optics.GasOptics(**{f: getattr(go, f).copy() for f in go.__dataclass_fields__})
+    bad.planck = bad.planck[:, :-1]
+    with pytest.raises(ValueError, match='shape'):
+        bad.validate()
