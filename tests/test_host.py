@@ -101,6 +101,44 @@ def test_run_model_call_order_and_instability_exit():
     assert not r.stable and r.steps == 3
 
 
+class _PhysicsRadiationStepper(_CountingStepper):
+    def physics_tendencies(self):
+        self.calls.append(('pt',))
+
+    def apply_physics(self, dt):
+        self.calls.append(('pa', dt))
+
+    def physics_halo(self):
+        self.calls.append(('ph',))
+
+    def radiative_heating(self, time):
+        self.calls.append(('rad', time))
+
+    def radiation_halo(self):
+        self.calls.append(('radh',))
+
+
+def test_run_model_radiation_schedule():
+    """run_model (mod_model.f90:112-199) with radiation: radiative heating
+    and its halo at the first step and whenever dt_radiation has passed,
+    before the physics tendencies and the C-grid step of that step, at the
+    step's start time; none without radiation=True."""
+    tc = model.TimeControl(dt_max=60.0, run_duration=600.0, dt_radiation=240.0, dt_physics=120.0, dt_remap=300.0)
+    s = _PhysicsRadiationStepper()
+    r = model.run_model(s, tc, physics=True, radiation=True)
+    assert r.steps == 10 and r.stable
+    rad = [c[1] for c in s.calls if c[0] == 'rad']
+    assert rad == [0.0, 240.0, 480.0]
+    for t in rad:
+        i = s.calls.index(('rad', t))
+        assert s.calls[i + 1] == ('radh',)
+        assert s.calls[i + 2][0] in ('pt', 'c')  # then the physics tendencies when due, or the C-grid step
+    assert s.calls[:4] == [('rad', 0.0), ('radh',), ('pt',), ('c', 30.0)]
+    s = _PhysicsRadiationStepper()
+    model.run_model(s, tc, physics=True, radiation=False)
+    assert not any(c[0] in ('rad', 'radh') for c in s.calls)
+
+
 def test_initial_conditions_are_hydrostatic_and_seeded():
     a = ic.jet_case(32, 32, 8, 50e3, 50e3, width=200e3, seed=5)
     b = ic.jet_case(32, 32, 8, 50e3, 50e3, width=200e3, seed=5)
